@@ -1,0 +1,266 @@
+/*
+ * vc1cu.h - C ABI of the B200 (sm_100a) backend for libvc1's encoder-analysis hot path.
+ *
+ * The library (libvc1_b200/libvc1cu.so) replaces three pieces of libvc1 (v0.2.69):
+ *
+ *   1. the motion-compute backend interface that the Vulkan path implements
+ *      (src/vulkan_compute.h:26-60, class VulkanComputeContext), as vc1cu_open /
+ *      vc1cu_close / vc1cu_device_name / vc1cu_device_index / vc1cu_score_motion_batch /
+ *      vc1cu_counters / vc1cu_reset_counters;
+ *   2. one whole-picture motion-analysis core pass,
+ *      Vc1Encoder::analyze_p_picture_core (src/encoder_motion.cpp:47-442), as
+ *      vc1cu_analyze_p_core (host buffers) and vc1cu_core_passes (device-resident batch);
+ *   3. the forward 8x8/8x4/4x8/4x4 transform + scalar quantiser of a motion-compensated
+ *      prediction, forward_transform_residual_part + scalar_quantize_level
+ *      (src/encoder_transform.cpp:935-1045, :1067-1085), as vc1cu_forward_quant.
+ *
+ * Conventions: every function is extern "C", returns an int status (VC1CU_OK on
+ * success), never throws, and records a message retrievable with vc1cu_last_error().
+ * There is no CPU fallback: a CUDA failure is reported, not hidden. Motion vectors are
+ * quarter-pel int32 pairs laid out exactly like VulkanMotionCandidate
+ * (src/vulkan_compute.h:11-14). Costs are uint64 like the reference's CPU law.
+ * Frames are 8-bit 4:2:0 planes with tight strides (Y: width, U/V: width/2), the
+ * layout of libvc1::Frame (src/encoder_internal.h:68-71).
+ *
+ * A context is bound to one CUDA device and owns one CUDA stream; calls on one context
+ * are serialised by an internal mutex (the reference serialises its Vulkan context the
+ * same way, src/vulkan_compute.cpp:385).
+ */
+#ifndef VC1CU_H
+#define VC1CU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+enum {
+    VC1CU_OK = 0,
+    VC1CU_ERR_ARG = 1,         /* invalid argument (size, id, mode, null pointer) */
+    VC1CU_ERR_CUDA = 2,        /* a CUDA runtime call or kernel launch failed */
+    VC1CU_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up (wavefront dependency) */
+    VC1CU_ERR_OOM = 4,         /* device or pinned host allocation failed */
+    VC1CU_ERR_STATE = 5,       /* e.g. a frame id that was never uploaded */
+    VC1CU_ERR_UNSUPPORTED = 6  /* a configuration this backend does not implement */
+};
+
+typedef struct vc1cu_ctx vc1cu_ctx;
+
+/* Quarter-pel motion vector; same layout as VulkanMotionCandidate / Vc1Encoder::MotionVector. */
+typedef struct vc1cu_mv {
+    int32_t xq;
+    int32_t yq;
+} vc1cu_mv;
+
+/* VulkanMotionMetric (src/vulkan_compute.h:16). */
+enum { VC1CU_METRIC_SAD = 0, VC1CU_METRIC_SATD = 1 };
+
+/* Vc1Encoder::ProgressiveMvMode (src/encoder_internal.h:335). */
+enum {
+    VC1CU_MV_QPEL = 0,
+    VC1CU_MV_HPEL = 1,
+    VC1CU_MV_HPEL_BILINEAR = 2,
+    VC1CU_MV_MIXED = 3
+};
+
+/* Cost law for vc1cu_score_motion_batch_law. */
+enum {
+    VC1CU_LAW_SHADER = 0, /* exactly src/shaders/vulkan_motion_cost.comp: no legality gates */
+    VC1CU_LAW_CPU = 1     /* the CPU law of block_sad_motion / mb_sad (encoder_motion.cpp:2197-2933):
+                             hidden-padding and odd-half-pel candidates cost UINT64_MAX/4 */
+};
+
+/*
+ * The subset of libvc1::EncoderConfig (src/encoder_internal.h:223-315) that the analysis
+ * path reads. Field meanings and defaults follow vc1_param_default
+ * (src/encoder_api_helpers.cpp:27-52); vc1cu_params_default fills them.
+ * Only Advanced Profile progressive syntax is implemented.
+ */
+typedef struct vc1cu_params {
+    int32_t width;              /* even internal coding raster, EncoderConfig::width */
+    int32_t height;             /* EncoderConfig::height */
+    int32_t display_width;      /* 0 = width; EncoderConfig::display_width */
+    int32_t display_height;     /* 0 = height */
+    int32_t pqindex;            /* 1..31 */
+    int32_t halfqp;             /* HALFQP bit, 0/1 */
+    int32_t nonuniform;         /* 0 = uniform quantiser, 1 = non-uniform */
+    int32_t search_range;       /* motion_search_range, integer pixels, 0..1024 */
+    int32_t local_search_range; /* motion_local_search_range */
+    int32_t me_algorithm;       /* 0 = UMH, 1 = diamond (vc1_me_algorithm_e) */
+    int32_t me_quality;         /* 0 SAD, 1 RATE, 2 SATD (vc1_me_quality_e); RD is not implemented */
+    int32_t subpel;             /* subpixel_refinement */
+    int32_t fast_subpel;        /* fast_subpixel_refinement */
+    int32_t subpel_range;       /* subpixel_refinement_range, integer pixels */
+    int32_t long_range_mode;    /* vc1_long_range_search_mode_e */
+    int32_t rnd;                /* rndctrl */
+    int32_t disable_p_intra;    /* debug_disable_p_intra */
+    int32_t reserved0;
+    double distant_match_max_mae;  /* default 255.0 */
+    double inter_intra_threshold;  /* default 0.80 */
+} vc1cu_params;
+
+/*
+ * Per-macroblock result of one core pass (Vc1Encoder::PAnalysis, src/encoder_internal.h:346-370).
+ * For vc1cu_analyze_p_core these are HOST arrays of mbw*mbh entries (block_mvs: 4 per MB,
+ * raster order of the four luma blocks); any array pointer may be NULL to skip it.
+ * The scalar fields are written by the call.
+ */
+typedef struct vc1cu_panalysis {
+    vc1cu_mv* mvs;
+    vc1cu_mv* block_mvs;
+    uint8_t* use_4mv;
+    uint8_t* use_intra;
+    uint64_t* screen_sads;
+    double* inter_intra_cost_ratio;
+    double* distant_local_mae;
+    double* distant_candidate_mae;
+    uint8_t* distant_match_decision;
+    double mean_abs_residual;
+    double rate_complexity;
+    uint64_t motion_sad;
+    uint64_t moved_macroblocks;
+    uint64_t fractional_chroma_macroblocks;
+    uint64_t four_mv_macroblocks;
+    uint64_t intra_macroblocks;
+    int32_t global_dx;          /* whole-frame translation of the unseeded pass */
+    int32_t global_dy;
+    uint64_t global_full_sad;
+} vc1cu_panalysis;
+
+/* VulkanComputeCounters (src/vulkan_compute.h:18-24); device time instead of submit-wait. */
+typedef struct vc1cu_counters {
+    uint64_t dispatches;
+    uint64_t candidates;
+    uint64_t frame_uploads;
+    uint64_t frame_upload_bytes;
+    uint64_t submit_wait_nanoseconds;
+    uint64_t macroblocks_analysed;
+} vc1cu_counters;
+
+/* ---- context (VulkanComputeContext::create / device_name / device_index) ---------- */
+
+/* Replaces VulkanComputeContext::create (src/vulkan_compute.h:28-29). device = -1 picks
+ * the current CUDA device. */
+int vc1cu_open(int device, vc1cu_ctx** out);
+int vc1cu_close(vc1cu_ctx* ctx);
+/* VulkanComputeContext::device_name / device_index (src/vulkan_compute.h:35-36). */
+const char* vc1cu_device_name(const vc1cu_ctx* ctx);
+int vc1cu_device_index(const vc1cu_ctx* ctx);
+/* Message of the last failing call on this context (or of vc1cu_open when ctx is NULL). */
+const char* vc1cu_last_error(const vc1cu_ctx* ctx);
+/* VulkanComputeContext::counters / reset_counters (src/vulkan_compute.h:53-54). */
+int vc1cu_counters_get(const vc1cu_ctx* ctx, vc1cu_counters* out);
+int vc1cu_reset_counters(vc1cu_ctx* ctx);
+
+/* Fills the defaults of vc1_param_default for a width x height raster. */
+void vc1cu_params_default(vc1cu_params* p, int width, int height);
+
+/* ---- candidate scoring (VulkanComputeContext::score_motion_batch) ----------------- */
+
+/*
+ * Replaces VulkanComputeContext::score_motion_batch (src/vulkan_compute.h:42-51), with
+ * the shader's law (src/shaders/vulkan_motion_cost.comp:109-183): SAD at sample_stride
+ * (costs x stride^2) or 4x4 Hadamard SATD, VC-1 bicubic or bilinear interpolation with
+ * rounding control, clamped edge sampling. cur/ref are host luma planes; they are copied
+ * to the device when not already cached (key: pointer, size and a sampled fingerprint,
+ * as the Vulkan backend does, src/vulkan_compute.cpp:30-45, :194-231). costs has n entries.
+ * n == 0 is a no-op. Batches above 4,194,240 candidates are rejected like the reference.
+ */
+int vc1cu_score_motion_batch(vc1cu_ctx* ctx, const uint8_t* cur, const uint8_t* ref,
+                             int width, int height, int x0, int y0, int bw, int bh,
+                             int sample_stride, int bilinear, int rnd, int metric,
+                             const vc1cu_mv* candidates, size_t n, uint64_t* costs);
+
+/*
+ * Same, choosing the cost law. With VC1CU_LAW_CPU, p supplies the display raster and the
+ * results equal Vc1Encoder::block_sad_motion / block_satd_motion / mb_sad (the reference's
+ * scalar path; encoder_motion.cpp:2197-2285, :2286-2933, :2962-3042).
+ */
+int vc1cu_score_motion_batch_law(vc1cu_ctx* ctx, const vc1cu_params* p, int law,
+                                 const uint8_t* cur, const uint8_t* ref, int x0, int y0,
+                                 int bw, int bh, int sample_stride, int mode, int metric,
+                                 const vc1cu_mv* candidates, size_t n, uint64_t* costs);
+
+/* ---- frames resident in HBM ---------------------------------------------------------- */
+
+/* Copies one 4:2:0 frame (host planes, tight strides) into frame slot frame_id
+ * (0 <= frame_id < 4096). u/v may be NULL (chroma then reads as 128). */
+int vc1cu_upload_frame(vc1cu_ctx* ctx, int frame_id, const uint8_t* y, const uint8_t* u,
+                       const uint8_t* v, int width, int height);
+/* Reads a frame slot back (for tests). */
+int vc1cu_download_frame(vc1cu_ctx* ctx, int frame_id, uint8_t* y, uint8_t* u, uint8_t* v);
+
+/* ---- whole-picture core pass (Vc1Encoder::analyze_p_picture_core) ------------------ */
+
+/*
+ * One analyze_p_picture_core pass of cur_id against ref_id, synchronous, host outputs.
+ * mode: VC1CU_MV_*; allow_intra: the P-intra proxy (encoder_motion.cpp:387-414);
+ * seed_mvs: NULL for the unseeded pass (global search + UMH/diamond + staged refinement),
+ * else mbw*mbh host MVs of the shared qpel seed (encoder_motion.cpp:119-131). For a
+ * seeded pass, seed_distant (may be NULL) carries the seed pass's distant_* arrays, which
+ * the reference copies through unchanged (encoder_motion.cpp:100-104).
+ */
+int vc1cu_analyze_p_core(vc1cu_ctx* ctx, const vc1cu_params* p, int cur_id, int ref_id,
+                         int mode, int allow_intra, const vc1cu_mv* seed_mvs,
+                         const vc1cu_panalysis* seed_distant, vc1cu_panalysis* out);
+
+/*
+ * Device-resident batch form. Every pass in the batch is independent of the others; all
+ * of them run in ONE persistent launch fed by a macroblock-row work queue (wavefront
+ * order inside each picture). Results stay on the device in result slot out_slot
+ * (0 <= slot < 4096); a seeded pass names the slot of its seed. Asynchronous on the
+ * context's stream; vc1cu_synchronize waits for it.
+ */
+typedef struct vc1cu_pass {
+    int32_t cur_id;
+    int32_t ref_id;
+    int32_t mode;
+    int32_t allow_intra;
+    int32_t seed_slot;   /* -1 = unseeded */
+    int32_t out_slot;
+} vc1cu_pass;
+
+int vc1cu_core_passes(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_pass* passes, int n);
+/* Copies a result slot to host arrays (and the scalar totals). Synchronous. */
+int vc1cu_read_result(vc1cu_ctx* ctx, int slot, vc1cu_panalysis* out);
+int vc1cu_synchronize(vc1cu_ctx* ctx);
+
+/* ---- motion compensation + forward transform + quantisation ------------------------ */
+
+/*
+ * Builds the decoder-equivalent prediction of result slot mv_slot against ref_id into
+ * frame slot pred_id (luma via luma_mc_sample[_mode] for 1-MV / 4-MV, chroma via
+ * chroma_mc_sample with the 4-MV median chroma vector; motion_compensate_mb /
+ * motion_compensate_4mv, src/encoder_motion_compensation.cpp:474-600). Intra MBs are
+ * predicted with zero motion. Asynchronous.
+ */
+int vc1cu_motion_compensate(vc1cu_ctx* ctx, const vc1cu_params* p, int ref_id, int mv_slot,
+                            int mv_mode, int pred_id);
+
+/*
+ * Forward transform and scalar quantisation of src_id - pred_id for every macroblock's
+ * six 8x8 parents (Y0..Y3, U, V) and every transform type in type_mask
+ * (bit (t-1) for TransformType t: 1 = 8x8, 2 = 8x4, 3 = 4x8, 4 = 4x4). Bit-exact with
+ * quantize_inter_part at trellis 0 (src/encoder_transform.cpp:1087-1171 scalar branch).
+ * Output layout: [type][mb][parent][64]; for type t the 64 entries hold the partitions
+ * at the reference's storage (8x8 transposed, rectangles row-major with stride 8,
+ * partition p at its transform_part_geometry offset, src/encoder_transform.cpp:915-933).
+ * coeffs (double) and levels (int16) are HOST arrays of n_types*mbs*6*64 entries; either
+ * may be NULL. Synchronous.
+ */
+int vc1cu_forward_quant(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id,
+                        int type_mask, double* coeffs, int16_t* levels);
+
+/* Device-output form of vc1cu_forward_quant: d_coeffs/d_levels are device pointers
+ * (either may be NULL). Asynchronous on the context stream. */
+int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id,
+                               int type_mask, double* d_coeffs, int16_t* d_levels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VC1CU_H */

@@ -1,0 +1,142 @@
+"""ctypes mirror of include/vc1cu.h: parameter, motion-vector and result structures.
+
+The structures match the C declarations field for field; `Analysis` owns numpy arrays for
+one core pass's per-macroblock results (the layout of libvc1's Vc1Encoder::PAnalysis,
+src/encoder_internal.h:346-370) and exposes them to C through a `vc1cu_panalysis`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+VC1CU_OK = 0
+ERRORS = {1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_TIMEOUT", 4: "ERR_OOM", 5: "ERR_STATE", 6: "ERR_UNSUPPORTED"}
+
+METRIC_SAD, METRIC_SATD = 0, 1
+MV_QPEL, MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED = 0, 1, 2, 3
+MODES = (MV_QPEL, MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED)
+LAW_SHADER, LAW_CPU = 0, 1
+BAD_COST = (2**64 - 1) // 4
+
+
+class Mv(C.Structure):
+    _fields_ = [("xq", C.c_int32), ("yq", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32),
+        ("display_width", C.c_int32), ("display_height", C.c_int32),
+        ("pqindex", C.c_int32), ("halfqp", C.c_int32), ("nonuniform", C.c_int32),
+        ("search_range", C.c_int32), ("local_search_range", C.c_int32),
+        ("me_algorithm", C.c_int32), ("me_quality", C.c_int32),
+        ("subpel", C.c_int32), ("fast_subpel", C.c_int32), ("subpel_range", C.c_int32),
+        ("long_range_mode", C.c_int32), ("rnd", C.c_int32), ("disable_p_intra", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("distant_match_max_mae", C.c_double), ("inter_intra_threshold", C.c_double),
+    ]
+
+
+class PAnalysisC(C.Structure):
+    _fields_ = [
+        ("mvs", C.c_void_p), ("block_mvs", C.c_void_p), ("use_4mv", C.c_void_p),
+        ("use_intra", C.c_void_p), ("screen_sads", C.c_void_p),
+        ("inter_intra_cost_ratio", C.c_void_p), ("distant_local_mae", C.c_void_p),
+        ("distant_candidate_mae", C.c_void_p), ("distant_match_decision", C.c_void_p),
+        ("mean_abs_residual", C.c_double), ("rate_complexity", C.c_double),
+        ("motion_sad", C.c_uint64), ("moved_macroblocks", C.c_uint64),
+        ("fractional_chroma_macroblocks", C.c_uint64), ("four_mv_macroblocks", C.c_uint64),
+        ("intra_macroblocks", C.c_uint64),
+        ("global_dx", C.c_int32), ("global_dy", C.c_int32), ("global_full_sad", C.c_uint64),
+    ]
+
+
+class Counters(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("dispatches", "candidates", "frame_uploads",
+                                          "frame_upload_bytes", "submit_wait_nanoseconds",
+                                          "macroblocks_analysed")]
+
+
+def make_params(width: int, height: int, **kw) -> Params:
+    """Defaults of vc1_param_default (src/encoder_api_helpers.cpp:27-52) for the fields the
+    analysis path reads; `width`/`height` are the even internal coding raster."""
+    p = Params()
+    p.width, p.height = width, height
+    p.display_width, p.display_height = 0, 0
+    p.pqindex, p.halfqp, p.nonuniform = 8, 0, 0
+    p.search_range, p.local_search_range = 1024, 32
+    p.me_algorithm, p.me_quality = 0, 2
+    p.subpel, p.fast_subpel, p.subpel_range = 1, 0, 1024
+    p.long_range_mode, p.rnd, p.disable_p_intra = 0, 0, 0
+    p.distant_match_max_mae, p.inter_intra_threshold = 255.0, 0.80
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def params_dict(p: Params) -> dict:
+    return {f[0]: getattr(p, f[0]) for f in Params._fields_}
+
+
+def mbs_of(p: Params) -> tuple[int, int]:
+    return (p.width + 15) // 16, (p.height + 15) // 16
+
+
+@dataclass
+class Analysis:
+    """One core pass's results (host numpy arrays) plus picture totals."""
+    mvs: np.ndarray            # (mbs, 2) int32
+    block_mvs: np.ndarray      # (mbs, 4, 2) int32
+    use_4mv: np.ndarray        # (mbs,) uint8
+    use_intra: np.ndarray      # (mbs,) uint8
+    screen_sads: np.ndarray    # (mbs,) uint64
+    inter_intra_cost_ratio: np.ndarray  # (mbs,) float64
+    distant_local_mae: np.ndarray
+    distant_candidate_mae: np.ndarray
+    distant_match_decision: np.ndarray  # uint8
+    totals: dict
+
+    ARRAYS = ("mvs", "block_mvs", "use_4mv", "use_intra", "screen_sads", "inter_intra_cost_ratio",
+              "distant_local_mae", "distant_candidate_mae", "distant_match_decision")
+
+    @classmethod
+    def empty(cls, mbs: int) -> "Analysis":
+        return cls(
+            mvs=np.zeros((mbs, 2), np.int32), block_mvs=np.zeros((mbs, 4, 2), np.int32),
+            use_4mv=np.zeros(mbs, np.uint8), use_intra=np.zeros(mbs, np.uint8),
+            screen_sads=np.zeros(mbs, np.uint64), inter_intra_cost_ratio=np.zeros(mbs, np.float64),
+            distant_local_mae=np.zeros(mbs, np.float64), distant_candidate_mae=np.zeros(mbs, np.float64),
+            distant_match_decision=np.zeros(mbs, np.uint8), totals={})
+
+    def as_c(self) -> PAnalysisC:
+        s = PAnalysisC()
+        for name in self.ARRAYS:
+            setattr(s, name, getattr(self, name).ctypes.data)
+        return s
+
+    def take_totals(self, s: PAnalysisC) -> "Analysis":
+        self.totals = {f[0]: getattr(s, f[0]) for f in PAnalysisC._fields_[9:]}
+        return self
+
+    def equal(self, other: "Analysis") -> list[str]:
+        """Names of fields that differ (bit-exact comparison, doubles by bit pattern)."""
+        bad = []
+        for name in self.ARRAYS:
+            a, b = getattr(self, name), getattr(other, name)
+            if a.dtype == np.float64:
+                if not np.array_equal(a.view(np.uint64), b.view(np.uint64)):
+                    bad.append(name)
+            elif not np.array_equal(a, b):
+                bad.append(name)
+        for k, v in self.totals.items():
+            w = other.totals.get(k)
+            if isinstance(v, float):
+                if np.float64(v).view(np.uint64) != np.float64(w).view(np.uint64):
+                    bad.append(k)
+            elif v != w:
+                bad.append(k)
+        return bad

@@ -1,0 +1,320 @@
+"""ctypes bindings of the two CPU checkers (see oracle/__init__.py)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from libvc1_b200.abi import Analysis, Mv, PAnalysisC, Params, mbs_of
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_oracle", "libvc1oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvc1ref.so")
+P = C.POINTER(Params)
+u64, i32, vp = C.c_uint64, C.c_int, C.c_void_p
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class VoFrame(C.Structure):
+    _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("y", vp), ("u", vp), ("v", vp)]
+
+
+class Counts(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("int_sad_samples", "qpel1d_samples", "qpel2d_samples",
+                                          "bilinear_samples", "satd_tiles", "frame_sad_samples",
+                                          "xform_flops", "quant_coeffs", "macroblocks")]
+
+
+def _planes(frame):
+    y, u, v = frame
+    y = np.ascontiguousarray(y, np.uint8)
+    u = np.ascontiguousarray(u, np.uint8)
+    v = np.ascontiguousarray(v, np.uint8)
+    return y, u, v
+
+
+def _seed_ptr(seed):
+    if seed is None:
+        return None, None
+    s = np.ascontiguousarray(seed, np.int32).reshape(-1, 2)
+    return s, s.ctypes.data
+
+
+class Oracle:
+    """Our C restatement of the reference path."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle oracle`")
+        L = self.lib = C.CDLL(path)
+        L.vo_mb_sad.argtypes = [P, vp, vp, i32, i32, i32, i32, i32]
+        L.vo_mb_sad.restype = u64
+        L.vo_block_sad_qpel.argtypes = [P, vp, vp, i32, i32, i32, i32, i32, i32]
+        L.vo_block_sad_qpel.restype = u64
+        L.vo_block_sad_motion.argtypes = [P, vp, vp, i32, i32, i32, i32, i32, i32, i32]
+        L.vo_block_sad_motion.restype = u64
+        L.vo_block_satd_motion.argtypes = [P, vp, vp, i32, i32, i32, i32, i32, i32, i32]
+        L.vo_block_satd_motion.restype = u64
+        L.vo_frame_sad.argtypes = [vp, vp, i32, i32, i32]
+        L.vo_frame_sad.restype = u64
+        L.vo_shader_cost.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, i32, i32]
+        L.vo_shader_cost.restype = u64
+        L.vo_hidden_padding.argtypes = [P, i32, i32, i32, i32, i32, i32, i32, i32]
+        L.vo_predict_luma.argtypes = [P, vp, i32, i32, i32, i32, i32, i32, i32, vp, i32]
+        L.vo_global_motion.argtypes = [P, vp, vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(u64)]
+        L.vo_integer_motion.argtypes = [P, vp, vp, i32, i32, vp, i32, i32, i32, C.POINTER(i32),
+                                        C.POINTER(i32), C.POINTER(u64)]
+        L.vo_analyze_p_core.argtypes = [P, vp, vp, i32, i32, vp, C.POINTER(PAnalysisC), C.POINTER(PAnalysisC)]
+        L.vo_motion_compensate.argtypes = [P, vp, vp, vp, vp, i32, vp, vp, vp]
+        L.vo_forward_part.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, vp]
+        L.vo_quantize_level.argtypes = [P, C.c_double]
+        L.vo_forward_quant.argtypes = [P, vp, vp, i32, vp, vp]
+        L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
+        L.vo_counts_get.argtypes = [C.POINTER(Counts)]
+        self._keep = []
+
+    def frame(self, frame) -> VoFrame:
+        y, u, v = _planes(frame)
+        f = VoFrame(y.shape[1], y.shape[0], y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        f._arrays = (y, u, v)
+        return f
+
+    def _f(self, fr):
+        return C.byref(fr if isinstance(fr, VoFrame) else self.frame(fr))
+
+    def counts(self) -> dict:
+        c = Counts()
+        self.lib.vo_counts_get(C.byref(c))
+        return {f[0]: getattr(c, f[0]) for f in Counts._fields_}
+
+    def reset_counts(self):
+        self.lib.vo_counts_reset()
+
+    def mb_sad(self, p, cur, ref, mx, my, dx, dy, stride=1):
+        return self.lib.vo_mb_sad(C.byref(p), self._f(cur), self._f(ref), mx, my, dx, dy, stride)
+
+    def block_sad_qpel(self, p, cur, ref, x0, y0, bw, bh, xq, yq):
+        return self.lib.vo_block_sad_qpel(C.byref(p), self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq)
+
+    def block_sad_motion(self, p, cur, ref, x0, y0, bw, bh, xq, yq, mode):
+        return self.lib.vo_block_sad_motion(C.byref(p), self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq, mode)
+
+    def block_satd_motion(self, p, cur, ref, x0, y0, bw, bh, xq, yq, mode):
+        return self.lib.vo_block_satd_motion(C.byref(p), self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq, mode)
+
+    def frame_sad(self, cur, ref, dx, dy, stride=1):
+        return self.lib.vo_frame_sad(self._f(cur), self._f(ref), dx, dy, stride)
+
+    def shader_cost(self, cur, ref, x0, y0, bw, bh, stride, bilinear, rnd, metric, xq, yq):
+        return self.lib.vo_shader_cost(self._f(cur), self._f(ref), x0, y0, bw, bh, stride, bilinear, rnd,
+                                       metric, xq, yq)
+
+    def hidden(self, p, x0, y0, bw, bh, xq, yq, mode, chroma):
+        return bool(self.lib.vo_hidden_padding(C.byref(p), x0, y0, bw, bh, xq, yq, mode, chroma))
+
+    def predict_luma(self, p, ref, x0, y0, bw, bh, xq, yq, mode):
+        out = np.zeros((bh, bw), np.uint8)
+        self.lib.vo_predict_luma(C.byref(p), self._f(ref), x0, y0, bw, bh, xq, yq, mode, out.ctypes.data, bw)
+        return out
+
+    def global_motion(self, p, cur, ref, rng):
+        dx, dy, s = i32(), i32(), u64()
+        self.lib.vo_global_motion(C.byref(p), self._f(cur), self._f(ref), rng, C.byref(dx), C.byref(dy), C.byref(s))
+        return dx.value, dy.value, s.value
+
+    def integer_motion(self, p, cur, ref, mx, my, field, gdx, gdy, rng):
+        fld = np.ascontiguousarray(field, np.int32).reshape(-1, 2)
+        dx, dy, s = i32(), i32(), u64()
+        self.lib.vo_integer_motion(C.byref(p), self._f(cur), self._f(ref), mx, my, fld.ctypes.data, gdx, gdy, rng,
+                                   C.byref(dx), C.byref(dy), C.byref(s))
+        return dx.value, dy.value, s.value
+
+    def analyze_p_core(self, p, cur, ref, mode, allow_intra, seed=None, seed_distant: Analysis | None = None):
+        mbw, mbh = mbs_of(p)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        s, sp = _seed_ptr(seed)
+        sd = seed_distant.as_c() if seed_distant is not None else None
+        rc = self.lib.vo_analyze_p_core(C.byref(p), self._f(cur), self._f(ref), mode, int(allow_intra), sp,
+                                        C.byref(sd) if sd is not None else None, C.byref(oc))
+        if rc:
+            raise RuntimeError("oracle analyze_p_core failed")
+        return out.take_totals(oc)
+
+    def motion_compensate(self, p, ref, a: Analysis, mode):
+        h, w = p.height, p.width
+        y = np.zeros((h, w), np.uint8)
+        u = np.full((h // 2, w // 2), 128, np.uint8)
+        v = u.copy()
+        self.lib.vo_motion_compensate(C.byref(p), self._f(ref), a.mvs.ctypes.data, a.block_mvs.ctypes.data,
+                                      a.use_4mv.ctypes.data, mode, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def forward_quant(self, p, src, pred, type_mask=1):
+        mbw, mbh = mbs_of(p)
+        nt = bin(type_mask & 15).count("1")
+        co = np.zeros((nt, mbw * mbh, 6, 64), np.float64)
+        lv = np.zeros((nt, mbw * mbh, 6, 64), np.int16)
+        self.lib.vo_forward_quant(C.byref(p), self._f(src), self._f(pred), type_mask, co.ctypes.data, lv.ctypes.data)
+        return co, lv
+
+    def quantize_level(self, p, c):
+        return self.lib.vo_quantize_level(C.byref(p), c)
+
+    def score_key(self, sad, lam, rate, bits=64):
+        hi, lo = u64(), u64()
+        self.lib.vo_score_key(sad, lam, rate, bits, C.byref(hi), C.byref(lo))
+        return (hi.value << 64) | lo.value
+
+
+class RefFrame:
+    def __init__(self, lib, frame):
+        y, u, v = _planes(frame)
+        self._lib = lib
+        self.h = lib.ref_frame_new(y.ctypes.data, u.ctypes.data, v.ctypes.data, y.shape[1], y.shape[0])
+
+    def __del__(self):
+        try:
+            self._lib.ref_frame_free(self.h)
+        except Exception:
+            pass
+
+
+class Reference:
+    """The reference's own functions (compiled from its sources; scalar or SIMD-dispatched)."""
+
+    def __init__(self, p: Params, simd_auto: bool = False, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle ref`")
+        L = self.lib = C.CDLL(path)
+        L.ref_frame_new.argtypes = [vp, vp, vp, i32, i32]
+        L.ref_frame_new.restype = vp
+        L.ref_frame_free.argtypes = [vp]
+        L.ref_frame_read.argtypes = [vp, vp, vp, vp]
+        L.ref_encoder_new.argtypes = [P, i32]
+        L.ref_encoder_new.restype = vp
+        L.ref_encoder_free.argtypes = [vp]
+        for n in ("ref_block_sad_motion", "ref_block_satd_motion"):
+            getattr(L, n).argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, i32]
+            getattr(L, n).restype = u64
+        L.ref_block_sad_qpel.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32]
+        L.ref_block_sad_qpel.restype = u64
+        L.ref_mb_sad.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32]
+        L.ref_mb_sad.restype = u64
+        L.ref_frame_sad.argtypes = [vp, vp, vp, i32, i32, i32]
+        L.ref_frame_sad.restype = u64
+        L.ref_global_motion.argtypes = [vp, vp, vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(u64)]
+        L.ref_predict_luma.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, vp, i32]
+        L.ref_integer_motion.argtypes = [vp, vp, vp, i32, i32, vp, i32, i32, i32, C.POINTER(i32), C.POINTER(i32),
+                                         C.POINTER(u64)]
+        L.ref_analyze_p_core.argtypes = [vp, vp, vp, i32, i32, vp, C.POINTER(PAnalysisC), C.POINTER(PAnalysisC)]
+        L.ref_analyze_p_core.restype = i32
+        L.ref_analyze_p_picture.argtypes = [vp, vp, vp, C.POINTER(PAnalysisC), C.POINTER(i32), C.POINTER(i32)]
+        L.ref_analyze_p_picture.restype = i32
+        L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+        L.ref_forward_quant.argtypes = [vp, vp, vp, i32, vp, vp]
+        L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
+        L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
+        L.ref_bench_analysis.restype = u64
+        self.p = p
+        self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
+
+    def __del__(self):
+        try:
+            self.lib.ref_encoder_free(self.h)
+        except Exception:
+            pass
+
+    def frame(self, frame) -> RefFrame:
+        return RefFrame(self.lib, frame)
+
+    def _f(self, fr):
+        return (fr if isinstance(fr, RefFrame) else self.frame(fr)).h
+
+    def mb_sad(self, cur, ref, mx, my, dx, dy, stride=1):
+        return self.lib.ref_mb_sad(self.h, self._f(cur), self._f(ref), mx, my, dx, dy, stride)
+
+    def block_sad_qpel(self, cur, ref, x0, y0, bw, bh, xq, yq):
+        return self.lib.ref_block_sad_qpel(self.h, self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq)
+
+    def block_sad_motion(self, cur, ref, x0, y0, bw, bh, xq, yq, mode):
+        return self.lib.ref_block_sad_motion(self.h, self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq, mode)
+
+    def block_satd_motion(self, cur, ref, x0, y0, bw, bh, xq, yq, mode):
+        return self.lib.ref_block_satd_motion(self.h, self._f(cur), self._f(ref), x0, y0, bw, bh, xq, yq, mode)
+
+    def frame_sad(self, cur, ref, dx, dy, stride=1):
+        return self.lib.ref_frame_sad(self.h, self._f(cur), self._f(ref), dx, dy, stride)
+
+    def global_motion(self, cur, ref, rng):
+        dx, dy, s = i32(), i32(), u64()
+        self.lib.ref_global_motion(self.h, self._f(cur), self._f(ref), rng, C.byref(dx), C.byref(dy), C.byref(s))
+        return dx.value, dy.value, s.value
+
+    def predict_luma(self, ref, x0, y0, bw, bh, xq, yq, mode):
+        out = np.zeros((bh, bw), np.uint8)
+        self.lib.ref_predict_luma(self.h, self._f(ref), x0, y0, bw, bh, xq, yq, mode, out.ctypes.data, bw)
+        return out
+
+    def integer_motion(self, cur, ref, mx, my, field, gdx, gdy, rng):
+        fld = np.ascontiguousarray(field, np.int32).reshape(-1, 2)
+        dx, dy, s = i32(), i32(), u64()
+        self.lib.ref_integer_motion(self.h, self._f(cur), self._f(ref), mx, my, fld.ctypes.data, gdx, gdy, rng,
+                                    C.byref(dx), C.byref(dy), C.byref(s))
+        return dx.value, dy.value, s.value
+
+    def analyze_p_core(self, cur, ref, mode, allow_intra, seed=None, seed_distant: Analysis | None = None):
+        mbw, mbh = mbs_of(self.p)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        s, sp = _seed_ptr(seed)
+        sd = seed_distant.as_c() if seed_distant is not None else None
+        rc = self.lib.ref_analyze_p_core(self.h, self._f(cur), self._f(ref), mode, int(allow_intra), sp,
+                                         C.byref(sd) if sd is not None else None, C.byref(oc))
+        if rc:
+            raise RuntimeError("reference analyze_p_picture_core threw")
+        return out.take_totals(oc)
+
+    def analyze_p_picture(self, cur, ref):
+        mbw, mbh = mbs_of(self.p)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        mode, ic = i32(), i32()
+        rc = self.lib.ref_analyze_p_picture(self.h, self._f(cur), self._f(ref), C.byref(oc), C.byref(mode), C.byref(ic))
+        if rc:
+            raise RuntimeError("reference analyze_p_picture threw")
+        out.take_totals(oc)
+        return out, mode.value, bool(ic.value)
+
+    def motion_compensate(self, ref, a: Analysis, mode):
+        h, w = self.p.height, self.p.width
+        dst = self.frame((np.zeros((h, w), np.uint8), np.full((h // 2, w // 2), 128, np.uint8),
+                          np.full((h // 2, w // 2), 128, np.uint8)))
+        self.lib.ref_motion_compensate(self.h, self._f(ref), a.mvs.ctypes.data, a.block_mvs.ctypes.data,
+                                       a.use_4mv.ctypes.data, mode, dst.h)
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def forward_quant(self, src, pred, type_mask=1):
+        mbw, mbh = mbs_of(self.p)
+        nt = bin(type_mask & 15).count("1")
+        co = np.zeros((nt, mbw * mbh, 6, 64), np.float64)
+        lv = np.zeros((nt, mbw * mbh, 6, 64), np.int16)
+        self.lib.ref_forward_quant(self.h, self._f(src), self._f(pred), type_mask, co.ctypes.data, lv.ctypes.data)
+        return co, lv
+
+    def quantize_level(self, c):
+        return self.lib.ref_scalar_quantize_level(self.h, c)
+
+    def bench_analysis(self, pairs, threads):
+        """Wall ns of analyze_p_picture + choose_transform_mb over (cur, ref) RefFrame pairs."""
+        curs = (vp * len(pairs))(*[c.h for c, _ in pairs])
+        refs = (vp * len(pairs))(*[r.h for _, r in pairs])
+        return self.lib.ref_bench_analysis(self.h, curs, refs, len(pairs), threads)

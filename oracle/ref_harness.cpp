@@ -1,0 +1,335 @@
+// ref_harness.cpp - C entry points into the reference encoder's own analysis functions.
+//
+// Test infrastructure only: this file is compiled together with the reference's
+// unmodified sources (see Makefile) into oracle/_ref/libvc1ref.so. It lets the tests,
+// the oracle's self-check and bench.py's CPU baseline call the reference's scalar (or
+// SIMD-dispatched) code directly, the way the reference's white-box tests do
+// (tests/staged_motion_estimation.cpp, tests/vulkan_compute_runtime.cpp link vc1_static and
+// call Vc1Encoder members). Nothing in the product links this library.
+#include "encoder_internal.h"
+
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+#include "../include/vc1cu.h"
+
+using libvc1::EncoderConfig;
+using libvc1::Frame;
+using libvc1::Vc1Encoder;
+using MV = Vc1Encoder::MotionVector;
+using Mode = Vc1Encoder::ProgressiveMvMode;
+
+namespace {
+
+struct RefEncoder {
+    EncoderConfig cfg;
+    std::unique_ptr<Vc1Encoder> enc;
+};
+
+EncoderConfig make_config(const vc1cu_params* p, int simd) {
+    EncoderConfig c;
+    c.width = p->width;
+    c.height = p->height;
+    c.display_width = p->display_width > 0 ? p->display_width : p->width;
+    c.display_height = p->display_height > 0 ? p->display_height : p->height;
+    c.pqindex = p->pqindex;
+    c.halfqp = p->halfqp != 0;
+    c.quantizer_type = p->nonuniform ? libvc1::QuantizerType::NonUniform : libvc1::QuantizerType::Uniform;
+    c.motion_search_range = p->search_range;
+    c.motion_local_search_range = std::min(p->local_search_range, p->search_range);
+    c.me_algorithm = static_cast<vc1_me_algorithm_e>(p->me_algorithm);
+    c.me_quality = static_cast<vc1_me_quality_e>(p->me_quality);
+    c.subpixel_refinement = p->subpel != 0;
+    c.fast_subpixel_refinement = p->fast_subpel != 0;
+    c.subpixel_refinement_range = p->subpel_range;
+    c.long_range_search_mode = static_cast<vc1_long_range_search_mode_e>(p->long_range_mode);
+    c.distant_match_max_mae = p->distant_match_max_mae;
+    c.inter_intra_threshold = p->inter_intra_threshold;
+    c.rndctrl = p->rnd != 0;
+    c.debug_disable_p_intra = p->disable_p_intra != 0;
+    c.syntax = libvc1::StreamSyntax::Advanced;
+    c.trellis = 0;
+    c.adaptive_quality = false;
+    c.aq_strength = 0.0;
+    c.dquant = false;
+    if (simd) {
+        // --simd auto: per-primitive startup benchmark (encoder_core.cpp:3240-3243).
+        auto r = libvc1::auto_select_simd(true, true);
+        c.simd_dispatch = r.dispatch;
+    } else {
+        c.simd_dispatch.tier.fill(libvc1::SimdTier::None);
+    }
+    return c;
+}
+
+Mode to_mode(int m) { return static_cast<Mode>(m); }
+
+void fill_out(const Vc1Encoder::PAnalysis& a, vc1cu_panalysis* out) {
+    const size_t n = a.mvs.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (out->mvs) out->mvs[i] = {a.mvs[i].xq, a.mvs[i].yq};
+        if (out->block_mvs)
+            for (int k = 0; k < 4; ++k) out->block_mvs[i * 4 + k] = {a.block_mvs[i][k].xq, a.block_mvs[i][k].yq};
+        if (out->use_4mv) out->use_4mv[i] = a.use_4mv[i];
+        if (out->use_intra) out->use_intra[i] = a.use_intra[i];
+        if (out->screen_sads) out->screen_sads[i] = a.screen_sads[i];
+        if (out->inter_intra_cost_ratio) out->inter_intra_cost_ratio[i] = a.inter_intra_cost_ratio[i];
+        if (out->distant_local_mae) out->distant_local_mae[i] = a.distant_local_mae[i];
+        if (out->distant_candidate_mae) out->distant_candidate_mae[i] = a.distant_candidate_mae[i];
+        if (out->distant_match_decision) out->distant_match_decision[i] = a.distant_match_decision[i];
+    }
+    out->mean_abs_residual = a.mean_abs_residual;
+    out->rate_complexity = a.rate_complexity;
+    out->motion_sad = a.motion_sad;
+    out->moved_macroblocks = a.moved_macroblocks;
+    out->fractional_chroma_macroblocks = a.fractional_chroma_macroblocks;
+    out->four_mv_macroblocks = a.four_mv_macroblocks;
+    out->intra_macroblocks = a.intra_macroblocks;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ref_frame_new(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h) {
+    auto* f = new Frame;
+    f->width = w;
+    f->height = h;
+    const size_t ny = static_cast<size_t>(w) * h, nc = static_cast<size_t>(w / 2) * (h / 2);
+    f->y.assign(y, y + ny);
+    if (u) f->u.assign(u, u + nc); else f->u.assign(nc, 128);
+    if (v) f->v.assign(v, v + nc); else f->v.assign(nc, 128);
+    return f;
+}
+
+void ref_frame_free(void* f) { delete static_cast<Frame*>(f); }
+
+void ref_frame_read(void* fp, uint8_t* y, uint8_t* u, uint8_t* v) {
+    const Frame& f = *static_cast<Frame*>(fp);
+    if (y) std::memcpy(y, f.y.data(), f.y.size());
+    if (u) std::memcpy(u, f.u.data(), f.u.size());
+    if (v) std::memcpy(v, f.v.data(), f.v.size());
+}
+
+void* ref_encoder_new(const vc1cu_params* p, int simd_auto) {
+    auto* r = new RefEncoder;
+    r->cfg = make_config(p, simd_auto);
+    r->enc = std::make_unique<Vc1Encoder>(r->cfg);
+    return r;
+}
+
+void ref_encoder_free(void* h) { delete static_cast<RefEncoder*>(h); }
+
+static Vc1Encoder& E(void* h) { return *static_cast<RefEncoder*>(h)->enc; }
+static const Frame& F(void* f) { return *static_cast<Frame*>(f); }
+
+uint64_t ref_block_sad_motion(void* h, void* cur, void* ref, int x0, int y0, int bw, int bh,
+                              int xq, int yq, int mode) {
+    return E(h).block_sad_motion(F(cur), F(ref), x0, y0, bw, bh, MV{xq, yq}, to_mode(mode));
+}
+
+uint64_t ref_block_sad_qpel(void* h, void* cur, void* ref, int x0, int y0, int bw, int bh, int xq, int yq) {
+    return E(h).block_sad_qpel(F(cur), F(ref), x0, y0, bw, bh, MV{xq, yq});
+}
+
+uint64_t ref_block_satd_motion(void* h, void* cur, void* ref, int x0, int y0, int bw, int bh,
+                               int xq, int yq, int mode) {
+    return E(h).block_satd_motion(F(cur), F(ref), x0, y0, bw, bh, MV{xq, yq}, to_mode(mode));
+}
+
+uint64_t ref_mb_sad(void* h, void* cur, void* ref, int mx, int my, int dx, int dy, int stride) {
+    return E(h).mb_sad(F(cur), F(ref), mx, my, dx, dy, stride);
+}
+
+uint64_t ref_frame_sad(void* h, void* cur, void* ref, int dx, int dy, int stride) {
+    return E(h).frame_sad(F(cur), F(ref), dx, dy, stride);
+}
+
+void ref_global_motion(void* h, void* cur, void* ref, int range, int* dx, int* dy, uint64_t* sad) {
+    const auto g = E(h).global_motion_search(F(cur), F(ref), range);
+    *dx = g.dx;
+    *dy = g.dy;
+    *sad = g.full_sad;
+}
+
+void ref_predict_luma(void* h, void* ref, int x0, int y0, int bw, int bh, int xq, int yq, int mode,
+                      uint8_t* dst, int dst_stride) {
+    E(h).predict_luma_motion_block(dst, dst_stride, F(ref), x0, y0, bw, bh, MV{xq, yq}, to_mode(mode));
+}
+
+// Integer motion search of one MB, given the spatial predictor state of a whole-pass
+// MV field (mvs: mbw*mbh, the 1-MV field analyze_p_picture_core keeps).
+void ref_integer_motion(void* h, void* cur, void* ref, int mx, int my, const vc1cu_mv* field,
+                        int gdx, int gdy, int range, int* dx, int* dy, uint64_t* sad) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    std::vector<MV> mv(static_cast<size_t>(mbw) * mbh);
+    for (size_t i = 0; i < mv.size(); ++i) mv[i] = MV{field[i].xq, field[i].yq};
+    const auto pi = e.predictor_info(mv, mbw, mbh, mx, my);
+    Vc1Encoder::GlobalMotionResult g{gdx, gdy, 0};
+    const auto r = e.integer_motion_local(F(cur), F(ref), mx, my, pi, g, range);
+    *dx = r.dx;
+    *dy = r.dy;
+    *sad = r.full_sad;
+}
+
+int ref_analyze_p_core(void* h, void* cur, void* ref, int mode, int allow_intra, const vc1cu_mv* seed,
+                       const vc1cu_panalysis* seed_distant, vc1cu_panalysis* out) {
+    try {
+        auto& e = E(h);
+        const auto& c = static_cast<RefEncoder*>(h)->cfg;
+        const size_t mbs = static_cast<size_t>((c.width + 15) / 16) * ((c.height + 15) / 16);
+        Vc1Encoder::PAnalysis s;
+        if (seed) {
+            s.mvs.resize(mbs);
+            for (size_t i = 0; i < mbs; ++i) s.mvs[i] = MV{seed[i].xq, seed[i].yq};
+            s.distant_local_mae.assign(mbs, -1.0);
+            s.distant_candidate_mae.assign(mbs, -1.0);
+            s.distant_match_decision.assign(mbs, 0);
+            if (seed_distant) {
+                for (size_t i = 0; i < mbs; ++i) {
+                    if (seed_distant->distant_local_mae) s.distant_local_mae[i] = seed_distant->distant_local_mae[i];
+                    if (seed_distant->distant_candidate_mae) s.distant_candidate_mae[i] = seed_distant->distant_candidate_mae[i];
+                    if (seed_distant->distant_match_decision) s.distant_match_decision[i] = seed_distant->distant_match_decision[i];
+                }
+            }
+        }
+        const auto a = e.analyze_p_picture_core(F(cur), F(ref), to_mode(mode), allow_intra != 0, seed ? &s : nullptr);
+        fill_out(a, out);
+        if (!seed) {
+            const auto g = e.global_motion_search(F(cur), F(ref),
+                                                  std::min(c.motion_search_range, std::max(0, c.motion_local_search_range)));
+            out->global_dx = g.dx;
+            out->global_dy = g.dy;
+            out->global_full_sad = g.full_sad;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
+// decision, final pass, optional fade passes). Reports the chosen mode and IC state.
+int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {
+    try {
+        const auto a = E(h).analyze_p_picture(F(cur), F(ref));
+        fill_out(a, out);
+        *chosen_mode = static_cast<int>(a.mv_mode);
+        *ic_enabled = a.intensity.enabled ? 1 : 0;
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// Prediction of a PAnalysis-like MV field (motion_compensate_mb / _4mv), intra MBs at zero
+// motion, into dst (a frame handle of the same size).
+void ref_motion_compensate(void* h, void* ref, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs,
+                           const uint8_t* use_4mv, int mode, void* dst) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    Frame& d = *static_cast<Frame*>(dst);
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            if (use_4mv && use_4mv[pos]) {
+                std::array<MV, 4> four;
+                for (int k = 0; k < 4; ++k) four[k] = MV{block_mvs[pos * 4 + k].xq, block_mvs[pos * 4 + k].yq};
+                e.motion_compensate_4mv(d, F(ref), mx, my, four);
+            } else {
+                e.motion_compensate_mb(d, F(ref), mx, my, MV{mvs[pos].xq, mvs[pos].yq}, to_mode(mode));
+            }
+        }
+}
+
+// Forward transform + scalar quantisation (trellis off) of src - pred for all MBs, parents
+// and the transform types in type_mask. Layout [type][mb][parent][64] over the set bits.
+void ref_forward_quant(void* h, void* src, void* pred, int type_mask, double* coeffs, int16_t* levels) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const size_t mbs = static_cast<size_t>(mbw) * mbh;
+    const Frame& s = F(src);
+    const Frame& p = F(pred);
+    size_t ti = 0;
+    for (int t = 1; t <= 4; ++t) {
+        if (!(type_mask & (1 << (t - 1)))) continue;
+        const auto type = static_cast<Vc1Encoder::TransformType>(t);
+        for (int my = 0; my < mbh; ++my)
+            for (int mx = 0; mx < mbw; ++mx)
+                for (int k = 0; k < 6; ++k) {
+                    const bool chroma = k >= 4;
+                    const auto& sp = chroma ? (k == 4 ? s.u : s.v) : s.y;
+                    const auto& pp = chroma ? (k == 4 ? p.u : p.v) : p.y;
+                    const int w = chroma ? c.width / 2 : c.width, hh = chroma ? c.height / 2 : c.height;
+                    const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
+                    const size_t base = ((ti * mbs + static_cast<size_t>(my) * mbw + mx) * 6 + k) * 64;
+                    double cc[64] = {0};
+                    int16_t qq[64] = {0};
+                    for (int part = 0; part < Vc1Encoder::transform_part_count(type); ++part) {
+                        int ox, oy, bw, bh;
+                        Vc1Encoder::transform_part_geometry(type, part, ox, oy, bw, bh);
+                        const int px = bx * 8 + ox, py = by * 8 + oy;
+                        std::array<double, 64> co{};
+                        if (!(px >= w || py >= hh || px + bw <= 0 || py + bh <= 0))
+                            co = e.forward_transform_residual_part(sp, pp, w, hh, px, py, bw, bh);
+                        const auto q = e.quantize_inter_part(sp, pp, w, hh, px, py, bw, bh, false);
+                        for (int y = 0; y < bh; ++y)
+                            for (int x = 0; x < bw; ++x) {
+                                cc[(oy + y) * 8 + ox + x] = co[y * 8 + x];
+                                qq[(oy + y) * 8 + ox + x] = static_cast<int16_t>(q[y * 8 + x]);
+                            }
+                    }
+                    if (coeffs) std::memcpy(coeffs + base, cc, sizeof cc);
+                    if (levels) std::memcpy(levels + base, qq, sizeof qq);
+                }
+        ++ti;
+    }
+}
+
+int ref_scalar_quantize_level(void* h, double coeff) { return E(h).scalar_quantize_level(coeff); }
+
+// CPU baseline: analyze_p_picture + choose_transform_mb of the chosen prediction for every
+// MB of every (cur, ref) pair, one pair per worker thread at a time. Returns wall ns.
+uint64_t ref_bench_analysis(void* h, void** curs, void** refs, int n_pairs, int threads) {
+    auto* r = static_cast<RefEncoder*>(h);
+    const auto& c = r->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        Vc1Encoder enc(c);
+        Frame pred;
+        pred.width = c.width;
+        pred.height = c.height;
+        pred.y.assign(static_cast<size_t>(c.width) * c.height, 0);
+        pred.u.assign(static_cast<size_t>(c.width / 2) * (c.height / 2), 128);
+        pred.v = pred.u;
+        const int coding_set = 0;
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n_pairs) break;
+            const Frame& cur = F(curs[i]);
+            const Frame& ref = F(refs[i]);
+            const auto a = enc.analyze_p_picture(cur, ref);
+            for (int my = 0; my < mbh; ++my)
+                for (int mx = 0; mx < mbw; ++mx) {
+                    const size_t pos = static_cast<size_t>(my) * mbw + mx;
+                    if (a.use_4mv[pos]) enc.motion_compensate_4mv(pred, ref, mx, my, a.block_mvs[pos]);
+                    else enc.motion_compensate_mb(pred, ref, mx, my, a.mvs[pos], a.mv_mode);
+                    (void)enc.choose_transform_mb(cur, pred, mx, my, coding_set, true, c.pqindex, false);
+                }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+}
+
+}  // extern "C"

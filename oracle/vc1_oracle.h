@@ -1,0 +1,98 @@
+/*
+ * vc1_oracle.h - CPU restatement of libvc1's encoder-analysis hot path (TEST INFRASTRUCTURE).
+ *
+ * This is the checker, not the product: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py load it. Every function follows the reference
+ * (blenheimears/libvc1 v0.2.69) line for line in behaviour; the file:line it restates is
+ * cited beside each definition in vc1_oracle.c. Parity is pinned: tests/test_oracle_pin.py
+ * compares this oracle with the reference's own code compiled from its sources
+ * (oracle/_ref/libvc1ref.so) and with the reference's known-answer fixtures.
+ */
+#ifndef VC1_ORACLE_H
+#define VC1_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/vc1cu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A frame as the reference holds it: tight planes, Y width x height, U/V (w/2) x (h/2). */
+typedef struct vo_frame {
+    int32_t w, h;
+    const uint8_t* y;
+    const uint8_t* u;
+    const uint8_t* v;
+} vo_frame;
+
+/* Evaluation counters (the algorithmic op count of the roofline). */
+typedef struct vo_counts {
+    uint64_t int_sad_samples;     /* integer-MV SAD samples (mb_sad, integer qpel/bilinear) */
+    uint64_t qpel1d_samples;      /* one-axis bicubic samples */
+    uint64_t qpel2d_samples;      /* two-axis bicubic samples */
+    uint64_t bilinear_samples;    /* fractional bilinear samples */
+    uint64_t satd_tiles;          /* 4x4 Hadamard tiles */
+    uint64_t frame_sad_samples;   /* whole-frame SAD samples of the global search */
+    uint64_t xform_flops;         /* FP64 multiply+add of the forward transform */
+    uint64_t quant_coeffs;        /* scalar_quantize_level calls */
+    uint64_t macroblocks;         /* MBs analysed (one per MB per core pass) */
+} vo_counts;
+
+void vo_counts_reset(void);
+void vo_counts_get(vo_counts* out);
+
+/* primitives (CPU law; results equal the reference's scalar functions) */
+uint64_t vo_mb_sad(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int mx, int my,
+                   int dx, int dy, int stride);
+uint64_t vo_block_sad_qpel(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int x0,
+                           int y0, int bw, int bh, int xq, int yq);
+uint64_t vo_block_sad_motion(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int x0,
+                             int y0, int bw, int bh, int xq, int yq, int mode);
+uint64_t vo_block_satd_motion(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int x0,
+                              int y0, int bw, int bh, int xq, int yq, int mode);
+uint64_t vo_frame_sad(const vo_frame* cur, const vo_frame* ref, int dx, int dy, int stride);
+int vo_hidden_padding(const vc1cu_params* p, int x0, int y0, int bw, int bh, int xq, int yq, int mode,
+                      int chroma);
+/* shader law of src/shaders/vulkan_motion_cost.comp (no legality gates) */
+uint64_t vo_shader_cost(const vo_frame* cur, const vo_frame* ref, int x0, int y0, int bw, int bh,
+                        int sample_stride, int bilinear, int rnd, int metric, int xq, int yq);
+void vo_predict_luma(const vc1cu_params* p, const vo_frame* ref, int x0, int y0, int bw, int bh, int xq,
+                     int yq, int mode, uint8_t* dst, int dst_stride);
+
+/* searches */
+void vo_global_motion(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int range,
+                      int* dx, int* dy, uint64_t* sad);
+void vo_integer_motion(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int mx, int my,
+                       const vc1cu_mv* field, int gdx, int gdy, int range, int* dx, int* dy,
+                       uint64_t* sad);
+
+/* whole core pass; seed NULL = unseeded */
+int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int mode,
+                      int allow_intra, const vc1cu_mv* seed, const vc1cu_panalysis* seed_distant,
+                      vc1cu_panalysis* out);
+
+/* prediction of an MV field (motion_compensate_mb / _4mv); dst planes tight */
+void vo_motion_compensate(const vc1cu_params* p, const vo_frame* ref, const vc1cu_mv* mvs,
+                          const vc1cu_mv* block_mvs, const uint8_t* use_4mv, int mode, uint8_t* dy,
+                          uint8_t* du, uint8_t* dv);
+
+/* transform + quantiser */
+void vo_forward_part(const uint8_t* src, const uint8_t* pred, int w, int h, int x0, int y0, int bw,
+                     int bh, double out[64]);
+int vo_quantize_level(const vc1cu_params* p, double coeff);
+void vo_forward_quant(const vc1cu_params* p, const vo_frame* src, const vo_frame* pred, int type_mask,
+                      double* coeffs, int16_t* levels);
+
+/* x87 extended-precision score emulation used by the GPU path, exposed for checking:
+ * the long double value of sad + lambda*rate, as an integer scaled by 2^shift
+ * (see vo_score_key in vc1_oracle.c). */
+void vo_score_key(uint64_t sad, double lambda, uint64_t rate, int mant_bits, uint64_t* hi, uint64_t* lo);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
