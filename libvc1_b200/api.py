@@ -1,0 +1,239 @@
+"""Host-side mirror of libvc1's motion-compute backend interface over the vc1cu C ABI.
+
+`CudaComputeContext` has the shape of libvc1's VulkanComputeContext
+(src/vulkan_compute.h:26-60): create / device_name / device_index / score_motion_batch /
+counters / reset_counters, with the same argument meaning and the same error behaviour
+(`score_motion_batch` returns False plus an error string on a recoverable failure; `create`
+returns None plus an error string). On top of that interface it exposes the whole-picture
+analysis path that the C ABI adds: frames resident in HBM, `analyze_p_core` (one
+Vc1Encoder::analyze_p_picture_core pass, src/encoder_motion.cpp:47-442), batched
+`core_passes`, `motion_compensate` and `forward_quant`.
+
+There is no CPU fallback: the library must load (libvc1_b200/libvc1cu.so, built by
+__graft_entry__.build()) and every device failure is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (Analysis, Counters, ERRORS, MV_QPEL, METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params,
+                  mbs_of)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
+_LIB = None
+
+# Every entry point declared in include/vc1cu.h.
+EXPORTS = (
+    "vc1cu_open", "vc1cu_close", "vc1cu_device_name", "vc1cu_device_index", "vc1cu_last_error",
+    "vc1cu_counters_get", "vc1cu_reset_counters", "vc1cu_params_default", "vc1cu_score_motion_batch",
+    "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
+    "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
+    "vc1cu_forward_quant", "vc1cu_forward_quant_device",
+)
+
+
+class Pass(C.Structure):
+    _fields_ = [("cur_id", C.c_int32), ("ref_id", C.c_int32), ("mode", C.c_int32), ("allow_intra", C.c_int32),
+                ("seed_slot", C.c_int32), ("out_slot", C.c_int32)]
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libvc1cu.so and declares its C signatures (no device work)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: the CUDA backend must be built (__graft_entry__.build())")
+    L = C.CDLL(path)
+    vp, i32, sz = C.c_void_p, C.c_int, C.c_size_t
+    PP = C.POINTER(Params)
+    L.vc1cu_open.argtypes = [i32, C.POINTER(vp)]
+    L.vc1cu_close.argtypes = [vp]
+    L.vc1cu_device_name.argtypes = [vp]
+    L.vc1cu_device_name.restype = C.c_char_p
+    L.vc1cu_device_index.argtypes = [vp]
+    L.vc1cu_last_error.argtypes = [vp]
+    L.vc1cu_last_error.restype = C.c_char_p
+    L.vc1cu_counters_get.argtypes = [vp, C.POINTER(Counters)]
+    L.vc1cu_reset_counters.argtypes = [vp]
+    L.vc1cu_params_default.argtypes = [PP, i32, i32]
+    L.vc1cu_params_default.restype = None
+    L.vc1cu_score_motion_batch.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, i32, i32, vp, sz, vp]
+    L.vc1cu_score_motion_batch_law.argtypes = [vp, PP, i32, vp, vp, i32, i32, i32, i32, i32, i32, i32, vp, sz, vp]
+    L.vc1cu_upload_frame.argtypes = [vp, i32, vp, vp, vp, i32, i32]
+    L.vc1cu_download_frame.argtypes = [vp, i32, vp, vp, vp]
+    L.vc1cu_analyze_p_core.argtypes = [vp, PP, i32, i32, i32, i32, vp, C.POINTER(PAnalysisC), C.POINTER(PAnalysisC)]
+    L.vc1cu_core_passes.argtypes = [vp, PP, C.POINTER(Pass), i32]
+    L.vc1cu_read_result.argtypes = [vp, i32, C.POINTER(PAnalysisC)]
+    L.vc1cu_synchronize.argtypes = [vp]
+    L.vc1cu_motion_compensate.argtypes = [vp, PP, i32, i32, i32, i32]
+    L.vc1cu_forward_quant.argtypes = [vp, PP, i32, i32, i32, vp, vp]
+    L.vc1cu_forward_quant_device.argtypes = [vp, PP, i32, i32, i32, vp, vp]
+    for name in EXPORTS:
+        getattr(L, name)  # AttributeError if the library lacks a declared entry point
+    _LIB = L
+    return L
+
+
+class Vc1cuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _u8(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+class CudaComputeContext:
+    """VulkanComputeContext's shape over the CUDA backend (one context per device)."""
+
+    def __init__(self, handle, lib):
+        self._h = handle
+        self._L = lib
+
+    # --- VulkanComputeContext::create / device_name / device_index -----------------------
+    @staticmethod
+    def create(requested_device: int = -1):
+        """Returns (context, "") or (None, error) like VulkanComputeContext::create."""
+        L = load_library()
+        h = C.c_void_p()
+        rc = L.vc1cu_open(requested_device, C.byref(h))
+        if rc:
+            return None, L.vc1cu_last_error(None).decode()
+        return CudaComputeContext(h, L), ""
+
+    def close(self):
+        if self._h:
+            self._L.vc1cu_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_name(self) -> str:
+        return self._L.vc1cu_device_name(self._h).decode()
+
+    def device_index(self) -> int:
+        return self._L.vc1cu_device_index(self._h)
+
+    def last_error(self) -> str:
+        return self._L.vc1cu_last_error(self._h).decode()
+
+    def _check(self, rc):
+        if rc:
+            raise Vc1cuError(rc, self.last_error())
+
+    # --- VulkanComputeContext::score_motion_batch ----------------------------------------
+    def score_motion_batch(self, cur, ref, width, height, x0, y0, bw, bh, sample_stride, bilinear, rnd, metric,
+                           candidates):
+        """Returns (ok, costs, error) with the semantics of score_motion_batch
+        (src/vulkan_compute.h:42-51): costs are uint64 per candidate."""
+        cand = np.ascontiguousarray(candidates, np.int32).reshape(-1, 2)
+        costs = np.zeros(len(cand), np.uint64)
+        cur, ref = _u8(cur), _u8(ref)
+        rc = self._L.vc1cu_score_motion_batch(self._h, cur.ctypes.data, ref.ctypes.data, width, height, x0, y0, bw, bh,
+                                             sample_stride, int(bilinear), int(rnd), metric, cand.ctypes.data,
+                                             len(cand), costs.ctypes.data)
+        if rc:
+            return False, np.zeros(0, np.uint64), self.last_error()
+        return True, costs, ""
+
+    def score_motion_batch_law(self, params: Params, law, cur, ref, x0, y0, bw, bh, sample_stride, mode, metric,
+                               candidates):
+        cand = np.ascontiguousarray(candidates, np.int32).reshape(-1, 2)
+        costs = np.zeros(len(cand), np.uint64)
+        cur, ref = _u8(cur), _u8(ref)
+        self._check(self._L.vc1cu_score_motion_batch_law(self._h, C.byref(params), law, cur.ctypes.data,
+                                                         ref.ctypes.data, x0, y0, bw, bh, sample_stride, mode,
+                                                         metric, cand.ctypes.data, len(cand), costs.ctypes.data))
+        return costs
+
+    # --- VulkanComputeContext::counters / reset_counters ---------------------------------
+    def counters(self) -> dict:
+        c = Counters()
+        self._check(self._L.vc1cu_counters_get(self._h, C.byref(c)))
+        return {f[0]: getattr(c, f[0]) for f in Counters._fields_}
+
+    def reset_counters(self):
+        self._check(self._L.vc1cu_reset_counters(self._h))
+
+    # --- the analysis path -------------------------------------------------------------
+    def upload_frame(self, frame_id: int, y, u=None, v=None):
+        """Copies one 4:2:0 frame into frame slot `frame_id`. With pinned host arrays the copy
+        is asynchronous: keep them unchanged until synchronize()."""
+        y = _u8(y)
+        h, w = y.shape
+        uu = _u8(u) if u is not None else None
+        vv = _u8(v) if v is not None else None
+        self._check(self._L.vc1cu_upload_frame(self._h, frame_id, y.ctypes.data,
+                                               uu.ctypes.data if uu is not None else None,
+                                               vv.ctypes.data if vv is not None else None, w, h))
+
+    def upload_frame_ptr(self, frame_id: int, y_ptr: int, u_ptr: int, v_ptr: int, w: int, h: int):
+        self._check(self._L.vc1cu_upload_frame(self._h, frame_id, y_ptr, u_ptr, v_ptr, w, h))
+
+    def download_frame(self, frame_id: int, w: int, h: int):
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self._check(self._L.vc1cu_download_frame(self._h, frame_id, y.ctypes.data, u.ctypes.data, v.ctypes.data))
+        return y, u, v
+
+    def analyze_p_core(self, params: Params, cur_id: int, ref_id: int, mode: int = MV_QPEL, allow_intra=False,
+                       seed=None, seed_distant: Analysis | None = None) -> Analysis:
+        mbw, mbh = mbs_of(params)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        s = None
+        if seed is not None:
+            s = np.ascontiguousarray(seed, np.int32).reshape(-1, 2)
+            if len(s) != mbw * mbh:
+                raise ValueError("shared P motion seed has the wrong macroblock count")
+        sd = seed_distant.as_c() if seed_distant is not None else None
+        self._check(self._L.vc1cu_analyze_p_core(self._h, C.byref(params), cur_id, ref_id, mode, int(allow_intra),
+                                                 s.ctypes.data if s is not None else None,
+                                                 C.byref(sd) if sd is not None else None, C.byref(oc)))
+        return out.take_totals(oc)
+
+    def core_passes(self, params: Params, passes):
+        """passes: iterable of (cur_id, ref_id, mode, allow_intra, seed_slot, out_slot)."""
+        arr = (Pass * len(passes))(*[Pass(*p) for p in passes])
+        self._check(self._L.vc1cu_core_passes(self._h, C.byref(params), arr, len(passes)))
+
+    def read_result(self, params: Params, slot: int) -> Analysis:
+        mbw, mbh = mbs_of(params)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        self._check(self._L.vc1cu_read_result(self._h, slot, C.byref(oc)))
+        return out.take_totals(oc)
+
+    def synchronize(self):
+        self._check(self._L.vc1cu_synchronize(self._h))
+
+    def motion_compensate(self, params: Params, ref_id: int, mv_slot: int, mv_mode: int, pred_id: int):
+        self._check(self._L.vc1cu_motion_compensate(self._h, C.byref(params), ref_id, mv_slot, mv_mode, pred_id))
+
+    def forward_quant(self, params: Params, src_id: int, pred_id: int, type_mask: int = 1):
+        mbw, mbh = mbs_of(params)
+        nt = bin(type_mask & 15).count("1")
+        co = np.zeros((nt, mbw * mbh, 6, 64), np.float64)
+        lv = np.zeros((nt, mbw * mbh, 6, 64), np.int16)
+        self._check(self._L.vc1cu_forward_quant(self._h, C.byref(params), src_id, pred_id, type_mask,
+                                                co.ctypes.data, lv.ctypes.data))
+        return co, lv
+
+    def forward_quant_device(self, params: Params, src_id: int, pred_id: int, type_mask: int, d_coeffs: int,
+                             d_levels: int):
+        self._check(self._L.vc1cu_forward_quant_device(self._h, C.byref(params), src_id, pred_id, type_mask,
+                                                       d_coeffs, d_levels))
+
+
+__all__ = ["CudaComputeContext", "Vc1cuError", "Pass", "load_library", "EXPORTS", "METRIC_SAD", "METRIC_SATD"]

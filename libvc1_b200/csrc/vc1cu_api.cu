@@ -1,0 +1,830 @@
+// vc1cu_api.cu - host shim exporting the C ABI of include/vc1cu.h.
+//
+// Owns the CUDA context state: one stream per context, frame slots and result slots in
+// HBM, the pointer+fingerprint frame cache of the Vulkan-compatible scoring entry point
+// (src/vulkan_compute.cpp:30-45, :194-231), launch descriptors and counters. Every entry
+// point returns a status code and never throws; failures are reported, never replaced by a
+// CPU computation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "vc1cu_core.cuh"
+
+namespace vc1cu {
+// kernels and drivers of the other translation units
+__global__ void core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, WinCfg wc,
+                                 uint32_t epoch, LaunchStatus* st);
+__global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
+int warp_bytes_for_host(const WinCfg& wc);
+struct GState;
+size_t gstate_bytes();
+void run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream);
+void init_gstate(GState* h, const DevFrame& cur, const DevFrame& ref, int range, int* out_global,
+                 unsigned long long* out_sad);
+void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
+               uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
+void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred, int type_mask, double* coeffs,
+                  int16_t* levels, cudaStream_t s);
+void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int n, unsigned long long* out,
+                  cudaStream_t s);
+}  // namespace vc1cu
+
+using namespace vc1cu;
+
+namespace {
+
+constexpr int kMaxSlot = 4096;
+constexpr int kInternalOut = kMaxSlot + 1;   // result slot of vc1cu_analyze_p_core
+constexpr int kInternalSeed = kMaxSlot + 2;  // its seed
+constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
+
+struct Status {
+    int code;
+    std::string msg;
+};
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) throw Fail{VC1CU_ERR_OOM, std::string(what) + ": out of device memory"};
+    if (e != cudaSuccess) throw Fail{VC1CU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+struct FrameSlot {
+    uint8_t* d = nullptr;
+    size_t cap = 0;
+    int w = 0, h = 0, pitch_y = 0, pitch_c = 0;
+    bool valid = false;
+    DevFrame view() const {
+        DevFrame f;
+        f.y = d;
+        f.pitch_y = pitch_y;
+        f.pitch_c = pitch_c;
+        f.u = d + (size_t)pitch_y * h;
+        f.v = f.u + (size_t)pitch_c * (h / 2);
+        return f;
+    }
+};
+
+struct ResultSlot {
+    void* d = nullptr;
+    int mbs = 0;
+    DevResult r{};
+    bool valid = false;
+};
+
+struct CacheSlot {
+    const uint8_t* host = nullptr;
+    int w = 0, h = 0;
+    uint64_t fp = 0, age = 0;
+    uint8_t* d = nullptr;
+    size_t cap = 0;
+    bool valid = false;
+};
+
+// frame_fingerprint, src/vulkan_compute.cpp:30-45 (cache-invalidation tag, not a hash)
+uint64_t frame_fingerprint(const uint8_t* p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    if (!p || !n) return h;
+    constexpr size_t samples = 97;
+    for (size_t i = 0; i < samples; ++i) {
+        const size_t pos = (i * (n - 1)) / (samples - 1);
+        h ^= static_cast<uint64_t>(p[pos]);
+        h *= 1099511628211ull;
+    }
+    h ^= static_cast<uint64_t>(n);
+    h *= 1099511628211ull;
+    return h;
+}
+
+thread_local std::string t_open_error;
+
+}  // namespace
+
+struct vc1cu_ctx {
+    int device = 0;
+    std::string name;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    std::unordered_map<int, FrameSlot> frames;
+    std::unordered_map<int, ResultSlot> results;
+    CacheSlot cache[8];
+    uint64_t age = 0;
+    vc1cu_counters counters{};
+    LaunchStatus* d_status = nullptr;
+    PassDesc* d_passes = nullptr;
+    int passes_cap = 0;
+    GState* d_gstates = nullptr;
+    int gstates_cap = 0;
+    void* d_scratch = nullptr;
+    size_t scratch_cap = 0;
+    void* h_pinned = nullptr;
+    size_t pinned_cap = 0;
+    uint32_t epoch = 0;
+    int sm_count = 0;
+    int max_smem = 0;
+};
+
+namespace {
+
+void* ensure(void*& p, size_t& cap, size_t bytes, const char* what) {
+    if (cap >= bytes && p) return p;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    ck(cudaMalloc(&p, bytes), what);
+    cap = bytes;
+    return p;
+}
+
+int fail(vc1cu_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else t_open_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(vc1cu_ctx* c, F&& f) {
+    if (!c) return fail(nullptr, VC1CU_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> lock(c->mu);
+    try {
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        return f();
+    } catch (const Fail& e) {
+        return fail(c, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(c, VC1CU_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(c, VC1CU_ERR_CUDA, e.what());
+    }
+}
+
+// Validates p and derives the device-side parameter block.
+int make_dev_params(const vc1cu_params* p, DevParams& P, std::string& why) {
+    if (!p) { why = "null params"; return VC1CU_ERR_ARG; }
+    if (p->width <= 0 || p->height <= 0 || (p->width & 1) || (p->height & 1) || p->width > 16384 || p->height > 16384) {
+        why = "width/height must be positive, even and <= 16384 (the internal 4:2:0 raster)";
+        return VC1CU_ERR_ARG;
+    }
+    if (p->pqindex < 1 || p->pqindex > 31) { why = "pqindex must be 1..31"; return VC1CU_ERR_ARG; }
+    if (p->search_range < 0 || p->search_range > 1024 || p->local_search_range < 0) {
+        why = "search_range must be 0..1024 and local_search_range >= 0";
+        return VC1CU_ERR_ARG;
+    }
+    if (p->me_quality == 3) { why = "me_quality RD (codec-aware finalists) is not implemented on the device"; return VC1CU_ERR_UNSUPPORTED; }
+    if (p->me_quality < 0 || p->me_quality > 3 || p->me_algorithm < 0 || p->me_algorithm > 1 || p->long_range_mode < 0 ||
+        p->long_range_mode > 2 || p->subpel_range < 0) {
+        why = "invalid me_quality / me_algorithm / long_range_mode / subpel_range";
+        return VC1CU_ERR_ARG;
+    }
+    P.W = p->width;
+    P.H = p->height;
+    P.vw = p->display_width > 0 ? p->display_width : p->width;
+    P.vh = p->display_height > 0 ? p->display_height : p->height;
+    if (P.vw > P.W || P.vh > P.H) { why = "display raster larger than the coding raster"; return VC1CU_ERR_ARG; }
+    P.mbw = (P.W + 15) / 16;
+    P.mbh = (P.H + 15) / 16;
+    P.cvw = (P.vw + 1) / 2;
+    P.cvh = (P.vh + 1) / 2;
+    P.right_pad = P.vw < P.mbw * 16;
+    P.bottom_pad = P.vh < P.mbh * 16;
+    P.cright_pad = P.cvw < P.mbw * 8;
+    P.cbottom_pad = P.cvh < P.mbh * 8;
+    P.pq = p->pqindex;
+    P.halfqp = p->halfqp != 0;
+    P.nonuniform = p->nonuniform != 0;
+    P.range = p->search_range;
+    P.local_range = std::min(p->search_range, std::max(0, p->local_search_range));
+    P.me_algorithm = p->me_algorithm;
+    P.me_quality = p->me_quality;
+    P.subpel = p->subpel != 0;
+    P.fast_subpel = p->fast_subpel != 0;
+    P.subpel_range = p->subpel_range;
+    P.long_range_mode = p->long_range_mode;
+    P.rnd = p->rnd != 0;
+    P.disable_p_intra = p->disable_p_intra != 0;
+    const int r = p->search_range;
+    P.mvrange = r <= 31 ? 0 : (r <= 63 ? 1 : (r <= 127 ? 2 : 3));
+    const double lam = 0.35 * static_cast<double>(p->pqindex);
+    P.lambda = std::max(1.0, lam);
+    int e = 0;
+    const double fr = std::frexp(P.lambda, &e);
+    P.lam_m = static_cast<uint64_t>(std::ldexp(fr, 53));
+    P.lam_s = 53 - e;
+    // the reference scores in long double; its significand width is the host ABI's
+    P.mant_bits = std::numeric_limits<long double>::digits;
+    P.distant_match_max_mae = p->distant_match_max_mae;
+    P.inter_intra_threshold = p->inter_intra_threshold;
+    return VC1CU_OK;
+}
+
+int stage_max(int R) {
+    int m = 32;
+    const int L = (2 * R) / 8 + 1;
+    if (R >= 8) m = std::max(m, L * L + 2 * L);
+    const int cs = R >= 96 ? 8 : (R >= 32 ? 4 : 2);
+    const int vlimit = std::min(R, std::max(8, R / 2));
+    m = std::max(m, 2 * (R / cs) + 2 * (vlimit / cs));
+    const int hs = R >= 96 ? 8 : (R >= 24 ? 4 : 2);
+    m = std::max(m, 6 * (R / hs));
+    return m;
+}
+
+FrameSlot& frame_slot(vc1cu_ctx* c, int id) {
+    auto it = c->frames.find(id);
+    if (it == c->frames.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "frame slot " + std::to_string(id) + " was never uploaded"};
+    return it->second;
+}
+
+ResultSlot& result_slot(vc1cu_ctx* c, int id, int mbs, bool create) {
+    auto& s = c->results[id];
+    if (s.valid && s.mbs == mbs) return s;
+    if (!create) throw Fail{VC1CU_ERR_STATE, "result slot " + std::to_string(id) + " holds no result of this size"};
+    if (s.d) cudaFree(s.d);
+    s = ResultSlot{};
+    const size_t n = (size_t)mbs;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bytes = al(8 * n) + al(32 * n) + al(n) * 2 + al(8 * n) * 4 + al(n) + al(8 * n) * 2 + al(n) + al(4 * n) +
+                         al(8) + al(8) + al(16) + al(40);
+    ck(cudaMalloc(&s.d, bytes), "cudaMalloc(result slot)");
+    ck(cudaMemsetAsync(s.d, 0, bytes, c->stream), "cudaMemsetAsync(result slot)");
+    uint8_t* p = static_cast<uint8_t*>(s.d);
+    auto take = [&](size_t b) { uint8_t* q = p; p += al(b); return q; };
+    s.r.mvs = (int2*)take(8 * n);
+    s.r.bmv = (int2*)take(32 * n);
+    s.r.use4 = take(n);
+    s.r.intra = take(n);
+    s.r.screen = (uint64_t*)take(8 * n);
+    s.r.ratio = (double*)take(8 * n);
+    s.r.dl = (double*)take(8 * n);
+    s.r.dc = (double*)take(8 * n);
+    s.r.dd = take(n);
+    s.r.chosen = (uint64_t*)take(8 * n);
+    s.r.temporal = (uint64_t*)take(8 * n);
+    s.r.flags = take(n);
+    s.r.done = (uint32_t*)take(4 * n);
+    s.r.global = (int*)take(8);
+    s.r.gsad = (unsigned long long*)take(8);
+    s.r.totals = (double*)take(16);
+    s.r.itotals = (unsigned long long*)take(40);
+    s.mbs = mbs;
+    s.valid = true;
+    return s;
+}
+
+FrameSlot& alloc_frame(vc1cu_ctx* c, int id, int w, int h) {
+    auto& f = c->frames[id];
+    const int py = (w + 15) & ~15, pc = (w / 2 + 15) & ~15;
+    const size_t bytes = (size_t)py * h + 2 * (size_t)pc * (h / 2);
+    if (!f.d || f.cap < bytes) {
+        if (f.d) cudaFree(f.d);
+        f.d = nullptr;
+        f.cap = 0;
+        void* d = nullptr;
+        ck(cudaMalloc(&d, bytes), "cudaMalloc(frame)");
+        f.d = static_cast<uint8_t*>(d);
+        f.cap = bytes;
+    }
+    f.w = w;
+    f.h = h;
+    f.pitch_y = py;
+    f.pitch_c = pc;
+    f.valid = true;
+    return f;
+}
+
+uint8_t* cache_frame(vc1cu_ctx* c, const uint8_t* data, int w, int h) {
+    const size_t bytes = (size_t)w * h;
+    const uint64_t fp = frame_fingerprint(data, bytes);
+    for (auto& s : c->cache)
+        if (s.valid && s.host == data && s.w == w && s.h == h && s.fp == fp) {
+            s.age = ++c->age;
+            return s.d;
+        }
+    CacheSlot* slot = &c->cache[0];
+    for (auto& s : c->cache) {
+        if (!s.valid) { slot = &s; break; }
+        if (s.age < slot->age) slot = &s;
+    }
+    void* d = slot->d;
+    ensure(d, slot->cap, bytes, "cudaMalloc(cached frame)");
+    slot->d = static_cast<uint8_t*>(d);
+    ck(cudaMemcpyAsync(slot->d, data, bytes, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(frame)");
+    slot->host = data;
+    slot->w = w;
+    slot->h = h;
+    slot->fp = fp;
+    slot->age = ++c->age;
+    slot->valid = true;
+    c->counters.frame_uploads++;
+    c->counters.frame_upload_bytes += bytes;
+    return slot->d;
+}
+
+void sync_checked(vc1cu_ctx* c) {
+    ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    ck(cudaGetLastError(), "kernel");
+}
+
+int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1cu_mv* cands, size_t n, uint64_t* costs) {
+    const size_t cb = n * sizeof(int2), ob = n * sizeof(unsigned long long);
+    ensure(c->d_scratch, c->scratch_cap, cb + ob + 256, "cudaMalloc(candidates)");
+    int2* dc = static_cast<int2*>(c->d_scratch);
+    unsigned long long* dout = reinterpret_cast<unsigned long long*>(static_cast<uint8_t*>(c->d_scratch) + ((cb + 255) & ~size_t(255)));
+    const auto t0 = std::chrono::steady_clock::now();
+    ck(cudaMemcpyAsync(dc, cands, cb, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(candidates)");
+    launch_score(P, a, dc, (int)n, dout, c->stream);
+    ck(cudaGetLastError(), "score_kernel launch");
+    ck(cudaMemcpyAsync(costs, dout, ob, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(costs)");
+    sync_checked(c);
+    const auto t1 = std::chrono::steady_clock::now();
+    c->counters.dispatches++;
+    c->counters.candidates += n;
+    c->counters.submit_wait_nanoseconds += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count();
+    return VC1CU_OK;
+}
+
+// Launches a batch of independent core passes (global search first for unseeded ones).
+int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
+    DevParams P;
+    std::string why;
+    int rc = make_dev_params(p, P, why);
+    if (rc) throw Fail{rc, why};
+    if (n <= 0) return VC1CU_OK;
+    const int mbs = P.mbw * P.mbh;
+    bool any_unseeded = false;
+    std::vector<PassDesc> h(n);
+    std::vector<int> unseeded;
+    for (int i = 0; i < n; ++i) {
+        const vc1cu_pass& q = passes[i];
+        if (q.mode < 0 || q.mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        if (q.out_slot < 0 || q.out_slot > kInternalSeed || q.seed_slot == q.out_slot)
+            throw Fail{VC1CU_ERR_ARG, "invalid result slot"};
+        FrameSlot& fc = frame_slot(c, q.cur_id);
+        FrameSlot& fr = frame_slot(c, q.ref_id);
+        if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "P-picture reference dimensions do not match the configuration"};
+        PassDesc& d = h[i];
+        d.cur = fc.view();
+        d.ref = fr.view();
+        d.mode = q.mode;
+        d.allow_intra = q.allow_intra != 0;
+        d.seeded = q.seed_slot >= 0;
+        if (d.seeded) {
+            ResultSlot& s = result_slot(c, q.seed_slot, mbs, false);
+            d.seed_mvs = s.r.mvs;
+            d.seed_dl = s.r.dl;
+            d.seed_dc = s.r.dc;
+            d.seed_dd = s.r.dd;
+        } else {
+            if (P.range > P.local_range)
+                throw Fail{VC1CU_ERR_UNSUPPORTED,
+                           "long-range search (search_range above local_search_range) is not implemented on the device"};
+            d.seed_mvs = nullptr;
+            d.seed_dl = d.seed_dc = nullptr;
+            d.seed_dd = nullptr;
+            any_unseeded = true;
+            unseeded.push_back(i);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < i; ++j)
+            if (passes[j].out_slot == passes[i].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
+        h[i].out = result_slot(c, passes[i].out_slot, mbs, true).r;
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            if (passes[i].seed_slot == passes[j].out_slot) throw Fail{VC1CU_ERR_ARG, "a pass seeds from a pass of the same batch"};
+    // global translation search of the unseeded passes
+    if (!unseeded.empty() && P.range > 0) {
+        const int nu = (int)unseeded.size();
+        const size_t gb = gstate_bytes();
+        if (c->gstates_cap < nu) {
+            if (c->d_gstates) cudaFree(c->d_gstates);
+            c->d_gstates = nullptr;
+            c->gstates_cap = 0;
+            void* d = nullptr;
+            ck(cudaMalloc(&d, gb * nu), "cudaMalloc(global search state)");
+            c->d_gstates = static_cast<GState*>(d);
+            c->gstates_cap = nu;
+        }
+        std::vector<uint8_t> hs(gb * nu);
+        const int grange = std::min(P.local_range, 32);
+        for (int k = 0; k < nu; ++k) {
+            const PassDesc& d = h[unseeded[k]];
+            init_gstate(reinterpret_cast<GState*>(hs.data() + gb * k), d.cur, d.ref, grange, d.out.global, d.out.gsad);
+        }
+        ck(cudaMemcpyAsync(c->d_gstates, hs.data(), gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
+        run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
+        ck(cudaGetLastError(), "global search launch");
+        // the host staging buffer must outlive the copy
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    }
+    // pass descriptors
+    if (c->passes_cap < n) {
+        if (c->d_passes) cudaFree(c->d_passes);
+        c->d_passes = nullptr;
+        c->passes_cap = 0;
+        void* d = nullptr;
+        ck(cudaMalloc(&d, sizeof(PassDesc) * n), "cudaMalloc(pass descriptors)");
+        c->d_passes = static_cast<PassDesc*>(d);
+        c->passes_cap = n;
+    }
+    // ordered on the context stream after any launch still reading the previous descriptors;
+    // a pageable source is staged before the call returns
+    ck(cudaMemcpyAsync(c->d_passes, h.data(), sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
+       "cudaMemcpyAsync(pass descriptors)");
+    // window / bitset geometry
+    WinCfg wc;
+    if (any_unseeded) {
+        wc.rw = P.local_range + 1;
+        wc.seen_r = P.local_range;
+        wc.seen_words = ((2 * P.local_range + 1) * (2 * P.local_range + 1) + 31) / 32;
+        wc.keys_cap = stage_max(P.local_range);
+    } else {
+        wc.rw = 4;
+        wc.seen_r = 0;
+        wc.seen_words = 1;
+        wc.keys_cap = 32;
+    }
+    wc.ww = 16 + 2 * wc.rw + 3;
+    wc.warp_bytes = warp_bytes_for_host(wc);
+    int warps = 4;
+    while (warps > 1 && (size_t)warps * wc.warp_bytes > (size_t)c->max_smem) --warps;
+    const size_t smem = (size_t)warps * wc.warp_bytes;
+    if (smem > (size_t)c->max_smem)
+        throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
+    ck(cudaFuncSetAttribute(core_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+       "cudaFuncSetAttribute");
+    int per_sm = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, core_pass_kernel, 32 * warps, smem), "occupancy");
+    per_sm = std::max(per_sm, 1);
+    const long items = (long)n * mbs;
+    const long need = (items + warps - 1) / warps;
+    const int grid = (int)std::max(1L, std::min<long>((long)per_sm * c->sm_count, need));
+    if (++c->epoch == 0) c->epoch = 1;
+    ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
+    core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, wc, c->epoch, c->d_status);
+    ck(cudaGetLastError(), "core_pass_kernel launch");
+    totals_kernel<<<n, 256, 0, c->stream>>>(P, c->d_passes, n);
+    ck(cudaGetLastError(), "totals_kernel launch");
+    c->counters.dispatches++;
+    c->counters.macroblocks_analysed += (uint64_t)items;
+    return VC1CU_OK;
+}
+
+int check_status(vc1cu_ctx* c) {
+    LaunchStatus st{};
+    ck(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(status)");
+    sync_checked(c);
+    if (st.error) throw Fail{st.error, "a wavefront wait timed out on the device (" + std::to_string(st.timeouts) + " waits)"};
+    return VC1CU_OK;
+}
+
+void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
+    const size_t n = (size_t)s.mbs;
+    auto cp = [&](void* dst, const void* src, size_t b) {
+        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(result)");
+    };
+    cp(out->mvs, s.r.mvs, 8 * n);
+    cp(out->block_mvs, s.r.bmv, 32 * n);
+    cp(out->use_4mv, s.r.use4, n);
+    cp(out->use_intra, s.r.intra, n);
+    cp(out->screen_sads, s.r.screen, 8 * n);
+    cp(out->inter_intra_cost_ratio, s.r.ratio, 8 * n);
+    cp(out->distant_local_mae, s.r.dl, 8 * n);
+    cp(out->distant_candidate_mae, s.r.dc, 8 * n);
+    cp(out->distant_match_decision, s.r.dd, n);
+    double tot[2];
+    unsigned long long it[5], gsad;
+    int g[2];
+    cp(tot, s.r.totals, 16);
+    cp(it, s.r.itotals, 40);
+    cp(g, s.r.global, 8);
+    cp(&gsad, s.r.gsad, 8);
+    sync_checked(c);
+    out->mean_abs_residual = tot[0];
+    out->rate_complexity = tot[1];
+    out->motion_sad = it[0];
+    out->moved_macroblocks = it[1];
+    out->fractional_chroma_macroblocks = it[2];
+    out->four_mv_macroblocks = it[3];
+    out->intra_macroblocks = it[4];
+    out->global_dx = g[0];
+    out->global_dy = g[1];
+    out->global_full_sad = gsad;
+}
+
+}  // namespace
+
+// ---- C ABI -------------------------------------------------------------------------------
+
+extern "C" {
+
+void vc1cu_params_default(vc1cu_params* p, int width, int height) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->width = width;
+    p->height = height;
+    p->pqindex = 8;
+    p->search_range = 1024;
+    p->local_search_range = 32;
+    p->me_algorithm = 0;
+    p->me_quality = 2;
+    p->subpel = 1;
+    p->subpel_range = 1024;
+    p->distant_match_max_mae = 255.0;
+    p->inter_intra_threshold = 0.80;
+}
+
+int vc1cu_open(int device, vc1cu_ctx** out) {
+    if (!out) return fail(nullptr, VC1CU_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(nullptr, VC1CU_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0) {
+        e = cudaGetDevice(&device);
+        if (e != cudaSuccess) return fail(nullptr, VC1CU_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (device >= count) return fail(nullptr, VC1CU_ERR_ARG, "device ordinal out of range");
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return fail(nullptr, VC1CU_ERR_CUDA, cudaGetErrorString(e));
+    if (prop.major < 10) return fail(nullptr, VC1CU_ERR_UNSUPPORTED, "this library is built for sm_100a (B200)");
+    auto* c = new (std::nothrow) vc1cu_ctx;
+    if (!c) return fail(nullptr, VC1CU_ERR_OOM, "host allocation failed");
+    c->device = device;
+    c->name = prop.name;
+    c->sm_count = prop.multiProcessorCount;
+    c->max_smem = (int)prop.sharedMemPerBlockOptin;
+    try {
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        void* d = nullptr;
+        ck(cudaMalloc(&d, sizeof(LaunchStatus)), "cudaMalloc(status)");
+        c->d_status = static_cast<LaunchStatus*>(d);
+        ck(cudaMemset(c->d_status, 0, sizeof(LaunchStatus)), "cudaMemset(status)");
+    } catch (const Fail& f) {
+        const int code = f.code;
+        t_open_error = f.msg;
+        vc1cu_close(c);
+        return code;
+    }
+    *out = c;
+    return VC1CU_OK;
+}
+
+int vc1cu_close(vc1cu_ctx* c) {
+    if (!c) return VC1CU_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->frames)
+        if (kv.second.d) cudaFree(kv.second.d);
+    for (auto& kv : c->results)
+        if (kv.second.d) cudaFree(kv.second.d);
+    for (auto& s : c->cache)
+        if (s.d) cudaFree(s.d);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->d_passes) cudaFree(c->d_passes);
+    if (c->d_gstates) cudaFree(c->d_gstates);
+    if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return VC1CU_OK;
+}
+
+const char* vc1cu_device_name(const vc1cu_ctx* c) { return c ? c->name.c_str() : ""; }
+int vc1cu_device_index(const vc1cu_ctx* c) { return c ? c->device : -1; }
+const char* vc1cu_last_error(const vc1cu_ctx* c) { return c ? c->err.c_str() : t_open_error.c_str(); }
+
+int vc1cu_counters_get(const vc1cu_ctx* c, vc1cu_counters* out) {
+    if (!c || !out) return VC1CU_ERR_ARG;
+    *out = c->counters;
+    return VC1CU_OK;
+}
+
+int vc1cu_reset_counters(vc1cu_ctx* c) {
+    if (!c) return VC1CU_ERR_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    c->counters = vc1cu_counters{};
+    return VC1CU_OK;
+}
+
+int vc1cu_score_motion_batch(vc1cu_ctx* c, const uint8_t* cur, const uint8_t* ref, int width, int height, int x0, int y0,
+                             int bw, int bh, int sample_stride, int bilinear, int rnd, int metric,
+                             const vc1cu_mv* candidates, size_t n, uint64_t* costs) {
+    return guarded(c, [&]() -> int {
+        // src/vulkan_compute.cpp:375-382: empty or degenerate batches are a successful no-op
+        if (!cur || !ref || width <= 0 || height <= 0 || bw <= 0 || bh <= 0 || !candidates || !n) return VC1CU_OK;
+        if (!costs) throw Fail{VC1CU_ERR_ARG, "null costs"};
+        if (n > kMaxBatch) throw Fail{VC1CU_ERR_ARG, "motion batches above 4,194,240 candidates are not supported"};
+        if (metric != VC1CU_METRIC_SAD && metric != VC1CU_METRIC_SATD) throw Fail{VC1CU_ERR_ARG, "invalid metric"};
+        if (x0 < 0 || y0 < 0 || sample_stride < 0) throw Fail{VC1CU_ERR_ARG, "block origin must lie in the picture"};
+        uint8_t* dcur = cache_frame(c, cur, width, height);
+        uint8_t* dref = cache_frame(c, ref, width, height);
+        DevParams P{};
+        P.W = width;
+        P.H = height;
+        ScoreArgs a{dcur, dref, width, width, height, x0, y0, bw, bh, sample_stride,
+                    bilinear ? VC1CU_MV_HPEL_BILINEAR : VC1CU_MV_QPEL, rnd != 0, metric, VC1CU_LAW_SHADER};
+        return score_common(c, P, a, candidates, n, costs);
+    });
+}
+
+int vc1cu_score_motion_batch_law(vc1cu_ctx* c, const vc1cu_params* p, int law, const uint8_t* cur, const uint8_t* ref,
+                                 int x0, int y0, int bw, int bh, int sample_stride, int mode, int metric,
+                                 const vc1cu_mv* candidates, size_t n, uint64_t* costs) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        if (!cur || !ref || bw <= 0 || bh <= 0 || !candidates || !n) return VC1CU_OK;
+        if (!costs) throw Fail{VC1CU_ERR_ARG, "null costs"};
+        if (n > kMaxBatch) throw Fail{VC1CU_ERR_ARG, "motion batches above 4,194,240 candidates are not supported"};
+        if (law != VC1CU_LAW_SHADER && law != VC1CU_LAW_CPU) throw Fail{VC1CU_ERR_ARG, "invalid law"};
+        if (mode < 0 || mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        if (metric != VC1CU_METRIC_SAD && metric != VC1CU_METRIC_SATD) throw Fail{VC1CU_ERR_ARG, "invalid metric"};
+        if (x0 < 0 || y0 < 0 || sample_stride < 0) throw Fail{VC1CU_ERR_ARG, "block origin must lie in the picture"};
+        if (law == VC1CU_LAW_CPU && metric == VC1CU_METRIC_SAD && sample_stride > 1 &&
+            (bw != 16 || bh != 16 || (x0 & 15) || (y0 & 15)))
+            throw Fail{VC1CU_ERR_ARG, "sampled SAD is defined for macroblock-aligned 16x16 blocks (mb_sad)"};
+        uint8_t* dcur = cache_frame(c, cur, p->width, p->height);
+        uint8_t* dref = cache_frame(c, ref, p->width, p->height);
+        ScoreArgs a{dcur, dref, p->width, p->width, p->height, x0, y0, bw, bh, sample_stride, mode, p->rnd != 0, metric, law};
+        return score_common(c, P, a, candidates, n, costs);
+    });
+}
+
+int vc1cu_upload_frame(vc1cu_ctx* c, int id, const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h) {
+    return guarded(c, [&]() -> int {
+        if (id < 0 || id >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "frame id out of range"};
+        if (!y || w <= 0 || h <= 0 || (w & 1) || (h & 1)) throw Fail{VC1CU_ERR_ARG, "invalid frame"};
+        FrameSlot& f = alloc_frame(c, id, w, h);
+        const DevFrame d = f.view();
+        ck(cudaMemcpy2DAsync((void*)d.y, f.pitch_y, y, w, w, h, cudaMemcpyHostToDevice, c->stream), "upload Y");
+        const int cw = w / 2, ch = h / 2;
+        if (u) ck(cudaMemcpy2DAsync((void*)d.u, f.pitch_c, u, cw, cw, ch, cudaMemcpyHostToDevice, c->stream), "upload U");
+        else ck(cudaMemset2DAsync((void*)d.u, f.pitch_c, 128, cw, ch, c->stream), "fill U");
+        if (v) ck(cudaMemcpy2DAsync((void*)d.v, f.pitch_c, v, cw, cw, ch, cudaMemcpyHostToDevice, c->stream), "upload V");
+        else ck(cudaMemset2DAsync((void*)d.v, f.pitch_c, 128, cw, ch, c->stream), "fill V");
+        c->counters.frame_uploads++;
+        c->counters.frame_upload_bytes += (size_t)w * h + 2 * (size_t)cw * ch;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_download_frame(vc1cu_ctx* c, int id, uint8_t* y, uint8_t* u, uint8_t* v) {
+    return guarded(c, [&]() -> int {
+        FrameSlot& f = frame_slot(c, id);
+        const DevFrame d = f.view();
+        const int cw = f.w / 2, ch = f.h / 2;
+        if (y) ck(cudaMemcpy2DAsync(y, f.w, d.y, f.pitch_y, f.w, f.h, cudaMemcpyDeviceToHost, c->stream), "download Y");
+        if (u) ck(cudaMemcpy2DAsync(u, cw, d.u, f.pitch_c, cw, ch, cudaMemcpyDeviceToHost, c->stream), "download U");
+        if (v) ck(cudaMemcpy2DAsync(v, cw, d.v, f.pitch_c, cw, ch, cudaMemcpyDeviceToHost, c->stream), "download V");
+        sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_core_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
+    return guarded(c, [&]() -> int {
+        if (n < 0 || (n > 0 && !passes)) throw Fail{VC1CU_ERR_ARG, "invalid pass list"};
+        for (int i = 0; i < n; ++i)
+            if (passes[i].out_slot < 0 || passes[i].out_slot >= kMaxSlot || passes[i].seed_slot >= kMaxSlot)
+                throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+        return launch_passes(c, p, passes, n);
+    });
+}
+
+int vc1cu_synchronize(vc1cu_ctx* c) {
+    return guarded(c, [&]() -> int { return check_status(c); });
+}
+
+int vc1cu_read_result(vc1cu_ctx* c, int slot, vc1cu_panalysis* out) {
+    return guarded(c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        check_status(c);
+        auto it = c->results.find(slot);
+        if (it == c->results.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "empty result slot"};
+        read_result(c, it->second, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_analyze_p_core(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int ref_id, int mode, int allow_intra,
+                         const vc1cu_mv* seed_mvs, const vc1cu_panalysis* seed_distant, vc1cu_panalysis* out) {
+    return guarded(c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        vc1cu_pass q{cur_id, ref_id, mode, allow_intra, -1, kInternalOut};
+        if (seed_mvs) {
+            ResultSlot& s = result_slot(c, kInternalSeed, mbs, true);
+            ck(cudaMemcpyAsync(s.r.mvs, seed_mvs, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload seed");
+            std::vector<double> neg(mbs, -1.0);
+            std::vector<uint8_t> zero(mbs, 0);
+            const double* dl = seed_distant && seed_distant->distant_local_mae ? seed_distant->distant_local_mae : neg.data();
+            const double* dc = seed_distant && seed_distant->distant_candidate_mae ? seed_distant->distant_candidate_mae : neg.data();
+            const uint8_t* dd = seed_distant && seed_distant->distant_match_decision ? seed_distant->distant_match_decision : zero.data();
+            ck(cudaMemcpyAsync(s.r.dl, dl, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload seed");
+            ck(cudaMemcpyAsync(s.r.dc, dc, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload seed");
+            ck(cudaMemcpyAsync(s.r.dd, dd, (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload seed");
+            ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+            q.seed_slot = kInternalSeed;
+        }
+        launch_passes(c, p, &q, 1);
+        check_status(c);
+        read_result(c, c->results[kInternalOut], out);
+        if (seed_mvs) {
+            out->global_dx = out->global_dy = 0;
+            out->global_full_sad = 0;
+        }
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_motion_compensate(vc1cu_ctx* c, const vc1cu_params* p, int ref_id, int mv_slot, int mv_mode, int pred_id) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        if (mv_mode < 0 || mv_mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        if (pred_id < 0 || pred_id >= kMaxSlot || pred_id == ref_id) throw Fail{VC1CU_ERR_ARG, "invalid prediction slot"};
+        FrameSlot& fr = frame_slot(c, ref_id);
+        if (fr.w != P.W || fr.h != P.H) throw Fail{VC1CU_ERR_ARG, "reference size mismatch"};
+        const DevFrame ref = fr.view();
+        ResultSlot& s = result_slot(c, mv_slot, P.mbw * P.mbh, false);
+        FrameSlot& fp = alloc_frame(c, pred_id, P.W, P.H);
+        const DevFrame pd = fp.view();
+        launch_mc(P, ref, s.r.mvs, s.r.bmv, s.r.use4, mv_mode, (uint8_t*)pd.y, (uint8_t*)pd.u, (uint8_t*)pd.v, fp.pitch_y,
+                  fp.pitch_c, c->stream);
+        ck(cudaGetLastError(), "mc_kernel launch");
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_forward_quant_device(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pred_id, int type_mask,
+                               double* d_coeffs, int16_t* d_levels) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        if (type_mask <= 0 || type_mask > 15) throw Fail{VC1CU_ERR_ARG, "type_mask must select 1..4 transform types"};
+        FrameSlot& fs = frame_slot(c, src_id);
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size mismatch"};
+        launch_xform(P, fs.view(), fp.view(), type_mask, d_coeffs, d_levels, c->stream);
+        ck(cudaGetLastError(), "xform_kernel launch");
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_forward_quant(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pred_id, int type_mask, double* coeffs,
+                        int16_t* levels) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        if (type_mask <= 0 || type_mask > 15) throw Fail{VC1CU_ERR_ARG, "type_mask must select 1..4 transform types"};
+        int nt = 0;
+        for (int t = 0; t < 4; ++t) nt += (type_mask >> t) & 1;
+        const size_t n = (size_t)nt * P.mbw * P.mbh * 6 * 64;
+        const size_t cb = n * 8, lb = n * 2;
+        ensure(c->d_scratch, c->scratch_cap, cb + lb + 256, "cudaMalloc(transform output)");
+        double* dco = static_cast<double*>(c->d_scratch);
+        int16_t* dlv = reinterpret_cast<int16_t*>(static_cast<uint8_t*>(c->d_scratch) + ((cb + 255) & ~size_t(255)));
+        FrameSlot& fs = frame_slot(c, src_id);
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size mismatch"};
+        launch_xform(P, fs.view(), fp.view(), type_mask, dco, dlv, c->stream);
+        ck(cudaGetLastError(), "xform_kernel launch");
+        if (coeffs) ck(cudaMemcpyAsync(coeffs, dco, cb, cudaMemcpyDeviceToHost, c->stream), "download coefficients");
+        if (levels) ck(cudaMemcpyAsync(levels, dlv, lb, cudaMemcpyDeviceToHost, c->stream), "download levels");
+        sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,1276 @@
+// vc1cu_core.cu - one Vc1Encoder::analyze_p_picture_core pass per picture, many pictures
+// per launch (encoder_motion.cpp:47-442).
+//
+// Execution model (sm_100a):
+//   * persistent grid; each warp owns one macroblock at a time, taken from a global work
+//     queue that interleaves the pictures of the batch in raster order, so every
+//     dependency of an item was handed out before it;
+//   * the raster-order dependency of the reference (left, top-left, top, top-right MVs of
+//     the same pass, encoder_motion.cpp:1312-1466) is a wavefront: a warp waits on the
+//     four neighbours' done flags (acquire loads, bounded spin that flags
+//     VC1CU_ERR_TIMEOUT instead of hanging) and publishes its own MB with a release store;
+//   * the reference search window of the MB is staged once into the warp's shared memory
+//     (edge-replicated), candidates outside it read HBM with clamping;
+//   * integer stages score one candidate per lane; sub-pel stages split each candidate's
+//     block into 8-pixel row segments across lanes; every selection uses the reference's
+//     total orders, so the parallel evaluation returns the reference's exact choice.
+#include <cuda_runtime.h>
+
+#include "vc1cu_core.cuh"
+#include "vc1cu_pred.cuh"
+
+namespace vc1cu {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kListCap = 24;
+
+// Per-warp shared-memory carve.
+struct WarpMem {
+    uint8_t* cur;          // 16x16 current MB (zero outside the visible raster)
+    uint8_t* win;          // reference window
+    uint32_t* seen;        // first-visit bitset of the sampled UMH stages
+    uint32_t* seen_full;   // first-visit bitset of the full-resolution stages
+    uint64_t* keys;        // per-stage candidate keys
+    int2* list_mv;         // staged-refinement candidate list
+    uint64_t* list_sad;
+    uint64_t* list_satd;
+    uint32_t* list_rate;
+    unsigned __int128* list_key;
+    int2* batch;           // scratch MV batch
+    uint64_t* batch_cost;
+    int* misc;             // small scalars
+};
+
+struct Mb {
+    int lane;
+    int mx, my, x0, y0, pos, aw, ah;  // aw/ah: visible wrt the internal raster (cur.width)
+    const PassDesc* d;
+    WarpMem sm;
+    int wx0, wy0, ww;
+    GlobSampler gref;
+};
+
+__device__ __forceinline__ bool win_inside(const Mb& m, int xa, int ya, int xb, int yb) {
+    return xa >= m.wx0 && ya >= m.wy0 && xb < m.wx0 + m.ww && yb < m.wy0 + m.ww;
+}
+
+// ---- integer SAD of the 16x16 MB, mb_sad (encoder_motion.cpp:2197-2285) ----------------
+
+template <int STRIDE, class S>
+__device__ __forceinline__ uint32_t sad_int_loop(const S& s, const uint8_t* cur, int x0, int y0, int dx, int dy, int aw,
+                                                 int ah) {
+    uint32_t acc = 0;
+#pragma unroll 4
+    for (int y = 0; y < ah; y += STRIDE) {
+#pragma unroll
+        for (int x = 0; x < 16; x += STRIDE) {
+            if (x < aw) acc += (uint32_t)iabs((int)cur[y * 16 + x] - s(x0 + x + dx, y0 + y + dy));
+        }
+    }
+    return acc;
+}
+
+__device__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int stride) {
+    if (hidden_padding(P, m.x0, m.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
+    uint32_t s;
+    const bool fast = win_inside(m, m.x0 + dx, m.y0 + dy, m.x0 + dx + 15, m.y0 + dy + 15);
+    const WinSampler ws{m.sm.win, m.ww, m.wx0, m.wy0};
+    if (fast) {
+        if (stride == 1) s = sad_int_loop<1>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else if (stride == 2) s = sad_int_loop<2>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else s = sad_int_loop<4>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+    } else {
+        if (stride == 1) s = sad_int_loop<1>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else if (stride == 2) s = sad_int_loop<2>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else s = sad_int_loop<4>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+    }
+    return stride > 1 ? (uint64_t)s * (uint64_t)(stride * stride) : (uint64_t)s;
+}
+
+// ---- sub-pel SAD / SATD batches (block_sad_motion :2670-2933, block_satd_motion :2960-3042)
+
+// SAD of n candidates of block (bx,by,bw,bh) (bw,bh in {8,16}) under the CPU law, written
+// to out[]. Each candidate's block is split into 8-pixel row segments over bh*bw/8 lanes.
+__device__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw, int bh,
+                          int mode, uint64_t* out) {
+    const int spr = bw >> 3;
+    const int segs = bh * spr;  // 32 (16x16) or 8 (8x8)
+    const int per_iter = 32 / segs;
+    const int aw = imax(0, imin(bw, P.W - bx)), ah = imax(0, imin(bh, P.H - by));
+    const bool bil = mode_bilinear(mode);
+    const bool cg = chroma_gate(bx, by, bw, bh);
+    const int cx = bx - m.x0, cy = by - m.y0;
+    for (int base = 0; base < n; base += per_iter) {
+        const int ci = base + m.lane / segs;
+        const int sidx = m.lane % segs;
+        const int r = sidx / spr, c0 = (sidx % spr) * 8;
+        const bool valid = ci < n;
+        const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
+        bool bad = false;
+        uint32_t part = 0;
+        if (valid) {
+            bad = hidden_padding(P, bx, by, bw, bh, mv.x, mv.y, mode, cg) || (bil && ((mv.x & 1) || (mv.y & 1)));
+            if (!bad && r < ah && c0 < aw) {
+                const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
+                int pred[8];
+                if (win_inside(m, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
+                    predict_row<8>(WinSampler{m.sm.win, m.ww, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                else
+                    predict_row<8>(m.gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                const uint8_t* c = m.sm.cur + (cy + r) * 16 + cx + c0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (c0 + i < aw) part += (uint32_t)iabs((int)c[i] - pred[i]);
+            }
+        }
+        for (int o = segs >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
+        if (valid && sidx == 0) out[ci] = bad ? kBad : (uint64_t)part;
+    }
+    __syncwarp();
+}
+
+__device__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw, int bh,
+                           int mode, uint64_t* out) {
+    const int tpr = bw >> 2;
+    const int tiles = tpr * (bh >> 2);  // 16 or 4
+    const int per_iter = 32 / tiles;
+    const int aw = imax(0, imin(bw, P.W - bx)), ah = imax(0, imin(bh, P.H - by));
+    const bool bil = mode_bilinear(mode);
+    const int cx = bx - m.x0, cy = by - m.y0;
+    for (int base = 0; base < n; base += per_iter) {
+        const int ci = base + m.lane / tiles;
+        const int t = m.lane % tiles;
+        const int tx = (t % tpr) * 4, ty = (t / tpr) * 4;
+        const bool valid = ci < n;
+        const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
+        const bool bad = valid && mode_halfpel(mode) && ((mv.x & 1) || (mv.y & 1));
+        uint32_t part = 0;
+        const int tw = imax(0, imin(4, aw - tx)), th = imax(0, imin(4, ah - ty));
+        if (valid && !bad && tw && th) {
+            const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
+            const bool fast = win_inside(m, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1);
+            int d[16];
+#pragma unroll
+            for (int yy = 0; yy < 4; ++yy) {
+                int pred[4];
+                if (fast)
+                    predict_row<4>(WinSampler{m.sm.win, m.ww, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                else
+                    predict_row<4>(m.gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx)
+                    d[yy * 4 + xx] = (xx < tw && yy < th) ? (int)m.sm.cur[(cy + ty + yy) * 16 + cx + tx + xx] - pred[xx] : 0;
+            }
+            part = satd4x4(d);
+        }
+        for (int o = tiles >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
+        if (valid && t == 0) out[ci] = (!aw || !ah) ? 0 : (bad ? kBad : (uint64_t)part);
+    }
+    __syncwarp();
+}
+
+// ---- first-visit bitsets ----------------------------------------------------------------
+
+__device__ __forceinline__ bool seen_test_set(uint32_t* bits, int r, int dx, int dy) {
+    const int side = 2 * r + 1;
+    const int bit = (dy + r) * side + (dx + r);
+    const uint32_t mask = 1u << (bit & 31);
+    return (atomicOr(&bits[bit >> 5], mask) & mask) != 0;
+}
+
+// ---- integer UMH (encoder_motion.cpp:1781-2023) -----------------------------------------
+
+struct Top8 {
+    uint64_t k[8];
+    int n;
+};
+
+// Merges the n keys of m.sm.keys (UINT64_MAX = skipped) into the sorted top-8 list.
+__device__ void top8_merge(const Mb& m, Top8& top, int n) {
+    uint64_t* keys = m.sm.keys;
+    uint64_t sel[8];
+    int ns = 0;
+    const uint64_t bound = top.n == 8 ? top.k[7] : UINT64_MAX;
+    for (int r = 0; r < 8; ++r) {
+        uint64_t lm = UINT64_MAX;
+        for (int i = m.lane; i < n; i += 32) lm = keys[i] < lm ? keys[i] : lm;
+        const uint64_t g = warp_min_u64(lm);
+        if (g == UINT64_MAX || g >= bound) break;
+        sel[ns++] = g;
+        for (int i = m.lane; i < n; i += 32)
+            if (keys[i] == g) keys[i] = UINT64_MAX;
+        __syncwarp();
+    }
+    // merge two sorted lists, keep 8
+    uint64_t out[8];
+    int a = 0, b = 0, o = 0;
+    while (o < 8 && (a < top.n || b < ns)) {
+        if (b >= ns || (a < top.n && top.k[a] < sel[b])) out[o++] = top.k[a++];
+        else out[o++] = sel[b++];
+    }
+    for (int i = 0; i < o; ++i) top.k[i] = out[i];
+    top.n = o;
+    __syncwarp();
+}
+
+// Scores the candidates produced by gen(i) for i < n at sampled stride 2 (the UMH
+// `consider` lambda, encoder_motion.cpp:1821-1839) and merges them into top.
+template <class Gen>
+__device__ void umh_stage(const DevParams& P, const Mb& m, Top8& top, int n, int range, Gen gen) {
+    for (int i = m.lane; i < n; i += 32) {
+        int2 c = gen(i);
+        c.x = iclamp(c.x, -range, range);
+        c.y = iclamp(c.y, -range, range);
+        uint64_t key = UINT64_MAX;
+        if (!seen_test_set(m.sm.seen, range, c.x, c.y)) key = int_key(mb_sad(P, m, c.x, c.y, 2), c.x, c.y);
+        m.sm.keys[i] = key;
+    }
+    __syncwarp();
+    top8_merge(m, top, n);
+}
+
+// Minimum key over full-resolution candidates (no top list), optional first-visit filter.
+template <class Gen>
+__device__ uint64_t full_stage(const DevParams& P, const Mb& m, int n, int range, int stride, bool use_seen, Gen gen) {
+    uint64_t best = UINT64_MAX;
+    for (int i = m.lane; i < n; i += 32) {
+        bool ok;
+        int2 c = gen(i, ok);
+        if (!ok) continue;
+        if (use_seen && seen_test_set(m.sm.seen_full, range, c.x, c.y)) continue;
+        const uint64_t k = int_key(mb_sad(P, m, c.x, c.y, stride), c.x, c.y);
+        best = k < best ? k : best;
+    }
+    return warp_min_u64(best);
+}
+
+__device__ __forceinline__ bool match_good(const DevParams& P, uint64_t sad, uint64_t pixels) {
+    if (!pixels || sad >= UINT64_MAX / 8) return false;
+    return sad <= pixels * 6u;
+}
+
+struct IntRes {
+    int dx, dy;
+    uint64_t cost;
+};
+
+__device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx, int gdy, int range, uint64_t pixels) {
+    // clear bitsets
+    const int words = ((2 * range + 1) * (2 * range + 1) + 31) >> 5;
+    for (int i = m.lane; i < words; i += 32) {
+        m.sm.seen[i] = 0;
+        m.sm.seen_full[i] = 0;
+    }
+    __syncwarp();
+    Top8 top;
+    top.n = 0;
+    // predictor seeds (:1843-1850)
+    {
+        int2 s[5];
+        int ns = 0;
+        s[ns++] = make_int2(iclamp(round_qpel_to_pixel(pi.pre.x), -range, range),
+                            iclamp(round_qpel_to_pixel(pi.pre.y), -range, range));
+        s[ns++] = make_int2(0, 0);
+        s[ns++] = make_int2(gdx, gdy);
+        if (pi.a_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
+        if (pi.c_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
+        umh_stage(P, m, top, ns, range, [&](int i) { return s[i]; });
+    }
+    // 5x5 around best (:1855-1859)
+    {
+        const int cx = key_dx(top.k[0]), cy = key_dy(top.k[0]);
+        umh_stage(P, m, top, 25, range, [&](int i) { return make_int2(cx + i % 5 - 2, cy + i / 5 - 2); });
+    }
+    // sparse lattice over the whole window (:1865-1870)
+    if (range >= 8) {
+        const int L = (2 * range) / 8 + 1;
+        umh_stage(P, m, top, L * L + 2 * L, range, [&](int i) {
+            if (i < L * L) return make_int2(-range + (i % L) * 8, -range + (i / L) * 8);
+            const int j = i - L * L;
+            const int d = -range + (j >> 1) * 8;
+            return (j & 1) ? make_int2(d, range) : make_int2(range, d);
+        });
+    }
+    // uneven cross (:1875-1884)
+    {
+        const int cs = range >= 96 ? 8 : (range >= 32 ? 4 : 2);
+        const int cx = key_dx(top.k[0]), cy = key_dy(top.k[0]);
+        const int vlimit = imin(range, imax(8, range / 2));
+        const int nh = range / cs, nv = vlimit / cs;
+        umh_stage(P, m, top, 2 * nh + 2 * nv, range, [&](int i) {
+            if (i < 2 * nh) {
+                const int d = cs * (i / 2 + 1);
+                return (i & 1) ? make_int2(cx + d, cy) : make_int2(cx - d, cy);
+            }
+            const int j = i - 2 * nh;
+            const int d = cs * (j / 2 + 1);
+            return (j & 1) ? make_int2(cx, cy + d) : make_int2(cx, cy - d);
+        });
+    }
+    // multi-hexagon rings (:1889-1897)
+    {
+        const int hs = range >= 96 ? 8 : (range >= 24 ? 4 : 2);
+        const int hx = key_dx(top.k[0]), hy = key_dy(top.k[0]);
+        const int nr = range / hs;
+        umh_stage(P, m, top, 6 * nr, range, [&](int i) {
+            const int r = hs * (i / 6 + 1), h = (r + 1) / 2;
+            switch (i % 6) {
+                case 0: return make_int2(hx - r, hy);
+                case 1: return make_int2(hx + r, hy);
+                case 2: return make_int2(hx - h, hy - r);
+                case 3: return make_int2(hx + h, hy - r);
+                case 4: return make_int2(hx - h, hy + r);
+                default: return make_int2(hx + h, hy + r);
+            }
+        });
+    }
+    // iterative small hexagon (:1902-1908)
+    for (int iter = 0; iter < 32; ++iter) {
+        const uint64_t before = top.k[0];
+        const int ox = key_dx(before), oy = key_dy(before);
+        umh_stage(P, m, top, 6, range, [&](int i) {
+            const int dxs[6] = {-2, 2, -1, 1, -1, 1}, dys[6] = {0, 0, -2, -2, 2, 2};
+            return make_int2(ox + dxs[i], oy + dys[i]);
+        });
+        if (key_dx(top.k[0]) == ox && key_dy(top.k[0]) == oy) break;
+    }
+    // closing diamond (:1909-1913)
+    {
+        const int ox = key_dx(top.k[0]), oy = key_dy(top.k[0]);
+        umh_stage(P, m, top, 4, range, [&](int i) {
+            const int dxs[4] = {-1, 1, 0, 0}, dys[4] = {0, 0, -1, 1};
+            return make_int2(ox + dxs[i], oy + dys[i]);
+        });
+    }
+    // full-resolution finalists (:1929-1952)
+    const int nf = imin(4, top.n);
+    uint64_t fk = full_stage(P, m, nf * 9, range, 1, true, [&](int i, bool& ok) {
+        ok = true;
+        const uint64_t t = top.k[i / 9];
+        return make_int2(iclamp(key_dx(t) + (i % 9) % 3 - 1, -range, range),
+                         iclamp(key_dy(t) + (i % 9) / 3 - 1, -range, range));
+    });
+    IntRes full{key_dx(fk), key_dy(fk), key_cost(fk)};
+    if (fk == UINT64_MAX) {  // unreachable in practice (:1948-1951)
+        full.dx = key_dx(top.k[0]);
+        full.dy = key_dy(top.k[0]);
+        full.cost = mb_sad(P, m, full.dx, full.dy, 1);
+        fk = int_key(full.cost, full.dx, full.dy);
+    }
+    // bounded rescue on a poor match (:1958-2020)
+    if (range > 0 && !match_good(P, full.cost, pixels)) {
+        const int step = range >= 8 ? 4 : (range >= 3 ? 2 : 1);
+        const int L = (2 * range) / step + 1;
+        const uint64_t ck = full_stage(P, m, L * L + 2 * L, range, 4, false, [&](int i, bool& ok) {
+            ok = true;
+            if (i < L * L) return make_int2(-range + (i % L) * step, -range + (i / L) * step);
+            const int j = i - L * L;
+            const int d = -range + (j >> 1) * step;
+            return (j & 1) ? make_int2(d, range) : make_int2(range, d);
+        });
+        const int cdx = key_dx(ck), cdy = key_dy(ck);
+        const int rr = imax(1, step - 1);
+        const int ylo = imax(-range, cdy - rr), yhi = imin(range, cdy + rr);
+        const int xlo = imax(-range, cdx - rr), xhi = imin(range, cdx + rr);
+        const int nx = xhi - xlo + 1, ny = yhi - ylo + 1;
+        const uint64_t rk = full_stage(P, m, nx * ny, range, 1, true, [&](int i, bool& ok) {
+            ok = true;
+            return make_int2(xlo + i % nx, ylo + i / nx);
+        });
+        if (rk < fk) fk = rk;
+        full = IntRes{key_dx(fk), key_dy(fk), key_cost(fk)};
+        if (pixels && full.cost > pixels * 24u && range <= 32) {
+            const int Ld = range + 1;  // -range..range step 2
+            const uint64_t dk = full_stage(P, m, Ld * Ld, range, 2, false, [&](int i, bool& ok) {
+                ok = true;
+                return make_int2(-range + (i % Ld) * 2, -range + (i / Ld) * 2);
+            });
+            const int ddx = key_dx(dk), ddy = key_dy(dk);
+            const int y0 = imax(-range, ddy - 2), y1 = imin(range, ddy + 2);
+            const int x0 = imax(-range, ddx - 2), x1 = imin(range, ddx + 2);
+            const int mx = x1 - x0 + 1, my = y1 - y0 + 1;
+            const uint64_t dfk = full_stage(P, m, mx * my, range, 1, true, [&](int i, bool& ok) {
+                ok = true;
+                return make_int2(x0 + i % mx, y0 + i / mx);
+            });
+            if (dfk < fk) fk = dfk;
+            full = IntRes{key_dx(fk), key_dy(fk), key_cost(fk)};
+        }
+    }
+    return full;
+}
+
+// integer_motion_diamond, encoder_motion_diamond.cpp:13-73
+__device__ IntRes diamond(const DevParams& P, const Mb& m, const PInfo& pi, int gdx, int gdy, int range) {
+    uint64_t best = int_key(mb_sad(P, m, 0, 0, 1), 0, 0);
+    if (key_cost(best) == 0) return IntRes{0, 0, 0};
+    int2 seeds[4];
+    int ns = 0;
+    seeds[ns++] = make_int2(round_qpel_to_pixel(pi.pre.x), round_qpel_to_pixel(pi.pre.y));
+    seeds[ns++] = make_int2(gdx, gdy);
+    if (pi.a_valid) seeds[ns++] = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
+    if (pi.c_valid) seeds[ns++] = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
+    {
+        uint64_t k = UINT64_MAX;
+        if (m.lane < ns) {
+            const int dx = iclamp(seeds[m.lane].x, -range, range), dy = iclamp(seeds[m.lane].y, -range, range);
+            k = int_key(mb_sad(P, m, dx, dy, 1), dx, dy);
+        }
+        k = warp_min_u64(k);
+        best = k < best ? k : best;
+    }
+    int px = key_dx(best), py = key_dy(best);
+    bool have_prev = false;
+    for (int step = 0; step <= 4 * range + 1; ++step) {
+        const uint64_t center = best;
+        const int cx = key_dx(center), cy = key_dy(center);
+        uint64_t k = UINT64_MAX;
+        if (m.lane < 4) {
+            const int dxs[4] = {-1, 1, 0, 0}, dys[4] = {0, 0, -1, 1};
+            const int dx = cx + dxs[m.lane], dy = cy + dys[m.lane];
+            if (!(dx < -range || dx > range || dy < -range || dy > range) && !(have_prev && dx == px && dy == py))
+                k = int_key(mb_sad(P, m, dx, dy, 1), dx, dy);
+        }
+        k = warp_min_u64(k);
+        const uint64_t winner = k < center ? k : center;
+        if (winner == center) break;
+        px = cx;
+        py = cy;
+        have_prev = true;
+        best = winner;
+        if (key_cost(best) == 0) break;
+    }
+    return IntRes{key_dx(best), key_dy(best), key_cost(best)};
+}
+
+// ---- staged sub-pel refinement (encoder_motion.cpp:3247-3594) ---------------------------
+
+struct RefineOut {
+    int2 mv;
+    uint64_t screen_sad;
+};
+
+__device__ __forceinline__ int make_even(int v) { return !(v & 1) ? v : (v > 0 ? v - 1 : v + 1); }
+
+// Appends the batch MVs that are not yet in the list (the `add` lambda, :3324-3337), scoring
+// the new ones with the CPU law in one warp-parallel pass.
+__device__ void list_add_batch(const DevParams& P, const Mb& m, int& n, const int2* mvs, int nb, int bx, int by, int bw,
+                               int bh, int mode) {
+    // dedup on every lane identically (tiny lists)
+    int2* nb_mv = m.sm.batch;
+    int nn = 0;
+    for (int i = 0; i < nb; ++i) {
+        bool dup = false;
+        for (int j = 0; j < n && !dup; ++j) dup = m.sm.list_mv[j].x == mvs[i].x && m.sm.list_mv[j].y == mvs[i].y;
+        for (int j = 0; j < nn && !dup; ++j) dup = nb_mv[j].x == mvs[i].x && nb_mv[j].y == mvs[i].y;
+        if (!dup) {
+            __syncwarp();
+            if (m.lane == 0) nb_mv[nn] = mvs[i];
+            __syncwarp();
+            ++nn;
+        }
+    }
+    if (!nn) return;
+    sad_batch(P, m, nb_mv, nn, bx, by, bw, bh, mode, m.sm.batch_cost);
+    if (m.lane < nn) {
+        m.sm.list_mv[n + m.lane] = nb_mv[m.lane];
+        m.sm.list_sad[n + m.lane] = m.sm.batch_cost[m.lane];  // hidden padding already BAD
+    }
+    n += nn;
+    __syncwarp();
+}
+
+__device__ __forceinline__ const uint64_t* list_find(const Mb& m, int n, int2 mv, int& idx) {
+    for (int j = 0; j < n; ++j)
+        if (m.sm.list_mv[j].x == mv.x && m.sm.list_mv[j].y == mv.y) {
+            idx = j;
+            return &m.sm.list_sad[j];
+        }
+    idx = -1;
+    return nullptr;
+}
+
+__device__ void update_min(const Mb& m, int n, const int2* mvs, int nb, int2& best, uint64_t& best_sad) {
+    for (int i = 0; i < nb; ++i) {
+        int j;
+        const uint64_t* s = list_find(m, n, mvs[i], j);
+        if (s && (*s < best_sad || (*s == best_sad && tie_less(mvs[i], best)))) {
+            best_sad = *s;
+            best = mvs[i];
+        }
+    }
+}
+
+// refine_motion_integer_only, encoder_motion.cpp:3247-3269
+__device__ RefineOut refine_integer_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
+                                         int range, int mode, uint64_t known) {
+    const Bounds qb = bounds_qpel(range);
+    auto snap = [](int q, int lo, int hi) {
+        q = iclamp(q, lo, hi);
+        const int nr = q >= 0 ? (q + 1) / 4 : (q - 1) / 4;
+        return iclamp(nr * 4, lo, hi / 4 * 4);
+    };
+    int2 integer = make_int2(snap(seed.x, qb.xmin, qb.xmax), snap(seed.y, qb.ymin, qb.ymax));
+    if (hidden_padding(P, bx, by, bw, bh, integer.x, integer.y, mode, chroma_gate(bx, by, bw, bh))) integer = make_int2(0, 0);
+    uint64_t s;
+    if (integer.x == seed.x && integer.y == seed.y && known != UINT64_MAX) {
+        s = known;
+    } else {
+        if (m.lane == 0) m.sm.batch[8] = integer;
+        __syncwarp();
+        sad_batch(P, m, m.sm.batch + 8, 1, bx, by, bw, bh, mode, m.sm.batch_cost + 8);
+        s = m.sm.batch_cost[8];
+    }
+    return RefineOut{integer, s};
+}
+
+// refine_qpel_block / refine_motion_block (me_quality SAD), encoder_motion.cpp:3596-3749
+__device__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
+                                     int mode, uint64_t known) {
+    const int limit_q = 4 * P.subpel_range;
+    if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q)
+        return refine_integer_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+    const Bounds qb = bounds_qpel(range);
+    const int xmin = imax(qb.xmin, -limit_q), xmax = imin(qb.xmax, limit_q);
+    const int ymin = imax(qb.ymin, -limit_q), ymax = imin(qb.ymax, limit_q);
+    const bool hp = mode_halfpel(mode);
+    const int emode = hp ? mode : VC1CU_MV_QPEL;
+    seed.x = iclamp(seed.x, xmin, xmax);
+    seed.y = iclamp(seed.y, ymin, ymax);
+    if (hp) { seed.x = make_even(seed.x); seed.y = make_even(seed.y); }
+    if (hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, emode, chroma_gate(bx, by, bw, bh))) {
+        seed = make_int2(0, 0);
+        known = UINT64_MAX;
+    }
+    int n = 0;
+    if (known != UINT64_MAX) {
+        if (m.lane == 0) { m.sm.list_mv[0] = seed; m.sm.list_sad[0] = known; }
+        __syncwarp();
+        n = 1;
+    } else {
+        list_add_batch(P, m, n, &seed, 1, bx, by, bw, bh, emode);
+    }
+    int2 best = seed;
+    uint64_t cost = m.sm.list_sad[0];
+    auto fix = [&](int2 v) {
+        v.x = iclamp(v.x, xmin, xmax);
+        v.y = iclamp(v.y, ymin, ymax);
+        if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
+        return v;
+    };
+    auto stage = [&](const int2* pts, int np) {
+        int2 b[9];
+        for (int i = 0; i < np; ++i) b[i] = fix(pts[i]);
+        list_add_batch(P, m, n, b, np, bx, by, bw, bh, emode);
+        update_min(m, n, b, np, best, cost);
+    };
+    if (P.fast_subpel) {
+        if (hp || true) {
+            if (cost == 0 && best.x == 0 && best.y == 0) return RefineOut{best, 0};
+        }
+        int2 c4[4] = {{seed.x - 2, seed.y}, {seed.x + 2, seed.y}, {seed.x, seed.y - 2}, {seed.x, seed.y + 2}};
+        stage(c4, 4);
+        const int2 axis = best;
+        const int dx = axis.x - seed.x, dy = axis.y - seed.y;
+        if (dx && !dy) { int2 c2[2] = {{axis.x, axis.y - 2}, {axis.x, axis.y + 2}}; stage(c2, 2); }
+        else if (dy && !dx) { int2 c2[2] = {{axis.x - 2, axis.y}, {axis.x + 2, axis.y}}; stage(c2, 2); }
+        if (!hp) {
+            const int2 half = best;
+            int2 q4[4] = {{half.x - 1, half.y}, {half.x + 1, half.y}, {half.x, half.y - 1}, {half.x, half.y + 1}};
+            stage(q4, 4);
+            const int2 qa = best;
+            const int qdx = qa.x - half.x, qdy = qa.y - half.y;
+            if (qdx && !qdy) { int2 c2[2] = {{qa.x, qa.y - 1}, {qa.x, qa.y + 1}}; stage(c2, 2); }
+            else if (qdy && !qdx) { int2 c2[2] = {{qa.x - 1, qa.y}, {qa.x + 1, qa.y}}; stage(c2, 2); }
+        }
+    } else {
+        int2 h9[9];
+        for (int i = 0; i < 9; ++i) h9[i] = make_int2(seed.x + (i % 3 - 1) * 2, seed.y + (i / 3 - 1) * 2);
+        stage(h9, 9);
+        if (!hp) {
+            const int2 half = best;
+            int2 q9[9];
+            for (int i = 0; i < 9; ++i) q9[i] = make_int2(half.x + i % 3 - 1, half.y + i / 3 - 1);
+            stage(q9, 9);
+        }
+    }
+    return RefineOut{best, cost};
+}
+
+// Vc1Encoder::refine_motion_block_staged (me_quality RATE / SATD), encoder_motion.cpp:3271-3535
+__device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
+                                   int mode, const PInfo& pi, bool more, uint64_t known) {
+    const int limit_q = 4 * P.subpel_range;
+    if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q)
+        return refine_integer_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+    if (P.me_quality == 0) return refine_sad_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+    const Bounds qb = bounds_qpel(range);
+    const int xmin = imax(qb.xmin, -limit_q), xmax = imin(qb.xmax, limit_q);
+    const int ymin = imax(qb.ymin, -limit_q), ymax = imin(qb.ymax, limit_q);
+    const bool hp = mode_halfpel(mode);
+    const bool cg = chroma_gate(bx, by, bw, bh);
+    seed.x = iclamp(seed.x, xmin, xmax);
+    seed.y = iclamp(seed.y, ymin, ymax);
+    if (hp) { seed.x = make_even(seed.x); seed.y = make_even(seed.y); }
+    int n = 0;
+    // add(seed, known)
+    if (known != UINT64_MAX) {
+        if (m.lane == 0) {
+            m.sm.list_mv[0] = seed;
+            m.sm.list_sad[0] = hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg) ? kBad : known;
+        }
+        __syncwarp();
+        n = 1;
+    } else {
+        list_add_batch(P, m, n, &seed, 1, bx, by, bw, bh, mode);
+    }
+    if (hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg)) {
+        const int2 z = make_int2(0, 0);
+        list_add_batch(P, m, n, &z, 1, bx, by, bw, bh, mode);
+    }
+    int2 half_best = seed;
+    uint64_t half_sad = m.sm.list_sad[0];
+    const bool fast = P.fast_subpel;
+    auto clampmv = [&](int x, int y) {
+        int2 v = make_int2(iclamp(x, xmin, xmax), iclamp(y, ymin, ymax));
+        if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
+        return v;
+    };
+    {
+        int2 hb[9];
+        int nb = 0;
+        if (fast) {
+            hb[nb++] = seed;
+            hb[nb++] = clampmv(seed.x - 2, seed.y);
+            hb[nb++] = clampmv(seed.x + 2, seed.y);
+            hb[nb++] = clampmv(seed.x, seed.y - 2);
+            hb[nb++] = clampmv(seed.x, seed.y + 2);
+        } else {
+            for (int oy = -2; oy <= 2; oy += 2)
+                for (int ox = -2; ox <= 2; ox += 2) hb[nb++] = clampmv(seed.x + ox, seed.y + oy);
+        }
+        list_add_batch(P, m, n, hb, nb, bx, by, bw, bh, mode);
+        update_min(m, n, hb, nb, half_best, half_sad);
+    }
+    if (fast && !(half_best.x == seed.x && half_best.y == seed.y)) {
+        int2 dg[2];
+        int nd = 0;
+        const int dx = half_best.x - seed.x, dy = half_best.y - seed.y;
+        if (dx && !dy) {
+            dg[nd++] = make_int2(half_best.x, iclamp(seed.y - 2, ymin, ymax));
+            dg[nd++] = make_int2(half_best.x, iclamp(seed.y + 2, ymin, ymax));
+        } else if (dy && !dx) {
+            dg[nd++] = make_int2(iclamp(seed.x - 2, xmin, xmax), half_best.y);
+            dg[nd++] = make_int2(iclamp(seed.x + 2, xmin, xmax), half_best.y);
+        }
+        if (hp)
+            for (int i = 0; i < nd; ++i) { dg[i].x = make_even(dg[i].x); dg[i].y = make_even(dg[i].y); }
+        if (nd) {
+            list_add_batch(P, m, n, dg, nd, bx, by, bw, bh, mode);
+            update_min(m, n, dg, nd, half_best, half_sad);
+        }
+    }
+    if (!hp) {
+        if (fast) {
+            const int2 qc = half_best;
+            int2 q5[5] = {qc, make_int2(iclamp(qc.x - 1, xmin, xmax), qc.y), make_int2(iclamp(qc.x + 1, xmin, xmax), qc.y),
+                          make_int2(qc.x, iclamp(qc.y - 1, ymin, ymax)), make_int2(qc.x, iclamp(qc.y + 1, ymin, ymax))};
+            list_add_batch(P, m, n, q5, 5, bx, by, bw, bh, mode);
+            int j;
+            uint64_t qcost = *list_find(m, n, qc, j);
+            int2 qbmv = qc;
+            update_min(m, n, q5, 5, qbmv, qcost);
+            int2 q2[2];
+            int n2 = 0;
+            const int dx = qbmv.x - qc.x, dy = qbmv.y - qc.y;
+            if (dx && !dy) {
+                q2[n2++] = make_int2(qbmv.x, iclamp(qc.y - 1, ymin, ymax));
+                q2[n2++] = make_int2(qbmv.x, iclamp(qc.y + 1, ymin, ymax));
+            } else if (dy && !dx) {
+                q2[n2++] = make_int2(iclamp(qc.x - 1, xmin, xmax), qbmv.y);
+                q2[n2++] = make_int2(iclamp(qc.x + 1, xmin, xmax), qbmv.y);
+            }
+            if (n2) list_add_batch(P, m, n, q2, n2, bx, by, bw, bh, mode);
+        } else {
+            int2 q9[9];
+            for (int i = 0; i < 9; ++i)
+                q9[i] = make_int2(iclamp(half_best.x + i % 3 - 1, xmin, xmax), iclamp(half_best.y + i / 3 - 1, ymin, ymax));
+            list_add_batch(P, m, n, q9, 9, bx, by, bw, bh, mode);
+        }
+    }
+    // sort by (sad, tie_less), keep 8 / 4 (:3445-3456)
+    const int keep = fast ? 4 : 8;
+    int2 my_mv = make_int2(0, 0);
+    uint64_t my_sad = 0;
+    int rank = 32;
+    if (m.lane < n) {
+        my_mv = m.sm.list_mv[m.lane];
+        my_sad = m.sm.list_sad[m.lane];
+        rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const uint64_t s = m.sm.list_sad[j];
+            const int2 v = m.sm.list_mv[j];
+            if (s < my_sad || (s == my_sad && tie_less(v, my_mv))) ++rank;
+        }
+    }
+    uint64_t screen = UINT64_MAX;
+    {
+        const uint64_t cand = rank == 0 ? my_sad : UINT64_MAX;
+        screen = warp_min_u64(cand);
+    }
+    __syncwarp();
+    const int nk = imin(n, keep);
+    // compact the kept candidates by rank: slot = rank
+    if (m.lane < n && rank < nk) {
+        m.sm.batch[rank] = my_mv;
+        m.sm.batch_cost[rank] = my_sad;
+    }
+    __syncwarp();
+    // rate + score (:3458-3476)
+    if (m.lane < nk) {
+        const int2 mv = m.sm.batch[m.lane];
+        int2 pred = pi.pre;
+        uint32_t rate = 0;
+        if (pi.hybrid) {
+            pred = modular_mv_distance(P, mv, pi.a) <= modular_mv_distance(P, mv, pi.c) ? pi.a : pi.c;
+            ++rate;
+        }
+        rate += mv_rate_bits(P, mv, pred, mode, more);
+        m.sm.list_rate[m.lane] = rate;
+        m.sm.list_key[m.lane] = score_key(P, m.sm.batch_cost[m.lane], rate);
+    }
+    __syncwarp();
+    // rate winner: min over (score, sad, tie_less)
+    int rw = 0;
+    for (int i = 1; i < nk; ++i) {
+        const unsigned __int128 a = m.sm.list_key[i], b = m.sm.list_key[rw];
+        const uint64_t sa = m.sm.batch_cost[i], sb = m.sm.batch_cost[rw];
+        if (a < b || (a == b && (sa < sb || (sa == sb && tie_less(m.sm.batch[i], m.sm.batch[rw]))))) rw = i;
+    }
+    if (P.me_quality == 1) return RefineOut{m.sm.batch[rw], screen};
+    const uint64_t rws = m.sm.batch_cost[rw];
+    const uint64_t pct3 = (rws / 100) * 3 + (((rws % 100) * 3 + 99) / 100);
+    const uint64_t slack = pct3 > 4 ? pct3 : 4;
+    const uint64_t limit = rws > UINT64_MAX - slack ? UINT64_MAX : rws + slack;
+    // SATD of the eligible shortlist (:3507-3524)
+    int2* el = m.sm.batch + 16;
+    int ne = 0;
+    for (int i = 0; i < nk; ++i) {
+        const uint64_t s = m.sm.batch_cost[i];
+        if (s < UINT64_MAX / 8 && s <= limit) {
+            if (m.lane == 0) el[ne] = m.sm.batch[i];
+            ++ne;
+        }
+    }
+    __syncwarp();
+    satd_batch(P, m, el, ne, bx, by, bw, bh, mode, m.sm.list_satd);
+    // final order (:3526-3531): eligible first, score, satd, sad, tie
+    int best = -1, ei = 0;
+    unsigned __int128 bkey = 0;
+    uint64_t bsatd = 0, bsad = 0;
+    for (int i = 0; i < nk; ++i) {
+        const uint64_t s = m.sm.batch_cost[i];
+        const bool elig = s < UINT64_MAX / 8 && s <= limit;
+        const uint64_t satd = elig ? m.sm.list_satd[ei++] : kBad;
+        const unsigned __int128 k = score_key(P, satd, m.sm.list_rate[i]);
+        bool better;
+        if (best < 0) better = true;
+        else {
+            const bool belig = m.sm.batch_cost[best] < UINT64_MAX / 8 && m.sm.batch_cost[best] <= limit;
+            if (elig != belig) better = elig;
+            else if (k != bkey) better = k < bkey;
+            else if (satd != bsatd) better = satd < bsatd;
+            else if (s != bsad) better = s < bsad;
+            else better = tie_less(m.sm.batch[i], m.sm.batch[best]);
+        }
+        if (better) {
+            best = i;
+            bkey = k;
+            bsatd = satd;
+            bsad = s;
+        }
+    }
+    const int2 res = m.sm.batch[best];
+    __syncwarp();
+    return RefineOut{res, screen};
+}
+
+// ---- predictor state of the current pass --------------------------------------------------
+
+__device__ __forceinline__ int2 ld_mv(const int2* p) {
+    const int2 v = __ldcg(p);
+    return v;
+}
+
+// Vc1Encoder::predictor_info, encoder_motion.cpp:1312-1352 (reads the pass's 1-MV field)
+__device__ PInfo predictor_info(const DevParams& P, const DevResult& o, int mx, int my) {
+    PInfo r;
+    const int mbw = P.mbw;
+    int2 A = make_int2(0, 0), B = A, C = A;
+    const bool a_valid = my > 0, c_valid = mx > 0, b_valid = my > 0 && mbw > 1;
+    if (a_valid) A = ld_mv(&o.mvs[(my - 1) * mbw + mx]);
+    if (c_valid) C = ld_mv(&o.mvs[my * mbw + mx - 1]);
+    if (b_valid) B = ld_mv(&o.mvs[(my - 1) * mbw + ((mx == mbw - 1) ? mx - 1 : mx + 1)]);
+    int2 pre = make_int2(0, 0);
+    if (a_valid) pre = A;
+    else if (c_valid) pre = C;
+    else if (b_valid) pre = B;
+    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
+        pre.x = median3(A.x, B.x, C.x);
+        pre.y = median3(A.y, B.y, C.y);
+    }
+    pullback(pre, mx * 64, my * 64, mbw * 64 - 4, P.mbh * 64 - 4, -60);
+    bool hybrid = false;
+    if (a_valid && c_valid) {
+        if (iabs(pre.x - A.x) + iabs(pre.y - A.y) > 32) hybrid = true;
+        else if (iabs(pre.x - C.x) + iabs(pre.y - C.y) > 32) hybrid = true;
+    }
+    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
+    return r;
+}
+
+// Block-MV field accessor: the current MB's blocks come from shared memory (cur4), the
+// neighbours' from HBM.
+struct Field {
+    const DevResult* o;
+    const int2* cur4;
+    int mbw, mbh, mx, my;
+    __device__ int2 get(int x, int y) const {
+        if (x < 0 || y < 0 || x >= mbw * 2 || y >= mbh * 2) return make_int2(0, 0);
+        const int bx = x >> 1, by = y >> 1, k = ((y & 1) << 1) | (x & 1);
+        if (bx == mx && by == my) return cur4[k];
+        return ld_mv(&o->bmv[(by * mbw + bx) * 4 + k]);
+    }
+    __device__ bool intra(int x, int y) const {
+        if (x < 0 || y < 0 || x >= mbw * 2 || y >= mbh * 2) return false;
+        const int bx = x >> 1, by = y >> 1;
+        if (bx == mx && by == my) return false;  // the current MB is never intra while it is searched
+        return __ldcg(&o->intra[by * mbw + bx]) != 0;
+    }
+};
+
+// Vc1Encoder::predictor_info_mixed_1mv, encoder_motion.cpp:1354-1406
+__device__ PInfo predictor_mixed_1mv(const DevParams& P, const Field& f, int mx, int my) {
+    PInfo r;
+    const int bx = mx * 2, by = my * 2, mbw = P.mbw;
+    const bool a_valid = my > 0, c_valid = mx > 0, b_valid = my > 0 && mbw > 1;
+    const int2 z = make_int2(0, 0);
+    const int2 A = a_valid ? f.get(bx, by - 1) : z;
+    const int2 C = c_valid ? f.get(bx - 1, by) : z;
+    int2 B = z;
+    if (b_valid) B = f.get(bx + ((mx == mbw - 1) ? -1 : 2), by - 1);
+    int2 pre = z;
+    if (a_valid) pre = A;
+    else if (c_valid) pre = C;
+    else if (b_valid) pre = B;
+    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
+        pre.x = median3(A.x, B.x, C.x);
+        pre.y = median3(A.y, B.y, C.y);
+    }
+    pullback(pre, mx * 64, my * 64, mbw * 64 - 4, P.mbh * 64 - 4, -60);
+    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
+    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
+    return r;
+}
+
+// Vc1Encoder::predictor_info_4mv, encoder_motion.cpp:1408-1466
+__device__ PInfo predictor_4mv(const DevParams& P, const Field& f, int mx, int my, int n) {
+    PInfo r;
+    const int mbw = P.mbw;
+    const int bx = mx * 2 + (n & 1), by = my * 2 + ((n >> 1) & 1);
+    const bool a_valid = my > 0 || n == 2 || n == 3;
+    const bool c_valid = mx > 0 || n == 1 || n == 3;
+    const bool b_valid = a_valid;
+    const int2 z = make_int2(0, 0);
+    const int2 A = a_valid ? f.get(bx, by - 1) : z;
+    const int2 C = c_valid ? f.get(bx - 1, by) : z;
+    int2 B = z;
+    if (b_valid) {
+        int bxx = bx;
+        if (n == 0) bxx += mx ? -1 : 1;
+        else if (n == 1) bxx += (mx == mbw - 1) ? -1 : 1;
+        else if (n == 2) bxx += 1;
+        else bxx -= 1;
+        B = f.get(bxx, by - 1);
+    }
+    int2 pre = z;
+    if (a_valid) pre = A;
+    else if (c_valid) pre = C;
+    else if (b_valid) pre = B;
+    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
+        pre.x = median3(A.x, B.x, C.x);
+        pre.y = median3(A.y, B.y, C.y);
+    }
+    pullback(pre, mx * 64 + ((n == 1 || n == 3) ? 32 : 0), my * 64 + ((n == 2 || n == 3) ? 32 : 0), mbw * 64 - 4,
+             P.mbh * 64 - 4, -28);
+    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
+    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
+    return r;
+}
+
+__device__ __forceinline__ int median4(int a, int b, int c, int d) {
+    if (a < b) {
+        if (c < d) return (imin(b, d) + imax(a, c)) / 2;
+        return (imin(b, c) + imax(a, d)) / 2;
+    }
+    if (c < d) return (imin(a, d) + imax(b, c)) / 2;
+    return (imin(a, c) + imax(b, d)) / 2;
+}
+
+// ---- wavefront synchronisation ----------------------------------------------------------
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits (bounded) until the MB at (x,y) of the same pass is published. Returns false and
+// raises the launch's abort flag on timeout.
+__device__ bool wait_mb(const DevParams& P, const DevResult& o, int x, int y, uint32_t epoch, LaunchStatus* st) {
+    if (x < 0 || y < 0 || x >= P.mbw) return true;
+    const uint32_t* f = &o.done[y * P.mbw + x];
+    for (long it = 0; it < (1L << 24); ++it) {
+        if (ld_acquire(f) == epoch) return true;
+        if (*(volatile int*)&st->abort) return false;
+        __nanosleep(128);
+    }
+    atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
+    atomicExch(&st->abort, 1);
+    atomicAdd(&st->timeouts, 1u);
+    return false;
+}
+
+// ---- the kernel ---------------------------------------------------------------------------
+
+__device__ void carve(WarpMem& s, uint8_t* base, const WinCfg& wc) {
+    uint8_t* p = base;
+    auto take = [&](size_t bytes) {
+        uint8_t* q = p;
+        p += (bytes + 15) & ~size_t(15);
+        return q;
+    };
+    s.list_key = (unsigned __int128*)take(sizeof(unsigned __int128) * kListCap);
+    s.list_sad = (uint64_t*)take(8 * kListCap);
+    s.list_satd = (uint64_t*)take(8 * kListCap);
+    s.batch_cost = (uint64_t*)take(8 * 32);
+    s.keys = (uint64_t*)take(8 * (size_t)wc.keys_cap);
+    s.list_mv = (int2*)take(8 * kListCap);
+    s.batch = (int2*)take(8 * 32);
+    s.list_rate = (uint32_t*)take(4 * kListCap);
+    s.misc = (int*)take(4 * 16);
+    s.seen = (uint32_t*)take(4 * (size_t)wc.seen_words);
+    s.seen_full = (uint32_t*)take(4 * (size_t)wc.seen_words);
+    s.cur = take(256);
+    s.win = take((size_t)wc.ww * wc.ww);
+}
+
+__host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
+    auto r = [](int b) { return (b + 15) & ~15; };
+    return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(8 * kListCap) + r(8 * 32) +
+           r(4 * kListCap) + r(64) + 2 * r(4 * wc.seen_words) + r(256) + r(wc.ww * wc.ww);
+}
+
+int warp_bytes_for_host(const WinCfg& wc) { return warp_bytes_for(wc); }
+
+__device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int cdx, int cdy, int rw) {
+    m.ww = 16 + 2 * rw + 3;
+    m.wx0 = m.x0 + cdx - rw - 1;
+    m.wy0 = m.y0 + cdy - rw - 1;
+    for (int r = 0; r < m.ww; ++r) {
+        const uint8_t* row = ref.y + (size_t)iclamp(m.wy0 + r, 0, P.H - 1) * ref.pitch_y;
+        uint8_t* dst = m.sm.win + r * m.ww;
+        for (int c = m.lane; c < m.ww; c += 32) dst[c] = __ldg(row + iclamp(m.wx0 + c, 0, P.W - 1));
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes,
+                                                          int npass, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    Mb m;
+    m.lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    carve(m.sm, smem + (size_t)warp * wc.warp_bytes, wc);
+    const unsigned total = (unsigned)npass * (unsigned)(P.mbw * P.mbh);
+    const int range = P.range, local_range = P.local_range;
+    for (;;) {
+        unsigned item = 0;
+        if (m.lane == 0) item = atomicAdd(&st->queue, 1u);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= total) break;
+        const int pi_idx = (int)(item % (unsigned)npass);
+        const int mbi = (int)(item / (unsigned)npass);
+        const PassDesc& d = passes[pi_idx];
+        m.d = &d;
+        m.mx = mbi % P.mbw;
+        m.my = mbi / P.mbw;
+        m.pos = mbi;
+        m.x0 = m.mx * 16;
+        m.y0 = m.my * 16;
+        m.aw = imax(0, imin(16, P.W - m.x0));
+        m.ah = imax(0, imin(16, P.H - m.y0));
+        m.gref = GlobSampler{d.ref.y, d.ref.pitch_y, P.W, P.H};
+        const DevResult& o = d.out;
+        const bool aborted = *(volatile int*)&st->abort;
+        // wavefront: left, top-left, top, top-right of the same pass
+        bool ok = !aborted;
+        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my - 1, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx, m.my - 1, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
+        __syncwarp();
+        if (ok) {
+            // current MB into shared memory (zero outside the raster)
+            for (int i = m.lane; i < 256; i += 32) {
+                const int y = i >> 4, x = i & 15;
+                m.sm.cur[i] = (x < m.aw && y < m.ah) ? __ldg(d.cur.y + (size_t)(m.y0 + y) * d.cur.pitch_y + m.x0 + x) : 0;
+            }
+            __syncwarp();
+        }
+        if (ok && P.range == 0) {
+            // --search-range 0 is a real no-search mode (encoder_motion.cpp:72-85)
+            m.ww = 0;
+            m.wx0 = m.wy0 = 0;
+            const uint64_t z = mb_sad(P, m, 0, 0, 1);
+            if (m.lane == 0) {
+                o.mvs[m.pos] = make_int2(0, 0);
+                for (int k = 0; k < 4; ++k) o.bmv[m.pos * 4 + k] = make_int2(0, 0);
+                o.use4[m.pos] = 0;
+                o.intra[m.pos] = 0;
+                o.screen[m.pos] = z;
+                o.ratio[m.pos] = -1.0;
+                o.dl[m.pos] = -1.0;  // the zero path returns before the seed's distant fields are copied
+                o.dc[m.pos] = -1.0;
+                o.dd[m.pos] = 0;
+                o.chosen[m.pos] = z;
+                o.temporal[m.pos] = z;
+                o.flags[m.pos] = 0;
+            }
+            ok = false;
+        }
+        if (ok) {
+            const bool allow_4mv = d.mode == VC1CU_MV_MIXED;
+            const int one_mode = allow_4mv ? VC1CU_MV_QPEL : d.mode;
+            __shared__ int2 cur4s[4][4];
+            int2* cur4 = cur4s[warp];
+            if (m.lane < 4) cur4[m.lane] = make_int2(0, 0);
+            __syncwarp();
+            Field field{&o, cur4, P.mbw, P.mbh, m.mx, m.my};
+            const PInfo rate_pi = predictor_mixed_1mv(P, field, m.mx, m.my);
+            const uint64_t pixels = (uint64_t)m.aw * (uint64_t)m.ah;
+            RefineOut one;
+            double dl = -1.0, dc = -1.0;
+            uint8_t dd = 0;
+            if (d.seeded) {
+                int2 seed = d.seed_mvs[m.pos];
+                const Bounds qb = bounds_qpel(range);
+                seed.x = iclamp(seed.x, qb.xmin, qb.xmax);
+                seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
+                load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc.rw);
+                one = refine_staged(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, rate_pi, true, UINT64_MAX);
+                dl = d.seed_dl[m.pos];
+                dc = d.seed_dc[m.pos];
+                dd = d.seed_dd[m.pos];
+            } else {
+                load_window(P, m, d.ref, 0, 0, wc.rw);
+                const PInfo pi = predictor_info(P, o, m.mx, m.my);
+                const int gdx = o.global[0], gdy = o.global[1];
+                const IntRes im = P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
+                                                      : umh(P, m, pi, gdx, gdy, local_range, pixels);
+                if (P.long_range_mode != 2 && pixels) dl = (double)im.cost / (double)pixels;
+                one = refine_staged(P, m, m.x0, m.y0, 16, 16, make_int2(im.dx * 4, im.dy * 4), range, one_mode, rate_pi,
+                                    true, im.cost);
+            }
+            if (hidden_padding(P, m.x0, m.y0, 16, 16, one.mv.x, one.mv.y, one_mode, true)) {
+                if (m.lane == 0) m.sm.batch[31] = make_int2(0, 0);
+                __syncwarp();
+                sad_batch(P, m, m.sm.batch + 31, 1, m.x0, m.y0, 16, 16, one_mode, m.sm.batch_cost + 31);
+                one.mv = make_int2(0, 0);
+                one.screen_sad = m.sm.batch_cost[31];
+            }
+            const uint64_t one_sad = one.screen_sad;
+            int2 out4[4] = {one.mv, one.mv, one.mv, one.mv};
+            int2 out_mv = one.mv;
+            uint8_t use4 = 0, intra = 0;
+            uint64_t chosen = one_sad, temporal_screen = one_sad;
+            const double lambda = P.lambda;
+            if (allow_4mv) {
+                if (m.lane < 4) cur4[m.lane] = one.mv;
+                __syncwarp();
+                int2 four[4];
+                uint64_t four_sad = 0, four_screen = 0, extra_bits = 1;
+                const int limit = 4 * P.subpel_range;
+                auto wsr = [&](int2 v) {
+                    if (imax(iabs(v.x), iabs(v.y)) > limit) { v.x = (v.x / 4) * 4; v.y = (v.y / 4) * 4; }
+                    return v;
+                };
+                const Bounds qb = bounds_qpel(range);
+                for (int k = 0; k < 4; ++k) {
+                    const PInfo pi4 = predictor_4mv(P, field, m.mx, m.my, k);
+                    const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
+                    // 10 seeds (:266-283), scored together, chosen in the reference's visit order
+                    int2 sd[11];
+                    sd[0] = wsr(one.mv);
+                    const int2 raw[10] = {one.mv, pi4.pre, {one.mv.x - 8, one.mv.y}, {one.mv.x + 8, one.mv.y},
+                                          {one.mv.x, one.mv.y - 8}, {one.mv.x, one.mv.y + 8}, {one.mv.x - 4, one.mv.y},
+                                          {one.mv.x + 4, one.mv.y}, {one.mv.x, one.mv.y - 4}, {one.mv.x, one.mv.y + 4}};
+                    for (int s = 0; s < 10; ++s)
+                        sd[s + 1] = wsr(make_int2(iclamp(raw[s].x, qb.xmin, qb.xmax), iclamp(raw[s].y, qb.ymin, qb.ymax)));
+                    if (m.lane < 11) m.sm.batch[m.lane] = sd[m.lane];
+                    __syncwarp();
+                    sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
+                    int2 best_seed = sd[0];
+                    uint64_t seed_cost = m.sm.batch_cost[0];
+                    for (int s = 1; s <= 10; ++s) {
+                        const int2 v = sd[s];
+                        if (v.x == best_seed.x && v.y == best_seed.y) continue;
+                        const uint64_t c = m.sm.batch_cost[s];
+                        const int cm = iabs(v.x) + iabs(v.y), bm = iabs(best_seed.x) + iabs(best_seed.y);
+                        if (c < seed_cost || (c == seed_cost && cm < bm)) { seed_cost = c; best_seed = v; }
+                    }
+                    __syncwarp();
+                    const RefineOut r = refine_staged(P, m, bx, by, 8, 8, best_seed, range, VC1CU_MV_MIXED, pi4, true, seed_cost);
+                    four_screen += r.screen_sad;
+                    four[k] = r.mv;
+                    if (m.lane == 0) cur4[k] = r.mv;
+                    __syncwarp();
+                    four_sad += r.screen_sad;
+                    int2 actual = pi4.pre;
+                    if (pi4.hybrid) {
+                        const int da = modular_mv_distance(P, r.mv, pi4.a), dcc = modular_mv_distance(P, r.mv, pi4.c);
+                        actual = (da <= dcc) ? pi4.a : pi4.c;
+                        ++extra_bits;
+                    }
+                    if (!(r.mv.x == actual.x && r.mv.y == actual.y)) extra_bits += mv_rate_bits(P, r.mv, actual, VC1CU_MV_MIXED, false);
+                }
+                const int cmx = median4(four[0].x, four[1].x, four[2].x, four[3].x);
+                const int cmy = median4(four[0].y, four[1].y, four[2].y, four[3].y);
+                const bool four_chroma_safe = !hidden_chroma(P, m.x0, m.y0, 16, 16, cmx, cmy);
+                bool choose4 = false;
+                if (four_chroma_safe)
+                    choose4 = four_sad + (uint64_t)llround(__dmul_rn(lambda, (double)extra_bits)) + 8 <
+                              (uint64_t)llround(__dmul_rn((double)one_sad, 0.985));
+                if (choose4) {
+                    for (int k = 0; k < 4; ++k) out4[k] = four[k];
+                    use4 = 1;
+                    out_mv = four[0];
+                    chosen = four_sad;
+                    temporal_screen = four_screen;
+                } else {
+                    temporal_screen = one_sad;
+                }
+            }
+            const uint64_t temporal = chosen;
+            double ratio = -1.0;
+            if (d.allow_intra && !P.disable_p_intra) {
+                // P-intra proxy (:384-415): lane = 8x8 block k*8 + row
+                uint32_t part = 0;
+                {
+                    const int k = m.lane >> 3, row = m.lane & 7;
+                    const int bx = (k & 1) * 8, by = ((k >> 1) & 1) * 8;
+                    const int vw = imax(0, imin(8, P.W - (m.x0 + bx))), vh = imax(0, imin(8, P.H - (m.y0 + by)));
+                    uint32_t rs = 0;
+                    if (row < vh)
+                        for (int x = 0; x < vw; ++x) rs += m.sm.cur[(by + row) * 16 + bx + x];
+                    // block sum over the 8 lanes of this block
+                    for (int o2 = 4; o2; o2 >>= 1) rs += __shfl_xor_sync(FULL, rs, o2);
+                    const uint32_t nn = (uint32_t)vw * (uint32_t)vh;
+                    const int mean = (!vw || !vh) ? 128 : (int)((rs + nn / 2) / nn);
+                    if (row < vh)
+                        for (int x = 0; x < vw; ++x) part += (uint32_t)iabs((int)m.sm.cur[(by + row) * 16 + bx + x] - mean);
+                }
+                const uint64_t intra_sad = warp_sum_u64(part);
+                const uint64_t intra_rate = (uint64_t)llround(__dmul_rn(lambda, 72.0));
+                ratio = temporal_screen > 0 ? __ddiv_rn((double)(intra_sad + intra_rate), (double)temporal_screen)
+                                            : __longlong_as_double(0x7ff0000000000000ll);
+                if (intra_sad + intra_rate < (uint64_t)llround(__dmul_rn((double)temporal_screen, P.inter_intra_threshold))) {
+                    intra = 1;
+                    use4 = 0;
+                    out_mv = make_int2(0, 0);
+                    for (int k = 0; k < 4; ++k) out4[k] = make_int2(0, 0);
+                    chosen = intra_sad;
+                }
+            }
+            bool moved = false, frac = false;
+            for (int k = 0; k < 4; ++k) {
+                moved |= out4[k].x != 0 || out4[k].y != 0;
+                frac |= (out4[k].x % 8) != 0 || (out4[k].y % 8) != 0;
+            }
+            if (m.lane == 0) {
+                o.mvs[m.pos] = out_mv;
+                for (int k = 0; k < 4; ++k) o.bmv[m.pos * 4 + k] = out4[k];
+                o.use4[m.pos] = use4;
+                o.intra[m.pos] = intra;
+                o.screen[m.pos] = temporal_screen;
+                o.ratio[m.pos] = ratio;
+                o.dl[m.pos] = dl;
+                o.dc[m.pos] = dc;
+                o.dd[m.pos] = dd;
+                o.chosen[m.pos] = chosen;
+                o.temporal[m.pos] = temporal;
+                o.flags[m.pos] = (uint8_t)((moved ? 1 : 0) | (frac ? 2 : 0));
+            }
+        }
+        __syncwarp();
+        if (m.lane == 0) {
+            __threadfence();
+            st_release(&o.done[m.pos], epoch);
+        }
+        __syncwarp();
+    }
+}
+
+// Picture totals of each pass (encoder_motion.cpp:428-441): integer sums, then the
+// reference's double expressions. One block per pass.
+__global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass) {
+    const PassDesc& d = passes[blockIdx.x];
+    const DevResult& o = d.out;
+    const int mbs = P.mbw * P.mbh;
+    uint64_t ts = 0, rs = 0, mv = 0, fr = 0, f4 = 0, in = 0, px = 0;
+    for (int i = threadIdx.x; i < mbs; i += blockDim.x) {
+        ts += o.chosen[i];
+        rs += o.temporal[i];
+        mv += o.flags[i] & 1;
+        fr += (o.flags[i] >> 1) & 1;
+        f4 += o.use4[i];
+        in += o.intra[i];
+        const int mx = i % P.mbw, my = i / P.mbw;
+        px += (uint64_t)imax(0, imin(16, P.W - mx * 16)) * (uint64_t)imax(0, imin(16, P.H - my * 16));
+    }
+    __shared__ unsigned long long red[7][32];
+    uint64_t v[7] = {ts, rs, mv, fr, f4, in, px};
+    for (int k = 0; k < 7; ++k) {
+        uint64_t x = warp_sum_u64(v[k]);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t s[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 7; ++k)
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s[k] += red[k][w];
+        const uint64_t total_pixels = s[6];
+        const double local_mad = total_pixels ? __ddiv_rn((double)s[0], (double)total_pixels) : 0.0;
+        double global_mad;
+        if (d.seeded) global_mad = local_mad;
+        else global_mad = (P.W > 0 && P.H > 0) ? __ddiv_rn((double)*o.gsad, (double)((uint64_t)P.W * P.H)) : 0.0;
+        const double rate_local = total_pixels ? __ddiv_rn((double)s[1], (double)total_pixels) : 0.0;
+        if (P.range == 0) {
+            o.totals[0] = local_mad;
+            o.totals[1] = local_mad;
+        } else {
+            o.totals[0] = local_mad < global_mad ? local_mad : global_mad;
+            o.totals[1] = rate_local < global_mad ? rate_local : global_mad;
+        }
+        o.itotals[0] = P.range == 0 ? 0 : s[0];
+        o.itotals[1] = s[2];
+        o.itotals[2] = s[3];
+        o.itotals[3] = s[4];
+        o.itotals[4] = s[5];
+    }
+}
+
+}  // namespace vc1cu

@@ -1,0 +1,76 @@
+// vc1cu_core.cuh - device-side descriptors shared by the core-pass, global-search and
+// transform kernels and the host shim.
+#pragma once
+
+#include <cstdint>
+
+#include "vc1cu_common.cuh"
+
+namespace vc1cu {
+
+// A frame slot in HBM: three planes with 16-byte-aligned row pitches.
+struct DevFrame {
+    const uint8_t* y;
+    const uint8_t* u;
+    const uint8_t* v;
+    int pitch_y, pitch_c;
+};
+
+// One result slot (Vc1Encoder::PAnalysis) in HBM, structure of arrays over macroblocks.
+struct DevResult {
+    int2* mvs;
+    int2* bmv;             // 4 per MB
+    uint8_t* use4;
+    uint8_t* intra;
+    uint64_t* screen;
+    double* ratio;
+    double* dl;
+    double* dc;
+    uint8_t* dd;
+    uint64_t* chosen;      // per-MB chosen SAD (motion_sad summand)
+    uint64_t* temporal;    // per-MB temporal SAD (rate_complexity summand)
+    uint8_t* flags;        // bit0 moved, bit1 fractional chroma, bit2 long-range propagated
+    uint32_t* done;        // wavefront flags (== epoch when the MB is final)
+    int* global;           // [dx, dy] of the unseeded pass
+    unsigned long long* gsad;
+    double* totals;        // mean_abs_residual, rate_complexity
+    unsigned long long* itotals;  // motion_sad, moved, frac, four, intra
+};
+
+struct PassDesc {
+    DevFrame cur, ref;
+    int mode, allow_intra;
+    int seeded;            // 1: seed fields below are valid
+    const int2* seed_mvs;
+    const double* seed_dl;
+    const double* seed_dc;
+    const uint8_t* seed_dd;
+    DevResult out;
+};
+
+// Shared-memory window geometry for one launch.
+struct WinCfg {
+    int rw;        // window radius in integer pixels around its centre MV
+    int ww;        // window side = 16 + 2*rw + 3
+    int seen_r;    // radius of the first-visit bitsets (0 = none)
+    int seen_words;
+    int keys_cap;  // capacity of the per-stage key array
+    int warp_bytes;
+};
+
+// Arguments of one candidate-scoring launch (vc1cu_score_motion_batch[_law]).
+struct ScoreArgs {
+    const uint8_t* cur;
+    const uint8_t* ref;
+    int pitch, W, H;
+    int x0, y0, bw, bh, stride, mode, rnd, metric, law;
+};
+
+struct LaunchStatus {
+    int error;          // 0 ok, VC1CU_ERR_TIMEOUT
+    int abort;
+    unsigned int queue;
+    unsigned int timeouts;
+};
+
+}  // namespace vc1cu

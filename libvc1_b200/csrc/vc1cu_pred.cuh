@@ -1,0 +1,118 @@
+// vc1cu_pred.cuh - VC-1 luma interpolation and block costs on the device.
+//
+// Samplers read a reference plane either from a per-warp shared-memory window (fast path)
+// or from HBM with clamped coordinates (edge emulation, Vc1Encoder::sample_clamped,
+// encoder_motion_compensation.cpp:350-353). Both return identical values wherever the
+// window is defined, because the window is filled with the same clamped samples.
+#pragma once
+
+#include "vc1cu_common.cuh"
+
+namespace vc1cu {
+
+struct WinSampler {
+    const uint8_t* win;
+    int ww, wx0, wy0;
+    __device__ __forceinline__ int operator()(int x, int y) const { return win[(y - wy0) * ww + (x - wx0)]; }
+};
+
+struct GlobSampler {
+    const uint8_t* p;
+    int pitch, W, H;
+    __device__ __forceinline__ int operator()(int x, int y) const {
+        x = iclamp(x, 0, W - 1);
+        y = iclamp(y, 0, H - 1);
+        return __ldg(p + (size_t)y * pitch + x);
+    }
+};
+
+// N consecutive luma predictions of row py starting at px for quarter-pel MV (xq,yq):
+// luma_mc_sample (VC-1 bicubic, encoder_motion_compensation.cpp:367-396) or, for the
+// bilinear half-pel mode, luma_mc_sample_mode (:398-415).
+template <int N, class S>
+__device__ __forceinline__ void predict_row(const S& s, bool bilinear, int rnd, int xq, int yq, int px, int py,
+                                            int out[N]) {
+    const int ix = floor_div4(xq), iy = floor_div4(yq);
+    const int hm = xq - ix * 4, vm = yq - iy * 4;
+    const int sx = px + ix, sy = py + iy;
+    if (bilinear) {
+        if (!hm && !vm) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) out[i] = s(sx + i, sy);
+        } else if (hm && vm) {
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+                out[i] = (s(sx + i, sy) + s(sx + i + 1, sy) + s(sx + i, sy + 1) + s(sx + i + 1, sy + 1) + (rnd ? 1 : 2)) >> 2;
+        } else if (hm) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) out[i] = (s(sx + i, sy) + s(sx + i + 1, sy) + (rnd ? 0 : 1)) >> 1;
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; ++i) out[i] = (s(sx + i, sy) + s(sx + i, sy + 1) + (rnd ? 0 : 1)) >> 1;
+        }
+        return;
+    }
+    if (!hm && !vm) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) out[i] = s(sx + i, sy);
+        return;
+    }
+    if (hm && vm) {
+        const int shift_value[4] = {0, 5, 1, 5};
+        const int shift = (shift_value[hm] + shift_value[vm]) >> 1;
+        const int r1 = (1 << (shift - 1)) + (rnd ? 1 : 0) - 1;
+        int t[N + 3];
+#pragma unroll
+        for (int k = -1; k <= N + 1; ++k) {
+            const int raw = mspel(s(sx + k, sy - 1), s(sx + k, sy), s(sx + k, sy + 1), s(sx + k, sy + 2), vm);
+            t[k + 1] = arshift(raw + r1, shift);
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const int raw = mspel(t[i], t[i + 1], t[i + 2], t[i + 3], hm);
+            out[i] = iclamp(arshift(raw + 64 - (rnd ? 1 : 0), 7), 0, 255);
+        }
+        return;
+    }
+    if (vm) {
+        const int bias = (vm == 2) ? (7 + (rnd ? 1 : 0)) : (31 + (rnd ? 1 : 0));
+        const int sh = vm == 2 ? 4 : 6;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const int raw = mspel(s(sx + i, sy - 1), s(sx + i, sy), s(sx + i, sy + 1), s(sx + i, sy + 2), vm);
+            out[i] = iclamp(arshift(raw + bias, sh), 0, 255);
+        }
+        return;
+    }
+    const int bias = (hm == 2) ? (8 - (rnd ? 1 : 0)) : (32 - (rnd ? 1 : 0));
+    const int sh = hm == 2 ? 4 : 6;
+    int r[N + 3];
+#pragma unroll
+    for (int k = -1; k <= N + 1; ++k) r[k + 1] = s(sx + k, sy);
+#pragma unroll
+    for (int i = 0; i < N; ++i) out[i] = iclamp(arshift(mspel(r[i], r[i + 1], r[i + 2], r[i + 3], hm) + bias, sh), 0, 255);
+}
+
+// 4x4 Hadamard SATD of a residual tile, satd4x4_scalar (encoder_motion.cpp:2936-2958).
+__device__ __forceinline__ uint32_t satd4x4(const int d[16]) {
+    int t[16];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+        const int a0 = d[y * 4 + 0] + d[y * 4 + 3], a1 = d[y * 4 + 1] + d[y * 4 + 2];
+        const int a2 = d[y * 4 + 1] - d[y * 4 + 2], a3 = d[y * 4 + 0] - d[y * 4 + 3];
+        t[y * 4 + 0] = a0 + a1;
+        t[y * 4 + 1] = a3 + a2;
+        t[y * 4 + 2] = a0 - a1;
+        t[y * 4 + 3] = a3 - a2;
+    }
+    uint32_t tile = 0;
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+        const int a0 = t[0 * 4 + x] + t[3 * 4 + x], a1 = t[1 * 4 + x] + t[2 * 4 + x];
+        const int a2 = t[1 * 4 + x] - t[2 * 4 + x], a3 = t[0 * 4 + x] - t[3 * 4 + x];
+        tile += (uint32_t)iabs(a0 + a1) + (uint32_t)iabs(a3 + a2) + (uint32_t)iabs(a0 - a1) + (uint32_t)iabs(a3 - a2);
+    }
+    return (tile + 1) >> 1;
+}
+
+}  // namespace vc1cu

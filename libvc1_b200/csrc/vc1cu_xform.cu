@@ -1,0 +1,198 @@
+// vc1cu_xform.cu - decoder-equivalent prediction of a motion field and the forward
+// 8x8/8x4/4x8/4x4 transform + scalar quantiser of its residual.
+//
+// Prediction follows motion_compensate_mb / motion_compensate_4mv
+// (encoder_motion_compensation.cpp:474-600). The transform is the reference's FP64 law
+// (forward_transform_residual[_part], encoder_transform.cpp:797-1045): residual rows
+// multiplied by the k8/k4 matrices in the reference's loop order, every product and sum
+// rounded separately (this translation unit is compiled with --fmad=false and spells the
+// operations with __dmul_rn/__dadd_rn), then scalar_quantize_level (:1067-1085).
+#include <cuda_runtime.h>
+
+#include "vc1cu_core.cuh"
+#include "vc1cu_pred.cuh"
+
+namespace vc1cu {
+
+// forward_transform::k4 / k8, forward_transform_tables.h:9-25 (inverse VC-1 basis)
+__constant__ double c_k4[4][4] = {
+    {0.0147058823529412, 0.0147058823529412, 0.0147058823529412, 0.0147058823529412},
+    {0.0188356164383562, 0.0085616438356164, -0.0085616438356164, -0.0188356164383562},
+    {0.0147058823529412, -0.0147058823529412, -0.0147058823529412, 0.0147058823529412},
+    {0.0085616438356164, -0.0188356164383562, 0.0188356164383562, -0.0085616438356164}};
+__constant__ double c_k8[8][8] = {
+    {0.010416666667, 0.010416666667, 0.010416666667, 0.010416666667, 0.010416666667, 0.010416666667, 0.010416666667, 0.010416666667},
+    {0.013840830450, 0.012975778547, 0.007785467128, 0.003460207612, -0.003460207612, -0.007785467128, -0.012975778547, -0.013840830450},
+    {0.013698630137, 0.005136986301, -0.005136986301, -0.013698630137, -0.013698630137, -0.005136986301, 0.005136986301, 0.013698630137},
+    {0.012975778547, -0.003460207612, -0.013840830450, -0.007785467128, 0.007785467128, 0.013840830450, 0.003460207612, -0.012975778547},
+    {0.010416666667, -0.010416666667, -0.010416666667, 0.010416666667, 0.010416666667, -0.010416666667, -0.010416666667, 0.010416666667},
+    {0.007785467128, -0.013840830450, 0.003460207612, 0.012975778547, -0.012975778547, -0.003460207612, 0.013840830450, -0.007785467128},
+    {0.005136986301, -0.013698630137, 0.013698630137, -0.005136986301, -0.005136986301, 0.013698630137, -0.013698630137, 0.005136986301},
+    {0.003460207612, -0.007785467128, 0.012975778547, -0.013840830450, 0.013840830450, -0.012975778547, 0.007785467128, -0.003460207612}};
+
+// Vc1Encoder::chroma_mc_sample, encoder_motion_compensation.cpp:417-447 (P: future = false)
+__device__ __forceinline__ int chroma_sample(const uint8_t* p, int pitch, int w, int h, int x, int y, int mvx, int mvy,
+                                             int rnd) {
+    int uvx = arshift(mvx + ((mvx & 3) == 3), 1);
+    int uvy = arshift(mvy + ((mvy & 3) == 3), 1);
+    if (uvx < 0) uvx += (uvx & 1); else uvx -= (uvx & 1);
+    if (uvy < 0) uvy += (uvy & 1); else uvy -= (uvy & 1);
+    const int ix = floor_div4(uvx), iy = floor_div4(uvy);
+    const int fx = (uvx - ix * 4) * 2, fy = (uvy - iy * 4) * 2;
+    const int sx = x + ix, sy = y + iy;
+    auto S = [&](int xx, int yy) { return (int)__ldg(p + (size_t)iclamp(yy, 0, h - 1) * pitch + iclamp(xx, 0, w - 1)); };
+    const int a = S(sx, sy);
+    if (!fx && !fy) return a;
+    const int b = S(sx + 1, sy), c = S(sx, sy + 1), d = S(sx + 1, sy + 1);
+    const int value = a * (8 - fx) * (8 - fy) + b * fx * (8 - fy) + c * (8 - fx) * fy + d * fx * fy;
+    return (value + (rnd ? 28 : 32)) >> 6;
+}
+
+__device__ __forceinline__ int median4(int a, int b, int c, int d) {
+    if (a < b) {
+        if (c < d) return (imin(b, d) + imax(a, c)) / 2;
+        return (imin(b, c) + imax(a, d)) / 2;
+    }
+    if (c < d) return (imin(a, d) + imax(b, c)) / 2;
+    return (imin(a, c) + imax(b, d)) / 2;
+}
+
+// One thread per luma pixel (and, for even pixels, the co-sited chroma pair).
+__global__ void mc_kernel(const __grid_constant__ DevParams P, DevFrame ref, const int2* mvs, const int2* bmv,
+                          const uint8_t* use4, int mode, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= P.W || y >= P.H) return;
+    const int mx = x >> 4, my = y >> 4, pos = my * P.mbw + mx;
+    const GlobSampler gs{ref.y, ref.pitch_y, P.W, P.H};
+    int out[1];
+    int2 cmv;
+    if (use4[pos]) {
+        const int k = ((y >> 3) & 1) * 2 + ((x >> 3) & 1);
+        const int2 v = bmv[pos * 4 + k];
+        predict_row<1>(gs, false, P.rnd, v.x, v.y, x, y, out);
+        const int2 a = bmv[pos * 4 + 0], b = bmv[pos * 4 + 1], c = bmv[pos * 4 + 2], d = bmv[pos * 4 + 3];
+        cmv = make_int2(median4(a.x, b.x, c.x, d.x), median4(a.y, b.y, c.y, d.y));
+    } else {
+        const int2 v = mvs[pos];
+        predict_row<1>(gs, mode_bilinear(mode), P.rnd, v.x, v.y, x, y, out);
+        cmv = v;
+    }
+    dy[(size_t)y * pitch_y + x] = (uint8_t)out[0];
+    if (!(x & 1) && !(y & 1)) {
+        const int cw = P.W / 2, ch = P.H / 2, cx = x >> 1, cy = y >> 1;
+        if (cx < cw && cy < ch) {
+            du[(size_t)cy * pitch_c + cx] = (uint8_t)chroma_sample(ref.u, ref.pitch_c, cw, ch, cx, cy, cmv.x, cmv.y, P.rnd);
+            dv[(size_t)cy * pitch_c + cx] = (uint8_t)chroma_sample(ref.v, ref.pitch_c, cw, ch, cx, cy, cmv.x, cmv.y, P.rnd);
+        }
+    }
+}
+
+// Vc1Encoder::scalar_quantize_level, encoder_transform.cpp:1067-1085 (mquant = PQINDEX)
+__device__ __forceinline__ int quantize_level(const DevParams& P, double coeff) {
+    if (coeff == 0.0) return 0;
+    const int sign = coeff < 0.0 ? -1 : 1;
+    const double a = fabs(coeff);
+    const double dq = (double)(2 * P.pq + (P.halfqp ? 1 : 0));
+    const double offset = P.nonuniform ? (double)P.pq : 0.0;
+    const int max_level = (1 << (P.pq < 8 ? 11 : 8)) - 1;
+    int center = (int)llround(__ddiv_rn(__dsub_rn(a, offset), dq > 1.0 ? dq : 1.0));
+    center = iclamp(center, 1, max_level);
+    int best = 0;
+    double besterr = __dmul_rn(a, a);
+    for (int n = imax(1, center - 1); n <= imin(max_level, center + 1); ++n) {
+        const double recon = __dadd_rn(__dmul_rn((double)n, dq), offset);
+        const double e = __dsub_rn(a, recon);
+        const double e2 = __dmul_rn(e, e);
+        if (e2 < besterr) { besterr = e2; best = n; }
+    }
+    return sign * best;
+}
+
+// One thread per (type, MB, parent, partition). Output layout [type][mb][parent][64].
+__global__ void xform_kernel(const __grid_constant__ DevParams P, DevFrame src, DevFrame pred, int type_mask, double* coeffs,
+                             int16_t* levels) {
+    const int mbs = P.mbw * P.mbh;
+    // partitions per parent for each of the up-to-4 types, in type order
+    int types[4], nt = 0;
+    for (int t = 1; t <= 4; ++t)
+        if (type_mask & (1 << (t - 1))) types[nt++] = t;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long per_type = (long)mbs * 6 * 4;  // up to 4 partitions
+    if (idx >= per_type * nt) return;
+    const int ti = (int)(idx / per_type);
+    const long rem = idx % per_type;
+    const int part = (int)(rem & 3);
+    const int k = (int)((rem >> 2) % 6);
+    const int mb = (int)((rem >> 2) / 6);
+    const int t = types[ti];
+    const int np = t == 1 ? 1 : (t == 4 ? 4 : 2);
+    if (part >= np) return;
+    int ox = 0, oy = 0, bw = 8, bh = 8;
+    if (t == 2) { bh = 4; oy = part * 4; }
+    else if (t == 3) { bw = 4; ox = part * 4; }
+    else if (t == 4) { bw = 4; bh = 4; ox = (part & 1) * 4; oy = (part >> 1) * 4; }
+    const int mx = mb % P.mbw, my = mb / P.mbw;
+    const bool chroma = k >= 4;
+    const uint8_t* sp = chroma ? (k == 4 ? src.u : src.v) : src.y;
+    const uint8_t* pp = chroma ? (k == 4 ? pred.u : pred.v) : pred.y;
+    const int spitch = chroma ? src.pitch_c : src.pitch_y, ppitch = chroma ? pred.pitch_c : pred.pitch_y;
+    const int w = chroma ? P.W / 2 : P.W, h = chroma ? P.H / 2 : P.H;
+    const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
+    const int x0 = bx * 8 + ox, y0 = by * 8 + oy;
+    const size_t base = (((size_t)ti * mbs + mb) * 6 + k) * 64;
+    if (x0 >= w || y0 >= h || x0 + bw <= 0 || y0 + bh <= 0) {
+        // a partition wholly outside the crop codes nothing (encoder_transform.cpp:1097)
+        for (int y = 0; y < bh; ++y)
+            for (int x = 0; x < bw; ++x) {
+                if (coeffs) coeffs[base + (oy + y) * 8 + ox + x] = 0.0;
+                if (levels) levels[base + (oy + y) * 8 + ox + x] = 0;
+            }
+        return;
+    }
+    double r[8][8];
+    for (int y = 0; y < bh; ++y)
+        for (int x = 0; x < bw; ++x) {
+            const int sx = x0 + x, sy = y0 + y;
+            r[y][x] = (sx < 0 || sy < 0 || sx >= w || sy >= h)
+                          ? 0.0
+                          : (double)((int)__ldg(sp + (size_t)sy * spitch + sx) - (int)__ldg(pp + (size_t)sy * ppitch + sx));
+        }
+    double tmp[8][8];
+    for (int a = 0; a < bh; ++a)
+        for (int x = 0; x < bw; ++x) {
+            double acc = 0.0;
+            for (int y = 0; y < bh; ++y) acc = __dadd_rn(acc, __dmul_rn(bh == 8 ? c_k8[a][y] : c_k4[a][y], r[y][x]));
+            tmp[a][x] = acc;
+        }
+    for (int a = 0; a < bh; ++a)
+        for (int b = 0; b < bw; ++b) {
+            double acc = 0.0;
+            for (int x = 0; x < bw; ++x) acc = __dadd_rn(acc, __dmul_rn(tmp[a][x], bw == 8 ? c_k8[b][x] : c_k4[b][x]));
+            // 8x8 output is transposed (c[row*8+col] = 1024*xform[col][row]), rectangles are not
+            const double c = __dmul_rn(1024.0, acc);
+            int row, col;
+            if (bw == 8 && bh == 8) { row = b; col = a; }
+            else { row = a; col = b; }
+            const size_t o = base + (size_t)(oy + row) * 8 + ox + col;
+            if (coeffs) coeffs[o] = c;
+            if (levels) levels[o] = (int16_t)quantize_level(P, c);
+        }
+}
+
+void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
+               uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
+    dim3 grid((P.W + 127) / 128, P.H);
+    mc_kernel<<<grid, 128, 0, s>>>(P, ref, mvs, bmv, use4, mode, dy, du, dv, pitch_y, pitch_c);
+}
+
+void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred, int type_mask, double* coeffs,
+                  int16_t* levels, cudaStream_t s) {
+    int nt = 0;
+    for (int t = 0; t < 4; ++t) nt += (type_mask >> t) & 1;
+    const long n = (long)P.mbw * P.mbh * 6 * 4 * nt;
+    if (!n) return;
+    xform_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, src, pred, type_mask, coeffs, levels);
+}
+
+}  // namespace vc1cu
