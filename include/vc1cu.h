@@ -138,7 +138,20 @@ typedef struct vc1cu_counters {
     uint64_t frame_upload_bytes;
     uint64_t submit_wait_nanoseconds;
     uint64_t macroblocks_analysed;
+    uint64_t kernel_launches;   /* every kernel this library launched */
 } vc1cu_counters;
+
+/* Device time of each kernel family, summed over launches since the last reset, from CUDA
+ * events recorded on the context's stream around every launch (vc1cu_set_timing(ctx, 1)). */
+typedef struct vc1cu_timing {
+    double core_ms;      /* core_pass_kernel */
+    double global_ms;    /* global translation search (scoring + fold launches) */
+    double totals_ms;    /* per-pass totals */
+    double mc_ms;        /* motion compensation */
+    double xform_ms;     /* forward transform + quantiser */
+    uint64_t core_launches;
+    uint64_t xform_launches;
+} vc1cu_timing;
 
 /* ---- context (VulkanComputeContext::create / device_name / device_index) ---------- */
 
@@ -154,6 +167,16 @@ const char* vc1cu_last_error(const vc1cu_ctx* ctx);
 /* VulkanComputeContext::counters / reset_counters (src/vulkan_compute.h:53-54). */
 int vc1cu_counters_get(const vc1cu_ctx* ctx, vc1cu_counters* out);
 int vc1cu_reset_counters(vc1cu_ctx* ctx);
+
+/* Turns per-launch event timing on (1) or off (0); vc1cu_timing_get synchronises the
+ * context stream and returns the sums; vc1cu_reset_counters clears them. */
+int vc1cu_set_timing(vc1cu_ctx* ctx, int enable);
+int vc1cu_timing_get(vc1cu_ctx* ctx, vc1cu_timing* out);
+/* The CUDA stream (cudaStream_t) every launch of this context is ordered on. */
+void* vc1cu_stream(const vc1cu_ctx* ctx);
+/* Measures this device's 32-bit integer lane-op throughput (ops/s) with a dependency-free
+ * add/xor kernel: the denominator of the analysis kernels' roofline. */
+int vc1cu_measure_int32_peak(vc1cu_ctx* ctx, double* ops_per_second);
 
 /* Fills the defaults of vc1_param_default for a width x height raster. */
 void vc1cu_params_default(vc1cu_params* p, int width, int height);
@@ -221,6 +244,7 @@ typedef struct vc1cu_pass {
     int32_t allow_intra;
     int32_t seed_slot;   /* -1 = unseeded */
     int32_t out_slot;
+    int32_t pqindex;     /* 0 = params->pqindex; else this picture's PQINDEX (1..31) */
 } vc1cu_pass;
 
 int vc1cu_core_passes(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_pass* passes, int n);

@@ -56,7 +56,13 @@ class PAnalysisC(C.Structure):
 class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("dispatches", "candidates", "frame_uploads",
                                           "frame_upload_bytes", "submit_wait_nanoseconds",
-                                          "macroblocks_analysed")]
+                                          "macroblocks_analysed", "kernel_launches")]
+
+
+class Timing(C.Structure):
+    _fields_ = [("core_ms", C.c_double), ("global_ms", C.c_double), ("totals_ms", C.c_double),
+                ("mc_ms", C.c_double), ("xform_ms", C.c_double), ("core_launches", C.c_uint64),
+                ("xform_launches", C.c_uint64)]
 
 
 def make_params(width: int, height: int, **kw) -> Params:

@@ -19,7 +19,7 @@ import os
 
 import numpy as np
 
-from .abi import (Analysis, Counters, ERRORS, MV_QPEL, METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params,
+from .abi import (Analysis, Counters, ERRORS, Timing, MV_QPEL, METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params,
                   mbs_of)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -32,13 +32,14 @@ EXPORTS = (
     "vc1cu_counters_get", "vc1cu_reset_counters", "vc1cu_params_default", "vc1cu_score_motion_batch",
     "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
-    "vc1cu_forward_quant", "vc1cu_forward_quant_device",
+    "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
+    "vc1cu_measure_int32_peak",
 )
 
 
 class Pass(C.Structure):
     _fields_ = [("cur_id", C.c_int32), ("ref_id", C.c_int32), ("mode", C.c_int32), ("allow_intra", C.c_int32),
-                ("seed_slot", C.c_int32), ("out_slot", C.c_int32)]
+                ("seed_slot", C.c_int32), ("out_slot", C.c_int32), ("pqindex", C.c_int32)]
 
 
 def load_library(path: str = LIB_PATH):
@@ -73,6 +74,11 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_motion_compensate.argtypes = [vp, PP, i32, i32, i32, i32]
     L.vc1cu_forward_quant.argtypes = [vp, PP, i32, i32, i32, vp, vp]
     L.vc1cu_forward_quant_device.argtypes = [vp, PP, i32, i32, i32, vp, vp]
+    L.vc1cu_set_timing.argtypes = [vp, i32]
+    L.vc1cu_timing_get.argtypes = [vp, C.POINTER(Timing)]
+    L.vc1cu_stream.argtypes = [vp]
+    L.vc1cu_stream.restype = vp
+    L.vc1cu_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
     _LIB = L
@@ -165,6 +171,24 @@ class CudaComputeContext:
     def reset_counters(self):
         self._check(self._L.vc1cu_reset_counters(self._h))
 
+    def set_timing(self, enable: bool):
+        self._check(self._L.vc1cu_set_timing(self._h, int(enable)))
+
+    def timing(self) -> dict:
+        t = Timing()
+        self._check(self._L.vc1cu_timing_get(self._h, C.byref(t)))
+        return {f[0]: getattr(t, f[0]) for f in Timing._fields_}
+
+    def measure_int32_peak(self) -> float:
+        """32-bit integer lane-ops per second of this device (calibration kernel)."""
+        v = C.c_double()
+        self._check(self._L.vc1cu_measure_int32_peak(self._h, C.byref(v)))
+        return v.value
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (every launch is ordered on it)."""
+        return self._L.vc1cu_stream(self._h) or 0
+
     # --- the analysis path -------------------------------------------------------------
     def upload_frame(self, frame_id: int, y, u=None, v=None):
         """Copies one 4:2:0 frame into frame slot `frame_id`. With pinned host arrays the copy
@@ -204,7 +228,7 @@ class CudaComputeContext:
         return out.take_totals(oc)
 
     def core_passes(self, params: Params, passes):
-        """passes: iterable of (cur_id, ref_id, mode, allow_intra, seed_slot, out_slot)."""
+        """passes: iterable of (cur_id, ref_id, mode, allow_intra, seed_slot, out_slot[, pqindex])."""
         arr = (Pass * len(passes))(*[Pass(*p) for p in passes])
         self._check(self._L.vc1cu_core_passes(self._h, C.byref(params), arr, len(passes)))
 

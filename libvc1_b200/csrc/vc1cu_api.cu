@@ -28,7 +28,7 @@ __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDes
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
 size_t gstate_bytes();
-void run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream);
+int run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream);
 void init_gstate(GState* h, const DevFrame& cur, const DevFrame& ref, int range, int* out_global,
                  unsigned long long* out_sad);
 void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
@@ -37,6 +37,7 @@ void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred,
                   int16_t* levels, cudaStream_t s);
 void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int n, unsigned long long* out,
                   cudaStream_t s);
+double measure_int32_peak(cudaStream_t s, int sms);
 }  // namespace vc1cu
 
 using namespace vc1cu;
@@ -134,9 +135,16 @@ struct vc1cu_ctx {
     size_t scratch_cap = 0;
     void* h_pinned = nullptr;
     size_t pinned_cap = 0;
+    cudaEvent_t staging_done = nullptr;  // last H2D copy out of h_pinned
     uint32_t epoch = 0;
     int sm_count = 0;
     int max_smem = 0;
+    // per-launch event timing
+    bool timing = false;
+    struct Timed { cudaEvent_t a, b; int family; };
+    std::vector<Timed> pending;
+    std::vector<cudaEvent_t> event_pool;
+    vc1cu_timing tsum{};
 };
 
 namespace {
@@ -230,6 +238,16 @@ int make_dev_params(const vc1cu_params* p, DevParams& P, std::string& why) {
     P.distant_match_max_mae = p->distant_match_max_mae;
     P.inter_intra_threshold = p->inter_intra_threshold;
     return VC1CU_OK;
+}
+
+// lambda_me = max(1, 0.35*PQ) (encoder_motion.cpp:3459), split as lam_m * 2^-lam_s exactly
+void set_lambda(PassDesc& d, int pq) {
+    d.pq = pq;
+    d.lambda = std::max(1.0, 0.35 * static_cast<double>(pq));
+    int e = 0;
+    const double fr = std::frexp(d.lambda, &e);
+    d.lam_m = static_cast<uint64_t>(std::ldexp(fr, 53));
+    d.lam_s = 53 - e;
 }
 
 int stage_max(int R) {
@@ -340,6 +358,75 @@ void sync_checked(vc1cu_ctx* c) {
     ck(cudaGetLastError(), "kernel");
 }
 
+enum Family { kCore = 0, kGlobal = 1, kTotals = 2, kMc = 3, kXform = 4, kScore = 5 };
+
+cudaEvent_t take_event(vc1cu_ctx* c) {
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    ck(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+// Brackets the launches of one kernel family with CUDA events on the context stream
+// when timing is on, and counts the launches.
+struct Timer {
+    vc1cu_ctx* c;
+    int family;
+    cudaEvent_t a = nullptr;
+    Timer(vc1cu_ctx* cc, int f) : c(cc), family(f) {
+        if (c->timing) {
+            a = take_event(c);
+            ck(cudaEventRecord(a, c->stream), "cudaEventRecord");
+        }
+    }
+    void stop(int launches) {
+        c->counters.kernel_launches += (uint64_t)launches;
+        if (!a) return;
+        cudaEvent_t b = take_event(c);
+        ck(cudaEventRecord(b, c->stream), "cudaEventRecord");
+        c->pending.push_back({a, b, family});
+        a = nullptr;
+    }
+};
+
+void collect_timing(vc1cu_ctx* c) {
+    if (c->pending.empty()) return;
+    ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    for (auto& t : c->pending) {
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, t.a, t.b), "cudaEventElapsedTime");
+        switch (t.family) {
+            case kCore: c->tsum.core_ms += ms; c->tsum.core_launches++; break;
+            case kGlobal: c->tsum.global_ms += ms; break;
+            case kTotals: c->tsum.totals_ms += ms; break;
+            case kMc: c->tsum.mc_ms += ms; break;
+            case kXform: c->tsum.xform_ms += ms; c->tsum.xform_launches++; break;
+            default: break;
+        }
+        c->event_pool.push_back(t.a);
+        c->event_pool.push_back(t.b);
+    }
+    c->pending.clear();
+}
+
+// Pinned staging for host->device launch descriptors; waits until its previous copy is done.
+void* staging(vc1cu_ctx* c, size_t bytes) {
+    if (c->staging_done) ck(cudaEventSynchronize(c->staging_done), "cudaEventSynchronize");
+    if (c->pinned_cap < bytes) {
+        if (c->h_pinned) cudaFreeHost(c->h_pinned);
+        c->h_pinned = nullptr;
+        c->pinned_cap = 0;
+        ck(cudaMallocHost(&c->h_pinned, bytes), "cudaMallocHost(staging)");
+        c->pinned_cap = bytes;
+    }
+    if (!c->staging_done) ck(cudaEventCreateWithFlags(&c->staging_done, cudaEventDisableTiming), "cudaEventCreate");
+    return c->h_pinned;
+}
+
 int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1cu_mv* cands, size_t n, uint64_t* costs) {
     const size_t cb = n * sizeof(int2), ob = n * sizeof(unsigned long long);
     ensure(c->d_scratch, c->scratch_cap, cb + ob + 256, "cudaMalloc(candidates)");
@@ -347,8 +434,10 @@ int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1
     unsigned long long* dout = reinterpret_cast<unsigned long long*>(static_cast<uint8_t*>(c->d_scratch) + ((cb + 255) & ~size_t(255)));
     const auto t0 = std::chrono::steady_clock::now();
     ck(cudaMemcpyAsync(dc, cands, cb, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(candidates)");
+    Timer tm(c, kScore);
     launch_score(P, a, dc, (int)n, dout, c->stream);
     ck(cudaGetLastError(), "score_kernel launch");
+    tm.stop(1);
     ck(cudaMemcpyAsync(costs, dout, ob, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(costs)");
     sync_checked(c);
     const auto t1 = std::chrono::steady_clock::now();
@@ -383,6 +472,8 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         d.ref = fr.view();
         d.mode = q.mode;
         d.allow_intra = q.allow_intra != 0;
+        if (q.pqindex < 0 || q.pqindex > 31) throw Fail{VC1CU_ERR_ARG, "pass pqindex must be 0 (params) or 1..31"};
+        set_lambda(d, q.pqindex ? q.pqindex : P.pq);
         d.seeded = q.seed_slot >= 0;
         if (d.seeded) {
             ResultSlot& s = result_slot(c, q.seed_slot, mbs, false);
@@ -409,7 +500,12 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j)
             if (passes[i].seed_slot == passes[j].out_slot) throw Fail{VC1CU_ERR_ARG, "a pass seeds from a pass of the same batch"};
-    // global translation search of the unseeded passes
+    // global translation search of the unseeded passes (none at --search-range 0)
+    if (!unseeded.empty() && P.range == 0)
+        for (int k : unseeded) {
+            ck(cudaMemsetAsync(h[k].out.global, 0, 8, c->stream), "cudaMemsetAsync(global)");
+            ck(cudaMemsetAsync(h[k].out.gsad, 0, 8, c->stream), "cudaMemsetAsync(global)");
+        }
     if (!unseeded.empty() && P.range > 0) {
         const int nu = (int)unseeded.size();
         const size_t gb = gstate_bytes();
@@ -422,17 +518,18 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
             c->d_gstates = static_cast<GState*>(d);
             c->gstates_cap = nu;
         }
-        std::vector<uint8_t> hs(gb * nu);
+        uint8_t* hs = static_cast<uint8_t*>(staging(c, gb * nu));
         const int grange = std::min(P.local_range, 32);
         for (int k = 0; k < nu; ++k) {
             const PassDesc& d = h[unseeded[k]];
-            init_gstate(reinterpret_cast<GState*>(hs.data() + gb * k), d.cur, d.ref, grange, d.out.global, d.out.gsad);
+            init_gstate(reinterpret_cast<GState*>(hs + gb * k), d.cur, d.ref, grange, d.out.global, d.out.gsad);
         }
-        ck(cudaMemcpyAsync(c->d_gstates, hs.data(), gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
-        run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
+        ck(cudaMemcpyAsync(c->d_gstates, hs, gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
+        ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+        Timer tm(c, kGlobal);
+        const int launches = run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
         ck(cudaGetLastError(), "global search launch");
-        // the host staging buffer must outlive the copy
-        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        tm.stop(launches);
     }
     // pass descriptors
     if (c->passes_cap < n) {
@@ -444,10 +541,14 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         c->d_passes = static_cast<PassDesc*>(d);
         c->passes_cap = n;
     }
-    // ordered on the context stream after any launch still reading the previous descriptors;
-    // a pageable source is staged before the call returns
-    ck(cudaMemcpyAsync(c->d_passes, h.data(), sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
-       "cudaMemcpyAsync(pass descriptors)");
+    // ordered on the context stream after any launch still reading the previous descriptors
+    {
+        void* hp = staging(c, sizeof(PassDesc) * n);
+        std::memcpy(hp, h.data(), sizeof(PassDesc) * n);
+        ck(cudaMemcpyAsync(c->d_passes, hp, sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
+           "cudaMemcpyAsync(pass descriptors)");
+        ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    }
     // window / bitset geometry
     WinCfg wc;
     if (any_unseeded) {
@@ -478,10 +579,18 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     const int grid = (int)std::max(1L, std::min<long>((long)per_sm * c->sm_count, need));
     if (++c->epoch == 0) c->epoch = 1;
     ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
-    core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, wc, c->epoch, c->d_status);
-    ck(cudaGetLastError(), "core_pass_kernel launch");
-    totals_kernel<<<n, 256, 0, c->stream>>>(P, c->d_passes, n);
-    ck(cudaGetLastError(), "totals_kernel launch");
+    {
+        Timer tm(c, kCore);
+        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, wc, c->epoch, c->d_status);
+        ck(cudaGetLastError(), "core_pass_kernel launch");
+        tm.stop(1);
+    }
+    {
+        Timer tm(c, kTotals);
+        totals_kernel<<<n, 256, 0, c->stream>>>(P, c->d_passes, n);
+        ck(cudaGetLastError(), "totals_kernel launch");
+        tm.stop(1);
+    }
     c->counters.dispatches++;
     c->counters.macroblocks_analysed += (uint64_t)items;
     return VC1CU_OK;
@@ -603,6 +712,13 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_passes) cudaFree(c->d_passes);
     if (c->d_gstates) cudaFree(c->d_gstates);
     if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->staging_done) cudaEventDestroy(c->staging_done);
+    for (auto& t : c->pending) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : c->event_pool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return VC1CU_OK;
@@ -619,10 +735,41 @@ int vc1cu_counters_get(const vc1cu_ctx* c, vc1cu_counters* out) {
 }
 
 int vc1cu_reset_counters(vc1cu_ctx* c) {
-    if (!c) return VC1CU_ERR_ARG;
-    std::lock_guard<std::mutex> lock(c->mu);
-    c->counters = vc1cu_counters{};
-    return VC1CU_OK;
+    return guarded(c, [&]() -> int {
+        collect_timing(c);
+        c->counters = vc1cu_counters{};
+        c->tsum = vc1cu_timing{};
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_set_timing(vc1cu_ctx* c, int enable) {
+    return guarded(c, [&]() -> int {
+        collect_timing(c);
+        c->timing = enable != 0;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_timing_get(vc1cu_ctx* c, vc1cu_timing* out) {
+    return guarded(c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        collect_timing(c);
+        *out = c->tsum;
+        return VC1CU_OK;
+    });
+}
+
+void* vc1cu_stream(const vc1cu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int vc1cu_measure_int32_peak(vc1cu_ctx* c, double* ops_per_second) {
+    return guarded(c, [&]() -> int {
+        if (!ops_per_second) throw Fail{VC1CU_ERR_ARG, "null output"};
+        *ops_per_second = measure_int32_peak(c->stream, c->sm_count);
+        ck(cudaGetLastError(), "int32_peak_kernel");
+        if (*ops_per_second <= 0.0) throw Fail{VC1CU_ERR_CUDA, "calibration kernel failed"};
+        return VC1CU_OK;
+    });
 }
 
 int vc1cu_score_motion_batch(vc1cu_ctx* c, const uint8_t* cur, const uint8_t* ref, int width, int height, int x0, int y0,
@@ -736,7 +883,7 @@ int vc1cu_analyze_p_core(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int re
         const int rc = make_dev_params(p, P, why);
         if (rc) throw Fail{rc, why};
         const int mbs = P.mbw * P.mbh;
-        vc1cu_pass q{cur_id, ref_id, mode, allow_intra, -1, kInternalOut};
+        vc1cu_pass q{cur_id, ref_id, mode, allow_intra, -1, kInternalOut, 0};
         if (seed_mvs) {
             ResultSlot& s = result_slot(c, kInternalSeed, mbs, true);
             ck(cudaMemcpyAsync(s.r.mvs, seed_mvs, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload seed");
@@ -776,9 +923,11 @@ int vc1cu_motion_compensate(vc1cu_ctx* c, const vc1cu_params* p, int ref_id, int
         ResultSlot& s = result_slot(c, mv_slot, P.mbw * P.mbh, false);
         FrameSlot& fp = alloc_frame(c, pred_id, P.W, P.H);
         const DevFrame pd = fp.view();
+        Timer tm(c, kMc);
         launch_mc(P, ref, s.r.mvs, s.r.bmv, s.r.use4, mv_mode, (uint8_t*)pd.y, (uint8_t*)pd.u, (uint8_t*)pd.v, fp.pitch_y,
                   fp.pitch_c, c->stream);
         ck(cudaGetLastError(), "mc_kernel launch");
+        tm.stop(1);
         return VC1CU_OK;
     });
 }
@@ -794,8 +943,10 @@ int vc1cu_forward_quant_device(vc1cu_ctx* c, const vc1cu_params* p, int src_id, 
         FrameSlot& fs = frame_slot(c, src_id);
         FrameSlot& fp = frame_slot(c, pred_id);
         if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size mismatch"};
+        Timer tm(c, kXform);
         launch_xform(P, fs.view(), fp.view(), type_mask, d_coeffs, d_levels, c->stream);
         ck(cudaGetLastError(), "xform_kernel launch");
+        tm.stop(1);
         return VC1CU_OK;
     });
 }
@@ -818,8 +969,10 @@ int vc1cu_forward_quant(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pre
         FrameSlot& fs = frame_slot(c, src_id);
         FrameSlot& fp = frame_slot(c, pred_id);
         if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size mismatch"};
+        Timer tm(c, kXform);
         launch_xform(P, fs.view(), fp.view(), type_mask, dco, dlv, c->stream);
         ck(cudaGetLastError(), "xform_kernel launch");
+        tm.stop(1);
         if (coeffs) ck(cudaMemcpyAsync(coeffs, dco, cb, cudaMemcpyDeviceToHost, c->stream), "download coefficients");
         if (levels) ck(cudaMemcpyAsync(levels, dlv, lb, cudaMemcpyDeviceToHost, c->stream), "download levels");
         sync_checked(c);

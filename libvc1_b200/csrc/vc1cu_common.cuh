@@ -198,8 +198,8 @@ __device__ inline bool hybrid_of(int2 pre, int2 A, int2 C, bool a_intra, bool c_
 // and the reference's long double is that integer rounded to mant_bits significant bits
 // (round to nearest, ties to even). Candidates of one call share lam_s, so comparing the
 // rounded integers orders them exactly as the reference's long double comparisons do.
-__device__ inline unsigned __int128 score_key(const DevParams& p, uint64_t sad, uint32_t rate) {
-    unsigned __int128 v = ((unsigned __int128)sad << p.lam_s) + (unsigned __int128)p.lam_m * rate;
+__device__ inline unsigned __int128 score_key(const DevParams& p, uint64_t lam_m, int lam_s, uint64_t sad, uint32_t rate) {
+    unsigned __int128 v = ((unsigned __int128)sad << lam_s) + (unsigned __int128)lam_m * rate;
     const uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;
     const int nbits = hi ? 128 - __clzll((long long)hi) : (lo ? 64 - __clzll((long long)lo) : 0);
     if (nbits > p.mant_bits) {

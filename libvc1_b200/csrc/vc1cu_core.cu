@@ -43,6 +43,8 @@ struct WarpMem {
 
 struct Mb {
     int lane;
+    uint64_t lam_m;   // this pass's lambda_me = lam_m * 2^-lam_s
+    int lam_s;
     int mx, my, x0, y0, pos, aw, ah;  // aw/ah: visible wrt the internal raster (cur.width)
     const PassDesc* d;
     WarpMem sm;
@@ -737,7 +739,7 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
         }
         rate += mv_rate_bits(P, mv, pred, mode, more);
         m.sm.list_rate[m.lane] = rate;
-        m.sm.list_key[m.lane] = score_key(P, m.sm.batch_cost[m.lane], rate);
+        m.sm.list_key[m.lane] = score_key(P, m.lam_m, m.lam_s, m.sm.batch_cost[m.lane], rate);
     }
     __syncwarp();
     // rate winner: min over (score, sad, tie_less)
@@ -772,7 +774,7 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
         const uint64_t s = m.sm.batch_cost[i];
         const bool elig = s < UINT64_MAX / 8 && s <= limit;
         const uint64_t satd = elig ? m.sm.list_satd[ei++] : kBad;
-        const unsigned __int128 k = score_key(P, satd, m.sm.list_rate[i]);
+        const unsigned __int128 k = score_key(P, m.lam_m, m.lam_s, satd, m.sm.list_rate[i]);
         bool better;
         if (best < 0) better = true;
         else {
@@ -1014,6 +1016,8 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         m.aw = imax(0, imin(16, P.W - m.x0));
         m.ah = imax(0, imin(16, P.H - m.y0));
         m.gref = GlobSampler{d.ref.y, d.ref.pitch_y, P.W, P.H};
+        m.lam_m = d.lam_m;
+        m.lam_s = d.lam_s;
         const DevResult& o = d.out;
         const bool aborted = *(volatile int*)&st->abort;
         // wavefront: left, top-left, top, top-right of the same pass
@@ -1097,7 +1101,7 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             int2 out_mv = one.mv;
             uint8_t use4 = 0, intra = 0;
             uint64_t chosen = one_sad, temporal_screen = one_sad;
-            const double lambda = P.lambda;
+            const double lambda = d.lambda;
             if (allow_4mv) {
                 if (m.lane < 4) cur4[m.lane] = one.mv;
                 __syncwarp();

@@ -40,6 +40,10 @@ struct DevResult {
 struct PassDesc {
     DevFrame cur, ref;
     int mode, allow_intra;
+    int pq;                // this picture's PQINDEX
+    double lambda;         // max(1, 0.35*pq)
+    uint64_t lam_m;        // lambda = lam_m * 2^-lam_s exactly
+    int lam_s;
     int seeded;            // 1: seed fields below are valid
     const int2* seed_mvs;
     const double* seed_dl;

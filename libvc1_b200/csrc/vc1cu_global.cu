@@ -309,7 +309,7 @@ size_t gstate_bytes() { return sizeof(GState); }
 // Host driver: runs the staged search for n states already initialised in device memory
 // (cur, ref, range, outputs, phase = 0). Every stage is one scoring launch sized to the
 // stage's largest candidate list and sampling stride, bracketed by plan/fold launches.
-void run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream) {
+int run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream) {
     struct Stage { int maxc, stride; };
     Stage st[4];
     int ns = 0;
@@ -338,6 +338,7 @@ void run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_
         gsad_kernel<<<grid, 256, 0, stream>>>(d_states, W, H, rows_per_slab);
         gplan_kernel<<<(n + 63) / 64, 64, 0, stream>>>(d_states, n);
     }
+    return 1 + 2 * ns;
 }
 
 void init_gstate(GState* h, const DevFrame& cur, const DevFrame& ref, int range, int* out_global,

@@ -84,3 +84,48 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
 }
 
 }  // namespace vc1cu
+
+namespace vc1cu {
+
+// INT32 lane-op throughput calibration: 8 independent chains of (add, xor) per thread, so
+// every instruction is one 32-bit integer op with no dependency stall at full occupancy.
+__global__ void int32_peak_kernel(uint32_t* out, int iters, uint32_t k1, uint32_t k2) {
+    uint32_t a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = threadIdx.x * 2654435761u + (uint32_t)j * 40503u + blockIdx.x;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            a[j] = a[j] + k1;
+            a[j] = a[j] ^ k2;
+        }
+    }
+    uint32_t r = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r ^= a[j];
+    if (r == 0x9E3779B9u) out[0] = r;  // keeps the chains live
+}
+
+// Returns int32 lane-ops per second (16 ops per thread per iteration).
+double measure_int32_peak(cudaStream_t s, int sms) {
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, 4) != cudaSuccess) return 0.0;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    int32_peak_kernel<<<blocks, threads, 0, s>>>(d, 64, 0x1234567u, 0x9abcdefu);  // warm-up
+    cudaEventRecord(a, s);
+    int32_peak_kernel<<<blocks, threads, 0, s>>>(d, iters, 0x1234567u, 0x9abcdefu);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (ms <= 0.f) return 0.0;
+    return 16.0 * iters * (double)blocks * threads / (ms * 1e-3);
+}
+
+}  // namespace vc1cu

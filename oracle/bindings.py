@@ -220,6 +220,8 @@ class Reference:
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
+        L.ref_bench_analysis_multi.argtypes = [C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), i32, i32]
+        L.ref_bench_analysis_multi.restype = u64
         self.p = p
         self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
 
@@ -312,6 +314,13 @@ class Reference:
 
     def quantize_level(self, c):
         return self.lib.ref_scalar_quantize_level(self.h, c)
+
+    def bench_analysis_multi(self, jobs, threads):
+        """Wall ns over (Reference, cur RefFrame, ref RefFrame) jobs, each with its own config."""
+        hs = (vp * len(jobs))(*[j[0].h for j in jobs])
+        curs = (vp * len(jobs))(*[j[1].h for j in jobs])
+        refs = (vp * len(jobs))(*[j[2].h for j in jobs])
+        return self.lib.ref_bench_analysis_multi(hs, curs, refs, len(jobs), threads)
 
     def bench_analysis(self, pairs, threads):
         """Wall ns of analyze_p_picture + choose_transform_mb over (cur, ref) RefFrame pairs."""

@@ -54,9 +54,10 @@ EncoderConfig make_config(const vc1cu_params* p, int simd) {
     c.aq_strength = 0.0;
     c.dquant = false;
     if (simd) {
-        // --simd auto: per-primitive startup benchmark (encoder_core.cpp:3240-3243).
-        auto r = libvc1::auto_select_simd(true, true);
-        c.simd_dispatch = r.dispatch;
+        // --simd auto: per-primitive startup benchmark (encoder_core.cpp:3240-3243), run once
+        // per process and reused by every encoder this harness creates.
+        static const libvc1::SimdDispatch dispatch = libvc1::auto_select_simd(true, true).dispatch;
+        c.simd_dispatch = dispatch;
     } else {
         c.simd_dispatch.tier.fill(libvc1::SimdTier::None);
     }
@@ -198,7 +199,9 @@ int ref_analyze_p_core(void* h, void* cur, void* ref, int mode, int allow_intra,
         }
         const auto a = e.analyze_p_picture_core(F(cur), F(ref), to_mode(mode), allow_intra != 0, seed ? &s : nullptr);
         fill_out(a, out);
-        if (!seed) {
+        out->global_dx = out->global_dy = 0;
+        out->global_full_sad = 0;
+        if (!seed && c.motion_search_range > 0) {
             const auto g = e.global_motion_search(F(cur), F(ref),
                                                   std::min(c.motion_search_range, std::max(0, c.motion_local_search_range)));
             out->global_dx = g.dx;
@@ -292,6 +295,45 @@ void ref_forward_quant(void* h, void* src, void* pred, int type_mask, double* co
 }
 
 int ref_scalar_quantize_level(void* h, double coeff) { return E(h).scalar_quantize_level(coeff); }
+
+// CPU baseline over pairs that each carry their own encoder configuration (e.g. per-picture
+// PQINDEX): analyze_p_picture + choose_transform_mb of the chosen prediction for every MB,
+// one pair per worker thread at a time. Returns wall ns.
+uint64_t ref_bench_analysis_multi(void** handles, void** curs, void** refs, int n_pairs, int threads) {
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n_pairs) break;
+            auto* r = static_cast<RefEncoder*>(handles[i]);
+            const auto& c = r->cfg;
+            const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+            Vc1Encoder enc(c);
+            Frame pred;
+            pred.width = c.width;
+            pred.height = c.height;
+            pred.y.assign(static_cast<size_t>(c.width) * c.height, 0);
+            pred.u.assign(static_cast<size_t>(c.width / 2) * (c.height / 2), 128);
+            pred.v = pred.u;
+            const Frame& cur = F(curs[i]);
+            const Frame& ref = F(refs[i]);
+            const auto a = enc.analyze_p_picture(cur, ref);
+            for (int my = 0; my < mbh; ++my)
+                for (int mx = 0; mx < mbw; ++mx) {
+                    const size_t pos = static_cast<size_t>(my) * mbw + mx;
+                    if (a.use_4mv[pos]) enc.motion_compensate_4mv(pred, ref, mx, my, a.block_mvs[pos]);
+                    else enc.motion_compensate_mb(pred, ref, mx, my, a.mvs[pos], a.mv_mode);
+                    (void)enc.choose_transform_mb(cur, pred, mx, my, 0, true, c.pqindex, false);
+                }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+}
 
 // CPU baseline: analyze_p_picture + choose_transform_mb of the chosen prediction for every
 // MB of every (cur, ref) pair, one pair per worker thread at a time. Returns wall ns.

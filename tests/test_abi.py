@@ -28,8 +28,9 @@ def test_struct_layouts_match_header():
     assert C.sizeof(abi.Params) == 18 * 4 + 2 * 8
     assert C.sizeof(abi.Mv) == 8
     assert C.sizeof(abi.PAnalysisC) == 9 * 8 + 2 * 8 + 5 * 8 + 2 * 4 + 8
-    assert C.sizeof(abi.Counters) == 6 * 8
-    assert C.sizeof(api.Pass) == 6 * 4
+    assert C.sizeof(abi.Counters) == 7 * 8
+    assert C.sizeof(abi.Timing) == 5 * 8 + 2 * 8
+    assert C.sizeof(api.Pass) == 7 * 4
 
 
 def test_params_default_matches_reference_defaults():
