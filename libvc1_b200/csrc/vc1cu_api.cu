@@ -22,8 +22,8 @@
 
 namespace vc1cu {
 // kernels and drivers of the other translation units
-__global__ void core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, WinCfg wc,
-                                 uint32_t epoch, LaunchStatus* st);
+__global__ void core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass,
+                                 const int* order, WinCfg wc, uint32_t epoch, LaunchStatus* st);
 __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
@@ -145,6 +145,9 @@ struct vc1cu_ctx {
     std::vector<Timed> pending;
     std::vector<cudaEvent_t> event_pool;
     vc1cu_timing tsum{};
+    // wavefront order of the current macroblock raster
+    int* d_order = nullptr;
+    int order_mbw = 0, order_mbh = 0;
 };
 
 namespace {
@@ -248,6 +251,27 @@ void set_lambda(PassDesc& d, int pq) {
     const double fr = std::frexp(d.lambda, &e);
     d.lam_m = static_cast<uint64_t>(std::ldexp(fr, 53));
     d.lam_s = 53 - e;
+}
+
+// Wavefront order of an mbw x mbh raster: sorted by t = x + 2y, then by y.
+const int* wavefront_order(vc1cu_ctx* c, int mbw, int mbh) {
+    if (c->d_order && c->order_mbw == mbw && c->order_mbh == mbh) return c->d_order;
+    std::vector<int> o;
+    o.reserve((size_t)mbw * mbh);
+    for (int t = 0; t <= (mbw - 1) + 2 * (mbh - 1); ++t)
+        for (int y = 0; y < mbh; ++y) {
+            const int x = t - 2 * y;
+            if (x >= 0 && x < mbw) o.push_back(y * mbw + x);
+        }
+    if (c->d_order) cudaFree(c->d_order);
+    c->d_order = nullptr;
+    void* d = nullptr;
+    ck(cudaMalloc(&d, sizeof(int) * o.size()), "cudaMalloc(order)");
+    c->d_order = static_cast<int*>(d);
+    ck(cudaMemcpy(c->d_order, o.data(), sizeof(int) * o.size(), cudaMemcpyHostToDevice), "cudaMemcpy(order)");
+    c->order_mbw = mbw;
+    c->order_mbh = mbh;
+    return c->d_order;
 }
 
 int stage_max(int R) {
@@ -581,7 +605,8 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
     {
         Timer tm(c, kCore);
-        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, wc, c->epoch, c->d_status);
+        const int* order = wavefront_order(c, P.mbw, P.mbh);
+        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, order, wc, c->epoch, c->d_status);
         ck(cudaGetLastError(), "core_pass_kernel launch");
         tm.stop(1);
     }
@@ -712,6 +737,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_passes) cudaFree(c->d_passes);
     if (c->d_gstates) cudaFree(c->d_gstates);
     if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->d_order) cudaFree(c->d_order);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->staging_done) cudaEventDestroy(c->staging_done);
     for (auto& t : c->pending) {

@@ -990,8 +990,12 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
     __syncwarp();
 }
 
+// order[j] = raster index of the j-th macroblock in wavefront order (t = x + 2y, then y):
+// every dependency of an MB (left, top-left, top, top-right) has a smaller t, and the MBs
+// of one t are mutually independent, so consecutive queue items can run concurrently.
 __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes,
-                                                          int npass, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
+                                                          int npass, const int* order, WinCfg wc, uint32_t epoch,
+                                                          LaunchStatus* st) {
     extern __shared__ __align__(16) uint8_t smem[];
     Mb m;
     m.lane = threadIdx.x & 31;
@@ -1005,7 +1009,7 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         item = __shfl_sync(FULL, item, 0);
         if (item >= total) break;
         const int pi_idx = (int)(item % (unsigned)npass);
-        const int mbi = (int)(item / (unsigned)npass);
+        const int mbi = __ldg(&order[item / (unsigned)npass]);
         const PassDesc& d = passes[pi_idx];
         m.d = &d;
         m.mx = mbi % P.mbw;
