@@ -109,11 +109,11 @@ def parse_clocks(path: str, device: int):
 class Runner:
     """Drives one step of the analysis path through the C ABI."""
 
-    def __init__(self, ctx, clip):
+    def __init__(self, ctx, clip, pictures=None):
         from libvc1_b200.abi import MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED, MV_QPEL
 
         self.ctx, self.clip = ctx, clip
-        self.pics = anchors_and_pictures()
+        self.pics = anchors_and_pictures()[:pictures]
         self.frames = sorted({f for p in self.pics for f in p[:2]})
         self.p0 = params(8)
         self.modes = (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED)
@@ -174,7 +174,7 @@ def run_ours(args, rank, world, device):
     if ctx is None:
         raise RuntimeError(f"CUDA backend unavailable: {err}")
     clip = make_clip(rank)
-    run = Runner(ctx, clip)
+    run = Runner(ctx, clip, args.pictures)
     run.upload_all()
     ext = torch.cuda.ExternalStream(ctx.stream_handle(), device=device)
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -222,7 +222,7 @@ def run_ours(args, rank, world, device):
         pinned[f] = tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (y, u, v))
     host_levels = torch.empty(run.levels.shape, dtype=torch.int16).pin_memory()
     e2e_s = []
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
         flush_l2(torch, l2)
         if world > 1:
             torch.distributed.barrier()
@@ -236,7 +236,7 @@ def run_ours(args, rank, world, device):
     te = torch.tensor([sum(e2e_s)], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * mbs_per_step * args.steps / float(te.item())
+    e2e_value = world * mbs_per_step * args.steps / float(te.item()) if e2e_s else None
     # ---- roofline of the dominant kernel (core_pass_kernel), INT32-bound
     n = len(run.pics)
     ops_step = n * MBS * (OPS_PER_MB["unseeded"] + OPS_PER_MB["seeded_hpel"] + OPS_PER_MB["seeded_bilinear"] +
@@ -259,7 +259,7 @@ def run_ours(args, rank, world, device):
                                    "pictures/step, search +/-64, Mixed-MV, nonuniform QP 4-12, 4 transform sizes",
                        "mb_per_step_per_gpu": mbs_per_step, "passes_per_picture": 5,
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
-            "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+            "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
                     "h2d_bytes_per_step": len(run.frames) * run.frame_bytes,
                     "d2h_bytes_per_step": run.result_bytes()},
             "gpu_launches": counters["kernel_launches"],
@@ -349,6 +349,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--pictures", type=int, default=None, help="analyse only the first N P pictures (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
