@@ -586,7 +586,8 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         wc.seen_words = 1;
         wc.keys_cap = 32;
     }
-    wc.ww = 16 + 2 * wc.rw + 3;
+    wc.wh = 16 + 2 * wc.rw + 3;
+    wc.wp = (wc.wh + 15 + 15) & ~15;
     wc.warp_bytes = warp_bytes_for_host(wc);
     int warps = 4;
     while (warps > 1 && (size_t)warps * wc.warp_bytes > (size_t)c->max_smem) --warps;

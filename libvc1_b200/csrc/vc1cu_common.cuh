@@ -122,9 +122,12 @@ __device__ inline int modular_component_distance(int a, int b, int range) {
     d = ((d + range) % span + span) % span - range;
     return iabs(d);
 }
+// mvrange_x_qpel {256,512,2048,4096} / mvrange_y_qpel {128,256,512,1024} (:1263-1271)
+__device__ __forceinline__ int mvrange_xq(int r) { return r < 2 ? (256 << r) : (2048 << (r - 2)); }
+__device__ __forceinline__ int mvrange_yq(int r) { return 128 << r; }
 __device__ inline int modular_mv_distance(const DevParams& p, int2 a, int2 b) {
-    const int xr[4] = {256, 512, 2048, 4096}, yr[4] = {128, 256, 512, 1024};
-    return modular_component_distance(a.x, b.x, xr[p.mvrange]) + modular_component_distance(a.y, b.y, yr[p.mvrange]);
+    return modular_component_distance(a.x, b.x, mvrange_xq(p.mvrange)) +
+           modular_component_distance(a.y, b.y, mvrange_yq(p.mvrange));
 }
 
 // groupa::kMvDiffBits[0], vc1_groupa_tables.h:26 (VC-1 MVDATA VLC lengths, table 0)
@@ -144,9 +147,10 @@ __device__ inline int mv_cat(int v, bool halfpel) {
     if (a <= (halfpel ? 94 : 158)) return 5;
     return -1;
 }
-__device__ inline int mv_component_bits(int cat, bool halfpel) {
-    const int sz[6] = {0, 2, 3, 4, 5, 8};
-    return sz[cat] - ((halfpel && cat == 5) ? 1 : 0);
+// {0,2,3,4,5,8}[cat] minus the half-pel category-5 bit (:1173-1176)
+__device__ __forceinline__ int mv_component_bits(int cat, bool halfpel) {
+    const int sz = cat == 5 ? 8 : (cat ? cat + 1 : 0);
+    return sz - ((halfpel && cat == 5) ? 1 : 0);
 }
 
 // Vc1Encoder::motion_vector_rate_bits, encoder_motion.cpp:3214-3225, with mvdata_for_mode
@@ -164,9 +168,10 @@ __device__ inline uint32_t mv_rate_bits(const DevParams& p, int2 desired, int2 p
     }
     int suffix;
     if (sym == 34 || sym == 71) {
-        const int kx[4] = {9, 10, 12, 13}, ky[4] = {8, 9, 10, 11};
+        // mvrange_kx {9,10,12,13} / mvrange_ky {8,9,10,11} (:1273-1281)
+        const int kx = p.mvrange < 2 ? 9 + p.mvrange : 10 + p.mvrange, ky = 8 + p.mvrange;
         const int h = hp ? 1 : 0;
-        suffix = (kx[p.mvrange] - h) + (ky[p.mvrange] - h);
+        suffix = (kx - h) + (ky - h);
     } else {
         suffix = mv_component_bits(xc, hp) + mv_component_bits(yc, hp);
     }

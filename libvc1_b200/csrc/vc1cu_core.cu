@@ -10,7 +10,8 @@
 //     four neighbours' done flags (acquire loads, bounded spin that flags
 //     VC1CU_ERR_TIMEOUT instead of hanging) and publishes its own MB with a release store;
 //   * the reference search window of the MB is staged once into the warp's shared memory
-//     (edge-replicated), candidates outside it read HBM with clamping;
+//     with 128-bit loads on a 16-byte-aligned grid (edge-replicated outside the picture);
+//     candidates outside it read HBM with clamping;
 //   * integer stages score one candidate per lane; sub-pel stages split each candidate's
 //     block into 8-pixel row segments across lanes; every selection uses the reference's
 //     total orders, so the parallel evaluation returns the reference's exact choice.
@@ -38,7 +39,11 @@ struct WarpMem {
     unsigned __int128* list_key;
     int2* batch;           // scratch MV batch
     uint64_t* batch_cost;
-    int* misc;             // small scalars
+    int2* stencil;         // sub-pel stencil MVs of the current refinement stage
+    uint64_t* top;         // sorted top-8 keys of the UMH search
+    uint32_t* cur2;        // current MB, even columns packed 4 per word: [row][2]
+    uint32_t* cur4;        // current MB, every 4th column packed: [row]
+    int* misc;             // small scalars: [0] top count, [1] compaction count
 };
 
 struct Mb {
@@ -48,12 +53,46 @@ struct Mb {
     int mx, my, x0, y0, pos, aw, ah;  // aw/ah: visible wrt the internal raster (cur.width)
     const PassDesc* d;
     WarpMem sm;
-    int wx0, wy0, ww;
+    int wx0, wy0, wp, wh;  // window origin (wx0 a multiple of 16), row pitch = width, height
     GlobSampler gref;
 };
 
 __device__ __forceinline__ bool win_inside(const Mb& m, int xa, int ya, int xb, int yb) {
-    return xa >= m.wx0 && ya >= m.wy0 && xb < m.wx0 + m.ww && yb < m.wy0 + m.ww;
+    return xa >= m.wx0 && ya >= m.wy0 && xb < m.wx0 + m.wp && yb < m.wy0 + m.wh;
+}
+
+// 16 window bytes starting at an arbitrary offset, as four little-endian words.
+__device__ __forceinline__ void win_load16(const uint8_t* p, uint32_t r[4]) {
+    const uint32_t* a = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+    const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8;
+    const uint32_t w0 = a[0], w1 = a[1], w2 = a[2], w3 = a[3], w4 = a[4];
+    r[0] = __funnelshift_r(w0, w1, sh);
+    r[1] = __funnelshift_r(w1, w2, sh);
+    r[2] = __funnelshift_r(w2, w3, sh);
+    r[3] = __funnelshift_r(w3, w4, sh);
+}
+
+// mb_sad of a full 16x16 MB from the window with packed byte SADs (__vsadu4), strides 1/2/4.
+template <int STRIDE>
+__device__ __forceinline__ uint32_t sad_packed(const Mb& m, const uint8_t* base) {
+    uint32_t acc = 0;
+    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur);
+#pragma unroll 4
+    for (int y = 0; y < 16; y += STRIDE) {
+        uint32_t r[4];
+        win_load16(base + y * m.wp, r);
+        if (STRIDE == 1) {
+            acc += __vsadu4(r[0], c32[y * 4 + 0]) + __vsadu4(r[1], c32[y * 4 + 1]) + __vsadu4(r[2], c32[y * 4 + 2]) +
+                   __vsadu4(r[3], c32[y * 4 + 3]);
+        } else if (STRIDE == 2) {
+            acc += __vsadu4(__byte_perm(r[0], r[1], 0x6420), m.sm.cur2[y * 2 + 0]) +
+                   __vsadu4(__byte_perm(r[2], r[3], 0x6420), m.sm.cur2[y * 2 + 1]);
+        } else {
+            const uint32_t e = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+            acc += __vsadu4(e, m.sm.cur4[y]);
+        }
+    }
+    return acc;
 }
 
 // ---- integer SAD of the 16x16 MB, mb_sad (encoder_motion.cpp:2197-2285) ----------------
@@ -76,8 +115,13 @@ __device__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int 
     if (hidden_padding(P, m.x0, m.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
     uint32_t s;
     const bool fast = win_inside(m, m.x0 + dx, m.y0 + dy, m.x0 + dx + 15, m.y0 + dy + 15);
-    const WinSampler ws{m.sm.win, m.ww, m.wx0, m.wy0};
-    if (fast) {
+    const WinSampler ws{m.sm.win, m.wp, m.wx0, m.wy0};
+    if (fast && m.aw == 16 && m.ah == 16) {
+        const uint8_t* base = m.sm.win + (m.y0 + dy - m.wy0) * m.wp + (m.x0 + dx - m.wx0);
+        if (stride == 1) s = sad_packed<1>(m, base);
+        else if (stride == 2) s = sad_packed<2>(m, base);
+        else s = sad_packed<4>(m, base);
+    } else if (fast) {
         if (stride == 1) s = sad_int_loop<1>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
         else if (stride == 2) s = sad_int_loop<2>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
         else s = sad_int_loop<4>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
@@ -116,7 +160,7 @@ __device__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int 
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
                 int pred[8];
                 if (win_inside(m, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
-                    predict_row<8>(WinSampler{m.sm.win, m.ww, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                    predict_row<8>(WinSampler{m.sm.win, m.wp, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
                 else
                     predict_row<8>(m.gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
                 const uint8_t* c = m.sm.cur + (cy + r) * 16 + cx + c0;
@@ -156,7 +200,7 @@ __device__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
                 if (fast)
-                    predict_row<4>(WinSampler{m.sm.win, m.ww, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                    predict_row<4>(WinSampler{m.sm.win, m.wp, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
                 else
                     predict_row<4>(m.gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
 #pragma unroll
@@ -182,43 +226,76 @@ __device__ __forceinline__ bool seen_test_set(uint32_t* bits, int r, int dx, int
 
 // ---- integer UMH (encoder_motion.cpp:1781-2023) -----------------------------------------
 
-struct Top8 {
-    uint64_t k[8];
-    int n;
-};
-
-// Merges the n keys of m.sm.keys (UINT64_MAX = skipped) into the sorted top-8 list.
-__device__ void top8_merge(const Mb& m, Top8& top, int n) {
+// Merges the n keys of m.sm.keys (UINT64_MAX = skipped) into the sorted top-8 list
+// m.sm.top / m.sm.misc[0]. Keys below the current 8th entry are compacted with a ballot
+// first; the few survivors are ranked and merged on every lane identically.
+__device__ void top8_merge(const Mb& m, int n) {
     uint64_t* keys = m.sm.keys;
-    uint64_t sel[8];
-    int ns = 0;
-    const uint64_t bound = top.n == 8 ? top.k[7] : UINT64_MAX;
-    for (int r = 0; r < 8; ++r) {
-        uint64_t lm = UINT64_MAX;
-        for (int i = m.lane; i < n; i += 32) lm = keys[i] < lm ? keys[i] : lm;
-        const uint64_t g = warp_min_u64(lm);
-        if (g == UINT64_MAX || g >= bound) break;
-        sel[ns++] = g;
-        for (int i = m.lane; i < n; i += 32)
-            if (keys[i] == g) keys[i] = UINT64_MAX;
+    uint64_t* top = m.sm.top;
+    const int tn = m.sm.misc[0];
+    const uint64_t bound = tn == 8 ? top[7] : UINT64_MAX;
+    int cnt = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + m.lane;
+        const uint64_t k = i < n ? keys[i] : UINT64_MAX;
+        const bool take = k < bound;
+        const unsigned b = __ballot_sync(FULL, take);
+        if (take) keys[cnt + __popc(b & ((1u << m.lane) - 1))] = k;
+        cnt += __popc(b);
         __syncwarp();
     }
-    // merge two sorted lists, keep 8
+    if (!cnt) return;
+    const uint64_t* sel;
+    int ns = 0;
+    if (cnt <= 32) {
+        // rank of each survivor (keys are distinct), the 8 lowest ranks in order
+        const uint64_t k = m.lane < cnt ? keys[m.lane] : UINT64_MAX;
+        int rank = 0;
+        for (int j = 0; j < cnt; ++j) rank += keys[j] < k;
+        __syncwarp();
+        if (m.lane < cnt && rank < 8) keys[rank] = k;
+        __syncwarp();
+        ns = cnt < 8 ? cnt : 8;
+        sel = keys;
+    } else {
+        uint64_t* out8 = m.sm.list_sad;  // idle during the integer search
+        for (int r = 0; r < 8; ++r) {
+            uint64_t lm = UINT64_MAX;
+            for (int i = m.lane; i < cnt; i += 32) lm = keys[i] < lm ? keys[i] : lm;
+            const uint64_t g = warp_min_u64(lm);
+            if (m.lane == 0) out8[r] = g;
+            for (int i = m.lane; i < cnt; i += 32)
+                if (keys[i] == g) keys[i] = UINT64_MAX;
+            __syncwarp();
+        }
+        ns = 8;
+        sel = out8;
+    }
     uint64_t out[8];
     int a = 0, b = 0, o = 0;
-    while (o < 8 && (a < top.n || b < ns)) {
-        if (b >= ns || (a < top.n && top.k[a] < sel[b])) out[o++] = top.k[a++];
-        else out[o++] = sel[b++];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        if (a < tn || b < ns) {
+            const uint64_t ta = a < tn ? top[a] : UINT64_MAX, tb = b < ns ? sel[b] : UINT64_MAX;
+            if (ta < tb) { out[q] = ta; ++a; } else { out[q] = tb; ++b; }
+            ++o;
+        }
     }
-    for (int i = 0; i < o; ++i) top.k[i] = out[i];
-    top.n = o;
+    __syncwarp();
+    if (m.lane < o) {
+        uint64_t v = out[0];
+#pragma unroll
+        for (int q = 1; q < 8; ++q) if (m.lane == q) v = out[q];
+        top[m.lane] = v;
+    }
+    if (m.lane == 0) m.sm.misc[0] = o;
     __syncwarp();
 }
 
 // Scores the candidates produced by gen(i) for i < n at sampled stride 2 (the UMH
 // `consider` lambda, encoder_motion.cpp:1821-1839) and merges them into top.
 template <class Gen>
-__device__ void umh_stage(const DevParams& P, const Mb& m, Top8& top, int n, int range, Gen gen) {
+__device__ void umh_stage(const DevParams& P, const Mb& m, int n, int range, Gen gen) {
     for (int i = m.lane; i < n; i += 32) {
         int2 c = gen(i);
         c.x = iclamp(c.x, -range, range);
@@ -228,7 +305,7 @@ __device__ void umh_stage(const DevParams& P, const Mb& m, Top8& top, int n, int
         m.sm.keys[i] = key;
     }
     __syncwarp();
-    top8_merge(m, top, n);
+    top8_merge(m, n);
 }
 
 // Minimum key over full-resolution candidates (no top list), optional first-visit filter.
@@ -263,9 +340,9 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
         m.sm.seen[i] = 0;
         m.sm.seen_full[i] = 0;
     }
+    if (m.lane == 0) m.sm.misc[0] = 0;
     __syncwarp();
-    Top8 top;
-    top.n = 0;
+    const uint64_t* top = m.sm.top;
     // predictor seeds (:1843-1850)
     {
         int2 s[5];
@@ -276,17 +353,17 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
         s[ns++] = make_int2(gdx, gdy);
         if (pi.a_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
         if (pi.c_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
-        umh_stage(P, m, top, ns, range, [&](int i) { return s[i]; });
+        umh_stage(P, m, ns, range, [&](int i) { return s[i]; });
     }
     // 5x5 around best (:1855-1859)
     {
-        const int cx = key_dx(top.k[0]), cy = key_dy(top.k[0]);
-        umh_stage(P, m, top, 25, range, [&](int i) { return make_int2(cx + i % 5 - 2, cy + i / 5 - 2); });
+        const int cx = key_dx(top[0]), cy = key_dy(top[0]);
+        umh_stage(P, m, 25, range, [&](int i) { return make_int2(cx + i % 5 - 2, cy + i / 5 - 2); });
     }
     // sparse lattice over the whole window (:1865-1870)
     if (range >= 8) {
         const int L = (2 * range) / 8 + 1;
-        umh_stage(P, m, top, L * L + 2 * L, range, [&](int i) {
+        umh_stage(P, m, L * L + 2 * L, range, [&](int i) {
             if (i < L * L) return make_int2(-range + (i % L) * 8, -range + (i / L) * 8);
             const int j = i - L * L;
             const int d = -range + (j >> 1) * 8;
@@ -296,10 +373,10 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
     // uneven cross (:1875-1884)
     {
         const int cs = range >= 96 ? 8 : (range >= 32 ? 4 : 2);
-        const int cx = key_dx(top.k[0]), cy = key_dy(top.k[0]);
+        const int cx = key_dx(top[0]), cy = key_dy(top[0]);
         const int vlimit = imin(range, imax(8, range / 2));
         const int nh = range / cs, nv = vlimit / cs;
-        umh_stage(P, m, top, 2 * nh + 2 * nv, range, [&](int i) {
+        umh_stage(P, m, 2 * nh + 2 * nv, range, [&](int i) {
             if (i < 2 * nh) {
                 const int d = cs * (i / 2 + 1);
                 return (i & 1) ? make_int2(cx + d, cy) : make_int2(cx - d, cy);
@@ -312,9 +389,9 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
     // multi-hexagon rings (:1889-1897)
     {
         const int hs = range >= 96 ? 8 : (range >= 24 ? 4 : 2);
-        const int hx = key_dx(top.k[0]), hy = key_dy(top.k[0]);
+        const int hx = key_dx(top[0]), hy = key_dy(top[0]);
         const int nr = range / hs;
-        umh_stage(P, m, top, 6 * nr, range, [&](int i) {
+        umh_stage(P, m, 6 * nr, range, [&](int i) {
             const int r = hs * (i / 6 + 1), h = (r + 1) / 2;
             switch (i % 6) {
                 case 0: return make_int2(hx - r, hy);
@@ -328,34 +405,34 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
     }
     // iterative small hexagon (:1902-1908)
     for (int iter = 0; iter < 32; ++iter) {
-        const uint64_t before = top.k[0];
+        const uint64_t before = top[0];
         const int ox = key_dx(before), oy = key_dy(before);
-        umh_stage(P, m, top, 6, range, [&](int i) {
+        umh_stage(P, m, 6, range, [&](int i) {
             const int dxs[6] = {-2, 2, -1, 1, -1, 1}, dys[6] = {0, 0, -2, -2, 2, 2};
             return make_int2(ox + dxs[i], oy + dys[i]);
         });
-        if (key_dx(top.k[0]) == ox && key_dy(top.k[0]) == oy) break;
+        if (key_dx(top[0]) == ox && key_dy(top[0]) == oy) break;
     }
     // closing diamond (:1909-1913)
     {
-        const int ox = key_dx(top.k[0]), oy = key_dy(top.k[0]);
-        umh_stage(P, m, top, 4, range, [&](int i) {
+        const int ox = key_dx(top[0]), oy = key_dy(top[0]);
+        umh_stage(P, m, 4, range, [&](int i) {
             const int dxs[4] = {-1, 1, 0, 0}, dys[4] = {0, 0, -1, 1};
             return make_int2(ox + dxs[i], oy + dys[i]);
         });
     }
     // full-resolution finalists (:1929-1952)
-    const int nf = imin(4, top.n);
+    const int nf = imin(4, m.sm.misc[0]);
     uint64_t fk = full_stage(P, m, nf * 9, range, 1, true, [&](int i, bool& ok) {
         ok = true;
-        const uint64_t t = top.k[i / 9];
+        const uint64_t t = top[i / 9];
         return make_int2(iclamp(key_dx(t) + (i % 9) % 3 - 1, -range, range),
                          iclamp(key_dy(t) + (i % 9) / 3 - 1, -range, range));
     });
     IntRes full{key_dx(fk), key_dy(fk), key_cost(fk)};
     if (fk == UINT64_MAX) {  // unreachable in practice (:1948-1951)
-        full.dx = key_dx(top.k[0]);
-        full.dy = key_dy(top.k[0]);
+        full.dx = key_dx(top[0]);
+        full.dy = key_dy(top[0]);
         full.cost = mb_sad(P, m, full.dx, full.dy, 1);
         fk = int_key(full.cost, full.dx, full.dy);
     }
@@ -482,6 +559,13 @@ __device__ void list_add_batch(const DevParams& P, const Mb& m, int& n, const in
     __syncwarp();
 }
 
+// Lanes i < nb write gen(i) to the warp's stencil buffer.
+template <class G>
+__device__ __forceinline__ void put_stencil(const Mb& m, int nb, G gen) {
+    if (m.lane < nb) m.sm.stencil[m.lane] = gen(m.lane);
+    __syncwarp();
+}
+
 __device__ __forceinline__ const uint64_t* list_find(const Mb& m, int n, int2 mv, int& idx) {
     for (int j = 0; j < n; ++j)
         if (m.sm.list_mv[j].x == mv.x && m.sm.list_mv[j].y == mv.y) {
@@ -550,7 +634,8 @@ __device__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, in
         __syncwarp();
         n = 1;
     } else {
-        list_add_batch(P, m, n, &seed, 1, bx, by, bw, bh, emode);
+        put_stencil(m, 1, [&](int) { return seed; });
+        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, emode);
     }
     int2 best = seed;
     uint64_t cost = m.sm.list_sad[0];
@@ -560,40 +645,43 @@ __device__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, in
         if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
         return v;
     };
-    auto stage = [&](const int2* pts, int np) {
-        int2 b[9];
-        for (int i = 0; i < np; ++i) b[i] = fix(pts[i]);
-        list_add_batch(P, m, n, b, np, bx, by, bw, bh, emode);
-        update_min(m, n, b, np, best, cost);
+    // one stencil stage: gen(i) for i < np, clamped, scored and folded into (cost, best)
+    auto stage = [&](int np, auto gen) {
+        put_stencil(m, np, [&](int i) { return fix(gen(i)); });
+        list_add_batch(P, m, n, m.sm.stencil, np, bx, by, bw, bh, emode);
+        update_min(m, n, m.sm.stencil, np, best, cost);
+    };
+    // the two candidates beside an axis move: (c.x, c.y -/+ d) or (c.x -/+ d, c.y)
+    auto side = [](int2 c, int d, bool vertical) {
+        return [=](int i) { const int o = i ? d : -d; return vertical ? make_int2(c.x, c.y + o) : make_int2(c.x + o, c.y); };
+    };
+    auto cross = [](int2 c, int d) {
+        return [=](int i) {
+            return i == 0 ? make_int2(c.x - d, c.y) : i == 1 ? make_int2(c.x + d, c.y) : i == 2 ? make_int2(c.x, c.y - d)
+                                                                                                   : make_int2(c.x, c.y + d);
+        };
     };
     if (P.fast_subpel) {
-        if (hp || true) {
-            if (cost == 0 && best.x == 0 && best.y == 0) return RefineOut{best, 0};
-        }
-        int2 c4[4] = {{seed.x - 2, seed.y}, {seed.x + 2, seed.y}, {seed.x, seed.y - 2}, {seed.x, seed.y + 2}};
-        stage(c4, 4);
+        if (cost == 0 && best.x == 0 && best.y == 0) return RefineOut{best, 0};
+        stage(4, cross(seed, 2));
         const int2 axis = best;
         const int dx = axis.x - seed.x, dy = axis.y - seed.y;
-        if (dx && !dy) { int2 c2[2] = {{axis.x, axis.y - 2}, {axis.x, axis.y + 2}}; stage(c2, 2); }
-        else if (dy && !dx) { int2 c2[2] = {{axis.x - 2, axis.y}, {axis.x + 2, axis.y}}; stage(c2, 2); }
+        if (dx && !dy) stage(2, side(axis, 2, true));
+        else if (dy && !dx) stage(2, side(axis, 2, false));
         if (!hp) {
             const int2 half = best;
-            int2 q4[4] = {{half.x - 1, half.y}, {half.x + 1, half.y}, {half.x, half.y - 1}, {half.x, half.y + 1}};
-            stage(q4, 4);
+            stage(4, cross(half, 1));
             const int2 qa = best;
             const int qdx = qa.x - half.x, qdy = qa.y - half.y;
-            if (qdx && !qdy) { int2 c2[2] = {{qa.x, qa.y - 1}, {qa.x, qa.y + 1}}; stage(c2, 2); }
-            else if (qdy && !qdx) { int2 c2[2] = {{qa.x - 1, qa.y}, {qa.x + 1, qa.y}}; stage(c2, 2); }
+            if (qdx && !qdy) stage(2, side(qa, 1, true));
+            else if (qdy && !qdx) stage(2, side(qa, 1, false));
         }
     } else {
-        int2 h9[9];
-        for (int i = 0; i < 9; ++i) h9[i] = make_int2(seed.x + (i % 3 - 1) * 2, seed.y + (i / 3 - 1) * 2);
-        stage(h9, 9);
+        const int2 sd = seed;
+        stage(9, [=](int i) { return make_int2(sd.x + (i % 3 - 1) * 2, sd.y + (i / 3 - 1) * 2); });
         if (!hp) {
             const int2 half = best;
-            int2 q9[9];
-            for (int i = 0; i < 9; ++i) q9[i] = make_int2(half.x + i % 3 - 1, half.y + i / 3 - 1);
-            stage(q9, 9);
+            stage(9, [=](int i) { return make_int2(half.x + i % 3 - 1, half.y + i / 3 - 1); });
         }
     }
     return RefineOut{best, cost};
@@ -624,11 +712,12 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
         __syncwarp();
         n = 1;
     } else {
-        list_add_batch(P, m, n, &seed, 1, bx, by, bw, bh, mode);
+        put_stencil(m, 1, [&](int) { return seed; });
+        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, mode);
     }
     if (hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg)) {
-        const int2 z = make_int2(0, 0);
-        list_add_batch(P, m, n, &z, 1, bx, by, bw, bh, mode);
+        put_stencil(m, 1, [](int) { return make_int2(0, 0); });
+        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, mode);
     }
     int2 half_best = seed;
     uint64_t half_sad = m.sm.list_sad[0];
@@ -639,65 +728,69 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
         return v;
     };
     {
-        int2 hb[9];
-        int nb = 0;
-        if (fast) {
-            hb[nb++] = seed;
-            hb[nb++] = clampmv(seed.x - 2, seed.y);
-            hb[nb++] = clampmv(seed.x + 2, seed.y);
-            hb[nb++] = clampmv(seed.x, seed.y - 2);
-            hb[nb++] = clampmv(seed.x, seed.y + 2);
-        } else {
-            for (int oy = -2; oy <= 2; oy += 2)
-                for (int ox = -2; ox <= 2; ox += 2) hb[nb++] = clampmv(seed.x + ox, seed.y + oy);
-        }
-        list_add_batch(P, m, n, hb, nb, bx, by, bw, bh, mode);
-        update_min(m, n, hb, nb, half_best, half_sad);
+        const int nb = fast ? 5 : 9;
+        if (fast)
+            put_stencil(m, 5, [&](int i) {
+                return i == 0 ? seed : i == 1 ? clampmv(seed.x - 2, seed.y) : i == 2 ? clampmv(seed.x + 2, seed.y)
+                                 : i == 3 ? clampmv(seed.x, seed.y - 2) : clampmv(seed.x, seed.y + 2);
+            });
+        else
+            put_stencil(m, 9, [&](int i) { return clampmv(seed.x + (i % 3 - 1) * 2, seed.y + (i / 3 - 1) * 2); });
+        list_add_batch(P, m, n, m.sm.stencil, nb, bx, by, bw, bh, mode);
+        update_min(m, n, m.sm.stencil, nb, half_best, half_sad);
     }
     if (fast && !(half_best.x == seed.x && half_best.y == seed.y)) {
-        int2 dg[2];
-        int nd = 0;
         const int dx = half_best.x - seed.x, dy = half_best.y - seed.y;
+        const int2 hbv = half_best;
+        int nd = 0;
         if (dx && !dy) {
-            dg[nd++] = make_int2(half_best.x, iclamp(seed.y - 2, ymin, ymax));
-            dg[nd++] = make_int2(half_best.x, iclamp(seed.y + 2, ymin, ymax));
+            nd = 2;
+            put_stencil(m, 2, [&](int i) {
+                int2 v = make_int2(hbv.x, iclamp(seed.y + (i ? 2 : -2), ymin, ymax));
+                if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
+                return v;
+            });
         } else if (dy && !dx) {
-            dg[nd++] = make_int2(iclamp(seed.x - 2, xmin, xmax), half_best.y);
-            dg[nd++] = make_int2(iclamp(seed.x + 2, xmin, xmax), half_best.y);
+            nd = 2;
+            put_stencil(m, 2, [&](int i) {
+                int2 v = make_int2(iclamp(seed.x + (i ? 2 : -2), xmin, xmax), hbv.y);
+                if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
+                return v;
+            });
         }
-        if (hp)
-            for (int i = 0; i < nd; ++i) { dg[i].x = make_even(dg[i].x); dg[i].y = make_even(dg[i].y); }
         if (nd) {
-            list_add_batch(P, m, n, dg, nd, bx, by, bw, bh, mode);
-            update_min(m, n, dg, nd, half_best, half_sad);
+            list_add_batch(P, m, n, m.sm.stencil, nd, bx, by, bw, bh, mode);
+            update_min(m, n, m.sm.stencil, nd, half_best, half_sad);
         }
     }
     if (!hp) {
         if (fast) {
             const int2 qc = half_best;
-            int2 q5[5] = {qc, make_int2(iclamp(qc.x - 1, xmin, xmax), qc.y), make_int2(iclamp(qc.x + 1, xmin, xmax), qc.y),
-                          make_int2(qc.x, iclamp(qc.y - 1, ymin, ymax)), make_int2(qc.x, iclamp(qc.y + 1, ymin, ymax))};
-            list_add_batch(P, m, n, q5, 5, bx, by, bw, bh, mode);
+            put_stencil(m, 5, [&](int i) {
+                return i == 0 ? qc : i == 1 ? make_int2(iclamp(qc.x - 1, xmin, xmax), qc.y)
+                                 : i == 2 ? make_int2(iclamp(qc.x + 1, xmin, xmax), qc.y)
+                                 : i == 3 ? make_int2(qc.x, iclamp(qc.y - 1, ymin, ymax))
+                                          : make_int2(qc.x, iclamp(qc.y + 1, ymin, ymax));
+            });
+            list_add_batch(P, m, n, m.sm.stencil, 5, bx, by, bw, bh, mode);
             int j;
             uint64_t qcost = *list_find(m, n, qc, j);
             int2 qbmv = qc;
-            update_min(m, n, q5, 5, qbmv, qcost);
-            int2 q2[2];
-            int n2 = 0;
+            update_min(m, n, m.sm.stencil, 5, qbmv, qcost);
             const int dx = qbmv.x - qc.x, dy = qbmv.y - qc.y;
             if (dx && !dy) {
-                q2[n2++] = make_int2(qbmv.x, iclamp(qc.y - 1, ymin, ymax));
-                q2[n2++] = make_int2(qbmv.x, iclamp(qc.y + 1, ymin, ymax));
+                put_stencil(m, 2, [&](int i) { return make_int2(qbmv.x, iclamp(qc.y + (i ? 1 : -1), ymin, ymax)); });
+                list_add_batch(P, m, n, m.sm.stencil, 2, bx, by, bw, bh, mode);
             } else if (dy && !dx) {
-                q2[n2++] = make_int2(iclamp(qc.x - 1, xmin, xmax), qbmv.y);
-                q2[n2++] = make_int2(iclamp(qc.x + 1, xmin, xmax), qbmv.y);
+                put_stencil(m, 2, [&](int i) { return make_int2(iclamp(qc.x + (i ? 1 : -1), xmin, xmax), qbmv.y); });
+                list_add_batch(P, m, n, m.sm.stencil, 2, bx, by, bw, bh, mode);
             }
-            if (n2) list_add_batch(P, m, n, q2, n2, bx, by, bw, bh, mode);
         } else {
-            int2 q9[9];
-            for (int i = 0; i < 9; ++i)
-                q9[i] = make_int2(iclamp(half_best.x + i % 3 - 1, xmin, xmax), iclamp(half_best.y + i / 3 - 1, ymin, ymax));
-            list_add_batch(P, m, n, q9, 9, bx, by, bw, bh, mode);
+            const int2 hbv = half_best;
+            put_stencil(m, 9, [&](int i) {
+                return make_int2(iclamp(hbv.x + i % 3 - 1, xmin, xmax), iclamp(hbv.y + i / 3 - 1, ymin, ymax));
+            });
+            list_add_batch(P, m, n, m.sm.stencil, 9, bx, by, bw, bh, mode);
         }
     }
     // sort by (sad, tie_less), keep 8 / 4 (:3445-3456)
@@ -960,39 +1053,90 @@ __device__ void carve(WarpMem& s, uint8_t* base, const WinCfg& wc) {
     s.list_satd = (uint64_t*)take(8 * kListCap);
     s.batch_cost = (uint64_t*)take(8 * 32);
     s.keys = (uint64_t*)take(8 * (size_t)wc.keys_cap);
+    s.top = (uint64_t*)take(8 * 8);
     s.list_mv = (int2*)take(8 * kListCap);
     s.batch = (int2*)take(8 * 32);
+    s.stencil = (int2*)take(8 * 16);
     s.list_rate = (uint32_t*)take(4 * kListCap);
+    s.cur2 = (uint32_t*)take(4 * 32);
+    s.cur4 = (uint32_t*)take(4 * 16);
     s.misc = (int*)take(4 * 16);
     s.seen = (uint32_t*)take(4 * (size_t)wc.seen_words);
     s.seen_full = (uint32_t*)take(4 * (size_t)wc.seen_words);
     s.cur = take(256);
-    s.win = take((size_t)wc.ww * wc.ww);
+    s.win = take((size_t)wc.wp * wc.wh + 32);
 }
 
 __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
     auto r = [](int b) { return (b + 15) & ~15; };
-    return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(8 * kListCap) + r(8 * 32) +
-           r(4 * kListCap) + r(64) + 2 * r(4 * wc.seen_words) + r(256) + r(wc.ww * wc.ww);
+    return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(64) + r(8 * kListCap) +
+           r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + 2 * r(4 * wc.seen_words) + r(256) +
+           r(wc.wp * wc.wh + 32);
 }
 
 int warp_bytes_for_host(const WinCfg& wc) { return warp_bytes_for(wc); }
 
-__device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int cdx, int cdy, int rw) {
-    m.ww = 16 + 2 * rw + 3;
-    m.wx0 = m.x0 + cdx - rw - 1;
-    m.wy0 = m.y0 + cdy - rw - 1;
-    for (int r = 0; r < m.ww; ++r) {
-        const uint8_t* row = ref.y + (size_t)iclamp(m.wy0 + r, 0, P.H - 1) * ref.pitch_y;
-        uint8_t* dst = m.sm.win + r * m.ww;
-        for (int c = m.lane; c < m.ww; c += 32) dst[c] = __ldg(row + iclamp(m.wx0 + c, 0, P.W - 1));
+// Stages the reference window around MV (cdx, cdy) integer pixels: rows wy0 .. wy0+wh-1,
+// columns from the 16-byte-aligned wx0, as 128-bit loads (edge chunks clamp per byte).
+__device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int cdx, int cdy, const WinCfg& wc) {
+    m.wh = wc.wh;
+    m.wp = wc.wp;
+    m.wx0 = (m.x0 + cdx - wc.rw - 1) & ~15;
+    m.wy0 = m.y0 + cdy - wc.rw - 1;
+    const int cpr = m.wp >> 4;
+    const int total = m.wh * cpr;
+#pragma unroll 4
+    for (int j = m.lane; j < total; j += 32) {
+        const int r = j / cpr, c = j - r * cpr;
+        const int gy = iclamp(m.wy0 + r, 0, P.H - 1), gx = m.wx0 + 16 * c;
+        const uint8_t* row = ref.y + (size_t)gy * ref.pitch_y;
+        uint4 v;
+        if (gx >= 0 && gx + 16 <= P.W) {
+            v = __ldg(reinterpret_cast<const uint4*>(row + gx));
+        } else {
+            uint32_t w[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t x = 0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) x |= (uint32_t)__ldg(row + iclamp(gx + 4 * k + i, 0, P.W - 1)) << (8 * i);
+                w[k] = x;
+            }
+            v = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        *reinterpret_cast<uint4*>(m.sm.win + r * m.wp + 16 * c) = v;
     }
     __syncwarp();
 }
 
-// order[j] = raster index of the j-th macroblock in wavefront order (t = x + 2y, then y):
-// every dependency of an MB (left, top-left, top, top-right) has a smaller t, and the MBs
-// of one t are mutually independent, so consecutive queue items can run concurrently.
+// Current MB into shared memory (zero outside the raster) plus its packed column subsets.
+__device__ void load_cur(const DevParams& P, Mb& m, const DevFrame& cur) {
+    if (m.aw == 16) {
+        if (m.lane < 16) {
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (m.lane < m.ah) v = __ldg(reinterpret_cast<const uint4*>(cur.y + (size_t)(m.y0 + m.lane) * cur.pitch_y + m.x0));
+            *reinterpret_cast<uint4*>(m.sm.cur + 16 * m.lane) = v;
+        }
+    } else {
+        for (int i = m.lane; i < 256; i += 32) {
+            const int y = i >> 4, x = i & 15;
+            m.sm.cur[i] = (x < m.aw && y < m.ah) ? __ldg(cur.y + (size_t)(m.y0 + y) * cur.pitch_y + m.x0 + x) : 0;
+        }
+    }
+    __syncwarp();
+    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur);
+    {
+        const int row = m.lane >> 1, k = m.lane & 1;
+        m.sm.cur2[row * 2 + k] = __byte_perm(c32[row * 4 + 2 * k], c32[row * 4 + 2 * k + 1], 0x6420);
+    }
+    if (m.lane < 16) {
+        const int row = m.lane;
+        m.sm.cur4[row] = __byte_perm(__byte_perm(c32[row * 4 + 0], c32[row * 4 + 1], 0x0040),
+                                     __byte_perm(c32[row * 4 + 2], c32[row * 4 + 3], 0x0040), 0x5410);
+    }
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes,
                                                           int npass, const int* order, WinCfg wc, uint32_t epoch,
                                                           LaunchStatus* st) {
@@ -1032,16 +1176,11 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
         __syncwarp();
         if (ok) {
-            // current MB into shared memory (zero outside the raster)
-            for (int i = m.lane; i < 256; i += 32) {
-                const int y = i >> 4, x = i & 15;
-                m.sm.cur[i] = (x < m.aw && y < m.ah) ? __ldg(d.cur.y + (size_t)(m.y0 + y) * d.cur.pitch_y + m.x0 + x) : 0;
-            }
-            __syncwarp();
+            load_cur(P, m, d.cur);
         }
         if (ok && P.range == 0) {
             // --search-range 0 is a real no-search mode (encoder_motion.cpp:72-85)
-            m.ww = 0;
+            m.wp = m.wh = 0;
             m.wx0 = m.wy0 = 0;
             const uint64_t z = mb_sad(P, m, 0, 0, 1);
             if (m.lane == 0) {
@@ -1078,13 +1217,13 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                 const Bounds qb = bounds_qpel(range);
                 seed.x = iclamp(seed.x, qb.xmin, qb.xmax);
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
-                load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc.rw);
+                load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
                 one = refine_staged(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, rate_pi, true, UINT64_MAX);
                 dl = d.seed_dl[m.pos];
                 dc = d.seed_dc[m.pos];
                 dd = d.seed_dd[m.pos];
             } else {
-                load_window(P, m, d.ref, 0, 0, wc.rw);
+                load_window(P, m, d.ref, 0, 0, wc);
                 const PInfo pi = predictor_info(P, o, m.mx, m.my);
                 const int gdx = o.global[0], gdy = o.global[1];
                 const IntRes im = P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)

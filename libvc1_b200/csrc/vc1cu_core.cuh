@@ -55,7 +55,8 @@ struct PassDesc {
 // Shared-memory window geometry for one launch.
 struct WinCfg {
     int rw;        // window radius in integer pixels around its centre MV
-    int ww;        // window side = 16 + 2*rw + 3
+    int wh;        // window height = 16 + 2*rw + 3
+    int wp;        // window row pitch = width: wh + 15 rounded up to 16 (16-byte-aligned origin)
     int seen_r;    // radius of the first-visit bitsets (0 = none)
     int seen_words;
     int keys_cap;  // capacity of the per-stage key array

@@ -58,8 +58,8 @@ __device__ __forceinline__ void predict_row(const S& s, bool bilinear, int rnd, 
         return;
     }
     if (hm && vm) {
-        const int shift_value[4] = {0, 5, 1, 5};
-        const int shift = (shift_value[hm] + shift_value[vm]) >> 1;
+        // shift_value {0,5,1,5}[m] of the reference (:375) is 1 for half-pel, 5 for quarter-pel
+        const int shift = ((hm == 2 ? 1 : 5) + (vm == 2 ? 1 : 5)) >> 1;
         const int r1 = (1 << (shift - 1)) + (rnd ? 1 : 0) - 1;
         int t[N + 3];
 #pragma unroll
