@@ -136,9 +136,12 @@ class Runner:
 
     def step(self):
         c, pics = self.ctx, self.pics
-        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)])
-        c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
-                                for m in self.modes])
+        # launch 1: every picture's quarter-pel seed pass and its three seeded mode passes;
+        # each seeded pass follows its seed pass's wavefront inside the same launch
+        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)] +
+                      [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
+                       for m in self.modes])
+        # launch 2: the final pass (after the host's mode decision over whole passes)
         c.core_passes(self.p0, [(t, r, self.MIXED, 1, 2000 + 4 * i + self.MIXED, 3000 + i, pq)
                                 for i, (t, r, pq) in enumerate(pics)])
         for i, (t, r, pq) in enumerate(pics):

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -23,7 +24,7 @@
 namespace vc1cu {
 // kernels and drivers of the other translation units
 __global__ void core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass,
-                                 const int* order, WinCfg wc, uint32_t epoch, LaunchStatus* st);
+                                 const uint32_t* items, unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st);
 __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
@@ -145,9 +146,8 @@ struct vc1cu_ctx {
     std::vector<Timed> pending;
     std::vector<cudaEvent_t> event_pool;
     vc1cu_timing tsum{};
-    // wavefront order of the current macroblock raster
-    int* d_order = nullptr;
-    int order_mbw = 0, order_mbh = 0;
+    // work-queue tables per launch shape (raster, pass levels)
+    std::map<std::vector<int>, std::pair<uint32_t*, unsigned>> items;
 };
 
 namespace {
@@ -253,25 +253,42 @@ void set_lambda(PassDesc& d, int pq) {
     d.lam_s = 53 - e;
 }
 
-// Wavefront order of an mbw x mbh raster: sorted by t = x + 2y, then by y.
-const int* wavefront_order(vc1cu_ctx* c, int mbw, int mbh) {
-    if (c->d_order && c->order_mbw == mbw && c->order_mbh == mbh) return c->d_order;
-    std::vector<int> o;
-    o.reserve((size_t)mbw * mbh);
+// Work-queue table of a launch: (pass << 20) | macroblock. Inside a pass the macroblocks
+// follow the wavefront order (t = x + 2y, then y); a pass at seed level L (seeded by a pass
+// of the same launch at level L-1) is delayed by L * lag positions, so each item follows all
+// of its dependencies. Cached per (raster, pass levels).
+const uint32_t* work_items(vc1cu_ctx* c, int mbw, int mbh, const std::vector<int>& level, unsigned& nitems) {
+    std::vector<int> key = {mbw, mbh};
+    key.insert(key.end(), level.begin(), level.end());
+    auto it = c->items.find(key);
+    if (it != c->items.end()) {
+        nitems = it->second.second;
+        return it->second.first;
+    }
+    std::vector<int> order;
+    order.reserve((size_t)mbw * mbh);
     for (int t = 0; t <= (mbw - 1) + 2 * (mbh - 1); ++t)
         for (int y = 0; y < mbh; ++y) {
             const int x = t - 2 * y;
-            if (x >= 0 && x < mbw) o.push_back(y * mbw + x);
+            if (x >= 0 && x < mbw) order.push_back(y * mbw + x);
         }
-    if (c->d_order) cudaFree(c->d_order);
-    c->d_order = nullptr;
+    const int mbs = mbw * mbh, n = (int)level.size();
+    const int lag = mbw;  // about two wavefront steps of the raster
+    int maxl = 0;
+    for (int l : level) maxl = std::max(maxl, l);
+    std::vector<uint32_t> items;
+    items.reserve((size_t)n * mbs);
+    for (long sstep = 0; sstep < (long)mbs + (long)lag * maxl; ++sstep)
+        for (int p = 0; p < n; ++p) {
+            const long j = sstep - (long)lag * level[p];
+            if (j >= 0 && j < mbs) items.push_back(((uint32_t)p << 20) | (uint32_t)order[j]);
+        }
     void* d = nullptr;
-    ck(cudaMalloc(&d, sizeof(int) * o.size()), "cudaMalloc(order)");
-    c->d_order = static_cast<int*>(d);
-    ck(cudaMemcpy(c->d_order, o.data(), sizeof(int) * o.size(), cudaMemcpyHostToDevice), "cudaMemcpy(order)");
-    c->order_mbw = mbw;
-    c->order_mbh = mbh;
-    return c->d_order;
+    ck(cudaMalloc(&d, items.size() * sizeof(uint32_t)), "cudaMalloc(work items)");
+    ck(cudaMemcpy(d, items.data(), items.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "cudaMemcpy(work items)");
+    nitems = (unsigned)items.size();
+    c->items[key] = {static_cast<uint32_t*>(d), nitems};
+    return static_cast<uint32_t*>(d);
 }
 
 int stage_max(int R) {
@@ -499,12 +516,17 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         if (q.pqindex < 0 || q.pqindex > 31) throw Fail{VC1CU_ERR_ARG, "pass pqindex must be 0 (params) or 1..31"};
         set_lambda(d, q.pqindex ? q.pqindex : P.pq);
         d.seeded = q.seed_slot >= 0;
-        if (d.seeded) {
+        d.seed_pass = -1;
+        for (int j = 0; j < n; ++j)
+            if (q.seed_slot >= 0 && passes[j].out_slot == q.seed_slot) d.seed_pass = j;
+        if (d.seeded && d.seed_pass < 0) {
             ResultSlot& s = result_slot(c, q.seed_slot, mbs, false);
             d.seed_mvs = s.r.mvs;
             d.seed_dl = s.r.dl;
             d.seed_dc = s.r.dc;
             d.seed_dd = s.r.dd;
+        } else if (d.seeded) {
+            d.seed_mvs = nullptr;  // bound to the seeding pass's result below
         } else {
             if (P.range > P.local_range)
                 throw Fail{VC1CU_ERR_UNSUPPORTED,
@@ -521,9 +543,23 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
             if (passes[j].out_slot == passes[i].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
         h[i].out = result_slot(c, passes[i].out_slot, mbs, true).r;
     }
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j)
-            if (passes[i].seed_slot == passes[j].out_slot) throw Fail{VC1CU_ERR_ARG, "a pass seeds from a pass of the same batch"};
+    // seed levels of in-launch seeds (a chain, never a cycle)
+    std::vector<int> level(n, 0);
+    for (int i = 0; i < n; ++i) {
+        int l = 0, j = i;
+        while (h[j].seed_pass >= 0) {
+            j = h[j].seed_pass;
+            if (++l > n) throw Fail{VC1CU_ERR_ARG, "passes of one launch seed each other in a cycle"};
+        }
+        level[i] = l;
+        if (h[i].seed_pass >= 0) {
+            const DevResult& so = h[h[i].seed_pass].out;
+            h[i].seed_mvs = so.mvs;
+            h[i].seed_dl = so.dl;
+            h[i].seed_dc = so.dc;
+            h[i].seed_dd = so.dd;
+        }
+    }
     // global translation search of the unseeded passes (none at --search-range 0)
     if (!unseeded.empty() && P.range == 0)
         for (int k : unseeded) {
@@ -606,8 +642,10 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
     {
         Timer tm(c, kCore);
-        const int* order = wavefront_order(c, P.mbw, P.mbh);
-        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, order, wc, c->epoch, c->d_status);
+        unsigned nitems = 0;
+        const uint32_t* items = work_items(c, P.mbw, P.mbh, level, nitems);
+        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, items, nitems, wc, c->epoch,
+                                                               c->d_status);
         ck(cudaGetLastError(), "core_pass_kernel launch");
         tm.stop(1);
     }
@@ -738,7 +776,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_passes) cudaFree(c->d_passes);
     if (c->d_gstates) cudaFree(c->d_gstates);
     if (c->d_scratch) cudaFree(c->d_scratch);
-    if (c->d_order) cudaFree(c->d_order);
+    for (auto& kv : c->items) cudaFree(kv.second.first);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->staging_done) cudaEventDestroy(c->staging_done);
     for (auto& t : c->pending) {

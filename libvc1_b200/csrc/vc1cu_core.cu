@@ -44,6 +44,10 @@ struct WarpMem {
     uint32_t* cur2;        // current MB, even columns packed 4 per word: [row][2]
     uint32_t* cur4;        // current MB, every 4th column packed: [row]
     int* misc;             // small scalars: [0] top count, [1] compaction count
+    int2* cur_bmv;         // the current MB's four block MVs while it is searched
+    int2* nb_mv;           // 1-MV field of the left, top-left, top, top-right neighbours
+    int2* nb_bmv;          // their block MVs [4][4]
+    int* nb_intra;         // their P-intra flags
 };
 
 struct Mb {
@@ -687,13 +691,35 @@ __device__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, in
     return RefineOut{best, cost};
 }
 
-// Vc1Encoder::refine_motion_block_staged (me_quality RATE / SATD), encoder_motion.cpp:3271-3535
-__device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
-                                   int mode, const PInfo& pi, bool more, uint64_t known) {
+// The SAD shortlist of one staged refinement, kept in the warp's shared memory between the
+// neighbour-independent half (candidate discovery, SAD, sort, and for me_quality SATD the
+// SATD of every shortlisted vector) and the half that needs the MV predictor (rate term,
+// score, SAD envelope, final order).
+struct Shortlist {
+    int direct;        // 1: the refinement needs no predictor; the result is `out`
+    int nk;            // shortlisted candidates in m.sm.batch / batch_cost [0, nk)
+    int satd_done;     // m.sm.list_satd[i] holds the SATD of shortlist entry i
+    uint64_t screen;   // best SAD discovered (best_sad of the reference)
+    RefineOut out;
+};
+
+// Vc1Encoder::refine_motion_block_staged up to the rate term (encoder_motion.cpp:3271-3456).
+__device__ Shortlist refine_prepare(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
+                                    int mode, uint64_t known, bool satd_all) {
+    Shortlist sl;
+    sl.direct = 1;
+    sl.nk = 0;
+    sl.satd_done = 0;
+    sl.screen = 0;
     const int limit_q = 4 * P.subpel_range;
-    if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q)
-        return refine_integer_only(P, m, bx, by, bw, bh, seed, range, mode, known);
-    if (P.me_quality == 0) return refine_sad_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+    if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q) {
+        sl.out = refine_integer_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+        return sl;
+    }
+    if (P.me_quality == 0) {
+        sl.out = refine_sad_only(P, m, bx, by, bw, bh, seed, range, mode, known);
+        return sl;
+    }
     const Bounds qb = bounds_qpel(range);
     const int xmin = imax(qb.xmin, -limit_q), xmax = imin(qb.xmax, limit_q);
     const int ymin = imax(qb.ymin, -limit_q), ymax = imin(qb.ymax, limit_q);
@@ -821,6 +847,25 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
         m.sm.batch_cost[rank] = my_sad;
     }
     __syncwarp();
+    sl.direct = 0;
+    sl.nk = nk;
+    sl.screen = screen;
+    sl.out = RefineOut{make_int2(0, 0), screen};
+    if (satd_all && P.me_quality != 1) {
+        // SATD of every shortlisted vector; the eligible subset is chosen after the rate
+        // term, and an eligible vector's SATD does not depend on which others are eligible
+        satd_batch(P, m, m.sm.batch, nk, bx, by, bw, bh, mode, m.sm.list_satd);
+        sl.satd_done = 1;
+    }
+    return sl;
+}
+
+// The rest of refine_motion_block_staged (encoder_motion.cpp:3458-3535) given the predictor.
+__device__ RefineOut refine_select(const DevParams& P, const Mb& m, const Shortlist& sl, int bx, int by, int bw, int bh,
+                                   int mode, const PInfo& pi, bool more) {
+    if (sl.direct) return sl.out;
+    const int nk = sl.nk;
+    const uint64_t screen = sl.screen;
     // rate + score (:3458-3476)
     if (m.lane < nk) {
         const int2 mv = m.sm.batch[m.lane];
@@ -847,18 +892,20 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
     const uint64_t pct3 = (rws / 100) * 3 + (((rws % 100) * 3 + 99) / 100);
     const uint64_t slack = pct3 > 4 ? pct3 : 4;
     const uint64_t limit = rws > UINT64_MAX - slack ? UINT64_MAX : rws + slack;
-    // SATD of the eligible shortlist (:3507-3524)
-    int2* el = m.sm.batch + 16;
-    int ne = 0;
-    for (int i = 0; i < nk; ++i) {
-        const uint64_t s = m.sm.batch_cost[i];
-        if (s < UINT64_MAX / 8 && s <= limit) {
-            if (m.lane == 0) el[ne] = m.sm.batch[i];
-            ++ne;
+    // SATD of the eligible shortlist (:3507-3524), unless already known for every entry
+    if (!sl.satd_done) {
+        int2* el = m.sm.batch + 16;
+        int ne = 0;
+        for (int i = 0; i < nk; ++i) {
+            const uint64_t s = m.sm.batch_cost[i];
+            if (s < UINT64_MAX / 8 && s <= limit) {
+                if (m.lane == 0) el[ne] = m.sm.batch[i];
+                ++ne;
+            }
         }
+        __syncwarp();
+        satd_batch(P, m, el, ne, bx, by, bw, bh, mode, m.sm.list_satd + 8);
     }
-    __syncwarp();
-    satd_batch(P, m, el, ne, bx, by, bw, bh, mode, m.sm.list_satd);
     // final order (:3526-3531): eligible first, score, satd, sad, tie
     int best = -1, ei = 0;
     unsigned __int128 bkey = 0;
@@ -866,7 +913,7 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
     for (int i = 0; i < nk; ++i) {
         const uint64_t s = m.sm.batch_cost[i];
         const bool elig = s < UINT64_MAX / 8 && s <= limit;
-        const uint64_t satd = elig ? m.sm.list_satd[ei++] : kBad;
+        const uint64_t satd = elig ? (sl.satd_done ? m.sm.list_satd[i] : m.sm.list_satd[8 + ei++]) : kBad;
         const unsigned __int128 k = score_key(P, m.lam_m, m.lam_s, satd, m.sm.list_rate[i]);
         bool better;
         if (best < 0) better = true;
@@ -890,22 +937,38 @@ __device__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int 
     return RefineOut{res, screen};
 }
 
-// ---- predictor state of the current pass --------------------------------------------------
+__device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
+                                                   int range, int mode, const PInfo& pi, bool more, uint64_t known) {
+    const Shortlist sl = refine_prepare(P, m, bx, by, bw, bh, seed, range, mode, known, false);
+    return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
+}
 
-__device__ __forceinline__ int2 ld_mv(const int2* p) {
-    const int2 v = __ldcg(p);
-    return v;
+// ---- predictor state of the current pass --------------------------------------------------
+//
+// Every predictor of the reference reads only the left, top-left, top and top-right
+// macroblocks and the current one (encoder_motion.cpp:1312-1466). Their state is fetched
+// into shared memory once, after the wavefront wait, with one load per lane.
+
+__device__ void load_neighbours(const DevParams& P, const Mb& m, const DevResult& o) {
+    const int q = m.lane < 16 ? (m.lane >> 2) : (m.lane & 3);
+    const int nx = m.mx + (q == 0 || q == 1 ? -1 : (q == 2 ? 0 : 1)), ny = m.my - (q == 0 ? 0 : 1);
+    const bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
+    const int nb = ny * P.mbw + nx;
+    if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&o.bmv[nb * 4 + (m.lane & 3)]) : make_int2(0, 0);
+    else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&o.mvs[nb]) : make_int2(0, 0);
+    else if (m.lane < 24) m.sm.nb_intra[q] = valid ? (int)__ldcg(&o.intra[nb]) : 0;
+    __syncwarp();
 }
 
 // Vc1Encoder::predictor_info, encoder_motion.cpp:1312-1352 (reads the pass's 1-MV field)
-__device__ PInfo predictor_info(const DevParams& P, const DevResult& o, int mx, int my) {
+__device__ PInfo predictor_info(const DevParams& P, const Mb& m) {
     PInfo r;
-    const int mbw = P.mbw;
+    const int mbw = P.mbw, mx = m.mx, my = m.my;
     int2 A = make_int2(0, 0), B = A, C = A;
     const bool a_valid = my > 0, c_valid = mx > 0, b_valid = my > 0 && mbw > 1;
-    if (a_valid) A = ld_mv(&o.mvs[(my - 1) * mbw + mx]);
-    if (c_valid) C = ld_mv(&o.mvs[my * mbw + mx - 1]);
-    if (b_valid) B = ld_mv(&o.mvs[(my - 1) * mbw + ((mx == mbw - 1) ? mx - 1 : mx + 1)]);
+    if (a_valid) A = m.sm.nb_mv[2];
+    if (c_valid) C = m.sm.nb_mv[0];
+    if (b_valid) B = (mx == mbw - 1) ? m.sm.nb_mv[1] : m.sm.nb_mv[3];
     int2 pre = make_int2(0, 0);
     if (a_valid) pre = A;
     else if (c_valid) pre = C;
@@ -924,23 +987,26 @@ __device__ PInfo predictor_info(const DevParams& P, const DevResult& o, int mx, 
     return r;
 }
 
-// Block-MV field accessor: the current MB's blocks come from shared memory (cur4), the
-// neighbours' from HBM.
+// Block-MV field accessor over the current MB (shared memory) and its prefetched neighbours.
 struct Field {
-    const DevResult* o;
     const int2* cur4;
+    const int2* nb_bmv;
+    const int* nb_intra;
     int mbw, mbh, mx, my;
+    __device__ __forceinline__ int nb_index(int bxm, int bym) const {
+        return bym == my ? 0 : (bxm < mx ? 1 : (bxm == mx ? 2 : 3));
+    }
     __device__ int2 get(int x, int y) const {
         if (x < 0 || y < 0 || x >= mbw * 2 || y >= mbh * 2) return make_int2(0, 0);
-        const int bx = x >> 1, by = y >> 1, k = ((y & 1) << 1) | (x & 1);
-        if (bx == mx && by == my) return cur4[k];
-        return ld_mv(&o->bmv[(by * mbw + bx) * 4 + k]);
+        const int bxm = x >> 1, bym = y >> 1, k = ((y & 1) << 1) | (x & 1);
+        if (bxm == mx && bym == my) return cur4[k];
+        return nb_bmv[nb_index(bxm, bym) * 4 + k];
     }
     __device__ bool intra(int x, int y) const {
         if (x < 0 || y < 0 || x >= mbw * 2 || y >= mbh * 2) return false;
-        const int bx = x >> 1, by = y >> 1;
-        if (bx == mx && by == my) return false;  // the current MB is never intra while it is searched
-        return __ldcg(&o->intra[by * mbw + bx]) != 0;
+        const int bxm = x >> 1, bym = y >> 1;
+        if (bxm == mx && bym == my) return false;  // the current MB is never intra while it is searched
+        return nb_intra[nb_index(bxm, bym)] != 0;
     }
 };
 
@@ -1023,20 +1089,24 @@ __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Waits (bounded) until the MB at (x,y) of the same pass is published. Returns false and
-// raises the launch's abort flag on timeout.
-__device__ bool wait_mb(const DevParams& P, const DevResult& o, int x, int y, uint32_t epoch, LaunchStatus* st) {
-    if (x < 0 || y < 0 || x >= P.mbw) return true;
-    const uint32_t* f = &o.done[y * P.mbw + x];
+// Waits (bounded) until *flag == epoch (a macroblock of this launch was published). On
+// timeout it raises the launch's error and abort flags and returns false.
+__device__ bool wait_flag(const uint32_t* flag, uint32_t epoch, LaunchStatus* st) {
     for (long it = 0; it < (1L << 24); ++it) {
-        if (ld_acquire(f) == epoch) return true;
+        if (ld_acquire(flag) == epoch) return true;
         if (*(volatile int*)&st->abort) return false;
-        __nanosleep(128);
+        __nanosleep(64);
     }
     atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
     atomicExch(&st->abort, 1);
     atomicAdd(&st->timeouts, 1u);
     return false;
+}
+
+// Waits for the MB at (x,y) of the same pass (outside the raster: nothing to wait for).
+__device__ bool wait_mb(const DevParams& P, const DevResult& o, int x, int y, uint32_t epoch, LaunchStatus* st) {
+    if (x < 0 || y < 0 || x >= P.mbw) return true;
+    return wait_flag(&o.done[y * P.mbw + x], epoch, st);
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
@@ -1061,6 +1131,10 @@ __device__ void carve(WarpMem& s, uint8_t* base, const WinCfg& wc) {
     s.cur2 = (uint32_t*)take(4 * 32);
     s.cur4 = (uint32_t*)take(4 * 16);
     s.misc = (int*)take(4 * 16);
+    s.cur_bmv = (int2*)take(8 * 4);
+    s.nb_mv = (int2*)take(8 * 4);
+    s.nb_bmv = (int2*)take(8 * 16);
+    s.nb_intra = (int*)take(4 * 4);
     s.seen = (uint32_t*)take(4 * (size_t)wc.seen_words);
     s.seen_full = (uint32_t*)take(4 * (size_t)wc.seen_words);
     s.cur = take(256);
@@ -1070,7 +1144,8 @@ __device__ void carve(WarpMem& s, uint8_t* base, const WinCfg& wc) {
 __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
     auto r = [](int b) { return (b + 15) & ~15; };
     return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(64) + r(8 * kListCap) +
-           r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + 2 * r(4 * wc.seen_words) + r(256) +
+           r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + r(32) + r(32) + r(128) + r(16) +
+           2 * r(4 * wc.seen_words) + r(256) +
            r(wc.wp * wc.wh + 32);
 }
 
@@ -1137,23 +1212,47 @@ __device__ void load_cur(const DevParams& P, Mb& m, const DevFrame& cur) {
     __syncwarp();
 }
 
+// P-intra proxy of the current MB (encoder_motion.cpp:384-396): sum over its four 8x8
+// blocks of |pixel - visible block mean|. Lane = block k * 8 + row.
+__device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
+    uint32_t part = 0;
+    const int k = m.lane >> 3, row = m.lane & 7;
+    const int bx = (k & 1) * 8, by = ((k >> 1) & 1) * 8;
+    const int vw = imax(0, imin(8, P.W - (m.x0 + bx))), vh = imax(0, imin(8, P.H - (m.y0 + by)));
+    uint32_t rs = 0;
+    if (row < vh)
+        for (int x = 0; x < vw; ++x) rs += m.sm.cur[(by + row) * 16 + bx + x];
+    for (int o2 = 4; o2; o2 >>= 1) rs += __shfl_xor_sync(FULL, rs, o2);
+    const uint32_t nn = (uint32_t)vw * (uint32_t)vh;
+    const int mean = (!vw || !vh) ? 128 : (int)((rs + nn / 2) / nn);  // visible_block_mean (encoder_entropy.cpp:496)
+    if (row < vh)
+        for (int x = 0; x < vw; ++x) part += (uint32_t)iabs((int)m.sm.cur[(by + row) * 16 + bx + x] - mean);
+    return warp_sum_u64(part);
+}
+
+// items[k] = (pass << 20) | macroblock: the launch's work queue. Inside one pass the
+// macroblocks come in wavefront order (t = x + 2y, then y), so every same-pass dependency
+// (left, top-left, top, top-right) of an item precedes it and the items of one t are
+// independent; a pass seeded by another pass of the launch is delayed behind it, so its
+// seed macroblock precedes it too. Items are handed out in order, hence no wait can
+// depend on an item that no running warp holds.
 __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes,
-                                                          int npass, const int* order, WinCfg wc, uint32_t epoch,
-                                                          LaunchStatus* st) {
+                                                          int npass, const uint32_t* items, unsigned nitems, WinCfg wc,
+                                                          uint32_t epoch, LaunchStatus* st) {
     extern __shared__ __align__(16) uint8_t smem[];
     Mb m;
     m.lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     carve(m.sm, smem + (size_t)warp * wc.warp_bytes, wc);
-    const unsigned total = (unsigned)npass * (unsigned)(P.mbw * P.mbh);
     const int range = P.range, local_range = P.local_range;
     for (;;) {
         unsigned item = 0;
         if (m.lane == 0) item = atomicAdd(&st->queue, 1u);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= total) break;
-        const int pi_idx = (int)(item % (unsigned)npass);
-        const int mbi = __ldg(&order[item / (unsigned)npass]);
+        if (item >= nitems) break;
+        const uint32_t code = __ldg(&items[item]);
+        const int pi_idx = (int)(code >> 20);
+        const int mbi = (int)(code & 0xFFFFFu);
         const PassDesc& d = passes[pi_idx];
         m.d = &d;
         m.mx = mbi % P.mbw;
@@ -1167,18 +1266,15 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         m.lam_m = d.lam_m;
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
-        const bool aborted = *(volatile int*)&st->abort;
-        // wavefront: left, top-left, top, top-right of the same pass
-        bool ok = !aborted;
-        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my - 1, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx, m.my - 1, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
-        __syncwarp();
-        if (ok) {
-            load_cur(P, m, d.cur);
-        }
-        if (ok && P.range == 0) {
+        const int mode = d.mode, seeded = d.seeded;
+        const bool allow_intra = d.allow_intra && !P.disable_p_intra;
+        const bool allow_4mv = mode == VC1CU_MV_MIXED;
+        const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
+        bool ok = !*(volatile int*)&st->abort;
+        // a seed produced by another pass of this launch
+        if (ok && d.seed_pass >= 0) ok = wait_flag(&passes[d.seed_pass].out.done[mbi], epoch, st);
+        if (ok) load_cur(P, m, d.cur);
+        if (ok && range == 0) {
             // --search-range 0 is a real no-search mode (encoder_motion.cpp:72-85)
             m.wp = m.wh = 0;
             m.wx0 = m.wy0 = 0;
@@ -1199,33 +1295,48 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             }
             ok = false;
         }
+        // ---- neighbour-independent work: staging, the seeded SAD shortlist, intra proxy ----
+        Shortlist sl;
+        sl.direct = 1;
+        double dl = -1.0, dc = -1.0;
+        uint8_t dd = 0;
+        uint64_t intra_sad = 0;
         if (ok) {
-            const bool allow_4mv = d.mode == VC1CU_MV_MIXED;
-            const int one_mode = allow_4mv ? VC1CU_MV_QPEL : d.mode;
-            __shared__ int2 cur4s[4][4];
-            int2* cur4 = cur4s[warp];
-            if (m.lane < 4) cur4[m.lane] = make_int2(0, 0);
-            __syncwarp();
-            Field field{&o, cur4, P.mbw, P.mbh, m.mx, m.my};
-            const PInfo rate_pi = predictor_mixed_1mv(P, field, m.mx, m.my);
-            const uint64_t pixels = (uint64_t)m.aw * (uint64_t)m.ah;
-            RefineOut one;
-            double dl = -1.0, dc = -1.0;
-            uint8_t dd = 0;
-            if (d.seeded) {
-                int2 seed = d.seed_mvs[m.pos];
+            if (seeded) {
+                int2 seed = __ldcg(&d.seed_mvs[m.pos]);
                 const Bounds qb = bounds_qpel(range);
                 seed.x = iclamp(seed.x, qb.xmin, qb.xmax);
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
-                one = refine_staged(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, rate_pi, true, UINT64_MAX);
-                dl = d.seed_dl[m.pos];
-                dc = d.seed_dc[m.pos];
-                dd = d.seed_dd[m.pos];
+                sl = refine_prepare(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
+                dl = __ldcg(&d.seed_dl[m.pos]);
+                dc = __ldcg(&d.seed_dc[m.pos]);
+                dd = __ldcg(&d.seed_dd[m.pos]);
             } else {
                 load_window(P, m, d.ref, 0, 0, wc);
-                const PInfo pi = predictor_info(P, o, m.mx, m.my);
-                const int gdx = o.global[0], gdy = o.global[1];
+            }
+            if (allow_intra) intra_sad = intra_proxy(P, m);
+        }
+        // ---- wavefront: left, top-left, top, top-right of the same pass ----
+        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my - 1, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx, m.my - 1, epoch, st);
+        if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
+        __syncwarp();
+        if (ok) {
+            load_neighbours(P, m, o);
+            int2* cur4 = m.sm.cur_bmv;
+            if (m.lane < 4) cur4[m.lane] = make_int2(0, 0);
+            __syncwarp();
+            Field field{cur4, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
+            const PInfo rate_pi = predictor_mixed_1mv(P, field, m.mx, m.my);
+            const uint64_t pixels = (uint64_t)m.aw * (uint64_t)m.ah;
+            RefineOut one;
+            if (seeded) {
+                one = refine_select(P, m, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+            } else {
+                const PInfo pi = predictor_info(P, m);
+                const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
                 const IntRes im = P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
                                                       : umh(P, m, pi, gdx, gdy, local_range, pixels);
                 if (P.long_range_mode != 2 && pixels) dl = (double)im.cost / (double)pixels;
@@ -1246,6 +1357,7 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             uint64_t chosen = one_sad, temporal_screen = one_sad;
             const double lambda = d.lambda;
             if (allow_4mv) {
+                // progressive Mixed-MV (:250-374, me_quality != RD)
                 if (m.lane < 4) cur4[m.lane] = one.mv;
                 __syncwarp();
                 int2 four[4];
@@ -1259,23 +1371,28 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                 for (int k = 0; k < 4; ++k) {
                     const PInfo pi4 = predictor_4mv(P, field, m.mx, m.my, k);
                     const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
-                    // 10 seeds (:266-283), scored together, chosen in the reference's visit order
-                    int2 sd[11];
-                    sd[0] = wsr(one.mv);
-                    const int2 raw[10] = {one.mv, pi4.pre, {one.mv.x - 8, one.mv.y}, {one.mv.x + 8, one.mv.y},
-                                          {one.mv.x, one.mv.y - 8}, {one.mv.x, one.mv.y + 8}, {one.mv.x - 4, one.mv.y},
-                                          {one.mv.x + 4, one.mv.y}, {one.mv.x, one.mv.y - 4}, {one.mv.x, one.mv.y + 4}};
-                    for (int s = 0; s < 10; ++s)
-                        sd[s + 1] = wsr(make_int2(iclamp(raw[s].x, qb.xmin, qb.xmax), iclamp(raw[s].y, qb.ymin, qb.ymax)));
-                    if (m.lane < 11) m.sm.batch[m.lane] = sd[m.lane];
+                    // slot 0: the within-radius vector `one`; slots 1..10: the reference's ten
+                    // seeds {one, pred, one-+8 x, one-+8 y, one-+4 x, one-+4 y}, clamped
+                    if (m.lane < 11) {
+                        int2 v;
+                        if (m.lane <= 1) v = one.mv;
+                        else if (m.lane == 2) v = pi4.pre;
+                        else {
+                            const int t = m.lane - 3, d4 = t < 4 ? 8 : 4, dir = t & 3;
+                            v = dir == 0 ? make_int2(one.mv.x - d4, one.mv.y) : dir == 1 ? make_int2(one.mv.x + d4, one.mv.y)
+                              : dir == 2 ? make_int2(one.mv.x, one.mv.y - d4) : make_int2(one.mv.x, one.mv.y + d4);
+                        }
+                        if (m.lane > 0) v = make_int2(iclamp(v.x, qb.xmin, qb.xmax), iclamp(v.y, qb.ymin, qb.ymax));
+                        m.sm.batch[m.lane] = wsr(v);
+                    }
                     __syncwarp();
                     sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
-                    int2 best_seed = sd[0];
+                    int2 best_seed = m.sm.batch[0];
                     uint64_t seed_cost = m.sm.batch_cost[0];
-                    for (int s = 1; s <= 10; ++s) {
-                        const int2 v = sd[s];
+                    for (int s2 = 1; s2 <= 10; ++s2) {
+                        const int2 v = m.sm.batch[s2];
                         if (v.x == best_seed.x && v.y == best_seed.y) continue;
-                        const uint64_t c = m.sm.batch_cost[s];
+                        const uint64_t c = m.sm.batch_cost[s2];
                         const int cm = iabs(v.x) + iabs(v.y), bm = iabs(best_seed.x) + iabs(best_seed.y);
                         if (c < seed_cost || (c == seed_cost && cm < bm)) { seed_cost = c; best_seed = v; }
                     }
@@ -1313,24 +1430,8 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             }
             const uint64_t temporal = chosen;
             double ratio = -1.0;
-            if (d.allow_intra && !P.disable_p_intra) {
-                // P-intra proxy (:384-415): lane = 8x8 block k*8 + row
-                uint32_t part = 0;
-                {
-                    const int k = m.lane >> 3, row = m.lane & 7;
-                    const int bx = (k & 1) * 8, by = ((k >> 1) & 1) * 8;
-                    const int vw = imax(0, imin(8, P.W - (m.x0 + bx))), vh = imax(0, imin(8, P.H - (m.y0 + by)));
-                    uint32_t rs = 0;
-                    if (row < vh)
-                        for (int x = 0; x < vw; ++x) rs += m.sm.cur[(by + row) * 16 + bx + x];
-                    // block sum over the 8 lanes of this block
-                    for (int o2 = 4; o2; o2 >>= 1) rs += __shfl_xor_sync(FULL, rs, o2);
-                    const uint32_t nn = (uint32_t)vw * (uint32_t)vh;
-                    const int mean = (!vw || !vh) ? 128 : (int)((rs + nn / 2) / nn);
-                    if (row < vh)
-                        for (int x = 0; x < vw; ++x) part += (uint32_t)iabs((int)m.sm.cur[(by + row) * 16 + bx + x] - mean);
-                }
-                const uint64_t intra_sad = warp_sum_u64(part);
+            if (allow_intra) {
+                // P-intra decision (:396-414)
                 const uint64_t intra_rate = (uint64_t)llround(__dmul_rn(lambda, 72.0));
                 ratio = temporal_screen > 0 ? __ddiv_rn((double)(intra_sad + intra_rate), (double)temporal_screen)
                                             : __longlong_as_double(0x7ff0000000000000ll);

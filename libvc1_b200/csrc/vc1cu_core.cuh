@@ -45,6 +45,7 @@ struct PassDesc {
     uint64_t lam_m;        // lambda = lam_m * 2^-lam_s exactly
     int lam_s;
     int seeded;            // 1: seed fields below are valid
+    int seed_pass;         // index of the seeding pass in the same launch, -1 if produced earlier
     const int2* seed_mvs;
     const double* seed_dl;
     const double* seed_dc;

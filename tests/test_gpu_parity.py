@@ -151,6 +151,27 @@ def test_batched_passes_match_oracle(ctx, oracle):
         assert ctx.read_result(p, 300 + t).equal(ef) == []
 
 
+def test_seeded_passes_in_the_seed_launch_match_oracle(ctx, oracle):
+    """Seed pass and seeded passes in ONE launch (per-MB cross-pass dependency), QP per pass."""
+    clip = synth.generate(322, 242, 4, 21)
+    p = make_params(322, 242, display_width=321, display_height=241, search_range=24, local_search_range=24)
+    for t in range(4):
+        ctx.upload_frame(t, *clip.frame(t))
+    pqs = {1: 4, 2: 9, 3: 13}
+    ctx.core_passes(p, [(t, t - 1, MV_QPEL, 0, -1, 400 + t, pqs[t]) for t in range(1, 4)] +
+                    [(t, t - 1, m, int(m == MV_MIXED), 400 + t, 500 + 10 * t + m, pqs[t]) for t in range(1, 4)
+                     for m in (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED)])
+    for t in range(1, 4):
+        q = make_params(322, 242, display_width=321, display_height=241, search_range=24, local_search_range=24,
+                        pqindex=pqs[t])
+        cur, ref = clip.frame(t), clip.frame(t - 1)
+        e = oracle.analyze_p_core(q, cur, ref, MV_QPEL, False)
+        assert ctx.read_result(p, 400 + t).equal(e) == []
+        for m in (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED):
+            em = oracle.analyze_p_core(q, cur, ref, m, m == MV_MIXED, seed=e.mvs, seed_distant=e)
+            assert ctx.read_result(p, 500 + 10 * t + m).equal(em) == [], (t, m)
+
+
 @pytest.mark.parametrize("pq,nonuniform,halfqp", [(1, 0, 0), (4, 1, 0), (7, 0, 1), (8, 1, 1), (12, 1, 0), (31, 0, 0)])
 def test_prediction_and_transform_match_oracle(ctx, oracle, pq, nonuniform, halfqp):
     clip = synth.generate(322, 242, 2, 4)
