@@ -136,12 +136,12 @@ class Runner:
 
     def step(self):
         c, pics = self.ctx, self.pics
-        # launch 1: every picture's quarter-pel seed pass and its three seeded mode passes;
-        # each seeded pass follows its seed pass's wavefront inside the same launch
-        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)] +
-                      [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
-                       for m in self.modes])
-        # launch 2: the final pass (after the host's mode decision over whole passes)
+        # launch 1: every picture's quarter-pel seed pass (full search window per warp)
+        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)])
+        # launch 2: the three seeded mode passes of every picture (small windows, high occupancy)
+        c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
+                                for m in self.modes])
+        # launch 3: the final pass (after the host's mode decision over whole passes)
         c.core_passes(self.p0, [(t, r, self.MIXED, 1, 2000 + 4 * i + self.MIXED, 3000 + i, pq)
                                 for i, (t, r, pq) in enumerate(pics)])
         for i, (t, r, pq) in enumerate(pics):
@@ -358,6 +358,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # the reference's CPU path runs on rank 0 alone; other ranks exit without work
+        out = run_reference(args, rank, world)
+        if out is not None and rank == 0:
+            print(json.dumps(out), flush=True)
+        return
     if world > 1:
         import datetime
 
@@ -365,13 +371,9 @@ def main():
         import torch.distributed as dist
 
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        if args.impl == "ours":
-            torch.cuda.set_device(local)
-        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=600))
-    if args.impl == "reference":
-        out = run_reference(args, rank, world)
-    else:
-        out = run_ours(args, rank, world, local)
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    out = run_ours(args, rank, world, local)
     if world > 1:
         import torch.distributed as dist
 

@@ -23,8 +23,10 @@
 
 namespace vc1cu {
 // kernels and drivers of the other translation units
-__global__ void core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass,
-                                 const uint32_t* items, unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st);
+const void* core_kernel(int kind);
+cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,
+                        const PassDesc* passes, int npass, const uint32_t* items, unsigned nitems, const WinCfg& wc,
+                        uint32_t epoch, LaunchStatus* st);
 __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
@@ -49,6 +51,10 @@ constexpr int kMaxSlot = 4096;
 constexpr int kInternalOut = kMaxSlot + 1;   // result slot of vc1cu_analyze_p_core
 constexpr int kInternalSeed = kMaxSlot + 2;  // its seed
 constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
+#ifndef VC1CU_SEEDED_MIXED_RW
+#define VC1CU_SEEDED_MIXED_RW 8
+#endif
+constexpr int kSeededMixedRw = VC1CU_SEEDED_MIXED_RW;  // window radius of seeded Mixed-MV launches
 
 struct Status {
     int code;
@@ -617,7 +623,11 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         wc.seen_words = ((2 * P.local_range + 1) * (2 * P.local_range + 1) + 31) / 32;
         wc.keys_cap = stage_max(P.local_range);
     } else {
-        wc.rw = 4;
+        // seeded refinement stays within 3 quarter-pels of the seed; the Mixed-MV block seeds
+        // add up to 8 more and their refinement 3 (samples outside the window read HBM)
+        bool any_mixed = false;
+        for (int i = 0; i < n; ++i) any_mixed |= passes[i].mode == VC1CU_MV_MIXED;
+        wc.rw = any_mixed ? kSeededMixedRw : 4;
         wc.seen_r = 0;
         wc.seen_words = 1;
         wc.keys_cap = 32;
@@ -630,10 +640,11 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     const size_t smem = (size_t)warps * wc.warp_bytes;
     if (smem > (size_t)c->max_smem)
         throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
-    ck(cudaFuncSetAttribute(core_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-       "cudaFuncSetAttribute");
+    const int kind = any_unseeded ? kCoreAny : kCoreSeeded;
+    const void* kern = core_kernel(kind);
+    ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, core_pass_kernel, 32 * warps, smem), "occupancy");
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem), "occupancy");
     per_sm = std::max(per_sm, 1);
     const long items = (long)n * mbs;
     const long need = (items + warps - 1) / warps;
@@ -644,9 +655,9 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         Timer tm(c, kCore);
         unsigned nitems = 0;
         const uint32_t* items = work_items(c, P.mbw, P.mbh, level, nitems);
-        core_pass_kernel<<<grid, 32 * warps, smem, c->stream>>>(P, c->d_passes, n, items, nitems, wc, c->epoch,
-                                                               c->d_status);
-        ck(cudaGetLastError(), "core_pass_kernel launch");
+        ck(launch_core(kind, grid, 32 * warps, smem, c->stream, P, c->d_passes, n, items, nitems, wc, c->epoch,
+                       c->d_status),
+           "core_pass_kernel launch");
         tm.stop(1);
     }
     {

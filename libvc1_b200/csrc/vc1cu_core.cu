@@ -25,29 +25,69 @@ namespace vc1cu {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kListCap = 24;
 
+// Optional per-phase SM-clock accounting of the core kernel, compiled only with
+// -DVC1CU_PHASE_CLOCKS (a profiling build): slot [kind * 16 + phase] accumulates the cycles
+// lane 0 of each warp spent in that phase, kind = seeded + 2 * Mixed-MV.
+#ifdef VC1CU_PHASE_CLOCKS
+__device__ unsigned long long g_phase_clk[64];
+__device__ unsigned long long g_phase_cnt[64];
+#define PHASE_START(kind) long long phase_t = clock64(); const int phase_kind = (kind)
+#define PHASE_MARK(k)                                                                 \
+    do {                                                                              \
+        const long long phase_n = clock64();                                          \
+        if (m.lane == 0) {                                                            \
+            atomicAdd(&g_phase_clk[phase_kind * 16 + (k)], (unsigned long long)(phase_n - phase_t)); \
+            atomicAdd(&g_phase_cnt[phase_kind * 16 + (k)], 1ull);                     \
+        }                                                                             \
+        phase_t = phase_n;                                                            \
+    } while (0)
+#else
+#define PHASE_START(kind)
+#define PHASE_MARK(k)
+#endif
+
+// The kernel's dynamic shared memory. Every per-warp buffer is addressed as an offset from
+// this symbol, so all of its accesses compile to shared-space loads and stores (a pointer
+// kept in a struct would otherwise degrade to generic addressing).
+extern __shared__ __align__(16) uint8_t g_smem[];
+
+template <class T>
+struct SPtr {
+    uint32_t off;
+    __device__ __forceinline__ T* get() const { return reinterpret_cast<T*>(g_smem + off); }
+    __device__ __forceinline__ operator T*() const { return get(); }
+    __device__ __forceinline__ T& operator[](int i) const { return get()[i]; }
+};
+
+struct SpecBlk;
+
 // Per-warp shared-memory carve.
 struct WarpMem {
-    uint8_t* cur;          // 16x16 current MB (zero outside the visible raster)
-    uint8_t* win;          // reference window
-    uint32_t* seen;        // first-visit bitset of the sampled UMH stages
-    uint32_t* seen_full;   // first-visit bitset of the full-resolution stages
-    uint64_t* keys;        // per-stage candidate keys
-    int2* list_mv;         // staged-refinement candidate list
-    uint64_t* list_sad;
-    uint64_t* list_satd;
-    uint32_t* list_rate;
-    unsigned __int128* list_key;
-    int2* batch;           // scratch MV batch
-    uint64_t* batch_cost;
-    int2* stencil;         // sub-pel stencil MVs of the current refinement stage
-    uint64_t* top;         // sorted top-8 keys of the UMH search
-    uint32_t* cur2;        // current MB, even columns packed 4 per word: [row][2]
-    uint32_t* cur4;        // current MB, every 4th column packed: [row]
-    int* misc;             // small scalars: [0] top count, [1] compaction count
-    int2* cur_bmv;         // the current MB's four block MVs while it is searched
-    int2* nb_mv;           // 1-MV field of the left, top-left, top, top-right neighbours
-    int2* nb_bmv;          // their block MVs [4][4]
-    int* nb_intra;         // their P-intra flags
+    SPtr<uint8_t> cur;          // 16x16 current MB (zero outside the visible raster)
+    SPtr<uint8_t> win;          // reference window
+    SPtr<uint32_t> seen;        // first-visit bitset of the sampled UMH stages
+    SPtr<uint32_t> seen_full;   // first-visit bitset of the full-resolution stages
+    SPtr<uint64_t> keys;        // per-stage candidate keys
+    SPtr<int2> list_mv;         // staged-refinement candidate list
+    SPtr<uint64_t> list_sad;
+    SPtr<uint64_t> list_satd;
+    SPtr<uint32_t> list_rate;
+    SPtr<unsigned __int128> list_key;
+    SPtr<int2> batch;           // scratch MV batch
+    SPtr<uint64_t> batch_cost;
+    SPtr<int2> stencil;         // sub-pel stencil MVs of the current refinement stage
+    SPtr<uint64_t> top;         // sorted top-8 keys of the UMH search
+    SPtr<uint32_t> cur2;        // current MB, even columns packed 4 per word: [row][2]
+    SPtr<uint32_t> cur4;        // current MB, every 4th column packed: [row]
+    SPtr<int> misc;             // small scalars: [0] top count, [1] compaction count
+    SPtr<int2> cur_bmv;         // the current MB's four block MVs while it is searched
+    SPtr<int2> nb_mv;           // 1-MV field of the left, top-left, top, top-right neighbours
+    SPtr<int2> nb_bmv;          // their block MVs [4][4]
+    SPtr<int> nb_intra;         // their P-intra flags
+    SPtr<int2> spec_mv;         // shortlists kept across the wavefront wait [5][8]
+    SPtr<uint64_t> spec_cost;   //   slot 0: the 16x16 refinement, slot k + 1: 8x8 block k
+    SPtr<uint64_t> spec_satd;
+    SPtr<SpecBlk> spec_blk;     // [5]
 };
 
 struct Mb {
@@ -80,7 +120,7 @@ __device__ __forceinline__ void win_load16(const uint8_t* p, uint32_t r[4]) {
 template <int STRIDE>
 __device__ __forceinline__ uint32_t sad_packed(const Mb& m, const uint8_t* base) {
     uint32_t acc = 0;
-    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur);
+    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur.get());
 #pragma unroll 4
     for (int y = 0; y < 16; y += STRIDE) {
         uint32_t r[4];
@@ -139,20 +179,50 @@ __device__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int 
 
 // ---- sub-pel SAD / SATD batches (block_sad_motion :2670-2933, block_satd_motion :2960-3042)
 
+// Everything the out-of-line batch scorers read about the current macroblock, by value
+// (shared-memory buffers as byte offsets of g_smem, so the callee keeps shared addressing).
+struct BatchCtx {
+    uint32_t win_off, cur_off;
+    int wp, wx0, wy0, wh;
+    int x0, y0;
+    int lane;
+    const uint8_t* gref;
+    int gpitch;
+};
+
+__device__ __forceinline__ uint32_t soff(const void* p) {
+    return (uint32_t)(reinterpret_cast<const uint8_t*>(p) - g_smem);
+}
+
+__device__ __forceinline__ BatchCtx batch_ctx(const Mb& m) {
+    return BatchCtx{m.sm.win.off, m.sm.cur.off, m.wp, m.wx0, m.wy0, m.wh, m.x0, m.y0, m.lane, m.gref.p, m.gref.pitch};
+}
+
+__device__ __forceinline__ bool ctx_inside(const BatchCtx& c, int xa, int ya, int xb, int yb) {
+    return xa >= c.wx0 && ya >= c.wy0 && xb < c.wx0 + c.wp && yb < c.wy0 + c.wh;
+}
+
 // SAD of n candidates of block (bx,by,bw,bh) (bw,bh in {8,16}) under the CPU law, written
 // to out[]. Each candidate's block is split into 8-pixel row segments over bh*bw/8 lanes.
-__device__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw, int bh,
-                          int mode, uint64_t* out) {
+// One out-of-line copy serves every call site.
+__device__ __noinline__ void sad_batch_core(const DevParams* Pp, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+                                            int bw, int bh, int mode, uint32_t out_off) {
+    const DevParams& P = *Pp;
+    const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
+    uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
+    const uint8_t* win = g_smem + c.win_off;
+    const uint8_t* curb = g_smem + c.cur_off;
+    const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int spr = bw >> 3;
     const int segs = bh * spr;  // 32 (16x16) or 8 (8x8)
     const int per_iter = 32 / segs;
     const int aw = imax(0, imin(bw, P.W - bx)), ah = imax(0, imin(bh, P.H - by));
     const bool bil = mode_bilinear(mode);
     const bool cg = chroma_gate(bx, by, bw, bh);
-    const int cx = bx - m.x0, cy = by - m.y0;
+    const int cx = bx - c.x0, cy = by - c.y0;
     for (int base = 0; base < n; base += per_iter) {
-        const int ci = base + m.lane / segs;
-        const int sidx = m.lane % segs;
+        const int ci = base + c.lane / segs;
+        const int sidx = c.lane % segs;
         const int r = sidx / spr, c0 = (sidx % spr) * 8;
         const bool valid = ci < n;
         const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
@@ -163,14 +233,14 @@ __device__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int 
             if (!bad && r < ah && c0 < aw) {
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
                 int pred[8];
-                if (win_inside(m, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
-                    predict_row<8>(WinSampler{m.sm.win, m.wp, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
+                    predict_row<8>(WinSampler{win, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
                 else
-                    predict_row<8>(m.gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
-                const uint8_t* c = m.sm.cur + (cy + r) * 16 + cx + c0;
+                    predict_row<8>(gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                const uint8_t* cp = curb + (cy + r) * 16 + cx + c0;
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
-                    if (c0 + i < aw) part += (uint32_t)iabs((int)c[i] - pred[i]);
+                    if (c0 + i < aw) part += (uint32_t)iabs((int)cp[i] - pred[i]);
             }
         }
         for (int o = segs >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
@@ -179,17 +249,23 @@ __device__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int 
     __syncwarp();
 }
 
-__device__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw, int bh,
-                           int mode, uint64_t* out) {
+__device__ __noinline__ void satd_batch_core(const DevParams* Pp, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+                                             int bw, int bh, int mode, uint32_t out_off) {
+    const DevParams& P = *Pp;
+    const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
+    uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
+    const uint8_t* win = g_smem + c.win_off;
+    const uint8_t* curb = g_smem + c.cur_off;
+    const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int tpr = bw >> 2;
     const int tiles = tpr * (bh >> 2);  // 16 or 4
     const int per_iter = 32 / tiles;
     const int aw = imax(0, imin(bw, P.W - bx)), ah = imax(0, imin(bh, P.H - by));
     const bool bil = mode_bilinear(mode);
-    const int cx = bx - m.x0, cy = by - m.y0;
+    const int cx = bx - c.x0, cy = by - c.y0;
     for (int base = 0; base < n; base += per_iter) {
-        const int ci = base + m.lane / tiles;
-        const int t = m.lane % tiles;
+        const int ci = base + c.lane / tiles;
+        const int t = c.lane % tiles;
         const int tx = (t % tpr) * 4, ty = (t / tpr) * 4;
         const bool valid = ci < n;
         const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
@@ -198,18 +274,18 @@ __device__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int
         const int tw = imax(0, imin(4, aw - tx)), th = imax(0, imin(4, ah - ty));
         if (valid && !bad && tw && th) {
             const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
-            const bool fast = win_inside(m, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1);
+            const bool fast = ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1);
             int d[16];
 #pragma unroll
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
                 if (fast)
-                    predict_row<4>(WinSampler{m.sm.win, m.wp, m.wx0, m.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                    predict_row<4>(WinSampler{win, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
                 else
-                    predict_row<4>(m.gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                    predict_row<4>(gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
 #pragma unroll
                 for (int xx = 0; xx < 4; ++xx)
-                    d[yy * 4 + xx] = (xx < tw && yy < th) ? (int)m.sm.cur[(cy + ty + yy) * 16 + cx + tx + xx] - pred[xx] : 0;
+                    d[yy * 4 + xx] = (xx < tw && yy < th) ? (int)curb[(cy + ty + yy) * 16 + cx + tx + xx] - pred[xx] : 0;
             }
             part = satd4x4(d);
         }
@@ -217,6 +293,17 @@ __device__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int
         if (valid && t == 0) out[ci] = (!aw || !ah) ? 0 : (bad ? kBad : (uint64_t)part);
     }
     __syncwarp();
+}
+
+// mvs and out point into the warp's shared-memory buffers.
+__device__ __forceinline__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
+                                          int bh, int mode, uint64_t* out) {
+    sad_batch_core(&P, batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
+}
+
+__device__ __forceinline__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
+                                           int bh, int mode, uint64_t* out) {
+    satd_batch_core(&P, batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
 }
 
 // ---- first-visit bitsets ----------------------------------------------------------------
@@ -349,15 +436,15 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
     const uint64_t* top = m.sm.top;
     // predictor seeds (:1843-1850)
     {
-        int2 s[5];
-        int ns = 0;
-        s[ns++] = make_int2(iclamp(round_qpel_to_pixel(pi.pre.x), -range, range),
-                            iclamp(round_qpel_to_pixel(pi.pre.y), -range, range));
-        s[ns++] = make_int2(0, 0);
-        s[ns++] = make_int2(gdx, gdy);
-        if (pi.a_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
-        if (pi.c_valid) s[ns++] = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
-        umh_stage(P, m, ns, range, [&](int i) { return s[i]; });
+        // predictor, zero, global, then A and C where they exist
+        const int2 sp = make_int2(iclamp(round_qpel_to_pixel(pi.pre.x), -range, range),
+                                  iclamp(round_qpel_to_pixel(pi.pre.y), -range, range));
+        const int2 sa = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
+        const int2 sc = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
+        const int ns = 3 + (pi.a_valid ? 1 : 0) + (pi.c_valid ? 1 : 0);
+        umh_stage(P, m, ns, range, [&](int i) {
+            return i == 0 ? sp : i == 1 ? make_int2(0, 0) : i == 2 ? make_int2(gdx, gdy) : (i == 3 && pi.a_valid) ? sa : sc;
+        });
     }
     // 5x5 around best (:1855-1859)
     {
@@ -412,8 +499,8 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
         const uint64_t before = top[0];
         const int ox = key_dx(before), oy = key_dy(before);
         umh_stage(P, m, 6, range, [&](int i) {
-            const int dxs[6] = {-2, 2, -1, 1, -1, 1}, dys[6] = {0, 0, -2, -2, 2, 2};
-            return make_int2(ox + dxs[i], oy + dys[i]);
+            // (-2,0) (2,0) (-1,-2) (1,-2) (-1,2) (1,2)
+            return i < 2 ? make_int2(ox + (i ? 2 : -2), oy) : make_int2(ox + ((i & 1) ? 1 : -1), oy + (i < 4 ? -2 : 2));
         });
         if (key_dx(top[0]) == ox && key_dy(top[0]) == oy) break;
     }
@@ -421,8 +508,8 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
     {
         const int ox = key_dx(top[0]), oy = key_dy(top[0]);
         umh_stage(P, m, 4, range, [&](int i) {
-            const int dxs[4] = {-1, 1, 0, 0}, dys[4] = {0, 0, -1, 1};
-            return make_int2(ox + dxs[i], oy + dys[i]);
+            // (-1,0) (1,0) (0,-1) (0,1)
+            return i < 2 ? make_int2(ox + (i ? 1 : -1), oy) : make_int2(ox, oy + (i == 3 ? 1 : -1));
         });
     }
     // full-resolution finalists (:1929-1952)
@@ -487,16 +574,17 @@ __device__ IntRes umh(const DevParams& P, const Mb& m, const PInfo& pi, int gdx,
 __device__ IntRes diamond(const DevParams& P, const Mb& m, const PInfo& pi, int gdx, int gdy, int range) {
     uint64_t best = int_key(mb_sad(P, m, 0, 0, 1), 0, 0);
     if (key_cost(best) == 0) return IntRes{0, 0, 0};
-    int2 seeds[4];
-    int ns = 0;
-    seeds[ns++] = make_int2(round_qpel_to_pixel(pi.pre.x), round_qpel_to_pixel(pi.pre.y));
-    seeds[ns++] = make_int2(gdx, gdy);
-    if (pi.a_valid) seeds[ns++] = make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y));
-    if (pi.c_valid) seeds[ns++] = make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
+    // predictor, global, then A and C where they exist
+    const int ns = 2 + (pi.a_valid ? 1 : 0) + (pi.c_valid ? 1 : 0);
     {
         uint64_t k = UINT64_MAX;
         if (m.lane < ns) {
-            const int dx = iclamp(seeds[m.lane].x, -range, range), dy = iclamp(seeds[m.lane].y, -range, range);
+            const int l = m.lane;
+            const int2 v = l == 0 ? make_int2(round_qpel_to_pixel(pi.pre.x), round_qpel_to_pixel(pi.pre.y))
+                         : l == 1 ? make_int2(gdx, gdy)
+                         : (l == 2 && pi.a_valid) ? make_int2(round_qpel_to_pixel(pi.a.x), round_qpel_to_pixel(pi.a.y))
+                                                  : make_int2(round_qpel_to_pixel(pi.c.x), round_qpel_to_pixel(pi.c.y));
+            const int dx = iclamp(v.x, -range, range), dy = iclamp(v.y, -range, range);
             k = int_key(mb_sad(P, m, dx, dy, 1), dx, dy);
         }
         k = warp_min_u64(k);
@@ -509,8 +597,8 @@ __device__ IntRes diamond(const DevParams& P, const Mb& m, const PInfo& pi, int 
         const int cx = key_dx(center), cy = key_dy(center);
         uint64_t k = UINT64_MAX;
         if (m.lane < 4) {
-            const int dxs[4] = {-1, 1, 0, 0}, dys[4] = {0, 0, -1, 1};
-            const int dx = cx + dxs[m.lane], dy = cy + dys[m.lane];
+            const int l = m.lane;  // (-1,0) (1,0) (0,-1) (0,1)
+            const int dx = cx + (l < 2 ? (l ? 1 : -1) : 0), dy = cy + (l < 2 ? 0 : (l == 3 ? 1 : -1));
             if (!(dx < -range || dx > range || dy < -range || dy > range) && !(have_prev && dx == px && dy == py))
                 k = int_key(mb_sad(P, m, dx, dy, 1), dx, dy);
         }
@@ -533,11 +621,23 @@ struct RefineOut {
     uint64_t screen_sad;
 };
 
+// A shortlist parked in shared memory while the warp waits on its neighbours, with the
+// 4MV seed it was refined from (slot k + 1 of block k).
+struct SpecBlk {
+    int2 seed;
+    uint64_t seed_cost;
+    int seed_slot, nk, direct, satd_done;
+    uint64_t screen;
+    RefineOut out;
+};
+constexpr int kSpecBlkBytes = 64;
+static_assert(sizeof(SpecBlk) <= kSpecBlkBytes, "SpecBlk layout");
+
 __device__ __forceinline__ int make_even(int v) { return !(v & 1) ? v : (v > 0 ? v - 1 : v + 1); }
 
 // Appends the batch MVs that are not yet in the list (the `add` lambda, :3324-3337), scoring
 // the new ones with the CPU law in one warp-parallel pass.
-__device__ void list_add_batch(const DevParams& P, const Mb& m, int& n, const int2* mvs, int nb, int bx, int by, int bw,
+__device__ __forceinline__ void list_add_batch(const DevParams& P, const Mb& m, int& n, const int2* mvs, int nb, int bx, int by, int bw,
                                int bh, int mode) {
     // dedup on every lane identically (tiny lists)
     int2* nb_mv = m.sm.batch;
@@ -615,7 +715,7 @@ __device__ RefineOut refine_integer_only(const DevParams& P, const Mb& m, int bx
 }
 
 // refine_qpel_block / refine_motion_block (me_quality SAD), encoder_motion.cpp:3596-3749
-__device__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
+__device__ __forceinline__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
                                      int mode, uint64_t known) {
     const int limit_q = 4 * P.subpel_range;
     if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q)
@@ -704,7 +804,7 @@ struct Shortlist {
 };
 
 // Vc1Encoder::refine_motion_block_staged up to the rate term (encoder_motion.cpp:3271-3456).
-__device__ Shortlist refine_prepare(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
+__device__ __forceinline__ Shortlist refine_prepare(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
                                     int mode, uint64_t known, bool satd_all) {
     Shortlist sl;
     sl.direct = 1;
@@ -943,6 +1043,102 @@ __device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb&
     return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
 }
 
+// ---- shortlists parked across the wavefront wait -----------------------------------------
+
+__device__ __forceinline__ void shortlist_save(const Mb& m, int slot, const Shortlist& sl, int2 seed, uint64_t seed_cost,
+                                               int seed_slot) {
+    if (!sl.direct && m.lane < sl.nk) {
+        m.sm.spec_mv[slot * 8 + m.lane] = m.sm.batch[m.lane];
+        m.sm.spec_cost[slot * 8 + m.lane] = m.sm.batch_cost[m.lane];
+        m.sm.spec_satd[slot * 8 + m.lane] = m.sm.list_satd[m.lane];
+    }
+    if (m.lane == 0) {
+        SpecBlk& b = m.sm.spec_blk[slot];
+        b.seed = seed;
+        b.seed_cost = seed_cost;
+        b.seed_slot = seed_slot;
+        b.nk = sl.nk;
+        b.direct = sl.direct;
+        b.satd_done = sl.satd_done;
+        b.screen = sl.screen;
+        b.out = sl.out;
+    }
+    __syncwarp();
+}
+
+// Puts a parked shortlist back into the working buffers refine_select reads.
+__device__ __forceinline__ Shortlist shortlist_restore(const Mb& m, int slot) {
+    const SpecBlk& b = m.sm.spec_blk[slot];
+    Shortlist sl;
+    sl.direct = b.direct;
+    sl.nk = b.nk;
+    sl.satd_done = b.satd_done;
+    sl.screen = b.screen;
+    sl.out = b.out;
+    if (!sl.direct && m.lane < sl.nk) {
+        m.sm.batch[m.lane] = m.sm.spec_mv[slot * 8 + m.lane];
+        m.sm.batch_cost[m.lane] = m.sm.spec_cost[slot * 8 + m.lane];
+        m.sm.list_satd[m.lane] = m.sm.spec_satd[slot * 8 + m.lane];
+    }
+    __syncwarp();
+    return sl;
+}
+
+// ---- Mixed-MV block seeds (encoder_motion.cpp:250-374) -----------------------------------
+
+// The eleven seed slots of one 8x8 block in m.sm.batch[0..10]: slot 0 the within-radius
+// `one`, then the reference's ten seeds {one, pred, one -/+8 x, one -/+8 y, one -/+4 x,
+// one -/+4 y}, clamped to the quarter-pel bounds.
+__device__ __forceinline__ void put_4mv_seeds(const DevParams& P, const Mb& m, int2 one, int2 pred, const Bounds& qb) {
+    const int limit = 4 * P.subpel_range;
+    if (m.lane < 11) {
+        int2 v;
+        if (m.lane <= 1) v = one;
+        else if (m.lane == 2) v = pred;
+        else {
+            const int t = m.lane - 3, d4 = t < 4 ? 8 : 4, dir = t & 3;
+            v = dir == 0 ? make_int2(one.x - d4, one.y) : dir == 1 ? make_int2(one.x + d4, one.y)
+              : dir == 2 ? make_int2(one.x, one.y - d4) : make_int2(one.x, one.y + d4);
+        }
+        if (m.lane > 0) v = make_int2(iclamp(v.x, qb.xmin, qb.xmax), iclamp(v.y, qb.ymin, qb.ymax));
+        if (imax(iabs(v.x), iabs(v.y)) > limit) { v.x = (v.x / 4) * 4; v.y = (v.y / 4) * 4; }
+        m.sm.batch[m.lane] = v;
+    }
+    __syncwarp();
+}
+
+struct SeedPick {
+    int2 v;
+    uint64_t cost;
+    int slot;
+};
+
+__device__ __forceinline__ int l1_norm(int2 v) { return iabs(v.x) + iabs(v.y); }
+
+// The reference's seed choice over the scored slots: the first slot that attains the least
+// (SAD, |mv|_1); with skip_pred the predictor slot 2 takes no part.
+__device__ __forceinline__ SeedPick pick_4mv_seed(const Mb& m, bool skip_pred) {
+    SeedPick b{m.sm.batch[0], m.sm.batch_cost[0], 0};
+    for (int s2 = 1; s2 <= 10; ++s2) {
+        if (skip_pred && s2 == 2) continue;
+        const int2 v = m.sm.batch[s2];
+        if (v.x == b.v.x && v.y == b.v.y) continue;
+        const uint64_t c = m.sm.batch_cost[s2];
+        if (c < b.cost || (c == b.cost && l1_norm(v) < l1_norm(b.v))) b = SeedPick{v, c, s2};
+    }
+    __syncwarp();
+    return b;
+}
+
+// True when slot `slot` holding (v, c) would have been chosen over the pick b.
+__device__ __forceinline__ bool seed_before(int2 v, uint64_t c, int slot, const SeedPick& b) {
+    if (v.x == b.v.x && v.y == b.v.y) return false;
+    if (c != b.cost) return c < b.cost;
+    const int lv = l1_norm(v), lb = l1_norm(b.v);
+    if (lv != lb) return lv < lb;
+    return slot < b.slot;
+}
+
 // ---- predictor state of the current pass --------------------------------------------------
 //
 // Every predictor of the reference reads only the left, top-left, top and top-right
@@ -957,6 +1153,21 @@ __device__ void load_neighbours(const DevParams& P, const Mb& m, const DevResult
     if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&o.bmv[nb * 4 + (m.lane & 3)]) : make_int2(0, 0);
     else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&o.mvs[nb]) : make_int2(0, 0);
     else if (m.lane < 24) m.sm.nb_intra[q] = valid ? (int)__ldcg(&o.intra[nb]) : 0;
+    __syncwarp();
+}
+
+// A stand-in neighbourhood for guessing before the wavefront wait: the seed pass's final
+// 1-MV vectors of the same four neighbours (that pass is complete), no intra neighbours,
+// and a zero current MB.
+__device__ void guess_neighbours(const DevParams& P, const Mb& m, const int2* seed_mvs) {
+    const int q = m.lane < 16 ? (m.lane >> 2) : (m.lane & 3);
+    const int nx = m.mx + (q == 0 || q == 1 ? -1 : (q == 2 ? 0 : 1)), ny = m.my - (q == 0 ? 0 : 1);
+    const bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
+    const int nb = ny * P.mbw + nx;
+    if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&seed_mvs[nb]) : make_int2(0, 0);
+    else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&seed_mvs[nb]) : make_int2(0, 0);
+    else if (m.lane < 24) m.sm.nb_intra[q] = 0;
+    else if (m.lane < 28) m.sm.cur_bmv[m.lane - 24] = make_int2(0, 0);
     __syncwarp();
 }
 
@@ -1111,40 +1322,46 @@ __device__ bool wait_mb(const DevParams& P, const DevResult& o, int x, int y, ui
 
 // ---- the kernel ---------------------------------------------------------------------------
 
-__device__ void carve(WarpMem& s, uint8_t* base, const WinCfg& wc) {
-    uint8_t* p = base;
-    auto take = [&](size_t bytes) {
-        uint8_t* q = p;
-        p += (bytes + 15) & ~size_t(15);
+// Carves one warp's buffers from byte offset `base` of the dynamic shared memory.
+__device__ void carve(WarpMem& s, uint32_t base, const WinCfg& wc) {
+    uint32_t p = base;
+    auto take = [&](uint32_t bytes) {
+        const uint32_t q = p;
+        p += (bytes + 15) & ~15u;
         return q;
     };
-    s.list_key = (unsigned __int128*)take(sizeof(unsigned __int128) * kListCap);
-    s.list_sad = (uint64_t*)take(8 * kListCap);
-    s.list_satd = (uint64_t*)take(8 * kListCap);
-    s.batch_cost = (uint64_t*)take(8 * 32);
-    s.keys = (uint64_t*)take(8 * (size_t)wc.keys_cap);
-    s.top = (uint64_t*)take(8 * 8);
-    s.list_mv = (int2*)take(8 * kListCap);
-    s.batch = (int2*)take(8 * 32);
-    s.stencil = (int2*)take(8 * 16);
-    s.list_rate = (uint32_t*)take(4 * kListCap);
-    s.cur2 = (uint32_t*)take(4 * 32);
-    s.cur4 = (uint32_t*)take(4 * 16);
-    s.misc = (int*)take(4 * 16);
-    s.cur_bmv = (int2*)take(8 * 4);
-    s.nb_mv = (int2*)take(8 * 4);
-    s.nb_bmv = (int2*)take(8 * 16);
-    s.nb_intra = (int*)take(4 * 4);
-    s.seen = (uint32_t*)take(4 * (size_t)wc.seen_words);
-    s.seen_full = (uint32_t*)take(4 * (size_t)wc.seen_words);
-    s.cur = take(256);
-    s.win = take((size_t)wc.wp * wc.wh + 32);
+    s.list_key.off = take(sizeof(unsigned __int128) * kListCap);
+    s.list_sad.off = take(8 * kListCap);
+    s.list_satd.off = take(8 * kListCap);
+    s.batch_cost.off = take(8 * 32);
+    s.keys.off = take(8 * (uint32_t)wc.keys_cap);
+    s.top.off = take(8 * 8);
+    s.list_mv.off = take(8 * kListCap);
+    s.batch.off = take(8 * 32);
+    s.stencil.off = take(8 * 16);
+    s.list_rate.off = take(4 * kListCap);
+    s.cur2.off = take(4 * 32);
+    s.cur4.off = take(4 * 16);
+    s.misc.off = take(4 * 16);
+    s.cur_bmv.off = take(8 * 4);
+    s.nb_mv.off = take(8 * 4);
+    s.nb_bmv.off = take(8 * 16);
+    s.nb_intra.off = take(4 * 4);
+    s.spec_mv.off = take(8 * 40);
+    s.spec_cost.off = take(8 * 40);
+    s.spec_satd.off = take(8 * 40);
+    s.spec_blk.off = take(kSpecBlkBytes * 5);
+    s.seen.off = take(4 * (uint32_t)wc.seen_words);
+    s.seen_full.off = take(4 * (uint32_t)wc.seen_words);
+    s.cur.off = take(256);
+    s.win.off = take((uint32_t)(wc.wp * wc.wh + 32));
 }
 
 __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
     auto r = [](int b) { return (b + 15) & ~15; };
     return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(64) + r(8 * kListCap) +
            r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + r(32) + r(32) + r(128) + r(16) +
+           3 * r(8 * 40) + r(kSpecBlkBytes * 5) +
            2 * r(4 * wc.seen_words) + r(256) +
            r(wc.wp * wc.wh + 32);
 }
@@ -1179,7 +1396,7 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
             }
             v = make_uint4(w[0], w[1], w[2], w[3]);
         }
-        *reinterpret_cast<uint4*>(m.sm.win + r * m.wp + 16 * c) = v;
+        *reinterpret_cast<uint4*>(m.sm.win.get() + r * m.wp + 16 * c) = v;
     }
     __syncwarp();
 }
@@ -1190,7 +1407,7 @@ __device__ void load_cur(const DevParams& P, Mb& m, const DevFrame& cur) {
         if (m.lane < 16) {
             uint4 v = make_uint4(0, 0, 0, 0);
             if (m.lane < m.ah) v = __ldg(reinterpret_cast<const uint4*>(cur.y + (size_t)(m.y0 + m.lane) * cur.pitch_y + m.x0));
-            *reinterpret_cast<uint4*>(m.sm.cur + 16 * m.lane) = v;
+            *reinterpret_cast<uint4*>(m.sm.cur.get() + 16 * m.lane) = v;
         }
     } else {
         for (int i = m.lane; i < 256; i += 32) {
@@ -1199,7 +1416,7 @@ __device__ void load_cur(const DevParams& P, Mb& m, const DevFrame& cur) {
         }
     }
     __syncwarp();
-    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur);
+    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur.get());
     {
         const int row = m.lane >> 1, k = m.lane & 1;
         m.sm.cur2[row * 2 + k] = __byte_perm(c32[row * 4 + 2 * k], c32[row * 4 + 2 * k + 1], 0x6420);
@@ -1236,14 +1453,23 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 // independent; a pass seeded by another pass of the launch is delayed behind it, so its
 // seed macroblock precedes it too. Items are handed out in order, hence no wait can
 // depend on an item that no running warp holds.
-__global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes,
-                                                          int npass, const uint32_t* items, unsigned nitems, WinCfg wc,
-                                                          uint32_t epoch, LaunchStatus* st) {
-    extern __shared__ __align__(16) uint8_t smem[];
+// Two instantiations: kCoreAny runs any mix of passes; kCoreSeeded runs seeded passes only
+// (no integer-search code, so fewer registers and more resident warps). Four warps per
+// block; at most 65536 / (128 * min blocks) registers per thread.
+#ifndef VC1CU_CORE_MIN_BLOCKS
+#define VC1CU_CORE_MIN_BLOCKS 3
+#endif
+#ifndef VC1CU_SEEDED_MIN_BLOCKS
+#define VC1CU_SEEDED_MIN_BLOCKS 4
+#endif
+template <int KIND>
+__global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS : VC1CU_CORE_MIN_BLOCKS)
+    core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
+                     unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
     m.lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    carve(m.sm, smem + (size_t)warp * wc.warp_bytes, wc);
+    carve(m.sm, (uint32_t)(warp * wc.warp_bytes), wc);
     const int range = P.range, local_range = P.local_range;
     for (;;) {
         unsigned item = 0;
@@ -1266,14 +1492,17 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         m.lam_m = d.lam_m;
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
-        const int mode = d.mode, seeded = d.seeded;
+        const int mode = d.mode, seeded = KIND == kCoreSeeded ? 1 : d.seeded;
         const bool allow_intra = d.allow_intra && !P.disable_p_intra;
         const bool allow_4mv = mode == VC1CU_MV_MIXED;
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
+        PHASE_START((seeded ? 1 : 0) + (allow_4mv ? 2 : 0));
         bool ok = !*(volatile int*)&st->abort;
         // a seed produced by another pass of this launch
         if (ok && d.seed_pass >= 0) ok = wait_flag(&passes[d.seed_pass].out.done[mbi], epoch, st);
+        PHASE_MARK(0);
         if (ok) load_cur(P, m, d.cur);
+        PHASE_MARK(1);
         if (ok && range == 0) {
             // --search-range 0 is a real no-search mode (encoder_motion.cpp:72-85)
             m.wp = m.wh = 0;
@@ -1301,6 +1530,10 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         double dl = -1.0, dc = -1.0;
         uint8_t dd = 0;
         uint64_t intra_sad = 0;
+        // Mixed-MV speculation: the 4MV block work for a guessed 1-MV vector runs before the
+        // wait and is kept when the vector chosen after it matches (seeds from earlier launches)
+        const bool spec4 = allow_4mv && seeded && d.seed_pass < 0;
+        int2 one_g = make_int2(0, 0);
         if (ok) {
             if (seeded) {
                 int2 seed = __ldcg(&d.seed_mvs[m.pos]);
@@ -1308,14 +1541,35 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                 seed.x = iclamp(seed.x, qb.xmin, qb.xmax);
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
+                PHASE_MARK(2);
                 sl = refine_prepare(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
+                PHASE_MARK(3);
                 dl = __ldcg(&d.seed_dl[m.pos]);
                 dc = __ldcg(&d.seed_dc[m.pos]);
                 dd = __ldcg(&d.seed_dd[m.pos]);
+                if (spec4) {
+                    guess_neighbours(P, m, d.seed_mvs);
+                    const Field fg{m.sm.cur_bmv, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
+                    const PInfo pig = predictor_mixed_1mv(P, fg, m.mx, m.my);
+                    shortlist_save(m, 0, sl, seed, 0, 0);
+                    one_g = refine_select(P, m, sl, m.x0, m.y0, 16, 16, one_mode, pig, true).mv;
+                    if (hidden_padding(P, m.x0, m.y0, 16, 16, one_g.x, one_g.y, one_mode, true)) one_g = make_int2(0, 0);
+                    for (int k = 0; k < 4; ++k) {
+                        const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
+                        put_4mv_seeds(P, m, one_g, one_g, qb);
+                        sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
+                        const SeedPick b = pick_4mv_seed(m, true);
+                        const Shortlist sk = refine_prepare(P, m, bx, by, 8, 8, b.v, range, VC1CU_MV_MIXED, b.cost, true);
+                        shortlist_save(m, k + 1, sk, b.v, b.cost, b.slot);
+                    }
+                    PHASE_MARK(12);
+                }
             } else {
                 load_window(P, m, d.ref, 0, 0, wc);
+                PHASE_MARK(2);
             }
             if (allow_intra) intra_sad = intra_proxy(P, m);
+            PHASE_MARK(4);
         }
         // ---- wavefront: left, top-left, top, top-right of the same pass ----
         if (ok) ok = wait_mb(P, o, m.mx - 1, m.my, epoch, st);
@@ -1323,6 +1577,7 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
         if (ok) ok = wait_mb(P, o, m.mx, m.my - 1, epoch, st);
         if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
         __syncwarp();
+        PHASE_MARK(5);
         if (ok) {
             load_neighbours(P, m, o);
             int2* cur4 = m.sm.cur_bmv;
@@ -1332,7 +1587,9 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             const PInfo rate_pi = predictor_mixed_1mv(P, field, m.mx, m.my);
             const uint64_t pixels = (uint64_t)m.aw * (uint64_t)m.ah;
             RefineOut one;
+            PHASE_MARK(6);
             if (seeded) {
+                if (spec4) shortlist_restore(m, 0);
                 one = refine_select(P, m, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
             } else {
                 const PInfo pi = predictor_info(P, m);
@@ -1340,9 +1597,11 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                 const IntRes im = P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
                                                       : umh(P, m, pi, gdx, gdy, local_range, pixels);
                 if (P.long_range_mode != 2 && pixels) dl = (double)im.cost / (double)pixels;
+                PHASE_MARK(7);
                 one = refine_staged(P, m, m.x0, m.y0, 16, 16, make_int2(im.dx * 4, im.dy * 4), range, one_mode, rate_pi,
                                     true, im.cost);
             }
+            PHASE_MARK(8);
             if (hidden_padding(P, m.x0, m.y0, 16, 16, one.mv.x, one.mv.y, one_mode, true)) {
                 if (m.lane == 0) m.sm.batch[31] = make_int2(0, 0);
                 __syncwarp();
@@ -1360,46 +1619,43 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                 // progressive Mixed-MV (:250-374, me_quality != RD)
                 if (m.lane < 4) cur4[m.lane] = one.mv;
                 __syncwarp();
-                int2 four[4];
                 uint64_t four_sad = 0, four_screen = 0, extra_bits = 1;
-                const int limit = 4 * P.subpel_range;
-                auto wsr = [&](int2 v) {
-                    if (imax(iabs(v.x), iabs(v.y)) > limit) { v.x = (v.x / 4) * 4; v.y = (v.y / 4) * 4; }
-                    return v;
-                };
                 const Bounds qb = bounds_qpel(range);
+                const bool hit = spec4 && one.mv.x == one_g.x && one.mv.y == one_g.y;
                 for (int k = 0; k < 4; ++k) {
                     const PInfo pi4 = predictor_4mv(P, field, m.mx, m.my, k);
                     const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
-                    // slot 0: the within-radius vector `one`; slots 1..10: the reference's ten
-                    // seeds {one, pred, one-+8 x, one-+8 y, one-+4 x, one-+4 y}, clamped
-                    if (m.lane < 11) {
-                        int2 v;
-                        if (m.lane <= 1) v = one.mv;
-                        else if (m.lane == 2) v = pi4.pre;
-                        else {
-                            const int t = m.lane - 3, d4 = t < 4 ? 8 : 4, dir = t & 3;
-                            v = dir == 0 ? make_int2(one.mv.x - d4, one.mv.y) : dir == 1 ? make_int2(one.mv.x + d4, one.mv.y)
-                              : dir == 2 ? make_int2(one.mv.x, one.mv.y - d4) : make_int2(one.mv.x, one.mv.y + d4);
+                    RefineOut r;
+                    bool have = false;
+                    int2 best_seed;
+                    uint64_t seed_cost;
+                    if (hit) {
+                        // the parked seed search covered every slot but the predictor's
+                        put_4mv_seeds(P, m, one.mv, pi4.pre, qb);
+                        const int2 v2 = m.sm.batch[2];
+                        sad_batch(P, m, m.sm.batch + 2, 1, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost + 2);
+                        const uint64_t c2 = m.sm.batch_cost[2];
+                        const SpecBlk& sb = m.sm.spec_blk[k + 1];
+                        const SeedPick b{sb.seed, sb.seed_cost, sb.seed_slot};
+                        if (seed_before(v2, c2, 2, b)) {
+                            best_seed = v2;
+                            seed_cost = c2;
+                        } else {
+                            const Shortlist sk = shortlist_restore(m, k + 1);
+                            r = refine_select(P, m, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
+                            have = true;
                         }
-                        if (m.lane > 0) v = make_int2(iclamp(v.x, qb.xmin, qb.xmax), iclamp(v.y, qb.ymin, qb.ymax));
-                        m.sm.batch[m.lane] = wsr(v);
+                    } else {
+                        put_4mv_seeds(P, m, one.mv, pi4.pre, qb);
+                        sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
+                        const SeedPick b = pick_4mv_seed(m, false);
+                        best_seed = b.v;
+                        seed_cost = b.cost;
                     }
-                    __syncwarp();
-                    sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
-                    int2 best_seed = m.sm.batch[0];
-                    uint64_t seed_cost = m.sm.batch_cost[0];
-                    for (int s2 = 1; s2 <= 10; ++s2) {
-                        const int2 v = m.sm.batch[s2];
-                        if (v.x == best_seed.x && v.y == best_seed.y) continue;
-                        const uint64_t c = m.sm.batch_cost[s2];
-                        const int cm = iabs(v.x) + iabs(v.y), bm = iabs(best_seed.x) + iabs(best_seed.y);
-                        if (c < seed_cost || (c == seed_cost && cm < bm)) { seed_cost = c; best_seed = v; }
-                    }
-                    __syncwarp();
-                    const RefineOut r = refine_staged(P, m, bx, by, 8, 8, best_seed, range, VC1CU_MV_MIXED, pi4, true, seed_cost);
+                    PHASE_MARK(9);
+                    if (!have) r = refine_staged(P, m, bx, by, 8, 8, best_seed, range, VC1CU_MV_MIXED, pi4, true, seed_cost);
+                    PHASE_MARK(10);
                     four_screen += r.screen_sad;
-                    four[k] = r.mv;
                     if (m.lane == 0) cur4[k] = r.mv;
                     __syncwarp();
                     four_sad += r.screen_sad;
@@ -1411,6 +1667,9 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
                     }
                     if (!(r.mv.x == actual.x && r.mv.y == actual.y)) extra_bits += mv_rate_bits(P, r.mv, actual, VC1CU_MV_MIXED, false);
                 }
+                int2 four[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) four[k] = cur4[k];
                 const int cmx = median4(four[0].x, four[1].x, four[2].x, four[3].x);
                 const int cmy = median4(four[0].y, four[1].y, four[2].y, four[3].y);
                 const bool four_chroma_safe = !hidden_chroma(P, m.x0, m.y0, 16, 16, cmx, cmy);
@@ -1469,7 +1728,24 @@ __global__ void __launch_bounds__(128) core_pass_kernel(const __grid_constant__ 
             st_release(&o.done[m.pos], epoch);
         }
         __syncwarp();
+        PHASE_MARK(11);
     }
+}
+
+// Host-side handles of the two instantiations (attributes, occupancy, launch).
+const void* core_kernel(int kind) {
+    return kind == kCoreSeeded ? reinterpret_cast<const void*>(&core_pass_kernel<kCoreSeeded>)
+                               : reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
+}
+
+cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,
+                        const PassDesc* passes, int npass, const uint32_t* items, unsigned nitems, const WinCfg& wc,
+                        uint32_t epoch, LaunchStatus* st) {
+    if (kind == kCoreSeeded)
+        core_pass_kernel<kCoreSeeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else
+        core_pass_kernel<kCoreAny><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    return cudaGetLastError();
 }
 
 // Picture totals of each pass (encoder_motion.cpp:428-441): integer sums, then the
@@ -1522,3 +1798,17 @@ __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDes
 }
 
 }  // namespace vc1cu
+
+#ifdef VC1CU_PHASE_CLOCKS
+// Profiling build only: copies (and with reset != 0 clears) the phase accumulators.
+extern "C" int vc1cu_phase_clocks(unsigned long long* clk, unsigned long long* cnt, int reset) {
+    if (cudaMemcpyFromSymbol(clk, vc1cu::g_phase_clk, sizeof vc1cu::g_phase_clk) != cudaSuccess) return -1;
+    if (cudaMemcpyFromSymbol(cnt, vc1cu::g_phase_cnt, sizeof vc1cu::g_phase_cnt) != cudaSuccess) return -1;
+    if (reset) {
+        static const unsigned long long z[64] = {};
+        if (cudaMemcpyToSymbol(vc1cu::g_phase_clk, z, sizeof z) != cudaSuccess) return -1;
+        if (cudaMemcpyToSymbol(vc1cu::g_phase_cnt, z, sizeof z) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+#endif

@@ -53,6 +53,10 @@ struct PassDesc {
     DevResult out;
 };
 
+// core_pass_kernel instantiations
+constexpr int kCoreAny = 0;     // any mix of seeded and unseeded passes
+constexpr int kCoreSeeded = 1;  // seeded passes only
+
 // Shared-memory window geometry for one launch.
 struct WinCfg {
     int rw;        // window radius in integer pixels around its centre MV

@@ -1,0 +1,218 @@
+"""Pins the oracle (our C restatement, oracle/vc1_oracle.c) to the reference (CPU only).
+
+1. Golden vectors produced by the reference's own code (tests/golden/*.npz, written by
+   tests/golden/make_golden.py from oracle/_ref) must be reproduced bit-exactly, and the
+   properties the reference's tests assert on the same inputs must hold.
+2. Where oracle/_ref is built in this tree, the oracle is also compared live with it on
+   further seeded inputs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from libvc1_b200 import synth
+from libvc1_b200.abi import BAD_COST, MODES, MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED, MV_QPEL, make_params
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def planes(y, chroma=128):
+    h, w = y.shape
+    u = np.full((h // 2, w // 2), chroma, np.uint8)
+    return (np.ascontiguousarray(y, np.uint8), u, u.copy())
+
+
+def test_runtime_kat(oracle):
+    """tests/vulkan_compute_runtime.cpp:39-98 on the CPU law."""
+    g = load("runtime_kat.npz")
+    cur, ref = planes(g["cur"]), planes(g["ref"])
+    p = make_params(48, 40)
+    assert [oracle.block_sad_motion(p, cur, ref, 5, 7, 16, 16, int(a), int(b), MV_QPEL) for a, b in g["mvs"]] == \
+        g["sad_qpel"].tolist()
+    assert [oracle.block_satd_motion(p, cur, ref, 5, 7, 16, 16, int(a), int(b), MV_QPEL) for a, b in g["mvs"]] == \
+        g["satd_qpel"].tolist()
+    assert [oracle.block_sad_motion(p, cur, ref, 3, 4, 16, 16, int(a), int(b), MV_HPEL_BILINEAR)
+            for a, b in g["half_mvs"]] == g["sad_bilinear"].tolist()
+    for s in (2, 4):
+        got = [oracle.shader_cost(cur, ref, 5, 7, 16, 16, s, 0, 0, 0, int(a), int(b)) for a, b in g["int_mvs"]]
+        assert got == g[f"sad_int_stride{s}"].tolist()
+
+
+def test_staged_kat(oracle):
+    """tests/staged_motion_estimation.cpp:26-39 and :134-147."""
+    g = load("staged_kat.npz")
+    p16 = make_params(16, 16, search_range=8, local_search_range=8)
+    c, f, n = planes(g["cur16"]), planes(g["flat16"]), planes(g["noisy16"])
+    sf = oracle.block_sad_motion(p16, c, f, 0, 0, 16, 16, 0, 0, MV_QPEL)
+    sn = oracle.block_sad_motion(p16, c, n, 0, 0, 16, 16, 0, 0, MV_QPEL)
+    tf = oracle.block_satd_motion(p16, c, f, 0, 0, 16, 16, 0, 0, MV_QPEL)
+    tn = oracle.block_satd_motion(p16, c, n, 0, 0, 16, 16, 0, 0, MV_QPEL)
+    assert (sf, sn, tf, tn) == (int(g["sad_flat"]), int(g["sad_noisy"]), int(g["satd_flat"]), int(g["satd_noisy"]))
+    assert sf == 256 and sn == 256 and tn > tf  # the reference test's own assertions
+    p32 = make_params(32, 32, search_range=8, local_search_range=8)
+    a, b = planes(g["cur32"]), planes(g["ref32"])
+    assert [oracle.block_satd_motion(p32, a, b, 8, 8, 16, 16, int(x), int(y), MV_QPEL) for x, y in g["qgrid"]] == \
+        g["satd_qgrid"].tolist()
+    assert [oracle.block_satd_motion(p32, a, b, 8, 8, 16, 16, int(x), int(y), MV_HPEL_BILINEAR)
+            for x, y in g["bgrid"]] == g["satd_bgrid"].tolist()
+
+
+def _gradient(w, h, horizontal):
+    x = np.arange(w)[None, :].repeat(h, 0)
+    y = np.arange(h)[:, None].repeat(w, 1)
+    return (20 + 3 * (x if horizontal else y)).astype(np.uint8)
+
+
+def test_diamond_kat(oracle):
+    """tests/diamond_motion.cpp:18-60: exact recovery of a translation, cropped-edge legality."""
+    g = load("diamond_kat.npz")
+    for i in range(2):
+        sx, sy, hor = g[f"shift{i}"].tolist()
+        ref = _gradient(64, 48, bool(hor))
+        cur = ref[np.clip(np.arange(48) + sy, 0, 47)][:, np.clip(np.arange(64) + sx, 0, 63)]
+        p = make_params(64, 48, search_range=12, local_search_range=12, me_algorithm=1)
+        got = oracle.integer_motion(p, planes(cur), planes(ref), 1, 1, np.zeros((12, 2), np.int32), 0, 0, 12)
+        assert list(got) == g[f"shift{i}.result"].tolist()
+        assert got == (sx, sy, 0)
+    pe = make_params(64, 48, display_height=42, search_range=8, local_search_range=8, me_algorithm=1)
+    f = planes(_gradient(64, 48, True))
+    s = oracle.mb_sad(pe, f, f, 1, 2, 0, 4, 1)
+    assert s == int(g["edge_mb_sad"]) and s >= (1 << 64) // 8
+
+
+def _frames(g, prefix):
+    return tuple(np.ascontiguousarray(g[f"{prefix}.{c}"]) for c in "yuv")
+
+
+ANALYSIS = {
+    "cif_r8": dict(search_range=8, local_search_range=8),
+    "odd_322x242": dict(display_width=321, display_height=241, search_range=16, local_search_range=16, rnd=1,
+                        pqindex=12, nonuniform=1),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ANALYSIS))
+def test_analysis_chain_golden(oracle, name):
+    """Five analyze_p_picture_core passes of one picture against the reference's outputs."""
+    g = load(f"analysis_{name}.npz")
+    cur, ref = _frames(g, "cur"), _frames(g, "ref")
+    p = make_params(cur[0].shape[1], cur[0].shape[0], **ANALYSIS[name])
+
+    def check(pass_name, a):
+        for field in a.ARRAYS:
+            want = g[f"{pass_name}.{field}"]
+            got = getattr(a, field)
+            if got.dtype == np.float64:
+                assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (pass_name, field)
+            else:
+                assert np.array_equal(got, want), (pass_name, field)
+        for k, v in a.totals.items():
+            w = g[f"{pass_name}.total.{k}"]
+            assert (np.float64(v).view(np.uint64) == w.view(np.uint64)) if w.dtype == np.float64 else int(v) == int(w), \
+                (pass_name, k)
+
+    q = oracle.analyze_p_core(p, cur, ref, MV_QPEL, False)
+    check("qpel", q)
+    for m, pn in ((MV_HPEL, "hpel"), (MV_HPEL_BILINEAR, "bilinear"), (MV_MIXED, "mixed")):
+        a = oracle.analyze_p_core(p, cur, ref, m, False, seed=q.mvs, seed_distant=q)
+        check(pn, a)
+    f = oracle.analyze_p_core(p, cur, ref, MV_MIXED, True, seed=a.mvs, seed_distant=a)
+    check("final", f)
+
+
+def test_xform_golden(oracle):
+    """Prediction, forward transform (all four sizes) and quantiser at four QP settings."""
+    g = load("xform_kat.npz")
+    cur, ref = _frames(g, "cur"), _frames(g, "ref")
+    for pq, nu, hq in ((3, 0, 1), (8, 1, 1), (17, 1, 0), (31, 0, 0)):
+        key = f"pq{pq}_nu{nu}_hq{hq}"
+        p = make_params(64, 48, pqindex=pq, nonuniform=nu, halfqp=hq, search_range=8, local_search_range=8)
+        q = oracle.analyze_p_core(p, cur, ref, MV_QPEL, False)
+        f = oracle.analyze_p_core(p, cur, ref, MV_MIXED, True, seed=q.mvs, seed_distant=q)
+        assert np.array_equal(f.mvs, g[f"{key}.mvs"]) and np.array_equal(f.block_mvs, g[f"{key}.block_mvs"])
+        pred = oracle.motion_compensate(p, ref, f, MV_MIXED)
+        for c, plane in zip("yuv", pred):
+            assert np.array_equal(plane, g[f"{key}.pred.{c}"]), (key, c)
+        co, lv = oracle.forward_quant(p, cur, pred, 15)
+        assert np.array_equal(co.view(np.uint64), g[f"{key}.coeffs"].view(np.uint64)), key
+        assert np.array_equal(lv, g[f"{key}.levels"]), key
+
+
+def test_global_golden(oracle):
+    g = load("global_kat.npz")
+    for i in range(3):
+        cur, ref = planes(g[f"g{i}.cur"]), planes(g[f"g{i}.ref"])
+        rng = int(g[f"g{i}.range"])
+        p = make_params(352, 288, search_range=rng, local_search_range=rng)
+        assert list(oracle.global_motion(p, cur, ref, rng)) == g[f"g{i}.result"].tolist()
+        got = [[oracle.frame_sad(cur, ref, int(dx), int(dy), s) for s in (1, 2, 4)]
+               for dx, dy in g[f"g{i}.frame_sad_offsets"]]
+        assert got == g[f"g{i}.frame_sad"].tolist()
+
+
+def test_synthetic_clip_is_deterministic():
+    a = synth.generate(64, 48, 3, 17)
+    b = synth.generate(64, 48, 3, 17)
+    for t in range(3):
+        for x, y in zip(a.frame(t), b.frame(t)):
+            assert np.array_equal(x, y)
+    c = synth.generate(64, 48, 3, 18)
+    assert not np.array_equal(a.frame(1)[0], c.frame(1)[0])
+
+
+# ---- live comparison with the reference build (skipped where oracle/_ref is absent) ----
+
+def _ref_or_skip():
+    from oracle import ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built in this tree")
+    from oracle import Reference
+
+    return Reference
+
+
+@pytest.mark.parametrize("rnd", [0, 1])
+def test_block_costs_match_reference_live(oracle, rnd):
+    Reference = _ref_or_skip()
+    clip = synth.generate(66, 50, 2, 3)
+    p = make_params(66, 50, display_width=61, display_height=45, search_range=16, local_search_range=16, rnd=rnd)
+    R = Reference(p)
+    cur, ref = clip.frame(1), clip.frame(0)
+    rc, rr = R.frame(cur), R.frame(ref)
+    rng = np.random.default_rng(31 + rnd)
+    for mode in MODES:
+        for (x0, y0, bw, bh) in ((48, 32, 16, 16), (56, 40, 8, 8), (0, 0, 16, 16), (24, 8, 8, 8)):
+            for a, b in rng.integers(-30, 31, (40, 2)):
+                a, b = int(a), int(b)
+                assert oracle.block_sad_motion(p, cur, ref, x0, y0, bw, bh, a, b, mode) == \
+                    R.block_sad_motion(rc, rr, x0, y0, bw, bh, a, b, mode)
+                assert oracle.block_satd_motion(p, cur, ref, x0, y0, bw, bh, a, b, mode) == \
+                    R.block_satd_motion(rc, rr, x0, y0, bw, bh, a, b, mode)
+    costs = [oracle.block_sad_motion(p, cur, ref, 48, 32, 16, 16, a, b, MV_QPEL) for a in range(-24, 25, 3)
+             for b in range(-24, 25, 3)]
+    assert BAD_COST in costs  # the hidden-padding gate is exercised
+
+
+@pytest.mark.parametrize("kw", [dict(search_range=16, local_search_range=16),
+                                dict(search_range=16, local_search_range=16, me_algorithm=1),
+                                dict(search_range=16, local_search_range=16, fast_subpel=1, me_quality=0),
+                                dict(search_range=24, local_search_range=8, pqindex=5, halfqp=1),
+                                dict(search_range=0, local_search_range=0)])
+def test_analysis_matches_reference_live(oracle, kw):
+    Reference = _ref_or_skip()
+    clip = synth.generate(98, 66, 2, 13)
+    p = make_params(98, 66, display_width=97, display_height=65, **kw)
+    R = Reference(p)
+    cur, ref = clip.frame(1), clip.frame(0)
+    rc, rr = R.frame(cur), R.frame(ref)
+    e = R.analyze_p_core(rc, rr, MV_QPEL, False)
+    assert oracle.analyze_p_core(p, cur, ref, MV_QPEL, False).equal(e) == []
+    for mode in (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED):
+        em = R.analyze_p_core(rc, rr, mode, True, seed=e.mvs, seed_distant=e)
+        assert oracle.analyze_p_core(p, cur, ref, mode, True, seed=e.mvs, seed_distant=e).equal(em) == [], mode
