@@ -283,6 +283,43 @@ int vc1cu_forward_quant(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int p
 int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id,
                                int type_mask, double* d_coeffs, int16_t* d_levels);
 
+/* ---- allocation-free whole-frame translation search ------------------------------ */
+
+/*
+ * No counterpart in the reference: an addition of this library for callers that cannot
+ * allocate device memory while they run (an encoder worker bound to a fixed device-memory
+ * budget, or code on a path where cudaMalloc is not allowed because it would synchronise
+ * the device). It needs no context and allocates nothing.
+ *
+ * Runs the whole-frame translation search of an unseeded analysis pass
+ * (Vc1Encoder::global_motion_search, src/encoder_motion.cpp:2025-2141) for n pictures
+ * and writes, per picture i, d_dxdy[2i], d_dxdy[2i+1] (integer pixels) and d_sad[i]
+ * (the full-resolution frame SAD at that offset): the global_dx / global_dy /
+ * global_full_sad that vc1cu_analyze_p_core reports for range =
+ * min(search_range, local_search_range, 32).
+ *
+ * cur_y / ref_y: HOST arrays of n DEVICE pointers to 8-bit luma planes of width x height
+ * with row pitch `pitch` bytes; d_dxdy (2n int32) and d_sad (n uint64) are DEVICE
+ * buffers. stream is a cudaStream_t (NULL: the legacy default stream) of the current
+ * device; the call only enqueues work on it and returns, so results are ready once that
+ * stream has been synchronised.
+ *
+ * Limits: 1 <= n <= 16 pictures per call and 0 <= range <= 32; larger requests are
+ * rejected with VC1CU_ERR_ARG. The search state lives in one fixed device array of
+ * 168,192 bytes that every GPU loading this library holds until the process exits. All
+ * calls on one device share that array: two calls whose GPU work can overlap (issued on
+ * different streams, or from threads that do not order them) race on it and give wrong
+ * results; calls issued in order on one stream are safe, and devices are independent.
+ * Each call resets the state it reads, so nothing carries over from an earlier call.
+ *
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture begins.
+ * On failure a message is written to err (err_len bytes, may be NULL).
+ */
+int vc1cu_global_motion_noalloc(const uint8_t* const* cur_y, const uint8_t* const* ref_y, int pitch,
+                                int width, int height, int range, int n, int32_t* d_dxdy,
+                                uint64_t* d_sad, void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,7 @@ EXPORTS = (
     "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
-    "vc1cu_measure_int32_peak",
+    "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc",
 )
 
 
@@ -260,4 +260,30 @@ class CudaComputeContext:
                                                        d_coeffs, d_levels))
 
 
-__all__ = ["CudaComputeContext", "Vc1cuError", "Pass", "load_library", "EXPORTS", "METRIC_SAD", "METRIC_SATD"]
+def global_motion_noalloc(cur_ptrs, ref_ptrs, pitch: int, width: int, height: int, search_range: int,
+                          d_dxdy: int, d_sad: int, stream: int = 0):
+    """Whole-frame translation search of len(cur_ptrs) pictures without any device allocation.
+
+    For callers that cannot allocate device memory while they run: every pointer is a
+    device address the caller already owns (luma planes, int32[2n] and uint64[n] outputs),
+    and the search state lives in a fixed array inside the library (at most 16 pictures
+    per call, search_range 0..32). Enqueued on `stream` (a cudaStream_t handle); the
+    results are ready once that stream is synchronised. Calls on one device must not
+    overlap on the GPU: they share that array.
+    """
+    L = load_library()
+    n = len(cur_ptrs)
+    cur = (C.c_void_p * max(n, 1))(*cur_ptrs)
+    ref = (C.c_void_p * max(n, 1))(*ref_ptrs)
+    err = C.create_string_buffer(256)
+    L.vc1cu_global_motion_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
+    L.vc1cu_global_motion_noalloc.restype = C.c_int
+    rc = L.vc1cu_global_motion_noalloc(cur, ref, pitch, width, height, search_range, n, d_dxdy, d_sad, stream or None,
+                                       err, 256)
+    if rc:
+        raise Vc1cuError(rc, err.value.decode())
+
+
+__all__ = ["CudaComputeContext", "Vc1cuError", "Pass", "load_library", "EXPORTS", "METRIC_SAD", "METRIC_SATD",
+           "global_motion_noalloc"]

@@ -9,6 +9,9 @@
 // replay of the reference's sequential fold over the precomputed costs.
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <mutex>
+
 #include "vc1cu_core.cuh"
 
 namespace vc1cu {
@@ -353,4 +356,111 @@ void init_gstate(GState* h, const DevFrame& cur, const DevFrame& ref, int range,
     h->phase = 0;
 }
 
+
+// ---- allocation-free form (vc1cu_global_motion_noalloc) ---------------------------------
+//
+// Some callers cannot allocate device memory while they run: an encoder thread working out
+// of a fixed device-memory budget, or code that runs where a cudaMalloc would synchronise
+// the device or is not permitted. For them the search state of up to
+// kNoAllocMaxPictures pictures lives in this fixed array, which every GPU that loads the
+// library holds until the process exits (16 states of 10,512 bytes: 168,192 bytes).
+// Every call shares it.
+constexpr int kNoAllocMaxPictures = 16;
+static __device__ __align__(256) GState g_noalloc_states[kNoAllocMaxPictures];
+static_assert(sizeof(GState) * kNoAllocMaxPictures <= 192 * 1024, "no-alloc scratch stays modest");
+
+struct NoAllocInit {
+    DevFrame cur[kNoAllocMaxPictures], ref[kNoAllocMaxPictures];
+    int* out_global;
+    unsigned long long* out_sad;
+    int range, n;
+};
+
+// Resets the fields the staged search reads before it writes them (the planner zeroes each
+// stage's costs itself), so a call never sees the previous call's state.
+__global__ void noalloc_init_kernel(GState* states, const __grid_constant__ NoAllocInit a) {
+    const int i = threadIdx.x;
+    if (i >= a.n) return;
+    GState& s = states[i];
+    s.cur = a.cur[i];
+    s.ref = a.ref[i];
+    s.range = a.range;
+    s.out_global = a.out_global + 2 * i;
+    s.out_sad = a.out_sad + i;
+    s.n = 0;
+    s.top_n = 0;
+    s.best_dx = s.best_dy = 0;
+    s.best_cost = 0;
+    s.phase = 0;
+}
+
 }  // namespace vc1cu
+
+namespace {
+
+// Device address of g_noalloc_states per device ordinal, looked up once per device with
+// that device current (the host-side name of a __device__ array is not a device address).
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+vc1cu::GState* g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_fail(char* err, size_t err_len, int code, const char* msg) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", msg);
+    return code;
+}
+
+}  // namespace
+
+extern "C" int vc1cu_global_motion_noalloc(const uint8_t* const* cur_y, const uint8_t* const* ref_y, int pitch,
+                                           int width, int height, int range, int n, int32_t* d_dxdy,
+                                           uint64_t* d_sad, void* stream, char* err, size_t err_len) {
+    using namespace vc1cu;
+    if (err && err_len) err[0] = 0;
+    if (n < 1 || n > kNoAllocMaxPictures)
+        return noalloc_fail(err, err_len, VC1CU_ERR_ARG,
+                            "vc1cu_global_motion_noalloc: n must be 1..16 pictures per call (the fixed scratch size)");
+    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || width > 16384 || height > 16384 || pitch < width)
+        return noalloc_fail(err, err_len, VC1CU_ERR_ARG,
+                            "vc1cu_global_motion_noalloc: width/height must be even, 1..16384, pitch >= width");
+    if (range < 0 || range > 32)
+        return noalloc_fail(err, err_len, VC1CU_ERR_ARG, "vc1cu_global_motion_noalloc: range must be 0..32");
+    if (!cur_y || !ref_y || !d_dxdy || !d_sad)
+        return noalloc_fail(err, err_len, VC1CU_ERR_ARG, "vc1cu_global_motion_noalloc: null pointer argument");
+    NoAllocInit a{};
+    for (int i = 0; i < n; ++i) {
+        if (!cur_y[i] || !ref_y[i])
+            return noalloc_fail(err, err_len, VC1CU_ERR_ARG, "vc1cu_global_motion_noalloc: null frame pointer");
+        a.cur[i] = DevFrame{cur_y[i], nullptr, nullptr, pitch, 0};
+        a.ref[i] = DevFrame{ref_y[i], nullptr, nullptr, pitch, 0};
+    }
+    a.out_global = reinterpret_cast<int*>(d_dxdy);
+    a.out_sad = reinterpret_cast<unsigned long long*>(d_sad);
+    a.range = range;
+    a.n = n;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(err, err_len, VC1CU_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return noalloc_fail(err, err_len, VC1CU_ERR_UNSUPPORTED, "vc1cu_global_motion_noalloc: device ordinal >= 64");
+    GState* states = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_noalloc_states);
+            if (e != cudaSuccess || !ptr)
+                return noalloc_fail(err, err_len, VC1CU_ERR_CUDA,
+                                    e != cudaSuccess ? cudaGetErrorString(e) : "cudaGetSymbolAddress returned null");
+            g_noalloc_ptr[dev] = static_cast<GState*>(ptr);
+        }
+        states = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    noalloc_init_kernel<<<1, 32, 0, s>>>(states, a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(err, err_len, VC1CU_ERR_CUDA, cudaGetErrorString(e));
+    run_global_search(states, n, range, width, height, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(err, err_len, VC1CU_ERR_CUDA, cudaGetErrorString(e));
+    return VC1CU_OK;
+}
