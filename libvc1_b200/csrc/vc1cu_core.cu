@@ -50,6 +50,17 @@ __device__ unsigned long long g_phase_cnt[64];
 // this symbol, so all of its accesses compile to shared-space loads and stores (a pointer
 // kept in a struct would otherwise degrade to generic addressing).
 extern __shared__ __align__(16) uint8_t g_smem[];
+extern __shared__ __align__(16) uint32_t g_smem32[];  // the same memory, 32-bit words
+
+// Reference-window sampler: bytes read by direct index into the shared array (so always
+// shared-space loads). off: byte offset of the window; ww: row pitch; (wx0, wy0): origin.
+struct WinSampler {
+    uint32_t off;
+    int ww, wx0, wy0;
+    __device__ __forceinline__ int operator()(int x, int y) const {
+        return g_smem[off + (uint32_t)((y - wy0) * ww + (x - wx0))];
+    }
+};
 
 template <class T>
 struct SPtr {
@@ -105,11 +116,12 @@ __device__ __forceinline__ bool win_inside(const Mb& m, int xa, int ya, int xb, 
     return xa >= m.wx0 && ya >= m.wy0 && xb < m.wx0 + m.wp && yb < m.wy0 + m.wh;
 }
 
-// 16 window bytes starting at an arbitrary offset, as four little-endian words.
-__device__ __forceinline__ void win_load16(const uint8_t* p, uint32_t r[4]) {
-    const uint32_t* a = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
-    const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8;
-    const uint32_t w0 = a[0], w1 = a[1], w2 = a[2], w3 = a[3], w4 = a[4];
+// 16 shared-memory bytes starting at byte offset `off`, as four little-endian words.
+__device__ __forceinline__ void win_load16(uint32_t off, uint32_t r[4]) {
+    const uint32_t w = off >> 2;
+    const uint32_t sh = (off & 3) * 8;
+    const uint32_t w0 = g_smem32[w], w1 = g_smem32[w + 1], w2 = g_smem32[w + 2], w3 = g_smem32[w + 3],
+                   w4 = g_smem32[w + 4];
     r[0] = __funnelshift_r(w0, w1, sh);
     r[1] = __funnelshift_r(w1, w2, sh);
     r[2] = __funnelshift_r(w2, w3, sh);
@@ -118,22 +130,22 @@ __device__ __forceinline__ void win_load16(const uint8_t* p, uint32_t r[4]) {
 
 // mb_sad of a full 16x16 MB from the window with packed byte SADs (__vsadu4), strides 1/2/4.
 template <int STRIDE>
-__device__ __forceinline__ uint32_t sad_packed(const Mb& m, const uint8_t* base) {
+__device__ __forceinline__ uint32_t sad_packed(const Mb& m, uint32_t base) {
     uint32_t acc = 0;
-    const uint32_t* c32 = reinterpret_cast<const uint32_t*>(m.sm.cur.get());
+    const uint32_t c = m.sm.cur.off >> 2, c2 = m.sm.cur2.off >> 2, c4 = m.sm.cur4.off >> 2;
 #pragma unroll 4
     for (int y = 0; y < 16; y += STRIDE) {
         uint32_t r[4];
-        win_load16(base + y * m.wp, r);
+        win_load16(base + (uint32_t)(y * m.wp), r);
         if (STRIDE == 1) {
-            acc += __vsadu4(r[0], c32[y * 4 + 0]) + __vsadu4(r[1], c32[y * 4 + 1]) + __vsadu4(r[2], c32[y * 4 + 2]) +
-                   __vsadu4(r[3], c32[y * 4 + 3]);
+            acc += __vsadu4(r[0], g_smem32[c + y * 4 + 0]) + __vsadu4(r[1], g_smem32[c + y * 4 + 1]) +
+                   __vsadu4(r[2], g_smem32[c + y * 4 + 2]) + __vsadu4(r[3], g_smem32[c + y * 4 + 3]);
         } else if (STRIDE == 2) {
-            acc += __vsadu4(__byte_perm(r[0], r[1], 0x6420), m.sm.cur2[y * 2 + 0]) +
-                   __vsadu4(__byte_perm(r[2], r[3], 0x6420), m.sm.cur2[y * 2 + 1]);
+            acc += __vsadu4(__byte_perm(r[0], r[1], 0x6420), g_smem32[c2 + y * 2 + 0]) +
+                   __vsadu4(__byte_perm(r[2], r[3], 0x6420), g_smem32[c2 + y * 2 + 1]);
         } else {
             const uint32_t e = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
-            acc += __vsadu4(e, m.sm.cur4[y]);
+            acc += __vsadu4(e, g_smem32[c4 + y]);
         }
     }
     return acc;
@@ -142,14 +154,14 @@ __device__ __forceinline__ uint32_t sad_packed(const Mb& m, const uint8_t* base)
 // ---- integer SAD of the 16x16 MB, mb_sad (encoder_motion.cpp:2197-2285) ----------------
 
 template <int STRIDE, class S>
-__device__ __forceinline__ uint32_t sad_int_loop(const S& s, const uint8_t* cur, int x0, int y0, int dx, int dy, int aw,
+__device__ __forceinline__ uint32_t sad_int_loop(const S& s, uint32_t cur, int x0, int y0, int dx, int dy, int aw,
                                                  int ah) {
     uint32_t acc = 0;
 #pragma unroll 4
     for (int y = 0; y < ah; y += STRIDE) {
 #pragma unroll
         for (int x = 0; x < 16; x += STRIDE) {
-            if (x < aw) acc += (uint32_t)iabs((int)cur[y * 16 + x] - s(x0 + x + dx, y0 + y + dy));
+            if (x < aw) acc += (uint32_t)iabs((int)g_smem[cur + y * 16 + x] - s(x0 + x + dx, y0 + y + dy));
         }
     }
     return acc;
@@ -159,20 +171,20 @@ __device__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int 
     if (hidden_padding(P, m.x0, m.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
     uint32_t s;
     const bool fast = win_inside(m, m.x0 + dx, m.y0 + dy, m.x0 + dx + 15, m.y0 + dy + 15);
-    const WinSampler ws{m.sm.win, m.wp, m.wx0, m.wy0};
+    const WinSampler ws{m.sm.win.off, m.wp, m.wx0, m.wy0};
     if (fast && m.aw == 16 && m.ah == 16) {
-        const uint8_t* base = m.sm.win + (m.y0 + dy - m.wy0) * m.wp + (m.x0 + dx - m.wx0);
+        const uint32_t base = m.sm.win.off + (uint32_t)((m.y0 + dy - m.wy0) * m.wp + (m.x0 + dx - m.wx0));
         if (stride == 1) s = sad_packed<1>(m, base);
         else if (stride == 2) s = sad_packed<2>(m, base);
         else s = sad_packed<4>(m, base);
     } else if (fast) {
-        if (stride == 1) s = sad_int_loop<1>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else if (stride == 2) s = sad_int_loop<2>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else s = sad_int_loop<4>(ws, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        if (stride == 1) s = sad_int_loop<1>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else if (stride == 2) s = sad_int_loop<2>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else s = sad_int_loop<4>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
     } else {
-        if (stride == 1) s = sad_int_loop<1>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else if (stride == 2) s = sad_int_loop<2>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else s = sad_int_loop<4>(m.gref, m.sm.cur, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        if (stride == 1) s = sad_int_loop<1>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else if (stride == 2) s = sad_int_loop<2>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
+        else s = sad_int_loop<4>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
     }
     return stride > 1 ? (uint64_t)s * (uint64_t)(stride * stride) : (uint64_t)s;
 }
@@ -190,6 +202,35 @@ struct BatchCtx {
     int gpitch;
 };
 
+// The picture geometry the scorers read (raster, rounding, cropped-padding flags), by value:
+// passing the kernel's parameter block by address would make every parameter read of the
+// kernel a generic load.
+struct ScoreGeo {
+    int W, H, vw, vh, cvw, cvh, rnd, pads;  // pads: right, bottom, chroma right, chroma bottom
+};
+
+__device__ __forceinline__ ScoreGeo score_geo(const DevParams& P) {
+    return ScoreGeo{P.W, P.H, P.vw, P.vh, P.cvw, P.cvh, P.rnd,
+                    (P.right_pad ? 1 : 0) | (P.bottom_pad ? 2 : 0) | (P.cright_pad ? 4 : 0) | (P.cbottom_pad ? 8 : 0)};
+}
+
+// A parameter block holding just the scorer's fields (the rest stay zero).
+__device__ __forceinline__ DevParams geo_params(const ScoreGeo& g) {
+    DevParams P{};
+    P.W = g.W;
+    P.H = g.H;
+    P.vw = g.vw;
+    P.vh = g.vh;
+    P.cvw = g.cvw;
+    P.cvh = g.cvh;
+    P.rnd = g.rnd;
+    P.right_pad = g.pads & 1;
+    P.bottom_pad = (g.pads >> 1) & 1;
+    P.cright_pad = (g.pads >> 2) & 1;
+    P.cbottom_pad = (g.pads >> 3) & 1;
+    return P;
+}
+
 __device__ __forceinline__ uint32_t soff(const void* p) {
     return (uint32_t)(reinterpret_cast<const uint8_t*>(p) - g_smem);
 }
@@ -205,13 +246,11 @@ __device__ __forceinline__ bool ctx_inside(const BatchCtx& c, int xa, int ya, in
 // SAD of n candidates of block (bx,by,bw,bh) (bw,bh in {8,16}) under the CPU law, written
 // to out[]. Each candidate's block is split into 8-pixel row segments over bh*bw/8 lanes.
 // One out-of-line copy serves every call site.
-__device__ __noinline__ void sad_batch_core(const DevParams* Pp, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+__device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
                                             int bw, int bh, int mode, uint32_t out_off) {
-    const DevParams& P = *Pp;
+    const DevParams P = geo_params(g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
-    const uint8_t* win = g_smem + c.win_off;
-    const uint8_t* curb = g_smem + c.cur_off;
     const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int spr = bw >> 3;
     const int segs = bh * spr;  // 32 (16x16) or 8 (8x8)
@@ -234,13 +273,13 @@ __device__ __noinline__ void sad_batch_core(const DevParams* Pp, const BatchCtx 
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
                 int pred[8];
                 if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
-                    predict_row<8>(WinSampler{win, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                    predict_row<8>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
                 else
                     predict_row<8>(gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
-                const uint8_t* cp = curb + (cy + r) * 16 + cx + c0;
+                const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
-                    if (c0 + i < aw) part += (uint32_t)iabs((int)cp[i] - pred[i]);
+                    if (c0 + i < aw) part += (uint32_t)iabs((int)g_smem[cp + i] - pred[i]);
             }
         }
         for (int o = segs >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
@@ -249,13 +288,11 @@ __device__ __noinline__ void sad_batch_core(const DevParams* Pp, const BatchCtx 
     __syncwarp();
 }
 
-__device__ __noinline__ void satd_batch_core(const DevParams* Pp, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+__device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
                                              int bw, int bh, int mode, uint32_t out_off) {
-    const DevParams& P = *Pp;
+    const DevParams P = geo_params(g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
-    const uint8_t* win = g_smem + c.win_off;
-    const uint8_t* curb = g_smem + c.cur_off;
     const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int tpr = bw >> 2;
     const int tiles = tpr * (bh >> 2);  // 16 or 4
@@ -280,12 +317,13 @@ __device__ __noinline__ void satd_batch_core(const DevParams* Pp, const BatchCtx
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
                 if (fast)
-                    predict_row<4>(WinSampler{win, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                    predict_row<4>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
                 else
                     predict_row<4>(gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
 #pragma unroll
                 for (int xx = 0; xx < 4; ++xx)
-                    d[yy * 4 + xx] = (xx < tw && yy < th) ? (int)curb[(cy + ty + yy) * 16 + cx + tx + xx] - pred[xx] : 0;
+                    d[yy * 4 + xx] =
+                        (xx < tw && yy < th) ? (int)g_smem[c.cur_off + (uint32_t)((cy + ty + yy) * 16 + cx + tx + xx)] - pred[xx] : 0;
             }
             part = satd4x4(d);
         }
@@ -298,12 +336,12 @@ __device__ __noinline__ void satd_batch_core(const DevParams* Pp, const BatchCtx
 // mvs and out point into the warp's shared-memory buffers.
 __device__ __forceinline__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
                                           int bh, int mode, uint64_t* out) {
-    sad_batch_core(&P, batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
+    sad_batch_core(score_geo(P), batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
 }
 
 __device__ __forceinline__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
                                            int bh, int mode, uint64_t* out) {
-    satd_batch_core(&P, batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
+    satd_batch_core(score_geo(P), batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
 }
 
 // ---- first-visit bitsets ----------------------------------------------------------------
@@ -1291,33 +1329,56 @@ __device__ __forceinline__ int median4(int a, int b, int c, int d) {
 
 // ---- wavefront synchronisation ----------------------------------------------------------
 
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Waits (bounded) until *flag == epoch (a macroblock of this launch was published). On
-// timeout it raises the launch's error and abort flags and returns false.
-__device__ bool wait_flag(const uint32_t* flag, uint32_t epoch, LaunchStatus* st) {
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Waits (bounded) until each lane's flag equals epoch (a macroblock of this launch was
+// published; a lane with a null flag waits for nothing). The flags are polled with relaxed
+// loads, all lanes at once, and one acquire fence follows the last poll, so a poll costs
+// no L1 invalidation. Every lane calls it. On timeout it raises the launch's error and
+// abort flags and returns false.
+__device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* st) {
+    bool mine = flag == nullptr;
     for (long it = 0; it < (1L << 24); ++it) {
-        if (ld_acquire(flag) == epoch) return true;
-        if (*(volatile int*)&st->abort) return false;
+        if (!mine) mine = ld_relaxed(flag) == epoch;
+        if (__all_sync(FULL, mine)) {
+            // the observing lanes acquire; the warp barrier orders the other lanes' reads after it
+            fence_acquire();
+            __syncwarp();
+            return true;
+        }
+        if ((it & 15) == 15) {
+            const int ab = __shfl_sync(FULL, (int)ld_relaxed(reinterpret_cast<const uint32_t*>(&st->abort)), 0);
+            if (ab) return false;
+        }
         __nanosleep(64);
     }
-    atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
-    atomicExch(&st->abort, 1);
-    atomicAdd(&st->timeouts, 1u);
+    if ((threadIdx.x & 31) == 0) {
+        atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
+        atomicExch(&st->abort, 1);
+        atomicAdd(&st->timeouts, 1u);
+    }
     return false;
 }
 
-// Waits for the MB at (x,y) of the same pass (outside the raster: nothing to wait for).
-__device__ bool wait_mb(const DevParams& P, const DevResult& o, int x, int y, uint32_t epoch, LaunchStatus* st) {
-    if (x < 0 || y < 0 || x >= P.mbw) return true;
-    return wait_flag(&o.done[y * P.mbw + x], epoch, st);
+// Waits for the left, top-left, top and top-right macroblocks of the same pass (lanes 0..3;
+// positions outside the raster need no wait).
+__device__ bool wait_neighbours(const DevParams& P, const DevResult& o, int mx, int my, int lane, uint32_t epoch,
+                                LaunchStatus* st) {
+    const uint32_t* f = nullptr;
+    if (lane < 4) {
+        const int x = mx + (lane == 3 ? 1 : (lane == 2 ? 0 : -1)), y = my - (lane == 0 ? 0 : 1);
+        if (x >= 0 && y >= 0 && x < P.mbw) f = &o.done[y * P.mbw + x];
+    }
+    return wait_flags(f, epoch, st);
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
@@ -1499,7 +1560,8 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         PHASE_START((seeded ? 1 : 0) + (allow_4mv ? 2 : 0));
         bool ok = !*(volatile int*)&st->abort;
         // a seed produced by another pass of this launch
-        if (ok && d.seed_pass >= 0) ok = wait_flag(&passes[d.seed_pass].out.done[mbi], epoch, st);
+        if (ok && d.seed_pass >= 0)
+            ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st);
         PHASE_MARK(0);
         if (ok) load_cur(P, m, d.cur);
         PHASE_MARK(1);
@@ -1572,10 +1634,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             PHASE_MARK(4);
         }
         // ---- wavefront: left, top-left, top, top-right of the same pass ----
-        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx - 1, m.my - 1, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx, m.my - 1, epoch, st);
-        if (ok) ok = wait_mb(P, o, m.mx + 1, m.my - 1, epoch, st);
+        if (ok) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st);
         __syncwarp();
         PHASE_MARK(5);
         if (ok) {

@@ -1,7 +1,7 @@
 // vc1cu_pred.cuh - VC-1 luma interpolation and block costs on the device.
 //
-// Samplers read a reference plane either from a per-warp shared-memory window (fast path)
-// or from HBM with clamped coordinates (edge emulation, Vc1Encoder::sample_clamped,
+// Samplers read a reference plane either from a per-warp shared-memory window (fast path,
+// WinSampler in vc1cu_core.cu) or from HBM with clamped coordinates (edge emulation, Vc1Encoder::sample_clamped,
 // encoder_motion_compensation.cpp:350-353). Both return identical values wherever the
 // window is defined, because the window is filled with the same clamped samples.
 #pragma once
@@ -9,12 +9,6 @@
 #include "vc1cu_common.cuh"
 
 namespace vc1cu {
-
-struct WinSampler {
-    const uint8_t* win;
-    int ww, wx0, wy0;
-    __device__ __forceinline__ int operator()(int x, int y) const { return win[(y - wy0) * ww + (x - wx0)]; }
-};
 
 struct GlobSampler {
     const uint8_t* p;
