@@ -251,7 +251,6 @@ __device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, 
     const DevParams P = geo_params(g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
-    const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int spr = bw >> 3;
     const int segs = bh * spr;  // 32 (16x16) or 8 (8x8)
     const int per_iter = 32 / segs;
@@ -272,10 +271,13 @@ __device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, 
             if (!bad && r < ah && c0 < aw) {
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
                 int pred[8];
-                if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1))
+                if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1)) {
                     predict_row<8>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
-                else
-                    predict_row<8>(gref, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                } else {
+                    const PredRow<8> g8 = predict_row_glob<8>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + c0, by + r);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) pred[i] = g8.v[i];
+                }
                 const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
@@ -293,7 +295,6 @@ __device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c,
     const DevParams P = geo_params(g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
-    const GlobSampler gref{c.gref, c.gpitch, P.W, P.H};
     const int tpr = bw >> 2;
     const int tiles = tpr * (bh >> 2);  // 16 or 4
     const int per_iter = 32 / tiles;
@@ -312,20 +313,30 @@ __device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c,
         if (valid && !bad && tw && th) {
             const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
             const bool fast = ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1);
-            int d[16];
-#pragma unroll
+            // rows one at a time (one copy of the interpolation code), row-transformed and
+            // rotated through four registers for the column stage
+            int4 r0 = make_int4(0, 0, 0, 0), r1 = r0, r2 = r0, r3 = r0;
+#pragma unroll 1
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
-                if (fast)
+                if (fast) {
                     predict_row<4>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
-                else
-                    predict_row<4>(gref, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                } else {
+                    const PredRow<4> g4 = predict_row_glob<4>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + tx,
+                                                              by + ty + yy);
 #pragma unroll
-                for (int xx = 0; xx < 4; ++xx)
-                    d[yy * 4 + xx] =
-                        (xx < tw && yy < th) ? (int)g_smem[c.cur_off + (uint32_t)((cy + ty + yy) * 16 + cx + tx + xx)] - pred[xx] : 0;
+                    for (int i = 0; i < 4; ++i) pred[i] = g4.v[i];
+                }
+                int d[4];
+                const uint32_t crow = c.cur_off + (uint32_t)((cy + ty + yy) * 16 + cx + tx);
+#pragma unroll
+                for (int xx = 0; xx < 4; ++xx) d[xx] = (xx < tw && yy < th) ? (int)g_smem[crow + xx] - pred[xx] : 0;
+                r0 = r1;
+                r1 = r2;
+                r2 = r3;
+                r3 = hadamard_row(d[0], d[1], d[2], d[3]);
             }
-            part = satd4x4(d);
+            part = hadamard_cols(r0, r1, r2, r3);
         }
         for (int o = tiles >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);
         if (valid && t == 0) out[ci] = (!aw || !ah) ? 0 : (bad ? kBad : (uint64_t)part);
@@ -673,60 +684,92 @@ static_assert(sizeof(SpecBlk) <= kSpecBlkBytes, "SpecBlk layout");
 
 __device__ __forceinline__ int make_even(int v) { return !(v & 1) ? v : (v > 0 ? v - 1 : v + 1); }
 
-// Appends the batch MVs that are not yet in the list (the `add` lambda, :3324-3337), scoring
-// the new ones with the CPU law in one warp-parallel pass.
-__device__ __forceinline__ void list_add_batch(const DevParams& P, const Mb& m, int& n, const int2* mvs, int nb, int bx, int by, int bw,
-                               int bh, int mode) {
-    // dedup on every lane identically (tiny lists)
-    int2* nb_mv = m.sm.batch;
-    int nn = 0;
-    for (int i = 0; i < nb; ++i) {
-        bool dup = false;
-        for (int j = 0; j < n && !dup; ++j) dup = m.sm.list_mv[j].x == mvs[i].x && m.sm.list_mv[j].y == mvs[i].y;
-        for (int j = 0; j < nn && !dup; ++j) dup = nb_mv[j].x == mvs[i].x && nb_mv[j].y == mvs[i].y;
-        if (!dup) {
-            __syncwarp();
-            if (m.lane == 0) nb_mv[nn] = mvs[i];
-            __syncwarp();
-            ++nn;
+// ---- the refinement's candidate list, held across the warp's lanes -------------------------
+//
+// Lane j < n holds list entry j (vector, CPU-law SAD). Entries are distinct vectors; their
+// order is immaterial because every selection over them uses a total order, so membership
+// tests, minima and ranks are warp votes and shuffles instead of serial scans.
+struct RegList {
+    int n;  // warp-uniform entry count (<= 32)
+    int2 mv;
+    uint64_t sad;
+};
+
+__device__ __forceinline__ bool sad_tie_less(uint64_t sa, int2 a, uint64_t sb, int2 b) {
+    if (sa != sb) return sa < sb;
+    return tie_less(a, b);
+}
+
+// Minimum over the lanes with `valid` of (s, v) under (sad, tie_less); the result on every lane.
+__device__ __forceinline__ void warp_argmin_sad(bool& valid, uint64_t& s, int2& v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const bool ov = __shfl_xor_sync(FULL, valid, o);
+        const uint64_t os = __shfl_xor_sync(FULL, s, o);
+        const int ox = __shfl_xor_sync(FULL, v.x, o), oy = __shfl_xor_sync(FULL, v.y, o);
+        if (ov && (!valid || sad_tie_less(os, make_int2(ox, oy), s, v))) {
+            valid = true;
+            s = os;
+            v = make_int2(ox, oy);
         }
     }
+}
+
+// Adds the candidates that lanes i < nb hold in `c` and the list lacks, in lane order, and
+// scores the new ones with the CPU law in one batch (the `add` lambda, :3324-3337).
+__device__ __forceinline__ void reg_add(const DevParams& P, const Mb& m, RegList& L, int2 c, int nb, int bx, int by,
+                                        int bw, int bh, int mode) {
+    const bool act = m.lane < nb;
+    bool listed = false;
+    for (int i = 0; i < nb; ++i) {
+        const int cx = __shfl_sync(FULL, c.x, i), cy = __shfl_sync(FULL, c.y, i);
+        const bool hit = __any_sync(FULL, m.lane < L.n && L.mv.x == cx && L.mv.y == cy);
+        if (m.lane == i) listed = hit;
+    }
+    bool first = false;
+    const unsigned amask = __ballot_sync(FULL, act);
+    if (act) {
+        const unsigned long long key = ((unsigned long long)(uint32_t)c.x << 32) | (uint32_t)c.y;
+        first = (__ffs(__match_any_sync(amask, key)) - 1) == m.lane;
+    }
+    const bool fresh = act && !listed && first;
+    const unsigned fm = __ballot_sync(FULL, fresh);
+    const int nn = __popc(fm);
     if (!nn) return;
-    sad_batch(P, m, nb_mv, nn, bx, by, bw, bh, mode, m.sm.batch_cost);
-    if (m.lane < nn) {
-        m.sm.list_mv[n + m.lane] = nb_mv[m.lane];
-        m.sm.list_sad[n + m.lane] = m.sm.batch_cost[m.lane];  // hidden padding already BAD
+    if (fresh) m.sm.batch[__popc(fm & ((1u << m.lane) - 1))] = c;
+    __syncwarp();
+    sad_batch(P, m, m.sm.batch, nn, bx, by, bw, bh, mode, m.sm.batch_cost);  // hidden padding costs BAD
+    if (m.lane >= L.n && m.lane < L.n + nn) {
+        L.mv = m.sm.batch[m.lane - L.n];
+        L.sad = m.sm.batch_cost[m.lane - L.n];
     }
-    n += nn;
+    L.n += nn;
     __syncwarp();
 }
 
-// Lanes i < nb write gen(i) to the warp's stencil buffer.
-template <class G>
-__device__ __forceinline__ void put_stencil(const Mb& m, int nb, G gen) {
-    if (m.lane < nb) m.sm.stencil[m.lane] = gen(m.lane);
-    __syncwarp();
-}
-
-__device__ __forceinline__ const uint64_t* list_find(const Mb& m, int n, int2 mv, int& idx) {
-    for (int j = 0; j < n; ++j)
-        if (m.sm.list_mv[j].x == mv.x && m.sm.list_mv[j].y == mv.y) {
-            idx = j;
-            return &m.sm.list_sad[j];
-        }
-    idx = -1;
-    return nullptr;
-}
-
-__device__ void update_min(const Mb& m, int n, const int2* mvs, int nb, int2& best, uint64_t& best_sad) {
+// The entry equal to the stencil vectors of lanes i < nb with the least (sad, tie_less),
+// folded into (best, best_sad) by the same order (every stencil vector is in the list).
+__device__ __forceinline__ void reg_update_min(const Mb& m, const RegList& L, int2 c, int nb, int2& best,
+                                               uint64_t& best_sad) {
+    bool in_st = false;
     for (int i = 0; i < nb; ++i) {
-        int j;
-        const uint64_t* s = list_find(m, n, mvs[i], j);
-        if (s && (*s < best_sad || (*s == best_sad && tie_less(mvs[i], best)))) {
-            best_sad = *s;
-            best = mvs[i];
-        }
+        const int cx = __shfl_sync(FULL, c.x, i), cy = __shfl_sync(FULL, c.y, i);
+        in_st |= m.lane < L.n && L.mv.x == cx && L.mv.y == cy;
     }
+    bool valid = in_st;
+    uint64_t s = L.sad;
+    int2 v = L.mv;
+    warp_argmin_sad(valid, s, v);
+    if (valid && sad_tie_less(s, v, best_sad, best)) {
+        best = v;
+        best_sad = s;
+    }
+}
+
+// SAD of the listed vector v (warp-uniform; it must be listed).
+__device__ __forceinline__ uint64_t reg_find(const RegList& L, int lane, int2 v) {
+    const unsigned hit = __ballot_sync(FULL, lane < L.n && L.mv.x == v.x && L.mv.y == v.y);
+    return __shfl_sync(FULL, L.sad, __ffs(hit) - 1);
 }
 
 // refine_motion_integer_only, encoder_motion.cpp:3247-3269
@@ -753,8 +796,8 @@ __device__ RefineOut refine_integer_only(const DevParams& P, const Mb& m, int bx
 }
 
 // refine_qpel_block / refine_motion_block (me_quality SAD), encoder_motion.cpp:3596-3749
-__device__ __forceinline__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed, int range,
-                                     int mode, uint64_t known) {
+__device__ __forceinline__ RefineOut refine_sad_only(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh,
+                                                     int2 seed, int range, int mode, uint64_t known) {
     const int limit_q = 4 * P.subpel_range;
     if (!P.subpel || limit_q == 0 || imax(iabs(seed.x), iabs(seed.y)) > limit_q)
         return refine_integer_only(P, m, bx, by, bw, bh, seed, range, mode, known);
@@ -770,17 +813,16 @@ __device__ __forceinline__ RefineOut refine_sad_only(const DevParams& P, const M
         seed = make_int2(0, 0);
         known = UINT64_MAX;
     }
-    int n = 0;
+    RegList L{0, make_int2(0, 0), 0};
     if (known != UINT64_MAX) {
-        if (m.lane == 0) { m.sm.list_mv[0] = seed; m.sm.list_sad[0] = known; }
-        __syncwarp();
-        n = 1;
+        L.n = 1;
+        L.mv = seed;
+        L.sad = known;
     } else {
-        put_stencil(m, 1, [&](int) { return seed; });
-        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, emode);
+        reg_add(P, m, L, seed, 1, bx, by, bw, bh, emode);
     }
     int2 best = seed;
-    uint64_t cost = m.sm.list_sad[0];
+    uint64_t cost = __shfl_sync(FULL, L.sad, 0);
     auto fix = [&](int2 v) {
         v.x = iclamp(v.x, xmin, xmax);
         v.y = iclamp(v.y, ymin, ymax);
@@ -789,9 +831,9 @@ __device__ __forceinline__ RefineOut refine_sad_only(const DevParams& P, const M
     };
     // one stencil stage: gen(i) for i < np, clamped, scored and folded into (cost, best)
     auto stage = [&](int np, auto gen) {
-        put_stencil(m, np, [&](int i) { return fix(gen(i)); });
-        list_add_batch(P, m, n, m.sm.stencil, np, bx, by, bw, bh, emode);
-        update_min(m, n, m.sm.stencil, np, best, cost);
+        const int2 c = m.lane < np ? fix(gen(m.lane)) : make_int2(0, 0);
+        reg_add(P, m, L, c, np, bx, by, bw, bh, emode);
+        reg_update_min(m, L, c, np, best, cost);
     };
     // the two candidates beside an axis move: (c.x, c.y -/+ d) or (c.x -/+ d, c.y)
     auto side = [](int2 c, int d, bool vertical) {
@@ -866,123 +908,86 @@ __device__ __forceinline__ Shortlist refine_prepare(const DevParams& P, const Mb
     seed.x = iclamp(seed.x, xmin, xmax);
     seed.y = iclamp(seed.y, ymin, ymax);
     if (hp) { seed.x = make_even(seed.x); seed.y = make_even(seed.y); }
-    int n = 0;
+    RegList L{0, seed, 0};
     // add(seed, known)
     if (known != UINT64_MAX) {
-        if (m.lane == 0) {
-            m.sm.list_mv[0] = seed;
-            m.sm.list_sad[0] = hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg) ? kBad : known;
-        }
-        __syncwarp();
-        n = 1;
+        L.n = 1;
+        L.sad = hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg) ? kBad : known;
     } else {
-        put_stencil(m, 1, [&](int) { return seed; });
-        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, mode);
+        reg_add(P, m, L, seed, 1, bx, by, bw, bh, mode);
     }
-    if (hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg)) {
-        put_stencil(m, 1, [](int) { return make_int2(0, 0); });
-        list_add_batch(P, m, n, m.sm.stencil, 1, bx, by, bw, bh, mode);
-    }
+    if (hidden_padding(P, bx, by, bw, bh, seed.x, seed.y, mode, cg)) reg_add(P, m, L, make_int2(0, 0), 1, bx, by, bw, bh, mode);
     int2 half_best = seed;
-    uint64_t half_sad = m.sm.list_sad[0];
+    uint64_t half_sad = __shfl_sync(FULL, L.sad, 0);
     const bool fast = P.fast_subpel;
     auto clampmv = [&](int x, int y) {
         int2 v = make_int2(iclamp(x, xmin, xmax), iclamp(y, ymin, ymax));
         if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
         return v;
     };
+    const int i = m.lane;
     {
         const int nb = fast ? 5 : 9;
-        if (fast)
-            put_stencil(m, 5, [&](int i) {
-                return i == 0 ? seed : i == 1 ? clampmv(seed.x - 2, seed.y) : i == 2 ? clampmv(seed.x + 2, seed.y)
-                                 : i == 3 ? clampmv(seed.x, seed.y - 2) : clampmv(seed.x, seed.y + 2);
-            });
-        else
-            put_stencil(m, 9, [&](int i) { return clampmv(seed.x + (i % 3 - 1) * 2, seed.y + (i / 3 - 1) * 2); });
-        list_add_batch(P, m, n, m.sm.stencil, nb, bx, by, bw, bh, mode);
-        update_min(m, n, m.sm.stencil, nb, half_best, half_sad);
+        const int2 c = fast ? (i == 0 ? seed : i == 1 ? clampmv(seed.x - 2, seed.y) : i == 2 ? clampmv(seed.x + 2, seed.y)
+                                             : i == 3 ? clampmv(seed.x, seed.y - 2) : clampmv(seed.x, seed.y + 2))
+                            : clampmv(seed.x + (i % 3 - 1) * 2, seed.y + (i / 3 - 1) * 2);
+        reg_add(P, m, L, c, nb, bx, by, bw, bh, mode);
+        reg_update_min(m, L, c, nb, half_best, half_sad);
     }
     if (fast && !(half_best.x == seed.x && half_best.y == seed.y)) {
         const int dx = half_best.x - seed.x, dy = half_best.y - seed.y;
         const int2 hbv = half_best;
         int nd = 0;
+        int2 c = make_int2(0, 0);
         if (dx && !dy) {
             nd = 2;
-            put_stencil(m, 2, [&](int i) {
-                int2 v = make_int2(hbv.x, iclamp(seed.y + (i ? 2 : -2), ymin, ymax));
-                if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
-                return v;
-            });
+            c = make_int2(hbv.x, iclamp(seed.y + (i ? 2 : -2), ymin, ymax));
         } else if (dy && !dx) {
             nd = 2;
-            put_stencil(m, 2, [&](int i) {
-                int2 v = make_int2(iclamp(seed.x + (i ? 2 : -2), xmin, xmax), hbv.y);
-                if (hp) { v.x = make_even(v.x); v.y = make_even(v.y); }
-                return v;
-            });
+            c = make_int2(iclamp(seed.x + (i ? 2 : -2), xmin, xmax), hbv.y);
         }
+        if (hp) { c.x = make_even(c.x); c.y = make_even(c.y); }
         if (nd) {
-            list_add_batch(P, m, n, m.sm.stencil, nd, bx, by, bw, bh, mode);
-            update_min(m, n, m.sm.stencil, nd, half_best, half_sad);
+            reg_add(P, m, L, c, nd, bx, by, bw, bh, mode);
+            reg_update_min(m, L, c, nd, half_best, half_sad);
         }
     }
     if (!hp) {
         if (fast) {
             const int2 qc = half_best;
-            put_stencil(m, 5, [&](int i) {
-                return i == 0 ? qc : i == 1 ? make_int2(iclamp(qc.x - 1, xmin, xmax), qc.y)
-                                 : i == 2 ? make_int2(iclamp(qc.x + 1, xmin, xmax), qc.y)
-                                 : i == 3 ? make_int2(qc.x, iclamp(qc.y - 1, ymin, ymax))
-                                          : make_int2(qc.x, iclamp(qc.y + 1, ymin, ymax));
-            });
-            list_add_batch(P, m, n, m.sm.stencil, 5, bx, by, bw, bh, mode);
-            int j;
-            uint64_t qcost = *list_find(m, n, qc, j);
+            const int2 c = i == 0 ? qc : i == 1 ? make_int2(iclamp(qc.x - 1, xmin, xmax), qc.y)
+                         : i == 2 ? make_int2(iclamp(qc.x + 1, xmin, xmax), qc.y)
+                         : i == 3 ? make_int2(qc.x, iclamp(qc.y - 1, ymin, ymax))
+                                  : make_int2(qc.x, iclamp(qc.y + 1, ymin, ymax));
+            reg_add(P, m, L, c, 5, bx, by, bw, bh, mode);
+            uint64_t qcost = reg_find(L, m.lane, qc);
             int2 qbmv = qc;
-            update_min(m, n, m.sm.stencil, 5, qbmv, qcost);
+            reg_update_min(m, L, c, 5, qbmv, qcost);
             const int dx = qbmv.x - qc.x, dy = qbmv.y - qc.y;
             if (dx && !dy) {
-                put_stencil(m, 2, [&](int i) { return make_int2(qbmv.x, iclamp(qc.y + (i ? 1 : -1), ymin, ymax)); });
-                list_add_batch(P, m, n, m.sm.stencil, 2, bx, by, bw, bh, mode);
+                reg_add(P, m, L, make_int2(qbmv.x, iclamp(qc.y + (i ? 1 : -1), ymin, ymax)), 2, bx, by, bw, bh, mode);
             } else if (dy && !dx) {
-                put_stencil(m, 2, [&](int i) { return make_int2(iclamp(qc.x + (i ? 1 : -1), xmin, xmax), qbmv.y); });
-                list_add_batch(P, m, n, m.sm.stencil, 2, bx, by, bw, bh, mode);
+                reg_add(P, m, L, make_int2(iclamp(qc.x + (i ? 1 : -1), xmin, xmax), qbmv.y), 2, bx, by, bw, bh, mode);
             }
         } else {
             const int2 hbv = half_best;
-            put_stencil(m, 9, [&](int i) {
-                return make_int2(iclamp(hbv.x + i % 3 - 1, xmin, xmax), iclamp(hbv.y + i / 3 - 1, ymin, ymax));
-            });
-            list_add_batch(P, m, n, m.sm.stencil, 9, bx, by, bw, bh, mode);
+            reg_add(P, m, L, make_int2(iclamp(hbv.x + i % 3 - 1, xmin, xmax), iclamp(hbv.y + i / 3 - 1, ymin, ymax)), 9,
+                    bx, by, bw, bh, mode);
         }
     }
-    // sort by (sad, tie_less), keep 8 / 4 (:3445-3456)
+    // sort by (sad, tie_less), keep 8 / 4 (:3445-3456): rank of each entry by shuffles
     const int keep = fast ? 4 : 8;
-    int2 my_mv = make_int2(0, 0);
-    uint64_t my_sad = 0;
-    int rank = 32;
-    if (m.lane < n) {
-        my_mv = m.sm.list_mv[m.lane];
-        my_sad = m.sm.list_sad[m.lane];
-        rank = 0;
-        for (int j = 0; j < n; ++j) {
-            const uint64_t s = m.sm.list_sad[j];
-            const int2 v = m.sm.list_mv[j];
-            if (s < my_sad || (s == my_sad && tie_less(v, my_mv))) ++rank;
-        }
+    int rank = 0;
+    for (int k = 0; k < L.n; ++k) {
+        const uint64_t sk = __shfl_sync(FULL, L.sad, k);
+        const int kx = __shfl_sync(FULL, L.mv.x, k), ky = __shfl_sync(FULL, L.mv.y, k);
+        rank += sad_tie_less(sk, make_int2(kx, ky), L.sad, L.mv) ? 1 : 0;
     }
-    uint64_t screen = UINT64_MAX;
-    {
-        const uint64_t cand = rank == 0 ? my_sad : UINT64_MAX;
-        screen = warp_min_u64(cand);
-    }
-    __syncwarp();
-    const int nk = imin(n, keep);
-    // compact the kept candidates by rank: slot = rank
-    if (m.lane < n && rank < nk) {
-        m.sm.batch[rank] = my_mv;
-        m.sm.batch_cost[rank] = my_sad;
+    const uint64_t screen = warp_min_u64(m.lane < L.n ? L.sad : UINT64_MAX);
+    const int nk = imin(L.n, keep);
+    if (m.lane < L.n && rank < nk) {
+        m.sm.batch[rank] = L.mv;
+        m.sm.batch_cost[rank] = L.sad;
     }
     __syncwarp();
     sl.direct = 0;
@@ -998,81 +1003,115 @@ __device__ __forceinline__ Shortlist refine_prepare(const DevParams& P, const Mb
     return sl;
 }
 
+// 128-bit value exchanged with the lane `o` positions away (xor).
+__device__ __forceinline__ unsigned __int128 shfl_xor_u128(unsigned __int128 x, int o) {
+    const uint64_t lo = __shfl_xor_sync(FULL, (uint64_t)x, o), hi = __shfl_xor_sync(FULL, (uint64_t)(x >> 64), o);
+    return ((unsigned __int128)hi << 64) | lo;
+}
+
+// One shortlisted candidate in a lane's registers during the final selection.
+struct SelCand {
+    bool valid, elig;
+    unsigned __int128 key;
+    uint64_t satd, sad;
+    int2 mv;
+};
+
+__device__ __forceinline__ SelCand shfl_xor_cand(const SelCand& c, int o) {
+    SelCand r;
+    r.valid = __shfl_xor_sync(FULL, c.valid, o);
+    r.elig = __shfl_xor_sync(FULL, c.elig, o);
+    r.key = shfl_xor_u128(c.key, o);
+    r.satd = __shfl_xor_sync(FULL, c.satd, o);
+    r.sad = __shfl_xor_sync(FULL, c.sad, o);
+    r.mv = make_int2(__shfl_xor_sync(FULL, c.mv.x, o), __shfl_xor_sync(FULL, c.mv.y, o));
+    return r;
+}
+
+// Rate winner order (:3477-3488): (score, sad, tie_less).
+__device__ __forceinline__ bool rate_less(const SelCand& a, const SelCand& b) {
+    if (a.valid != b.valid) return a.valid;
+    if (a.key != b.key) return a.key < b.key;
+    return sad_tie_less(a.sad, a.mv, b.sad, b.mv);
+}
+
+// Final order (:3526-3531): eligible first, then (score, satd, sad, tie_less).
+__device__ __forceinline__ bool final_less(const SelCand& a, const SelCand& b) {
+    if (a.valid != b.valid) return a.valid;
+    if (a.elig != b.elig) return a.elig;
+    if (a.key != b.key) return a.key < b.key;
+    if (a.satd != b.satd) return a.satd < b.satd;
+    return sad_tie_less(a.sad, a.mv, b.sad, b.mv);
+}
+
+// Least candidate of lanes 0..7 under `less`, on every lane.
+template <class Less>
+__device__ __forceinline__ SelCand warp_min8(SelCand c, Less less) {
+#pragma unroll
+    for (int o = 4; o; o >>= 1) {
+        const SelCand d = shfl_xor_cand(c, o);
+        if (less(d, c)) c = d;
+    }
+    SelCand r;
+    r.valid = __shfl_sync(FULL, c.valid, 0);
+    r.elig = __shfl_sync(FULL, c.elig, 0);
+    r.key = ((unsigned __int128)__shfl_sync(FULL, (uint64_t)(c.key >> 64), 0) << 64) | __shfl_sync(FULL, (uint64_t)c.key, 0);
+    r.satd = __shfl_sync(FULL, c.satd, 0);
+    r.sad = __shfl_sync(FULL, c.sad, 0);
+    r.mv = make_int2(__shfl_sync(FULL, c.mv.x, 0), __shfl_sync(FULL, c.mv.y, 0));
+    return r;
+}
+
 // The rest of refine_motion_block_staged (encoder_motion.cpp:3458-3535) given the predictor.
+// Lane i < nk holds shortlist entry i; both selections are warp reductions.
 __device__ RefineOut refine_select(const DevParams& P, const Mb& m, const Shortlist& sl, int bx, int by, int bw, int bh,
                                    int mode, const PInfo& pi, bool more) {
     if (sl.direct) return sl.out;
-    const int nk = sl.nk;
-    const uint64_t screen = sl.screen;
-    // rate + score (:3458-3476)
-    if (m.lane < nk) {
-        const int2 mv = m.sm.batch[m.lane];
+    const int nk = sl.nk;  // <= 8
+    SelCand c;
+    c.valid = m.lane < nk;
+    c.elig = false;
+    c.mv = c.valid ? m.sm.batch[m.lane] : make_int2(0, 0);
+    c.sad = c.valid ? m.sm.batch_cost[m.lane] : UINT64_MAX;
+    c.satd = kBad;
+    uint32_t rate = 0;
+    c.key = 0;
+    if (c.valid) {
+        // rate + score (:3458-3476)
         int2 pred = pi.pre;
-        uint32_t rate = 0;
         if (pi.hybrid) {
-            pred = modular_mv_distance(P, mv, pi.a) <= modular_mv_distance(P, mv, pi.c) ? pi.a : pi.c;
+            pred = modular_mv_distance(P, c.mv, pi.a) <= modular_mv_distance(P, c.mv, pi.c) ? pi.a : pi.c;
             ++rate;
         }
-        rate += mv_rate_bits(P, mv, pred, mode, more);
-        m.sm.list_rate[m.lane] = rate;
-        m.sm.list_key[m.lane] = score_key(P, m.lam_m, m.lam_s, m.sm.batch_cost[m.lane], rate);
+        rate += mv_rate_bits(P, c.mv, pred, mode, more);
+        c.key = score_key(P, m.lam_m, m.lam_s, c.sad, rate);
     }
-    __syncwarp();
-    // rate winner: min over (score, sad, tie_less)
-    int rw = 0;
-    for (int i = 1; i < nk; ++i) {
-        const unsigned __int128 a = m.sm.list_key[i], b = m.sm.list_key[rw];
-        const uint64_t sa = m.sm.batch_cost[i], sb = m.sm.batch_cost[rw];
-        if (a < b || (a == b && (sa < sb || (sa == sb && tie_less(m.sm.batch[i], m.sm.batch[rw]))))) rw = i;
+    const SelCand rw = warp_min8(c, rate_less);
+    if (P.me_quality == 1) {
+        __syncwarp();
+        return RefineOut{rw.mv, sl.screen};
     }
-    if (P.me_quality == 1) return RefineOut{m.sm.batch[rw], screen};
-    const uint64_t rws = m.sm.batch_cost[rw];
+    const uint64_t rws = rw.sad;
     const uint64_t pct3 = (rws / 100) * 3 + (((rws % 100) * 3 + 99) / 100);
     const uint64_t slack = pct3 > 4 ? pct3 : 4;
     const uint64_t limit = rws > UINT64_MAX - slack ? UINT64_MAX : rws + slack;
+    c.elig = c.valid && c.sad < UINT64_MAX / 8 && c.sad <= limit;
     // SATD of the eligible shortlist (:3507-3524), unless already known for every entry
-    if (!sl.satd_done) {
+    if (sl.satd_done) {
+        if (c.elig) c.satd = m.sm.list_satd[m.lane];
+    } else {
+        const unsigned em = __ballot_sync(FULL, c.elig);
+        const int pos = __popc(em & ((1u << m.lane) - 1));
         int2* el = m.sm.batch + 16;
-        int ne = 0;
-        for (int i = 0; i < nk; ++i) {
-            const uint64_t s = m.sm.batch_cost[i];
-            if (s < UINT64_MAX / 8 && s <= limit) {
-                if (m.lane == 0) el[ne] = m.sm.batch[i];
-                ++ne;
-            }
-        }
+        if (c.elig) el[pos] = c.mv;
         __syncwarp();
-        satd_batch(P, m, el, ne, bx, by, bw, bh, mode, m.sm.list_satd + 8);
+        satd_batch(P, m, el, __popc(em), bx, by, bw, bh, mode, m.sm.list_satd + 8);
+        if (c.elig) c.satd = m.sm.list_satd[8 + pos];
     }
-    // final order (:3526-3531): eligible first, score, satd, sad, tie
-    int best = -1, ei = 0;
-    unsigned __int128 bkey = 0;
-    uint64_t bsatd = 0, bsad = 0;
-    for (int i = 0; i < nk; ++i) {
-        const uint64_t s = m.sm.batch_cost[i];
-        const bool elig = s < UINT64_MAX / 8 && s <= limit;
-        const uint64_t satd = elig ? (sl.satd_done ? m.sm.list_satd[i] : m.sm.list_satd[8 + ei++]) : kBad;
-        const unsigned __int128 k = score_key(P, m.lam_m, m.lam_s, satd, m.sm.list_rate[i]);
-        bool better;
-        if (best < 0) better = true;
-        else {
-            const bool belig = m.sm.batch_cost[best] < UINT64_MAX / 8 && m.sm.batch_cost[best] <= limit;
-            if (elig != belig) better = elig;
-            else if (k != bkey) better = k < bkey;
-            else if (satd != bsatd) better = satd < bsatd;
-            else if (s != bsad) better = s < bsad;
-            else better = tie_less(m.sm.batch[i], m.sm.batch[best]);
-        }
-        if (better) {
-            best = i;
-            bkey = k;
-            bsatd = satd;
-            bsad = s;
-        }
-    }
-    const int2 res = m.sm.batch[best];
+    if (c.valid) c.key = score_key(P, m.lam_m, m.lam_s, c.satd, rate);
+    const SelCand best = warp_min8(c, final_less);
     __syncwarp();
-    return RefineOut{res, screen};
+    return RefineOut{best.mv, sl.screen};
 }
 
 __device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
@@ -1154,16 +1193,37 @@ struct SeedPick {
 __device__ __forceinline__ int l1_norm(int2 v) { return iabs(v.x) + iabs(v.y); }
 
 // The reference's seed choice over the scored slots: the first slot that attains the least
-// (SAD, |mv|_1); with skip_pred the predictor slot 2 takes no part.
+// (SAD, |mv|_1); with skip_pred the predictor slot 2 takes no part. A warp reduction over
+// lanes 0..10 by (SAD, |mv|_1, slot).
 __device__ __forceinline__ SeedPick pick_4mv_seed(const Mb& m, bool skip_pred) {
-    SeedPick b{m.sm.batch[0], m.sm.batch_cost[0], 0};
-    for (int s2 = 1; s2 <= 10; ++s2) {
-        if (skip_pred && s2 == 2) continue;
-        const int2 v = m.sm.batch[s2];
-        if (v.x == b.v.x && v.y == b.v.y) continue;
-        const uint64_t c = m.sm.batch_cost[s2];
-        if (c < b.cost || (c == b.cost && l1_norm(v) < l1_norm(b.v))) b = SeedPick{v, c, s2};
+    const int l = m.lane;
+    bool valid = l <= 10 && !(skip_pred && l == 2);
+    int2 v = valid ? m.sm.batch[l] : make_int2(0, 0);
+    uint64_t c = valid ? m.sm.batch_cost[l] : 0;
+    int slot = l;
+#pragma unroll
+    for (int o = 8; o; o >>= 1) {
+        const bool ov = __shfl_xor_sync(FULL, valid, o);
+        const uint64_t oc = __shfl_xor_sync(FULL, c, o);
+        const int ox = __shfl_xor_sync(FULL, v.x, o), oy = __shfl_xor_sync(FULL, v.y, o);
+        const int os = __shfl_xor_sync(FULL, slot, o);
+        const int2 ovv = make_int2(ox, oy);
+        bool take = false;
+        if (ov && !valid) take = true;
+        else if (ov) {
+            if (oc != c) take = oc < c;
+            else if (l1_norm(ovv) != l1_norm(v)) take = l1_norm(ovv) < l1_norm(v);
+            else take = os < slot;
+        }
+        if (take) {
+            valid = true;
+            c = oc;
+            v = ovv;
+            slot = os;
+        }
     }
+    SeedPick b{make_int2(__shfl_sync(FULL, v.x, 0), __shfl_sync(FULL, v.y, 0)), __shfl_sync(FULL, c, 0),
+               __shfl_sync(FULL, slot, 0)};
     __syncwarp();
     return b;
 }

@@ -87,6 +87,38 @@ __device__ __forceinline__ void predict_row(const S& s, bool bilinear, int rnd, 
     for (int i = 0; i < N; ++i) out[i] = iclamp(arshift(mspel(r[i], r[i + 1], r[i + 2], r[i + 3], hm) + bias, sh), 0, 255);
 }
 
+template <int N>
+struct PredRow {
+    int v[N];
+};
+
+// predict_row over HBM with clamped coordinates, out of line: the rarely taken path of the
+// shared-window scorers, kept out of their instruction stream.
+template <int N>
+__device__ __noinline__ PredRow<N> predict_row_glob(const uint8_t* p, int pitch, int W, int H, bool bilinear, int rnd, int xq,
+                                                   int yq, int px, int py) {
+    PredRow<N> r;
+    predict_row<N>(GlobSampler{p, pitch, W, H}, bilinear, rnd, xq, yq, px, py, r.v);
+    return r;
+}
+
+// Horizontal 4-point Hadamard of one residual row (the row stage of satd4x4_scalar).
+__device__ __forceinline__ int4 hadamard_row(int d0, int d1, int d2, int d3) {
+    const int a0 = d0 + d3, a1 = d1 + d2, a2 = d1 - d2, a3 = d0 - d3;
+    return make_int4(a0 + a1, a3 + a2, a0 - a1, a3 - a2);
+}
+
+// Column stage of satd4x4_scalar over four row-transformed rows, with its (tile + 1) >> 1.
+__device__ __forceinline__ uint32_t hadamard_cols(const int4& r0, const int4& r1, const int4& r2, const int4& r3) {
+    auto col = [](int t0, int t1, int t2, int t3) {
+        const int a0 = t0 + t3, a1 = t1 + t2, a2 = t1 - t2, a3 = t0 - t3;
+        return (uint32_t)iabs(a0 + a1) + (uint32_t)iabs(a3 + a2) + (uint32_t)iabs(a0 - a1) + (uint32_t)iabs(a3 - a2);
+    };
+    const uint32_t tile = col(r0.x, r1.x, r2.x, r3.x) + col(r0.y, r1.y, r2.y, r3.y) + col(r0.z, r1.z, r2.z, r3.z) +
+                          col(r0.w, r1.w, r2.w, r3.w);
+    return (tile + 1) >> 1;
+}
+
 // 4x4 Hadamard SATD of a residual tile, satd4x4_scalar (encoder_motion.cpp:2936-2958).
 __device__ __forceinline__ uint32_t satd4x4(const int d[16]) {
     int t[16];
