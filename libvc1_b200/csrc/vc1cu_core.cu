@@ -1114,10 +1114,86 @@ __device__ RefineOut refine_select(const DevParams& P, const Mb& m, const Shortl
     return RefineOut{best.mv, sl.screen};
 }
 
+// ---- out-of-line refinement ---------------------------------------------------------------
+//
+// The staged refinement is reached from several places of the kernel; one out-of-line copy
+// of each half keeps the kernel's instruction footprint small enough for the instruction
+// cache. Only values cross the call (never the address of the kernel's parameter block or
+// of the macroblock state), so the caller's state stays in registers.
+
+struct RefCtx {
+    ScoreGeo g;
+    int subpel, fast_subpel, subpel_range, me_quality, mvrange, mant_bits, lam_s;
+    uint64_t lam_m;
+    BatchCtx bc;
+    uint32_t batch, cost, satd;  // the warp's shortlist buffers
+};
+
+__device__ __forceinline__ RefCtx ref_ctx(const DevParams& P, const Mb& m) {
+    RefCtx r;
+    r.g = score_geo(P);
+    r.subpel = P.subpel;
+    r.fast_subpel = P.fast_subpel;
+    r.subpel_range = P.subpel_range;
+    r.me_quality = P.me_quality;
+    r.mvrange = P.mvrange;
+    r.mant_bits = P.mant_bits;
+    r.lam_s = m.lam_s;
+    r.lam_m = m.lam_m;
+    r.bc = batch_ctx(m);
+    r.batch = m.sm.batch.off;
+    r.cost = m.sm.batch_cost.off;
+    r.satd = m.sm.list_satd.off;
+    return r;
+}
+
+// The parameter block and macroblock state the refinement reads, rebuilt from a RefCtx.
+__device__ __forceinline__ void ref_unpack(const RefCtx& r, DevParams& P, Mb& m) {
+    P = geo_params(r.g);
+    P.subpel = r.subpel;
+    P.fast_subpel = r.fast_subpel;
+    P.subpel_range = r.subpel_range;
+    P.me_quality = r.me_quality;
+    P.mvrange = r.mvrange;
+    P.mant_bits = r.mant_bits;
+    m.lane = r.bc.lane;
+    m.lam_m = r.lam_m;
+    m.lam_s = r.lam_s;
+    m.x0 = r.bc.x0;
+    m.y0 = r.bc.y0;
+    m.wx0 = r.bc.wx0;
+    m.wy0 = r.bc.wy0;
+    m.wp = r.bc.wp;
+    m.wh = r.bc.wh;
+    m.gref = GlobSampler{r.bc.gref, r.bc.gpitch, P.W, P.H};
+    m.sm.win.off = r.bc.win_off;
+    m.sm.cur.off = r.bc.cur_off;
+    m.sm.batch.off = r.batch;
+    m.sm.batch_cost.off = r.cost;
+    m.sm.list_satd.off = r.satd;
+}
+
+__device__ __noinline__ Shortlist refine_prepare_ool(const RefCtx r, int bx, int by, int bw, int bh, int2 seed, int range,
+                                                     int mode, uint64_t known, bool satd_all) {
+    DevParams P;
+    Mb m{};
+    ref_unpack(r, P, m);
+    return refine_prepare(P, m, bx, by, bw, bh, seed, range, mode, known, satd_all);
+}
+
+__device__ __noinline__ RefineOut refine_select_ool(const RefCtx r, const Shortlist sl, int bx, int by, int bw, int bh,
+                                                    int mode, const PInfo pi, bool more) {
+    DevParams P;
+    Mb m{};
+    ref_unpack(r, P, m);
+    return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
+}
+
 __device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
                                                    int range, int mode, const PInfo& pi, bool more, uint64_t known) {
-    const Shortlist sl = refine_prepare(P, m, bx, by, bw, bh, seed, range, mode, known, false);
-    return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
+    const RefCtx r = ref_ctx(P, m);
+    const Shortlist sl = refine_prepare_ool(r, bx, by, bw, bh, seed, range, mode, known, false);
+    return refine_select_ool(r, sl, bx, by, bw, bh, mode, pi, more);
 }
 
 // ---- shortlists parked across the wavefront wait -----------------------------------------
@@ -1664,7 +1740,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
                 PHASE_MARK(2);
-                sl = refine_prepare(P, m, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
+                sl = refine_prepare_ool(ref_ctx(P, m), m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
                 PHASE_MARK(3);
                 dl = __ldcg(&d.seed_dl[m.pos]);
                 dc = __ldcg(&d.seed_dc[m.pos]);
@@ -1674,14 +1750,14 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                     const Field fg{m.sm.cur_bmv, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
                     const PInfo pig = predictor_mixed_1mv(P, fg, m.mx, m.my);
                     shortlist_save(m, 0, sl, seed, 0, 0);
-                    one_g = refine_select(P, m, sl, m.x0, m.y0, 16, 16, one_mode, pig, true).mv;
+                    one_g = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, pig, true).mv;
                     if (hidden_padding(P, m.x0, m.y0, 16, 16, one_g.x, one_g.y, one_mode, true)) one_g = make_int2(0, 0);
                     for (int k = 0; k < 4; ++k) {
                         const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
                         put_4mv_seeds(P, m, one_g, one_g, qb);
                         sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
                         const SeedPick b = pick_4mv_seed(m, true);
-                        const Shortlist sk = refine_prepare(P, m, bx, by, 8, 8, b.v, range, VC1CU_MV_MIXED, b.cost, true);
+                        const Shortlist sk = refine_prepare_ool(ref_ctx(P, m), bx, by, 8, 8, b.v, range, VC1CU_MV_MIXED, b.cost, true);
                         shortlist_save(m, k + 1, sk, b.v, b.cost, b.slot);
                     }
                     PHASE_MARK(12);
@@ -1709,7 +1785,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             PHASE_MARK(6);
             if (seeded) {
                 if (spec4) shortlist_restore(m, 0);
-                one = refine_select(P, m, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+                one = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
             } else {
                 const PInfo pi = predictor_info(P, m);
                 const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
@@ -1761,7 +1837,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                             seed_cost = c2;
                         } else {
                             const Shortlist sk = shortlist_restore(m, k + 1);
-                            r = refine_select(P, m, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
+                            r = refine_select_ool(ref_ctx(P, m), sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
                             have = true;
                         }
                     } else {
