@@ -528,6 +528,8 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         if (d.seeded && d.seed_pass < 0) {
             ResultSlot& s = result_slot(c, q.seed_slot, mbs, false);
             d.seed_mvs = s.r.mvs;
+            d.seed_bmv = s.r.bmv;
+            d.seed_intra = s.r.intra;
             d.seed_dl = s.r.dl;
             d.seed_dc = s.r.dc;
             d.seed_dd = s.r.dd;
@@ -561,6 +563,8 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         if (h[i].seed_pass >= 0) {
             const DevResult& so = h[h[i].seed_pass].out;
             h[i].seed_mvs = so.mvs;
+            h[i].seed_bmv = so.bmv;
+            h[i].seed_intra = so.intra;
             h[i].seed_dl = so.dl;
             h[i].seed_dc = so.dc;
             h[i].seed_dd = so.dd;

@@ -670,16 +670,23 @@ struct RefineOut {
     uint64_t screen_sad;
 };
 
-// A shortlist parked in shared memory while the warp waits on its neighbours, with the
-// 4MV seed it was refined from (slot k + 1 of block k).
+// A refinement worked out before the wavefront wait under a guessed predictor and parked in
+// shared memory (slot 0: the 16x16 refinement; slot k + 1: 8x8 block k): its shortlist,
+// the 4MV seed it was refined from (with and without the predictor slot), the guessed
+// predictor and the result under it.
 struct SpecBlk {
     int2 seed;
     uint64_t seed_cost;
     int seed_slot, nk, direct, satd_done;
     uint64_t screen;
     RefineOut out;
+    int2 b10;            // the seed chosen without the predictor slot
+    uint64_t b10_cost;
+    int b10_slot;
+    RefineOut res;       // refine_select under `pi`
+    PInfo pi;
 };
-constexpr int kSpecBlkBytes = 64;
+constexpr int kSpecBlkBytes = 160;
 static_assert(sizeof(SpecBlk) <= kSpecBlkBytes, "SpecBlk layout");
 
 __device__ __forceinline__ int make_even(int v) { return !(v & 1) ? v : (v > 0 ? v - 1 : v + 1); }
@@ -1331,17 +1338,32 @@ __device__ void load_neighbours(const DevParams& P, const Mb& m, const DevResult
 }
 
 // A stand-in neighbourhood for guessing before the wavefront wait: the seed pass's final
-// 1-MV vectors of the same four neighbours (that pass is complete), no intra neighbours,
-// and a zero current MB.
-__device__ void guess_neighbours(const DevParams& P, const Mb& m, const int2* seed_mvs) {
+// vectors and P-intra flags of the same four neighbours (that pass is complete), and a
+// zero current MB.
+__device__ void guess_neighbours(const DevParams& P, const Mb& m, const PassDesc& d) {
     const int q = m.lane < 16 ? (m.lane >> 2) : (m.lane & 3);
     const int nx = m.mx + (q == 0 || q == 1 ? -1 : (q == 2 ? 0 : 1)), ny = m.my - (q == 0 ? 0 : 1);
     const bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
     const int nb = ny * P.mbw + nx;
-    if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&seed_mvs[nb]) : make_int2(0, 0);
-    else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&seed_mvs[nb]) : make_int2(0, 0);
-    else if (m.lane < 24) m.sm.nb_intra[q] = 0;
+    if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&d.seed_bmv[nb * 4 + (m.lane & 3)]) : make_int2(0, 0);
+    else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&d.seed_mvs[nb]) : make_int2(0, 0);
+    else if (m.lane < 24) m.sm.nb_intra[q] = valid ? (int)__ldcg(&d.seed_intra[nb]) : 0;
     else if (m.lane < 28) m.sm.cur_bmv[m.lane - 24] = make_int2(0, 0);
+    __syncwarp();
+}
+
+__device__ __forceinline__ bool pinfo_equal(const PInfo& a, const PInfo& b) {
+    return a.pre.x == b.pre.x && a.pre.y == b.pre.y && a.a.x == b.a.x && a.a.y == b.a.y && a.c.x == b.c.x &&
+           a.c.y == b.c.y && a.a_valid == b.a_valid && a.c_valid == b.c_valid && a.hybrid == b.hybrid;
+}
+
+// Parks the guessed predictor and the result under it in slot `slot`.
+__device__ __forceinline__ void spec_result_save(const Mb& m, int slot, const PInfo& pi, const RefineOut& res) {
+    if (m.lane == 0) {
+        SpecBlk& b = m.sm.spec_blk[slot];
+        b.pi = pi;
+        b.res = res;
+    }
     __syncwarp();
 }
 
@@ -1730,7 +1752,12 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         uint64_t intra_sad = 0;
         // Mixed-MV speculation: the 4MV block work for a guessed 1-MV vector runs before the
         // wait and is kept when the vector chosen after it matches (seeds from earlier launches)
-        const bool spec4 = allow_4mv && seeded && d.seed_pass < 0;
+        // Speculation: with the seed pass's neighbourhood standing in for this pass's, the
+        // refinements (and for Mixed-MV every block's) run before the wait; after it each
+        // result is kept where the real predictor equals the guessed one (seeds produced by
+        // earlier launches only)
+        const bool spec = seeded && d.seed_pass < 0;
+        const bool spec4 = allow_4mv && spec;
         int2 one_g = make_int2(0, 0);
         if (ok) {
             if (seeded) {
@@ -1745,20 +1772,39 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 dl = __ldcg(&d.seed_dl[m.pos]);
                 dc = __ldcg(&d.seed_dc[m.pos]);
                 dd = __ldcg(&d.seed_dd[m.pos]);
-                if (spec4) {
-                    guess_neighbours(P, m, d.seed_mvs);
-                    const Field fg{m.sm.cur_bmv, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
+                if (spec) {
+                    guess_neighbours(P, m, d);
+                    int2* cur4g = m.sm.cur_bmv;
+                    const Field fg{cur4g, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
                     const PInfo pig = predictor_mixed_1mv(P, fg, m.mx, m.my);
                     shortlist_save(m, 0, sl, seed, 0, 0);
-                    one_g = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, pig, true).mv;
+                    const RefineOut og = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, pig, true);
+                    spec_result_save(m, 0, pig, og);
+                    one_g = og.mv;
                     if (hidden_padding(P, m.x0, m.y0, 16, 16, one_g.x, one_g.y, one_mode, true)) one_g = make_int2(0, 0);
-                    for (int k = 0; k < 4; ++k) {
-                        const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
-                        put_4mv_seeds(P, m, one_g, one_g, qb);
-                        sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
-                        const SeedPick b = pick_4mv_seed(m, true);
-                        const Shortlist sk = refine_prepare_ool(ref_ctx(P, m), bx, by, 8, 8, b.v, range, VC1CU_MV_MIXED, b.cost, true);
-                        shortlist_save(m, k + 1, sk, b.v, b.cost, b.slot);
+                    if (spec4) {
+                        if (m.lane < 4) cur4g[m.lane] = one_g;
+                        __syncwarp();
+                        for (int k = 0; k < 4; ++k) {
+                            const int bx = m.x0 + (k & 1) * 8, by = m.y0 + ((k >> 1) & 1) * 8;
+                            const PInfo pi4g = predictor_4mv(P, fg, m.mx, m.my, k);
+                            put_4mv_seeds(P, m, one_g, pi4g.pre, qb);
+                            sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
+                            const SeedPick b10 = pick_4mv_seed(m, true);
+                            const SeedPick bf = pick_4mv_seed(m, false);
+                            const RefCtx rc = ref_ctx(P, m);
+                            const Shortlist sk = refine_prepare_ool(rc, bx, by, 8, 8, bf.v, range, VC1CU_MV_MIXED, bf.cost, true);
+                            shortlist_save(m, k + 1, sk, bf.v, bf.cost, bf.slot);
+                            const RefineOut rk = refine_select_ool(rc, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4g, true);
+                            if (m.lane == 0) {
+                                SpecBlk& sb = m.sm.spec_blk[k + 1];
+                                sb.b10 = b10.v;
+                                sb.b10_cost = b10.cost;
+                                sb.b10_slot = b10.slot;
+                                cur4g[k] = rk.mv;
+                            }
+                            spec_result_save(m, k + 1, pi4g, rk);
+                        }
                     }
                     PHASE_MARK(12);
                 }
@@ -1784,8 +1830,12 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             RefineOut one;
             PHASE_MARK(6);
             if (seeded) {
-                if (spec4) shortlist_restore(m, 0);
-                one = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+                if (spec && pinfo_equal(rate_pi, m.sm.spec_blk[0].pi)) {
+                    one = m.sm.spec_blk[0].res;
+                } else {
+                    if (spec) shortlist_restore(m, 0);
+                    one = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+                }
             } else {
                 const PInfo pi = predictor_info(P, m);
                 const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
@@ -1824,21 +1874,29 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                     bool have = false;
                     int2 best_seed;
                     uint64_t seed_cost;
-                    if (hit) {
+                    const SpecBlk& sb = m.sm.spec_blk[k + 1];
+                    if (hit && pinfo_equal(pi4, sb.pi)) {
+                        // same seeds, same shortlist, same predictor: the parked result
+                        r = sb.res;
+                        have = true;
+                    } else if (hit) {
                         // the parked seed search covered every slot but the predictor's
                         put_4mv_seeds(P, m, one.mv, pi4.pre, qb);
                         const int2 v2 = m.sm.batch[2];
                         sad_batch(P, m, m.sm.batch + 2, 1, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost + 2);
                         const uint64_t c2 = m.sm.batch_cost[2];
-                        const SpecBlk& sb = m.sm.spec_blk[k + 1];
-                        const SeedPick b{sb.seed, sb.seed_cost, sb.seed_slot};
+                        const SeedPick b{sb.b10, sb.b10_cost, sb.b10_slot};
                         if (seed_before(v2, c2, 2, b)) {
                             best_seed = v2;
                             seed_cost = c2;
-                        } else {
+                        } else if (sb.seed_slot != 2) {
+                            // the parked shortlist was refined from this same seed
                             const Shortlist sk = shortlist_restore(m, k + 1);
                             r = refine_select_ool(ref_ctx(P, m), sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
                             have = true;
+                        } else {
+                            best_seed = b.v;
+                            seed_cost = b.cost;
                         }
                     } else {
                         put_4mv_seeds(P, m, one.mv, pi4.pre, qb);

@@ -47,6 +47,8 @@ struct PassDesc {
     int seeded;            // 1: seed fields below are valid
     int seed_pass;         // index of the seeding pass in the same launch, -1 if produced earlier
     const int2* seed_mvs;
+    const int2* seed_bmv;        // the seed pass's block vectors and P-intra flags (only used to
+    const uint8_t* seed_intra;   // guess this pass's predictors before the wavefront wait)
     const double* seed_dl;
     const double* seed_dc;
     const uint8_t* seed_dd;
