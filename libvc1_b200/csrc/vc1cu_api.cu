@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -495,7 +496,7 @@ int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1
 }
 
 // Launches a batch of independent core passes (global search first for unseeded ones).
-int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
+int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
     DevParams P;
     std::string why;
     int rc = make_dev_params(p, P, why);
@@ -546,11 +547,7 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
             unseeded.push_back(i);
         }
     }
-    for (int i = 0; i < n; ++i) {
-        for (int j = 0; j < i; ++j)
-            if (passes[j].out_slot == passes[i].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
-        h[i].out = result_slot(c, passes[i].out_slot, mbs, true).r;
-    }
+    for (int i = 0; i < n; ++i) h[i].out = result_slot(c, passes[i].out_slot, mbs, true).r;
     // seed levels of in-launch seeds (a chain, never a cycle)
     std::vector<int> level(n, 0);
     for (int i = 0; i < n; ++i) {
@@ -654,7 +651,10 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     const long need = (items + warps - 1) / warps;
     const int grid = (int)std::max(1L, std::min<long>((long)per_sm * c->sm_count, need));
     if (++c->epoch == 0) c->epoch = 1;
-    ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
+    // only the work counter restarts: an error (and its abort flag) stays until check_status reports it
+    ck(cudaMemsetAsync(reinterpret_cast<char*>(c->d_status) + offsetof(LaunchStatus, queue), 0, sizeof(unsigned int),
+                       c->stream),
+       "cudaMemsetAsync(status)");
     {
         Timer tm(c, kCore);
         unsigned nitems = 0;
@@ -675,11 +675,45 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     return VC1CU_OK;
 }
 
+// Launches a batch of core passes. Passes of different kinds (seeded or not, MV mode, P-intra)
+// run as separate launches in the order the kinds first appear: each launch then executes
+// one code path, whose instructions stay in the SMs' instruction caches. A batch in which a
+// pass is seeded by another pass of the same batch runs as one launch.
+int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
+    bool chained = false;
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) {
+            if (j < i && passes[j].out_slot == passes[i].out_slot)
+                throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
+            if (passes[i].seed_slot >= 0 && passes[j].out_slot == passes[i].seed_slot) chained = true;
+        }
+    }
+    if (n <= 1 || chained) return launch_group(c, p, passes, n);
+    std::vector<int> keys;
+    std::vector<std::vector<vc1cu_pass>> groups;
+    for (int i = 0; i < n; ++i) {
+        const int key = (passes[i].seed_slot >= 0 ? 8 : 0) + 2 * passes[i].mode + (passes[i].allow_intra ? 1 : 0);
+        size_t g = 0;
+        while (g < keys.size() && keys[g] != key) ++g;
+        if (g == keys.size()) {
+            keys.push_back(key);
+            groups.emplace_back();
+        }
+        groups[g].push_back(passes[i]);
+    }
+    for (const auto& g : groups) launch_group(c, p, g.data(), (int)g.size());
+    return VC1CU_OK;
+}
+
 int check_status(vc1cu_ctx* c) {
     LaunchStatus st{};
     ck(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(status)");
     sync_checked(c);
-    if (st.error) throw Fail{st.error, "a wavefront wait timed out on the device (" + std::to_string(st.timeouts) + " waits)"};
+    if (st.error) {
+        ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
+        sync_checked(c);
+        throw Fail{st.error, "a wavefront wait timed out on the device (" + std::to_string(st.timeouts) + " waits)"};
+    }
     return VC1CU_OK;
 }
 

@@ -728,6 +728,7 @@ __device__ __forceinline__ void reg_add(const DevParams& P, const Mb& m, RegList
                                         int bw, int bh, int mode) {
     const bool act = m.lane < nb;
     bool listed = false;
+#pragma unroll 1
     for (int i = 0; i < nb; ++i) {
         const int cx = __shfl_sync(FULL, c.x, i), cy = __shfl_sync(FULL, c.y, i);
         const bool hit = __any_sync(FULL, m.lane < L.n && L.mv.x == cx && L.mv.y == cy);
@@ -759,6 +760,7 @@ __device__ __forceinline__ void reg_add(const DevParams& P, const Mb& m, RegList
 __device__ __forceinline__ void reg_update_min(const Mb& m, const RegList& L, int2 c, int nb, int2& best,
                                                uint64_t& best_sad) {
     bool in_st = false;
+#pragma unroll 1
     for (int i = 0; i < nb; ++i) {
         const int cx = __shfl_sync(FULL, c.x, i), cy = __shfl_sync(FULL, c.y, i);
         in_st |= m.lane < L.n && L.mv.x == cx && L.mv.y == cy;
@@ -985,6 +987,7 @@ __device__ __forceinline__ Shortlist refine_prepare(const DevParams& P, const Mb
     // sort by (sad, tie_less), keep 8 / 4 (:3445-3456): rank of each entry by shuffles
     const int keep = fast ? 4 : 8;
     int rank = 0;
+#pragma unroll 1
     for (int k = 0; k < L.n; ++k) {
         const uint64_t sk = __shfl_sync(FULL, L.sad, k);
         const int kx = __shfl_sync(FULL, L.mv.x, k), ky = __shfl_sync(FULL, L.mv.y, k);
