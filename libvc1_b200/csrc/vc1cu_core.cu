@@ -116,6 +116,94 @@ __device__ __forceinline__ bool win_inside(const Mb& m, int xa, int ya, int xb, 
     return xa >= m.wx0 && ya >= m.wy0 && xb < m.wx0 + m.wp && yb < m.wy0 + m.wh;
 }
 
+// SAD of one row segment of n <= 8 visible pixels against the current block at shared
+// byte offset `cur`: the same predictions as predict_row<8> (sx = px + floor(xq/4) ...),
+// evaluated with rolled loops and sliding windows so that each interpolation case is a few
+// dozen instructions rather than an unrolled block.
+template <class S>
+__device__ __forceinline__ uint32_t sad_row8(const S& s, bool bilinear, int rnd, int xq, int yq, int px, int py, uint32_t cur,
+                                             int n) {
+    const int ix = floor_div4(xq), iy = floor_div4(yq);
+    const int hm = xq - ix * 4, vm = yq - iy * 4;
+    const int sx = px + ix, sy = py + iy;
+    uint32_t acc = 0;
+    if (!hm && !vm) {
+#pragma unroll 1
+        for (int i = 0; i < n; ++i) acc += (uint32_t)iabs((int)g_smem[cur + i] - s(sx + i, sy));
+        return acc;
+    }
+    if (bilinear) {
+        if (hm && vm) {
+            const int r = rnd ? 1 : 2;
+            int a0 = s(sx, sy) + s(sx, sy + 1);
+#pragma unroll 1
+            for (int i = 0; i < n; ++i) {
+                const int a1 = s(sx + i + 1, sy) + s(sx + i + 1, sy + 1);
+                acc += (uint32_t)iabs((int)g_smem[cur + i] - ((a0 + a1 + r) >> 2));
+                a0 = a1;
+            }
+        } else if (hm) {
+            const int r = rnd ? 0 : 1;
+            int a0 = s(sx, sy);
+#pragma unroll 1
+            for (int i = 0; i < n; ++i) {
+                const int a1 = s(sx + i + 1, sy);
+                acc += (uint32_t)iabs((int)g_smem[cur + i] - ((a0 + a1 + r) >> 1));
+                a0 = a1;
+            }
+        } else {
+            const int r = rnd ? 0 : 1;
+#pragma unroll 1
+            for (int i = 0; i < n; ++i)
+                acc += (uint32_t)iabs((int)g_smem[cur + i] - ((s(sx + i, sy) + s(sx + i, sy + 1) + r) >> 1));
+        }
+        return acc;
+    }
+    if (hm && vm) {
+        const int shift = ((hm == 2 ? 1 : 5) + (vm == 2 ? 1 : 5)) >> 1;
+        const int r1 = (1 << (shift - 1)) + (rnd ? 1 : 0) - 1;
+        const Taps tv = mspel_taps(vm), th = mspel_taps(hm);
+        auto col = [&](int x) { return arshift(apply(tv, s(x, sy - 1), s(x, sy), s(x, sy + 1), s(x, sy + 2)) + r1, shift); };
+        int t0 = col(sx - 1), t1 = col(sx), t2 = col(sx + 1);
+#pragma unroll 1
+        for (int i = 0; i < n; ++i) {
+            const int t3 = col(sx + i + 2);
+            const int v = iclamp(arshift(apply(th, t0, t1, t2, t3) + 64 - (rnd ? 1 : 0), 7), 0, 255);
+            acc += (uint32_t)iabs((int)g_smem[cur + i] - v);
+            t0 = t1;
+            t1 = t2;
+            t2 = t3;
+        }
+        return acc;
+    }
+    if (vm) {
+        const int bias = (vm == 2) ? (7 + (rnd ? 1 : 0)) : (31 + (rnd ? 1 : 0));
+        const int sh = vm == 2 ? 4 : 6;
+        const Taps tv = mspel_taps(vm);
+#pragma unroll 1
+        for (int i = 0; i < n; ++i) {
+            const int x = sx + i;
+            const int v = iclamp(arshift(apply(tv, s(x, sy - 1), s(x, sy), s(x, sy + 1), s(x, sy + 2)) + bias, sh), 0, 255);
+            acc += (uint32_t)iabs((int)g_smem[cur + i] - v);
+        }
+        return acc;
+    }
+    const int bias = (hm == 2) ? (8 - (rnd ? 1 : 0)) : (32 - (rnd ? 1 : 0));
+    const int sh = hm == 2 ? 4 : 6;
+    const Taps th = mspel_taps(hm);
+    int r0 = s(sx - 1, sy), r1 = s(sx, sy), r2 = s(sx + 1, sy);
+#pragma unroll 1
+    for (int i = 0; i < n; ++i) {
+        const int r3 = s(sx + i + 2, sy);
+        const int v = iclamp(arshift(apply(th, r0, r1, r2, r3) + bias, sh), 0, 255);
+        acc += (uint32_t)iabs((int)g_smem[cur + i] - v);
+        r0 = r1;
+        r1 = r2;
+        r2 = r3;
+    }
+    return acc;
+}
+
 // 16 shared-memory bytes starting at byte offset `off`, as four little-endian words.
 __device__ __forceinline__ void win_load16(uint32_t off, uint32_t r[4]) {
     const uint32_t w = off >> 2;
@@ -270,18 +358,16 @@ __device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, 
             bad = hidden_padding(P, bx, by, bw, bh, mv.x, mv.y, mode, cg) || (bil && ((mv.x & 1) || (mv.y & 1)));
             if (!bad && r < ah && c0 < aw) {
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
-                int pred[8];
+                const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
+                const int nvis = imin(8, aw - c0);
                 if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1)) {
-                    predict_row<8>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, pred);
+                    part = sad_row8(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, cp, nvis);
                 } else {
                     const PredRow<8> g8 = predict_row_glob<8>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + c0, by + r);
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) pred[i] = g8.v[i];
+                    for (int i = 0; i < 8; ++i)
+                        if (i < nvis) part += (uint32_t)iabs((int)g_smem[cp + i] - g8.v[i]);
                 }
-                const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    if (c0 + i < aw) part += (uint32_t)iabs((int)g_smem[cp + i] - pred[i]);
             }
         }
         for (int o = segs >> 1; o; o >>= 1) part += __shfl_xor_sync(FULL, part, o);

@@ -87,6 +87,17 @@ __device__ __forceinline__ void predict_row(const S& s, bool bilinear, int rnd, 
     for (int i = 0; i < N; ++i) out[i] = iclamp(arshift(mspel(r[i], r[i + 1], r[i + 2], r[i + 3], hm) + bias, sh), 0, 255);
 }
 
+// mspel_filter4 taps of a quarter-pel phase (1: 1/4, 2: 1/2, 3: 3/4).
+struct Taps {
+    int w0, w1, w2, w3;
+};
+__device__ __forceinline__ Taps mspel_taps(int mode) {
+    return mode == 1 ? Taps{-4, 53, 18, -3} : mode == 2 ? Taps{-1, 9, 9, -1} : Taps{-3, 18, 53, -4};
+}
+__device__ __forceinline__ int apply(const Taps& t, int a, int b, int c, int d) {
+    return t.w0 * a + t.w1 * b + t.w2 * c + t.w3 * d;
+}
+
 template <int N>
 struct PredRow {
     int v[N];
