@@ -204,6 +204,72 @@ __device__ __forceinline__ uint32_t sad_row8(const S& s, bool bilinear, int rnd,
     return acc;
 }
 
+// The four predictions of predict_row<4>, evaluated like sad_row8 (rolled loops with
+// sliding windows), delivered through a four-register queue.
+template <class S>
+__device__ __forceinline__ int4 pred_row4(const S& s, bool bilinear, int rnd, int xq, int yq, int px, int py) {
+    const int ix = floor_div4(xq), iy = floor_div4(yq);
+    const int hm = xq - ix * 4, vm = yq - iy * 4;
+    const int sx = px + ix, sy = py + iy;
+    int q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+    auto push = [&](int v) {
+        q0 = q1;
+        q1 = q2;
+        q2 = q3;
+        q3 = v;
+    };
+    if (!hm && !vm) {
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) push(s(sx + i, sy));
+    } else if (bilinear) {
+        const int r2 = rnd ? 1 : 2, r1 = rnd ? 0 : 1;
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int x = sx + i;
+            push(hm && vm ? (s(x, sy) + s(x + 1, sy) + s(x, sy + 1) + s(x + 1, sy + 1) + r2) >> 2
+                 : hm     ? (s(x, sy) + s(x + 1, sy) + r1) >> 1
+                          : (s(x, sy) + s(x, sy + 1) + r1) >> 1);
+        }
+    } else if (hm && vm) {
+        const int shift = ((hm == 2 ? 1 : 5) + (vm == 2 ? 1 : 5)) >> 1;
+        const int r1 = (1 << (shift - 1)) + (rnd ? 1 : 0) - 1;
+        const Taps tv = mspel_taps(vm), th = mspel_taps(hm);
+        auto col = [&](int x) { return arshift(apply(tv, s(x, sy - 1), s(x, sy), s(x, sy + 1), s(x, sy + 2)) + r1, shift); };
+        int t0 = col(sx - 1), t1 = col(sx), t2 = col(sx + 1);
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int t3 = col(sx + i + 2);
+            push(iclamp(arshift(apply(th, t0, t1, t2, t3) + 64 - (rnd ? 1 : 0), 7), 0, 255));
+            t0 = t1;
+            t1 = t2;
+            t2 = t3;
+        }
+    } else if (vm) {
+        const int bias = (vm == 2) ? (7 + (rnd ? 1 : 0)) : (31 + (rnd ? 1 : 0));
+        const int sh = vm == 2 ? 4 : 6;
+        const Taps tv = mspel_taps(vm);
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int x = sx + i;
+            push(iclamp(arshift(apply(tv, s(x, sy - 1), s(x, sy), s(x, sy + 1), s(x, sy + 2)) + bias, sh), 0, 255));
+        }
+    } else {
+        const int bias = (hm == 2) ? (8 - (rnd ? 1 : 0)) : (32 - (rnd ? 1 : 0));
+        const int sh = hm == 2 ? 4 : 6;
+        const Taps th = mspel_taps(hm);
+        int r0 = s(sx - 1, sy), r1 = s(sx, sy), r2 = s(sx + 1, sy);
+#pragma unroll 1
+        for (int i = 0; i < 4; ++i) {
+            const int r3 = s(sx + i + 2, sy);
+            push(iclamp(arshift(apply(th, r0, r1, r2, r3) + bias, sh), 0, 255));
+            r0 = r1;
+            r1 = r2;
+            r2 = r3;
+        }
+    }
+    return make_int4(q0, q1, q2, q3);
+}
+
 // 16 shared-memory bytes starting at byte offset `off`, as four little-endian words.
 __device__ __forceinline__ void win_load16(uint32_t off, uint32_t r[4]) {
     const uint32_t w = off >> 2;
@@ -406,7 +472,11 @@ __device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c,
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
                 if (fast) {
-                    predict_row<4>(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy, pred);
+                    const int4 w4 = pred_row4(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy);
+                    pred[0] = w4.x;
+                    pred[1] = w4.y;
+                    pred[2] = w4.z;
+                    pred[3] = w4.w;
                 } else {
                     const PredRow<4> g4 = predict_row_glob<4>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + tx,
                                                               by + ty + yy);
@@ -795,7 +865,7 @@ __device__ __forceinline__ bool sad_tie_less(uint64_t sa, int2 a, uint64_t sb, i
 
 // Minimum over the lanes with `valid` of (s, v) under (sad, tie_less); the result on every lane.
 __device__ __forceinline__ void warp_argmin_sad(bool& valid, uint64_t& s, int2& v) {
-#pragma unroll
+#pragma unroll 1
     for (int o = 16; o; o >>= 1) {
         const bool ov = __shfl_xor_sync(FULL, valid, o);
         const uint64_t os = __shfl_xor_sync(FULL, s, o);
@@ -1143,7 +1213,7 @@ __device__ __forceinline__ bool final_less(const SelCand& a, const SelCand& b) {
 // Least candidate of lanes 0..7 under `less`, on every lane.
 template <class Less>
 __device__ __forceinline__ SelCand warp_min8(SelCand c, Less less) {
-#pragma unroll
+#pragma unroll 1
     for (int o = 4; o; o >>= 1) {
         const SelCand d = shfl_xor_cand(c, o);
         if (less(d, c)) c = d;
@@ -1373,7 +1443,7 @@ __device__ __forceinline__ SeedPick pick_4mv_seed(const Mb& m, bool skip_pred) {
     int2 v = valid ? m.sm.batch[l] : make_int2(0, 0);
     uint64_t c = valid ? m.sm.batch_cost[l] : 0;
     int slot = l;
-#pragma unroll
+#pragma unroll 1
     for (int o = 8; o; o >>= 1) {
         const bool ov = __shfl_xor_sync(FULL, valid, o);
         const uint64_t oc = __shfl_xor_sync(FULL, c, o);
