@@ -284,13 +284,13 @@ __device__ __forceinline__ void win_load16(uint32_t off, uint32_t r[4]) {
 
 // mb_sad of a full 16x16 MB from the window with packed byte SADs (__vsadu4), strides 1/2/4.
 template <int STRIDE>
-__device__ __forceinline__ uint32_t sad_packed(const Mb& m, uint32_t base) {
+__device__ __forceinline__ uint32_t sad_packed(uint32_t cur_off, uint32_t cur2_off, uint32_t cur4_off, int wp, uint32_t base) {
     uint32_t acc = 0;
-    const uint32_t c = m.sm.cur.off >> 2, c2 = m.sm.cur2.off >> 2, c4 = m.sm.cur4.off >> 2;
+    const uint32_t c = cur_off >> 2, c2 = cur2_off >> 2, c4 = cur4_off >> 2;
 #pragma unroll 4
     for (int y = 0; y < 16; y += STRIDE) {
         uint32_t r[4];
-        win_load16(base + (uint32_t)(y * m.wp), r);
+        win_load16(base + (uint32_t)(y * wp), r);
         if (STRIDE == 1) {
             acc += __vsadu4(r[0], g_smem32[c + y * 4 + 0]) + __vsadu4(r[1], g_smem32[c + y * 4 + 1]) +
                    __vsadu4(r[2], g_smem32[c + y * 4 + 2]) + __vsadu4(r[3], g_smem32[c + y * 4 + 3]);
@@ -311,50 +311,15 @@ template <int STRIDE, class S>
 __device__ __forceinline__ uint32_t sad_int_loop(const S& s, uint32_t cur, int x0, int y0, int dx, int dy, int aw,
                                                  int ah) {
     uint32_t acc = 0;
-#pragma unroll 4
+#pragma unroll 1
     for (int y = 0; y < ah; y += STRIDE) {
-#pragma unroll
+#pragma unroll 1
         for (int x = 0; x < 16; x += STRIDE) {
             if (x < aw) acc += (uint32_t)iabs((int)g_smem[cur + y * 16 + x] - s(x0 + x + dx, y0 + y + dy));
         }
     }
     return acc;
 }
-
-__device__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int stride) {
-    if (hidden_padding(P, m.x0, m.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
-    uint32_t s;
-    const bool fast = win_inside(m, m.x0 + dx, m.y0 + dy, m.x0 + dx + 15, m.y0 + dy + 15);
-    const WinSampler ws{m.sm.win.off, m.wp, m.wx0, m.wy0};
-    if (fast && m.aw == 16 && m.ah == 16) {
-        const uint32_t base = m.sm.win.off + (uint32_t)((m.y0 + dy - m.wy0) * m.wp + (m.x0 + dx - m.wx0));
-        if (stride == 1) s = sad_packed<1>(m, base);
-        else if (stride == 2) s = sad_packed<2>(m, base);
-        else s = sad_packed<4>(m, base);
-    } else if (fast) {
-        if (stride == 1) s = sad_int_loop<1>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else if (stride == 2) s = sad_int_loop<2>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else s = sad_int_loop<4>(ws, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-    } else {
-        if (stride == 1) s = sad_int_loop<1>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else if (stride == 2) s = sad_int_loop<2>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-        else s = sad_int_loop<4>(m.gref, m.sm.cur.off, m.x0, m.y0, dx, dy, m.aw, m.ah);
-    }
-    return stride > 1 ? (uint64_t)s * (uint64_t)(stride * stride) : (uint64_t)s;
-}
-
-// ---- sub-pel SAD / SATD batches (block_sad_motion :2670-2933, block_satd_motion :2960-3042)
-
-// Everything the out-of-line batch scorers read about the current macroblock, by value
-// (shared-memory buffers as byte offsets of g_smem, so the callee keeps shared addressing).
-struct BatchCtx {
-    uint32_t win_off, cur_off;
-    int wp, wx0, wy0, wh;
-    int x0, y0;
-    int lane;
-    const uint8_t* gref;
-    int gpitch;
-};
 
 // The picture geometry the scorers read (raster, rounding, cropped-padding flags), by value:
 // passing the kernel's parameter block by address would make every parameter read of the
@@ -384,6 +349,61 @@ __device__ __forceinline__ DevParams geo_params(const ScoreGeo& g) {
     P.cbottom_pad = (g.pads >> 3) & 1;
     return P;
 }
+
+// Everything the integer 16x16 SAD reads about the current macroblock, by value.
+struct IntSadCtx {
+    ScoreGeo g;
+    uint32_t win_off, cur_off, cur2_off, cur4_off;
+    int wp, wx0, wy0, wh, x0, y0, aw, ah;
+    const uint8_t* gref;
+    int gpitch;
+};
+
+// mb_sad at integer offset (dx, dy) and sampling stride 1/2/4 (encoder_motion.cpp:2197-2285);
+// one out-of-line copy serves every search stage.
+__device__ __noinline__ uint64_t mb_sad_core(const IntSadCtx c, int dx, int dy, int stride) {
+    const DevParams P = geo_params(c.g);
+    if (hidden_padding(P, c.x0, c.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
+    uint32_t s;
+    const int xa = c.x0 + dx, ya = c.y0 + dy;
+    const bool fast = xa >= c.wx0 && ya >= c.wy0 && xa + 15 < c.wx0 + c.wp && ya + 15 < c.wy0 + c.wh;
+    if (fast && c.aw == 16 && c.ah == 16) {
+        const uint32_t base = c.win_off + (uint32_t)((ya - c.wy0) * c.wp + (xa - c.wx0));
+        if (stride == 1) s = sad_packed<1>(c.cur_off, c.cur2_off, c.cur4_off, c.wp, base);
+        else if (stride == 2) s = sad_packed<2>(c.cur_off, c.cur2_off, c.cur4_off, c.wp, base);
+        else s = sad_packed<4>(c.cur_off, c.cur2_off, c.cur4_off, c.wp, base);
+    } else if (fast) {
+        const WinSampler ws{c.win_off, c.wp, c.wx0, c.wy0};
+        if (stride == 1) s = sad_int_loop<1>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+        else if (stride == 2) s = sad_int_loop<2>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+        else s = sad_int_loop<4>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+    } else {
+        const GlobSampler gs{c.gref, c.gpitch, P.W, P.H};
+        if (stride == 1) s = sad_int_loop<1>(gs, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+        else if (stride == 2) s = sad_int_loop<2>(gs, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+        else s = sad_int_loop<4>(gs, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+    }
+    return stride > 1 ? (uint64_t)s * (uint64_t)(stride * stride) : (uint64_t)s;
+}
+
+__device__ __forceinline__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int stride) {
+    const IntSadCtx c{score_geo(P), m.sm.win.off, m.sm.cur.off, m.sm.cur2.off, m.sm.cur4.off, m.wp, m.wx0, m.wy0, m.wh,
+                      m.x0, m.y0, m.aw, m.ah, m.gref.p, m.gref.pitch};
+    return mb_sad_core(c, dx, dy, stride);
+}
+
+// ---- sub-pel SAD / SATD batches (block_sad_motion :2670-2933, block_satd_motion :2960-3042)
+
+// Everything the out-of-line batch scorers read about the current macroblock, by value
+// (shared-memory buffers as byte offsets of g_smem, so the callee keeps shared addressing).
+struct BatchCtx {
+    uint32_t win_off, cur_off;
+    int wp, wx0, wy0, wh;
+    int x0, y0;
+    int lane;
+    const uint8_t* gref;
+    int gpitch;
+};
 
 __device__ __forceinline__ uint32_t soff(const void* p) {
     return (uint32_t)(reinterpret_cast<const uint8_t*>(p) - g_smem);
@@ -525,18 +545,20 @@ __device__ __forceinline__ bool seen_test_set(uint32_t* bits, int r, int dx, int
 // Merges the n keys of m.sm.keys (UINT64_MAX = skipped) into the sorted top-8 list
 // m.sm.top / m.sm.misc[0]. Keys below the current 8th entry are compacted with a ballot
 // first; the few survivors are ranked and merged on every lane identically.
-__device__ void top8_merge(const Mb& m, int n) {
-    uint64_t* keys = m.sm.keys;
-    uint64_t* top = m.sm.top;
-    const int tn = m.sm.misc[0];
+__device__ __noinline__ void top8_merge_core(int lane, uint32_t keys_off, uint32_t top_off, uint32_t misc_off,
+                                             uint32_t out8_off, int n) {
+    uint64_t* keys = reinterpret_cast<uint64_t*>(g_smem + keys_off);
+    uint64_t* top = reinterpret_cast<uint64_t*>(g_smem + top_off);
+    int* misc = reinterpret_cast<int*>(g_smem + misc_off);
+    const int tn = misc[0];
     const uint64_t bound = tn == 8 ? top[7] : UINT64_MAX;
     int cnt = 0;
     for (int base = 0; base < n; base += 32) {
-        const int i = base + m.lane;
+        const int i = base + lane;
         const uint64_t k = i < n ? keys[i] : UINT64_MAX;
         const bool take = k < bound;
         const unsigned b = __ballot_sync(FULL, take);
-        if (take) keys[cnt + __popc(b & ((1u << m.lane) - 1))] = k;
+        if (take) keys[cnt + __popc(b & ((1u << lane) - 1))] = k;
         cnt += __popc(b);
         __syncwarp();
     }
@@ -545,22 +567,22 @@ __device__ void top8_merge(const Mb& m, int n) {
     int ns = 0;
     if (cnt <= 32) {
         // rank of each survivor (keys are distinct), the 8 lowest ranks in order
-        const uint64_t k = m.lane < cnt ? keys[m.lane] : UINT64_MAX;
+        const uint64_t k = lane < cnt ? keys[lane] : UINT64_MAX;
         int rank = 0;
         for (int j = 0; j < cnt; ++j) rank += keys[j] < k;
         __syncwarp();
-        if (m.lane < cnt && rank < 8) keys[rank] = k;
+        if (lane < cnt && rank < 8) keys[rank] = k;
         __syncwarp();
         ns = cnt < 8 ? cnt : 8;
         sel = keys;
     } else {
-        uint64_t* out8 = m.sm.list_sad;  // idle during the integer search
+        uint64_t* out8 = reinterpret_cast<uint64_t*>(g_smem + out8_off);  // idle during the integer search
         for (int r = 0; r < 8; ++r) {
             uint64_t lm = UINT64_MAX;
-            for (int i = m.lane; i < cnt; i += 32) lm = keys[i] < lm ? keys[i] : lm;
+            for (int i = lane; i < cnt; i += 32) lm = keys[i] < lm ? keys[i] : lm;
             const uint64_t g = warp_min_u64(lm);
-            if (m.lane == 0) out8[r] = g;
-            for (int i = m.lane; i < cnt; i += 32)
+            if (lane == 0) out8[r] = g;
+            for (int i = lane; i < cnt; i += 32)
                 if (keys[i] == g) keys[i] = UINT64_MAX;
             __syncwarp();
         }
@@ -578,14 +600,18 @@ __device__ void top8_merge(const Mb& m, int n) {
         }
     }
     __syncwarp();
-    if (m.lane < o) {
+    if (lane < o) {
         uint64_t v = out[0];
 #pragma unroll
-        for (int q = 1; q < 8; ++q) if (m.lane == q) v = out[q];
-        top[m.lane] = v;
+        for (int q = 1; q < 8; ++q) if (lane == q) v = out[q];
+        top[lane] = v;
     }
-    if (m.lane == 0) m.sm.misc[0] = o;
+    if (lane == 0) misc[0] = o;
     __syncwarp();
+}
+
+__device__ __forceinline__ void top8_merge(const Mb& m, int n) {
+    top8_merge_core(m.lane, m.sm.keys.off, m.sm.top.off, m.sm.misc.off, m.sm.list_sad.off, n);
 }
 
 // Scores the candidates produced by gen(i) for i < n at sampled stride 2 (the UMH
