@@ -99,6 +99,7 @@ struct WarpMem {
     SPtr<uint64_t> spec_cost;   //   slot 0: the 16x16 refinement, slot k + 1: 8x8 block k
     SPtr<uint64_t> spec_satd;
     SPtr<SpecBlk> spec_blk;     // [5]
+    SPtr<uint8_t> ctx;          // the macroblock's MbCtx
 };
 
 struct Mb {
@@ -350,18 +351,28 @@ __device__ __forceinline__ DevParams geo_params(const ScoreGeo& g) {
     return P;
 }
 
-// Everything the integer 16x16 SAD reads about the current macroblock, by value.
-struct IntSadCtx {
+// The per-macroblock values the out-of-line search routines read. It lives in the warp's
+// shared memory (written once per macroblock, after its window is staged), and the routines
+// take only its offset, so no structure travels through the stack on a call.
+struct MbCtx {
     ScoreGeo g;
     uint32_t win_off, cur_off, cur2_off, cur4_off;
     int wp, wx0, wy0, wh, x0, y0, aw, ah;
     const uint8_t* gref;
     int gpitch;
+    int subpel, fast_subpel, subpel_range, me_quality, mvrange, mant_bits, lam_s;
+    uint64_t lam_m;
+    uint32_t batch, cost, satd;  // the warp's shortlist buffers
 };
+constexpr int kMbCtxBytes = 192;
+static_assert(sizeof(MbCtx) <= kMbCtxBytes, "MbCtx layout");
+
+__device__ __forceinline__ const MbCtx& mbctx(uint32_t off) { return *reinterpret_cast<const MbCtx*>(g_smem + off); }
 
 // mb_sad at integer offset (dx, dy) and sampling stride 1/2/4 (encoder_motion.cpp:2197-2285);
 // one out-of-line copy serves every search stage.
-__device__ __noinline__ uint64_t mb_sad_core(const IntSadCtx c, int dx, int dy, int stride) {
+__device__ __noinline__ uint64_t mb_sad_core(uint32_t ctx, int dx, int dy, int stride) {
+    const MbCtx& c = mbctx(ctx);
     const DevParams P = geo_params(c.g);
     if (hidden_padding(P, c.x0, c.y0, 16, 16, dx * 4, dy * 4, VC1CU_MV_QPEL, true)) return kBad;
     uint32_t s;
@@ -386,43 +397,28 @@ __device__ __noinline__ uint64_t mb_sad_core(const IntSadCtx c, int dx, int dy, 
     return stride > 1 ? (uint64_t)s * (uint64_t)(stride * stride) : (uint64_t)s;
 }
 
-__device__ __forceinline__ uint64_t mb_sad(const DevParams& P, const Mb& m, int dx, int dy, int stride) {
-    const IntSadCtx c{score_geo(P), m.sm.win.off, m.sm.cur.off, m.sm.cur2.off, m.sm.cur4.off, m.wp, m.wx0, m.wy0, m.wh,
-                      m.x0, m.y0, m.aw, m.ah, m.gref.p, m.gref.pitch};
-    return mb_sad_core(c, dx, dy, stride);
+__device__ __forceinline__ uint64_t mb_sad(const DevParams&, const Mb& m, int dx, int dy, int stride) {
+    return mb_sad_core(m.sm.ctx.off, dx, dy, stride);
 }
 
 // ---- sub-pel SAD / SATD batches (block_sad_motion :2670-2933, block_satd_motion :2960-3042)
-
-// Everything the out-of-line batch scorers read about the current macroblock, by value
-// (shared-memory buffers as byte offsets of g_smem, so the callee keeps shared addressing).
-struct BatchCtx {
-    uint32_t win_off, cur_off;
-    int wp, wx0, wy0, wh;
-    int x0, y0;
-    int lane;
-    const uint8_t* gref;
-    int gpitch;
-};
 
 __device__ __forceinline__ uint32_t soff(const void* p) {
     return (uint32_t)(reinterpret_cast<const uint8_t*>(p) - g_smem);
 }
 
-__device__ __forceinline__ BatchCtx batch_ctx(const Mb& m) {
-    return BatchCtx{m.sm.win.off, m.sm.cur.off, m.wp, m.wx0, m.wy0, m.wh, m.x0, m.y0, m.lane, m.gref.p, m.gref.pitch};
-}
-
-__device__ __forceinline__ bool ctx_inside(const BatchCtx& c, int xa, int ya, int xb, int yb) {
+__device__ __forceinline__ bool ctx_inside(const MbCtx& c, int xa, int ya, int xb, int yb) {
     return xa >= c.wx0 && ya >= c.wy0 && xb < c.wx0 + c.wp && yb < c.wy0 + c.wh;
 }
 
 // SAD of n candidates of block (bx,by,bw,bh) (bw,bh in {8,16}) under the CPU law, written
 // to out[]. Each candidate's block is split into 8-pixel row segments over bh*bw/8 lanes.
 // One out-of-line copy serves every call site.
-__device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+__device__ __noinline__ void sad_batch_core(uint32_t ctx, uint32_t mvs_off, int n, int bx, int by,
                                             int bw, int bh, int mode, uint32_t out_off) {
-    const DevParams P = geo_params(g);
+    const MbCtx& c = mbctx(ctx);
+    const int lane = threadIdx.x & 31;
+    const DevParams P = geo_params(c.g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
     const int spr = bw >> 3;
@@ -433,8 +429,8 @@ __device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, 
     const bool cg = chroma_gate(bx, by, bw, bh);
     const int cx = bx - c.x0, cy = by - c.y0;
     for (int base = 0; base < n; base += per_iter) {
-        const int ci = base + c.lane / segs;
-        const int sidx = c.lane % segs;
+        const int ci = base + lane / segs;
+        const int sidx = lane % segs;
         const int r = sidx / spr, c0 = (sidx % spr) * 8;
         const bool valid = ci < n;
         const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
@@ -462,9 +458,11 @@ __device__ __noinline__ void sad_batch_core(const ScoreGeo g, const BatchCtx c, 
     __syncwarp();
 }
 
-__device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c, uint32_t mvs_off, int n, int bx, int by,
+__device__ __noinline__ void satd_batch_core(uint32_t ctx, uint32_t mvs_off, int n, int bx, int by,
                                              int bw, int bh, int mode, uint32_t out_off) {
-    const DevParams P = geo_params(g);
+    const MbCtx& c = mbctx(ctx);
+    const int lane = threadIdx.x & 31;
+    const DevParams P = geo_params(c.g);
     const int2* mvs = reinterpret_cast<const int2*>(g_smem + mvs_off);
     uint64_t* out = reinterpret_cast<uint64_t*>(g_smem + out_off);
     const int tpr = bw >> 2;
@@ -474,8 +472,8 @@ __device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c,
     const bool bil = mode_bilinear(mode);
     const int cx = bx - c.x0, cy = by - c.y0;
     for (int base = 0; base < n; base += per_iter) {
-        const int ci = base + c.lane / tiles;
-        const int t = c.lane % tiles;
+        const int ci = base + lane / tiles;
+        const int t = lane % tiles;
         const int tx = (t % tpr) * 4, ty = (t / tpr) * 4;
         const bool valid = ci < n;
         const int2 mv = valid ? mvs[ci] : make_int2(0, 0);
@@ -523,12 +521,12 @@ __device__ __noinline__ void satd_batch_core(const ScoreGeo g, const BatchCtx c,
 // mvs and out point into the warp's shared-memory buffers.
 __device__ __forceinline__ void sad_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
                                           int bh, int mode, uint64_t* out) {
-    sad_batch_core(score_geo(P), batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
+    sad_batch_core(m.sm.ctx.off, soff(mvs), n, bx, by, bw, bh, mode, soff(out));
 }
 
 __device__ __forceinline__ void satd_batch(const DevParams& P, const Mb& m, const int2* mvs, int n, int bx, int by, int bw,
                                            int bh, int mode, uint64_t* out) {
-    satd_batch_core(score_geo(P), batch_ctx(m), soff(mvs), n, bx, by, bw, bh, mode, soff(out));
+    satd_batch_core(m.sm.ctx.off, soff(mvs), n, bx, by, bw, bh, mode, soff(out));
 }
 
 // ---- first-visit bitsets ----------------------------------------------------------------
@@ -1313,34 +1311,43 @@ __device__ RefineOut refine_select(const DevParams& P, const Mb& m, const Shortl
 // cache. Only values cross the call (never the address of the kernel's parameter block or
 // of the macroblock state), so the caller's state stays in registers.
 
-struct RefCtx {
-    ScoreGeo g;
-    int subpel, fast_subpel, subpel_range, me_quality, mvrange, mant_bits, lam_s;
-    uint64_t lam_m;
-    BatchCtx bc;
-    uint32_t batch, cost, satd;  // the warp's shortlist buffers
-};
-
-__device__ __forceinline__ RefCtx ref_ctx(const DevParams& P, const Mb& m) {
-    RefCtx r;
-    r.g = score_geo(P);
-    r.subpel = P.subpel;
-    r.fast_subpel = P.fast_subpel;
-    r.subpel_range = P.subpel_range;
-    r.me_quality = P.me_quality;
-    r.mvrange = P.mvrange;
-    r.mant_bits = P.mant_bits;
-    r.lam_s = m.lam_s;
-    r.lam_m = m.lam_m;
-    r.bc = batch_ctx(m);
-    r.batch = m.sm.batch.off;
-    r.cost = m.sm.batch_cost.off;
-    r.satd = m.sm.list_satd.off;
-    return r;
+// Writes the macroblock's MbCtx (lane 0) once its window geometry is known.
+__device__ void publish_ctx(const DevParams& P, const Mb& m) {
+    if (m.lane == 0) {
+        MbCtx& r = *reinterpret_cast<MbCtx*>(g_smem + m.sm.ctx.off);
+        r.g = score_geo(P);
+        r.win_off = m.sm.win.off;
+        r.cur_off = m.sm.cur.off;
+        r.cur2_off = m.sm.cur2.off;
+        r.cur4_off = m.sm.cur4.off;
+        r.wp = m.wp;
+        r.wx0 = m.wx0;
+        r.wy0 = m.wy0;
+        r.wh = m.wh;
+        r.x0 = m.x0;
+        r.y0 = m.y0;
+        r.aw = m.aw;
+        r.ah = m.ah;
+        r.gref = m.gref.p;
+        r.gpitch = m.gref.pitch;
+        r.subpel = P.subpel;
+        r.fast_subpel = P.fast_subpel;
+        r.subpel_range = P.subpel_range;
+        r.me_quality = P.me_quality;
+        r.mvrange = P.mvrange;
+        r.mant_bits = P.mant_bits;
+        r.lam_s = m.lam_s;
+        r.lam_m = m.lam_m;
+        r.batch = m.sm.batch.off;
+        r.cost = m.sm.batch_cost.off;
+        r.satd = m.sm.list_satd.off;
+    }
+    __syncwarp();
 }
 
-// The parameter block and macroblock state the refinement reads, rebuilt from a RefCtx.
-__device__ __forceinline__ void ref_unpack(const RefCtx& r, DevParams& P, Mb& m) {
+// The parameter block and macroblock state the refinement reads, rebuilt from the MbCtx.
+__device__ __forceinline__ void ref_unpack(uint32_t ctx, DevParams& P, Mb& m) {
+    const MbCtx& r = mbctx(ctx);
     P = geo_params(r.g);
     P.subpel = r.subpel;
     P.fast_subpel = r.fast_subpel;
@@ -1348,42 +1355,47 @@ __device__ __forceinline__ void ref_unpack(const RefCtx& r, DevParams& P, Mb& m)
     P.me_quality = r.me_quality;
     P.mvrange = r.mvrange;
     P.mant_bits = r.mant_bits;
-    m.lane = r.bc.lane;
+    m.lane = threadIdx.x & 31;
     m.lam_m = r.lam_m;
     m.lam_s = r.lam_s;
-    m.x0 = r.bc.x0;
-    m.y0 = r.bc.y0;
-    m.wx0 = r.bc.wx0;
-    m.wy0 = r.bc.wy0;
-    m.wp = r.bc.wp;
-    m.wh = r.bc.wh;
-    m.gref = GlobSampler{r.bc.gref, r.bc.gpitch, P.W, P.H};
-    m.sm.win.off = r.bc.win_off;
-    m.sm.cur.off = r.bc.cur_off;
+    m.x0 = r.x0;
+    m.y0 = r.y0;
+    m.aw = r.aw;
+    m.ah = r.ah;
+    m.wx0 = r.wx0;
+    m.wy0 = r.wy0;
+    m.wp = r.wp;
+    m.wh = r.wh;
+    m.gref = GlobSampler{r.gref, r.gpitch, P.W, P.H};
+    m.sm.ctx.off = ctx;
+    m.sm.win.off = r.win_off;
+    m.sm.cur.off = r.cur_off;
+    m.sm.cur2.off = r.cur2_off;
+    m.sm.cur4.off = r.cur4_off;
     m.sm.batch.off = r.batch;
     m.sm.batch_cost.off = r.cost;
     m.sm.list_satd.off = r.satd;
 }
 
-__device__ __noinline__ Shortlist refine_prepare_ool(const RefCtx r, int bx, int by, int bw, int bh, int2 seed, int range,
+__device__ __noinline__ Shortlist refine_prepare_ool(uint32_t ctx, int bx, int by, int bw, int bh, int2 seed, int range,
                                                      int mode, uint64_t known, bool satd_all) {
     DevParams P;
     Mb m{};
-    ref_unpack(r, P, m);
+    ref_unpack(ctx, P, m);
     return refine_prepare(P, m, bx, by, bw, bh, seed, range, mode, known, satd_all);
 }
 
-__device__ __noinline__ RefineOut refine_select_ool(const RefCtx r, const Shortlist sl, int bx, int by, int bw, int bh,
+__device__ __noinline__ RefineOut refine_select_ool(uint32_t ctx, const Shortlist sl, int bx, int by, int bw, int bh,
                                                     int mode, const PInfo pi, bool more) {
     DevParams P;
     Mb m{};
-    ref_unpack(r, P, m);
+    ref_unpack(ctx, P, m);
     return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
 }
 
 __device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
                                                    int range, int mode, const PInfo& pi, bool more, uint64_t known) {
-    const RefCtx r = ref_ctx(P, m);
+    const uint32_t r = m.sm.ctx.off;
     const Shortlist sl = refine_prepare_ool(r, bx, by, bw, bh, seed, range, mode, known, false);
     return refine_select_ool(r, sl, bx, by, bw, bh, mode, pi, more);
 }
@@ -1755,6 +1767,7 @@ __device__ void carve(WarpMem& s, uint32_t base, const WinCfg& wc) {
     s.spec_cost.off = take(8 * 40);
     s.spec_satd.off = take(8 * 40);
     s.spec_blk.off = take(kSpecBlkBytes * 5);
+    s.ctx.off = take(kMbCtxBytes);
     s.seen.off = take(4 * (uint32_t)wc.seen_words);
     s.seen_full.off = take(4 * (uint32_t)wc.seen_words);
     s.cur.off = take(256);
@@ -1765,7 +1778,7 @@ __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
     auto r = [](int b) { return (b + 15) & ~15; };
     return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(64) + r(8 * kListCap) +
            r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + r(32) + r(32) + r(128) + r(16) +
-           3 * r(8 * 40) + r(kSpecBlkBytes * 5) +
+           3 * r(8 * 40) + r(kSpecBlkBytes * 5) + r(kMbCtxBytes) +
            2 * r(4 * wc.seen_words) + r(256) +
            r(wc.wp * wc.wh + 32);
 }
@@ -1912,6 +1925,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             // --search-range 0 is a real no-search mode (encoder_motion.cpp:72-85)
             m.wp = m.wh = 0;
             m.wx0 = m.wy0 = 0;
+            publish_ctx(P, m);
             const uint64_t z = mb_sad(P, m, 0, 0, 1);
             if (m.lane == 0) {
                 o.mvs[m.pos] = make_int2(0, 0);
@@ -1951,8 +1965,9 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 seed.x = iclamp(seed.x, qb.xmin, qb.xmax);
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
+                publish_ctx(P, m);
                 PHASE_MARK(2);
-                sl = refine_prepare_ool(ref_ctx(P, m), m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
+                sl = refine_prepare_ool(m.sm.ctx.off, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
                 PHASE_MARK(3);
                 dl = __ldcg(&d.seed_dl[m.pos]);
                 dc = __ldcg(&d.seed_dc[m.pos]);
@@ -1963,7 +1978,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                     const Field fg{cur4g, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
                     const PInfo pig = predictor_mixed_1mv(P, fg, m.mx, m.my);
                     shortlist_save(m, 0, sl, seed, 0, 0);
-                    const RefineOut og = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, pig, true);
+                    const RefineOut og = refine_select_ool(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, pig, true);
                     spec_result_save(m, 0, pig, og);
                     one_g = og.mv;
                     if (hidden_padding(P, m.x0, m.y0, 16, 16, one_g.x, one_g.y, one_mode, true)) one_g = make_int2(0, 0);
@@ -1977,7 +1992,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                             sad_batch(P, m, m.sm.batch, 11, bx, by, 8, 8, VC1CU_MV_QPEL, m.sm.batch_cost);
                             const SeedPick b10 = pick_4mv_seed(m, true);
                             const SeedPick bf = pick_4mv_seed(m, false);
-                            const RefCtx rc = ref_ctx(P, m);
+                            const uint32_t rc = m.sm.ctx.off;
                             const Shortlist sk = refine_prepare_ool(rc, bx, by, 8, 8, bf.v, range, VC1CU_MV_MIXED, bf.cost, true);
                             shortlist_save(m, k + 1, sk, bf.v, bf.cost, bf.slot);
                             const RefineOut rk = refine_select_ool(rc, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4g, true);
@@ -1995,6 +2010,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 }
             } else {
                 load_window(P, m, d.ref, 0, 0, wc);
+                publish_ctx(P, m);
                 PHASE_MARK(2);
             }
             if (allow_intra) intra_sad = intra_proxy(P, m);
@@ -2019,7 +2035,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                     one = m.sm.spec_blk[0].res;
                 } else {
                     if (spec) shortlist_restore(m, 0);
-                    one = refine_select_ool(ref_ctx(P, m), sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+                    one = refine_select_ool(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
                 }
             } else {
                 const PInfo pi = predictor_info(P, m);
@@ -2077,7 +2093,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                         } else if (sb.seed_slot != 2) {
                             // the parked shortlist was refined from this same seed
                             const Shortlist sk = shortlist_restore(m, k + 1);
-                            r = refine_select_ool(ref_ctx(P, m), sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
+                            r = refine_select_ool(m.sm.ctx.off, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
                             have = true;
                         } else {
                             best_seed = b.v;
