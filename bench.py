@@ -65,8 +65,9 @@ def anchors_and_pictures():
 
 def make_clip(rank: int):
     from libvc1_b200 import synth
+    from libvc1_b200.replicas import clip_seed
 
-    return synth.hd1080(frames=FRAMES, seed=2 + rank)
+    return synth.hd1080(frames=FRAMES, seed=clip_seed(rank))
 
 
 def params(pq: int):
@@ -136,12 +137,12 @@ class Runner:
 
     def step(self):
         c, pics = self.ctx, self.pics
-        # launch 1: every picture's quarter-pel seed pass (full search window per warp)
+        # every picture's quarter-pel seed pass (full search window per warp)
         c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)])
-        # launch 2: the three seeded mode passes of every picture (small windows, high occupancy)
+        # the three seeded mode passes of every picture (the library runs one launch per mode)
         c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
                                 for m in self.modes])
-        # launch 3: the final pass (after the host's mode decision over whole passes)
+        # the final pass (after the host's mode decision over whole passes)
         c.core_passes(self.p0, [(t, r, self.MIXED, 1, 2000 + 4 * i + self.MIXED, 3000 + i, pq)
                                 for i, (t, r, pq) in enumerate(pics)])
         for i, (t, r, pq) in enumerate(pics):
@@ -171,6 +172,7 @@ def run_ours(args, rank, world, device):
     import torch
 
     from libvc1_b200.api import CudaComputeContext
+    from libvc1_b200.replicas import slowest, whole_job_rate
 
     torch.cuda.set_device(device)
     ctx, err = CudaComputeContext.create(device)
@@ -211,12 +213,9 @@ def run_ours(args, rank, world, device):
     counters = ctx.counters()
     ctx.set_timing(False)
     total_ms = float(sum(step_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
     mbs_per_step = len(run.pics) * MBS
-    value = world * mbs_per_step * args.steps / (max_ms * 1e-3)
+    max_ms = 1e3 * slowest(total_ms * 1e-3, world, "cuda")
+    value = whole_job_rate(mbs_per_step * args.steps, max_ms * 1e-3, world)
     clocks = parse_clocks(clock_log, device)
     # ---- e2e: pinned host frames -> upload -> analysis -> results back, wall clock
     pinned = {}
@@ -236,10 +235,8 @@ def run_ours(args, rank, world, device):
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_s.append(t1 - t0)
-    te = torch.tensor([sum(e2e_s)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * mbs_per_step * args.steps / float(te.item()) if e2e_s else None
+    e2e_worst = slowest(sum(e2e_s), world, "cuda")
+    e2e_value = world * mbs_per_step * args.steps / e2e_worst if e2e_s else None
     # ---- roofline of the dominant kernel (core_pass_kernel), INT32-bound
     n = len(run.pics)
     ops_step = n * MBS * (OPS_PER_MB["unseeded"] + OPS_PER_MB["seeded_hpel"] + OPS_PER_MB["seeded_bilinear"] +
