@@ -25,6 +25,7 @@
 namespace vc1cu {
 // kernels and drivers of the other translation units
 const void* core_kernel(int kind);
+cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cudaStream_t s);
 cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,
                         const PassDesc* passes, int npass, const uint32_t* items, unsigned nitems, const WinCfg& wc,
                         uint32_t epoch, LaunchStatus* st);
@@ -139,6 +140,8 @@ struct vc1cu_ctx {
     int passes_cap = 0;
     GState* d_gstates = nullptr;
     int gstates_cap = 0;
+    void* d_lr = nullptr;      // long-range signature indexes of a launch's reference pictures
+    size_t lr_cap = 0;
     void* d_scratch = nullptr;
     size_t scratch_cap = 0;
     void* h_pinned = nullptr;
@@ -537,9 +540,6 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         } else if (d.seeded) {
             d.seed_mvs = nullptr;  // bound to the seeding pass's result below
         } else {
-            if (P.range > P.local_range)
-                throw Fail{VC1CU_ERR_UNSUPPORTED,
-                           "long-range search (search_range above local_search_range) is not implemented on the device"};
             d.seed_mvs = nullptr;
             d.seed_dl = d.seed_dc = nullptr;
             d.seed_dd = nullptr;
@@ -598,6 +598,20 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         ck(cudaGetLastError(), "global search launch");
         tm.stop(launches);
     }
+    // long-range signature index of each long-range pass's reference (build_long_range_index)
+    if (!unseeded.empty() && P.range > P.local_range) {
+        const int nx = (P.W + 7) / 8, ny = (P.H + 7) / 8;
+        const size_t per = sizeof(uint64_t) * (size_t)nx * ny;
+        uint64_t* base = static_cast<uint64_t*>(ensure(c->d_lr, c->lr_cap, per * unseeded.size(), "cudaMalloc(long-range index)"));
+        for (size_t k = 0; k < unseeded.size(); ++k) {
+            PassDesc& d = h[unseeded[k]];
+            d.lr_sig = base + (size_t)nx * ny * k;
+            d.lr_nx = nx;
+            d.lr_ny = ny;
+            ck(launch_lr_index(d.ref, P.W, P.H, const_cast<uint64_t*>(d.lr_sig), c->stream), "lr_index_kernel launch");
+            c->counters.kernel_launches++;
+        }
+    }
     // pass descriptors
     if (c->passes_cap < n) {
         if (c->d_passes) cudaFree(c->d_passes);
@@ -622,7 +636,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         wc.rw = P.local_range + 1;
         wc.seen_r = P.local_range;
         wc.seen_words = ((2 * P.local_range + 1) * (2 * P.local_range + 1) + 31) / 32;
-        wc.keys_cap = stage_max(P.local_range);
+        wc.keys_cap = std::max(stage_max(P.local_range), 32);  // >= one warp of staged long-range keys
     } else {
         // seeded refinement stays within 3 quarter-pels of the seed; the Mixed-MV block seeds
         // add up to 8 more and their refinement 3 (samples outside the window read HBM)
@@ -824,6 +838,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_status) cudaFree(c->d_status);
     if (c->d_passes) cudaFree(c->d_passes);
     if (c->d_gstates) cudaFree(c->d_gstates);
+    if (c->d_lr) cudaFree(c->d_lr);
     if (c->d_scratch) cudaFree(c->d_scratch);
     for (auto& kv : c->items) cudaFree(kv.second.first);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);

@@ -845,6 +845,246 @@ __device__ IntRes diamond(const DevParams& P, const Mb& m, const PInfo& pi, int 
 
 // ---- staged sub-pel refinement (encoder_motion.cpp:3247-3594) ---------------------------
 
+// ---- long-range search (encoder_motion.cpp:1578-1779) -------------------------------------
+
+// motion_match_good, encoder_motion.cpp:1627-1635
+__device__ __forceinline__ bool match_good(const Mb& m, uint64_t sad) {
+    const uint64_t px = (uint64_t)m.aw * (uint64_t)m.ah;
+    return px && sad < UINT64_MAX / 8 && sad <= px * 6u;
+}
+
+// sad > px * mae, exactly: the reference compares in long double, where the product of a
+// pixel count and a double is exact. mae = mant * 2^k with a 53-bit integer mant.
+__device__ bool sad_above(uint64_t sad, uint64_t px, double mae) {
+    if (isnan(mae)) return false;
+    if (mae < 0.0) return true;
+    if (isinf(mae)) return false;
+    if (mae == 0.0) return sad > 0;
+    int e = 0;
+    const double fr = frexp(mae, &e);                 // mae = fr * 2^e, fr in [0.5, 1)
+    const uint64_t mant = (uint64_t)ldexp(fr, 53);    // exact
+    const int k = e - 53;
+    const unsigned __int128 rhs0 = (unsigned __int128)px * mant;  // < 2^62
+    if (k >= 0) {
+        if (k > 64) return false;
+        return (unsigned __int128)sad > (rhs0 << k);
+    }
+    if (-k > 64) return sad > 0;
+    return ((unsigned __int128)sad << (-k)) > rhs0;
+}
+
+// distant_match_decision, encoder_motion.cpp:1637-1656
+__device__ int distant_decision(const DevParams& P, const Mb& m, uint64_t cand, uint64_t local) {
+    const uint64_t px = (uint64_t)m.aw * (uint64_t)m.ah;
+    if (!px || cand >= UINT64_MAX / 8) return 0;
+    if (cand <= px * 6u) return 2;
+    if (sad_above(cand, px, P.distant_match_max_mae)) return 1;
+    if (local >= UINT64_MAX / 8) return 3;
+    return cand * 4u <= local * 3u ? 3 : 1;
+}
+
+// Least (sad, |dx|+|dy|, lane) over the lanes with `valid`, on every lane.
+__device__ void warp_argmin_int(bool& valid, uint64_t& sad, int& dx, int& dy, int& idx) {
+#pragma unroll 1
+    for (int o = 16; o; o >>= 1) {
+        const bool ov = __shfl_xor_sync(FULL, valid, o);
+        const uint64_t os = __shfl_xor_sync(FULL, sad, o);
+        const int ox = __shfl_xor_sync(FULL, dx, o), oy = __shfl_xor_sync(FULL, dy, o);
+        const int oi = __shfl_xor_sync(FULL, idx, o);
+        bool take = ov && !valid;
+        if (ov && valid) {
+            const int l1 = iabs(ox) + iabs(oy), l0 = iabs(dx) + iabs(dy);
+            take = os != sad ? os < sad : (l1 != l0 ? l1 < l0 : oi < idx);
+        }
+        if (take) {
+            valid = true;
+            sad = os;
+            dx = ox;
+            dy = oy;
+            idx = oi;
+        }
+    }
+}
+
+// The 13 offsets of propagated_long_range_motion (:1671-1673), by lane.
+__device__ __forceinline__ int2 lr_prop_offset(int l) {
+    if (l == 0) return make_int2(0, 0);
+    if (l <= 8) {
+        const int a = (l - 1) & 3, d = l <= 4 ? 1 : 2;  // (-d,0) (d,0) (0,-d) (0,d)
+        return a == 0 ? make_int2(-d, 0) : a == 1 ? make_int2(d, 0) : a == 2 ? make_int2(0, -d) : make_int2(0, d);
+    }
+    const int a = l - 9;  // (-1,-1) (1,-1) (-1,1) (1,1)
+    return make_int2((a & 1) ? 1 : -1, (a & 2) ? 1 : -1);
+}
+
+// Vc1Encoder::propagated_long_range_motion, encoder_motion.cpp:1658-1694: around the integer
+// vectors of the left, top, top-left and top-right neighbours whose search took a long-range
+// vector (flags bit 2), in that order, stopping once the match is good.
+__device__ IntRes lr_propagated(const DevParams& P, const Mb& m, const DevResult& o, int range) {
+    IntRes best{0, 0, UINT64_MAX};
+    const Bounds b = bounds_px(range);
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+        const int nx = m.mx + (k == 0 || k == 2 ? -1 : (k == 3 ? 1 : 0)), ny = m.my - (k == 0 ? 0 : 1);
+        if (nx < 0 || ny < 0 || nx >= P.mbw) continue;
+        const int pos = ny * P.mbw + nx;
+        if (!(__ldcg(&o.flags[pos]) & 4)) continue;
+        const int2 f = __ldcg(&o.mvs[pos]);
+        const int cx = round_qpel_to_pixel(f.x), cy = round_qpel_to_pixel(f.y);
+        bool valid = m.lane < 13;
+        uint64_t sad = UINT64_MAX;
+        int dx = 0, dy = 0, idx = m.lane;
+        if (valid) {
+            const int2 of = lr_prop_offset(m.lane);
+            dx = iclamp(cx + of.x, b.xmin, b.xmax);
+            dy = iclamp(cy + of.y, b.ymin, b.ymax);
+            sad = mb_sad(P, m, dx, dy, 1);
+        }
+        warp_argmin_int(valid, sad, dx, dy, idx);
+        if (sad < best.cost || (sad == best.cost && iabs(dx) + iabs(dy) < iabs(best.dx) + iabs(best.dy))) {
+            best.cost = sad;
+            best.dx = dx;
+            best.dy = dy;
+        }
+        if (match_good(m, best.cost)) break;
+    }
+    return best;
+}
+
+// mean_region (:1578-1590) of an 8x8 region of a plane, by the warp (two samples per lane).
+__device__ uint32_t warp_mean8(const uint8_t* plane, int pitch, int pw, int ph, int x0, int y0, int lane) {
+    uint32_t sum = 0, n = 0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int i = lane * 2 + j, x = x0 + (i & 7), y = y0 + (i >> 3);
+        if (x >= 0 && y >= 0 && x < pw && y < ph) {
+            sum += __ldg(plane + (size_t)y * pitch + x);
+            ++n;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        sum += __shfl_xor_sync(FULL, sum, o);
+        n += __shfl_xor_sync(FULL, n, o);
+    }
+    return n ? (sum + n / 2) / n : 128;
+}
+
+// long_range_signature (:1592-1603) packed as bytes ydc0..3, udc, vdc.
+__device__ uint64_t warp_signature(const DevFrame& f, int W, int H, int x0, int y0, int lane) {
+    uint64_t s = 0;
+    s |= (uint64_t)warp_mean8(f.y, f.pitch_y, W, H, x0, y0, lane);
+    s |= (uint64_t)warp_mean8(f.y, f.pitch_y, W, H, x0 + 8, y0, lane) << 8;
+    s |= (uint64_t)warp_mean8(f.y, f.pitch_y, W, H, x0, y0 + 8, lane) << 16;
+    s |= (uint64_t)warp_mean8(f.y, f.pitch_y, W, H, x0 + 8, y0 + 8, lane) << 24;
+    s |= (uint64_t)warp_mean8(f.u, f.pitch_c, W / 2, H / 2, x0 / 2, y0 / 2, lane) << 32;
+    s |= (uint64_t)warp_mean8(f.v, f.pitch_c, W / 2, H / 2, x0 / 2, y0 / 2, lane) << 40;
+    return s;
+}
+
+// long_range_signature_distance (:1605-1614)
+__device__ __forceinline__ uint32_t sig_distance(uint64_t a, uint64_t b) {
+    uint32_t d = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d += (uint32_t)iabs((int)((a >> (8 * i)) & 255) - (int)((b >> (8 * i)) & 255)) * 2u;
+    d += (uint32_t)iabs((int)((a >> 32) & 255) - (int)((b >> 32) & 255)) * 3u;
+    d += (uint32_t)iabs((int)((a >> 40) & 255) - (int)((b >> 40) & 255)) * 3u;
+    return d;
+}
+
+// Vc1Encoder::extended_content_motion, encoder_motion.cpp:1696-1779: the 16 lattice cells
+// whose signature is nearest the macroblock's (order (distance, |d|, dy, dx), cells within
+// 32 pixels excluded), each refined by a 5x5 grid of step 4 at stride 2 and a 5x5 full
+// search; `local` stands unless the best is both cheaper and a good enough distant match.
+__device__ IntRes lr_extended(const DevParams& P, const Mb& m, const PassDesc& d, int range, const IntRes& local,
+                              uint64_t& cand_sad, int& decision) {
+    const Bounds b = bounds_px(range);
+    const uint64_t want = warp_signature(d.cur, P.W, P.H, m.x0, m.y0, m.lane);
+    uint64_t* top = m.sm.list_sad;  // 16 sorted keys (idle after the integer search)
+    uint64_t* stage = m.sm.keys;
+    int tn = 0;
+    const int n = d.lr_nx * d.lr_ny;
+#pragma unroll 1
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + m.lane;
+        uint64_t key = UINT64_MAX;
+        if (i < n) {
+            const int dx = (i % d.lr_nx) * 8 - m.x0, dy = (i / d.lr_nx) * 8 - m.y0;
+            if (dx >= b.xmin && dx <= b.xmax && dy >= b.ymin && dy <= b.ymax && !(iabs(dx) <= 32 && iabs(dy) <= 32)) {
+                const uint64_t dist = sig_distance(want, __ldg(&d.lr_sig[i]));
+                key = (dist << 36) | ((uint64_t)(iabs(dx) + iabs(dy)) << 24) | ((uint64_t)(dy + 2048) << 12) |
+                      (uint64_t)(dx + 2048);
+            }
+        }
+        const uint64_t bound = tn == 16 ? top[15] : UINT64_MAX;
+        const bool take = key < bound;
+        const unsigned tm = __ballot_sync(FULL, take);
+        if (!tm) continue;
+        if (take) stage[__popc(tm & ((1u << m.lane) - 1))] = key;
+        __syncwarp();
+        if (m.lane == 0) {
+            const int cnt = __popc(tm);
+            for (int j = 0; j < cnt; ++j) {
+                const uint64_t k = stage[j];
+                if (tn == 16 && k >= top[15]) continue;
+                int at = tn < 16 ? tn : 15;
+                while (at > 0 && top[at - 1] > k) {
+                    top[at] = top[at - 1];
+                    --at;
+                }
+                top[at] = k;
+                if (tn < 16) ++tn;
+            }
+        }
+        tn = __shfl_sync(FULL, tn, 0);
+        __syncwarp();
+    }
+    IntRes best{0, 0, UINT64_MAX};
+#pragma unroll 1
+    for (int t = 0; t < tn; ++t) {
+        const uint64_t key = top[t];
+        const int cdx = (int)(key & 0xFFF) - 2048, cdy = (int)((key >> 12) & 0xFFF) - 2048;
+        // 5x5 at step 4, stride 2: the first least SAD in scan order
+        bool valid = m.lane < 25;
+        uint64_t sad = UINT64_MAX;
+        int dx = 0, dy = 0, idx = m.lane;
+        if (valid) {
+            dx = iclamp(cdx - 8 + 4 * (m.lane % 5), b.xmin, b.xmax);
+            dy = iclamp(cdy - 8 + 4 * (m.lane / 5), b.ymin, b.ymax);
+            sad = mb_sad(P, m, dx, dy, 2);
+        }
+        {
+            uint64_t s = sad;
+            const uint64_t mn = warp_min_u64(valid ? s : UINT64_MAX);
+            const unsigned at = __ballot_sync(FULL, valid && s == mn);
+            const int src = __ffs(at) - 1;
+            dx = __shfl_sync(FULL, dx, src);
+            dy = __shfl_sync(FULL, dy, src);
+        }
+        const int sx = dx, sy = dy;
+        // 5x5 full search around it: least (sad, |d|), first in scan order
+        valid = m.lane < 25;
+        sad = UINT64_MAX;
+        idx = m.lane;
+        if (valid) {
+            dx = iclamp(sx + m.lane % 5 - 2, b.xmin, b.xmax);
+            dy = iclamp(sy + m.lane / 5 - 2, b.ymin, b.ymax);
+            sad = mb_sad(P, m, dx, dy, 1);
+        }
+        warp_argmin_int(valid, sad, dx, dy, idx);
+        if (sad < best.cost) {
+            best.cost = sad;
+            best.dx = dx;
+            best.dy = dy;
+        }
+        if (match_good(m, best.cost)) break;
+    }
+    cand_sad = best.cost;
+    decision = best.cost < UINT64_MAX / 8 ? distant_decision(P, m, best.cost, local.cost) : 0;
+    __syncwarp();
+    if (best.cost >= local.cost || decision < 2) return local;
+    return best;
+}
+
 struct RefineOut {
     int2 mv;
     uint64_t screen_sad;
@@ -2029,6 +2269,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             const PInfo rate_pi = predictor_mixed_1mv(P, field, m.mx, m.my);
             const uint64_t pixels = (uint64_t)m.aw * (uint64_t)m.ah;
             RefineOut one;
+            bool distant = false;  // the integer vector came from a long-range search
             PHASE_MARK(6);
             if (seeded) {
                 if (spec && pinfo_equal(rate_pi, m.sm.spec_blk[0].pi)) {
@@ -2040,9 +2281,64 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             } else {
                 const PInfo pi = predictor_info(P, m);
                 const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
-                const IntRes im = P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
-                                                      : umh(P, m, pi, gdx, gdy, local_range, pixels);
-                if (P.long_range_mode != 2 && pixels) dl = (double)im.cost / (double)pixels;
+                auto local_search = [&]() {
+                    return P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
+                                               : umh(P, m, pi, gdx, gdy, local_range, pixels);
+                };
+                // a distant candidate's MAE, kept when it is the least seen (record_distant, :176-183)
+                auto record = [&](uint64_t s, int decision) {
+                    if (!pixels || s >= UINT64_MAX / 8) return;
+                    const double mae = (double)s / (double)pixels;
+                    if (dc < 0.0 || mae < dc) {
+                        dc = mae;
+                        dd = (uint8_t)decision;
+                    }
+                };
+                const bool long_range = range > local_range;
+                IntRes im{0, 0, UINT64_MAX};
+                if (P.long_range_mode == 2) {
+                    // legacy distant-first policy (:144-160)
+                    bool short_circuit = false;
+                    if (long_range) {
+                        const IntRes pr = lr_propagated(P, m, o, range);
+                        if (match_good(m, pr.cost)) {
+                            im = pr;
+                            short_circuit = true;
+                            distant = true;
+                        }
+                    }
+                    if (!short_circuit) im = local_search();
+                } else {
+                    // local search first, then the propagated distant candidate (:161-196)
+                    im = local_search();
+                    const uint64_t local_sad = im.cost;
+                    if (pixels) dl = (double)local_sad / (double)pixels;
+                    const bool skip = P.long_range_mode == 1 && match_good(m, im.cost);
+                    if (long_range && !skip) {
+                        const IntRes pr = lr_propagated(P, m, o, range);
+                        const int decision = distant_decision(P, m, pr.cost, local_sad);
+                        record(pr.cost, decision);
+                        const bool less = pr.cost != im.cost ? pr.cost < im.cost
+                                        : (iabs(pr.dx) + iabs(pr.dy) != iabs(im.dx) + iabs(im.dy)
+                                               ? iabs(pr.dx) + iabs(pr.dy) < iabs(im.dx) + iabs(im.dy)
+                                               : (pr.dy != im.dy ? pr.dy < im.dy : pr.dx < im.dx));
+                        if (less && decision >= 2) {
+                            im = pr;
+                            distant = true;
+                        }
+                    }
+                }
+                if (long_range && !match_good(m, im.cost)) {
+                    // content-signature search (:201-225)
+                    uint64_t ext_sad = UINT64_MAX;
+                    int ext_decision = 0;
+                    const IntRes ext = lr_extended(P, m, d, range, im, ext_sad, ext_decision);
+                    if (P.long_range_mode != 2) record(ext_sad, ext_decision);
+                    if (ext.dx != im.dx || ext.dy != im.dy) {
+                        im = ext;
+                        distant = true;
+                    }
+                }
                 PHASE_MARK(7);
                 one = refine_staged(P, m, m.x0, m.y0, 16, 16, make_int2(im.dx * 4, im.dy * 4), range, one_mode, rate_pi,
                                     true, im.cost);
@@ -2059,6 +2355,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             int2 out4[4] = {one.mv, one.mv, one.mv, one.mv};
             int2 out_mv = one.mv;
             uint8_t use4 = 0, intra = 0;
+            bool chose4 = false;
             uint64_t chosen = one_sad, temporal_screen = one_sad;
             const double lambda = d.lambda;
             if (allow_4mv) {
@@ -2131,6 +2428,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 if (four_chroma_safe)
                     choose4 = four_sad + (uint64_t)llround(__dmul_rn(lambda, (double)extra_bits)) + 8 <
                               (uint64_t)llround(__dmul_rn((double)one_sad, 0.985));
+                chose4 = choose4;
                 if (choose4) {
                     for (int k = 0; k < 4; ++k) out4[k] = four[k];
                     use4 = 1;
@@ -2173,7 +2471,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 o.dd[m.pos] = dd;
                 o.chosen[m.pos] = chosen;
                 o.temporal[m.pos] = temporal;
-                o.flags[m.pos] = (uint8_t)((moved ? 1 : 0) | (frac ? 2 : 0));
+                o.flags[m.pos] = (uint8_t)((moved ? 1 : 0) | (frac ? 2 : 0) | (distant ? 4 : 0) | (chose4 ? 8 : 0));
             }
         }
         __syncwarp();
@@ -2184,6 +2482,41 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         __syncwarp();
         PHASE_MARK(11);
     }
+}
+
+// mean_region (:1578-1590) of one 8x8 region, by one thread.
+__device__ uint32_t mean8(const uint8_t* plane, int pitch, int pw, int ph, int x0, int y0) {
+    uint32_t sum = 0, n = 0;
+    for (int y = 0; y < 8 && y0 + y < ph; ++y) {
+        if (y0 + y < 0) continue;
+        for (int x = 0; x < 8 && x0 + x < pw; ++x) {
+            if (x0 + x < 0) continue;
+            sum += __ldg(plane + (size_t)(y0 + y) * pitch + x0 + x);
+            ++n;
+        }
+    }
+    return n ? (sum + n / 2) / n : 128;
+}
+
+// build_long_range_index (:1616-1625): the signature of every 8-pixel lattice cell of a
+// reference picture, one thread per cell, raster order.
+__global__ void lr_index_kernel(DevFrame ref, int W, int H, int nx, int ny, uint64_t* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return;
+    const int x0 = (i % nx) * 8, y0 = (i / nx) * 8;
+    uint64_t s = (uint64_t)mean8(ref.y, ref.pitch_y, W, H, x0, y0);
+    s |= (uint64_t)mean8(ref.y, ref.pitch_y, W, H, x0 + 8, y0) << 8;
+    s |= (uint64_t)mean8(ref.y, ref.pitch_y, W, H, x0, y0 + 8) << 16;
+    s |= (uint64_t)mean8(ref.y, ref.pitch_y, W, H, x0 + 8, y0 + 8) << 24;
+    s |= (uint64_t)mean8(ref.u, ref.pitch_c, W / 2, H / 2, x0 / 2, y0 / 2) << 32;
+    s |= (uint64_t)mean8(ref.v, ref.pitch_c, W / 2, H / 2, x0 / 2, y0 / 2) << 40;
+    out[i] = s;
+}
+
+cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cudaStream_t s) {
+    const int nx = (W + 7) / 8, ny = (H + 7) / 8;
+    lr_index_kernel<<<(nx * ny + 255) / 256, 256, 0, s>>>(ref, W, H, nx, ny, out);
+    return cudaGetLastError();
 }
 
 // Host-side handles of the two instantiations (attributes, occupancy, launch).
@@ -2214,7 +2547,7 @@ __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDes
         rs += o.temporal[i];
         mv += o.flags[i] & 1;
         fr += (o.flags[i] >> 1) & 1;
-        f4 += o.use4[i];
+        f4 += (o.flags[i] >> 3) & 1;  // 4MV chosen, also where P-intra then replaced it (:370)
         in += o.intra[i];
         const int mx = i % P.mbw, my = i / P.mbw;
         px += (uint64_t)imax(0, imin(16, P.W - mx * 16)) * (uint64_t)imax(0, imin(16, P.H - my * 16));

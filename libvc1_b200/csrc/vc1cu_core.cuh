@@ -29,7 +29,7 @@ struct DevResult {
     uint8_t* dd;
     uint64_t* chosen;      // per-MB chosen SAD (motion_sad summand)
     uint64_t* temporal;    // per-MB temporal SAD (rate_complexity summand)
-    uint8_t* flags;        // bit0 moved, bit1 fractional chroma, bit2 long-range propagated
+    uint8_t* flags;        // bit0 moved, bit1 fractional chroma, bit2 long-range vector, bit3 4MV chosen
     uint32_t* done;        // wavefront flags (== epoch when the MB is final)
     int* global;           // [dx, dy] of the unseeded pass
     unsigned long long* gsad;
@@ -49,6 +49,8 @@ struct PassDesc {
     const int2* seed_mvs;
     const int2* seed_bmv;        // the seed pass's block vectors and P-intra flags (only used to
     const uint8_t* seed_intra;   // guess this pass's predictors before the wavefront wait)
+    const uint64_t* lr_sig;      // long-range signature index of `ref` (long-range passes only)
+    int lr_nx, lr_ny;            // its 8-pixel lattice
     const double* seed_dl;
     const double* seed_dc;
     const uint8_t* seed_dd;

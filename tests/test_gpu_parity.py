@@ -110,6 +110,16 @@ CASES = {
                      dict(search_range=16, local_search_range=16, pqindex=20, subpel_range=2)),
     "range0": (lambda: synth.cif_plain(frames=2, seed=2), dict(search_range=0, local_search_range=0)),
     "tiny_16x16": (lambda: synth.generate(16, 16, 2, 2, n_objects=0), dict(search_range=8, local_search_range=8)),
+    # long-range search (search range beyond the local range): compare, local-good skip, legacy
+    "longrange_compare": (lambda: synth.generate(352, 288, 2, 9, global_px=40.0, n_objects=2),
+                          dict(search_range=128, local_search_range=16)),
+    "longrange_skip": (lambda: synth.generate(352, 288, 2, 9, global_px=40.0, n_objects=2),
+                       dict(search_range=128, local_search_range=16, long_range_mode=1)),
+    "longrange_legacy": (lambda: synth.generate(352, 288, 2, 9, global_px=40.0, n_objects=2),
+                         dict(search_range=128, local_search_range=16, long_range_mode=2)),
+    "longrange_odd_diamond": (lambda: synth.generate(322, 242, 2, 31, global_px=60.0, n_objects=3),
+                              dict(display_width=321, display_height=241, search_range=96, local_search_range=8,
+                                   me_algorithm=1)),
 }
 
 

@@ -203,7 +203,9 @@ def test_block_costs_match_reference_live(oracle, rnd):
                                 dict(search_range=16, local_search_range=16, me_algorithm=1),
                                 dict(search_range=16, local_search_range=16, fast_subpel=1, me_quality=0),
                                 dict(search_range=24, local_search_range=8, pqindex=5, halfqp=1),
-                                dict(search_range=0, local_search_range=0)])
+                                dict(search_range=0, local_search_range=0),
+                                dict(search_range=96, local_search_range=8),
+                                dict(search_range=96, local_search_range=8, long_range_mode=2)])
 def test_analysis_matches_reference_live(oracle, kw):
     Reference = _ref_or_skip()
     clip = synth.generate(98, 66, 2, 13)
