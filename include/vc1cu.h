@@ -97,7 +97,7 @@ typedef struct vc1cu_params {
     int32_t long_range_mode;    /* vc1_long_range_search_mode_e */
     int32_t rnd;                /* rndctrl */
     int32_t disable_p_intra;    /* debug_disable_p_intra */
-    int32_t reserved0;
+    int32_t disable_b_intra;    /* debug_disable_b_intra */
     double distant_match_max_mae;  /* default 255.0 */
     double inter_intra_threshold;  /* default 0.80 */
 } vc1cu_params;
@@ -251,6 +251,91 @@ int vc1cu_core_passes(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_pass* p
 /* Copies a result slot to host arrays (and the scalar totals). Synchronous. */
 int vc1cu_read_result(vc1cu_ctx* ctx, int slot, vc1cu_panalysis* out);
 int vc1cu_synchronize(vc1cu_ctx* ctx);
+
+/* ---- B-picture analysis (Vc1Encoder::analyze_b_picture_mode) --------------------- */
+
+/* Vc1Encoder::BMbMode (src/encoder_internal.h:407). */
+enum {
+    VC1CU_BMB_FORWARD = 0,
+    VC1CU_BMB_BACKWARD = 1,
+    VC1CU_BMB_INTERPOLATED = 2,
+    VC1CU_BMB_DIRECT = 3,
+    VC1CU_BMB_INTRA = 4
+};
+
+/*
+ * Vc1Encoder::BAnalysis (src/encoder_internal.h:408-434). Per-macroblock HOST arrays of
+ * mbw*mbh entries; any pointer may be NULL to skip it. The distant_* arrays are the two
+ * core passes' own (PAnalysis::distant_*), copied through as the reference does
+ * (encoder_motion.cpp:812-817). The scalar fields are written by the call.
+ */
+typedef struct vc1cu_banalysis {
+    uint8_t* modes;                     /* VC1CU_BMB_* */
+    vc1cu_mv* forward_mvs;              /* decoder forward MV state of every MB */
+    vc1cu_mv* backward_mvs;             /* decoder backward MV state */
+    double* inter_intra_cost_ratio;
+    double* forward_distant_local_mae;
+    double* forward_distant_candidate_mae;
+    uint8_t* forward_distant_match_decision;
+    double* backward_distant_local_mae;
+    double* backward_distant_candidate_mae;
+    uint8_t* backward_distant_match_decision;
+    uint64_t forward_macroblocks;
+    uint64_t backward_macroblocks;
+    uint64_t interpolated_macroblocks;
+    uint64_t direct_macroblocks;
+    uint64_t intra_macroblocks;
+    uint64_t moved_macroblocks;
+    uint64_t fractional_chroma_macroblocks;
+    double mean_abs_residual;
+    double rate_complexity;
+    uint64_t motion_sad;
+    uint64_t motion_bits;
+    int32_t mv_mode;
+    int32_t reserved;
+} vc1cu_banalysis;
+
+/*
+ * Replaces one Vc1Encoder::analyze_b_picture_mode call (src/encoder_motion.cpp:753-1005):
+ * two unseeded core passes of cur_id (forward against past_id, backward against future_id,
+ * allow_intra = 0, the given mode), then the per-macroblock Direct / Forward / Backward /
+ * Interpolated / Intra decision with the direct vectors scaled from the future anchor's
+ * collocated vectors. anchor_mvs / anchor_4mv: HOST arrays of mbw*mbh entries, the future
+ * P anchor's MVs and Mixed-MV flags (future_anchor_mvs / future_anchor_4mv). fraction:
+ * 1/2, 1/3 or 2/3. past_id holds the (already intensity-compensated, when the anchor
+ * signals intensity compensation) past reference. The caller keeps the reference's two
+ * encoder-level decisions around this call: the minimal zero-motion configuration
+ * (encoder_motion.cpp:770-785, no analysis) and the qpel-versus-half-pel picture RD of
+ * analyze_b_picture (:1062-1095). Synchronous.
+ */
+int vc1cu_analyze_b_picture(vc1cu_ctx* ctx, const vc1cu_params* p, int cur_id, int past_id,
+                            int future_id, const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv,
+                            int fraction_num, int fraction_den, int mode, vc1cu_banalysis* out);
+
+/*
+ * Device-resident batch form: the decision stage for n B pictures whose two core passes
+ * already ran (vc1cu_core_passes: unseeded, allow_intra 0, the same mode). anchor_slot
+ * names the result slot whose mvs / use_4mv are the future anchor's. The B results go to
+ * B-result slots (0 <= out_bslot < 4096, a namespace separate from the core result
+ * slots). Asynchronous on the context stream.
+ */
+typedef struct vc1cu_bpass {
+    int32_t cur_id;
+    int32_t past_id;
+    int32_t future_id;
+    int32_t fwd_slot;      /* result slot of the forward core pass */
+    int32_t bwd_slot;      /* result slot of the backward core pass */
+    int32_t anchor_slot;   /* result slot holding the future anchor's MVs / Mixed-MV flags */
+    int32_t fraction_num;
+    int32_t fraction_den;
+    int32_t mode;
+    int32_t out_bslot;
+    int32_t pqindex;       /* 0 = params->pqindex */
+} vc1cu_bpass;
+
+int vc1cu_b_decide(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_bpass* passes, int n);
+/* Copies a B-result slot to host arrays (and the scalar totals). Synchronous. */
+int vc1cu_read_bresult(vc1cu_ctx* ctx, int bslot, vc1cu_banalysis* out);
 
 /* ---- motion compensation + forward transform + quantisation ------------------------ */
 

@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("me_algorithm", C.c_int32), ("me_quality", C.c_int32),
         ("subpel", C.c_int32), ("fast_subpel", C.c_int32), ("subpel_range", C.c_int32),
         ("long_range_mode", C.c_int32), ("rnd", C.c_int32), ("disable_p_intra", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("disable_b_intra", C.c_int32),
         ("distant_match_max_mae", C.c_double), ("inter_intra_threshold", C.c_double),
     ]
 
@@ -129,6 +129,91 @@ class Analysis:
         return self
 
     def equal(self, other: "Analysis") -> list[str]:
+        """Names of fields that differ (bit-exact comparison, doubles by bit pattern)."""
+        bad = []
+        for name in self.ARRAYS:
+            a, b = getattr(self, name), getattr(other, name)
+            if a.dtype == np.float64:
+                if not np.array_equal(a.view(np.uint64), b.view(np.uint64)):
+                    bad.append(name)
+            elif not np.array_equal(a, b):
+                bad.append(name)
+        for k, v in self.totals.items():
+            w = other.totals.get(k)
+            if isinstance(v, float):
+                if np.float64(v).view(np.uint64) != np.float64(w).view(np.uint64):
+                    bad.append(k)
+            elif v != w:
+                bad.append(k)
+        return bad
+
+
+BMB_FORWARD, BMB_BACKWARD, BMB_INTERPOLATED, BMB_DIRECT, BMB_INTRA = 0, 1, 2, 3, 4
+
+
+class BAnalysisC(C.Structure):
+    _fields_ = [
+        ("modes", C.c_void_p), ("forward_mvs", C.c_void_p), ("backward_mvs", C.c_void_p),
+        ("inter_intra_cost_ratio", C.c_void_p),
+        ("forward_distant_local_mae", C.c_void_p), ("forward_distant_candidate_mae", C.c_void_p),
+        ("forward_distant_match_decision", C.c_void_p),
+        ("backward_distant_local_mae", C.c_void_p), ("backward_distant_candidate_mae", C.c_void_p),
+        ("backward_distant_match_decision", C.c_void_p),
+        ("forward_macroblocks", C.c_uint64), ("backward_macroblocks", C.c_uint64),
+        ("interpolated_macroblocks", C.c_uint64), ("direct_macroblocks", C.c_uint64),
+        ("intra_macroblocks", C.c_uint64), ("moved_macroblocks", C.c_uint64),
+        ("fractional_chroma_macroblocks", C.c_uint64),
+        ("mean_abs_residual", C.c_double), ("rate_complexity", C.c_double),
+        ("motion_sad", C.c_uint64), ("motion_bits", C.c_uint64),
+        ("mv_mode", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+class BPass(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("cur_id", "past_id", "future_id", "fwd_slot", "bwd_slot", "anchor_slot",
+                                         "fraction_num", "fraction_den", "mode", "out_bslot", "pqindex")]
+
+
+@dataclass
+class BAnalysis:
+    """One B-picture analysis (Vc1Encoder::BAnalysis, src/encoder_internal.h:408-434)."""
+    modes: np.ndarray                   # (mbs,) uint8, BMB_*
+    forward_mvs: np.ndarray             # (mbs, 2) int32
+    backward_mvs: np.ndarray            # (mbs, 2) int32
+    inter_intra_cost_ratio: np.ndarray  # (mbs,) float64
+    forward_distant_local_mae: np.ndarray
+    forward_distant_candidate_mae: np.ndarray
+    forward_distant_match_decision: np.ndarray
+    backward_distant_local_mae: np.ndarray
+    backward_distant_candidate_mae: np.ndarray
+    backward_distant_match_decision: np.ndarray
+    totals: dict
+
+    ARRAYS = ("modes", "forward_mvs", "backward_mvs", "inter_intra_cost_ratio",
+              "forward_distant_local_mae", "forward_distant_candidate_mae", "forward_distant_match_decision",
+              "backward_distant_local_mae", "backward_distant_candidate_mae", "backward_distant_match_decision")
+
+    @classmethod
+    def empty(cls, mbs: int) -> "BAnalysis":
+        f64 = lambda: np.zeros(mbs, np.float64)  # noqa: E731
+        return cls(modes=np.zeros(mbs, np.uint8), forward_mvs=np.zeros((mbs, 2), np.int32),
+                   backward_mvs=np.zeros((mbs, 2), np.int32), inter_intra_cost_ratio=f64(),
+                   forward_distant_local_mae=f64(), forward_distant_candidate_mae=f64(),
+                   forward_distant_match_decision=np.zeros(mbs, np.uint8),
+                   backward_distant_local_mae=f64(), backward_distant_candidate_mae=f64(),
+                   backward_distant_match_decision=np.zeros(mbs, np.uint8), totals={})
+
+    def as_c(self) -> BAnalysisC:
+        s = BAnalysisC()
+        for name in self.ARRAYS:
+            setattr(s, name, getattr(self, name).ctypes.data)
+        return s
+
+    def take_totals(self, s: BAnalysisC) -> "BAnalysis":
+        self.totals = {f[0]: getattr(s, f[0]) for f in BAnalysisC._fields_[10:-1]}
+        return self
+
+    def equal(self, other: "BAnalysis") -> list[str]:
         """Names of fields that differ (bit-exact comparison, doubles by bit pattern)."""
         bad = []
         for name in self.ARRAYS:

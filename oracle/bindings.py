@@ -6,7 +6,7 @@ import os
 
 import numpy as np
 
-from libvc1_b200.abi import Analysis, Mv, PAnalysisC, Params, mbs_of
+from libvc1_b200.abi import Analysis, BAnalysis, BAnalysisC, Mv, PAnalysisC, Params, mbs_of
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_oracle", "libvc1oracle.so")
@@ -73,6 +73,8 @@ class Oracle:
         L.vo_forward_part.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, vp]
         L.vo_quantize_level.argtypes = [P, C.c_double]
         L.vo_forward_quant.argtypes = [P, vp, vp, i32, vp, vp]
+        L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
+        L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
         L.vo_counts_get.argtypes = [C.POINTER(Counts)]
         self._keep = []
@@ -143,6 +145,18 @@ class Oracle:
                                         C.byref(sd) if sd is not None else None, C.byref(oc))
         if rc:
             raise RuntimeError("oracle analyze_p_core failed")
+        return out.take_totals(oc)
+
+    def analyze_b(self, p, cur, past, future, anchor_mvs, anchor_4mv, num, den, mode):
+        mbw, mbh = mbs_of(p)
+        out = BAnalysis.empty(mbw * mbh)
+        oc = out.as_c()
+        am = np.ascontiguousarray(anchor_mvs, np.int32).reshape(-1, 2)
+        a4 = np.ascontiguousarray(anchor_4mv, np.uint8)
+        rc = self.lib.vo_analyze_b(C.byref(p), self._f(cur), self._f(past), self._f(future), am.ctypes.data,
+                                   a4.ctypes.data, num, den, mode, C.byref(oc))
+        if rc:
+            raise RuntimeError("oracle analyze_b failed")
         return out.take_totals(oc)
 
     def motion_compensate(self, p, ref, a: Analysis, mode):
@@ -218,6 +232,7 @@ class Reference:
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
         L.ref_forward_quant.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
+        L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
         L.ref_bench_analysis_multi.argtypes = [C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), i32, i32]
@@ -279,6 +294,18 @@ class Reference:
                                          C.byref(sd) if sd is not None else None, C.byref(oc))
         if rc:
             raise RuntimeError("reference analyze_p_picture_core threw")
+        return out.take_totals(oc)
+
+    def analyze_b(self, cur, past, future, anchor_mvs, anchor_4mv, num, den, mode):
+        mbw, mbh = mbs_of(self.p)
+        out = BAnalysis.empty(mbw * mbh)
+        oc = out.as_c()
+        am = np.ascontiguousarray(anchor_mvs, np.int32).reshape(-1, 2)
+        a4 = np.ascontiguousarray(anchor_4mv, np.uint8)
+        rc = self.lib.ref_analyze_b(self.h, self._f(cur), self._f(past), self._f(future), am.ctypes.data,
+                                    a4.ctypes.data, num, den, mode, C.byref(oc))
+        if rc:
+            raise RuntimeError("reference analyze_b_picture_mode threw")
         return out.take_totals(oc)
 
     def analyze_p_picture(self, cur, ref):

@@ -48,6 +48,7 @@ EncoderConfig make_config(const vc1cu_params* p, int simd) {
     c.inter_intra_threshold = p->inter_intra_threshold;
     c.rndctrl = p->rnd != 0;
     c.debug_disable_p_intra = p->disable_p_intra != 0;
+    c.debug_disable_b_intra = p->disable_b_intra != 0;
     c.syntax = libvc1::StreamSyntax::Advanced;
     c.trellis = 0;
     c.adaptive_quality = false;
@@ -208,6 +209,49 @@ int ref_analyze_p_core(void* h, void* cur, void* ref, int mode, int allow_intra,
             out->global_dy = g.dy;
             out->global_full_sad = g.full_sad;
         }
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// One analyze_b_picture_mode call (forward + backward core passes and the per-MB B mode
+// decision) with intensity compensation off and no search reuse cache.
+int ref_analyze_b(void* h, void* cur, void* past, void* future, const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv,
+                  int fraction_num, int fraction_den, int mode, vc1cu_banalysis* out) {
+    try {
+        auto& e = E(h);
+        const auto& c = static_cast<RefEncoder*>(h)->cfg;
+        const size_t mbs = static_cast<size_t>((c.width + 15) / 16) * ((c.height + 15) / 16);
+        std::vector<MV> amv(mbs);
+        std::vector<uint8_t> a4(anchor_4mv, anchor_4mv + mbs);
+        for (size_t i = 0; i < mbs; ++i) amv[i] = MV{anchor_mvs[i].xq, anchor_mvs[i].yq};
+        const auto a = e.analyze_b_picture_mode(F(cur), F(past), F(future), amv, a4, Vc1Encoder::IntensityComp{},
+                                                fraction_num, fraction_den, to_mode(mode), nullptr, nullptr, nullptr);
+        for (size_t i = 0; i < mbs; ++i) {
+            if (out->modes) out->modes[i] = static_cast<uint8_t>(a.modes[i]);
+            if (out->forward_mvs) out->forward_mvs[i] = {a.forward_mvs[i].xq, a.forward_mvs[i].yq};
+            if (out->backward_mvs) out->backward_mvs[i] = {a.backward_mvs[i].xq, a.backward_mvs[i].yq};
+            if (out->inter_intra_cost_ratio) out->inter_intra_cost_ratio[i] = a.inter_intra_cost_ratio[i];
+            if (out->forward_distant_local_mae) out->forward_distant_local_mae[i] = a.forward_distant_local_mae[i];
+            if (out->forward_distant_candidate_mae) out->forward_distant_candidate_mae[i] = a.forward_distant_candidate_mae[i];
+            if (out->forward_distant_match_decision) out->forward_distant_match_decision[i] = a.forward_distant_match_decision[i];
+            if (out->backward_distant_local_mae) out->backward_distant_local_mae[i] = a.backward_distant_local_mae[i];
+            if (out->backward_distant_candidate_mae) out->backward_distant_candidate_mae[i] = a.backward_distant_candidate_mae[i];
+            if (out->backward_distant_match_decision) out->backward_distant_match_decision[i] = a.backward_distant_match_decision[i];
+        }
+        out->forward_macroblocks = a.forward_macroblocks;
+        out->backward_macroblocks = a.backward_macroblocks;
+        out->interpolated_macroblocks = a.interpolated_macroblocks;
+        out->direct_macroblocks = a.direct_macroblocks;
+        out->intra_macroblocks = a.intra_macroblocks;
+        out->moved_macroblocks = a.moved_macroblocks;
+        out->fractional_chroma_macroblocks = a.fractional_chroma_macroblocks;
+        out->mean_abs_residual = a.mean_abs_residual;
+        out->rate_complexity = a.rate_complexity;
+        out->motion_sad = a.motion_sad;
+        out->motion_bits = a.motion_bits;
+        out->mv_mode = static_cast<int32_t>(a.mv_mode);
         return 0;
     } catch (const std::exception&) {
         return 1;

@@ -166,8 +166,9 @@ static int hidden_luma(const vc1cu_params* p, int x0, int y0, int bw, int bh, in
     return (right_padding && x0 + aw - 1 + ix + right >= vw) || (bottom_padding && y0 + ah - 1 + iy + bottom >= vh);
 }
 
-/* Vc1Encoder::motion_uses_hidden_chroma, encoder_motion.cpp:2167-2189 (future = false) */
-static int hidden_chroma(const vc1cu_params* p, int x0, int y0, int bw, int bh, int xq, int yq) {
+/* Vc1Encoder::motion_uses_hidden_chroma, encoder_motion.cpp:2167-2189; future selects the
+ * B future-reference rounding of the chroma vector (:2178-2181) */
+static int hidden_chroma_f(const vc1cu_params* p, int x0, int y0, int bw, int bh, int xq, int yq, int future) {
     const int cw = (vis_w(p) + 1) / 2, ch = (vis_h(p) + 1) / 2;
     const int right_padding = cw < mbw_of(p) * 8;
     const int bottom_padding = ch < mbh_of(p) * 8;
@@ -177,12 +178,20 @@ static int hidden_chroma(const vc1cu_params* p, int x0, int y0, int bw, int bh, 
     if (!aw || !ah) return 0;
     int uvx = arshift(xq + ((xq & 3) == 3), 1);
     int uvy = arshift(yq + ((yq & 3) == 3), 1);
-    uvx = uvx < 0 ? uvx + (uvx & 1) : uvx - (uvx & 1);
-    uvy = uvy < 0 ? uvy + (uvy & 1) : uvy - (uvy & 1);
+    if (future) {
+        uvx = uvx < 0 ? uvx - (uvx & 1) : uvx + (uvx & 1);
+        uvy = uvy < 0 ? uvy - (uvy & 1) : uvy + (uvy & 1);
+    } else {
+        uvx = uvx < 0 ? uvx + (uvx & 1) : uvx - (uvx & 1);
+        uvy = uvy < 0 ? uvy + (uvy & 1) : uvy - (uvy & 1);
+    }
     const int ix = floor_div4(uvx), iy = floor_div4(uvy);
     const int fx = (uvx - ix * 4) != 0, fy = (uvy - iy * 4) != 0;
     return (right_padding && cx + aw - 1 + ix + (fx ? 1 : 0) >= cw) ||
            (bottom_padding && cy + ah - 1 + iy + (fy ? 1 : 0) >= ch);
+}
+static int hidden_chroma(const vc1cu_params* p, int x0, int y0, int bw, int bh, int xq, int yq) {
+    return hidden_chroma_f(p, x0, y0, bw, bh, xq, yq, 0);
 }
 
 /* Vc1Encoder::motion_uses_hidden_padding, encoder_motion.cpp:2191-2195 */
@@ -1914,4 +1923,191 @@ void vo_score_key(uint64_t sad, double lambda, uint64_t rate, int mant_bits, uin
     }
     *hi = (uint64_t)(v >> 64);
     *lo = (uint64_t)v;
+}
+
+/* ---- B-picture analysis ------------------------------------------------------------- */
+
+/* scale_direct of Vc1Encoder::analyze_b_picture_mode, encoder_motion.cpp:819-833: the
+ * direct-mode vector of a collocated anchor MV, BFRACTION-scaled and pulled into the
+ * decoder's MV range */
+static vc1cu_mv b_scale_direct(const vc1cu_params* p, vc1cu_mv col, int bfrac, int inverse, int mode, int mx,
+                               int my) {
+    const int n = inverse ? bfrac - 256 : bfrac;
+    vc1cu_mv mv;
+    if (mode_halfpel(mode)) {
+        mv.xq = 2 * arshift(col.xq * n + 255, 9);
+        mv.yq = 2 * arshift(col.yq * n + 255, 9);
+    } else {
+        mv.xq = arshift(col.xq * n + 128, 8);
+        mv.yq = arshift(col.yq * n + 128, 8);
+    }
+    const int mbw = mbw_of(p), mbh = mbh_of(p);
+    mv.xq = iclamp(mv.xq, -60 - mx * 64, mbw * 64 - 4 - mx * 64);
+    mv.yq = iclamp(mv.yq, -60 - my * 64, mbh * 64 - 4 - my * 64);
+    return mv;
+}
+
+/* motion_uses_hidden_padding(x0, y0, 16, 16, mv, mode, chroma = true, future) */
+static int b_unsafe(const vc1cu_params* p, int x0, int y0, vc1cu_mv mv, int mode, int future) {
+    return hidden_luma(p, x0, y0, 16, 16, mv.xq, mv.yq, mode) || hidden_chroma_f(p, x0, y0, 16, 16, mv.xq, mv.yq, future);
+}
+
+/* The four candidate costs of one B macroblock (encoder_motion.cpp:846-887): SAD of the
+ * forward, backward, interpolated ((pf+pb+1)>>1) and direct predictions over the coded
+ * raster, each replaced by 2^54 when a reference it uses reads hidden padding. Also the
+ * four-8x8 mean proxy of the B-intra decision (:929-937). */
+void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
+                int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]) {
+    const int x0 = mx * 16, y0 = my * 16;
+    const int vw = imin(16, p->width - x0), vh = imin(16, p->height - y0);
+    uint8_t pf[256], pb[256], pdf[256], pdb[256];
+    memset(pf, 0, sizeof pf); memset(pb, 0, sizeof pb); memset(pdf, 0, sizeof pdf); memset(pdb, 0, sizeof pdb);
+    vo_predict_luma(p, past, x0, y0, vw, vh, fm.xq, fm.yq, mode, pf, 16);
+    vo_predict_luma(p, future, x0, y0, vw, vh, bm.xq, bm.yq, mode, pb, 16);
+    vo_predict_luma(p, past, x0, y0, vw, vh, df.xq, df.yq, mode, pdf, 16);
+    vo_predict_luma(p, future, x0, y0, vw, vh, db.xq, db.yq, mode, pdb, 16);
+    uint64_t cf = 0, cb = 0, ci = 0, cd = 0;
+    for (int y = 0; y < vh; ++y)
+        for (int x = 0; x < vw; ++x) {
+            const int o = y * 16 + x;
+            const int src = f->y[(size_t)(y0 + y) * p->width + x0 + x];
+            cf += (uint64_t)iabs(src - pf[o]);
+            cb += (uint64_t)iabs(src - pb[o]);
+            ci += (uint64_t)iabs(src - ((pf[o] + pb[o] + 1) >> 1));
+            cd += (uint64_t)iabs(src - ((pdf[o] + pdb[o] + 1) >> 1));
+        }
+    const uint64_t invalid = (uint64_t)1 << 54;
+    const int safe_fm = !b_unsafe(p, x0, y0, fm, mode, 0), safe_bm = !b_unsafe(p, x0, y0, bm, mode, 1);
+    const int safe_df = !b_unsafe(p, x0, y0, df, mode, 0), safe_db = !b_unsafe(p, x0, y0, db, mode, 1);
+    if (!safe_fm) cf = invalid;
+    if (!safe_bm) cb = invalid;
+    if (!safe_fm || !safe_bm) ci = invalid;
+    if (!safe_df || !safe_db) cd = invalid;
+    uint64_t intra_sad = 0;
+    for (int k = 0; k < 4; ++k) {
+        const int bx = x0 + (k & 1) * 8, by = y0 + ((k >> 1) & 1) * 8;
+        const int mean = visible_block_mean(f->y, p->width, p->height, bx, by);
+        for (int yy = 0; yy < 8 && by + yy < p->height; ++yy)
+            for (int xx = 0; xx < 8 && bx + xx < p->width; ++xx)
+                intra_sad += (uint64_t)iabs((int)f->y[(size_t)(by + yy) * p->width + bx + xx] - mean);
+    }
+    out[0] = cf; out[1] = cb; out[2] = ci; out[3] = cd; out[4] = intra_sad;
+}
+
+/* Vc1Encoder::analyze_b_picture_mode, encoder_motion.cpp:753-1005 (Advanced Profile
+ * predictors, no minimal zero-motion shortcut: that configuration check is the caller's). */
+int vo_analyze_b(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future,
+                 const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv, int fraction_num, int fraction_den,
+                 int mode, vc1cu_banalysis* out) {
+    if (!((fraction_den == 2 && fraction_num == 1) || (fraction_den == 3 && (fraction_num == 1 || fraction_num == 2))))
+        return 1;
+    const int mbw = mbw_of(p), mbh = mbh_of(p);
+    const size_t mbs = (size_t)mbw * mbh;
+    vc1cu_mv* fmv = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    vc1cu_mv* bmv = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    uint64_t* fscreen = (uint64_t*)calloc(mbs, sizeof(uint64_t));
+    uint64_t* bscreen = (uint64_t*)calloc(mbs, sizeof(uint64_t));
+    vc1cu_mv* ofm = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    vc1cu_mv* obm = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    vc1cu_panalysis fa, ba;
+    memset(&fa, 0, sizeof fa);
+    memset(&ba, 0, sizeof ba);
+    fa.mvs = fmv; fa.screen_sads = fscreen;
+    fa.distant_local_mae = out->forward_distant_local_mae;
+    fa.distant_candidate_mae = out->forward_distant_candidate_mae;
+    fa.distant_match_decision = out->forward_distant_match_decision;
+    ba.mvs = bmv; ba.screen_sads = bscreen;
+    ba.distant_local_mae = out->backward_distant_local_mae;
+    ba.distant_candidate_mae = out->backward_distant_candidate_mae;
+    ba.distant_match_decision = out->backward_distant_match_decision;
+    int rc = vo_analyze_p_core(p, f, past, mode, 0, NULL, NULL, &fa);
+    if (!rc) rc = vo_analyze_p_core(p, f, future, mode, 0, NULL, NULL, &ba);
+    if (rc) goto done;
+    {
+        const int bfrac = fraction_den == 2 ? 128 : (fraction_num == 1 ? 85 : 170);
+        const int below_half = 2 * fraction_num < fraction_den;
+        const double lambda = fmax(1.0, 0.45 * (double)p->pqindex);
+        const uint64_t intra_guard = (uint64_t)llround(lambda * 72.0);
+        const uint64_t intra_marker_bits =
+            (uint64_t)(kMvDiffBits0[35] > kMvDiffBits0[72] ? kMvDiffBits0[35] : kMvDiffBits0[72]) + 1u;
+        const uint64_t ftype = below_half ? 1u : 2u, btype = below_half ? 2u : 1u;
+        uint64_t sel_sad = 0, rate_sad = 0, sel_rate = 1, sel_pixels = 0;
+        uint64_t nf = 0, nb = 0, ni = 0, nd = 0, nintra = 0, moved = 0, frac = 0;
+        for (int my = 0; my < mbh; ++my)
+            for (int mx = 0; mx < mbw; ++mx) {
+                const size_t pos = (size_t)my * mbw + mx;
+                const vc1cu_mv df = b_scale_direct(p, anchor_mvs[pos], bfrac, 0, mode, mx, my);
+                const vc1cu_mv db = b_scale_direct(p, anchor_mvs[pos], bfrac, 1, mode, mx, my);
+                const vc1cu_mv fm = fmv[pos], bm = bmv[pos];
+                uint64_t c[5];
+                vo_b_costs(p, f, past, future, mx, my, fm, bm, df, db, mode, c);
+                const vc1cu_mv fpred = predictor_info(ofm, mbw, mbh, mx, my).pre;
+                const vc1cu_mv bpred = predictor_info(obm, mbw, mbh, mx, my).pre;
+                const uint64_t fbits = mv_rate_bits(p, fm, fpred, mode, 0);
+                const uint64_t bbits = mv_rate_bits(p, bm, bpred, mode, 0);
+                const uint64_t ibits = mv_rate_bits(p, bm, bpred, mode, 1) + mv_rate_bits(p, fm, fpred, mode, 0) + 2;
+                const uint64_t penalty = anchor_4mv[pos] ? 1000000000ull : 0ull;
+                /* candidate order Direct, Forward, Backward, Interpolated (:912-917) */
+                const int cmode[4] = {VC1CU_BMB_DIRECT, VC1CU_BMB_FORWARD, VC1CU_BMB_BACKWARD, VC1CU_BMB_INTERPOLATED};
+                const uint64_t ccost[4] = {c[3] + penalty, c[0] + penalty, c[1] + penalty, c[2]};
+                const uint64_t crate[4] = {0, fbits + ftype, bbits + btype, ibits};
+                int best = 0;
+                long double best_score = (long double)ccost[0] + (long double)(lambda * (double)crate[0]);
+                for (int k = 1; k < 4; ++k) {
+                    const long double sc = (long double)ccost[k] + (long double)(lambda * (double)crate[k]);
+                    if (sc < best_score) { best_score = sc; best = k; }
+                }
+                const uint64_t intra_sad = c[4];
+                uint64_t gate = ccost[best];
+                if (fscreen[pos] < gate) gate = fscreen[pos];
+                if (bscreen[pos] < gate) gate = bscreen[pos];
+                if (out->inter_intra_cost_ratio)
+                    out->inter_intra_cost_ratio[pos] =
+                        gate > 0 ? (double)(intra_sad + intra_guard) / (double)gate : INFINITY;
+                const int choose_intra =
+                    !p->disable_b_intra &&
+                    intra_sad + intra_guard < (uint64_t)llround((double)gate * p->inter_intra_threshold);
+                sel_sad += choose_intra ? intra_sad : ccost[best];
+                rate_sad += ccost[best];
+                sel_rate += choose_intra ? intra_marker_bits : crate[best];
+                sel_pixels += (uint64_t)imax(0, imin(16, p->width - mx * 16)) * (uint64_t)imax(0, imin(16, p->height - my * 16));
+                int m;
+                vc1cu_mv of, ob;
+                if (choose_intra) {
+                    m = VC1CU_BMB_INTRA;
+                    of.xq = of.yq = ob.xq = ob.yq = 0;
+                    ++nintra;
+                } else {
+                    m = cmode[best];
+                    if (m == VC1CU_BMB_DIRECT) { of = df; ob = db; ++nd; }
+                    else if (m == VC1CU_BMB_FORWARD) { of = fm; ob = db; ++nf; }
+                    else if (m == VC1CU_BMB_BACKWARD) { of = df; ob = bm; ++nb; }
+                    else { of = fm; ob = bm; ++ni; }
+                }
+                ofm[pos] = of;
+                obm[pos] = ob;
+                if (out->modes) out->modes[pos] = (uint8_t)m;
+                if (of.xq || of.yq || ob.xq || ob.yq) ++moved;
+#define VO_FRAC_CHROMA(v) (((v).xq & 3) || ((v).yq & 3) || (((v).xq / 4) & 1) || (((v).yq / 4) & 1))
+                if (VO_FRAC_CHROMA(of) || VO_FRAC_CHROMA(ob)) ++frac;
+#undef VO_FRAC_CHROMA
+            }
+        if (out->forward_mvs) memcpy(out->forward_mvs, ofm, mbs * sizeof(vc1cu_mv));
+        if (out->backward_mvs) memcpy(out->backward_mvs, obm, mbs * sizeof(vc1cu_mv));
+        out->forward_macroblocks = nf;
+        out->backward_macroblocks = nb;
+        out->interpolated_macroblocks = ni;
+        out->direct_macroblocks = nd;
+        out->intra_macroblocks = nintra;
+        out->moved_macroblocks = moved;
+        out->fractional_chroma_macroblocks = frac;
+        out->mean_abs_residual = sel_pixels ? (double)sel_sad / (double)sel_pixels : 0.0;
+        out->rate_complexity = sel_pixels ? (double)rate_sad / (double)sel_pixels : 0.0;
+        out->motion_sad = sel_sad;
+        out->motion_bits = sel_rate;
+        out->mv_mode = mode;
+    }
+done:
+    free(fmv); free(bmv); free(fscreen); free(bscreen); free(ofm); free(obm);
+    return rc;
 }

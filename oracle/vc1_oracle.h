@@ -74,6 +74,13 @@ int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* cur, const vo_frame
                       int allow_intra, const vc1cu_mv* seed, const vc1cu_panalysis* seed_distant,
                       vc1cu_panalysis* out);
 
+/* B-picture analysis: the two core passes + the per-MB mode decision */
+void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
+                int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]);
+int vo_analyze_b(const vc1cu_params* p, const vo_frame* cur, const vo_frame* past, const vo_frame* future,
+                 const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv, int fraction_num, int fraction_den,
+                 int mode, vc1cu_banalysis* out);
+
 /* prediction of an MV field (motion_compensate_mb / _4mv); dst planes tight */
 void vo_motion_compensate(const vc1cu_params* p, const vo_frame* ref, const vc1cu_mv* mvs,
                           const vc1cu_mv* block_mvs, const uint8_t* use_4mv, int mode, uint8_t* dy,

@@ -13,9 +13,13 @@ script calls it through oracle.Reference on inputs restated from the reference's
                     final Mixed-MV pass with P-intra) on seeded synthetic pictures
   xform_kat.npz     forward transform + quantiser of a motion-compensated prediction
   global_kat.npz    whole-frame translation search and frame SADs
+  b_kat.npz         analyze_b_picture_mode (two core passes + the per-MB B mode decision) of a
+                    seeded three-picture group, anchor vectors from the future picture's own
+                    Mixed-MV analysis, several fractions, modes and parameter sets
 
 Run it where the reference tree is present (it is not needed to run the tests):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py b_kat      # only the named ones
 """
 from __future__ import annotations
 
@@ -125,7 +129,48 @@ def flatten(prefix, a, d):
         d[f"{prefix}.total.{k}"] = np.array(v)
 
 
-def main():
+# B-picture fixtures: (mode, fraction_num, fraction_den, params)
+B_CASES = (
+    (MV_QPEL, 1, 2, dict(display_width=125, display_height=93, search_range=16, local_search_range=16)),
+    (MV_HPEL_BILINEAR, 1, 3, dict(display_width=125, display_height=93, search_range=16, local_search_range=16)),
+    (MV_QPEL, 2, 3, dict(search_range=16, local_search_range=16, rnd=1, pqindex=20)),
+    (MV_HPEL, 1, 2, dict(display_width=125, display_height=93, search_range=24, local_search_range=8)),
+    (MV_MIXED, 1, 3, dict(search_range=16, local_search_range=16, pqindex=3)),
+    (MV_QPEL, 1, 2, dict(search_range=16, local_search_range=16, disable_b_intra=1)),
+)
+
+
+def make_b_kat():
+    from oracle import Reference
+
+    clip = synth.generate(130, 98, 3, 15)
+    past, cur, fut = clip.frame(0), clip.frame(1), clip.frame(2)
+    d = {}
+    for c, pl in zip("yuv", past):
+        d[f"past.{c}"] = pl
+    for c, pl in zip("yuv", cur):
+        d[f"cur.{c}"] = pl
+    for c, pl in zip("yuv", fut):
+        d[f"future.{c}"] = pl
+    p0 = make_params(130, 98, search_range=16, local_search_range=16)
+    R = Reference(p0)
+    rp, rf = R.frame(past), R.frame(fut)
+    q = R.analyze_p_core(rf, rp, MV_QPEL, False)
+    anc = R.analyze_p_core(rf, rp, MV_MIXED, True, seed=q.mvs, seed_distant=q)
+    d["anchor.mvs"], d["anchor.use_4mv"] = anc.mvs, anc.use_4mv
+    for i, (mode, num, den, kw) in enumerate(B_CASES):
+        p = make_params(130, 98, **kw)
+        R = Reference(p)
+        b = R.analyze_b(R.frame(cur), R.frame(past), R.frame(fut), anc.mvs, anc.use_4mv, num, den, mode)
+        flatten(f"b{i}", b, d)
+    np.savez_compressed(os.path.join(HERE, "b_kat.npz"), **d)
+
+
+def main(only=()):
+    if only:
+        for name in only:
+            {"b_kat": make_b_kat}[name]()
+        return
     from oracle import Reference, ref_available
 
     if not ref_available():
@@ -240,10 +285,11 @@ def main():
         d[f"g{i}.frame_sad"] = np.array([[R.frame_sad(rc, rr, dx, dy, s) for s in (1, 2, 4)] for dx, dy in offs],
                                         np.uint64)
     np.savez_compressed(os.path.join(HERE, "global_kat.npz"), **d)
+    make_b_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -155,6 +155,40 @@ def test_global_golden(oracle):
         assert got == g[f"g{i}.frame_sad"].tolist()
 
 
+# analyze_b_picture_mode fixtures (tests/golden/make_golden.py B_CASES)
+B_CASES = (
+    (MV_QPEL, 1, 2, dict(display_width=125, display_height=93, search_range=16, local_search_range=16)),
+    (MV_HPEL_BILINEAR, 1, 3, dict(display_width=125, display_height=93, search_range=16, local_search_range=16)),
+    (MV_QPEL, 2, 3, dict(search_range=16, local_search_range=16, rnd=1, pqindex=20)),
+    (MV_HPEL, 1, 2, dict(display_width=125, display_height=93, search_range=24, local_search_range=8)),
+    (MV_MIXED, 1, 3, dict(search_range=16, local_search_range=16, pqindex=3)),
+    (MV_QPEL, 1, 2, dict(search_range=16, local_search_range=16, disable_b_intra=1)),
+)
+
+
+@pytest.mark.parametrize("i", range(len(B_CASES)))
+def test_b_analysis_golden(oracle, i):
+    """B-picture analysis (both core passes + the per-MB mode decision) against the reference."""
+    g = load("b_kat.npz")
+    past, cur, fut = _frames(g, "past"), _frames(g, "cur"), _frames(g, "future")
+    mode, num, den, kw = B_CASES[i]
+    p = make_params(130, 98, **kw)
+    b = oracle.analyze_b(p, cur, past, fut, g["anchor.mvs"], g["anchor.use_4mv"], num, den, mode)
+    for field in b.ARRAYS:
+        got, want = getattr(b, field), g[f"b{i}.{field}"]
+        if got.dtype == np.float64:
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), field
+        else:
+            assert np.array_equal(got, want), field
+    for k, v in b.totals.items():
+        w = g[f"b{i}.total.{k}"]
+        assert (np.float64(v).view(np.uint64) == w.view(np.uint64)) if w.dtype == np.float64 else int(v) == int(w), k
+    # every decision kind the fixture set is meant to cover
+    if i == 0:
+        modes = set(np.concatenate([g[f"b{j}.modes"] for j in range(len(B_CASES))]).tolist())
+        assert modes == {0, 1, 2, 3, 4}
+
+
 def test_synthetic_clip_is_deterministic():
     a = synth.generate(64, 48, 3, 17)
     b = synth.generate(64, 48, 3, 17)
@@ -218,3 +252,21 @@ def test_analysis_matches_reference_live(oracle, kw):
     for mode in (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED):
         em = R.analyze_p_core(rc, rr, mode, True, seed=e.mvs, seed_distant=e)
         assert oracle.analyze_p_core(p, cur, ref, mode, True, seed=e.mvs, seed_distant=e).equal(em) == [], mode
+
+
+@pytest.mark.parametrize("case", [(MV_QPEL, 1, 2, 13, dict(display_width=97, display_height=65, search_range=16,
+                                                            local_search_range=16)),
+                                  (MV_HPEL_BILINEAR, 2, 3, 14, dict(search_range=16, local_search_range=16, rnd=1)),
+                                  (MV_QPEL, 1, 3, 17, dict(search_range=0, local_search_range=0)),
+                                  (MV_QPEL, 2, 3, 19, dict(search_range=96, local_search_range=8, long_range_mode=1))])
+def test_b_analysis_matches_reference_live(oracle, case):
+    Reference = _ref_or_skip()
+    mode, num, den, seed, kw = case
+    clip = synth.generate(98, 66, 3, seed)
+    p = make_params(98, 66, **kw)
+    R = Reference(p)
+    past, cur, fut = clip.frame(0), clip.frame(1), clip.frame(2)
+    rp, rc, rf = R.frame(past), R.frame(cur), R.frame(fut)
+    anc = R.analyze_p_core(rf, rp, MV_MIXED, True, seed=R.analyze_p_core(rf, rp, MV_QPEL, False).mvs)
+    e = R.analyze_b(rc, rp, rf, anc.mvs, anc.use_4mv, num, den, mode)
+    assert oracle.analyze_b(p, cur, past, fut, anc.mvs, anc.use_4mv, num, den, mode).equal(e) == []
