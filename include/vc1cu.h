@@ -151,6 +151,7 @@ typedef struct vc1cu_timing {
     double xform_ms;     /* forward transform + quantiser */
     uint64_t core_launches;
     uint64_t xform_launches;
+    double b_ms;         /* B-picture decision (b_cost_kernel + b_decide_kernel) */
 } vc1cu_timing;
 
 /* ---- context (VulkanComputeContext::create / device_name / device_index) ---------- */
@@ -267,7 +268,7 @@ enum {
  * Vc1Encoder::BAnalysis (src/encoder_internal.h:408-434). Per-macroblock HOST arrays of
  * mbw*mbh entries; any pointer may be NULL to skip it. The distant_* arrays are the two
  * core passes' own (PAnalysis::distant_*), copied through as the reference does
- * (encoder_motion.cpp:812-817). The scalar fields are written by the call.
+ * (encoder_motion.cpp:810-815). The scalar fields are written by the call.
  */
 typedef struct vc1cu_banalysis {
     uint8_t* modes;                     /* VC1CU_BMB_* */

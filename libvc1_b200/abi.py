@@ -62,7 +62,7 @@ class Counters(C.Structure):
 class Timing(C.Structure):
     _fields_ = [("core_ms", C.c_double), ("global_ms", C.c_double), ("totals_ms", C.c_double),
                 ("mc_ms", C.c_double), ("xform_ms", C.c_double), ("core_launches", C.c_uint64),
-                ("xform_launches", C.c_uint64)]
+                ("xform_launches", C.c_uint64), ("b_ms", C.c_double)]
 
 
 def make_params(width: int, height: int, **kw) -> Params:

@@ -19,8 +19,8 @@ import os
 
 import numpy as np
 
-from .abi import (Analysis, Counters, ERRORS, Timing, MV_QPEL, METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params,
-                  mbs_of)
+from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, Timing, MV_QPEL, METRIC_SAD, METRIC_SATD,
+                  Mv, PAnalysisC, Params, mbs_of)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
@@ -33,7 +33,8 @@ EXPORTS = (
     "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
-    "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc",
+    "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
+    "vc1cu_read_bresult",
 )
 
 
@@ -79,6 +80,9 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_stream.argtypes = [vp]
     L.vc1cu_stream.restype = vp
     L.vc1cu_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
+    L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
+    L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
     _LIB = L
@@ -241,6 +245,36 @@ class CudaComputeContext:
 
     def synchronize(self):
         self._check(self._L.vc1cu_synchronize(self._h))
+
+    def analyze_b_picture(self, params: Params, cur_id: int, past_id: int, future_id: int, anchor_mvs, anchor_4mv,
+                          fraction_num: int, fraction_den: int, mode: int = MV_QPEL) -> BAnalysis:
+        """One Vc1Encoder::analyze_b_picture_mode (src/encoder_motion.cpp:753-1005): forward and
+        backward core passes plus the per-macroblock B mode decision. anchor_mvs / anchor_4mv are
+        the future P anchor's MVs and Mixed-MV flags."""
+        mbw, mbh = mbs_of(params)
+        am = np.ascontiguousarray(anchor_mvs, np.int32).reshape(-1, 2)
+        a4 = np.ascontiguousarray(anchor_4mv, np.uint8).reshape(-1)
+        if len(am) != mbw * mbh or len(a4) != mbw * mbh:
+            raise ValueError("B analysis needs the future anchor's collocated P MV/type fields")
+        out = BAnalysis.empty(mbw * mbh)
+        oc = out.as_c()
+        self._check(self._L.vc1cu_analyze_b_picture(self._h, C.byref(params), cur_id, past_id, future_id,
+                                                    am.ctypes.data, a4.ctypes.data, fraction_num, fraction_den,
+                                                    mode, C.byref(oc)))
+        return out.take_totals(oc)
+
+    def b_decide(self, params: Params, bpasses):
+        """bpasses: iterable of (cur_id, past_id, future_id, fwd_slot, bwd_slot, anchor_slot,
+        fraction_num, fraction_den, mode, out_bslot[, pqindex])."""
+        arr = (BPass * len(bpasses))(*[BPass(*b) for b in bpasses])
+        self._check(self._L.vc1cu_b_decide(self._h, C.byref(params), arr, len(bpasses)))
+
+    def read_bresult(self, params: Params, bslot: int) -> BAnalysis:
+        mbw, mbh = mbs_of(params)
+        out = BAnalysis.empty(mbw * mbh)
+        oc = out.as_c()
+        self._check(self._L.vc1cu_read_bresult(self._h, bslot, C.byref(oc)))
+        return out.take_totals(oc)
 
     def motion_compensate(self, params: Params, ref_id: int, mv_slot: int, mv_mode: int, pred_id: int):
         self._check(self._L.vc1cu_motion_compensate(self._h, C.byref(params), ref_id, mv_slot, mv_mode, pred_id))

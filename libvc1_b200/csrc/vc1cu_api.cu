@@ -43,6 +43,7 @@ void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred,
 void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int n, unsigned long long* out,
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
+cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
 }  // namespace vc1cu
 
 using namespace vc1cu;
@@ -52,6 +53,11 @@ namespace {
 constexpr int kMaxSlot = 4096;
 constexpr int kInternalOut = kMaxSlot + 1;   // result slot of vc1cu_analyze_p_core
 constexpr int kInternalSeed = kMaxSlot + 2;  // its seed
+constexpr int kInternalFwd = kMaxSlot + 3;   // the forward / backward core passes and the anchor
+constexpr int kInternalBwd = kMaxSlot + 4;   // of vc1cu_analyze_b_picture
+constexpr int kInternalAnchor = kMaxSlot + 5;
+constexpr int kInternalLast = kInternalAnchor;
+constexpr int kInternalB = kMaxSlot + 1;     // B-result slot of vc1cu_analyze_b_picture
 constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
 #ifndef VC1CU_SEEDED_MIXED_RW
 #define VC1CU_SEEDED_MIXED_RW 8
@@ -94,6 +100,17 @@ struct ResultSlot {
     int mbs = 0;
     DevResult r{};
     bool valid = false;
+    int mode = -1;         // how the slot's last pass ran (-1: uploaded, not computed)
+    bool seeded = false;
+    bool allow_intra = false;
+};
+
+struct BSlot {
+    void* d = nullptr;
+    int mbs = 0;
+    DevBResult r{};
+    bool valid = false;
+    int mode = 0;
 };
 
 struct CacheSlot {
@@ -132,12 +149,15 @@ struct vc1cu_ctx {
     std::string err;
     std::unordered_map<int, FrameSlot> frames;
     std::unordered_map<int, ResultSlot> results;
+    std::unordered_map<int, BSlot> bresults;
     CacheSlot cache[8];
     uint64_t age = 0;
     vc1cu_counters counters{};
     LaunchStatus* d_status = nullptr;
     PassDesc* d_passes = nullptr;
     int passes_cap = 0;
+    BDesc* d_bdescs = nullptr;
+    int bdescs_cap = 0;
     GState* d_gstates = nullptr;
     int gstates_cap = 0;
     void* d_lr = nullptr;      // long-range signature indexes of a launch's reference pictures
@@ -238,6 +258,7 @@ int make_dev_params(const vc1cu_params* p, DevParams& P, std::string& why) {
     P.long_range_mode = p->long_range_mode;
     P.rnd = p->rnd != 0;
     P.disable_p_intra = p->disable_p_intra != 0;
+    P.disable_b_intra = p->disable_b_intra != 0;
     const int r = p->search_range;
     P.mvrange = r <= 31 ? 0 : (r <= 63 ? 1 : (r <= 127 ? 2 : 3));
     const double lam = 0.35 * static_cast<double>(p->pqindex);
@@ -409,7 +430,7 @@ void sync_checked(vc1cu_ctx* c) {
     ck(cudaGetLastError(), "kernel");
 }
 
-enum Family { kCore = 0, kGlobal = 1, kTotals = 2, kMc = 3, kXform = 4, kScore = 5 };
+enum Family { kCore = 0, kGlobal = 1, kTotals = 2, kMc = 3, kXform = 4, kScore = 5, kB = 6 };
 
 cudaEvent_t take_event(vc1cu_ctx* c) {
     if (!c->event_pool.empty()) {
@@ -456,6 +477,7 @@ void collect_timing(vc1cu_ctx* c) {
             case kTotals: c->tsum.totals_ms += ms; break;
             case kMc: c->tsum.mc_ms += ms; break;
             case kXform: c->tsum.xform_ms += ms; c->tsum.xform_launches++; break;
+            case kB: c->tsum.b_ms += ms; break;
             default: break;
         }
         c->event_pool.push_back(t.a);
@@ -512,7 +534,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     for (int i = 0; i < n; ++i) {
         const vc1cu_pass& q = passes[i];
         if (q.mode < 0 || q.mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
-        if (q.out_slot < 0 || q.out_slot > kInternalSeed || q.seed_slot == q.out_slot)
+        if (q.out_slot < 0 || q.out_slot > kInternalLast || q.seed_slot == q.out_slot)
             throw Fail{VC1CU_ERR_ARG, "invalid result slot"};
         FrameSlot& fc = frame_slot(c, q.cur_id);
         FrameSlot& fr = frame_slot(c, q.ref_id);
@@ -547,7 +569,13 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
             unseeded.push_back(i);
         }
     }
-    for (int i = 0; i < n; ++i) h[i].out = result_slot(c, passes[i].out_slot, mbs, true).r;
+    for (int i = 0; i < n; ++i) {
+        ResultSlot& o = result_slot(c, passes[i].out_slot, mbs, true);
+        o.mode = passes[i].mode;
+        o.seeded = passes[i].seed_slot >= 0;
+        o.allow_intra = passes[i].allow_intra != 0;
+        h[i].out = o.r;
+    }
     // seed levels of in-launch seeds (a chain, never a cycle)
     std::vector<int> level(n, 0);
     for (int i = 0; i < n; ++i) {
@@ -765,6 +793,163 @@ void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
     out->global_full_sad = gsad;
 }
 
+BSlot& bresult_slot(vc1cu_ctx* c, int id, int mbs) {
+    auto& s = c->bresults[id];
+    if (s.d && s.mbs == mbs) {
+        s.valid = true;
+        return s;
+    }
+    if (s.d) cudaFree(s.d);
+    s = BSlot{};
+    const size_t n = (size_t)mbs;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bytes = al(n) * 3 + al(8 * n) * 7 + al(16 * n) + al(4 * n) + al(8 * kBTotCount) + al(16);
+    ck(cudaMalloc(&s.d, bytes), "cudaMalloc(B result slot)");
+    ck(cudaMemsetAsync(s.d, 0, bytes, c->stream), "cudaMemsetAsync(B result slot)");
+    uint8_t* p = static_cast<uint8_t*>(s.d);
+    auto take = [&](size_t b) { uint8_t* q = p; p += al(b); return q; };
+    s.r.modes = take(n);
+    s.r.fmv = (int2*)take(8 * n);
+    s.r.bmv = (int2*)take(8 * n);
+    s.r.ratio = (double*)take(8 * n);
+    s.r.fdl = (double*)take(8 * n);
+    s.r.fdc = (double*)take(8 * n);
+    s.r.fdd = take(n);
+    s.r.bdl = (double*)take(8 * n);
+    s.r.bdc = (double*)take(8 * n);
+    s.r.bdd = take(n);
+    s.r.cost = (uint4*)take(16 * n);
+    s.r.intra = (uint32_t*)take(4 * n);
+    s.r.itotals = (unsigned long long*)take(8 * kBTotCount);
+    s.r.totals = (double*)take(16);
+    s.mbs = mbs;
+    s.valid = true;
+    return s;
+}
+
+// A core result slot usable as one direction of a B picture: an unseeded pass with P-intra
+// off in the B picture's mode (analyze_b_picture_mode, encoder_motion.cpp:800-801).
+const ResultSlot& b_direction(vc1cu_ctx* c, int slot, int mbs, int mode, const char* what) {
+    const ResultSlot& s = result_slot(c, slot, mbs, false);
+    if (s.mode != mode || s.seeded || s.allow_intra)
+        throw Fail{VC1CU_ERR_ARG, std::string(what) + " slot does not hold an unseeded, P-intra-off core pass of this mode"};
+    return s;
+}
+
+// Decision stage of a batch of B pictures (b_cost_kernel + b_decide_kernel).
+void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, int max_out) {
+    DevParams P;
+    std::string why;
+    const int rc = make_dev_params(p, P, why);
+    if (rc) throw Fail{rc, why};
+    if (n <= 0) return;
+    const int mbs = P.mbw * P.mbh;
+    std::vector<BDesc> h(n);
+    for (int i = 0; i < n; ++i) {
+        const vc1cu_bpass& q = b[i];
+        if (!((q.fraction_den == 2 && q.fraction_num == 1) ||
+              (q.fraction_den == 3 && (q.fraction_num == 1 || q.fraction_num == 2))))
+            throw Fail{VC1CU_ERR_ARG, "unsupported B-picture temporal fraction (1/2, 1/3 and 2/3 are)"};
+        if (q.mode < 0 || q.mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        if (q.pqindex < 0 || q.pqindex > 31) throw Fail{VC1CU_ERR_ARG, "pass pqindex must be 0 (params) or 1..31"};
+        if (q.out_bslot < 0 || q.out_bslot > max_out) throw Fail{VC1CU_ERR_ARG, "B-result slot out of range"};
+        for (int j = 0; j < i; ++j)
+            if (b[j].out_bslot == q.out_bslot) throw Fail{VC1CU_ERR_ARG, "two B pictures of one call share a result slot"};
+        FrameSlot& fc = frame_slot(c, q.cur_id);
+        FrameSlot& fp = frame_slot(c, q.past_id);
+        FrameSlot& ff = frame_slot(c, q.future_id);
+        if (fc.w != P.W || fc.h != P.H || fp.w != P.W || fp.h != P.H || ff.w != P.W || ff.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "B-picture reference dimensions do not match the configuration"};
+        const ResultSlot& fs = b_direction(c, q.fwd_slot, mbs, q.mode, "forward");
+        const ResultSlot& bs = b_direction(c, q.bwd_slot, mbs, q.mode, "backward");
+        const ResultSlot& as = result_slot(c, q.anchor_slot, mbs, false);
+        BDesc& d = h[i];
+        d.cur = fc.view();
+        d.past = fp.view();
+        d.future = ff.view();
+        d.fmv = fs.r.mvs;
+        d.bmv = bs.r.mvs;
+        d.fscreen = fs.r.screen;
+        d.bscreen = bs.r.screen;
+        d.fdl = fs.r.dl;
+        d.fdc = fs.r.dc;
+        d.fdd = fs.r.dd;
+        d.bdl = bs.r.dl;
+        d.bdc = bs.r.dc;
+        d.bdd = bs.r.dd;
+        d.anchor = as.r.mvs;
+        d.anchor4 = as.r.use4;
+        d.bfrac = q.fraction_den == 2 ? 128 : (q.fraction_num == 1 ? 85 : 170);
+        d.below_half = 2 * q.fraction_num < q.fraction_den;
+        d.mode = q.mode;
+        // lambda = max(1, 0.45*PQ) (encoder_motion.cpp:919), split as lam_m * 2^-lam_s exactly
+        const int pq = q.pqindex ? q.pqindex : P.pq;
+        const double lambda = std::max(1.0, 0.45 * static_cast<double>(pq));
+        int e = 0;
+        const double fr = std::frexp(lambda, &e);
+        d.lam_m = static_cast<uint64_t>(std::ldexp(fr, 53));
+        d.lam_s = 53 - e;
+        d.intra_guard = static_cast<uint64_t>(std::llround(lambda * 72.0));
+    }
+    for (int i = 0; i < n; ++i) {
+        BSlot& o = bresult_slot(c, b[i].out_bslot, mbs);
+        o.mode = b[i].mode;
+        h[i].out = o.r;
+    }
+    if (c->bdescs_cap < n) {
+        if (c->d_bdescs) cudaFree(c->d_bdescs);
+        c->d_bdescs = nullptr;
+        c->bdescs_cap = 0;
+        void* d = nullptr;
+        ck(cudaMalloc(&d, sizeof(BDesc) * n), "cudaMalloc(B descriptors)");
+        c->d_bdescs = static_cast<BDesc*>(d);
+        c->bdescs_cap = n;
+    }
+    void* hp = staging(c, sizeof(BDesc) * n);
+    std::memcpy(hp, h.data(), sizeof(BDesc) * n);
+    ck(cudaMemcpyAsync(c->d_bdescs, hp, sizeof(BDesc) * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(B descriptors)");
+    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    Timer tm(c, kB);
+    ck(launch_bpictures(P, c->d_bdescs, n, c->stream), "B-picture kernel launch");
+    tm.stop(2);
+    c->counters.macroblocks_analysed += (uint64_t)mbs * (uint64_t)n;
+}
+
+void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
+    const size_t n = (size_t)s.mbs;
+    auto cp = [&](void* dst, const void* src, size_t b) {
+        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(B result)");
+    };
+    cp(out->modes, s.r.modes, n);
+    cp(out->forward_mvs, s.r.fmv, 8 * n);
+    cp(out->backward_mvs, s.r.bmv, 8 * n);
+    cp(out->inter_intra_cost_ratio, s.r.ratio, 8 * n);
+    cp(out->forward_distant_local_mae, s.r.fdl, 8 * n);
+    cp(out->forward_distant_candidate_mae, s.r.fdc, 8 * n);
+    cp(out->forward_distant_match_decision, s.r.fdd, n);
+    cp(out->backward_distant_local_mae, s.r.bdl, 8 * n);
+    cp(out->backward_distant_candidate_mae, s.r.bdc, 8 * n);
+    cp(out->backward_distant_match_decision, s.r.bdd, n);
+    unsigned long long it[kBTotCount];
+    double tot[2];
+    cp(it, s.r.itotals, sizeof it);
+    cp(tot, s.r.totals, sizeof tot);
+    sync_checked(c);
+    out->forward_macroblocks = it[kBTotForward];
+    out->backward_macroblocks = it[kBTotBackward];
+    out->interpolated_macroblocks = it[kBTotInterpolated];
+    out->direct_macroblocks = it[kBTotDirect];
+    out->intra_macroblocks = it[kBTotIntra];
+    out->moved_macroblocks = it[kBTotMoved];
+    out->fractional_chroma_macroblocks = it[kBTotFrac];
+    out->mean_abs_residual = tot[0];
+    out->rate_complexity = tot[1];
+    out->motion_sad = it[kBTotSelSad];
+    out->motion_bits = it[kBTotSelRate];
+    out->mv_mode = s.mode;
+    out->reserved = 0;
+}
+
 }  // namespace
 
 // ---- C ABI -------------------------------------------------------------------------------
@@ -833,6 +1018,9 @@ int vc1cu_close(vc1cu_ctx* c) {
         if (kv.second.d) cudaFree(kv.second.d);
     for (auto& kv : c->results)
         if (kv.second.d) cudaFree(kv.second.d);
+    for (auto& kv : c->bresults)
+        if (kv.second.d) cudaFree(kv.second.d);
+    if (c->d_bdescs) cudaFree(c->d_bdescs);
     for (auto& s : c->cache)
         if (s.d) cudaFree(s.d);
     if (c->d_status) cudaFree(c->d_status);
@@ -1034,6 +1222,63 @@ int vc1cu_analyze_p_core(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int re
             out->global_dx = out->global_dy = 0;
             out->global_full_sad = 0;
         }
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_b_decide(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* passes, int n) {
+    return guarded(c, [&]() -> int {
+        if (n < 0 || (n > 0 && !passes)) throw Fail{VC1CU_ERR_ARG, "invalid B pass list"};
+        for (int i = 0; i < n; ++i) {
+            const vc1cu_bpass& q = passes[i];
+            if (q.fwd_slot < 0 || q.fwd_slot >= kMaxSlot || q.bwd_slot < 0 || q.bwd_slot >= kMaxSlot ||
+                q.anchor_slot < 0 || q.anchor_slot >= kMaxSlot)
+                throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+        }
+        launch_b(c, p, passes, n, kMaxSlot - 1);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_read_bresult(vc1cu_ctx* c, int bslot, vc1cu_banalysis* out) {
+    return guarded(c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        check_status(c);
+        auto it = c->bresults.find(bslot);
+        if (it == c->bresults.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "empty B-result slot"};
+        read_bresult(c, it->second, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_analyze_b_picture(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int past_id, int future_id,
+                            const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv, int fraction_num, int fraction_den,
+                            int mode, vc1cu_banalysis* out) {
+    return guarded(c, [&]() -> int {
+        if (!out || !anchor_mvs || !anchor_4mv) throw Fail{VC1CU_ERR_ARG, "null output or anchor field"};
+        if (!((fraction_den == 2 && fraction_num == 1) || (fraction_den == 3 && (fraction_num == 1 || fraction_num == 2))))
+            throw Fail{VC1CU_ERR_ARG, "unsupported B-picture temporal fraction (1/2, 1/3 and 2/3 are)"};
+        if (mode < 0 || mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        // the direct-mode scaling multiplies anchor components by at most 256 in 32-bit ints
+        for (int i = 0; i < mbs; ++i)
+            if (anchor_mvs[i].xq < -65536 || anchor_mvs[i].xq > 65536 || anchor_mvs[i].yq < -65536 || anchor_mvs[i].yq > 65536)
+                throw Fail{VC1CU_ERR_ARG, "anchor MV component outside +-65536 quarter pixels"};
+        ResultSlot& as = result_slot(c, kInternalAnchor, mbs, true);
+        as.mode = -1;
+        ck(cudaMemcpyAsync(as.r.mvs, anchor_mvs, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload anchor");
+        ck(cudaMemcpyAsync(as.r.use4, anchor_4mv, (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload anchor");
+        const vc1cu_pass q[2] = {{cur_id, past_id, mode, 0, -1, kInternalFwd, 0}, {cur_id, future_id, mode, 0, -1, kInternalBwd, 0}};
+        launch_passes(c, p, q, 2);
+        const vc1cu_bpass b{cur_id, past_id, future_id, kInternalFwd, kInternalBwd, kInternalAnchor,
+                            fraction_num, fraction_den, mode, kInternalB, 0};
+        launch_b(c, p, &b, 1, kInternalB);
+        check_status(c);
+        read_bresult(c, c->bresults[kInternalB], out);
         return VC1CU_OK;
     });
 }

@@ -25,7 +25,7 @@ struct DevParams {
     int local_range;     // min(range, local range)
     int me_algorithm, me_quality;
     int subpel, fast_subpel, subpel_range;
-    int long_range_mode, rnd, disable_p_intra;
+    int long_range_mode, rnd, disable_p_intra, disable_b_intra;
     int mvrange;         // motion_mvrange()
     double lambda;       // max(1, 0.35*PQ), the Mixed-MV / intra lambda
     uint64_t lam_m;      // lambda = lam_m * 2^-lam_s exactly
@@ -67,20 +67,31 @@ __host__ __device__ inline bool hidden_luma(const DevParams& p, int x0, int y0, 
     return (p.right_pad && x0 + aw - 1 + ix + right >= p.vw) || (p.bottom_pad && y0 + ah - 1 + iy + bottom >= p.vh);
 }
 
-// Vc1Encoder::motion_uses_hidden_chroma, encoder_motion.cpp:2167-2189 (P pictures: future = false)
-__host__ __device__ inline bool hidden_chroma(const DevParams& p, int x0, int y0, int bw, int bh, int xq, int yq) {
+// Vc1Encoder::motion_uses_hidden_chroma, encoder_motion.cpp:2167-2189. future: the B
+// future-reference rounding of the chroma vector (away from zero instead of towards it).
+__host__ __device__ inline bool hidden_chroma_f(const DevParams& p, int x0, int y0, int bw, int bh, int xq, int yq,
+                                                bool future) {
     if (!p.cright_pad && !p.cbottom_pad) return false;
     const int cx = x0 / 2, cy = y0 / 2;
     const int aw = imax(0, imin(bw / 2, p.cvw - cx)), ah = imax(0, imin(bh / 2, p.cvh - cy));
     if (!aw || !ah) return false;
     int uvx = arshift(xq + ((xq & 3) == 3), 1);
     int uvy = arshift(yq + ((yq & 3) == 3), 1);
-    uvx = uvx < 0 ? uvx + (uvx & 1) : uvx - (uvx & 1);
-    uvy = uvy < 0 ? uvy + (uvy & 1) : uvy - (uvy & 1);
+    if (future) {
+        uvx = uvx < 0 ? uvx - (uvx & 1) : uvx + (uvx & 1);
+        uvy = uvy < 0 ? uvy - (uvy & 1) : uvy + (uvy & 1);
+    } else {
+        uvx = uvx < 0 ? uvx + (uvx & 1) : uvx - (uvx & 1);
+        uvy = uvy < 0 ? uvy + (uvy & 1) : uvy - (uvy & 1);
+    }
     const int ix = floor_div4(uvx), iy = floor_div4(uvy);
     const bool fx = (uvx - ix * 4) != 0, fy = (uvy - iy * 4) != 0;
     return (p.cright_pad && cx + aw - 1 + ix + (fx ? 1 : 0) >= p.cvw) ||
            (p.cbottom_pad && cy + ah - 1 + iy + (fy ? 1 : 0) >= p.cvh);
+}
+// P pictures: future = false
+__host__ __device__ inline bool hidden_chroma(const DevParams& p, int x0, int y0, int bw, int bh, int xq, int yq) {
+    return hidden_chroma_f(p, x0, y0, bw, bh, xq, yq, false);
 }
 
 // Vc1Encoder::motion_uses_hidden_padding, encoder_motion.cpp:2191-2195

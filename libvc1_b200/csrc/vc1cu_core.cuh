@@ -87,4 +87,51 @@ struct LaunchStatus {
     unsigned int timeouts;
 };
 
+// One B-result slot (Vc1Encoder::BAnalysis) in HBM, structure of arrays over macroblocks.
+struct DevBResult {
+    uint8_t* modes;
+    int2* fmv;                 // decoder forward / backward MV state
+    int2* bmv;
+    double* ratio;
+    double* fdl;               // the core passes' distant_* arrays, copied through
+    double* fdc;
+    uint8_t* fdd;
+    double* bdl;
+    double* bdc;
+    uint8_t* bdd;
+    uint4* cost;               // per MB: forward, backward, interpolated, direct SAD (kBCostInvalid: 2^54)
+    uint32_t* intra;           // per MB: the four-8x8 mean proxy
+    unsigned long long* itotals;  // kBTot* below
+    double* totals;            // mean_abs_residual, rate_complexity
+};
+constexpr uint32_t kBCostInvalid = 0xFFFFFFFFu;
+enum {
+    kBTotForward = 0, kBTotBackward, kBTotInterpolated, kBTotDirect, kBTotIntra, kBTotMoved, kBTotFrac,
+    kBTotSelSad, kBTotRateSad, kBTotSelRate, kBTotPixels, kBTotCount
+};
+
+// One B picture's decision stage (encoder_motion.cpp:817-1001).
+struct BDesc {
+    DevFrame cur, past, future;
+    const int2* fmv;           // forward / backward core passes
+    const int2* bmv;
+    const uint64_t* fscreen;
+    const uint64_t* bscreen;
+    const double* fdl;
+    const double* fdc;
+    const uint8_t* fdd;
+    const double* bdl;
+    const double* bdc;
+    const uint8_t* bdd;
+    const int2* anchor;        // the future anchor's MVs and Mixed-MV flags
+    const uint8_t* anchor4;
+    int bfrac;                 // BFRACTION scale: 128 (1/2), 85 (1/3), 170 (2/3)
+    int below_half;
+    int mode;
+    uint64_t lam_m;            // B lambda max(1, 0.45*PQ) = lam_m * 2^-lam_s exactly
+    int lam_s;
+    uint64_t intra_guard;      // llround(lambda * 72)
+    DevBResult out;
+};
+
 }  // namespace vc1cu

@@ -1952,10 +1952,10 @@ static int b_unsafe(const vc1cu_params* p, int x0, int y0, vc1cu_mv mv, int mode
     return hidden_luma(p, x0, y0, 16, 16, mv.xq, mv.yq, mode) || hidden_chroma_f(p, x0, y0, 16, 16, mv.xq, mv.yq, future);
 }
 
-/* The four candidate costs of one B macroblock (encoder_motion.cpp:846-887): SAD of the
+/* The four candidate costs of one B macroblock (encoder_motion.cpp:844-888): SAD of the
  * forward, backward, interpolated ((pf+pb+1)>>1) and direct predictions over the coded
  * raster, each replaced by 2^54 when a reference it uses reads hidden padding. Also the
- * four-8x8 mean proxy of the B-intra decision (:929-937). */
+ * four-8x8 mean proxy of the B-intra decision (:936-943). */
 void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
                 int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]) {
     const int x0 = mx * 16, y0 = my * 16;
@@ -2047,7 +2047,7 @@ int vo_analyze_b(const vc1cu_params* p, const vo_frame* f, const vo_frame* past,
                 const uint64_t bbits = mv_rate_bits(p, bm, bpred, mode, 0);
                 const uint64_t ibits = mv_rate_bits(p, bm, bpred, mode, 1) + mv_rate_bits(p, fm, fpred, mode, 0) + 2;
                 const uint64_t penalty = anchor_4mv[pos] ? 1000000000ull : 0ull;
-                /* candidate order Direct, Forward, Backward, Interpolated (:912-917) */
+                /* candidate order Direct, Forward, Backward, Interpolated (:920-925) */
                 const int cmode[4] = {VC1CU_BMB_DIRECT, VC1CU_BMB_FORWARD, VC1CU_BMB_BACKWARD, VC1CU_BMB_INTERPOLATED};
                 const uint64_t ccost[4] = {c[3] + penalty, c[0] + penalty, c[1] + penalty, c[2]};
                 const uint64_t crate[4] = {0, fbits + ftype, bbits + btype, ibits};

@@ -23,14 +23,39 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
 
 
-def test_struct_layouts_match_header():
-    # vc1cu_params: 18 int32 + 2 double; vc1cu_panalysis: 9 pointers + 2 double + 5 u64 + 2 i32 + u64
-    assert C.sizeof(abi.Params) == 18 * 4 + 2 * 8
-    assert C.sizeof(abi.Mv) == 8
-    assert C.sizeof(abi.PAnalysisC) == 9 * 8 + 2 * 8 + 5 * 8 + 2 * 4 + 8
-    assert C.sizeof(abi.Counters) == 7 * 8
-    assert C.sizeof(abi.Timing) == 5 * 8 + 2 * 8
-    assert C.sizeof(api.Pass) == 7 * 4
+# ctypes mirror -> C struct name in include/vc1cu.h
+STRUCTS = {"Params": (abi.Params, "vc1cu_params"), "Mv": (abi.Mv, "vc1cu_mv"),
+           "PAnalysisC": (abi.PAnalysisC, "vc1cu_panalysis"), "Counters": (abi.Counters, "vc1cu_counters"),
+           "Timing": (abi.Timing, "vc1cu_timing"), "Pass": (api.Pass, "vc1cu_pass"),
+           "BAnalysisC": (abi.BAnalysisC, "vc1cu_banalysis"), "BPass": (abi.BPass, "vc1cu_bpass")}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Size and every field offset of the ctypes mirrors equal the C compiler's for the header."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+
+        pytest.skip("no C compiler")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "vc1cu.h"', "int main(void) {"]
+    for key, (cls, cname) in STRUCTS.items():
+        lines.append(f'printf("{key} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{key} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    want = []
+    for key, (cls, _) in STRUCTS.items():
+        want.append(f"{key} size {C.sizeof(cls)}")
+        want += [f"{key} {f[0]} {getattr(cls, f[0]).offset}" for f in cls._fields_]
+    assert [g for g in got if g] == want
 
 
 def test_params_default_matches_reference_defaults():
