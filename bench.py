@@ -1,18 +1,27 @@
 #!/usr/bin/env python
-"""Encoder-analysis throughput of libvc1's P-picture hot path on B200, in macroblocks/s.
+"""Encoder-analysis throughput of libvc1's analysis hot path on B200, in macroblocks/s.
 
 Workload (the 1080p configuration): 1920x1080 8-bit 4:2:0, 60 seeded synthetic frames
 (value-noise texture, zoom 1.002/frame, 8 objects at up to 8 px/frame, sigma 2), GOP 12
-IBBP, so 15 P pictures per clip, each analysed against the previous anchor (3 frames back)
-with search range +/-64, Mixed-MV, non-uniform quantiser at QP 4/6/8/10/12 (one per GOP).
+IBBP planned the way the reference's encoder plans it (encoder_core.cpp:928-962: segments
+start at each I picture, anchors every 3 frames, the segment's last frame an anchor), so per
+GOP P pictures at 3, 6, 9, 11 and B pictures at 1, 2, 4, 5, 7, 8, 10: 20 P and 35 B
+pictures per clip. Search range +/-64, Mixed-MV, non-uniform quantiser at QP 4/6/8/10/12
+(one per GOP; a B picture takes its GOP's QP).
 
-One step = every P picture of the clip fully analysed: the quarter-pel seed pass, the three
-seeded mode passes (half-pel, half-pel bilinear, Mixed-MV), the final Mixed-MV pass with
-P-intra, the decoder-equivalent prediction, and the forward transform + quantiser of that
-prediction for all four transform sizes (Vc1Encoder::analyze_p_picture_core x5 and
-quantize_inter_part, src/encoder_motion.cpp:47-597, src/encoder_transform.cpp:935-1171).
-The final pass is timed in Mixed-MV mode, the most expensive of the reference's four
-candidates (the reference chooses it on the host by sampled RD).
+One step = every picture of the clip analysed:
+  P pictures: the quarter-pel seed pass, the three seeded mode passes (half-pel, half-pel
+    bilinear, Mixed-MV), the final Mixed-MV pass with P-intra, the decoder-equivalent
+    prediction, and the forward transform + quantiser of that prediction for all four
+    transform sizes (Vc1Encoder::analyze_p_picture_core x5 and quantize_inter_part,
+    src/encoder_motion.cpp:47-597, src/encoder_transform.cpp:935-1171). The final pass is
+    timed in Mixed-MV mode, the most expensive of the reference's four candidates (the
+    reference chooses it on the host by sampled RD).
+  B pictures: analyze_b_picture_mode in quarter-pel and in half-pel bilinear mode (the two
+    modes analyze_b_picture compares, encoder_motion.cpp:1062-1095): per mode the forward
+    and backward core passes and the per-macroblock Direct / Forward / Backward /
+    Interpolated / Intra decision against the future P anchor's final-pass vectors
+    (src/encoder_motion.cpp:753-1005).
 
   value : MB/s with the clip resident in HBM (CUDA events on the library's stream, L2
           flushed between steps)
@@ -23,6 +32,7 @@ candidates (the reference chooses it on the host by sampled RD).
 
 Multi-GPU: one process per GPU (torchrun); each rank analyses its own clip (seeded by
 rank), no collective on the data path; value = all ranks' MBs / max rank time.
+Profiling: --gops N analyses only the pictures of the first N GOPs.
 """
 from __future__ import annotations
 
@@ -47,20 +57,36 @@ METRIC = "1080p ME+qpel+xform MB/s on 1 B200: plain (bit-exact) vs learned @<=1%
 UNIT = "MB/s"
 
 # Algorithmic integer ops per macroblock of each core pass on this workload, from the
-# instrumented oracle (oracle/count_ops.py over two P pictures of the clip; weights there).
-OPS_PER_MB = {"unseeded": 286531.9, "seeded_hpel": 56280.0, "seeded_bilinear": 25312.1, "seeded_mixed": 474288.5,
-              "final_mixed_intra": 474771.4}
+# instrumented oracle (oracle/count_ops.py over pictures of the clip's first GOP; weights there).
+OPS_PER_MB = {"unseeded": 286137.3, "seeded_hpel": 56261.4, "seeded_bilinear": 25321.8, "seeded_mixed": 471920.4,
+              "final_mixed_intra": 472178.7, "b_qpel_forward": 286981.1, "b_qpel_backward": 289317.5,
+              "b_bilinear_forward": 121400.1, "b_bilinear_backward": 122512.3}
+WORKLOAD = ("1080p IBBP analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP as the reference plans it -> 20 P + 35 B "
+            "pictures/step; P: 5 core passes + prediction + 4-size transform/quant; B: forward+backward core passes and "
+            "the MB decision in qpel and hpel-bilinear mode; search +/-64, Mixed-MV, nonuniform QP 4-12")
+P_PASSES = ("unseeded", "seeded_hpel", "seeded_bilinear", "seeded_mixed", "final_mixed_intra")
+B_PASSES = ("b_qpel_forward", "b_qpel_backward", "b_bilinear_forward", "b_bilinear_backward")
 XFORM_FLOPS_PER_MB = 51911.5
 
 
-def anchors_and_pictures():
-    """(P frame, reference anchor, PQINDEX) of GOP 12 IBBP over FRAMES frames."""
-    pics = []
-    for t in range(0, FRAMES, BFRAMES + 1):
-        if t % GOP == 0:
-            continue  # I picture
-        pics.append((t, t - (BFRAMES + 1), 4 + 2 * ((t // GOP) % 5)))
-    return pics
+def gop_plan(gops=None):
+    """P pictures [(frame, past anchor, PQINDEX)] and B pictures [(frame, past, future,
+    fraction_num, fraction_den, PQINDEX, index of the future anchor in the P list)] of GOP 12
+    IBBP over FRAMES frames, planned like the reference's encoder (encoder_core.cpp:928-962)."""
+    ps, bs = [], []
+    for seg in range(0, FRAMES, GOP):
+        if gops is not None and seg // GOP >= gops:
+            break
+        end = min(seg + GOP, FRAMES)
+        pq = 4 + 2 * ((seg // GOP) % 5)
+        prev = seg
+        while prev + 1 < end:
+            nxt = min(prev + BFRAMES + 1, end - 1)
+            ps.append((nxt, prev, pq))
+            for j in range(prev + 1, nxt):
+                bs.append((j, prev, nxt, j - prev, nxt - prev, pq, len(ps) - 1))
+            prev = nxt
+    return ps, bs
 
 
 def make_clip(rank: int):
@@ -110,15 +136,15 @@ def parse_clocks(path: str, device: int):
 class Runner:
     """Drives one step of the analysis path through the C ABI."""
 
-    def __init__(self, ctx, clip, pictures=None):
+    def __init__(self, ctx, clip, gops=None):
         from libvc1_b200.abi import MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED, MV_QPEL
 
         self.ctx, self.clip = ctx, clip
-        self.pics = anchors_and_pictures()[:pictures]
-        self.frames = sorted({f for p in self.pics for f in p[:2]})
+        self.pics, self.bpics = gop_plan(gops)
+        self.frames = sorted({f for p in self.pics for f in p[:2]} | {f for b in self.bpics for f in b[:3]})
         self.p0 = params(8)
         self.modes = (MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED)
-        self.QPEL, self.MIXED = MV_QPEL, MV_MIXED
+        self.QPEL, self.MIXED, self.BIL = MV_QPEL, MV_MIXED, MV_HPEL_BILINEAR
         import torch
 
         self.torch = torch
@@ -139,8 +165,13 @@ class Runner:
         """Enqueues one step on the library's stream; levels go to `levels` (default self.levels)."""
         levels = self.levels if levels is None else levels
         c, pics = self.ctx, self.pics
-        # every picture's quarter-pel seed pass (full search window per warp)
-        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)])
+        # every P picture's quarter-pel seed pass and the four unseeded core passes of every B
+        # picture (forward / backward in quarter-pel and in half-pel bilinear mode); the library
+        # runs one launch per pass kind
+        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)] +
+                      [(t, ref, m, 0, -1, 3100 + 4 * k + 2 * (m == self.BIL) + (ref == fut), pq)
+                       for k, (t, past, fut, _n, _d, pq, _a) in enumerate(self.bpics)
+                       for m in (self.QPEL, self.BIL) for ref in (past, fut)])
         # the three seeded mode passes of every picture (the library runs one launch per mode)
         c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
                                 for m in self.modes])
@@ -151,14 +182,25 @@ class Runner:
             p = params(pq)
             c.motion_compensate(p, r, 3000 + i, self.MIXED, 3500 + i)
             c.forward_quant_device(p, t, 3500 + i, 15, 0, levels[i].data_ptr())
+        # the B decisions of both modes against the future anchor's final pass
+        if self.bpics:
+            c.b_decide(self.p0, [(t, past, fut, 3100 + 4 * k + 2 * j, 3101 + 4 * k + 2 * j, 3000 + a, num, den, m,
+                                  2 * k + j, pq)
+                                 for k, (t, past, fut, num, den, pq, a) in enumerate(self.bpics)
+                                 for j, m in enumerate((self.QPEL, self.BIL))])
 
     def read_results(self):
-        """D2H of the final-pass analysis of every picture (waits for the step)."""
-        return [self.ctx.read_result(self.p0, 3000 + i) for i in range(len(self.pics))]
+        """D2H of every P picture's final-pass analysis and every B analysis (waits for the step)."""
+        return ([self.ctx.read_result(self.p0, 3000 + i) for i in range(len(self.pics))] +
+                [self.ctx.read_bresult(self.p0, j) for j in range(2 * len(self.bpics))])
+
+    def mbs_per_step(self):
+        return (len(self.pics) + len(self.bpics)) * MBS
 
     def result_bytes(self):
         per_mb = 8 + 32 + 1 + 1 + 8 + 8 + 8 + 8 + 1
-        return len(self.pics) * (MBS * per_mb) + self.levels.numel() * 2
+        per_b_mb = 1 + 8 + 8 + 8 + 2 * (8 + 8 + 1)
+        return len(self.pics) * (MBS * per_mb) + 2 * len(self.bpics) * MBS * per_b_mb + self.levels.numel() * 2
 
 
 def flush_l2(torch, buf):
@@ -177,7 +219,7 @@ def run_ours(args, rank, world, device):
     if ctx is None:
         raise RuntimeError(f"CUDA backend unavailable: {err}")
     clip = make_clip(rank)
-    run = Runner(ctx, clip, args.pictures)
+    run = Runner(ctx, clip, args.gops)
     run.upload_all()
     ext = torch.cuda.ExternalStream(ctx.stream_handle(), device=device)
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -211,7 +253,7 @@ def run_ours(args, rank, world, device):
     counters = ctx.counters()
     ctx.set_timing(False)
     total_ms = float(sum(step_ms))
-    mbs_per_step = len(run.pics) * MBS
+    mbs_per_step = run.mbs_per_step()
     max_ms = 1e3 * slowest(total_ms * 1e-3, world, "cuda")
     value = whole_job_rate(mbs_per_step * args.steps, max_ms * 1e-3, world)
     clocks = parse_clocks(clock_log, device)
@@ -262,8 +304,7 @@ def run_ours(args, rank, world, device):
     e2e_value = world * mbs_per_step * args.steps / e2e_worst if e2e_s else None
     # ---- roofline of the dominant kernel (core_pass_kernel), INT32-bound
     n = len(run.pics)
-    ops_step = n * MBS * (OPS_PER_MB["unseeded"] + OPS_PER_MB["seeded_hpel"] + OPS_PER_MB["seeded_bilinear"] +
-                          OPS_PER_MB["seeded_mixed"] + OPS_PER_MB["final_mixed_intra"])
+    ops_step = n * MBS * sum(OPS_PER_MB[k] for k in P_PASSES) + len(run.bpics) * MBS * sum(OPS_PER_MB[k] for k in B_PASSES)
     core_launches = max(1, timing["core_launches"])
     core_ms = timing["core_ms"]
     achieved_ops = ops_step * args.steps / (core_ms * 1e-3) if core_ms > 0 else 0.0
@@ -278,9 +319,9 @@ def run_ours(args, rank, world, device):
             "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32 (integer SAD/SATD/interpolation) + f64 transform",
             "data": "synthetic (seeded value-noise clip with the 1080p config's motion, zoom, objects and noise)",
-            "config": {"workload": "1080p P-picture analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP -> 15 P "
-                                   "pictures/step, search +/-64, Mixed-MV, nonuniform QP 4-12, 4 transform sizes",
-                       "mb_per_step_per_gpu": mbs_per_step, "passes_per_picture": 5,
+            "config": {"workload": WORKLOAD,
+                       "mb_per_step_per_gpu": mbs_per_step, "p_pictures": len(run.pics), "b_pictures": len(run.bpics),
+                       "core_passes_per_step": 5 * len(run.pics) + 4 * len(run.bpics),
                        "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
                     "h2d_bytes_per_step": len(run.frames) * run.frame_bytes,
@@ -290,10 +331,11 @@ def run_ours(args, rank, world, device):
                          "peak": round(peak_ops / 1e9, 1), "unit": "Gop/s (int32 lane ops)",
                          "frac": round(achieved_ops / peak_ops, 4) if peak_ops else None,
                          "peak_source": "measured live: vc1cu_measure_int32_peak add/xor kernel",
-                         "ops_per_mb": round(sum(OPS_PER_MB.values()), 1),
+                         "ops_per_p_mb": round(sum(OPS_PER_MB[k] for k in P_PASSES), 1),
+                         "ops_per_b_mb": round(sum(OPS_PER_MB[k] for k in B_PASSES), 1),
                          "core_ms_per_launch": round(core_ms / core_launches, 3), "traffic": None},
             "kernel_ms_per_step": {k: round(timing[k] / args.steps, 3)
-                                   for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms")},
+                                   for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms")},
             "xform_roofline": {"bound": "fp64", "achieved_gflops": round(xform_flops / (xform_ms * 1e-3) / 1e9, 1)
                                if xform_ms > 0 else None},
             "clocks": clocks,
@@ -304,33 +346,46 @@ def run_ours(args, rank, world, device):
     return out
 
 
-def reference_jobs(clip, pics):
-    """One (Reference, cur, ref) job per P picture, each encoder at the picture's PQINDEX."""
+def reference_jobs(clip):
+    """The reference's jobs of one step: P jobs (Reference at the picture's PQINDEX, cur, ref)
+    and B jobs (Reference, cur, past, future, future anchor's P index, num, den)."""
     from oracle import Reference
 
-    refs = {pq: Reference(params(pq), simd_auto=True) for pq in sorted({p[2] for p in pics})}
+    ps, bs = gop_plan()
+    refs = {pq: Reference(params(pq), simd_auto=True) for pq in sorted({p[2] for p in ps} | {b[5] for b in bs})}
     any_ref = next(iter(refs.values()))
-    jobs = [(refs[pq], any_ref.frame(clip.frame(t)), any_ref.frame(clip.frame(r))) for t, r, pq in pics]
-    return any_ref, jobs
+    frames = {}
+
+    def fr(t):
+        if t not in frames:
+            frames[t] = any_ref.frame(clip.frame(t))
+        return frames[t]
+
+    pjobs = [(refs[pq], fr(t), fr(r)) for t, r, pq in ps]
+    bjobs = [(refs[pq], fr(t), fr(past), fr(fut), a, num, den) for t, past, fut, num, den, pq, a in bs]
+    return any_ref, pjobs, bjobs
+
+
+REF_SAMPLE = ("every picture of the clip once (one step): the 20 P pictures (analyze_p_picture + choose_transform_mb of "
+              "the chosen prediction), then the 35 B pictures (analyze_b_picture against the P analyses), one picture "
+              "per thread, SIMD dispatch auto")
 
 
 def cpu_baseline(args, clip):
     """The reference's own CPU path (oracle/_ref, SIMD dispatch on) over a bounded sample of
-    the same workload: every P picture of the clip once, one picture per host thread."""
+    the same workload: every picture of the clip once, one picture per host thread."""
     try:
         from oracle import ref_available
     except Exception as e:  # pragma: no cover
         return {"unavailable": f"oracle import failed: {e}"}
     if not ref_available():
         return {"unavailable": "oracle/_ref/libvc1ref.so not built"}
-    pics = anchors_and_pictures()
     cores = os.cpu_count() or 1
-    anyref, jobs = reference_jobs(clip, pics)
-    threads = min(len(jobs), cores)
-    ns = anyref.bench_analysis_multi(jobs, threads)
-    return {"value": round(len(jobs) * MBS / (ns * 1e-9), 1), "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{len(jobs)} P pictures of the 1080p clip (one step), one per thread: analyze_p_picture + "
-                      f"choose_transform_mb of the chosen prediction, SIMD dispatch auto"}
+    anyref, pjobs, bjobs = reference_jobs(clip)
+    threads = min(len(pjobs) + len(bjobs), cores)
+    ns = anyref.bench_gop_multi(pjobs, bjobs, threads)
+    return {"value": round((len(pjobs) + len(bjobs)) * MBS / (ns * 1e-9), 1), "unit": UNIT, "cores": threads,
+            "kind": "reference", "sample": REF_SAMPLE}
 
 
 def run_reference(args, rank, world):
@@ -343,25 +398,22 @@ def run_reference(args, rank, world):
     if not ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libvc1ref.so was not built (reference tree absent)"}
     clip = make_clip(0)
-    pics = anchors_and_pictures()
     cores = os.cpu_count() or 1
-    anyref, jobs = reference_jobs(clip, pics)
-    threads = min(len(jobs), cores)
+    anyref, pjobs, bjobs = reference_jobs(clip)
+    threads = min(len(pjobs) + len(bjobs), cores)
     per = []
     for i in range(args.warmup + args.steps):
-        ns = anyref.bench_analysis_multi(jobs, threads)
+        ns = anyref.bench_gop_multi(pjobs, bjobs, threads)
         if i >= args.warmup:
             per.append(ns * 1e-9)
-    value = len(jobs) * MBS * len(per) / sum(per)
+    value = (len(pjobs) + len(bjobs)) * MBS * len(per) / sum(per)
     return {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(per) / len(per), 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 + f64 (CPU)",
             "data": "synthetic (same seeded clip as ours)",
-            "config": {"workload": "1080p P-picture analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP -> 15 P "
-                                   "pictures/step, search +/-64, Mixed-MV, nonuniform QP 4-12, 4 transform sizes"},
+            "config": {"workload": WORKLOAD},
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": "every P picture of the clip per step, one per thread: analyze_p_picture + "
-                                       "choose_transform_mb, SIMD dispatch auto"},
+                             "sample": REF_SAMPLE},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -373,7 +425,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--pictures", type=int, default=None, help="analyse only the first N P pictures (profiling)")
+    ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -237,6 +237,10 @@ class Reference:
         L.ref_bench_analysis.restype = u64
         L.ref_bench_analysis_multi.argtypes = [C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis_multi.restype = u64
+        L.ref_bench_gop_multi.argtypes = [C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), i32, C.POINTER(vp),
+                                          C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(i32), C.POINTER(i32),
+                                          C.POINTER(i32), i32, i32]
+        L.ref_bench_gop_multi.restype = u64
         self.p = p
         self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
 
@@ -341,6 +345,17 @@ class Reference:
 
     def quantize_level(self, c):
         return self.lib.ref_scalar_quantize_level(self.h, c)
+
+    def bench_gop_multi(self, pjobs, bjobs, threads):
+        """Wall ns of every P job (Reference, cur, ref) and then every B job (Reference, cur, past,
+        future, index of its future anchor in pjobs, fraction_num, fraction_den)."""
+        vpa = lambda xs: (vp * max(1, len(xs)))(*xs)  # noqa: E731
+        ia = lambda xs: (i32 * max(1, len(xs)))(*xs)  # noqa: E731
+        return self.lib.ref_bench_gop_multi(vpa([j[0].h for j in pjobs]), vpa([j[1].h for j in pjobs]),
+                                            vpa([j[2].h for j in pjobs]), len(pjobs), vpa([j[0].h for j in bjobs]),
+                                            vpa([j[1].h for j in bjobs]), vpa([j[2].h for j in bjobs]),
+                                            vpa([j[3].h for j in bjobs]), ia([j[4] for j in bjobs]),
+                                            ia([j[5] for j in bjobs]), ia([j[6] for j in bjobs]), len(bjobs), threads)
 
     def bench_analysis_multi(self, jobs, threads):
         """Wall ns over (Reference, cur RefFrame, ref RefFrame) jobs, each with its own config."""

@@ -379,6 +379,69 @@ uint64_t ref_bench_analysis_multi(void** handles, void** curs, void** refs, int 
     return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
 }
 
+// CPU baseline of one GOP-planned step: first every P picture (analyze_p_picture +
+// choose_transform_mb of its chosen prediction), then every B picture (analyze_b_picture
+// against its two anchors, with the future anchor's MVs, Mixed-MV flags and intensity
+// compensation from that P picture's analysis, as encoder_core.cpp:1086-1097 passes them),
+// each phase one picture per worker thread at a time. Returns wall ns.
+uint64_t ref_bench_gop_multi(void** p_handles, void** p_curs, void** p_refs, int n_p, void** b_handles, void** b_curs,
+                             void** b_pasts, void** b_futures, const int* b_anchor, const int* b_num, const int* b_den,
+                             int n_b, int threads) {
+    std::vector<Vc1Encoder::PAnalysis> anchors(static_cast<size_t>(std::max(0, n_p)));
+    std::atomic<int> next{0};
+    auto p_worker = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n_p) break;
+            const auto& c = static_cast<RefEncoder*>(p_handles[i])->cfg;
+            const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+            Vc1Encoder enc(c);
+            Frame pred;
+            pred.width = c.width;
+            pred.height = c.height;
+            pred.y.assign(static_cast<size_t>(c.width) * c.height, 0);
+            pred.u.assign(static_cast<size_t>(c.width / 2) * (c.height / 2), 128);
+            pred.v = pred.u;
+            const Frame& cur = F(p_curs[i]);
+            const Frame& ref = F(p_refs[i]);
+            anchors[i] = enc.analyze_p_picture(cur, ref);
+            const auto& a = anchors[i];
+            for (int my = 0; my < mbh; ++my)
+                for (int mx = 0; mx < mbw; ++mx) {
+                    const size_t pos = static_cast<size_t>(my) * mbw + mx;
+                    if (a.use_4mv[pos]) enc.motion_compensate_4mv(pred, ref, mx, my, a.block_mvs[pos]);
+                    else enc.motion_compensate_mb(pred, ref, mx, my, a.mvs[pos], a.mv_mode);
+                    (void)enc.choose_transform_mb(cur, pred, mx, my, 0, true, c.pqindex, false);
+                }
+        }
+    };
+    std::atomic<int> bnext{0};
+    auto b_worker = [&]() {
+        for (;;) {
+            const int i = bnext.fetch_add(1);
+            if (i >= n_b) break;
+            const auto& c = static_cast<RefEncoder*>(b_handles[i])->cfg;
+            Vc1Encoder enc(c);
+            const auto& a = anchors[static_cast<size_t>(b_anchor[i])];
+            (void)enc.analyze_b_picture(F(b_curs[i]), F(b_pasts[i]), F(b_futures[i]), a.mvs, a.use_4mv, a.intensity,
+                                        b_num[i], b_den[i]);
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(p_worker);
+        for (auto& t : pool) t.join();
+    }
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(b_worker);
+        for (auto& t : pool) t.join();
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+}
+
 // CPU baseline: analyze_p_picture + choose_transform_mb of the chosen prediction for every
 // MB of every (cur, ref) pair, one pair per worker thread at a time. Returns wall ns.
 uint64_t ref_bench_analysis(void* h, void** curs, void** refs, int n_pairs, int threads) {
