@@ -11,6 +11,7 @@
 #include <cstddef>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -316,7 +317,12 @@ const uint32_t* work_items(vc1cu_ctx* c, int mbw, int mbh, const std::vector<int
         }
     void* d = nullptr;
     ck(cudaMalloc(&d, items.size() * sizeof(uint32_t)), "cudaMalloc(work items)");
-    ck(cudaMemcpy(d, items.data(), items.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "cudaMemcpy(work items)");
+    // Ordered on the context stream, which does not synchronise with the legacy default stream:
+    // a plain cudaMemcpy from pageable memory may return before its DMA lands, and the kernel
+    // that reads the table could then start first.
+    ck(cudaMemcpyAsync(d, items.data(), items.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream),
+       "cudaMemcpyAsync(work items)");
+    ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize(work items)");  // `items` is freed on return
     nitems = (unsigned)items.size();
     c->items[key] = {static_cast<uint32_t*>(d), nitems};
     return static_cast<uint32_t*>(d);
@@ -754,7 +760,18 @@ int check_status(vc1cu_ctx* c) {
     if (st.error) {
         ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
         sync_checked(c);
-        throw Fail{st.error, "a wavefront wait timed out on the device (" + std::to_string(st.timeouts) + " waits)"};
+        std::string where;
+        if (st.tcode) {
+            const unsigned code = st.tcode - 1u;
+            where = "; first: pass " + std::to_string(code >> 20) + " of its launch, macroblock " +
+                    std::to_string(code & 0xFFFFFu) + ", lanes still waiting 0x" + [&] {
+                        char b[16];
+                        std::snprintf(b, sizeof b, "%x", st.tmask);
+                        return std::string(b);
+                    }();
+        }
+        throw Fail{st.error, "a wavefront wait timed out on the device (" + std::to_string(st.timeouts) + " waits" +
+                                 where + ")"};
     }
     return VC1CU_OK;
 }
@@ -999,7 +1016,8 @@ int vc1cu_open(int device, vc1cu_ctx** out) {
         void* d = nullptr;
         ck(cudaMalloc(&d, sizeof(LaunchStatus)), "cudaMalloc(status)");
         c->d_status = static_cast<LaunchStatus*>(d);
-        ck(cudaMemset(c->d_status, 0, sizeof(LaunchStatus)), "cudaMemset(status)");
+        ck(cudaMemsetAsync(c->d_status, 0, sizeof(LaunchStatus), c->stream), "cudaMemsetAsync(status)");
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     } catch (const Fail& f) {
         const int code = f.code;
         t_open_error = f.msg;

@@ -1940,7 +1940,9 @@ __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gp
 // loads, all lanes at once, and one acquire fence follows the last poll, so a poll costs
 // no L1 invalidation. Every lane calls it. On timeout it raises the launch's error and
 // abort flags and returns false.
-__device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* st) {
+// code: the waiting work item, recorded (with the lanes still waiting) by the first wait
+// that gives up.
+__device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* st, uint32_t code) {
     bool mine = flag == nullptr;
     for (long it = 0; it < (1L << 24); ++it) {
         if (!mine) mine = ld_relaxed(flag) == epoch;
@@ -1956,7 +1958,9 @@ __device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* s
         }
         __nanosleep(64);
     }
+    const unsigned waiting = __ballot_sync(FULL, !mine);
     if ((threadIdx.x & 31) == 0) {
+        if (atomicCAS(&st->tcode, 0u, code + 1u) == 0u) st->tmask = waiting;
         atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
         atomicExch(&st->abort, 1);
         atomicAdd(&st->timeouts, 1u);
@@ -1967,13 +1971,13 @@ __device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* s
 // Waits for the left, top-left, top and top-right macroblocks of the same pass (lanes 0..3;
 // positions outside the raster need no wait).
 __device__ bool wait_neighbours(const DevParams& P, const DevResult& o, int mx, int my, int lane, uint32_t epoch,
-                                LaunchStatus* st) {
+                                LaunchStatus* st, uint32_t code) {
     const uint32_t* f = nullptr;
     if (lane < 4) {
         const int x = mx + (lane == 3 ? 1 : (lane == 2 ? 0 : -1)), y = my - (lane == 0 ? 0 : 1);
         if (x >= 0 && y >= 0 && x < P.mbw) f = &o.done[y * P.mbw + x];
     }
-    return wait_flags(f, epoch, st);
+    return wait_flags(f, epoch, st, code);
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
@@ -2157,7 +2161,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         bool ok = !*(volatile int*)&st->abort;
         // a seed produced by another pass of this launch
         if (ok && d.seed_pass >= 0)
-            ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st);
+            ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st, code);
         PHASE_MARK(0);
         if (ok) load_cur(P, m, d.cur);
         PHASE_MARK(1);
@@ -2257,7 +2261,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
             PHASE_MARK(4);
         }
         // ---- wavefront: left, top-left, top, top-right of the same pass ----
-        if (ok) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st);
+        if (ok) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st, code);
         __syncwarp();
         PHASE_MARK(5);
         if (ok) {

@@ -85,6 +85,8 @@ struct LaunchStatus {
     int abort;
     unsigned int queue;
     unsigned int timeouts;
+    unsigned int tcode;  // 1 + the work item of the first wait that gave up (0: none)
+    unsigned int tmask;  // its lanes still waiting (lanes 0-3: left, top-left, top, top-right; lane 0: seed)
 };
 
 // One B-result slot (Vc1Encoder::BAnalysis) in HBM, structure of arrays over macroblocks.
