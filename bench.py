@@ -64,6 +64,10 @@ OPS_PER_MB = {"unseeded": 286137.3, "seeded_hpel": 56261.4, "seeded_bilinear": 2
 WORKLOAD = ("1080p IBBP analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP as the reference plans it -> 20 P + 35 B "
             "pictures/step; P: 5 core passes + prediction + 4-size transform/quant; B: forward+backward core passes and "
             "the MB decision in qpel and hpel-bilinear mode; search +/-64, Mixed-MV, nonuniform QP 4-12")
+# DRAM bytes (read + write) of core_pass_kernel per launch on this workload: an ncu capture of the
+# first GOP's six core launches (121.6 MB; profiles/core_pass_kernel_1080p_first_gop.md) scaled by
+# macroblocks to the five GOPs of a step and divided over the step's six launches.
+CORE_DRAM_BYTES_PER_LAUNCH = 121.6e6 * 5 / 6
 P_PASSES = ("unseeded", "seeded_hpel", "seeded_bilinear", "seeded_mixed", "final_mixed_intra")
 B_PASSES = ("b_qpel_forward", "b_qpel_backward", "b_bilinear_forward", "b_bilinear_backward")
 XFORM_FLOPS_PER_MB = 51911.5
@@ -333,7 +337,9 @@ def run_ours(args, rank, world, device):
                          "peak_source": "measured live: vc1cu_measure_int32_peak add/xor kernel",
                          "ops_per_p_mb": round(sum(OPS_PER_MB[k] for k in P_PASSES), 1),
                          "ops_per_b_mb": round(sum(OPS_PER_MB[k] for k in B_PASSES), 1),
-                         "core_ms_per_launch": round(core_ms / core_launches, 3), "traffic": None},
+                         "core_ms_per_launch": round(core_ms / core_launches, 3),
+                         "traffic": round(CORE_DRAM_BYTES_PER_LAUNCH) if args.gops is None else None,
+                         "traffic_unit": "DRAM bytes per launch (ncu, first GOP scaled by macroblocks)"},
             "kernel_ms_per_step": {k: round(timing[k] / args.steps, 3)
                                    for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms")},
             "xform_roofline": {"bound": "fp64", "achieved_gflops": round(xform_flops / (xform_ms * 1e-3) / 1e9, 1)
