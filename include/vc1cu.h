@@ -152,6 +152,7 @@ typedef struct vc1cu_timing {
     uint64_t core_launches;
     uint64_t xform_launches;
     double b_ms;         /* B-picture decision (b_cost_kernel + b_decide_kernel) */
+    double ic_ms;        /* intensity-compensation estimate */
 } vc1cu_timing;
 
 /* ---- context (VulkanComputeContext::create / device_name / device_index) ---------- */
@@ -337,6 +338,43 @@ typedef struct vc1cu_bpass {
 int vc1cu_b_decide(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_bpass* passes, int n);
 /* Copies a B-result slot to host arrays (and the scalar totals). Synchronous. */
 int vc1cu_read_bresult(vc1cu_ctx* ctx, int bslot, vc1cu_banalysis* out);
+
+/* ---- intensity compensation (fades) ---------------------------------------------- */
+
+/* Vc1Encoder::IntensityComp (src/encoder_internal.h:341-345): LUMSCALE / LUMSHIFT codes 0..63. */
+typedef struct vc1cu_intensity {
+    int32_t enabled;
+    int32_t lumscale;
+    int32_t lumshift;
+} vc1cu_intensity;
+
+/*
+ * Replaces Vc1Encoder::estimate_intensity_comp (src/encoder_motion_compensation.cpp:296-348),
+ * which analyze_p_picture runs on its chosen pass when fade compensation is on
+ * (encoder_motion.cpp:570-573): the LUMSCALE/LUMSHIFT that map ref_id onto cur_id along the
+ * 1-MV field mvs (HOST array of mbw*mbh vectors). The device samples one pixel per 4x4 luma
+ * cell along the field and scores every (LUMSCALE, shift) pair; the least-squares fit and the
+ * choice in its 7x7 neighbourhood follow the reference's long double arithmetic on the host.
+ * When no fade is found out is {0, 32, 0}, the reference's IntensityComp{}. Synchronous.
+ */
+int vc1cu_estimate_intensity_comp(vc1cu_ctx* ctx, const vc1cu_params* p, int cur_id, int ref_id,
+                                  const vc1cu_mv* mvs, vc1cu_intensity* out);
+
+/* Batch form: picture i takes its field from the mvs of result slot passes[i].mv_slot; the
+ * device work of all n pictures runs in one set of launches. out has n entries. Synchronous. */
+typedef struct vc1cu_icpass {
+    int32_t cur_id;
+    int32_t ref_id;
+    int32_t mv_slot;
+} vc1cu_icpass;
+
+int vc1cu_estimate_intensity_batch(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
+                                   vc1cu_intensity* out);
+
+/* Replaces Vc1Encoder::intensity_compensated_reference (encoder_motion_compensation.cpp:195-294):
+ * frame slot out_id becomes ref_id with the luma and chroma maps of ic (intensity_map_y /
+ * intensity_map_uv, :175-193), or a copy of it when ic->enabled is 0. Asynchronous. */
+int vc1cu_intensity_compensate(vc1cu_ctx* ctx, int ref_id, const vc1cu_intensity* ic, int out_id);
 
 /* ---- motion compensation + forward transform + quantisation ------------------------ */
 

@@ -62,7 +62,7 @@ class Counters(C.Structure):
 class Timing(C.Structure):
     _fields_ = [("core_ms", C.c_double), ("global_ms", C.c_double), ("totals_ms", C.c_double),
                 ("mc_ms", C.c_double), ("xform_ms", C.c_double), ("core_launches", C.c_uint64),
-                ("xform_launches", C.c_uint64), ("b_ms", C.c_double)]
+                ("xform_launches", C.c_uint64), ("b_ms", C.c_double), ("ic_ms", C.c_double)]
 
 
 def make_params(width: int, height: int, **kw) -> Params:
@@ -231,3 +231,15 @@ class BAnalysis:
             elif v != w:
                 bad.append(k)
         return bad
+
+
+class Intensity(C.Structure):
+    """vc1cu_intensity: Vc1Encoder::IntensityComp (enabled, LUMSCALE, LUMSHIFT codes)."""
+    _fields_ = [("enabled", C.c_int32), ("lumscale", C.c_int32), ("lumshift", C.c_int32)]
+
+    def as_tuple(self):
+        return (int(self.enabled), int(self.lumscale), int(self.lumshift))
+
+
+class IcPass(C.Structure):
+    _fields_ = [("cur_id", C.c_int32), ("ref_id", C.c_int32), ("mv_slot", C.c_int32)]

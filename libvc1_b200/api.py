@@ -19,8 +19,8 @@ import os
 
 import numpy as np
 
-from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, Timing, MV_QPEL, METRIC_SAD, METRIC_SATD,
-                  Mv, PAnalysisC, Params, mbs_of)
+from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, IcPass, Intensity, Timing, MV_QPEL,
+                  METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params, mbs_of)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
@@ -34,7 +34,8 @@ EXPORTS = (
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
-    "vc1cu_read_bresult",
+    "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
+    "vc1cu_intensity_compensate",
 )
 
 
@@ -83,6 +84,9 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
+    L.vc1cu_estimate_intensity_comp.argtypes = [vp, PP, i32, i32, vp, C.POINTER(Intensity)]
+    L.vc1cu_estimate_intensity_batch.argtypes = [vp, PP, C.POINTER(IcPass), i32, C.POINTER(Intensity)]
+    L.vc1cu_intensity_compensate.argtypes = [vp, i32, C.POINTER(Intensity), i32]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
     _LIB = L
@@ -245,6 +249,30 @@ class CudaComputeContext:
 
     def synchronize(self):
         self._check(self._L.vc1cu_synchronize(self._h))
+
+    def estimate_intensity_comp(self, params: Params, cur_id: int, ref_id: int, mvs) -> tuple:
+        """Vc1Encoder::estimate_intensity_comp (src/encoder_motion_compensation.cpp:296-348) along a
+        host 1-MV field: (enabled, LUMSCALE, LUMSHIFT)."""
+        mbw, mbh = mbs_of(params)
+        m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)
+        if len(m) != mbw * mbh:
+            raise ValueError("MV field has the wrong macroblock count")
+        out = Intensity()
+        self._check(self._L.vc1cu_estimate_intensity_comp(self._h, C.byref(params), cur_id, ref_id, m.ctypes.data,
+                                                          C.byref(out)))
+        return out.as_tuple()
+
+    def estimate_intensity_batch(self, params: Params, passes) -> list:
+        """passes: iterable of (cur_id, ref_id, mv_slot); one estimate per picture."""
+        arr = (IcPass * max(1, len(passes)))(*[IcPass(*q) for q in passes])
+        out = (Intensity * max(1, len(passes)))()
+        self._check(self._L.vc1cu_estimate_intensity_batch(self._h, C.byref(params), arr, len(passes), out))
+        return [out[i].as_tuple() for i in range(len(passes))]
+
+    def intensity_compensate(self, ref_id: int, ic, out_id: int):
+        """Frame slot out_id = the intensity-compensated reference of ref_id (intensity_compensated_reference)."""
+        k = Intensity(*ic)
+        self._check(self._L.vc1cu_intensity_compensate(self._h, ref_id, C.byref(k), out_id))
 
     def analyze_b_picture(self, params: Params, cur_id: int, past_id: int, future_id: int, anchor_mvs, anchor_4mv,
                           fraction_num: int, fraction_den: int, mode: int = MV_QPEL) -> BAnalysis:

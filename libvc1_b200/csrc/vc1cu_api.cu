@@ -45,6 +45,16 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
+struct IcDesc;
+size_t ic_scratch_bytes();
+size_t ic_table_offset();
+size_t ic_sums_offset();
+size_t ic_hist_bytes();
+size_t ic_desc_bytes();
+void ic_fill_desc(void* desc, const DevFrame& cur, const DevFrame& ref, const int2* mvs, void* scratch);
+cudaError_t launch_ic_estimate(const IcDesc* d_descs, int n, int W, int H, cudaStream_t s);
+cudaError_t launch_ic_map(const DevFrame& ref, uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H,
+                          int enabled, int scale, int shift, int cscale, cudaStream_t s);
 }  // namespace vc1cu
 
 using namespace vc1cu;
@@ -57,7 +67,8 @@ constexpr int kInternalSeed = kMaxSlot + 2;  // its seed
 constexpr int kInternalFwd = kMaxSlot + 3;   // the forward / backward core passes and the anchor
 constexpr int kInternalBwd = kMaxSlot + 4;   // of vc1cu_analyze_b_picture
 constexpr int kInternalAnchor = kMaxSlot + 5;
-constexpr int kInternalLast = kInternalAnchor;
+constexpr int kInternalIc = kMaxSlot + 6;     // MV field of vc1cu_estimate_intensity_comp
+constexpr int kInternalLast = kInternalIc;
 constexpr int kInternalB = kMaxSlot + 1;     // B-result slot of vc1cu_analyze_b_picture
 constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
 #ifndef VC1CU_SEEDED_MIXED_RW
@@ -159,6 +170,10 @@ struct vc1cu_ctx {
     int passes_cap = 0;
     BDesc* d_bdescs = nullptr;
     int bdescs_cap = 0;
+    void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
+    size_t ic_cap = 0;
+    void* d_icdesc = nullptr;
+    size_t icdesc_cap = 0;
     GState* d_gstates = nullptr;
     int gstates_cap = 0;
     void* d_lr = nullptr;      // long-range signature indexes of a launch's reference pictures
@@ -436,7 +451,7 @@ void sync_checked(vc1cu_ctx* c) {
     ck(cudaGetLastError(), "kernel");
 }
 
-enum Family { kCore = 0, kGlobal = 1, kTotals = 2, kMc = 3, kXform = 4, kScore = 5, kB = 6 };
+enum Family { kCore = 0, kGlobal = 1, kTotals = 2, kMc = 3, kXform = 4, kScore = 5, kB = 6, kIc = 7 };
 
 cudaEvent_t take_event(vc1cu_ctx* c) {
     if (!c->event_pool.empty()) {
@@ -484,6 +499,7 @@ void collect_timing(vc1cu_ctx* c) {
             case kMc: c->tsum.mc_ms += ms; break;
             case kXform: c->tsum.xform_ms += ms; c->tsum.xform_launches++; break;
             case kB: c->tsum.b_ms += ms; break;
+            case kIc: c->tsum.ic_ms += ms; break;
             default: break;
         }
         c->event_pool.push_back(t.a);
@@ -915,6 +931,8 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
     }
     if (c->bdescs_cap < n) {
         if (c->d_bdescs) cudaFree(c->d_bdescs);
+    if (c->d_ic) cudaFree(c->d_ic);
+    if (c->d_icdesc) cudaFree(c->d_icdesc);
         c->d_bdescs = nullptr;
         c->bdescs_cap = 0;
         void* d = nullptr;
@@ -930,6 +948,82 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
     ck(launch_bpictures(P, c->d_bdescs, n, c->stream), "B-picture kernel launch");
     tm.stop(2);
     c->counters.macroblocks_analysed += (uint64_t)mbs * (uint64_t)n;
+}
+
+// The host half of Vc1Encoder::estimate_intensity_comp (encoder_motion_compensation.cpp:321-347):
+// the long double least-squares fit from the exact integer sums, then the pair of smallest
+// sample SAD in the fit's 7x7 neighbourhood, read from the device's table of every pair.
+vc1cu_intensity ic_decide(const unsigned long long sums[5], const unsigned long long* table) {
+    vc1cu_intensity out{0, 32, 0};  // IntensityComp{}: off, LUMSCALE 32, LUMSHIFT 0
+    const uint64_t n = sums[0];
+    if (n < 16) return out;
+    const long double sx = (long double)sums[1], sy = (long double)sums[2], sxx = (long double)sums[3],
+                      sxy = (long double)sums[4];
+    const long double denom = static_cast<long double>(n) * sxx - sx * sx;
+    long double a = 1.0L, b = 0.0L;
+    if (std::fabs(denom) > 1e-9L) {
+        a = (static_cast<long double>(n) * sxy - sx * sy) / denom;
+        b = (sy - a * sx) / static_cast<long double>(n);
+    } else {
+        b = (sy - sx) / static_cast<long double>(n);
+    }
+    const int ls = std::clamp(static_cast<int>(std::llround(a * 64.0L - 32.0L)), 1, 63);
+    const int sh = std::clamp(static_cast<int>(std::llround(b)), -32, 31);
+    uint64_t best = std::numeric_limits<uint64_t>::max();
+    int best_ls = 32, best_sh = 0;
+    for (int l = std::max(1, ls - 3); l <= std::min(63, ls + 3); ++l)
+        for (int z = std::max(-32, sh - 3); z <= std::min(31, sh + 3); ++z) {
+            const uint64_t sad = table[(l - 1) * 64 + (z + 32)];
+            if (sad < best || (sad == best && std::abs(l - 32) + std::abs(z) < std::abs(best_ls - 32) + std::abs(best_sh))) {
+                best = sad;
+                best_ls = l;
+                best_sh = z;
+            }
+        }
+    if (best_ls == 32 && best_sh == 0) return out;
+    out.enabled = 1;
+    out.lumscale = best_ls;
+    out.lumshift = best_sh < 0 ? best_sh + 64 : best_sh;
+    return out;
+}
+
+struct IcJob {
+    DevFrame cur, ref;
+    const int2* mvs;
+};
+
+// Device part of the estimate for a batch of pictures (one set of launches), then the host part.
+void ic_estimate(vc1cu_ctx* c, const DevParams& P, const std::vector<IcJob>& jobs, vc1cu_intensity* out) {
+    const int n = (int)jobs.size();
+    if (!n) return;
+    const size_t sb = ic_scratch_bytes(), db = (ic_desc_bytes() + 15) & ~size_t(15);
+    uint8_t* scratch = static_cast<uint8_t*>(ensure(c->d_ic, c->ic_cap, sb * n, "cudaMalloc(intensity scratch)"));
+    void* ddesc = ensure(c->d_icdesc, c->icdesc_cap, db * n, "cudaMalloc(intensity descriptors)");
+    uint8_t* hp = static_cast<uint8_t*>(staging(c, db * n));
+    for (int i = 0; i < n; ++i) ic_fill_desc(hp + db * i, jobs[i].cur, jobs[i].ref, jobs[i].mvs, scratch + sb * i);
+    ck(cudaMemcpyAsync(ddesc, hp, db * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(intensity descriptors)");
+    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    for (int i = 0; i < n; ++i) {
+        ck(cudaMemsetAsync(scratch + sb * i, 0, ic_hist_bytes(), c->stream), "cudaMemsetAsync(histogram)");
+        ck(cudaMemsetAsync(scratch + sb * i + ic_sums_offset(), 0, 5 * sizeof(unsigned long long), c->stream),
+           "cudaMemsetAsync(sums)");
+    }
+    {
+        Timer tm(c, kIc);
+        ck(launch_ic_estimate(static_cast<const IcDesc*>(ddesc), n, P.W, P.H, c->stream), "intensity estimate launch");
+        tm.stop(3);
+    }
+    constexpr size_t kTable = 63 * 64;
+    std::vector<unsigned long long> tables(kTable * n), sums(5 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        ck(cudaMemcpyAsync(tables.data() + kTable * i, scratch + sb * i + ic_table_offset(), kTable * 8,
+                           cudaMemcpyDeviceToHost, c->stream),
+           "cudaMemcpyAsync(intensity table)");
+        ck(cudaMemcpyAsync(sums.data() + 5 * i, scratch + sb * i + ic_sums_offset(), 40, cudaMemcpyDeviceToHost, c->stream),
+           "cudaMemcpyAsync(intensity sums)");
+    }
+    sync_checked(c);
+    for (int i = 0; i < n; ++i) out[i] = ic_decide(sums.data() + 5 * i, tables.data() + kTable * i);
 }
 
 void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
@@ -1297,6 +1391,83 @@ int vc1cu_analyze_b_picture(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int
         launch_b(c, p, &b, 1, kInternalB);
         check_status(c);
         read_bresult(c, c->bresults[kInternalB], out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_estimate_intensity_comp(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int ref_id, const vc1cu_mv* mvs,
+                                  vc1cu_intensity* out) {
+    return guarded(c, [&]() -> int {
+        if (!out || !mvs) throw Fail{VC1CU_ERR_ARG, "null output or MV field"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fr = frame_slot(c, ref_id);
+        if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "intensity estimate frame dimensions do not match the configuration"};
+        ResultSlot& s = result_slot(c, kInternalIc, mbs, true);
+        s.mode = -1;
+        ck(cudaMemcpyAsync(s.r.mvs, mvs, 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload MV field");
+        ic_estimate(c, P, {IcJob{fc.view(), fr.view(), s.r.mvs}}, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_estimate_intensity_batch(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
+                                   vc1cu_intensity* out) {
+    return guarded(c, [&]() -> int {
+        if (n < 0 || (n > 0 && (!passes || !out))) throw Fail{VC1CU_ERR_ARG, "invalid intensity batch"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        check_status(c);
+        std::vector<IcJob> jobs;
+        for (int i = 0; i < n; ++i) {
+            FrameSlot& fc = frame_slot(c, passes[i].cur_id);
+            FrameSlot& fr = frame_slot(c, passes[i].ref_id);
+            if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+                throw Fail{VC1CU_ERR_ARG, "intensity estimate frame dimensions do not match the configuration"};
+            if (passes[i].mv_slot < 0 || passes[i].mv_slot >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+            jobs.push_back(IcJob{fc.view(), fr.view(), result_slot(c, passes[i].mv_slot, mbs, false).r.mvs});
+        }
+        ic_estimate(c, P, jobs, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_intensity_compensate(vc1cu_ctx* c, int ref_id, const vc1cu_intensity* ic, int out_id) {
+    return guarded(c, [&]() -> int {
+        if (!ic) throw Fail{VC1CU_ERR_ARG, "null intensity parameters"};
+        if (ic->lumscale < 0 || ic->lumscale > 63 || ic->lumshift < 0 || ic->lumshift > 63)
+            throw Fail{VC1CU_ERR_ARG, "LUMSCALE and LUMSHIFT are 6-bit codes (0..63)"};
+        if (out_id < 0 || out_id >= kMaxSlot || out_id == ref_id) throw Fail{VC1CU_ERR_ARG, "invalid output frame slot"};
+        FrameSlot& fr = frame_slot(c, ref_id);
+        const int W = fr.w, H = fr.h;
+        const DevFrame ref = fr.view();
+        FrameSlot& fo = alloc_frame(c, out_id, W, H);
+        const DevFrame o = fo.view();
+        // the luma law of intensity_map_y and the chroma scale of intensity_map_uv
+        // (encoder_motion_compensation.cpp:175-193)
+        int scale, shift;
+        if (ic->lumscale == 0) {
+            scale = -64;
+            shift = (255 - ic->lumshift * 2) * 64;
+            if (ic->lumshift > 31) shift += 128 * 64;
+        } else {
+            scale = ic->lumscale + 32;
+            shift = (ic->lumshift > 31 ? ic->lumshift - 64 : ic->lumshift) * 64;
+        }
+        const int cscale = ic->lumscale == 0 ? -64 : ic->lumscale + 32;
+        Timer tm(c, kMc);
+        ck(launch_ic_map(ref, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v, fo.pitch_y, fo.pitch_c, W, H, ic->enabled != 0, scale,
+                         shift, cscale, c->stream),
+           "intensity map launch");
+        tm.stop(1);
         return VC1CU_OK;
     });
 }

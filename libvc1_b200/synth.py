@@ -88,3 +88,15 @@ def long_pan(frames=60, seed=5):
     """1920x1080 camera pans up to 200 px/frame horizontal, 60 px vertical, 4 objects."""
     return generate(1920, 1080, frames, seed, global_px=200.0, global_py=60.0, n_objects=4, obj_vel=8.0,
                     sigma=2.0)
+
+
+def fade(frame, scale: float, offset: float, seed: int, sigma: float = 1.0):
+    """A brightness fade of one picture: luma scale*y + offset plus Gaussian noise (sigma), chroma
+    scaled about 128, rounded and clipped to 8 bits (content for the intensity-compensation
+    estimate; seeded, so repeatable)."""
+    y, u, v = frame
+    rng = np.random.default_rng(seed)
+    yy = np.clip(np.rint(y.astype(np.float64) * scale + offset + rng.normal(0.0, sigma, y.shape)), 0, 255)
+    uu = np.clip(np.rint((u.astype(np.float64) - 128.0) * scale + 128.0), 0, 255)
+    vv = np.clip(np.rint((v.astype(np.float64) - 128.0) * scale + 128.0), 0, 255)
+    return yy.astype(np.uint8), uu.astype(np.uint8), vv.astype(np.uint8)

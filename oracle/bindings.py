@@ -6,7 +6,7 @@ import os
 
 import numpy as np
 
-from libvc1_b200.abi import Analysis, BAnalysis, BAnalysisC, Mv, PAnalysisC, Params, mbs_of
+from libvc1_b200.abi import Analysis, BAnalysis, BAnalysisC, Intensity, Mv, PAnalysisC, Params, mbs_of
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_oracle", "libvc1oracle.so")
@@ -73,6 +73,8 @@ class Oracle:
         L.vo_forward_part.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, vp]
         L.vo_quantize_level.argtypes = [P, C.c_double]
         L.vo_forward_quant.argtypes = [P, vp, vp, i32, vp, vp]
+        L.vo_estimate_intensity_comp.argtypes = [P, vp, vp, vp, C.POINTER(Intensity)]
+        L.vo_intensity_compensate.argtypes = [vp, C.POINTER(Intensity), vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -146,6 +148,20 @@ class Oracle:
         if rc:
             raise RuntimeError("oracle analyze_p_core failed")
         return out.take_totals(oc)
+
+    def estimate_intensity_comp(self, p, cur, ref, mvs):
+        m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)
+        out = Intensity()
+        self.lib.vo_estimate_intensity_comp(C.byref(p), self._f(cur), self._f(ref), m.ctypes.data, C.byref(out))
+        return out.as_tuple()
+
+    def intensity_compensate(self, ref, ic):
+        y, u, v = _planes(ref)
+        h, w = y.shape
+        k = Intensity(*ic)
+        oy, ou, ov = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
+        self.lib.vo_intensity_compensate(self._f(ref), C.byref(k), oy.ctypes.data, ou.ctypes.data, ov.ctypes.data)
+        return oy, ou, ov
 
     def analyze_b(self, p, cur, past, future, anchor_mvs, anchor_4mv, num, den, mode):
         mbw, mbh = mbs_of(p)
@@ -232,6 +248,8 @@ class Reference:
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
         L.ref_forward_quant.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
+        L.ref_estimate_ic.argtypes = [vp, vp, vp, vp, C.POINTER(Intensity)]
+        L.ref_ic_reference.argtypes = [vp, vp, C.POINTER(Intensity), vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -299,6 +317,24 @@ class Reference:
         if rc:
             raise RuntimeError("reference analyze_p_picture_core threw")
         return out.take_totals(oc)
+
+    def estimate_intensity_comp(self, cur, ref, mvs):
+        m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)
+        out = Intensity()
+        self.lib.ref_estimate_ic(self.h, self._f(cur), self._f(ref), m.ctypes.data, C.byref(out))
+        return out.as_tuple()
+
+    def intensity_compensate(self, ref, ic):
+        h, w = self.p.height, self.p.width
+        dst = self.frame((np.zeros((h, w), np.uint8), np.zeros((h // 2, w // 2), np.uint8),
+                          np.zeros((h // 2, w // 2), np.uint8)))
+        k = Intensity(*ic)
+        self.lib.ref_ic_reference(self.h, self._f(ref), C.byref(k), dst.h)
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
 
     def analyze_b(self, cur, past, future, anchor_mvs, anchor_4mv, num, den, mode):
         mbw, mbh = mbs_of(self.p)

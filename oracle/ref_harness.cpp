@@ -258,6 +258,24 @@ int ref_analyze_b(void* h, void* cur, void* past, void* future, const vc1cu_mv* 
     }
 }
 
+// Vc1Encoder::estimate_intensity_comp along a host MV field.
+void ref_estimate_ic(void* h, void* cur, void* ref, const vc1cu_mv* mvs, vc1cu_intensity* out) {
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const size_t mbs = static_cast<size_t>((c.width + 15) / 16) * ((c.height + 15) / 16);
+    std::vector<MV> field(mbs);
+    for (size_t i = 0; i < mbs; ++i) field[i] = MV{mvs[i].xq, mvs[i].yq};
+    const auto ic = E(h).estimate_intensity_comp(F(cur), F(ref), field);
+    out->enabled = ic.enabled ? 1 : 0;
+    out->lumscale = ic.lumscale;
+    out->lumshift = ic.lumshift;
+}
+
+// Vc1Encoder::intensity_compensated_reference into dst (a frame handle of the same size).
+void ref_ic_reference(void* h, void* ref, const vc1cu_intensity* ic, void* dst) {
+    Vc1Encoder::IntensityComp k{ic->enabled != 0, static_cast<uint8_t>(ic->lumscale), static_cast<uint8_t>(ic->lumshift)};
+    *static_cast<Frame*>(dst) = E(h).intensity_compensated_reference(F(ref), k);
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

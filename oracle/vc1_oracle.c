@@ -2111,3 +2111,103 @@ done:
     free(fmv); free(bmv); free(fscreen); free(bscreen); free(ofm); free(obm);
     return rc;
 }
+
+/* ---- intensity compensation --------------------------------------------------------- */
+
+/* The LUMSCALE / LUMSHIFT luma law of Vc1Encoder::intensity_map_y,
+ * encoder_motion_compensation.cpp:175-187 (scale and shift of (scale*v + shift + 32) >> 6) */
+static void ic_luma_law(int lumscale, int lumshift, int* scale, int* shift) {
+    if (lumscale == 0) {
+        *scale = -64;
+        *shift = (255 - lumshift * 2) * 64;
+        if (lumshift > 31) *shift += 128 * 64;
+    } else {
+        *scale = lumscale + 32;
+        *shift = (lumshift > 31 ? lumshift - 64 : lumshift) * 64;
+    }
+}
+static int ic_map_y(int v, int scale, int shift) { return iclamp((scale * v + shift + 32) >> 6, 0, 255); }
+
+/* Vc1Encoder::intensity_compensated_reference, encoder_motion_compensation.cpp:195-294, with
+ * intensity_map_uv (:189-193) for chroma; a plain copy when the compensation is off */
+void vo_intensity_compensate(const vo_frame* ref, const vc1cu_intensity* ic, uint8_t* y, uint8_t* u, uint8_t* v) {
+    const size_t ny = (size_t)ref->w * ref->h, nc = (size_t)(ref->w / 2) * (ref->h / 2);
+    if (!ic->enabled) {
+        memcpy(y, ref->y, ny);
+        if (ref->u) memcpy(u, ref->u, nc); else memset(u, 128, nc);
+        if (ref->v) memcpy(v, ref->v, nc); else memset(v, 128, nc);
+        return;
+    }
+    int scale, shift;
+    ic_luma_law(ic->lumscale, ic->lumshift, &scale, &shift);
+    for (size_t i = 0; i < ny; ++i) y[i] = (uint8_t)ic_map_y(ref->y[i], scale, shift);
+    const int cs = ic->lumscale == 0 ? -64 : ic->lumscale + 32;
+    for (size_t i = 0; i < nc; ++i) {
+        const int cu = ref->u ? ref->u[i] : 128, cv = ref->v ? ref->v[i] : 128;
+        u[i] = (uint8_t)iclamp((cs * (cu - 128) + 128 * 64 + 32) >> 6, 0, 255);
+        v[i] = (uint8_t)iclamp((cs * (cv - 128) + 128 * 64 + 32) >> 6, 0, 255);
+    }
+}
+
+/* Vc1Encoder::estimate_intensity_comp, encoder_motion_compensation.cpp:296-348: one sample per
+ * 4x4 luma cell along the MV field, a long double least-squares fit cur ~ a*ref + b, then the
+ * (LUMSCALE, shift) pair of smallest sample SAD in the fit's 7x7 neighbourhood. */
+void vo_estimate_intensity_comp(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, const vc1cu_mv* mvs,
+                                vc1cu_intensity* out) {
+    const int mbw = mbw_of(p), mbh = mbh_of(p), W = p->width, H = p->height;
+    out->enabled = 0;  /* IntensityComp{} (encoder_internal.h:341-345): off, LUMSCALE 32, LUMSHIFT 0 */
+    out->lumscale = 32;
+    out->lumshift = 0;
+    const size_t cap = (size_t)((W + 3) / 4) * ((H + 3) / 4) + 16;
+    uint8_t* rs = (uint8_t*)malloc(cap);
+    uint8_t* cs = (uint8_t*)malloc(cap);
+    long double sx = 0, sy = 0, sxx = 0, sxy = 0;
+    uint64_t n = 0;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const vc1cu_mv mv = mvs[(size_t)my * mbw + mx];
+            const int dx = round_qpel_to_pixel(mv.xq), dy = round_qpel_to_pixel(mv.yq);
+            const int x0 = mx * 16, y0 = my * 16;
+            for (int y = 0; y < 16 && y0 + y < H; y += 4)
+                for (int x = 0; x < 16 && x0 + x < W; x += 4) {
+                    const int px = x0 + x, py = y0 + y;
+                    const int rv = sample_clamped(ref->y, W, H, px + dx, py + dy);
+                    const int cv = f->y[(size_t)py * W + px];
+                    rs[n] = (uint8_t)rv;
+                    cs[n] = (uint8_t)cv;
+                    sx += rv; sy += cv; sxx += (long double)rv * rv; sxy += (long double)rv * cv;
+                    ++n;
+                }
+        }
+    if (n >= 16) {
+        const long double denom = (long double)n * sxx - sx * sx;
+        long double a = 1.0L, b = 0.0L;
+        if (fabsl(denom) > 1e-9L) {
+            a = ((long double)n * sxy - sx * sy) / denom;
+            b = (sy - a * sx) / (long double)n;
+        } else {
+            b = (sy - sx) / (long double)n;
+        }
+        const int ls = iclamp((int)llroundl(a * 64.0L - 32.0L), 1, 63);
+        const int sh = iclamp((int)llroundl(b), -32, 31);
+        uint64_t best = UINT64_MAX;
+        int best_ls = 32, best_sh = 0;
+        for (int l = imax(1, ls - 3); l <= imin(63, ls + 3); ++l)
+            for (int z = imax(-32, sh - 3); z <= imin(31, sh + 3); ++z) {
+                uint64_t sad = 0;
+                for (uint64_t i = 0; i < n; ++i) sad += (uint64_t)iabs(cs[i] - ic_map_y(rs[i], l + 32, z * 64));
+                if (sad < best || (sad == best && iabs(l - 32) + iabs(z) < iabs(best_ls - 32) + iabs(best_sh))) {
+                    best = sad;
+                    best_ls = l;
+                    best_sh = z;
+                }
+            }
+        if (!(best_ls == 32 && best_sh == 0)) {
+            out->enabled = 1;
+            out->lumscale = best_ls;
+            out->lumshift = best_sh < 0 ? best_sh + 64 : best_sh;
+        }
+    }
+    free(rs);
+    free(cs);
+}

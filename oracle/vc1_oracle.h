@@ -74,6 +74,11 @@ int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* cur, const vo_frame
                       int allow_intra, const vc1cu_mv* seed, const vc1cu_panalysis* seed_distant,
                       vc1cu_panalysis* out);
 
+/* intensity compensation (fades) */
+void vo_intensity_compensate(const vo_frame* ref, const vc1cu_intensity* ic, uint8_t* y, uint8_t* u, uint8_t* v);
+void vo_estimate_intensity_comp(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, const vc1cu_mv* mvs,
+                                vc1cu_intensity* out);
+
 /* B-picture analysis: the two core passes + the per-MB mode decision */
 void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
                 int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]);

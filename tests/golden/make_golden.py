@@ -13,6 +13,9 @@ script calls it through oracle.Reference on inputs restated from the reference's
                     final Mixed-MV pass with P-intra) on seeded synthetic pictures
   xform_kat.npz     forward transform + quantiser of a motion-compensated prediction
   global_kat.npz    whole-frame translation search and frame SADs
+  ic_kat.npz        estimate_intensity_comp along each picture's quarter-pel field on seeded
+                    synthetic fades, and (small pictures) intensity_compensated_reference with
+                    the estimate and fixed LUMSCALE/LUMSHIFT codes covering the LUMSCALE 0 law
   b_kat.npz         analyze_b_picture_mode (two core passes + the per-MB B mode decision) of a
                     seeded three-picture group, anchor vectors from the future picture's own
                     Mixed-MV analysis, several fractions, modes and parameter sets
@@ -166,10 +169,47 @@ def make_b_kat():
     np.savez_compressed(os.path.join(HERE, "b_kat.npz"), **d)
 
 
+# intensity fixtures: (width, height, seed, fade scale, fade offset, params)
+IC_CASES = (
+    (98, 66, 1, 0.8, 10.0, dict(search_range=16, local_search_range=16)),
+    (130, 98, 2, 1.2, -20.0, dict(display_width=125, display_height=93, search_range=16, local_search_range=16)),
+    (352, 288, 4, 0.6, 30.0, dict(search_range=16, local_search_range=16)),
+    (66, 50, 5, 1.0, 0.0, dict(search_range=8, local_search_range=8)),
+    (16, 16, 6, 0.9, 5.0, dict(search_range=8, local_search_range=8)),
+)
+IC_FIXED = ((1, 0, 5), (1, 0, 40), (1, 63, 60), (1, 17, 33), (0, 0, 0))
+
+
+def make_ic_kat():
+    from oracle import Reference
+
+    d = {}
+    for i, (w, h, seed, a, b, kw) in enumerate(IC_CASES):
+        clip = synth.generate(w, h, 2, seed)
+        ref, cur = clip.frame(0), synth.fade(clip.frame(1), a, b, seed)
+        p = make_params(w, h, **kw)
+        R = Reference(p)
+        rc, rr = R.frame(cur), R.frame(ref)
+        q = R.analyze_p_core(rc, rr, MV_QPEL, False)
+        for c, pl in zip("yuv", ref):
+            d[f"c{i}.ref.{c}"] = pl
+        for c, pl in zip("yuv", cur):
+            d[f"c{i}.cur.{c}"] = pl
+        d[f"c{i}.mvs"] = q.mvs
+        ic = R.estimate_intensity_comp(rc, rr, q.mvs)
+        d[f"c{i}.ic"] = np.array(ic, np.int32)
+        if w * h > 130 * 98:
+            continue  # the mapped planes of the small pictures cover the law; keep the file small
+        for j, k in enumerate((ic,) + IC_FIXED):
+            for c, pl in zip("yuv", R.intensity_compensate(rr, k)):
+                d[f"c{i}.map{j}.{c}"] = pl
+    np.savez_compressed(os.path.join(HERE, "ic_kat.npz"), **d)
+
+
 def main(only=()):
     if only:
         for name in only:
-            {"b_kat": make_b_kat}[name]()
+            {"b_kat": make_b_kat, "ic_kat": make_ic_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -286,6 +326,7 @@ def main(only=()):
                                         np.uint64)
     np.savez_compressed(os.path.join(HERE, "global_kat.npz"), **d)
     make_b_kat()
+    make_ic_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -27,7 +27,8 @@ def test_library_exports_every_declared_symbol():
 STRUCTS = {"Params": (abi.Params, "vc1cu_params"), "Mv": (abi.Mv, "vc1cu_mv"),
            "PAnalysisC": (abi.PAnalysisC, "vc1cu_panalysis"), "Counters": (abi.Counters, "vc1cu_counters"),
            "Timing": (abi.Timing, "vc1cu_timing"), "Pass": (api.Pass, "vc1cu_pass"),
-           "BAnalysisC": (abi.BAnalysisC, "vc1cu_banalysis"), "BPass": (abi.BPass, "vc1cu_bpass")}
+           "BAnalysisC": (abi.BAnalysisC, "vc1cu_banalysis"), "BPass": (abi.BPass, "vc1cu_bpass"),
+           "Intensity": (abi.Intensity, "vc1cu_intensity"), "IcPass": (abi.IcPass, "vc1cu_icpass")}
 
 
 def test_struct_layouts_match_header(tmp_path):

@@ -270,3 +270,51 @@ def test_b_analysis_matches_reference_live(oracle, case):
     anc = R.analyze_p_core(rf, rp, MV_MIXED, True, seed=R.analyze_p_core(rf, rp, MV_QPEL, False).mvs)
     e = R.analyze_b(rc, rp, rf, anc.mvs, anc.use_4mv, num, den, mode)
     assert oracle.analyze_b(p, cur, past, fut, anc.mvs, anc.use_4mv, num, den, mode).equal(e) == []
+
+
+# ---- intensity compensation (estimate_intensity_comp, intensity_compensated_reference) ----
+
+IC_CASES = ((98, 66), (130, 98), (352, 288), (66, 50), (16, 16))
+IC_FIXED = ((1, 0, 5), (1, 0, 40), (1, 63, 60), (1, 17, 33), (0, 0, 0))
+IC_PARAMS = (dict(search_range=16, local_search_range=16),
+             dict(display_width=125, display_height=93, search_range=16, local_search_range=16),
+             dict(search_range=16, local_search_range=16), dict(search_range=8, local_search_range=8),
+             dict(search_range=8, local_search_range=8))
+
+
+@pytest.mark.parametrize("i", range(len(IC_CASES)))
+def test_intensity_golden(oracle, i):
+    """The fade estimate along the reference's own quarter-pel field, and the compensated planes."""
+    g = load("ic_kat.npz")
+    w, h = IC_CASES[i]
+    p = make_params(w, h, **IC_PARAMS[i])
+    ref, cur = _frames(g, f"c{i}.ref"), _frames(g, f"c{i}.cur")
+    ic = oracle.estimate_intensity_comp(p, cur, ref, g[f"c{i}.mvs"])
+    assert ic == tuple(g[f"c{i}.ic"].tolist())
+    if f"c{i}.map0.y" in g.files:
+        for j, k in enumerate((ic,) + IC_FIXED):
+            for got, c in zip(oracle.intensity_compensate(ref, k), "yuv"):
+                assert np.array_equal(got, g[f"c{i}.map{j}.{c}"]), (j, c)
+
+
+def test_intensity_fixture_covers_both_outcomes():
+    g = load("ic_kat.npz")
+    states = {int(g[f"c{i}.ic"][0]) for i in range(len(IC_CASES))}
+    assert states == {0, 1}
+
+
+@pytest.mark.parametrize("case", [(98, 66, 11, 0.7, 25.0), (322, 242, 12, 1.15, -12.0), (130, 98, 13, 1.0, 0.0)])
+def test_intensity_matches_reference_live(oracle, case):
+    Reference = _ref_or_skip()
+    w, h, seed, a, b = case
+    clip = synth.generate(w, h, 2, seed)
+    ref, cur = clip.frame(0), synth.fade(clip.frame(1), a, b, seed)
+    p = make_params(w, h, search_range=16, local_search_range=16)
+    R = Reference(p)
+    rc, rr = R.frame(cur), R.frame(ref)
+    q = R.analyze_p_core(rc, rr, MV_QPEL, False)
+    ic = R.estimate_intensity_comp(rc, rr, q.mvs)
+    assert oracle.estimate_intensity_comp(p, cur, ref, q.mvs) == ic
+    for k in (ic, (1, 0, 33), (1, 45, 12)):
+        for x, y in zip(oracle.intensity_compensate(ref, k), R.intensity_compensate(rr, k)):
+            assert np.array_equal(x, y)
