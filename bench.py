@@ -11,9 +11,9 @@ pictures per clip. Search range +/-64, Mixed-MV, non-uniform quantiser at QP 4/6
 
 One step = every picture of the clip analysed:
   P pictures: the quarter-pel seed pass, the three seeded mode passes (half-pel, half-pel
-    bilinear, Mixed-MV), the final Mixed-MV pass with P-intra, the decoder-equivalent
-    prediction, and the forward transform + quantiser of that prediction for all four
-    transform sizes (Vc1Encoder::analyze_p_picture_core x5 and quantize_inter_part,
+    bilinear, Mixed-MV), the final Mixed-MV pass with P-intra, the fade (intensity
+    compensation) estimate along its vectors, the decoder-equivalent prediction, and the
+    forward transform + quantiser of that prediction for all four transform sizes (Vc1Encoder::analyze_p_picture_core x5 and quantize_inter_part,
     src/encoder_motion.cpp:47-597, src/encoder_transform.cpp:935-1171). The final pass is
     timed in Mixed-MV mode, the most expensive of the reference's four candidates (the
     reference chooses it on the host by sampled RD).
@@ -62,7 +62,8 @@ OPS_PER_MB = {"unseeded": 286137.3, "seeded_hpel": 56261.4, "seeded_bilinear": 2
               "final_mixed_intra": 472178.7, "b_qpel_forward": 286981.1, "b_qpel_backward": 289317.5,
               "b_bilinear_forward": 121400.1, "b_bilinear_backward": 122512.3}
 WORKLOAD = ("1080p IBBP analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP as the reference plans it -> 20 P + 35 B "
-            "pictures/step; P: 5 core passes + prediction + 4-size transform/quant; B: forward+backward core passes and "
+            "pictures/step; P: 5 core passes + fade estimate + prediction + 4-size transform/quant; B: forward+backward "
+            "core passes and "
             "the MB decision in qpel and hpel-bilinear mode; search +/-64, Mixed-MV, nonuniform QP 4-12")
 # DRAM bytes (read + write) of core_pass_kernel per launch on this workload: an ncu capture of the
 # first GOP's six core launches (121.6 MB; profiles/core_pass_kernel_1080p_first_gop.md) scaled by
@@ -192,6 +193,9 @@ class Runner:
                                   2 * k + j, pq)
                                  for k, (t, past, fut, num, den, pq, a) in enumerate(self.bpics)
                                  for j, m in enumerate((self.QPEL, self.BIL))])
+        # the fade estimate analyze_p_picture runs on its final pass when fade compensation is on
+        # (the default; encoder_motion.cpp:570-573); it waits for the step's device work
+        self.ic = c.estimate_intensity_batch(self.p0, [(t, r, 3000 + i) for i, (t, r, pq) in enumerate(pics)])
 
     def read_results(self):
         """D2H of every P picture's final-pass analysis and every B analysis (waits for the step)."""
@@ -341,7 +345,7 @@ def run_ours(args, rank, world, device):
                          "traffic": round(CORE_DRAM_BYTES_PER_LAUNCH) if args.gops is None else None,
                          "traffic_unit": "DRAM bytes per launch (ncu, first GOP scaled by macroblocks)"},
             "kernel_ms_per_step": {k: round(timing[k] / args.steps, 3)
-                                   for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms")},
+                                   for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms", "ic_ms")},
             "xform_roofline": {"bound": "fp64", "achieved_gflops": round(xform_flops / (xform_ms * 1e-3) / 1e9, 1)
                                if xform_ms > 0 else None},
             "clocks": clocks,
