@@ -1,7 +1,7 @@
 /*
  * vc1cu.h - C ABI of the B200 (sm_100a) backend for libvc1's encoder-analysis hot path.
  *
- * The library (libvc1_b200/libvc1cu.so) replaces three pieces of libvc1 (v0.2.69):
+ * The library (libvc1_b200/libvc1cu.so) replaces these pieces of libvc1 (v0.2.69):
  *
  *   1. the motion-compute backend interface that the Vulkan path implements
  *      (src/vulkan_compute.h:26-60, class VulkanComputeContext), as vc1cu_open /
@@ -12,7 +12,12 @@
  *      vc1cu_analyze_p_core (host buffers) and vc1cu_core_passes (device-resident batch);
  *   3. the forward 8x8/8x4/4x8/4x4 transform + scalar quantiser of a motion-compensated
  *      prediction, forward_transform_residual_part + scalar_quantize_level
- *      (src/encoder_transform.cpp:935-1045, :1067-1085), as vc1cu_forward_quant.
+ *      (src/encoder_transform.cpp:935-1045, :1067-1085), as vc1cu_forward_quant;
+ *   4. the B-picture analysis, Vc1Encoder::analyze_b_picture_mode (encoder_motion.cpp:753-1005),
+ *      as vc1cu_analyze_b_picture / vc1cu_b_decide;
+ *   5. the fade and scene-cut analysis: estimate_intensity_comp and
+ *      intensity_compensated_reference (encoder_motion_compensation.cpp:175-348) and
+ *      scene_change_score (encoder_motion.cpp:599-676).
  *
  * Conventions: every function is extern "C", returns an int status (VC1CU_OK on
  * success), never throws, and records a message retrievable with vc1cu_last_error().
@@ -370,6 +375,19 @@ typedef struct vc1cu_icpass {
 
 int vc1cu_estimate_intensity_batch(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
                                    vc1cu_intensity* out);
+
+/*
+ * Replaces Vc1Encoder::scene_change_score (src/encoder_motion.cpp:599-676), the scene-cut test
+ * the encoder runs between consecutive frames (encoder_core.cpp:828): the whole-frame
+ * translation SAD per pixel at min(search_range, 32); with fade_compensation, the same against
+ * the fade-compensated reference found along the uniform translation field, keeping the
+ * smaller; and when the score still reaches scene_threshold, an unseeded quarter-pel core pass
+ * whose field, if it fits a camera zoom, may replace the score by its mean residual. The
+ * searches and the pass run on the device; the fits use the reference's long double
+ * arithmetic on the host. Synchronous.
+ */
+int vc1cu_scene_change_score(vc1cu_ctx* ctx, const vc1cu_params* p, int cur_id, int ref_id, int fade_compensation,
+                             double scene_threshold, double* score);
 
 /* Replaces Vc1Encoder::intensity_compensated_reference (encoder_motion_compensation.cpp:195-294):
  * frame slot out_id becomes ref_id with the luma and chroma maps of ic (intensity_map_y /

@@ -35,7 +35,7 @@ EXPORTS = (
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
-    "vc1cu_intensity_compensate",
+    "vc1cu_intensity_compensate", "vc1cu_scene_change_score",
 )
 
 
@@ -87,6 +87,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_estimate_intensity_comp.argtypes = [vp, PP, i32, i32, vp, C.POINTER(Intensity)]
     L.vc1cu_estimate_intensity_batch.argtypes = [vp, PP, C.POINTER(IcPass), i32, C.POINTER(Intensity)]
     L.vc1cu_intensity_compensate.argtypes = [vp, i32, C.POINTER(Intensity), i32]
+    L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
     _LIB = L
@@ -268,6 +269,15 @@ class CudaComputeContext:
         out = (Intensity * max(1, len(passes)))()
         self._check(self._L.vc1cu_estimate_intensity_batch(self._h, C.byref(params), arr, len(passes), out))
         return [out[i].as_tuple() for i in range(len(passes))]
+
+    def scene_change_score(self, params: Params, cur_id: int, ref_id: int, fade_compensation: bool = True,
+                           scene_threshold: float = 28.0) -> float:
+        """Vc1Encoder::scene_change_score (src/encoder_motion.cpp:599-676): the scene-cut score of
+        cur_id against ref_id (a cut when it reaches the encoder's scene threshold)."""
+        out = C.c_double()
+        self._check(self._L.vc1cu_scene_change_score(self._h, C.byref(params), cur_id, ref_id, int(fade_compensation),
+                                                     float(scene_threshold), C.byref(out)))
+        return out.value
 
     def intensity_compensate(self, ref_id: int, ic, out_id: int):
         """Frame slot out_id = the intensity-compensated reference of ref_id (intensity_compensated_reference)."""

@@ -70,6 +70,7 @@ constexpr int kInternalAnchor = kMaxSlot + 5;
 constexpr int kInternalIc = kMaxSlot + 6;     // MV field of vc1cu_estimate_intensity_comp
 constexpr int kInternalLast = kInternalIc;
 constexpr int kInternalB = kMaxSlot + 1;     // B-result slot of vc1cu_analyze_b_picture
+constexpr int kInternalFrame = kMaxSlot + 1; // frame slot of the scene score's compensated reference
 constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
 #ifndef VC1CU_SEEDED_MIXED_RW
 #define VC1CU_SEEDED_MIXED_RW 8
@@ -1026,6 +1027,81 @@ void ic_estimate(vc1cu_ctx* c, const DevParams& P, const std::vector<IcJob>& job
     for (int i = 0; i < n; ++i) out[i] = ic_decide(sums.data() + 5 * i, tables.data() + kTable * i);
 }
 
+// Vc1Encoder::global_motion_search (encoder_motion.cpp:2076-2141) of one picture pair at
+// min(range, 32), on the device; the result lands in result slot `slot`'s global fields.
+void global_search_one(vc1cu_ctx* c, const DevFrame& cur, const DevFrame& ref, int range, int W, int H, int slot, int mbs,
+                       int* dx, int* dy, uint64_t* sad) {
+    ResultSlot& s = result_slot(c, slot, mbs, true);
+    const size_t gb = gstate_bytes();
+    if (c->gstates_cap < 1) {
+        void* d = nullptr;
+        ck(cudaMalloc(&d, gb), "cudaMalloc(global search state)");
+        c->d_gstates = static_cast<GState*>(d);
+        c->gstates_cap = 1;
+    }
+    uint8_t* hs = static_cast<uint8_t*>(staging(c, gb));
+    const int grange = std::min(range, 32);
+    init_gstate(reinterpret_cast<GState*>(hs), cur, ref, grange, s.r.global, s.r.gsad);
+    ck(cudaMemcpyAsync(c->d_gstates, hs, gb, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
+    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    {
+        Timer tm(c, kGlobal);
+        const int launches = run_global_search(c->d_gstates, 1, grange, W, H, c->stream);
+        ck(cudaGetLastError(), "global search launch");
+        tm.stop(launches);
+    }
+    int g[2];
+    unsigned long long gs = 0;
+    ck(cudaMemcpyAsync(g, s.r.global, 8, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(global)");
+    ck(cudaMemcpyAsync(&gs, s.r.gsad, 8, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(global)");
+    sync_checked(c);
+    *dx = g[0];
+    *dy = g[1];
+    *sad = gs;
+}
+
+// The zoom-coherence test of Vc1Encoder::scene_change_score (encoder_motion.cpp:636-671), in
+// the reference's long double arithmetic.
+bool zoom_coherent(const std::vector<vc1cu_mv>& mvs, int mbw, int mbh) {
+    long double mx = 0.0L, my = 0.0L, mdx = 0.0L, mdy = 0.0L;
+    size_t samples = 0;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[static_cast<size_t>(by) * mbw + bx];
+            mx += bx * 16.0L + 8.0L;
+            my += by * 16.0L + 8.0L;
+            mdx += mv.xq / 4.0L;
+            mdy += mv.yq / 4.0L;
+            ++samples;
+        }
+    if (samples < 12) return false;
+    mx /= samples;
+    my /= samples;
+    mdx /= samples;
+    mdy /= samples;
+    long double num = 0.0L, den = 0.0L;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[static_cast<size_t>(by) * mbw + bx];
+            const long double x = bx * 16.0L + 8.0L - mx, y = by * 16.0L + 8.0L - my;
+            const long double dx = mv.xq / 4.0L - mdx, dy = mv.yq / 4.0L - mdy;
+            num += x * dx + y * dy;
+            den += x * x + y * y;
+        }
+    const long double z = den > 0.0L ? num / den : 0.0L;
+    size_t inliers = 0;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[static_cast<size_t>(by) * mbw + bx];
+            const long double x = bx * 16.0L + 8.0L - mx, y = by * 16.0L + 8.0L - my;
+            const long double ex = mv.xq / 4.0L - (mdx + z * x);
+            const long double ey = mv.yq / 4.0L - (mdy + z * y);
+            if (ex * ex + ey * ey <= 6.25L) ++inliers;
+        }
+    const long double az = std::fabs(z);
+    return inliers * 5 >= samples * 3 && az >= 0.005L && az <= 0.08L;
+}
+
 void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
     const size_t n = (size_t)s.mbs;
     auto cp = [&](void* dst, const void* src, size_t b) {
@@ -1436,6 +1512,66 @@ int vc1cu_estimate_intensity_batch(vc1cu_ctx* c, const vc1cu_params* p, const vc
             jobs.push_back(IcJob{fc.view(), fr.view(), result_slot(c, passes[i].mv_slot, mbs, false).r.mvs});
         }
         ic_estimate(c, P, jobs, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_scene_change_score(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, int ref_id, int fade_compensation,
+                             double scene_threshold, double* score) {
+    return guarded(c, [&]() -> int {
+        if (!score) throw Fail{VC1CU_ERR_ARG, "null output"};
+        if (!(scene_threshold >= 0.0 && scene_threshold <= 255.0)) throw Fail{VC1CU_ERR_ARG, "scene threshold must be 0..255"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        check_status(c);
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fr = frame_slot(c, ref_id);
+        if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "scene-analysis dimensions do not match the configuration"};
+        const DevFrame cur = fc.view(), ref = fr.view();
+        int gdx = 0, gdy = 0;
+        uint64_t gsad = 0;
+        global_search_one(c, cur, ref, P.range, P.W, P.H, kInternalIc, mbs, &gdx, &gdy, &gsad);
+        const uint64_t pixels = static_cast<uint64_t>(P.W) * P.H;
+        double best = pixels ? static_cast<double>(gsad) / static_cast<double>(pixels) : 0.0;
+        if (fade_compensation) {
+            // the fade estimate along the uniform global field (encoder_motion.cpp:606-616)
+            std::vector<vc1cu_mv> uniform(mbs, vc1cu_mv{gdx * 4, gdy * 4});
+            ResultSlot& s = result_slot(c, kInternalIc, mbs, true);
+            ck(cudaMemcpyAsync(s.r.mvs, uniform.data(), 8 * (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload field");
+            vc1cu_intensity ic{};
+            ic_estimate(c, P, {IcJob{cur, ref, s.r.mvs}}, &ic);
+            if (ic.enabled) {
+                FrameSlot& fw = alloc_frame(c, kInternalFrame, P.W, P.H);
+                const DevFrame w = fw.view();
+                const int scale = ic.lumscale + 32, shift = (ic.lumshift > 31 ? ic.lumshift - 64 : ic.lumshift) * 64;
+                ck(launch_ic_map(ref, (uint8_t*)w.y, (uint8_t*)w.u, (uint8_t*)w.v, fw.pitch_y, fw.pitch_c, P.W, P.H, 1, scale,
+                                 shift, ic.lumscale + 32, c->stream),
+                   "intensity map launch");
+                c->counters.kernel_launches++;
+                int wdx = 0, wdy = 0;
+                uint64_t wsad = 0;
+                global_search_one(c, cur, w, P.range, P.W, P.H, kInternalIc, mbs, &wdx, &wdy, &wsad);
+                const double wm = pixels ? static_cast<double>(wsad) / static_cast<double>(pixels) : 0.0;
+                best = std::min(best, wm);
+            }
+        }
+        if (best >= scene_threshold) {
+            // a local quarter-pel core pass may rescue a camera zoom (encoder_motion.cpp:627-674)
+            const vc1cu_pass q{cur_id, ref_id, VC1CU_MV_QPEL, 0, -1, kInternalOut, 0};
+            launch_passes(c, p, &q, 1);
+            check_status(c);
+            std::vector<vc1cu_mv> mvs(mbs);
+            vc1cu_panalysis a{};
+            a.mvs = mvs.data();
+            read_result(c, c->results[kInternalOut], &a);
+            const double lm = a.mean_abs_residual;
+            if (zoom_coherent(mvs, P.mbw, P.mbh) && lm < best * 0.72 && lm < scene_threshold * 0.86) best = lm;
+        }
+        *score = best;
         return VC1CU_OK;
     });
 }

@@ -75,6 +75,9 @@ class Oracle:
         L.vo_forward_quant.argtypes = [P, vp, vp, i32, vp, vp]
         L.vo_estimate_intensity_comp.argtypes = [P, vp, vp, vp, C.POINTER(Intensity)]
         L.vo_intensity_compensate.argtypes = [vp, C.POINTER(Intensity), vp, vp, vp]
+        L.vo_scene_change_score.argtypes = [P, vp, vp, i32, C.c_double]
+        L.vo_scene_change_score.restype = C.c_double
+        L.vo_zoom_coherent.argtypes = [vp, i32, i32]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -148,6 +151,14 @@ class Oracle:
         if rc:
             raise RuntimeError("oracle analyze_p_core failed")
         return out.take_totals(oc)
+
+    def scene_change_score(self, p, cur, ref, fade_compensation=True, scene_threshold=28.0):
+        return self.lib.vo_scene_change_score(C.byref(p), self._f(cur), self._f(ref), int(fade_compensation),
+                                              float(scene_threshold))
+
+    def zoom_coherent(self, mvs, mbw, mbh):
+        m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)
+        return bool(self.lib.vo_zoom_coherent(m.ctypes.data, mbw, mbh))
 
     def estimate_intensity_comp(self, p, cur, ref, mvs):
         m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)
@@ -250,6 +261,8 @@ class Reference:
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
         L.ref_estimate_ic.argtypes = [vp, vp, vp, vp, C.POINTER(Intensity)]
         L.ref_ic_reference.argtypes = [vp, vp, C.POINTER(Intensity), vp]
+        L.ref_scene_change_score.argtypes = [vp, vp, vp, i32, C.c_double]
+        L.ref_scene_change_score.restype = C.c_double
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -317,6 +330,10 @@ class Reference:
         if rc:
             raise RuntimeError("reference analyze_p_picture_core threw")
         return out.take_totals(oc)
+
+    def scene_change_score(self, cur, ref, fade_compensation=True, scene_threshold=28.0):
+        return self.lib.ref_scene_change_score(self.h, self._f(cur), self._f(ref), int(fade_compensation),
+                                               float(scene_threshold))
 
     def estimate_intensity_comp(self, cur, ref, mvs):
         m = np.ascontiguousarray(mvs, np.int32).reshape(-1, 2)

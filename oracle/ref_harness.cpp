@@ -276,6 +276,15 @@ void ref_ic_reference(void* h, void* ref, const vc1cu_intensity* ic, void* dst) 
     *static_cast<Frame*>(dst) = E(h).intensity_compensated_reference(F(ref), k);
 }
 
+// Vc1Encoder::scene_change_score with the given fade-compensation switch and threshold.
+double ref_scene_change_score(void* h, void* cur, void* ref, int fade_compensation, double scene_threshold) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.fade_compensation = fade_compensation != 0;
+    c.scene_threshold = scene_threshold;
+    Vc1Encoder enc(c);
+    return enc.scene_change_score(F(cur), F(ref));
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

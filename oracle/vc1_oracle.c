@@ -2211,3 +2211,89 @@ void vo_estimate_intensity_comp(const vc1cu_params* p, const vo_frame* f, const 
     free(rs);
     free(cs);
 }
+
+/* ---- scene-change score ------------------------------------------------------------ */
+
+/* The zoom-coherence test of Vc1Encoder::scene_change_score, encoder_motion.cpp:636-671:
+ * the interior vectors fitted to translation + isotropic scale in long double; coherent when
+ * 60% of them lie within 2.5 px of the fitted field and 0.005 <= |scale| <= 0.08. */
+int vo_zoom_coherent(const vc1cu_mv* mvs, int mbw, int mbh) {
+    long double mx = 0.0L, my = 0.0L, mdx = 0.0L, mdy = 0.0L;
+    size_t samples = 0;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[(size_t)by * mbw + bx];
+            mx += bx * 16.0L + 8.0L;
+            my += by * 16.0L + 8.0L;
+            mdx += mv.xq / 4.0L;
+            mdy += mv.yq / 4.0L;
+            ++samples;
+        }
+    if (samples < 12) return 0;
+    mx /= samples; my /= samples; mdx /= samples; mdy /= samples;
+    long double num = 0.0L, den = 0.0L;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[(size_t)by * mbw + bx];
+            const long double x = bx * 16.0L + 8.0L - mx, y = by * 16.0L + 8.0L - my;
+            const long double dx = mv.xq / 4.0L - mdx, dy = mv.yq / 4.0L - mdy;
+            num += x * dx + y * dy;
+            den += x * x + y * y;
+        }
+    const long double z = den > 0.0L ? num / den : 0.0L;
+    size_t inliers = 0;
+    for (int by = 1; by < mbh - 1; ++by)
+        for (int bx = 1; bx < mbw - 1; ++bx) {
+            const vc1cu_mv mv = mvs[(size_t)by * mbw + bx];
+            const long double x = bx * 16.0L + 8.0L - mx, y = by * 16.0L + 8.0L - my;
+            const long double ex = mv.xq / 4.0L - (mdx + z * x);
+            const long double ey = mv.yq / 4.0L - (mdy + z * y);
+            if (ex * ex + ey * ey <= 6.25L) ++inliers;
+        }
+    const long double az = fabsl(z);
+    return inliers * 5 >= samples * 3 && az >= 0.005L && az <= 0.08L;
+}
+
+/* Vc1Encoder::scene_change_score, encoder_motion.cpp:599-676: the whole-frame translation
+ * SAD per pixel, the same after fade compensation along the uniform global field, and when
+ * that still looks like a cut, a quarter-pel core pass whose field must fit a camera zoom. */
+double vo_scene_change_score(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int fade_compensation,
+                             double scene_threshold) {
+    const int W = p->width, H = p->height, mbw = mbw_of(p), mbh = mbh_of(p);
+    const size_t mbs = (size_t)mbw * mbh;
+    int gdx, gdy;
+    uint64_t gsad;
+    vo_global_motion(p, f, ref, p->search_range, &gdx, &gdy, &gsad);
+    const uint64_t pixels = (uint64_t)W * H;
+    double best = pixels ? (double)gsad / (double)pixels : 0.0;
+    if (fade_compensation) {
+        vc1cu_mv* uniform = (vc1cu_mv*)malloc(mbs * sizeof(vc1cu_mv));
+        for (size_t i = 0; i < mbs; ++i) { uniform[i].xq = gdx * 4; uniform[i].yq = gdy * 4; }
+        vc1cu_intensity ic;
+        vo_estimate_intensity_comp(p, f, ref, uniform, &ic);
+        free(uniform);
+        if (ic.enabled) {
+            const size_t ny = (size_t)W * H, nc = (size_t)(W / 2) * (H / 2);
+            uint8_t* buf = (uint8_t*)malloc(ny + 2 * nc);
+            vo_intensity_compensate(ref, &ic, buf, buf + ny, buf + ny + nc);
+            const vo_frame weighted = {W, H, buf, buf + ny, buf + ny + nc};
+            int wdx, wdy;
+            uint64_t wsad;
+            vo_global_motion(p, f, &weighted, p->search_range, &wdx, &wdy, &wsad);
+            const double wm = pixels ? (double)wsad / (double)pixels : 0.0;
+            if (wm < best) best = wm;
+            free(buf);
+        }
+    }
+    if (best >= scene_threshold) {
+        vc1cu_panalysis a;
+        memset(&a, 0, sizeof a);
+        vc1cu_mv* mvs = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+        a.mvs = mvs;
+        vo_analyze_p_core(p, f, ref, VC1CU_MV_QPEL, 0, NULL, NULL, &a);
+        const double lm = a.mean_abs_residual;
+        if (vo_zoom_coherent(mvs, mbw, mbh) && lm < best * 0.72 && lm < scene_threshold * 0.86) best = lm;
+        free(mvs);
+    }
+    return best;
+}

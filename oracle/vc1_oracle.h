@@ -79,6 +79,11 @@ void vo_intensity_compensate(const vo_frame* ref, const vc1cu_intensity* ic, uin
 void vo_estimate_intensity_comp(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, const vc1cu_mv* mvs,
                                 vc1cu_intensity* out);
 
+/* scene-change score (scene cut detection) */
+int vo_zoom_coherent(const vc1cu_mv* mvs, int mbw, int mbh);
+double vo_scene_change_score(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int fade_compensation,
+                             double scene_threshold);
+
 /* B-picture analysis: the two core passes + the per-MB mode decision */
 void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
                 int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]);

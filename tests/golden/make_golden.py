@@ -16,6 +16,9 @@ script calls it through oracle.Reference on inputs restated from the reference's
   ic_kat.npz        estimate_intensity_comp along each picture's quarter-pel field on seeded
                     synthetic fades, and (small pictures) intensity_compensated_reference with
                     the estimate and fixed LUMSCALE/LUMSHIFT codes covering the LUMSCALE 0 law
+  scene_kat.npz     scene_change_score on seeded pictures: motion, a cut (two thresholds),
+                    a fade with and without fade compensation, two camera zooms that the
+                    local-motion fit rescues, and search range 0
   b_kat.npz         analyze_b_picture_mode (two core passes + the per-MB B mode decision) of a
                     seeded three-picture group, anchor vectors from the future picture's own
                     Mixed-MV analysis, several fractions, modes and parameter sets
@@ -206,10 +209,24 @@ def make_ic_kat():
     np.savez_compressed(os.path.join(HERE, "ic_kat.npz"), **d)
 
 
+def make_scene_kat():
+    from oracle import Reference
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from scene_cases import scene_pictures
+
+    d = {}
+    for name, (cur, ref, fade, thr, kw) in scene_pictures().items():
+        h, w = cur[0].shape
+        R = Reference(make_params(w, h, **kw))
+        d[f"{name}.score"] = np.float64(R.scene_change_score(R.frame(cur), R.frame(ref), fade, thr))
+    np.savez_compressed(os.path.join(HERE, "scene_kat.npz"), **d)
+
+
 def main(only=()):
     if only:
         for name in only:
-            {"b_kat": make_b_kat, "ic_kat": make_ic_kat}[name]()
+            {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -327,6 +344,7 @@ def main(only=()):
     np.savez_compressed(os.path.join(HERE, "global_kat.npz"), **d)
     make_b_kat()
     make_ic_kat()
+    make_scene_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -318,3 +318,38 @@ def test_intensity_matches_reference_live(oracle, case):
     for k in (ic, (1, 0, 33), (1, 45, 12)):
         for x, y in zip(oracle.intensity_compensate(ref, k), R.intensity_compensate(rr, k)):
             assert np.array_equal(x, y)
+
+
+# ---- scene-change score (scene_change_score) ----
+
+@pytest.mark.parametrize("name", ["motion", "cut", "cut_low_threshold", "fade", "fade_no_compensation", "zoom_rescue",
+                                  "zoom_rescue_fade", "range0"])
+def test_scene_score_golden(oracle, name):
+    from scene_cases import scene_pictures
+
+    g = load("scene_kat.npz")
+    cur, ref, fade, thr, kw = scene_pictures()[name]
+    h, w = cur[0].shape
+    got = oracle.scene_change_score(make_params(w, h, **kw), cur, ref, fade, thr)
+    assert np.float64(got).view(np.uint64) == g[f"{name}.score"].view(np.uint64)
+
+
+def test_scene_fixture_covers_every_path():
+    """The cases reach the cut, the fade rescue and the zoom rescue (scores below the plain one)."""
+    g = load("scene_kat.npz")
+    assert float(g["cut.score"]) >= 28.0
+    assert float(g["fade.score"]) < float(g["fade_no_compensation.score"])
+    assert float(g["zoom_rescue.score"]) < 10.0 * 0.86 and float(g["zoom_rescue_fade.score"]) < 12.0 * 0.86
+
+
+@pytest.mark.parametrize("case", [(322, 242, 21, 1.0, 0.0, 1, 28.0), (98, 66, 22, 0.7, 20.0, 1, 3.0),
+                                  (194, 146, 23, 1.0, 0.0, 0, 0.5)])
+def test_scene_score_matches_reference_live(oracle, case):
+    Reference = _ref_or_skip()
+    w, h, seed, a, b, fade, thr = case
+    clip = synth.generate(w, h, 2, seed, global_px=12.0)
+    cur = synth.fade(clip.frame(1), a, b, seed) if a != 1.0 else clip.frame(1)
+    p = make_params(w, h, search_range=48, local_search_range=16)
+    R = Reference(p)
+    assert oracle.scene_change_score(p, cur, clip.frame(0), fade, thr) == \
+        R.scene_change_score(R.frame(cur), R.frame(clip.frame(0)), fade, thr)
