@@ -187,6 +187,7 @@ struct vc1cu_ctx {
     uint32_t epoch = 0;
     int sm_count = 0;
     int max_smem = 0;
+    int max_smem_sm = 0;  // shared memory per SM
     // per-launch event timing
     bool timing = false;
     struct Timed { cudaEvent_t a, b; int family; };
@@ -706,7 +707,9 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     const size_t smem = (size_t)warps * wc.warp_bytes;
     if (smem > (size_t)c->max_smem)
         throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
-    const int kind = any_unseeded ? kCoreAny : kCoreSeeded;
+    int kind = any_unseeded ? kCoreAny : kCoreSeeded;
+    // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
+    if (kind == kCoreAny && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm) kind = kCoreAnyWide;
     const void* kern = core_kernel(kind);
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;
@@ -1180,6 +1183,7 @@ int vc1cu_open(int device, vc1cu_ctx** out) {
     c->name = prop.name;
     c->sm_count = prop.multiProcessorCount;
     c->max_smem = (int)prop.sharedMemPerBlockOptin;
+    c->max_smem_sm = (int)prop.sharedMemPerMultiprocessor;
     try {
         ck(cudaSetDevice(device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");

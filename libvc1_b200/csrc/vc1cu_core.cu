@@ -2124,7 +2124,8 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #define VC1CU_SEEDED_MIN_BLOCKS 4
 #endif
 template <int KIND>
-__global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS : VC1CU_CORE_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS
+                                                           : (KIND == kCoreAnyWide ? 1 : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
@@ -2523,10 +2524,11 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     return cudaGetLastError();
 }
 
-// Host-side handles of the two instantiations (attributes, occupancy, launch).
+// Host-side handles of the instantiations (attributes, occupancy, launch).
 const void* core_kernel(int kind) {
-    return kind == kCoreSeeded ? reinterpret_cast<const void*>(&core_pass_kernel<kCoreSeeded>)
-                               : reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
+    if (kind == kCoreSeeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreSeeded>);
+    if (kind == kCoreAnyWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAnyWide>);
+    return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
 }
 
 cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,
@@ -2534,6 +2536,8 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
                         uint32_t epoch, LaunchStatus* st) {
     if (kind == kCoreSeeded)
         core_pass_kernel<kCoreSeeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else if (kind == kCoreAnyWide)
+        core_pass_kernel<kCoreAnyWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     else
         core_pass_kernel<kCoreAny><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     return cudaGetLastError();

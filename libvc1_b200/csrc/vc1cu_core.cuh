@@ -58,8 +58,10 @@ struct PassDesc {
 };
 
 // core_pass_kernel instantiations
-constexpr int kCoreAny = 0;     // any mix of seeded and unseeded passes
-constexpr int kCoreSeeded = 1;  // seeded passes only
+constexpr int kCoreAny = 0;      // any mix of seeded and unseeded passes
+constexpr int kCoreSeeded = 1;   // seeded passes only
+constexpr int kCoreAnyWide = 2;  // kCoreAny compiled for one block per SM (all 255 registers), for
+                                 // launches whose search windows let only one block per SM anyway
 
 // Shared-memory window geometry for one launch.
 struct WinCfg {
