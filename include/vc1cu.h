@@ -341,6 +341,16 @@ typedef struct vc1cu_bpass {
 } vc1cu_bpass;
 
 int vc1cu_b_decide(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_bpass* passes, int n);
+/*
+ * The prediction of the B analysis in bslot into frame slot pred_id, as the reference builds it
+ * for every macroblock it codes or samples (encoder_motion.cpp:1030-1053): Forward and Backward
+ * with motion_compensate_mb, Direct and Interpolated with motion_compensate_bi_mb
+ * (encoder_motion_compensation.cpp:474-525, :659-711), B-intra macroblocks with the visible
+ * mean of each source 8x8 block. vc1cu_forward_quant(_device) of (cur_id, pred_id) then gives
+ * the B picture's coefficients and levels. Asynchronous.
+ */
+int vc1cu_b_predict(vc1cu_ctx* ctx, const vc1cu_params* p, int bslot, int cur_id, int past_id, int future_id,
+                    int pred_id);
 /* Copies a B-result slot to host arrays (and the scalar totals). Synchronous. */
 int vc1cu_read_bresult(vc1cu_ctx* ctx, int bslot, vc1cu_banalysis* out);
 

@@ -35,7 +35,7 @@ EXPORTS = (
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
-    "vc1cu_intensity_compensate", "vc1cu_scene_change_score",
+    "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict",
 )
 
 
@@ -87,6 +87,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_estimate_intensity_comp.argtypes = [vp, PP, i32, i32, vp, C.POINTER(Intensity)]
     L.vc1cu_estimate_intensity_batch.argtypes = [vp, PP, C.POINTER(IcPass), i32, C.POINTER(Intensity)]
     L.vc1cu_intensity_compensate.argtypes = [vp, i32, C.POINTER(Intensity), i32]
+    L.vc1cu_b_predict.argtypes = [vp, PP, i32, i32, i32, i32, i32]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
@@ -306,6 +307,11 @@ class CudaComputeContext:
         fraction_num, fraction_den, mode, out_bslot[, pqindex])."""
         arr = (BPass * len(bpasses))(*[BPass(*b) for b in bpasses])
         self._check(self._L.vc1cu_b_decide(self._h, C.byref(params), arr, len(bpasses)))
+
+    def b_predict(self, params: Params, bslot: int, cur_id: int, past_id: int, future_id: int, pred_id: int):
+        """Frame slot pred_id = the prediction of the B analysis in bslot (Forward / Backward /
+        Direct / Interpolated motion compensation, block means for B-intra)."""
+        self._check(self._L.vc1cu_b_predict(self._h, C.byref(params), bslot, cur_id, past_id, future_id, pred_id))
 
     def read_bresult(self, params: Params, bslot: int) -> BAnalysis:
         mbw, mbh = mbs_of(params)

@@ -45,6 +45,9 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
+cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
+                        const uint8_t* modes, const int2* fmv, const int2* bmv, int mode, uint8_t* dy, uint8_t* du,
+                        uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
 struct IcDesc;
 size_t ic_scratch_bytes();
 size_t ic_table_offset();
@@ -1439,6 +1442,35 @@ int vc1cu_read_bresult(vc1cu_ctx* c, int bslot, vc1cu_banalysis* out) {
         auto it = c->bresults.find(bslot);
         if (it == c->bresults.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "empty B-result slot"};
         read_bresult(c, it->second, out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_b_predict(vc1cu_ctx* c, const vc1cu_params* p, int bslot, int cur_id, int past_id, int future_id, int pred_id) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        auto it = c->bresults.find(bslot);
+        if (it == c->bresults.end() || !it->second.valid || it->second.mbs != P.mbw * P.mbh)
+            throw Fail{VC1CU_ERR_STATE, "B-result slot holds no analysis of this size"};
+        if (pred_id < 0 || pred_id >= kMaxSlot || pred_id == cur_id || pred_id == past_id || pred_id == future_id)
+            throw Fail{VC1CU_ERR_ARG, "invalid prediction slot"};
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fp = frame_slot(c, past_id);
+        FrameSlot& ff = frame_slot(c, future_id);
+        if (fc.w != P.W || fc.h != P.H || fp.w != P.W || fp.h != P.H || ff.w != P.W || ff.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "B-picture reference dimensions do not match the configuration"};
+        const DevFrame cur = fc.view(), past = fp.view(), fut = ff.view();
+        FrameSlot& fo = alloc_frame(c, pred_id, P.W, P.H);
+        const DevFrame o = fo.view();
+        const BSlot& b = it->second;
+        Timer tm(c, kMc);
+        ck(launch_b_mc(P, cur, past, fut, b.r.modes, b.r.fmv, b.r.bmv, b.mode, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v,
+                       fo.pitch_y, fo.pitch_c, c->stream),
+           "B prediction launch");
+        tm.stop(1);
         return VC1CU_OK;
     });
 }

@@ -266,6 +266,97 @@ __global__ void __launch_bounds__(128) b_decide_kernel(const __grid_constant__ D
     }
 }
 
+// Vc1Encoder::chroma_mc_sample (encoder_motion_compensation.cpp:417-447): future selects the
+// B future-reference rounding of the chroma vector (away from the even value).
+__device__ __forceinline__ int chroma_mc(const uint8_t* p, int pitch, int w, int h, int x, int y, int mvx, int mvy,
+                                         bool future, int rnd) {
+    int uvx = arshift(mvx + ((mvx & 3) == 3), 1);
+    int uvy = arshift(mvy + ((mvy & 3) == 3), 1);
+    if (future) {
+        uvx = uvx < 0 ? uvx - (uvx & 1) : uvx + (uvx & 1);
+        uvy = uvy < 0 ? uvy - (uvy & 1) : uvy + (uvy & 1);
+    } else {
+        uvx = uvx < 0 ? uvx + (uvx & 1) : uvx - (uvx & 1);
+        uvy = uvy < 0 ? uvy + (uvy & 1) : uvy - (uvy & 1);
+    }
+    const int ix = floor_div4(uvx), iy = floor_div4(uvy);
+    const int fx = (uvx - ix * 4) * 2, fy = (uvy - iy * 4) * 2;
+    const int sx = x + ix, sy = y + iy;
+    auto S = [&](int xx, int yy) { return (int)__ldg(p + (size_t)iclamp(yy, 0, h - 1) * pitch + iclamp(xx, 0, w - 1)); };
+    const int a = S(sx, sy);
+    if (!fx && !fy) return a;
+    const int b = S(sx + 1, sy), c = S(sx, sy + 1), d = S(sx + 1, sy + 1);
+    return (a * (8 - fx) * (8 - fy) + b * fx * (8 - fy) + c * (8 - fx) * fy + d * fx * fy + (rnd ? 28 : 32)) >> 6;
+}
+
+// Vc1Encoder::visible_block_mean (encoder_entropy.cpp:496-509) of the 8x8 block at (x0, y0)
+__device__ int block_mean(const uint8_t* p, int pitch, int w, int h, int x0, int y0) {
+    const int vw = imax(0, imin(8, w - x0)), vh = imax(0, imin(8, h - y0));
+    if (!vw || !vh) return 128;
+    uint32_t sum = 0;
+    for (int y = 0; y < vh; ++y)
+        for (int x = 0; x < vw; ++x) sum += __ldg(p + (size_t)(y0 + y) * pitch + x0 + x);
+    const uint32_t n = (uint32_t)(vw * vh);
+    return (int)((sum + n / 2) / n);
+}
+
+// The B prediction of an analysis (encoder_motion.cpp:1030-1053): one thread per luma pixel and,
+// for even coordinates, the co-sited chroma pair. Forward / Backward: motion_compensate_mb
+// (encoder_motion_compensation.cpp:474-525); Direct / Interpolated: motion_compensate_bi_mb
+// (:659-711); Intra: the visible mean of each source 8x8 block.
+__global__ void b_mc_kernel(const __grid_constant__ DevParams P, DevFrame cur, DevFrame past, DevFrame fut,
+                            const uint8_t* modes, const int2* fmv, const int2* bmv, int mode, uint8_t* dy, uint8_t* du,
+                            uint8_t* dv, int pitch_y, int pitch_c) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= P.W || y >= P.H) return;
+    const int pos = (y >> 4) * P.mbw + (x >> 4);
+    const int m = modes[pos];
+    const int cw = P.W / 2, ch = P.H / 2, cx = x >> 1, cy = y >> 1;
+    const bool chroma = !(x & 1) && !(y & 1) && cx < cw && cy < ch;
+    if (m == VC1CU_BMB_INTRA) {
+        dy[(size_t)y * pitch_y + x] = (uint8_t)block_mean(cur.y, cur.pitch_y, P.W, P.H, x & ~7, y & ~7);
+        if (chroma) {
+            du[(size_t)cy * pitch_c + cx] = (uint8_t)block_mean(cur.u, cur.pitch_c, cw, ch, cx & ~7, cy & ~7);
+            dv[(size_t)cy * pitch_c + cx] = (uint8_t)block_mean(cur.v, cur.pitch_c, cw, ch, cx & ~7, cy & ~7);
+        }
+        return;
+    }
+    const bool bil = mode_bilinear(mode);
+    if (m == VC1CU_BMB_FORWARD || m == VC1CU_BMB_BACKWARD) {
+        const DevFrame& r = m == VC1CU_BMB_FORWARD ? past : fut;
+        const int2 mv = m == VC1CU_BMB_FORWARD ? fmv[pos] : bmv[pos];
+        int o[1];
+        predict_row<1>(GlobSampler{r.y, r.pitch_y, P.W, P.H}, bil, P.rnd, mv.x, mv.y, x, y, o);
+        dy[(size_t)y * pitch_y + x] = (uint8_t)o[0];
+        if (chroma) {
+            du[(size_t)cy * pitch_c + cx] = (uint8_t)chroma_mc(r.u, r.pitch_c, cw, ch, cx, cy, mv.x, mv.y, false, P.rnd);
+            dv[(size_t)cy * pitch_c + cx] = (uint8_t)chroma_mc(r.v, r.pitch_c, cw, ch, cx, cy, mv.x, mv.y, false, P.rnd);
+        }
+        return;
+    }
+    const int2 a = fmv[pos], b = bmv[pos];
+    int pa[1], pb[1];
+    predict_row<1>(GlobSampler{past.y, past.pitch_y, P.W, P.H}, bil, P.rnd, a.x, a.y, x, y, pa);
+    predict_row<1>(GlobSampler{fut.y, fut.pitch_y, P.W, P.H}, bil, P.rnd, b.x, b.y, x, y, pb);
+    dy[(size_t)y * pitch_y + x] = (uint8_t)((pa[0] + pb[0] + 1) >> 1);
+    if (chroma) {
+        const int au = chroma_mc(past.u, past.pitch_c, cw, ch, cx, cy, a.x, a.y, false, P.rnd);
+        const int bu = chroma_mc(fut.u, fut.pitch_c, cw, ch, cx, cy, b.x, b.y, true, P.rnd);
+        const int av = chroma_mc(past.v, past.pitch_c, cw, ch, cx, cy, a.x, a.y, false, P.rnd);
+        const int bv = chroma_mc(fut.v, fut.pitch_c, cw, ch, cx, cy, b.x, b.y, true, P.rnd);
+        du[(size_t)cy * pitch_c + cx] = (uint8_t)((au + bu + 1) >> 1);
+        dv[(size_t)cy * pitch_c + cx] = (uint8_t)((av + bv + 1) >> 1);
+    }
+}
+
+cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
+                        const uint8_t* modes, const int2* fmv, const int2* bmv, int mode, uint8_t* dy, uint8_t* du,
+                        uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
+    b_mc_kernel<<<dim3((unsigned)((P.W + 127) / 128), (unsigned)P.H), 128, 0, s>>>(P, cur, past, fut, modes, fmv, bmv, mode,
+                                                                                  dy, du, dv, pitch_y, pitch_c);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s) {
     const unsigned mbs = (unsigned)(P.mbw * P.mbh);
     b_cost_kernel<<<dim3(mbs, (unsigned)n), 256, 0, s>>>(P, d_descs);

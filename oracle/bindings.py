@@ -78,6 +78,7 @@ class Oracle:
         L.vo_scene_change_score.argtypes = [P, vp, vp, i32, C.c_double]
         L.vo_scene_change_score.restype = C.c_double
         L.vo_zoom_coherent.argtypes = [vp, i32, i32]
+        L.vo_b_predict.argtypes = [P, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -174,6 +175,16 @@ class Oracle:
         self.lib.vo_intensity_compensate(self._f(ref), C.byref(k), oy.ctypes.data, ou.ctypes.data, ov.ctypes.data)
         return oy, ou, ov
 
+    def b_predict(self, p, cur, past, future, b: BAnalysis, mode):
+        h, w = p.height, p.width
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.vo_b_predict(C.byref(p), self._f(cur), self._f(past), self._f(future), b.modes.ctypes.data,
+                              b.forward_mvs.ctypes.data, b.backward_mvs.ctypes.data, mode, y.ctypes.data,
+                              u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
     def analyze_b(self, p, cur, past, future, anchor_mvs, anchor_4mv, num, den, mode):
         mbw, mbh = mbs_of(p)
         out = BAnalysis.empty(mbw * mbh)
@@ -263,6 +274,7 @@ class Reference:
         L.ref_ic_reference.argtypes = [vp, vp, C.POINTER(Intensity), vp]
         L.ref_scene_change_score.argtypes = [vp, vp, vp, i32, C.c_double]
         L.ref_scene_change_score.restype = C.c_double
+        L.ref_b_predict.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -347,6 +359,18 @@ class Reference:
                           np.zeros((h // 2, w // 2), np.uint8)))
         k = Intensity(*ic)
         self.lib.ref_ic_reference(self.h, self._f(ref), C.byref(k), dst.h)
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def b_predict(self, cur, past, future, b: BAnalysis, mode):
+        h, w = self.p.height, self.p.width
+        dst = self.frame((np.zeros((h, w), np.uint8), np.zeros((h // 2, w // 2), np.uint8),
+                          np.zeros((h // 2, w // 2), np.uint8)))
+        self.lib.ref_b_predict(self.h, self._f(cur), self._f(past), self._f(future), b.modes.ctypes.data,
+                               b.forward_mvs.ctypes.data, b.backward_mvs.ctypes.data, mode, dst.h)
         y = np.zeros((h, w), np.uint8)
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)

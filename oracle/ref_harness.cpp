@@ -285,6 +285,47 @@ double ref_scene_change_score(void* h, void* cur, void* ref, int fade_compensati
     return enc.scene_change_score(F(cur), F(ref));
 }
 
+// The B prediction of an analysis (modes, forward/backward MV state) exactly as
+// sampled_b_mode_rd builds it for a macroblock (encoder_motion.cpp:1030-1053), for every MB.
+void ref_b_predict(void* h, void* cur, void* past, void* future, const uint8_t* modes, const vc1cu_mv* fmv,
+                   const vc1cu_mv* bmv, int mode, void* dst) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const Frame& f = F(cur);
+    Frame& pred = *static_cast<Frame*>(dst);
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            const MV fm{fmv[pos].xq, fmv[pos].yq}, bm{bmv[pos].xq, bmv[pos].yq};
+            const auto m = static_cast<Vc1Encoder::BMbMode>(modes[pos]);
+            if (m == Vc1Encoder::BMbMode::Intra) {
+                for (int k = 0; k < 6; ++k) {
+                    const std::vector<uint8_t>* src = nullptr;
+                    std::vector<uint8_t>* d = nullptr;
+                    int sw = 0, sh = 0, dw = 0, dh = 0, bx = 0, by = 0;
+                    if (k < 4) {
+                        src = &f.y; d = &pred.y; sw = c.width; sh = c.height; dw = pred.width; dh = pred.height;
+                        bx = mx * 2 + (k & 1); by = my * 2 + ((k >> 1) & 1);
+                    } else {
+                        src = (k == 4) ? &f.u : &f.v; d = (k == 4) ? &pred.u : &pred.v;
+                        sw = c.width / 2; sh = c.height / 2; dw = pred.width / 2; dh = pred.height / 2; bx = mx; by = my;
+                    }
+                    const int mean = Vc1Encoder::visible_block_mean(*src, sw, sh, bx * 8, by * 8);
+                    for (int yy = 0; yy < 8 && by * 8 + yy < dh; ++yy)
+                        for (int xx = 0; xx < 8 && bx * 8 + xx < dw; ++xx)
+                            (*d)[static_cast<size_t>(by * 8 + yy) * dw + bx * 8 + xx] = static_cast<uint8_t>(mean);
+                }
+            } else if (m == Vc1Encoder::BMbMode::Forward) {
+                e.motion_compensate_mb(pred, F(past), mx, my, fm, to_mode(mode));
+            } else if (m == Vc1Encoder::BMbMode::Backward) {
+                e.motion_compensate_mb(pred, F(future), mx, my, bm, to_mode(mode));
+            } else {
+                e.motion_compensate_bi_mb(pred, F(past), F(future), mx, my, fm, bm, to_mode(mode));
+            }
+        }
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

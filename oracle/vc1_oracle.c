@@ -2297,3 +2297,71 @@ double vo_scene_change_score(const vc1cu_params* p, const vo_frame* f, const vo_
     }
     return best;
 }
+
+/* ---- B-picture prediction ------------------------------------------------------------ */
+
+/* The prediction of a B analysis as sampled_b_mode_rd builds it for every macroblock
+ * (encoder_motion.cpp:1030-1053): Forward from the past reference and Backward from the future
+ * one with motion_compensate_mb (encoder_motion_compensation.cpp:474-525, chroma rounded as
+ * for a P vector), Direct and Interpolated with motion_compensate_bi_mb (:659-711: the rounded
+ * average of both, the future chroma vector rounded away from the even value), and B-intra
+ * macroblocks filled with the visible mean of each source 8x8 block. */
+void vo_b_predict(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future,
+                  const uint8_t* modes, const vc1cu_mv* fmv, const vc1cu_mv* bmv, int mode, uint8_t* dy, uint8_t* du,
+                  uint8_t* dv) {
+    const int W = p->width, H = p->height, mbw = mbw_of(p), mbh = mbh_of(p);
+    const int cw = W / 2, ch = H / 2;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = (size_t)my * mbw + mx;
+            const int m = modes[pos];
+            const int x0 = mx * 16, y0 = my * 16, cx0 = mx * 8, cy0 = my * 8;
+            const int vw = imax(0, imin(16, W - x0)), vh = imax(0, imin(16, H - y0));
+            const int cvw = imax(0, imin(8, cw - cx0)), cvh = imax(0, imin(8, ch - cy0));
+            if (m == VC1CU_BMB_INTRA) {
+                for (int k = 0; k < 6; ++k) {
+                    const uint8_t* src = k < 4 ? f->y : (k == 4 ? f->u : f->v);
+                    uint8_t* dst = k < 4 ? dy : (k == 4 ? du : dv);
+                    const int sw = k < 4 ? W : cw, sh = k < 4 ? H : ch;
+                    const int bx = k < 4 ? mx * 2 + (k & 1) : mx, by = k < 4 ? my * 2 + ((k >> 1) & 1) : my;
+                    const int mean = visible_block_mean(src, sw, sh, bx * 8, by * 8);
+                    for (int yy = 0; yy < 8 && by * 8 + yy < sh; ++yy)
+                        for (int xx = 0; xx < 8 && bx * 8 + xx < sw; ++xx)
+                            dst[(size_t)(by * 8 + yy) * sw + bx * 8 + xx] = (uint8_t)mean;
+                }
+                continue;
+            }
+            if (m == VC1CU_BMB_FORWARD || m == VC1CU_BMB_BACKWARD) {
+                const vo_frame* r = m == VC1CU_BMB_FORWARD ? past : future;
+                const vc1cu_mv mv = m == VC1CU_BMB_FORWARD ? fmv[pos] : bmv[pos];
+                for (int y = 0; y < vh; ++y)
+                    for (int x = 0; x < vw; ++x)
+                        dy[(size_t)(y0 + y) * W + x0 + x] =
+                            (uint8_t)luma_mc_sample_mode(r->y, W, H, x0 + x, y0 + y, mv.xq, mv.yq, mode, p->rnd);
+                for (int y = 0; y < cvh; ++y)
+                    for (int x = 0; x < cvw; ++x) {
+                        const size_t off = (size_t)(cy0 + y) * cw + cx0 + x;
+                        du[off] = (uint8_t)chroma_mc_sample(r->u, cw, ch, cx0 + x, cy0 + y, mv.xq, mv.yq, 0, p->rnd);
+                        dv[off] = (uint8_t)chroma_mc_sample(r->v, cw, ch, cx0 + x, cy0 + y, mv.xq, mv.yq, 0, p->rnd);
+                    }
+                continue;
+            }
+            const vc1cu_mv a = fmv[pos], b = bmv[pos];
+            for (int y = 0; y < vh; ++y)
+                for (int x = 0; x < vw; ++x) {
+                    const int pa = luma_mc_sample_mode(past->y, W, H, x0 + x, y0 + y, a.xq, a.yq, mode, p->rnd);
+                    const int pb = luma_mc_sample_mode(future->y, W, H, x0 + x, y0 + y, b.xq, b.yq, mode, p->rnd);
+                    dy[(size_t)(y0 + y) * W + x0 + x] = (uint8_t)((pa + pb + 1) >> 1);
+                }
+            for (int y = 0; y < cvh; ++y)
+                for (int x = 0; x < cvw; ++x) {
+                    const size_t off = (size_t)(cy0 + y) * cw + cx0 + x;
+                    const int au = chroma_mc_sample(past->u, cw, ch, cx0 + x, cy0 + y, a.xq, a.yq, 0, p->rnd);
+                    const int bu = chroma_mc_sample(future->u, cw, ch, cx0 + x, cy0 + y, b.xq, b.yq, 1, p->rnd);
+                    const int av = chroma_mc_sample(past->v, cw, ch, cx0 + x, cy0 + y, a.xq, a.yq, 0, p->rnd);
+                    const int bv = chroma_mc_sample(future->v, cw, ch, cx0 + x, cy0 + y, b.xq, b.yq, 1, p->rnd);
+                    du[off] = (uint8_t)((au + bu + 1) >> 1);
+                    dv[off] = (uint8_t)((av + bv + 1) >> 1);
+                }
+        }
+}

@@ -87,6 +87,9 @@ double vo_scene_change_score(const vc1cu_params* p, const vo_frame* f, const vo_
 /* B-picture analysis: the two core passes + the per-MB mode decision */
 void vo_b_costs(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future, int mx,
                 int my, vc1cu_mv fm, vc1cu_mv bm, vc1cu_mv df, vc1cu_mv db, int mode, uint64_t out[5]);
+void vo_b_predict(const vc1cu_params* p, const vo_frame* f, const vo_frame* past, const vo_frame* future,
+                  const uint8_t* modes, const vc1cu_mv* fmv, const vc1cu_mv* bmv, int mode, uint8_t* dy, uint8_t* du,
+                  uint8_t* dv);
 int vo_analyze_b(const vc1cu_params* p, const vo_frame* cur, const vo_frame* past, const vo_frame* future,
                  const vc1cu_mv* anchor_mvs, const uint8_t* anchor_4mv, int fraction_num, int fraction_den,
                  int mode, vc1cu_banalysis* out);

@@ -21,7 +21,8 @@ script calls it through oracle.Reference on inputs restated from the reference's
                     local-motion fit rescues, and search range 0
   b_kat.npz         analyze_b_picture_mode (two core passes + the per-MB B mode decision) of a
                     seeded three-picture group, anchor vectors from the future picture's own
-                    Mixed-MV analysis, several fractions, modes and parameter sets
+                    Mixed-MV analysis, several fractions, modes and parameter sets, and the
+                    B prediction of each analysis (motion_compensate_mb / _bi_mb, intra means)
 
 Run it where the reference tree is present (it is not needed to run the tests):
     python tests/golden/make_golden.py            # every fixture
@@ -169,6 +170,8 @@ def make_b_kat():
         R = Reference(p)
         b = R.analyze_b(R.frame(cur), R.frame(past), R.frame(fut), anc.mvs, anc.use_4mv, num, den, mode)
         flatten(f"b{i}", b, d)
+        for c, pl in zip("yuv", R.b_predict(R.frame(cur), R.frame(past), R.frame(fut), b, mode)):
+            d[f"b{i}.pred.{c}"] = pl
     np.savez_compressed(os.path.join(HERE, "b_kat.npz"), **d)
 
 

@@ -135,3 +135,30 @@ def test_b_picture_rejects_bad_arguments(ctx):
     # the context stays usable
     ctx.b_decide(p, [(1, 0, 2, 40, 41, 40, 1, 2, MV_QPEL, 7)])
     assert ctx.read_bresult(p, 7).totals["mv_mode"] == MV_QPEL
+
+
+@pytest.mark.parametrize("i", range(len(B_GOLDEN)))
+def test_b_prediction_matches_reference_fixture(ctx, oracle, i):
+    """The prediction of the reference's own analysis (decided on the device through the batch
+    form, anchor from the fixture), then its transform + quantiser against the oracle's."""
+    g = np.load(os.path.join(GOLDEN, "b_kat.npz"))
+    mode, num, den, kw = B_GOLDEN[i]
+    p = make_params(130, 98, **kw)
+    past, cur, fut = _frames(g, "past"), _frames(g, "cur"), _frames(g, "future")
+    for fid, fr in ((0, past), (1, cur), (2, fut)):
+        ctx.upload_frame(fid, *fr)
+    # the anchor's field: the future picture's own passes on the device equal the fixture's anchor
+    p0 = make_params(130, 98, search_range=16, local_search_range=16)  # the anchor's own configuration
+    ctx.core_passes(p, [(1, 0, mode, 0, -1, 70), (1, 2, mode, 0, -1, 71)])
+    ctx.core_passes(p0, [(2, 0, MV_QPEL, 0, -1, 72)])
+    ctx.core_passes(p0, [(2, 0, MV_MIXED, 1, 72, 73)])
+    anc = ctx.read_result(p0, 73)
+    assert np.array_equal(anc.mvs, g["anchor.mvs"]) and np.array_equal(anc.use_4mv, g["anchor.use_4mv"])
+    ctx.b_decide(p, [(1, 0, 2, 70, 71, 73, num, den, mode, 9)])
+    ctx.b_predict(p, 9, 1, 0, 2, 5)
+    pred = ctx.download_frame(5, 130, 98)
+    for got, c in zip(pred, "yuv"):
+        assert np.array_equal(got, g[f"b{i}.pred.{c}"]), c
+    co, lv = ctx.forward_quant(p, 1, 5, 15)
+    eco, elv = oracle.forward_quant(p, cur, pred, 15)
+    assert np.array_equal(co.view(np.uint64), eco.view(np.uint64)) and np.array_equal(lv, elv)

@@ -183,6 +183,8 @@ def test_b_analysis_golden(oracle, i):
     for k, v in b.totals.items():
         w = g[f"b{i}.total.{k}"]
         assert (np.float64(v).view(np.uint64) == w.view(np.uint64)) if w.dtype == np.float64 else int(v) == int(w), k
+    for got, c in zip(oracle.b_predict(p, cur, past, fut, b, mode), "yuv"):
+        assert np.array_equal(got, g[f"b{i}.pred.{c}"]), c
     # every decision kind the fixture set is meant to cover
     if i == 0:
         modes = set(np.concatenate([g[f"b{j}.modes"] for j in range(len(B_CASES))]).tolist())
