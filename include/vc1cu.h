@@ -435,6 +435,19 @@ int vc1cu_forward_quant(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int p
 int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id,
                                int type_mask, double* d_coeffs, int16_t* d_levels);
 
+/*
+ * The reconstruction a transform decision implies (evaluate_transform_parent,
+ * src/encoder_transform.cpp:1569-1585): for every MB and parent block (Y0..Y3, U, V), the levels
+ * of its chosen type dequantised (dequant_level at PQINDEX, :1058-1065), inverse-transformed
+ * (inverse_partition with its DC-only shortcuts, :1173-1274, the VC-1 inverse transforms) and
+ * added to frame slot pred_id with 8-bit clamping, into frame slot out_id. d_levels: DEVICE
+ * levels in vc1cu_forward_quant_device's layout for type_mask; block_types: HOST array of
+ * mbw*mbh*6 TransformType codes (1 = 8x8, 2 = 8x4, 3 = 4x8, 4 = 4x4), each one of type_mask's
+ * (the type decision itself, choose_transform_mb, stays with the caller). Asynchronous.
+ */
+int vc1cu_reconstruct(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
+                      const uint8_t* block_types, int out_id);
+
 /* ---- allocation-free whole-frame translation search ------------------------------ */
 
 /*

@@ -35,7 +35,7 @@ EXPORTS = (
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
-    "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict",
+    "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
 )
 
 
@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_estimate_intensity_batch.argtypes = [vp, PP, C.POINTER(IcPass), i32, C.POINTER(Intensity)]
     L.vc1cu_intensity_compensate.argtypes = [vp, i32, C.POINTER(Intensity), i32]
     L.vc1cu_b_predict.argtypes = [vp, PP, i32, i32, i32, i32, i32]
+    L.vc1cu_reconstruct.argtypes = [vp, PP, i32, vp, i32, vp, i32]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
@@ -331,6 +332,13 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_forward_quant(self._h, C.byref(params), src_id, pred_id, type_mask,
                                                 co.ctypes.data, lv.ctypes.data))
         return co, lv
+
+    def reconstruct(self, params: Params, pred_id: int, d_levels: int, type_mask: int, block_types, out_id: int):
+        """Frame slot out_id = pred_id + the inverse-transformed levels of each block's type
+        (device levels in forward_quant_device's layout; block_types: (mbs, 6) TransformType codes)."""
+        bt = np.ascontiguousarray(block_types, np.uint8)
+        self._check(self._L.vc1cu_reconstruct(self._h, C.byref(params), pred_id, d_levels, type_mask, bt.ctypes.data,
+                                              out_id))
 
     def forward_quant_device(self, params: Params, src_id: int, pred_id: int, type_mask: int, d_coeffs: int,
                              d_levels: int):

@@ -45,6 +45,8 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
+void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
+                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
 cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
                         const uint8_t* modes, const int2* fmv, const int2* bmv, int mode, uint8_t* dy, uint8_t* du,
                         uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
@@ -174,6 +176,8 @@ struct vc1cu_ctx {
     int passes_cap = 0;
     BDesc* d_bdescs = nullptr;
     int bdescs_cap = 0;
+    void* d_btypes = nullptr;  // per-block transform types of vc1cu_reconstruct
+    size_t btypes_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -939,6 +943,7 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
     if (c->bdescs_cap < n) {
         if (c->d_bdescs) cudaFree(c->d_bdescs);
     if (c->d_ic) cudaFree(c->d_ic);
+    if (c->d_btypes) cudaFree(c->d_btypes);
     if (c->d_icdesc) cudaFree(c->d_icdesc);
         c->d_bdescs = nullptr;
         c->bdescs_cap = 0;
@@ -1662,6 +1667,40 @@ int vc1cu_motion_compensate(vc1cu_ctx* c, const vc1cu_params* p, int ref_id, int
         launch_mc(P, ref, s.r.mvs, s.r.bmv, s.r.use4, mv_mode, (uint8_t*)pd.y, (uint8_t*)pd.u, (uint8_t*)pd.v, fp.pitch_y,
                   fp.pitch_c, c->stream);
         ck(cudaGetLastError(), "mc_kernel launch");
+        tm.stop(1);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_reconstruct(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
+                      const uint8_t* block_types, int out_id) {
+    return guarded(c, [&]() -> int {
+        if (!d_levels || !block_types) throw Fail{VC1CU_ERR_ARG, "null levels or block types"};
+        if (type_mask < 1 || type_mask > 15) throw Fail{VC1CU_ERR_ARG, "type_mask must select 1..4 transform types"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const int mbs = P.mbw * P.mbh;
+        for (int i = 0; i < mbs * 6; ++i) {
+            const int t = block_types[i];
+            if (t < 1 || t > 4 || !(type_mask & (1 << (t - 1))))
+                throw Fail{VC1CU_ERR_ARG, "a block's transform type is not one of type_mask's"};
+        }
+        if (out_id < 0 || out_id >= kMaxSlot || out_id == pred_id) throw Fail{VC1CU_ERR_ARG, "invalid output frame slot"};
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fp.w != P.W || fp.h != P.H) throw Fail{VC1CU_ERR_ARG, "prediction size does not match the configuration"};
+        const DevFrame pred = fp.view();
+        FrameSlot& fo = alloc_frame(c, out_id, P.W, P.H);
+        const DevFrame o = fo.view();
+        uint8_t* dt = static_cast<uint8_t*>(ensure(c->d_btypes, c->btypes_cap, (size_t)mbs * 6, "cudaMalloc(block types)"));
+        ck(cudaMemcpyAsync(dt, block_types, (size_t)mbs * 6, cudaMemcpyHostToDevice, c->stream), "upload block types");
+        int ti[4], n = 0;
+        for (int t = 0; t < 4; ++t) ti[t] = (type_mask >> t) & 1 ? n++ : -1;
+        Timer tm(c, kXform);
+        launch_recon(P, pred, d_levels, make_int4(ti[0], ti[1], ti[2], ti[3]), dt, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v,
+                     fo.pitch_y, fo.pitch_c, c->stream);
+        ck(cudaGetLastError(), "reconstruction launch");
         tm.stop(1);
         return VC1CU_OK;
     });

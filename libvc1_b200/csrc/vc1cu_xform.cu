@@ -180,6 +180,122 @@ __global__ void xform_kernel(const __grid_constant__ DevParams P, DevFrame src, 
         }
 }
 
+// ---- inverse transform and reconstruction (encoder_transform.cpp:1058-1274, :1569-1585) ----
+
+// Vc1Encoder::dequant_level at mquant = PQINDEX without DQUANT (2*PQ + HALFQP, plus PQ away from
+// zero for the non-uniform quantiser)
+__device__ __forceinline__ int dequant(const DevParams& P, int level) {
+    if (!level) return 0;
+    const int v = level * (2 * P.pq + (P.halfqp ? 1 : 0));
+    return P.nonuniform ? v + (level > 0 ? P.pq : -P.pq) : v;
+}
+
+// The VC-1 8-point inverse butterfly (inverse_transform_8x8, :566-609); tail adds the second
+// stage's +1 to the lower four outputs.
+__device__ __forceinline__ void inv8(const int* s, int st, int* o, int ot, int bias, int shift, int tail) {
+    int t1 = 12 * (s[0] + s[4 * st]) + bias, t2 = 12 * (s[0] - s[4 * st]) + bias;
+    int t3 = 16 * s[2 * st] + 6 * s[6 * st], t4 = 6 * s[2 * st] - 16 * s[6 * st];
+    const int t5 = t1 + t3, t6 = t2 + t4, t7 = t2 - t4, t8 = t1 - t3;
+    t1 = 16 * s[st] + 15 * s[3 * st] + 9 * s[5 * st] + 4 * s[7 * st];
+    t2 = 15 * s[st] - 4 * s[3 * st] - 16 * s[5 * st] - 9 * s[7 * st];
+    t3 = 9 * s[st] - 16 * s[3 * st] + 4 * s[5 * st] + 15 * s[7 * st];
+    t4 = 4 * s[st] - 9 * s[3 * st] + 15 * s[5 * st] - 16 * s[7 * st];
+    o[0] = arshift(t5 + t1, shift);
+    o[ot] = arshift(t6 + t2, shift);
+    o[2 * ot] = arshift(t7 + t3, shift);
+    o[3 * ot] = arshift(t8 + t4, shift);
+    o[4 * ot] = arshift(t8 - t4 + tail, shift);
+    o[5 * ot] = arshift(t7 - t3 + tail, shift);
+    o[6 * ot] = arshift(t6 - t2 + tail, shift);
+    o[7 * ot] = arshift(t5 - t1 + tail, shift);
+}
+// The 4-point one of the 8x4 / 4x8 / 4x4 partitions (inverse_partition, :1213-1272)
+__device__ __forceinline__ void inv4(const int* s, int st, int* o, int ot, int bias, int shift) {
+    const int t1 = 17 * (s[0] + s[2 * st]) + bias, t2 = 17 * (s[0] - s[2 * st]) + bias;
+    const int t3 = 22 * s[st] + 10 * s[3 * st], t4 = 22 * s[3 * st] - 10 * s[st];
+    o[0] = arshift(t1 + t3, shift);
+    o[ot] = arshift(t2 - t4, shift);
+    o[2 * ot] = arshift(t2 + t4, shift);
+    o[3 * ot] = arshift(t1 - t3, shift);
+}
+
+// One thread per (MB, parent): every partition of the block's chosen type dequantised,
+// inverse-transformed (with the DC-only shortcut of a partition whose only level is its DC)
+// and added to the prediction with 8-bit clamping. tindex[t] is type t's index in the levels
+// layout [type][mb][parent][64] (-1 for a type the layout does not hold).
+__global__ void recon_kernel(const __grid_constant__ DevParams P, DevFrame pred, const int16_t* levels, int4 tindex,
+                             const uint8_t* block_types, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c) {
+    const int mbs = P.mbw * P.mbh;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= mbs * 6) return;
+    const int mb = idx / 6, k = idx - mb * 6, mx = mb % P.mbw, my = mb / P.mbw;
+    const int t = block_types[idx];
+    const int ti = t == 1 ? tindex.x : (t == 2 ? tindex.y : (t == 3 ? tindex.z : tindex.w));
+    const int16_t* q64 = levels + (((size_t)ti * mbs + mb) * 6 + k) * 64;
+    int res[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) res[i] = 0;
+    const int np = t == 1 ? 1 : (t == 4 ? 4 : 2);
+    for (int part = 0; part < np; ++part) {
+        int ox = 0, oy = 0, bw = 8, bh = 8;
+        if (t == 2) { bh = 4; oy = part * 4; }
+        else if (t == 3) { bw = 4; ox = part * 4; }
+        else if (t == 4) { bw = bh = 4; ox = (part & 1) * 4; oy = (part >> 1) * 4; }
+        int a[64], tmp[64];
+        int nonzero = 0, q0 = 0;
+        for (int y = 0; y < 8; ++y)
+            for (int x = 0; x < 8; ++x) {
+                const int lv = (y < bh && x < bw) ? q64[(oy + y) * 8 + ox + x] : 0;
+                nonzero += lv != 0;
+                if (!y && !x) q0 = lv;
+                a[y * 8 + x] = dequant(P, lv);
+                tmp[y * 8 + x] = 0;
+            }
+        if (nonzero == 1 && q0 != 0) {
+            int dc = a[0];
+            if (t == 1) { dc = arshift(3 * dc + 1, 1); dc = arshift(3 * dc + 16, 5); }
+            else if (t == 2) { dc = arshift(3 * dc + 1, 1); dc = arshift(17 * dc + 64, 7); }
+            else if (t == 3) { dc = arshift(17 * dc + 4, 3); dc = arshift(12 * dc + 64, 7); }
+            else { dc = arshift(17 * dc + 4, 3); dc = arshift(17 * dc + 64, 7); }
+            for (int y = 0; y < bh; ++y)
+                for (int x = 0; x < bw; ++x) res[(oy + y) * 8 + ox + x] = dc;
+            continue;
+        }
+        if (t == 1) {
+            for (int col = 0; col < 8; ++col) inv8(a + col, 8, tmp + col * 8, 1, 4, 3, 0);
+            for (int col = 0; col < 8; ++col) inv8(tmp + col, 8, a + col, 8, 64, 7, 1);
+        } else if (t == 2) {
+            for (int y = 0; y < 4; ++y) inv8(a + y * 8, 1, tmp + y * 8, 1, 4, 3, 0);
+            for (int x = 0; x < 8; ++x) inv4(tmp + x, 8, a + x, 8, 64, 7);
+        } else if (t == 3) {
+            for (int y = 0; y < 8; ++y) inv4(a + y * 8, 1, tmp + y * 8, 1, 4, 3);
+            for (int x = 0; x < 4; ++x) inv8(tmp + x, 8, a + x, 8, 64, 7, 1);
+        } else {
+            for (int y = 0; y < 4; ++y) inv4(a + y * 8, 1, tmp + y * 8, 1, 4, 3);
+            for (int x = 0; x < 4; ++x) inv4(tmp + x, 8, a + x, 8, 64, 7);
+        }
+        for (int y = 0; y < bh; ++y)
+            for (int x = 0; x < bw; ++x) res[(oy + y) * 8 + ox + x] = a[y * 8 + x];
+    }
+    const bool luma = k < 4;
+    const int w = luma ? P.W : P.W / 2, h = luma ? P.H : P.H / 2;
+    const int bx = luma ? mx * 2 + (k & 1) : mx, by = luma ? my * 2 + ((k >> 1) & 1) : my;
+    const uint8_t* pp = luma ? pred.y : (k == 4 ? pred.u : pred.v);
+    uint8_t* dp = luma ? dy : (k == 4 ? du : dv);
+    const int pps = luma ? pred.pitch_y : pred.pitch_c, dps = luma ? pitch_y : pitch_c;
+    for (int y = 0; y < 8 && by * 8 + y < h; ++y)
+        for (int x = 0; x < 8 && bx * 8 + x < w; ++x) {
+            const int v = pp[(size_t)(by * 8 + y) * pps + bx * 8 + x] + res[y * 8 + x];
+            dp[(size_t)(by * 8 + y) * dps + bx * 8 + x] = (uint8_t)iclamp(v, 0, 255);
+        }
+}
+
+void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
+                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
+    const int n = P.mbw * P.mbh * 6;
+    recon_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, pred, levels, tindex, block_types, dy, du, dv, pitch_y, pitch_c);
+}
+
 void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
                uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
     dim3 grid((P.W + 127) / 128, P.H);

@@ -79,6 +79,7 @@ class Oracle:
         L.vo_scene_change_score.restype = C.c_double
         L.vo_zoom_coherent.argtypes = [vp, i32, i32]
         L.vo_b_predict.argtypes = [P, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp]
+        L.vo_reconstruct.argtypes = [P, vp, vp, i32, vp, vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -174,6 +175,17 @@ class Oracle:
         oy, ou, ov = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
         self.lib.vo_intensity_compensate(self._f(ref), C.byref(k), oy.ctypes.data, ou.ctypes.data, ov.ctypes.data)
         return oy, ou, ov
+
+    def reconstruct(self, p, pred, levels, type_mask, block_types):
+        h, w = p.height, p.width
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        lv = np.ascontiguousarray(levels, np.int16)
+        bt = np.ascontiguousarray(block_types, np.uint8)
+        self.lib.vo_reconstruct(C.byref(p), self._f(pred), lv.ctypes.data, type_mask, bt.ctypes.data, y.ctypes.data,
+                                u.ctypes.data, v.ctypes.data)
+        return y, u, v
 
     def b_predict(self, p, cur, past, future, b: BAnalysis, mode):
         h, w = p.height, p.width
@@ -275,6 +287,7 @@ class Reference:
         L.ref_scene_change_score.argtypes = [vp, vp, vp, i32, C.c_double]
         L.ref_scene_change_score.restype = C.c_double
         L.ref_b_predict.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, vp]
+        L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -359,6 +372,19 @@ class Reference:
                           np.zeros((h // 2, w // 2), np.uint8)))
         k = Intensity(*ic)
         self.lib.ref_ic_reference(self.h, self._f(ref), C.byref(k), dst.h)
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def reconstruct(self, pred, levels, type_mask, block_types):
+        h, w = self.p.height, self.p.width
+        dst = self.frame((np.zeros((h, w), np.uint8), np.zeros((h // 2, w // 2), np.uint8),
+                          np.zeros((h // 2, w // 2), np.uint8)))
+        lv = np.ascontiguousarray(levels, np.int16)
+        bt = np.ascontiguousarray(block_types, np.uint8)
+        self.lib.ref_reconstruct(self.h, self._f(pred), lv.ctypes.data, type_mask, bt.ctypes.data, dst.h)
         y = np.zeros((h, w), np.uint8)
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)

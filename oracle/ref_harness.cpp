@@ -326,6 +326,49 @@ void ref_b_predict(void* h, void* cur, void* past, void* future, const uint8_t* 
         }
 }
 
+// Reconstruction of each (MB, parent) with its chosen transform type as
+// evaluate_transform_parent forms it (encoder_transform.cpp:1569-1585): inverse_partition of
+// every partition's levels (layout of ref_forward_quant for type_mask) added to the prediction.
+void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, const uint8_t* block_types, void* dst) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const size_t mbs = static_cast<size_t>(mbw) * mbh;
+    int tindex[5] = {-1, -1, -1, -1, -1}, nt = 0;
+    for (int t = 1; t <= 4; ++t)
+        if (type_mask & (1 << (t - 1))) tindex[t] = nt++;
+    const Frame& pf = F(pred);
+    Frame& out = *static_cast<Frame*>(dst);
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx)
+            for (int k = 0; k < 6; ++k) {
+                const size_t mb = static_cast<size_t>(my) * mbw + mx;
+                const int t = block_types[mb * 6 + k];
+                const auto type = static_cast<Vc1Encoder::TransformType>(t);
+                const int16_t* q64 = levels + ((static_cast<size_t>(tindex[t]) * mbs + mb) * 6 + k) * 64;
+                const std::vector<uint8_t>& pp = k < 4 ? pf.y : (k == 4 ? pf.u : pf.v);
+                std::vector<uint8_t>& dp = k < 4 ? out.y : (k == 4 ? out.u : out.v);
+                const int w = k < 4 ? c.width : c.width / 2, hh = k < 4 ? c.height : c.height / 2;
+                const int bx = k < 4 ? mx * 2 + (k & 1) : mx, by = k < 4 ? my * 2 + ((k >> 1) & 1) : my;
+                std::array<int, 64> residual{};
+                for (int part = 0; part < Vc1Encoder::transform_part_count(type); ++part) {
+                    int ox, oy, bw, bh;
+                    Vc1Encoder::transform_part_geometry(type, part, ox, oy, bw, bh);
+                    std::array<int, 64> q{};
+                    for (int y = 0; y < bh; ++y)
+                        for (int x = 0; x < bw; ++x) q[y * 8 + x] = q64[(oy + y) * 8 + ox + x];
+                    const auto r = e.inverse_partition(type, q, c.pqindex, false);
+                    for (int y = 0; y < bh; ++y)
+                        for (int x = 0; x < bw; ++x) residual[(oy + y) * 8 + ox + x] = r[y * 8 + x];
+                }
+                for (int yy = 0; yy < 8 && by * 8 + yy < hh; ++yy)
+                    for (int xx = 0; xx < 8 && bx * 8 + xx < w; ++xx) {
+                        const size_t off = static_cast<size_t>(by * 8 + yy) * w + bx * 8 + xx;
+                        dp[off] = static_cast<uint8_t>(std::clamp(static_cast<int>(pp[off]) + residual[yy * 8 + xx], 0, 255));
+                    }
+            }
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

@@ -2365,3 +2365,123 @@ void vo_b_predict(const vc1cu_params* p, const vo_frame* f, const vo_frame* past
                 }
         }
 }
+
+/* ---- inverse transform and reconstruction ------------------------------------------- */
+
+/* Vc1Encoder::dequant_level, encoder_transform.cpp:1058-1065, at mquant = PQINDEX without
+ * DQUANT (picture_double_quant :1052-1056: 2*PQ + HALFQP) */
+static int dequant_level(const vc1cu_params* p, int level) {
+    if (!level) return 0;
+    long v = (long)level * (2 * p->pqindex + (p->halfqp ? 1 : 0));
+    if (p->nonuniform) v += level > 0 ? p->pqindex : -p->pqindex;
+    return (int)v;
+}
+
+/* The VC-1 8-point inverse butterfly of inverse_transform_8x8 (encoder_transform.cpp:566-609):
+ * s[k*st] are the 8 inputs, bias and shift the stage's rounding; out[k*ot] the outputs; tail
+ * adds the second stage's +1 to the lower half. */
+static void inv8(const int* s, int st, int* o, int ot, int bias, int shift, int tail) {
+    int t1 = 12 * (s[0] + s[4 * st]) + bias, t2 = 12 * (s[0] - s[4 * st]) + bias;
+    int t3 = 16 * s[2 * st] + 6 * s[6 * st], t4 = 6 * s[2 * st] - 16 * s[6 * st];
+    const int t5 = t1 + t3, t6 = t2 + t4, t7 = t2 - t4, t8 = t1 - t3;
+    t1 = 16 * s[st] + 15 * s[3 * st] + 9 * s[5 * st] + 4 * s[7 * st];
+    t2 = 15 * s[st] - 4 * s[3 * st] - 16 * s[5 * st] - 9 * s[7 * st];
+    t3 = 9 * s[st] - 16 * s[3 * st] + 4 * s[5 * st] + 15 * s[7 * st];
+    t4 = 4 * s[st] - 9 * s[3 * st] + 15 * s[5 * st] - 16 * s[7 * st];
+    o[0] = arshift(t5 + t1, shift); o[ot] = arshift(t6 + t2, shift);
+    o[2 * ot] = arshift(t7 + t3, shift); o[3 * ot] = arshift(t8 + t4, shift);
+    o[4 * ot] = arshift(t8 - t4 + tail, shift); o[5 * ot] = arshift(t7 - t3 + tail, shift);
+    o[6 * ot] = arshift(t6 - t2 + tail, shift); o[7 * ot] = arshift(t5 - t1 + tail, shift);
+}
+/* The 4-point one (inverse_partition's 8x4 / 4x8 / 4x4 stages, :1213-1272) */
+static void inv4(const int* s, int st, int* o, int ot, int bias, int shift) {
+    const int t1 = 17 * (s[0] + s[2 * st]) + bias, t2 = 17 * (s[0] - s[2 * st]) + bias;
+    const int t3 = 22 * s[st] + 10 * s[3 * st], t4 = 22 * s[3 * st] - 10 * s[st];
+    o[0] = arshift(t1 + t3, shift); o[ot] = arshift(t2 - t4, shift);
+    o[2 * ot] = arshift(t2 + t4, shift); o[3 * ot] = arshift(t1 - t3, shift);
+}
+
+/* Vc1Encoder::inverse_partition, encoder_transform.cpp:1173-1274: dequantisation, the DC-only
+ * shortcut of a partition whose only coefficient is its DC, then the type's inverse transform;
+ * q and a are partition-local (row-major, stride 8). */
+static void inverse_partition(const vc1cu_params* p, int t, const int q[64], int a[64]) {
+    int ox, oy, bw, bh;
+    part_geometry(t, 0, &ox, &oy, &bw, &bh);
+    int nonzero = 0;
+    memset(a, 0, 64 * sizeof(int));
+    for (int y = 0; y < bh; ++y)
+        for (int x = 0; x < bw; ++x) {
+            if (q[y * 8 + x]) ++nonzero;
+            a[y * 8 + x] = dequant_level(p, q[y * 8 + x]);
+        }
+    if (nonzero == 1 && q[0] != 0) {
+        int dc = a[0];
+        if (t == 1) { dc = arshift(3 * dc + 1, 1); dc = arshift(3 * dc + 16, 5); }
+        else if (t == 2) { dc = arshift(3 * dc + 1, 1); dc = arshift(17 * dc + 64, 7); }
+        else if (t == 3) { dc = arshift(17 * dc + 4, 3); dc = arshift(12 * dc + 64, 7); }
+        else { dc = arshift(17 * dc + 4, 3); dc = arshift(17 * dc + 64, 7); }
+        memset(a, 0, 64 * sizeof(int));
+        for (int y = 0; y < bh; ++y)
+            for (int x = 0; x < bw; ++x) a[y * 8 + x] = dc;
+        return;
+    }
+    int tmp[64];
+    memset(tmp, 0, sizeof tmp);
+    if (t == 1) {
+        /* columns first into rows of tmp, then columns of tmp (inverse_transform_8x8) */
+        for (int col = 0; col < 8; ++col) inv8(a + col, 8, tmp + col * 8, 1, 4, 3, 0);
+        for (int col = 0; col < 8; ++col) inv8(tmp + col, 8, a + col, 8, 64, 7, 1);
+    } else if (t == 2) {
+        for (int y = 0; y < 4; ++y) inv8(a + y * 8, 1, tmp + y * 8, 1, 4, 3, 0);
+        for (int x = 0; x < 8; ++x) inv4(tmp + x, 8, a + x, 8, 64, 7);
+    } else if (t == 3) {
+        for (int y = 0; y < 8; ++y) inv4(a + y * 8, 1, tmp + y * 8, 1, 4, 3);
+        for (int x = 0; x < 4; ++x) inv8(tmp + x, 8, a + x, 8, 64, 7, 1);
+    } else {
+        for (int y = 0; y < 4; ++y) inv4(a + y * 8, 1, tmp + y * 8, 1, 4, 3);
+        for (int x = 0; x < 4; ++x) inv4(tmp + x, 8, a + x, 8, 64, 7);
+    }
+}
+
+/* The reconstruction of evaluate_transform_parent, encoder_transform.cpp:1569-1585: every
+ * partition of the chosen type inverse-transformed and added to the prediction, clamped to 8
+ * bits. levels: vo_forward_quant's layout for type_mask; block_types: the TransformType (1..4)
+ * of each (MB, parent). Pixels of MBs outside the raster are untouched. */
+void vo_reconstruct(const vc1cu_params* p, const vo_frame* pred, const int16_t* levels, int type_mask,
+                    const uint8_t* block_types, uint8_t* y, uint8_t* u, uint8_t* v) {
+    const int mbw = mbw_of(p), mbh = mbh_of(p);
+    const size_t mbs = (size_t)mbw * mbh;
+    int tindex[5] = {-1, -1, -1, -1, -1}, nt = 0;
+    for (int t = 1; t <= 4; ++t)
+        if (type_mask & (1 << (t - 1))) tindex[t] = nt++;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx)
+            for (int k = 0; k < 6; ++k) {
+                const size_t mb = (size_t)my * mbw + mx;
+                const int t = block_types[mb * 6 + k];
+                const int16_t* q64 = levels + (((size_t)tindex[t] * mbs + mb) * 6 + k) * 64;
+                const uint8_t* pp = k < 4 ? pred->y : (k == 4 ? pred->u : pred->v);
+                uint8_t* dp = k < 4 ? y : (k == 4 ? u : v);
+                const int w = k < 4 ? p->width : p->width / 2, h = k < 4 ? p->height : p->height / 2;
+                const int bx = k < 4 ? mx * 2 + (k & 1) : mx, by = k < 4 ? my * 2 + ((k >> 1) & 1) : my;
+                int residual[64];
+                memset(residual, 0, sizeof residual);
+                const int np = t == 1 ? 1 : (t == 4 ? 4 : 2);
+                for (int part = 0; part < np; ++part) {
+                    int ox, oy, bw, bh;
+                    part_geometry(t, part, &ox, &oy, &bw, &bh);
+                    int q[64], r[64];
+                    memset(q, 0, sizeof q);
+                    for (int yy = 0; yy < bh; ++yy)
+                        for (int xx = 0; xx < bw; ++xx) q[yy * 8 + xx] = q64[(oy + yy) * 8 + ox + xx];
+                    inverse_partition(p, t, q, r);
+                    for (int yy = 0; yy < bh; ++yy)
+                        for (int xx = 0; xx < bw; ++xx) residual[(oy + yy) * 8 + ox + xx] = r[yy * 8 + xx];
+                }
+                for (int yy = 0; yy < 8 && by * 8 + yy < h; ++yy)
+                    for (int xx = 0; xx < 8 && bx * 8 + xx < w; ++xx) {
+                        const size_t off = (size_t)(by * 8 + yy) * w + bx * 8 + xx;
+                        dp[off] = (uint8_t)iclamp(pp[off] + residual[yy * 8 + xx], 0, 255);
+                    }
+            }
+}

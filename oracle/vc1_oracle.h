@@ -106,6 +106,10 @@ int vo_quantize_level(const vc1cu_params* p, double coeff);
 void vo_forward_quant(const vc1cu_params* p, const vo_frame* src, const vo_frame* pred, int type_mask,
                       double* coeffs, int16_t* levels);
 
+/* reconstruction: prediction + inverse-transformed dequantised levels of each block's type */
+void vo_reconstruct(const vc1cu_params* p, const vo_frame* pred, const int16_t* levels, int type_mask,
+                    const uint8_t* block_types, uint8_t* y, uint8_t* u, uint8_t* v);
+
 /* x87 extended-precision score emulation used by the GPU path, exposed for checking:
  * the long double value of sad + lambda*rate, as an integer scaled by 2^shift
  * (see vo_score_key in vc1_oracle.c). */

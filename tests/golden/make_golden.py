@@ -16,6 +16,9 @@ script calls it through oracle.Reference on inputs restated from the reference's
   ic_kat.npz        estimate_intensity_comp along each picture's quarter-pel field on seeded
                     synthetic fades, and (small pictures) intensity_compensated_reference with
                     the estimate and fixed LUMSCALE/LUMSHIFT codes covering the LUMSCALE 0 law
+  recon_kat.npz     the reconstruction of xform_kat's pictures (levels of all four types, a
+                    seeded transform type per block) and of seeded random levels, through the
+                    reference's inverse_partition
   scene_kat.npz     scene_change_score on seeded pictures: motion, a cut (two thresholds),
                     a fade with and without fade compensation, two camera zooms that the
                     local-motion fit rescues, and search range 0
@@ -212,6 +215,29 @@ def make_ic_kat():
     np.savez_compressed(os.path.join(HERE, "ic_kat.npz"), **d)
 
 
+def make_recon_kat():
+    from oracle import Oracle, Reference
+
+    g = np.load(os.path.join(HERE, "xform_kat.npz"))
+    cur = tuple(np.ascontiguousarray(g[f"cur.{c}"]) for c in "yuv")
+    d = {}
+    for pq, nu, hq in ((3, 0, 1), (8, 1, 1), (17, 1, 0), (31, 0, 0)):
+        key = f"pq{pq}_nu{nu}_hq{hq}"
+        p = make_params(64, 48, pqindex=pq, nonuniform=nu, halfqp=hq, search_range=8, local_search_range=8)
+        R = Reference(p)
+        pred = tuple(np.ascontiguousarray(g[f"{key}.pred.{c}"]) for c in "yuv")
+        _co, lv = Oracle().forward_quant(p, cur, pred, 15)
+        rng = np.random.default_rng(pq)
+        types = rng.integers(1, 5, (lv.shape[1], 6)).astype(np.uint8)
+        rand = (rng.integers(-60, 61, lv.shape) * (rng.random(lv.shape) < 0.1)).astype(np.int16)
+        rand[..., 0] = rng.integers(-400, 401, rand.shape[:-1])
+        d[f"{key}.types"], d[f"{key}.random_levels"] = types, rand
+        for name, levels in (("coded", lv), ("random", rand)):
+            for c, pl in zip("yuv", R.reconstruct(R.frame(pred), levels, 15, types)):
+                d[f"{key}.{name}.{c}"] = pl
+    np.savez_compressed(os.path.join(HERE, "recon_kat.npz"), **d)
+
+
 def make_scene_kat():
     from oracle import Reference
 
@@ -229,7 +255,8 @@ def make_scene_kat():
 def main(only=()):
     if only:
         for name in only:
-            {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat}[name]()
+            {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat,
+             "recon_kat": make_recon_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -348,6 +375,7 @@ def main(only=()):
     make_b_kat()
     make_ic_kat()
     make_scene_kat()
+    make_recon_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

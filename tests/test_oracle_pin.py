@@ -355,3 +355,37 @@ def test_scene_score_matches_reference_live(oracle, case):
     R = Reference(p)
     assert oracle.scene_change_score(p, cur, clip.frame(0), fade, thr) == \
         R.scene_change_score(R.frame(cur), R.frame(clip.frame(0)), fade, thr)
+
+
+# ---- reconstruction (inverse_partition + add, evaluate_transform_parent) ----
+
+RECON_QP = ((3, 0, 1), (8, 1, 1), (17, 1, 0), (31, 0, 0))
+
+
+@pytest.mark.parametrize("qp", RECON_QP)
+def test_reconstruction_golden(oracle, qp):
+    pq, nu, hq = qp
+    key = f"pq{pq}_nu{nu}_hq{hq}"
+    g, x = load("recon_kat.npz"), load("xform_kat.npz")
+    p = make_params(64, 48, pqindex=pq, nonuniform=nu, halfqp=hq, search_range=8, local_search_range=8)
+    cur, pred = _frames(x, "cur"), _frames(x, f"{key}.pred")
+    _co, lv = oracle.forward_quant(p, cur, pred, 15)
+    for name, levels in (("coded", lv), ("random", g[f"{key}.random_levels"])):
+        for got, c in zip(oracle.reconstruct(p, pred, levels, 15, g[f"{key}.types"]), "yuv"):
+            assert np.array_equal(got, g[f"{key}.{name}.{c}"]), (name, c)
+
+
+@pytest.mark.parametrize("tm", [1, 2, 4, 8, 6])
+def test_reconstruction_matches_reference_live(oracle, tm):
+    Reference = _ref_or_skip()
+    clip = synth.generate(98, 66, 2, 40 + tm)
+    p = make_params(98, 66, search_range=8, local_search_range=8, pqindex=6, nonuniform=1, halfqp=1)
+    R = Reference(p)
+    cur, ref = clip.frame(1), clip.frame(0)
+    q = oracle.analyze_p_core(p, cur, ref, MV_QPEL, False)
+    pred = oracle.motion_compensate(p, ref, q, MV_QPEL)
+    _co, lv = oracle.forward_quant(p, cur, pred, tm)
+    rng = np.random.default_rng(tm)
+    types = rng.choice([t for t in range(1, 5) if tm & (1 << (t - 1))], (lv.shape[1], 6)).astype(np.uint8)
+    for x, y in zip(oracle.reconstruct(p, pred, lv, tm, types), R.reconstruct(R.frame(pred), lv, tm, types)):
+        assert np.array_equal(x, y)
