@@ -448,6 +448,20 @@ int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id
 int vc1cu_reconstruct(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
                       const uint8_t* block_types, int out_id);
 
+/*
+ * In-loop deblocking of frame slot frame_id in place, at params->pqindex.
+ * vc1cu_loop_filter_i: Vc1Encoder::apply_i_like_loop_filter (src/encoder_filter.cpp:426-441),
+ * every 8-pixel block edge. vc1cu_loop_filter_p: the Advanced Profile apply_p_loop_filter
+ * (:610-738) of a coded P picture, HOST arrays per macroblock: block_mvs (4 luma block vectors),
+ * cbp (6 loop_filter_pattern codes, 4 bits each), tt (6 loop_filter_tt codes: 0, 3, 6, 7) and
+ * intra (bit k set when block k is intra). The device result equals the reference's raster
+ * order. vc1cu_loop_filter_i is asynchronous; vc1cu_loop_filter_p returns once its metadata
+ * copies are done.
+ */
+int vc1cu_loop_filter_i(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id);
+int vc1cu_loop_filter_p(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
+                        const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
+
 /* ---- allocation-free whole-frame translation search ------------------------------ */
 
 /*

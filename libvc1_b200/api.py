@@ -36,6 +36,7 @@ EXPORTS = (
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
+    "vc1cu_loop_filter_i", "vc1cu_loop_filter_p",
 )
 
 
@@ -89,6 +90,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_intensity_compensate.argtypes = [vp, i32, C.POINTER(Intensity), i32]
     L.vc1cu_b_predict.argtypes = [vp, PP, i32, i32, i32, i32, i32]
     L.vc1cu_reconstruct.argtypes = [vp, PP, i32, vp, i32, vp, i32]
+    L.vc1cu_loop_filter_i.argtypes = [vp, PP, i32]
+    L.vc1cu_loop_filter_p.argtypes = [vp, PP, i32, vp, vp, vp, vp]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
@@ -332,6 +335,17 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_forward_quant(self._h, C.byref(params), src_id, pred_id, type_mask,
                                                 co.ctypes.data, lv.ctypes.data))
         return co, lv
+
+    def loop_filter(self, params: Params, frame_id: int, block_mvs=None, cbp=None, tt=None, intra=None):
+        """In-place deblocking of frame slot frame_id: the I-like filter when block_mvs is None, else
+        the P filter of the coded blocks (per MB: 4 block vectors, 6 patterns, 6 kinds, intra bits)."""
+        if block_mvs is None:
+            self._check(self._L.vc1cu_loop_filter_i(self._h, C.byref(params), frame_id))
+            return
+        b = np.ascontiguousarray(block_mvs, np.int32)
+        cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
+        self._check(self._L.vc1cu_loop_filter_p(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data,
+                                                t.ctypes.data, i.ctypes.data))
 
     def reconstruct(self, params: Params, pred_id: int, d_levels: int, type_mask: int, block_types, out_id: int):
         """Frame slot out_id = pred_id + the inverse-transformed levels of each block's type

@@ -45,6 +45,11 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
+cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
+                                 cudaStream_t s);
+cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
+                                 const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
+                                 cudaStream_t s);
 void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
                   uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
 cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
@@ -176,6 +181,8 @@ struct vc1cu_ctx {
     int passes_cap = 0;
     BDesc* d_bdescs = nullptr;
     int bdescs_cap = 0;
+    void* d_lf = nullptr;      // coded-block metadata of vc1cu_loop_filter_p
+    size_t lf_cap = 0;
     void* d_btypes = nullptr;  // per-block transform types of vc1cu_reconstruct
     size_t btypes_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
@@ -944,6 +951,7 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
         if (c->d_bdescs) cudaFree(c->d_bdescs);
     if (c->d_ic) cudaFree(c->d_ic);
     if (c->d_btypes) cudaFree(c->d_btypes);
+    if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_icdesc) cudaFree(c->d_icdesc);
         c->d_bdescs = nullptr;
         c->bdescs_cap = 0;
@@ -1668,6 +1676,55 @@ int vc1cu_motion_compensate(vc1cu_ctx* c, const vc1cu_params* p, int ref_id, int
                   fp.pitch_c, c->stream);
         ck(cudaGetLastError(), "mc_kernel launch");
         tm.stop(1);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_loop_filter_i(vc1cu_ctx* c, const vc1cu_params* p, int frame_id) {
+    return guarded(c, [&]() -> int {
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& f = frame_slot(c, frame_id);
+        if (f.w != P.W || f.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const DevFrame d = f.view();
+        Timer tm(c, kMc);
+        ck(launch_loop_filter_i((uint8_t*)d.y, (uint8_t*)d.u, (uint8_t*)d.v, f.pitch_y, f.pitch_c, P.W, P.H, P.pq, c->stream),
+           "loop filter launch");
+        tm.stop(2);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs, const uint8_t* cbp,
+                        const uint8_t* tt, const uint8_t* intra) {
+    return guarded(c, [&]() -> int {
+        if (!block_mvs || !cbp || !tt || !intra) throw Fail{VC1CU_ERR_ARG, "null block metadata"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& f = frame_slot(c, frame_id);
+        if (f.w != P.W || f.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        for (size_t i = 0; i < mbs * 6; ++i)
+            if (cbp[i] > 15 || !(tt[i] == 0 || tt[i] == 3 || tt[i] == 6 || tt[i] == 7))
+                throw Fail{VC1CU_ERR_ARG, "block patterns are 4-bit and transform kinds 0, 3, 6 or 7"};
+        const size_t bm = 32 * mbs, al = (bm + 255) & ~size_t(255);
+        uint8_t* d = static_cast<uint8_t*>(ensure(c->d_lf, c->lf_cap, al + 13 * mbs + 256, "cudaMalloc(loop filter metadata)"));
+        ck(cudaMemcpyAsync(d, block_mvs, bm, cudaMemcpyHostToDevice, c->stream), "upload block vectors");
+        ck(cudaMemcpyAsync(d + al, cbp, 6 * mbs, cudaMemcpyHostToDevice, c->stream), "upload block patterns");
+        ck(cudaMemcpyAsync(d + al + 6 * mbs, tt, 6 * mbs, cudaMemcpyHostToDevice, c->stream), "upload transform kinds");
+        ck(cudaMemcpyAsync(d + al + 12 * mbs, intra, mbs, cudaMemcpyHostToDevice, c->stream), "upload intra bits");
+        const DevFrame fr = f.view();
+        Timer tm(c, kMc);
+        ck(launch_loop_filter_p((uint8_t*)fr.y, (uint8_t*)fr.u, (uint8_t*)fr.v, f.pitch_y, f.pitch_c, P.W, P.H, P.pq,
+                                reinterpret_cast<const int2*>(d), d + al, d + al + 6 * mbs, d + al + 12 * mbs, c->stream),
+           "loop filter launch");
+        tm.stop(2);
+        // the metadata copies read the caller's pageable arrays; finish before returning
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
         return VC1CU_OK;
     });
 }

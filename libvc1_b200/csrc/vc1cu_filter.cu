@@ -1,0 +1,248 @@
+// vc1cu_filter.cu - VC-1 in-loop deblocking on the device: the I-like all-edges filter
+// (Vc1Encoder::apply_i_like_loop_filter, encoder_filter.cpp:426-441) and the Advanced Profile
+// P-picture filter of the coded blocks (apply_p_loop_filter, :610-738).
+//
+// Each edge filter works on groups of four lines across the edge (the third line decides for
+// its group) and only reads and writes along its lines, so the groups of one edge are
+// independent. The reference walks the picture in raster order (per macroblock row, the
+// horizontal edges of MB x before the vertical edges of MB x-1). That order is equivalent to:
+// every horizontal edge first, each 4-column strip walked top to bottom (a strip's edges read
+// rows the edge above it wrote), then every vertical edge, each 4-row strip walked left to right
+// (an inner 4x4 edge reads the column the block's left neighbour's border wrote); strips of one
+// phase touch disjoint pixels. So one thread owns one strip:
+//   lfp_h_kernel  one thread per 4-column strip of a plane: the horizontal edges, top to bottom;
+//   lfp_v_kernel  one thread per 4-row strip: the vertical edges, left to right.
+// The I-like filter has no order between its edges of one direction (8 pixels apart, each reads
+// 4 on either side and writes 1): one thread per 4-line group of every edge.
+#include <cuda_runtime.h>
+
+#include "vc1cu_core.cuh"
+
+namespace vc1cu {
+
+struct LfPlane {
+    uint8_t* p;
+    int pitch, w, h;
+};
+
+// Vc1Encoder::loop_filter_line (encoder_filter.cpp:366-395): the line across the edge between
+// (x - cross) and (x, y); false when ineligible.
+__device__ bool lf_line(const LfPlane& pl, int x, int y, int cdx, int cdy, int pq) {
+    if (x - 4 * cdx < 0 || y - 4 * cdy < 0 || x + 3 * cdx >= pl.w || y + 3 * cdy >= pl.h || x < 0 || y < 0 ||
+        x >= pl.w || y >= pl.h)
+        return false;
+    const int step = cdy * pl.pitch + cdx;
+    uint8_t* c = pl.p + (size_t)y * pl.pitch + x;
+    auto S = [&](int k) { return (int)c[k * step]; };
+    int a0 = arshift(2 * (S(-2) - S(1)) - 5 * (S(-1) - S(0)) + 4, 3);
+    const bool a0_neg = a0 < 0;
+    a0 = iabs(a0);
+    if (a0 >= pq) return false;
+    const int a1 = iabs(arshift(2 * (S(-4) - S(-1)) - 5 * (S(-3) - S(-2)) + 4, 3));
+    const int a2 = iabs(arshift(2 * (S(0) - S(3)) - 5 * (S(1) - S(2)) + 4, 3));
+    if (!(a1 < a0 || a2 < a0)) return false;
+    const int edge = S(-1) - S(0);
+    const int limit = iabs(edge) >> 1;
+    if (!limit) return false;
+    int delta = (5 * (a0 - imin(a1, a2))) >> 3;
+    if (a0_neg != (edge < 0)) {
+        delta = imin(delta, limit);
+        if (edge < 0) delta = -delta;
+        c[-step] = (uint8_t)iclamp(S(-1) - delta, 0, 255);
+        c[0] = (uint8_t)iclamp(S(0) + delta, 0, 255);
+    }
+    return true;
+}
+
+// One 4-line group of loop_filter_edge (:397-416) starting at (x, y) along (adx, ady).
+__device__ void lf_group(const LfPlane& pl, int x, int y, int adx, int ady, int cdx, int cdy, int pq) {
+    if (!lf_line(pl, x + 2 * adx, y + 2 * ady, cdx, cdy, pq)) return;
+    lf_line(pl, x, y, cdx, cdy, pq);
+    lf_line(pl, x + adx, y + ady, cdx, cdy, pq);
+    lf_line(pl, x + 3 * adx, y + 3 * ady, cdx, cdy, pq);
+}
+// the group of a horizontal edge (columns x..x+3, edge above row y) / of a vertical edge
+__device__ __forceinline__ void lf_hgroup(const LfPlane& pl, int x, int y, int pq) { lf_group(pl, x, y, 1, 0, 0, 1, pq); }
+__device__ __forceinline__ void lf_vgroup(const LfPlane& pl, int x, int y, int pq) { lf_group(pl, x, y, 0, 1, 1, 0, pq); }
+
+// The three planes of a frame slot; strip index -> (plane, strip within it).
+struct LfFrame {
+    LfPlane pl[3];
+};
+
+// I-like filter, horizontal borders (apply_i_like_loop_filter_plane, :426-434): every row y = 8k
+// (k >= 1), every 4-column group.
+__global__ void lfi_h_kernel(LfFrame f, int pq) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < 3; ++k) {
+        const LfPlane& pl = f.pl[k];
+        const int gx = (pl.w + 3) / 4, ey = (pl.h - 1) / 8;  // edges at y = 8..8*ey
+        if (idx < gx * ey) {
+            lf_hgroup(pl, (idx % gx) * 4, (idx / gx + 1) * 8, pq);
+            return;
+        }
+        idx -= gx * ey;
+    }
+}
+// I-like filter, vertical borders: every column x = 8k (k >= 1), every 4-row group.
+__global__ void lfi_v_kernel(LfFrame f, int pq) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < 3; ++k) {
+        const LfPlane& pl = f.pl[k];
+        const int gy = (pl.h + 3) / 4, ex = (pl.w - 1) / 8;
+        if (idx < gy * ex) {
+            lf_vgroup(pl, (idx / gy + 1) * 8, (idx % gy) * 4, pq);
+            return;
+        }
+        idx -= gy * ex;
+    }
+}
+
+// Coded-block metadata of the P filter: 4 block vectors, 6 loop_filter_pattern and 6
+// loop_filter_tt codes and one intra bit per block, per macroblock.
+struct LfMeta {
+    const int2* bmv;
+    const uint8_t* cbp;
+    const uint8_t* tt;
+    const uint8_t* intra;
+    int mbw, mbh;
+};
+
+struct LfBlock {
+    int cbp, tt;
+    bool intra;
+    int2 mv;
+};
+
+// The block (bx, by) of plane k (luma 8x8 grid, chroma one block per MB), with mv_at's vector:
+// the luma block vector, or for chroma the pre-FASTUVMC representative of the 4-MV median
+// (encoder_filter.cpp:628-637).
+__device__ LfBlock lf_block(const LfMeta& m, int k, int bx, int by) {
+    const bool luma = k == 0;
+    const int mx = luma ? bx >> 1 : bx, my = luma ? by >> 1 : by;
+    const int bk = luma ? (((by & 1) << 1) | (bx & 1)) : 3 + k;
+    const int mb = my * m.mbw + mx;
+    LfBlock b;
+    b.cbp = m.cbp[mb * 6 + bk];
+    b.tt = m.tt[mb * 6 + bk];
+    b.intra = (m.intra[mb] >> bk) & 1;
+    const int2* v = m.bmv + mb * 4;
+    if (luma) {
+        b.mv = v[bk];
+    } else {
+        auto med4 = [](int a, int b2, int c, int d) {
+            if (a < b2) {
+                if (c < d) return (imin(b2, d) + imax(a, c)) / 2;
+                return (imin(b2, c) + imax(a, d)) / 2;
+            }
+            if (c < d) return (imin(a, d) + imax(b2, c)) / 2;
+            return (imin(a, c) + imax(b2, d)) / 2;
+        };
+        const int cx = med4(v[0].x, v[1].x, v[2].x, v[3].x), cy = med4(v[0].y, v[1].y, v[2].y, v[3].y);
+        b.mv = make_int2(arshift(cx + ((cx & 3) == 3), 1), arshift(cy + ((cy & 3) == 3), 1));
+    }
+    return b;
+}
+
+// Horizontal edges of one 4-column strip, top to bottom (process_v_parent, :654-676): each
+// block's bottom border, then its inner 4-row edge.
+__global__ void lfp_h_kernel(LfFrame f, LfMeta m, int pq) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < 3; ++k) {
+        const LfPlane& pl = f.pl[k];
+        const int gx = (pl.w + 3) / 4;
+        if (idx >= gx) {
+            idx -= gx;
+            continue;
+        }
+        const int cx = idx * 4, bx = cx >> 3, half = (cx >> 2) & 1;
+        const int grid_h = k == 0 ? m.mbh * 2 : m.mbh;
+        for (int by = 0; by < grid_h; ++by) {
+            const int x0 = bx * 8, y0 = by * 8;
+            if (x0 >= pl.w || y0 >= pl.h) break;
+            const LfBlock b = lf_block(m, k, bx, by);
+            if (by + 1 < grid_h && y0 + 8 < pl.h) {
+                const LfBlock n = lf_block(m, k, bx, by + 1);
+                if (b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
+                    if (half * 4 < imin(8, pl.w - x0)) lf_hgroup(pl, cx, y0 + 8, pq);
+                } else {
+                    const int mask = (b.cbp | (n.cbp >> 2)) & 3;
+                    if (half == 0 ? (mask & 2) != 0 : ((mask & 1) && x0 + 4 < pl.w)) lf_hgroup(pl, cx, y0 + 8, pq);
+                }
+            }
+            if ((b.tt == 7 || b.tt == 3) && y0 + 4 < pl.h) {
+                if (half == 0 ? (b.cbp & 10) != 0 : ((b.cbp & 5) && x0 + 4 < pl.w)) lf_hgroup(pl, cx, y0 + 4, pq);
+            }
+        }
+        return;
+    }
+}
+
+// Vertical edges of one 4-row strip, left to right (process_h_parent, :677-699): each block's
+// right border, then its inner 4-column edge.
+__global__ void lfp_v_kernel(LfFrame f, LfMeta m, int pq) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < 3; ++k) {
+        const LfPlane& pl = f.pl[k];
+        const int gy = (pl.h + 3) / 4;
+        if (idx >= gy) {
+            idx -= gy;
+            continue;
+        }
+        const int ry = idx * 4, by = ry >> 3, half = (ry >> 2) & 1;
+        const int grid_w = k == 0 ? m.mbw * 2 : m.mbw;
+        for (int bx = 0; bx < grid_w; ++bx) {
+            const int x0 = bx * 8, y0 = by * 8;
+            if (x0 >= pl.w || y0 >= pl.h) break;
+            const LfBlock b = lf_block(m, k, bx, by);
+            if (bx + 1 < grid_w && x0 + 8 < pl.w) {
+                const LfBlock n = lf_block(m, k, bx + 1, by);
+                if (b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
+                    if (half * 4 < imin(8, pl.h - y0)) lf_vgroup(pl, x0 + 8, ry, pq);
+                } else {
+                    const int mask = (b.cbp | (n.cbp >> 1)) & 5;
+                    if (half == 0 ? (mask & 4) != 0 : ((mask & 1) && y0 + 4 < pl.h)) lf_vgroup(pl, x0 + 8, ry, pq);
+                }
+            }
+            if ((b.tt == 7 || b.tt == 6) && x0 + 4 < pl.w) {
+                if (half == 0 ? (b.cbp & 12) != 0 : ((b.cbp & 3) && y0 + 4 < pl.h)) lf_vgroup(pl, x0 + 4, ry, pq);
+            }
+        }
+        return;
+    }
+}
+
+static LfFrame lf_frame(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H) {
+    LfFrame f;
+    f.pl[0] = LfPlane{y, pitch_y, W, H};
+    f.pl[1] = LfPlane{u, pitch_c, W / 2, H / 2};
+    f.pl[2] = LfPlane{v, pitch_c, W / 2, H / 2};
+    return f;
+}
+
+cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
+                                 cudaStream_t s) {
+    const LfFrame f = lf_frame(y, u, v, pitch_y, pitch_c, W, H);
+    int nh = 0, nv = 0;
+    for (int k = 0; k < 3; ++k) {
+        const LfPlane& pl = f.pl[k];
+        nh += ((pl.w + 3) / 4) * imax(0, (pl.h - 1) / 8);
+        nv += ((pl.h + 3) / 4) * imax(0, (pl.w - 1) / 8);
+    }
+    if (nh) lfi_h_kernel<<<(unsigned)((nh + 127) / 128), 128, 0, s>>>(f, pq);
+    if (nv) lfi_v_kernel<<<(unsigned)((nv + 127) / 128), 128, 0, s>>>(f, pq);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
+                                 const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
+                                 cudaStream_t s) {
+    const LfFrame f = lf_frame(y, u, v, pitch_y, pitch_c, W, H);
+    const LfMeta m{bmv, cbp, tt, intra, (W + 15) / 16, (H + 15) / 16};
+    const int nh = (W + 3) / 4 + 2 * ((W / 2 + 3) / 4), nv = (H + 3) / 4 + 2 * ((H / 2 + 3) / 4);
+    lfp_h_kernel<<<(unsigned)((nh + 63) / 64), 64, 0, s>>>(f, m, pq);
+    lfp_v_kernel<<<(unsigned)((nv + 63) / 64), 64, 0, s>>>(f, m, pq);
+    return cudaGetLastError();
+}
+
+}  // namespace vc1cu

@@ -80,6 +80,8 @@ class Oracle:
         L.vo_zoom_coherent.argtypes = [vp, i32, i32]
         L.vo_b_predict.argtypes = [P, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp]
         L.vo_reconstruct.argtypes = [P, vp, vp, i32, vp, vp, vp, vp]
+        L.vo_loop_filter_i.argtypes = [P, vp, vp, vp]
+        L.vo_loop_filter_p.argtypes = [P, vp, vp, vp, vp, vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -175,6 +177,18 @@ class Oracle:
         oy, ou, ov = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
         self.lib.vo_intensity_compensate(self._f(ref), C.byref(k), oy.ctypes.data, ou.ctypes.data, ov.ctypes.data)
         return oy, ou, ov
+
+    def loop_filter(self, p, frame, block_mvs=None, cbp=None, tt=None, intra=None):
+        """A filtered copy of frame: the I-like filter when block_mvs is None, else the P filter."""
+        y, u, v = (np.array(a, np.uint8, copy=True) for a in _planes(frame))
+        if block_mvs is None:
+            self.lib.vo_loop_filter_i(C.byref(p), y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        else:
+            b = np.ascontiguousarray(block_mvs, np.int32)
+            cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
+            self.lib.vo_loop_filter_p(C.byref(p), y.ctypes.data, u.ctypes.data, v.ctypes.data, b.ctypes.data,
+                                      cb.ctypes.data, t.ctypes.data, i.ctypes.data)
+        return y, u, v
 
     def reconstruct(self, p, pred, levels, type_mask, block_types):
         h, w = p.height, p.width
@@ -288,6 +302,8 @@ class Reference:
         L.ref_scene_change_score.restype = C.c_double
         L.ref_b_predict.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, vp]
         L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
+        L.ref_loop_filter_i.argtypes = [vp, vp]
+        L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -376,6 +392,21 @@ class Reference:
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)
         self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def loop_filter(self, frame, block_mvs=None, cbp=None, tt=None, intra=None):
+        h, w = self.p.height, self.p.width
+        f = self.frame(frame)
+        if block_mvs is None:
+            self.lib.ref_loop_filter_i(self.h, f.h)
+        else:
+            b = np.ascontiguousarray(block_mvs, np.int32)
+            cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
+            self.lib.ref_loop_filter_p(self.h, f.h, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data)
+        y = np.zeros((h, w), np.uint8)
+        u = np.zeros((h // 2, w // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(f.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
         return y, u, v
 
     def reconstruct(self, pred, levels, type_mask, block_types):

@@ -369,6 +369,28 @@ void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, 
             }
 }
 
+// In-place loop filters of a frame handle: apply_i_like_loop_filter, or apply_p_loop_filter
+// with per-MB block vectors (4), coded-block patterns and transform kinds (6) and intra bits.
+void ref_loop_filter_i(void* h, void* frame) { E(h).apply_i_like_loop_filter(*static_cast<Frame*>(frame)); }
+
+void ref_loop_filter_p(void* h, void* frame, const vc1cu_mv* bmv, const uint8_t* cbp, const uint8_t* tt,
+                       const uint8_t* intra) {
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const size_t mbs = static_cast<size_t>(mbw) * mbh;
+    std::vector<std::array<MV, 4>> b(mbs);
+    std::vector<std::array<uint8_t, 6>> cb(mbs), t(mbs);
+    std::vector<uint8_t> in(intra, intra + mbs);
+    for (size_t i = 0; i < mbs; ++i) {
+        for (int k = 0; k < 4; ++k) b[i][k] = MV{bmv[i * 4 + k].xq, bmv[i * 4 + k].yq};
+        for (int k = 0; k < 6; ++k) {
+            cb[i][k] = cbp[i * 6 + k];
+            t[i][k] = tt[i * 6 + k];
+        }
+    }
+    E(h).apply_p_loop_filter(*static_cast<Frame*>(frame), b, cb, t, in, mbw, mbh);
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

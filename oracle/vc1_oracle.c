@@ -2485,3 +2485,174 @@ void vo_reconstruct(const vc1cu_params* p, const vo_frame* pred, const int16_t* 
                     }
             }
 }
+
+/* ---- in-loop deblocking --------------------------------------------------------------- */
+
+/* Vc1Encoder::loop_filter_line, encoder_filter.cpp:366-395: one 8-sample line across an edge
+ * between (x - cross) and (x, y); returns whether the line was eligible (its a0 test). */
+static int lf_line(uint8_t* p, int w, int h, int x, int y, int cdx, int cdy, int pq) {
+    for (int k = -4; k <= 3; ++k) {
+        const int xx = x + k * cdx, yy = y + k * cdy;
+        if (xx < 0 || yy < 0 || xx >= w || yy >= h) return 0;
+    }
+#define LFS(k) ((int)p[(size_t)(y + (k) * cdy) * w + x + (k) * cdx])
+    int a0 = arshift(2 * (LFS(-2) - LFS(1)) - 5 * (LFS(-1) - LFS(0)) + 4, 3);
+    const int a0_neg = a0 < 0;
+    a0 = iabs(a0);
+    if (a0 >= pq) return 0;
+    const int a1 = iabs(arshift(2 * (LFS(-4) - LFS(-1)) - 5 * (LFS(-3) - LFS(-2)) + 4, 3));
+    const int a2 = iabs(arshift(2 * (LFS(0) - LFS(3)) - 5 * (LFS(1) - LFS(2)) + 4, 3));
+    if (!(a1 < a0 || a2 < a0)) return 0;
+    const int edge = LFS(-1) - LFS(0);
+#undef LFS
+    const int limit = iabs(edge) >> 1;
+    if (!limit) return 0;
+    int delta = (5 * (a0 - imin(a1, a2))) >> 3;
+    if (a0_neg != (edge < 0)) {
+        delta = imin(delta, limit);
+        if (edge < 0) delta = -delta;
+        const size_t po = (size_t)(y - cdy) * w + x - cdx, qo = (size_t)y * w + x;
+        p[po] = (uint8_t)iclamp((int)p[po] - delta, 0, 255);
+        p[qo] = (uint8_t)iclamp((int)p[qo] + delta, 0, 255);
+    }
+    return 1;
+}
+
+/* Vc1Encoder::loop_filter_edge, encoder_filter.cpp:397-416 (scalar): groups of 4 lines, the
+ * third line decides for its group */
+static void lf_edge(uint8_t* p, int w, int h, int x, int y, int adx, int ady, int cdx, int cdy, int len, int pq) {
+    for (int i = 0; i < len; i += 4) {
+        const int bx = x + i * adx, by = y + i * ady;
+        if (!lf_line(p, w, h, bx + 2 * adx, by + 2 * ady, cdx, cdy, pq)) continue;
+        lf_line(p, w, h, bx, by, cdx, cdy, pq);
+        lf_line(p, w, h, bx + adx, by + ady, cdx, cdy, pq);
+        lf_line(p, w, h, bx + 3 * adx, by + 3 * ady, cdx, cdy, pq);
+    }
+}
+static void lf_hborder(uint8_t* p, int w, int h, int x, int y, int len, int pq) { lf_edge(p, w, h, x, y, 1, 0, 0, 1, len, pq); }
+static void lf_vborder(uint8_t* p, int w, int h, int x, int y, int len, int pq) { lf_edge(p, w, h, x, y, 0, 1, 1, 0, len, pq); }
+
+/* Vc1Encoder::apply_i_like_loop_filter_plane, encoder_filter.cpp:426-434 */
+static void lf_i_plane(uint8_t* p, int w, int h, int pq) {
+    for (int y = 8; y < h; y += 8)
+        for (int x = 0; x < w; x += 16) lf_hborder(p, w, h, x, y, imin(16, w - x), pq);
+    for (int x = 8; x < w; x += 8)
+        for (int y = 0; y < h; y += 16) lf_vborder(p, w, h, x, y, imin(16, h - y), pq);
+}
+
+/* Vc1Encoder::apply_i_like_loop_filter, encoder_filter.cpp:436-441 (in place) */
+void vo_loop_filter_i(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v) {
+    lf_i_plane(y, p->width, p->height, p->pqindex);
+    lf_i_plane(u, p->width / 2, p->height / 2, p->pqindex);
+    lf_i_plane(v, p->width / 2, p->height / 2, p->pqindex);
+}
+
+typedef struct lf_meta {
+    const vc1cu_mv* bmv;   /* 4 per MB */
+    const uint8_t* cbp;    /* 6 per MB: loop_filter_pattern of each block */
+    const uint8_t* tt;     /* 6 per MB: loop_filter_tt of each block */
+    const uint8_t* intra;  /* per MB: bit k = block k intra */
+    int mbw, mbh, luma, plane_k;
+} lf_meta;
+
+static void lf_at(const lf_meta* m, int bx, int by, int* mx, int* my, int* k) {
+    if (m->luma) { *mx = bx >> 1; *my = by >> 1; *k = ((by & 1) << 1) | (bx & 1); }
+    else { *mx = bx; *my = by; *k = m->plane_k; }
+}
+/* mv_at of apply_p_loop_filter_plane (encoder_filter.cpp:628-637): the block's vector, or for
+ * chroma the pre-FASTUVMC representative of the 4-MV median */
+static vc1cu_mv lf_mv(const lf_meta* m, int bx, int by) {
+    int mx, my, k;
+    lf_at(m, bx, by, &mx, &my, &k);
+    const vc1cu_mv* b = m->bmv + ((size_t)my * m->mbw + mx) * 4;
+    if (m->luma) return b[k];
+    const int cx = median4(b[0].xq, b[1].xq, b[2].xq, b[3].xq), cy = median4(b[0].yq, b[1].yq, b[2].yq, b[3].yq);
+    vc1cu_mv r;
+    r.xq = arshift(cx + ((cx & 3) == 3), 1);
+    r.yq = arshift(cy + ((cy & 3) == 3), 1);
+    return r;
+}
+static int lf_cbp(const lf_meta* m, int bx, int by) { int mx, my, k; lf_at(m, bx, by, &mx, &my, &k); return m->cbp[((size_t)my * m->mbw + mx) * 6 + k]; }
+static int lf_tt(const lf_meta* m, int bx, int by) { int mx, my, k; lf_at(m, bx, by, &mx, &my, &k); return m->tt[((size_t)my * m->mbw + mx) * 6 + k]; }
+static int lf_intra(const lf_meta* m, int bx, int by) {
+    int mx, my, k;
+    lf_at(m, bx, by, &mx, &my, &k);
+    return (m->intra[(size_t)my * m->mbw + mx] >> k) & 1;
+}
+static int lf_same_mv(vc1cu_mv a, vc1cu_mv b) { return a.xq == b.xq && a.yq == b.yq; }
+
+/* process_v_parent, encoder_filter.cpp:654-676: the block's bottom border and its inner
+ * horizontal 4-line edge */
+static void lf_v_parent(const lf_meta* m, uint8_t* p, int w, int h, int bx, int by, int pq) {
+    const int x0 = bx * 8, y0 = by * 8;
+    if (x0 >= w || y0 >= h) return;
+    const int grid_h = m->luma ? m->mbh * 2 : m->mbh;
+    if (by + 1 < grid_h && y0 + 8 < h) {
+        const int top = lf_cbp(m, bx, by), bottom = lf_cbp(m, bx, by + 1);
+        if (lf_intra(m, bx, by) || lf_intra(m, bx, by + 1) || !lf_same_mv(lf_mv(m, bx, by), lf_mv(m, bx, by + 1))) {
+            lf_hborder(p, w, h, x0, y0 + 8, imin(8, w - x0), pq);
+        } else {
+            const int mask = (top | (bottom >> 2)) & 3;
+            if ((mask & 2) && x0 < w) lf_hborder(p, w, h, x0, y0 + 8, imin(4, w - x0), pq);
+            if ((mask & 1) && x0 + 4 < w) lf_hborder(p, w, h, x0 + 4, y0 + 8, imin(4, w - (x0 + 4)), pq);
+        }
+    }
+    const int kind = lf_tt(m, bx, by), pat = lf_cbp(m, bx, by);
+    if ((kind == 7 || kind == 3) && y0 + 4 < h) {
+        if ((pat & 10) && x0 < w) lf_hborder(p, w, h, x0, y0 + 4, imin(4, w - x0), pq);
+        if ((pat & 5) && x0 + 4 < w) lf_hborder(p, w, h, x0 + 4, y0 + 4, imin(4, w - (x0 + 4)), pq);
+    }
+}
+/* process_h_parent, encoder_filter.cpp:677-699: the block's right border and inner vertical edge */
+static void lf_h_parent(const lf_meta* m, uint8_t* p, int w, int h, int bx, int by, int pq) {
+    const int x0 = bx * 8, y0 = by * 8;
+    if (x0 >= w || y0 >= h) return;
+    const int grid_w = m->luma ? m->mbw * 2 : m->mbw;
+    if (bx + 1 < grid_w && x0 + 8 < w) {
+        const int left = lf_cbp(m, bx, by), right = lf_cbp(m, bx + 1, by);
+        if (lf_intra(m, bx, by) || lf_intra(m, bx + 1, by) || !lf_same_mv(lf_mv(m, bx, by), lf_mv(m, bx + 1, by))) {
+            lf_vborder(p, w, h, x0 + 8, y0, imin(8, h - y0), pq);
+        } else {
+            const int mask = (left | (right >> 1)) & 5;
+            if ((mask & 4) && y0 < h) lf_vborder(p, w, h, x0 + 8, y0, imin(4, h - y0), pq);
+            if ((mask & 1) && y0 + 4 < h) lf_vborder(p, w, h, x0 + 8, y0 + 4, imin(4, h - (y0 + 4)), pq);
+        }
+    }
+    const int kind = lf_tt(m, bx, by), pat = lf_cbp(m, bx, by);
+    if ((kind == 7 || kind == 6) && x0 + 4 < w) {
+        if ((pat & 12) && y0 < h) lf_vborder(p, w, h, x0 + 4, y0, imin(4, h - y0), pq);
+        if ((pat & 3) && y0 + 4 < h) lf_vborder(p, w, h, x0 + 4, y0 + 4, imin(4, h - (y0 + 4)), pq);
+    }
+}
+static void lf_mb(const lf_meta* m, uint8_t* p, int w, int h, int mx, int my, int pq, int vertical) {
+    if (m->luma) {
+        for (int k = 0; k < 4; ++k) {
+            const int bx = mx * 2 + (k & 1), by = my * 2 + (k >> 1);
+            if (vertical) lf_v_parent(m, p, w, h, bx, by, pq); else lf_h_parent(m, p, w, h, bx, by, pq);
+        }
+    } else if (vertical) {
+        lf_v_parent(m, p, w, h, mx, my, pq);
+    } else {
+        lf_h_parent(m, p, w, h, mx, my, pq);
+    }
+}
+
+/* Vc1Encoder::apply_p_loop_filter (Advanced Profile), encoder_filter.cpp:610-738, in place: per
+ * macroblock row, the horizontal edges of MB x before the vertical edges of MB x-1 */
+void vo_loop_filter_p(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v, const vc1cu_mv* block_mvs,
+                      const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra) {
+    lf_meta m = {block_mvs, cbp, tt, intra, mbw_of(p), mbh_of(p), 1, 0};
+    for (int plane = 0; plane < 3; ++plane) {
+        uint8_t* pl = plane == 0 ? y : (plane == 1 ? u : v);
+        const int w = plane ? p->width / 2 : p->width, h = plane ? p->height / 2 : p->height;
+        m.luma = plane == 0;
+        m.plane_k = plane == 0 ? 0 : 3 + plane;
+        for (int my = 0; my < m.mbh; ++my) {
+            for (int mx = 0; mx < m.mbw; ++mx) {
+                lf_mb(&m, pl, w, h, mx, my, p->pqindex, 1);
+                if (mx > 0) lf_mb(&m, pl, w, h, mx - 1, my, p->pqindex, 0);
+            }
+            if (m.mbw > 0) lf_mb(&m, pl, w, h, m.mbw - 1, my, p->pqindex, 0);
+        }
+    }
+}

@@ -110,6 +110,12 @@ void vo_forward_quant(const vc1cu_params* p, const vo_frame* src, const vo_frame
 void vo_reconstruct(const vc1cu_params* p, const vo_frame* pred, const int16_t* levels, int type_mask,
                     const uint8_t* block_types, uint8_t* y, uint8_t* u, uint8_t* v);
 
+/* in-loop deblocking (in place): the I-like all-edges filter and the P filter of the coded
+ * blocks (block_mvs 4 per MB, cbp / tt 6 per MB, intra one bit per block) */
+void vo_loop_filter_i(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v);
+void vo_loop_filter_p(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v, const vc1cu_mv* block_mvs,
+                      const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
+
 /* x87 extended-precision score emulation used by the GPU path, exposed for checking:
  * the long double value of sad + lambda*rate, as an integer scaled by 2^shift
  * (see vo_score_key in vc1_oracle.c). */

@@ -19,6 +19,9 @@ script calls it through oracle.Reference on inputs restated from the reference's
   recon_kat.npz     the reconstruction of xform_kat's pictures (levels of all four types, a
                     seeded transform type per block) and of seeded random levels, through the
                     reference's inverse_partition
+  lf_kat.npz        the reference's apply_i_like_loop_filter and apply_p_loop_filter of blocky
+                    seeded pictures with seeded coded-block metadata (tests/lf_cases.py), at
+                    four PQINDEX values, dense 4-MV and 1-MV fields
   scene_kat.npz     scene_change_score on seeded pictures: motion, a cut (two thresholds),
                     a fade with and without fade compensation, two camera zooms that the
                     local-motion fit rescues, and search range 0
@@ -238,6 +241,30 @@ def make_recon_kat():
     np.savez_compressed(os.path.join(HERE, "recon_kat.npz"), **d)
 
 
+LF_CASES = ((98, 66, 1, 8, True), (130, 98, 2, 20, False), (66, 50, 3, 3, True), (194, 146, 4, 31, True))
+
+
+def make_lf_kat():
+    from oracle import Reference
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from lf_cases import blocky_frame, metadata
+
+    d = {}
+    for i, (w, h, seed, pq, dense) in enumerate(LF_CASES):
+        R = Reference(make_params(w, h, pqindex=pq))
+        fr = blocky_frame(w, h, seed)
+        for c, pl in zip("yuv", fr):
+            d[f"c{i}.in.{c}"] = pl
+        for c, pl in zip("yuv", R.loop_filter(fr)):
+            d[f"c{i}.i.{c}"] = pl
+        bmv, cbp, tt, intra = metadata(w, h, seed, dense)
+        d[f"c{i}.bmv"], d[f"c{i}.cbp"], d[f"c{i}.tt"], d[f"c{i}.intra"] = bmv, cbp, tt, intra
+        for c, pl in zip("yuv", R.loop_filter(fr, bmv, cbp, tt, intra)):
+            d[f"c{i}.p.{c}"] = pl
+    np.savez_compressed(os.path.join(HERE, "lf_kat.npz"), **d)
+
+
 def make_scene_kat():
     from oracle import Reference
 
@@ -256,7 +283,7 @@ def main(only=()):
     if only:
         for name in only:
             {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat,
-             "recon_kat": make_recon_kat}[name]()
+             "recon_kat": make_recon_kat, "lf_kat": make_lf_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -376,6 +403,7 @@ def main(only=()):
     make_ic_kat()
     make_scene_kat()
     make_recon_kat()
+    make_lf_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,64 @@
+"""In-loop deblocking on the device (vc1cu_loop_filter_i / _p) against the reference's
+filtered pictures (tests/golden/lf_kat.npz) and the oracle, bit-exact, through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+from libvc1_b200.abi import make_params
+from libvc1_b200.api import Vc1cuError
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+LF_CASES = ((98, 66, 8), (130, 98, 20), (66, 50, 3), (194, 146, 31))
+
+
+def _frames(g, prefix):
+    return tuple(np.ascontiguousarray(g[f"{prefix}.{c}"]) for c in "yuv")
+
+
+@pytest.mark.parametrize("i", range(len(LF_CASES)))
+def test_loop_filter_matches_reference_fixture(ctx, i):
+    g = np.load(os.path.join(GOLDEN, "lf_kat.npz"))
+    w, h, pq = LF_CASES[i]
+    p = make_params(w, h, pqindex=pq)
+    fr = _frames(g, f"c{i}.in")
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0)
+    for got, c in zip(ctx.download_frame(0, w, h), "yuv"):
+        assert np.array_equal(got, g[f"c{i}.i.{c}"]), ("i", c)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0, *[g[f"c{i}.{k}"] for k in ("bmv", "cbp", "tt", "intra")])
+    for got, c in zip(ctx.download_frame(0, w, h), "yuv"):
+        assert np.array_equal(got, g[f"c{i}.p.{c}"]), ("p", c)
+
+
+@pytest.mark.parametrize("case", [(1920, 1080, 11, 9, True), (322, 242, 12, 25, False), (16, 16, 13, 5, True),
+                                  (354, 290, 14, 14, True)])
+def test_loop_filter_matches_oracle(ctx, oracle, case):
+    from lf_cases import blocky_frame, metadata
+
+    w, h, seed, pq, dense = case
+    p = make_params(w, h, pqindex=pq)
+    fr = blocky_frame(w, h, seed)
+    meta = metadata(w, h, seed, dense)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0, *meta)
+    for got, want in zip(ctx.download_frame(0, w, h), oracle.loop_filter(p, fr, *meta)):
+        assert np.array_equal(got, want)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0)
+    for got, want in zip(ctx.download_frame(0, w, h), oracle.loop_filter(p, fr)):
+        assert np.array_equal(got, want)
+
+
+def test_loop_filter_rejects_bad_codes(ctx):
+    from lf_cases import blocky_frame, metadata
+
+    p = make_params(64, 48, pqindex=8)
+    ctx.upload_frame(0, *blocky_frame(64, 48, 15))
+    bmv, cbp, tt, intra = metadata(64, 48, 15)
+    tt[0, 0] = 5
+    with pytest.raises(Vc1cuError, match="transform kinds"):
+        ctx.loop_filter(p, 0, bmv, cbp, tt, intra)

@@ -389,3 +389,36 @@ def test_reconstruction_matches_reference_live(oracle, tm):
     types = rng.choice([t for t in range(1, 5) if tm & (1 << (t - 1))], (lv.shape[1], 6)).astype(np.uint8)
     for x, y in zip(oracle.reconstruct(p, pred, lv, tm, types), R.reconstruct(R.frame(pred), lv, tm, types)):
         assert np.array_equal(x, y)
+
+
+# ---- in-loop deblocking (apply_i_like_loop_filter, apply_p_loop_filter) ----
+
+LF_CASES = ((98, 66, 8), (130, 98, 20), (66, 50, 3), (194, 146, 31))
+
+
+@pytest.mark.parametrize("i", range(len(LF_CASES)))
+def test_loop_filter_golden(oracle, i):
+    g = load("lf_kat.npz")
+    w, h, pq = LF_CASES[i]
+    p = make_params(w, h, pqindex=pq)
+    fr = _frames(g, f"c{i}.in")
+    for got, c in zip(oracle.loop_filter(p, fr), "yuv"):
+        assert np.array_equal(got, g[f"c{i}.i.{c}"]), ("i", c)
+    meta = [g[f"c{i}.{k}"] for k in ("bmv", "cbp", "tt", "intra")]
+    for got, c in zip(oracle.loop_filter(p, fr, *meta), "yuv"):
+        assert np.array_equal(got, g[f"c{i}.p.{c}"]), ("p", c)
+    assert not np.array_equal(g[f"c{i}.p.y"], fr[0])  # the filter does change the picture
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_loop_filter_matches_reference_live(oracle, seed):
+    from lf_cases import blocky_frame, metadata
+
+    Reference = _ref_or_skip()
+    w, h = 322, 242
+    p = make_params(w, h, pqindex=10 + seed)
+    R = Reference(p)
+    fr = blocky_frame(w, h, seed)
+    meta = metadata(w, h, seed, dense=seed % 2 == 0)
+    for x, y in zip(oracle.loop_filter(p, fr, *meta), R.loop_filter(fr, *meta)):
+        assert np.array_equal(x, y)
