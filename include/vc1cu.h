@@ -436,6 +436,17 @@ int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id
                                int type_mask, double* d_coeffs, int16_t* d_levels);
 
 /*
+ * The transform type (1 = 8x8, 2 = 8x4, 3 = 4x8, 4 = 4x4) that Vc1Encoder::choose_transform_mb
+ * picks for each MB with the throughput preset (fast transform RDO with variable transforms,
+ * trellis 0, no DQUANT; src/encoder_transform.cpp:1605-1712): the residual metrics of
+ * transform_metrics (src/transform_residual_metrics.h:29-61) between src_id and pred_id, the
+ * candidate list (split shapes where the coded raster crops an MB) and the preset's pick.
+ * types: HOST array of mbw*mbh. The RD search of the other presets stays with the caller.
+ * Synchronous.
+ */
+int vc1cu_fast_transform_types(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id, uint8_t* types);
+
+/*
  * The reconstruction a transform decision implies (evaluate_transform_parent,
  * src/encoder_transform.cpp:1569-1585): for every MB and parent block (Y0..Y3, U, V), the levels
  * of its chosen type dequantised (dequant_level at PQINDEX, :1058-1065), inverse-transformed

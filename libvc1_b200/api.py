@@ -36,7 +36,7 @@ EXPORTS = (
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
-    "vc1cu_loop_filter_i", "vc1cu_loop_filter_p",
+    "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_fast_transform_types",
 )
 
 
@@ -91,6 +91,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_b_predict.argtypes = [vp, PP, i32, i32, i32, i32, i32]
     L.vc1cu_reconstruct.argtypes = [vp, PP, i32, vp, i32, vp, i32]
     L.vc1cu_loop_filter_i.argtypes = [vp, PP, i32]
+    L.vc1cu_fast_transform_types.argtypes = [vp, PP, i32, i32, vp]
     L.vc1cu_loop_filter_p.argtypes = [vp, PP, i32, vp, vp, vp, vp]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
@@ -335,6 +336,13 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_forward_quant(self._h, C.byref(params), src_id, pred_id, type_mask,
                                                 co.ctypes.data, lv.ctypes.data))
         return co, lv
+
+    def fast_transform_types(self, params: Params, src_id: int, pred_id: int):
+        """The throughput preset's transform type (1..4) of every MB of src_id against pred_id."""
+        mbw, mbh = mbs_of(params)
+        out = np.zeros(mbw * mbh, np.uint8)
+        self._check(self._L.vc1cu_fast_transform_types(self._h, C.byref(params), src_id, pred_id, out.ctypes.data))
+        return out
 
     def loop_filter(self, params: Params, frame_id: int, block_mvs=None, cbp=None, tt=None, intra=None):
         """In-place deblocking of frame slot frame_id: the I-like filter when block_mvs is None, else

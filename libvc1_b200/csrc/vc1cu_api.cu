@@ -50,6 +50,7 @@ cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y
 cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
                                  cudaStream_t s);
+void launch_fast_tt(const DevParams& P, const DevFrame& src, const DevFrame& pred, uint8_t* types, cudaStream_t s);
 void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
                   uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
 cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
@@ -1676,6 +1677,29 @@ int vc1cu_motion_compensate(vc1cu_ctx* c, const vc1cu_params* p, int ref_id, int
                   fp.pitch_c, c->stream);
         ck(cudaGetLastError(), "mc_kernel launch");
         tm.stop(1);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_fast_transform_types(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pred_id, uint8_t* types) {
+    return guarded(c, [&]() -> int {
+        if (!types) throw Fail{VC1CU_ERR_ARG, "null output"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& fs = frame_slot(c, src_id);
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        uint8_t* d = static_cast<uint8_t*>(ensure(c->d_btypes, c->btypes_cap, std::max<size_t>(mbs * 6, 256), "cudaMalloc(types)"));
+        Timer tm(c, kXform);
+        launch_fast_tt(P, fs.view(), fp.view(), d, c->stream);
+        ck(cudaGetLastError(), "transform type launch");
+        tm.stop(1);
+        ck(cudaMemcpyAsync(types, d, mbs, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(types)");
+        sync_checked(c);
         return VC1CU_OK;
     });
 }

@@ -296,6 +296,71 @@ void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* level
     recon_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, pred, levels, tindex, block_types, dy, du, dv, pitch_y, pitch_c);
 }
 
+// ---- transform type of the throughput preset (encoder_transform.cpp:1605-1712) ----------------
+
+// One warp per MB: transform_metrics::scalar (transform_residual_metrics.h:29-61) with each lane
+// summing half a row, then choose_transform_mb's candidate list and the preset's pick.
+__global__ void fast_tt_kernel(const __grid_constant__ DevParams P, DevFrame src, DevFrame pred, uint8_t* types) {
+    const int mb = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (mb >= P.mbw * P.mbh) return;
+    const int mx = mb % P.mbw, my = mb / P.mbw;
+    const int py = lane >> 1, px0 = (lane & 1) * 8;
+    uint32_t sad = 0, hedge = 0, vedge = 0, grad = 0;
+    const int y = my * 16 + py;
+    if (y < P.H) {
+        auto R = [&](int xx, int yy) {
+            return (int)src.y[(size_t)yy * src.pitch_y + xx] - (int)pred.y[(size_t)yy * pred.pitch_y + xx];
+        };
+        for (int px = px0; px < px0 + 8 && mx * 16 + px < P.W; ++px) {
+            const int x = mx * 16 + px;
+            const int r = R(x, y);
+            sad += (uint32_t)iabs(r);
+            if ((py & 7) == 4) hedge += (uint32_t)iabs(r - R(x, y - 1));
+            if ((px & 7) == 4) vedge += (uint32_t)iabs(r - R(x - 1, y));
+            if (px > 0) grad += (uint32_t)iabs(r - R(x - 1, y));
+            if (py > 0) grad += (uint32_t)iabs(r - R(x, y - 1));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        sad += __shfl_xor_sync(0xffffffffu, sad, o);
+        hedge += __shfl_xor_sync(0xffffffffu, hedge, o);
+        vedge += __shfl_xor_sync(0xffffffffu, vedge, o);
+        grad += __shfl_xor_sync(0xffffffffu, grad, o);
+    }
+    if (lane) return;
+    const uint64_t S = sad, HE = hedge, VE = vedge, G = grad, lim = (uint64_t)(64 * P.pq);
+    int list[4] = {1, 1, 1, 1}, count = 0;
+    const bool split_x = mx == P.mbw - 1 && (P.W & 15) != 0, split_y = my == P.mbh - 1 && (P.H & 15) != 0;
+    if (split_x && split_y) {
+        list[count++] = 4;
+    } else if (split_x || split_y) {
+        list[count++] = split_x ? 3 : 2;
+        if (S > lim && G > S * 2) list[count++] = 4;
+    } else {
+        list[count++] = 1;
+        if (S > lim) {
+            if (HE * 5 > VE * 6) list[count++] = 2;
+            else if (VE * 5 > HE * 6) list[count++] = 3;
+            else { list[count++] = 2; list[count++] = 3; }
+            if (count < 4 && G > S * 2) list[count++] = 4;
+        }
+    }
+    int chosen = list[0];
+    if (count > 1) {
+        int index = count - 1;
+        if (list[index] == 4 && G * 2 <= S * 5) --index;
+        chosen = list[index];
+        if (chosen == 3 && index > 0 && list[index - 1] == 2 && HE >= VE) chosen = 2;
+    }
+    types[mb] = (uint8_t)chosen;
+}
+
+void launch_fast_tt(const DevParams& P, const DevFrame& src, const DevFrame& pred, uint8_t* types, cudaStream_t s) {
+    const int mbs = P.mbw * P.mbh;
+    fast_tt_kernel<<<(unsigned)((mbs + 3) / 4), 128, 0, s>>>(P, src, pred, types);
+}
+
 void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
                uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
     dim3 grid((P.W + 127) / 128, P.H);

@@ -82,6 +82,7 @@ class Oracle:
         L.vo_reconstruct.argtypes = [P, vp, vp, i32, vp, vp, vp, vp]
         L.vo_loop_filter_i.argtypes = [P, vp, vp, vp]
         L.vo_loop_filter_p.argtypes = [P, vp, vp, vp, vp, vp, vp, vp]
+        L.vo_fast_transform_types.argtypes = [P, vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
         L.vo_score_key.argtypes = [u64, C.c_double, u64, i32, C.POINTER(u64), C.POINTER(u64)]
@@ -189,6 +190,12 @@ class Oracle:
             self.lib.vo_loop_filter_p(C.byref(p), y.ctypes.data, u.ctypes.data, v.ctypes.data, b.ctypes.data,
                                       cb.ctypes.data, t.ctypes.data, i.ctypes.data)
         return y, u, v
+
+    def fast_transform_types(self, p, src, pred):
+        mbw, mbh = mbs_of(p)
+        out = np.zeros(mbw * mbh, np.uint8)
+        self.lib.vo_fast_transform_types(C.byref(p), self._f(src), self._f(pred), out.ctypes.data)
+        return out
 
     def reconstruct(self, p, pred, levels, type_mask, block_types):
         h, w = p.height, p.width
@@ -304,6 +311,7 @@ class Reference:
         L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_loop_filter_i.argtypes = [vp, vp]
         L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.ref_fast_transform_types.argtypes = [vp, vp, vp, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
         L.ref_bench_analysis.restype = u64
@@ -408,6 +416,12 @@ class Reference:
         v = np.zeros_like(u)
         self.lib.ref_frame_read(f.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
         return y, u, v
+
+    def fast_transform_types(self, src, pred):
+        mbw, mbh = mbs_of(self.p)
+        out = np.zeros(mbw * mbh, np.uint8)
+        self.lib.ref_fast_transform_types(self.h, self._f(src), self._f(pred), out.ctypes.data)
+        return out
 
     def reconstruct(self, pred, levels, type_mask, block_types):
         h, w = self.p.height, self.p.width

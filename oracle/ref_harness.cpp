@@ -391,6 +391,22 @@ void ref_loop_filter_p(void* h, void* frame, const vc1cu_mv* bmv, const uint8_t*
     E(h).apply_p_loop_filter(*static_cast<Frame*>(frame), b, cb, t, in, mbw, mbh);
 }
 
+// The transform type choose_transform_mb picks per MB with the throughput preset
+// (fast_transform_rdo, variable transforms, trellis 0, no DQUANT).
+void ref_fast_transform_types(void* h, void* src, void* pred, uint8_t* types) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.fast_transform_rdo = true;
+    c.variable_transforms = true;
+    c.trellis = 0;
+    c.dquant = false;
+    Vc1Encoder enc(c);
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx)
+            types[my * mbw + mx] =
+                static_cast<uint8_t>(enc.choose_transform_mb(F(src), F(pred), mx, my, 0, true, c.pqindex, false).type);
+}
+
 // The whole analyze_p_picture (qpel seed pass, seeded mode passes, sampled-RD mode
 // decision, final pass, optional fade passes). Reports the chosen mode and IC state.
 int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, int* chosen_mode, int* ic_enabled) {

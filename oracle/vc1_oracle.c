@@ -2656,3 +2656,63 @@ void vo_loop_filter_p(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v,
         }
     }
 }
+
+/* ---- transform type of the throughput preset --------------------------------------- */
+
+/* transform_metrics::scalar, transform_residual_metrics.h:29-61: residual SAD, the 4-row and
+ * 4-column inner-edge activity and the residual gradient of one MB's luma */
+static void tx_metrics(const uint8_t* src, const uint8_t* pred, int stride, int height, int mx, int my, uint64_t m[4]) {
+    m[0] = m[1] = m[2] = m[3] = 0;
+    for (int py = 0; py < 16 && my * 16 + py < height; ++py)
+        for (int px = 0; px < 16 && mx * 16 + px < stride; ++px) {
+            const int x = mx * 16 + px, y = my * 16 + py;
+            const size_t o = (size_t)y * stride + x;
+            const int r = (int)src[o] - (int)pred[o];
+            m[0] += (uint64_t)iabs(r);
+            if ((py & 7) == 4 && py > 0) m[1] += (uint64_t)iabs(r - ((int)src[o - stride] - (int)pred[o - stride]));
+            if ((px & 7) == 4 && px > 0) m[2] += (uint64_t)iabs(r - ((int)src[o - 1] - (int)pred[o - 1]));
+            if (px > 0) m[3] += (uint64_t)iabs(r - ((int)src[o - 1] - (int)pred[o - 1]));
+            if (py > 0) m[3] += (uint64_t)iabs(r - ((int)src[o - stride] - (int)pred[o - stride]));
+        }
+}
+
+/* The TransformType choose_transform_mb returns with the throughput preset (fast transform RDO,
+ * variable transforms, trellis 0, no DQUANT; encoder_transform.cpp:1605-1712): the candidate
+ * list of the residual metrics (split shapes at a cropped raster edge), then the preset's pick. */
+void vo_fast_transform_types(const vc1cu_params* p, const vo_frame* src, const vo_frame* pred, uint8_t* types) {
+    const int mbw = mbw_of(p), mbh = mbh_of(p), mquant = p->pqindex;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            uint64_t m[4];
+            tx_metrics(src->y, pred->y, p->width, p->height, mx, my, m);
+            const uint64_t sad = m[0], hedge = m[1], vedge = m[2], grad = m[3];
+            int list[4] = {1, 1, 1, 1}, count = 0;
+            const int split_x = mx == mbw - 1 && (p->width & 15) != 0;
+            const int split_y = my == mbh - 1 && (p->height & 15) != 0;
+            if (split_x && split_y) {
+                list[count++] = 4;
+            } else if (split_x) {
+                list[count++] = 3;
+                if (sad > (uint64_t)(64 * mquant) && grad > sad * 2) list[count++] = 4;
+            } else if (split_y) {
+                list[count++] = 2;
+                if (sad > (uint64_t)(64 * mquant) && grad > sad * 2) list[count++] = 4;
+            } else {
+                list[count++] = 1;
+                if (sad > (uint64_t)(64 * mquant)) {
+                    if (hedge * 5 > vedge * 6) list[count++] = 2;
+                    else if (vedge * 5 > hedge * 6) list[count++] = 3;
+                    else { list[count++] = 2; list[count++] = 3; }
+                    if (count < 4 && grad > sad * 2) list[count++] = 4;
+                }
+            }
+            int chosen = list[0];
+            if (count > 1) {
+                int index = count - 1;
+                if (list[index] == 4 && grad * 2 <= sad * 5) --index;
+                chosen = list[index];
+                if (chosen == 3 && index > 0 && list[index - 1] == 2 && hedge >= vedge) chosen = 2;
+            }
+            types[(size_t)my * mbw + mx] = (uint8_t)chosen;
+        }
+}

@@ -116,6 +116,9 @@ void vo_loop_filter_i(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v)
 void vo_loop_filter_p(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v, const vc1cu_mv* block_mvs,
                       const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
 
+/* the throughput preset's transform type per MB (TransformType 1..4) */
+void vo_fast_transform_types(const vc1cu_params* p, const vo_frame* src, const vo_frame* pred, uint8_t* types);
+
 /* x87 extended-precision score emulation used by the GPU path, exposed for checking:
  * the long double value of sad + lambda*rate, as an integer scaled by 2^shift
  * (see vo_score_key in vc1_oracle.c). */

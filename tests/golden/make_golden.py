@@ -22,6 +22,9 @@ script calls it through oracle.Reference on inputs restated from the reference's
   lf_kat.npz        the reference's apply_i_like_loop_filter and apply_p_loop_filter of blocky
                     seeded pictures with seeded coded-block metadata (tests/lf_cases.py), at
                     four PQINDEX values, dense 4-MV and 1-MV fields
+  tt_kat.npz        the transform type choose_transform_mb picks with the throughput preset for
+                    noisy seeded pictures against a quarter-pel prediction (cropped rasters
+                    included, every type reached)
   scene_kat.npz     scene_change_score on seeded pictures: motion, a cut (two thresholds),
                     a fade with and without fade compensation, two camera zooms that the
                     local-motion fit rescues, and search range 0
@@ -265,6 +268,29 @@ def make_lf_kat():
     np.savez_compressed(os.path.join(HERE, "lf_kat.npz"), **d)
 
 
+TT_CASES = ((98, 66, 1, 4, 30), (130, 98, 2, 12, 8), (322, 242, 4, 6, 25), (16, 16, 5, 1, 60), (354, 290, 6, 3, 50),
+            (98, 66, 7, 10, 0))
+
+
+def make_tt_kat():
+    from oracle import Oracle, Reference
+
+    d = {}
+    for i, (w, h, seed, pq, noise) in enumerate(TT_CASES):
+        clip = synth.generate(w, h, 2, seed)
+        p = make_params(w, h, search_range=8, local_search_range=8, pqindex=pq)
+        R = Reference(p)
+        cur, ref = clip.frame(1), clip.frame(0)
+        rng = np.random.default_rng(seed)
+        cur = tuple(np.clip(pl.astype(int) + rng.integers(-noise, noise + 1, pl.shape), 0, 255).astype(np.uint8)
+                    for pl in cur)
+        q = R.analyze_p_core(R.frame(cur), R.frame(ref), MV_QPEL, False)
+        pred = R.motion_compensate(R.frame(ref), q, MV_QPEL)
+        d[f"c{i}.cur"], d[f"c{i}.pred"] = cur[0], pred[0]
+        d[f"c{i}.types"] = R.fast_transform_types(R.frame(cur), R.frame(pred))
+    np.savez_compressed(os.path.join(HERE, "tt_kat.npz"), **d)
+
+
 def make_scene_kat():
     from oracle import Reference
 
@@ -283,7 +309,7 @@ def main(only=()):
     if only:
         for name in only:
             {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat,
-             "recon_kat": make_recon_kat, "lf_kat": make_lf_kat}[name]()
+             "recon_kat": make_recon_kat, "lf_kat": make_lf_kat, "tt_kat": make_tt_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -404,6 +430,7 @@ def main(only=()):
     make_scene_kat()
     make_recon_kat()
     make_lf_kat()
+    make_tt_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -422,3 +422,22 @@ def test_loop_filter_matches_reference_live(oracle, seed):
     meta = metadata(w, h, seed, dense=seed % 2 == 0)
     for x, y in zip(oracle.loop_filter(p, fr, *meta), R.loop_filter(fr, *meta)):
         assert np.array_equal(x, y)
+
+
+# ---- transform type of the throughput preset (choose_transform_mb, fast transform RDO) ----
+
+TT_CASES = ((98, 66, 4), (130, 98, 12), (322, 242, 6), (16, 16, 1), (354, 290, 3), (98, 66, 10))
+
+
+@pytest.mark.parametrize("i", range(len(TT_CASES)))
+def test_fast_transform_types_golden(oracle, i):
+    g = load("tt_kat.npz")
+    w, h, pq = TT_CASES[i]
+    p = make_params(w, h, search_range=8, local_search_range=8, pqindex=pq)
+    got = oracle.fast_transform_types(p, planes(g[f"c{i}.cur"]), planes(g[f"c{i}.pred"]))
+    assert np.array_equal(got, g[f"c{i}.types"])
+
+
+def test_fast_transform_fixture_reaches_every_type():
+    g = load("tt_kat.npz")
+    assert set(np.concatenate([g[f"c{i}.types"] for i in range(len(TT_CASES))]).tolist()) == {1, 2, 3, 4}
