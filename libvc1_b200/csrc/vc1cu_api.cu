@@ -560,7 +560,8 @@ int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1
 }
 
 // Launches a batch of independent core passes (global search first for unseeded ones).
-int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n) {
+// globals_ready: the unseeded passes' global translation results are already in their slots.
+int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false) {
     DevParams P;
     std::string why;
     int rc = make_dev_params(p, P, why);
@@ -635,12 +636,12 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         }
     }
     // global translation search of the unseeded passes (none at --search-range 0)
-    if (!unseeded.empty() && P.range == 0)
+    if (!globals_ready && !unseeded.empty() && P.range == 0)
         for (int k : unseeded) {
             ck(cudaMemsetAsync(h[k].out.global, 0, 8, c->stream), "cudaMemsetAsync(global)");
             ck(cudaMemsetAsync(h[k].out.gsad, 0, 8, c->stream), "cudaMemsetAsync(global)");
         }
-    if (!unseeded.empty() && P.range > 0) {
+    if (!globals_ready && !unseeded.empty() && P.range > 0) {
         const int nu = (int)unseeded.size();
         const size_t gb = gstate_bytes();
         if (c->gstates_cap < nu) {
@@ -784,7 +785,76 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
         }
         groups[g].push_back(passes[i]);
     }
-    for (const auto& g : groups) launch_group(c, p, g.data(), (int)g.size());
+    // The global translation search depends only on (cur, ref) at the call's range, so passes of
+    // one picture pair in different groups (a B picture's quarter-pel and bilinear passes) share
+    // one search, as the reference shares it through BSearchReuse (encoder_motion.cpp:90-95).
+    DevParams P;
+    std::string why;
+    const int rc = make_dev_params(p, P, why);
+    if (rc) throw Fail{rc, why};
+    const int mbs = P.mbw * P.mbh;
+    std::vector<int> first_of;  // per unseeded pass: index of the pass whose search it reuses
+    std::vector<int> un;
+    for (int i = 0; i < n; ++i) {
+        if (passes[i].seed_slot >= 0) continue;
+        int f = i;
+        for (int j : un)
+            if (passes[j].cur_id == passes[i].cur_id && passes[j].ref_id == passes[i].ref_id) {
+                f = j;
+                break;
+            }
+        if (f == i) un.push_back(i);
+        first_of.push_back(f);
+    }
+    std::vector<int> unseeded_idx;
+    for (int i = 0; i < n; ++i)
+        if (passes[i].seed_slot < 0) unseeded_idx.push_back(i);
+    if (!un.empty()) {
+        std::vector<DevResult*> outs(n, nullptr);
+        for (int i : unseeded_idx) outs[i] = &result_slot(c, passes[i].out_slot, mbs, true).r;
+        if (P.range == 0) {
+            for (int i : unseeded_idx) {
+                ck(cudaMemsetAsync(outs[i]->global, 0, 8, c->stream), "cudaMemsetAsync(global)");
+                ck(cudaMemsetAsync(outs[i]->gsad, 0, 8, c->stream), "cudaMemsetAsync(global)");
+            }
+        } else {
+            const int nu = (int)un.size();
+            const size_t gb = gstate_bytes();
+            if (c->gstates_cap < nu) {
+                if (c->d_gstates) cudaFree(c->d_gstates);
+                c->d_gstates = nullptr;
+                c->gstates_cap = 0;
+                void* d = nullptr;
+                ck(cudaMalloc(&d, gb * nu), "cudaMalloc(global search state)");
+                c->d_gstates = static_cast<GState*>(d);
+                c->gstates_cap = nu;
+            }
+            uint8_t* hs = static_cast<uint8_t*>(staging(c, gb * nu));
+            const int grange = std::min(P.local_range, 32);
+            for (int k = 0; k < nu; ++k) {
+                const vc1cu_pass& q = passes[un[k]];
+                FrameSlot& fc = frame_slot(c, q.cur_id);
+                FrameSlot& fr = frame_slot(c, q.ref_id);
+                if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+                    throw Fail{VC1CU_ERR_ARG, "P-picture reference dimensions do not match the configuration"};
+                init_gstate(reinterpret_cast<GState*>(hs + gb * k), fc.view(), fr.view(), grange, outs[un[k]]->global,
+                            outs[un[k]]->gsad);
+            }
+            ck(cudaMemcpyAsync(c->d_gstates, hs, gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
+            ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+            Timer tm(c, kGlobal);
+            const int launches = run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
+            ck(cudaGetLastError(), "global search launch");
+            tm.stop(launches);
+            for (size_t k = 0; k < unseeded_idx.size(); ++k) {
+                const int i = unseeded_idx[k], f = first_of[k];
+                if (f == i) continue;
+                ck(cudaMemcpyAsync(outs[i]->global, outs[f]->global, 8, cudaMemcpyDeviceToDevice, c->stream), "copy global");
+                ck(cudaMemcpyAsync(outs[i]->gsad, outs[f]->gsad, 8, cudaMemcpyDeviceToDevice, c->stream), "copy global");
+            }
+        }
+    }
+    for (const auto& g : groups) launch_group(c, p, g.data(), (int)g.size(), true);
     return VC1CU_OK;
 }
 
