@@ -166,10 +166,12 @@ class Runner:
                 y, u, v = pinned[f]
                 self.ctx.upload_frame_ptr(f, y.data_ptr(), u.data_ptr(), v.data_ptr(), W, H)
 
-    def step(self, levels=None):
-        """Enqueues one step on the library's stream; levels go to `levels` (default self.levels)."""
+    def step(self, levels=None, mark=None):
+        """Enqueues one step on the library's stream; levels go to `levels` (default self.levels).
+        mark(stage), when given, is called after each stage (to record a timing event)."""
         levels = self.levels if levels is None else levels
         c, pics = self.ctx, self.pics
+        mark = mark or (lambda stage: None)
         # every P picture's quarter-pel seed pass and the four unseeded core passes of every B
         # picture (forward / backward in quarter-pel and in half-pel bilinear mode); the library
         # runs one launch per pass kind
@@ -177,25 +179,31 @@ class Runner:
                       [(t, ref, m, 0, -1, 3100 + 4 * k + 2 * (m == self.BIL) + (ref == fut), pq)
                        for k, (t, past, fut, _n, _d, pq, _a) in enumerate(self.bpics)
                        for m in (self.QPEL, self.BIL) for ref in (past, fut)])
+        mark("unseeded passes")
         # the three seeded mode passes of every picture (the library runs one launch per mode)
         c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
                                 for m in self.modes])
+        mark("seeded mode passes")
         # the final pass (after the host's mode decision over whole passes)
         c.core_passes(self.p0, [(t, r, self.MIXED, 1, 2000 + 4 * i + self.MIXED, 3000 + i, pq)
                                 for i, (t, r, pq) in enumerate(pics)])
+        mark("final passes")
         for i, (t, r, pq) in enumerate(pics):
             p = params(pq)
             c.motion_compensate(p, r, 3000 + i, self.MIXED, 3500 + i)
             c.forward_quant_device(p, t, 3500 + i, 15, 0, levels[i].data_ptr())
+        mark("prediction + transform")
         # the B decisions of both modes against the future anchor's final pass
         if self.bpics:
             c.b_decide(self.p0, [(t, past, fut, 3100 + 4 * k + 2 * j, 3101 + 4 * k + 2 * j, 3000 + a, num, den, m,
                                   2 * k + j, pq)
                                  for k, (t, past, fut, num, den, pq, a) in enumerate(self.bpics)
                                  for j, m in enumerate((self.QPEL, self.BIL))])
+        mark("B decisions")
         # the fade estimate analyze_p_picture runs on its final pass when fade compensation is on
         # (the default; encoder_motion.cpp:570-573); it waits for the step's device work
         self.ic = c.estimate_intensity_batch(self.p0, [(t, r, 3000 + i) for i, (t, r, pq) in enumerate(pics)])
+        mark("fade estimates")
 
     def read_results(self):
         """D2H of every P picture's final-pass analysis and every B analysis (waits for the step)."""
@@ -243,15 +251,27 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     step_ms = []
+    stage_ms = {}
     for _ in range(args.steps):
         flush_l2(torch, l2)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
+        marks = []
+
+        def mark(stage):
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(ext)
+            marks.append((stage, e))
+
         a.record(ext)
-        run.step()
+        run.step(mark=mark)
         b.record(ext)
         b.synchronize()
         step_ms.append(a.elapsed_time(b))
+        prev = a
+        for stage, e in marks:
+            stage_ms[stage] = stage_ms.get(stage, 0.0) + prev.elapsed_time(e)
+            prev = e
     ctx.synchronize()
     torch.cuda.synchronize()
     if sampler:
@@ -344,6 +364,13 @@ def run_ours(args, rank, world, device):
                          "core_ms_per_launch": round(core_ms / core_launches, 3),
                          "traffic": round(CORE_DRAM_BYTES_PER_LAUNCH) if args.gops is None else None,
                          "traffic_unit": "DRAM bytes per launch (ncu, first GOP scaled by macroblocks)"},
+            "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage_ms.items()},
+            "pass_mb_per_s": {
+                "unseeded (P seed + B forward/backward)": round((len(run.pics) + 4 * len(run.bpics)) * MBS * args.steps
+                                                              / (stage_ms["unseeded passes"] * 1e-3), 1),
+                "seeded mode passes": round(3 * len(run.pics) * MBS * args.steps / (stage_ms["seeded mode passes"] * 1e-3), 1),
+                "final Mixed-MV + intra": round(len(run.pics) * MBS * args.steps / (stage_ms["final passes"] * 1e-3), 1),
+            } if stage_ms else None,
             "kernel_ms_per_step": {k: round(timing[k] / args.steps, 3)
                                    for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms", "ic_ms")},
             "xform_roofline": {"bound": "fp64", "achieved_gflops": round(xform_flops / (xform_ms * 1e-3) / 1e9, 1)
@@ -394,8 +421,21 @@ def cpu_baseline(args, clip):
     anyref, pjobs, bjobs = reference_jobs(clip)
     threads = min(len(pjobs) + len(bjobs), cores)
     ns = anyref.bench_gop_multi(pjobs, bjobs, threads)
-    return {"value": round((len(pjobs) + len(bjobs)) * MBS / (ns * 1e-9), 1), "unit": UNIT, "cores": threads,
-            "kind": "reference", "sample": REF_SAMPLE}
+    out = {"value": round((len(pjobs) + len(bjobs)) * MBS / (ns * 1e-9), 1), "unit": UNIT, "cores": threads,
+           "kind": "reference", "sample": REF_SAMPLE}
+    # one core: the first P picture and the first B picture anchored on it, with the SIMD dispatch
+    # on and with the scalar path (the reference's parity configuration)
+    from oracle import Reference
+
+    one = {}
+    for name, simd in (("simd_auto", True), ("simd_none", False)):
+        R = Reference(params(pjobs[0][0].p.pqindex), simd_auto=simd)
+        pj = [(R, pjobs[0][1], pjobs[0][2])]
+        bj = [(R,) + tuple(bjobs[0][1:])]
+        ns1 = R.bench_gop_multi(pj, bj, 1)
+        one[name] = round(2 * MBS / (ns1 * 1e-9), 1)
+    out["one_thread"] = dict(one, sample="P picture 3 and B picture 1 of the clip on one host thread")
+    return out
 
 
 def run_reference(args, rank, world):
