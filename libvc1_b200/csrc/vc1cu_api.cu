@@ -99,6 +99,9 @@ struct Fail {
 };
 
 inline void ck(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    // reset the runtime's last error, so a later launch check does not report this one again
+    (void)cudaGetLastError();
     if (e == cudaErrorMemoryAllocation) throw Fail{VC1CU_ERR_OOM, std::string(what) + ": out of device memory"};
     if (e != cudaSuccess) throw Fail{VC1CU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
@@ -1020,10 +1023,6 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
     }
     if (c->bdescs_cap < n) {
         if (c->d_bdescs) cudaFree(c->d_bdescs);
-    if (c->d_ic) cudaFree(c->d_ic);
-    if (c->d_btypes) cudaFree(c->d_btypes);
-    if (c->d_lf) cudaFree(c->d_lf);
-    if (c->d_icdesc) cudaFree(c->d_icdesc);
         c->d_bdescs = nullptr;
         c->bdescs_cap = 0;
         void* d = nullptr;
@@ -1300,6 +1299,10 @@ int vc1cu_close(vc1cu_ctx* c) {
     for (auto& kv : c->bresults)
         if (kv.second.d) cudaFree(kv.second.d);
     if (c->d_bdescs) cudaFree(c->d_bdescs);
+    if (c->d_ic) cudaFree(c->d_ic);
+    if (c->d_icdesc) cudaFree(c->d_icdesc);
+    if (c->d_btypes) cudaFree(c->d_btypes);
+    if (c->d_lf) cudaFree(c->d_lf);
     for (auto& s : c->cache)
         if (s.d) cudaFree(s.d);
     if (c->d_status) cudaFree(c->d_status);
