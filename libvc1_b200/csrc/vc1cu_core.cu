@@ -2029,8 +2029,24 @@ __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
 
 int warp_bytes_for_host(const WinCfg& wc) { return warp_bytes_for(wc); }
 
+// 16 bytes from global to shared memory without a register round trip (cp.async; both
+// addresses 16-byte aligned). The copy lands by the next window_wait().
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+// Completes this thread's cp.async copies; the warp barrier makes every lane's copies
+// visible to the whole warp.
+__device__ __forceinline__ void window_wait() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+}
+
 // Stages the reference window around MV (cdx, cdy) integer pixels: rows wy0 .. wy0+wh-1,
-// columns from the 16-byte-aligned wx0, as 128-bit loads (edge chunks clamp per byte).
+// columns from the 16-byte-aligned wx0. Chunks inside the raster are asynchronous 16-byte
+// copies (all of a lane's in flight at once) that land at the next window_wait(); edge
+// chunks clamp per byte and are stored at once.
 __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int cdx, int cdy, const WinCfg& wc) {
     m.wh = wc.wh;
     m.wp = wc.wp;
@@ -2043,9 +2059,9 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
         const int r = j / cpr, c = j - r * cpr;
         const int gy = iclamp(m.wy0 + r, 0, P.H - 1), gx = m.wx0 + 16 * c;
         const uint8_t* row = ref.y + (size_t)gy * ref.pitch_y;
-        uint4 v;
+        uint8_t* dst = m.sm.win.get() + r * m.wp + 16 * c;
         if (gx >= 0 && gx + 16 <= P.W) {
-            v = __ldg(reinterpret_cast<const uint4*>(row + gx));
+            cp_async16(dst, row + gx);
         } else {
             uint32_t w[4];
 #pragma unroll
@@ -2055,11 +2071,9 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
                 for (int i = 0; i < 4; ++i) x |= (uint32_t)__ldg(row + iclamp(gx + 4 * k + i, 0, P.W - 1)) << (8 * i);
                 w[k] = x;
             }
-            v = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-        *reinterpret_cast<uint4*>(m.sm.win.get() + r * m.wp + 16 * c) = v;
     }
-    __syncwarp();
 }
 
 // Current MB into shared memory (zero outside the raster) plus its packed column subsets.
@@ -2211,6 +2225,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
                 publish_ctx(P, m);
+                window_wait();
                 PHASE_MARK(2);
                 sl = refine_prepare_ool(m.sm.ctx.off, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
                 PHASE_MARK(3);
@@ -2263,7 +2278,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         }
         // ---- wavefront: left, top-left, top, top-right of the same pass ----
         if (ok) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st, code);
-        __syncwarp();
+        window_wait();  // an unseeded pass's window copies (none pending otherwise)
         PHASE_MARK(5);
         if (ok) {
             load_neighbours(P, m, o);
