@@ -473,6 +473,32 @@ int vc1cu_loop_filter_i(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id);
 int vc1cu_loop_filter_p(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
                         const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
 
+/*
+ * Overlap smoothing of a signed (unclamped, unbiased) reconstruction in place:
+ * apply_overlap_plane_signed (src/encoder_filter.cpp:217-243) on each plane, as
+ * Vc1Encoder::apply_i_overlap (:344-352) and apply_p_overlap (:354-365) call it. d_y, d_u, d_v
+ * are DEVICE int32 planes of the padded raster, (mbh*16) x (mbw*16) luma and half that chroma,
+ * rows packed (pitch = width). First every vertical 8x8 edge (4 samples across it, rows by
+ * 8-row segment), then every horizontal edge, each enabled when all != 0 (CONDOVER ALL) or by
+ * the HOST per-macroblock flags[mbw*mbh] (OVERFLAGS: an edge inside a macroblock needs its flag,
+ * an edge between two needs both; apply_p_overlap passes the intra map). flags may be NULL when
+ * all != 0. The picture-level condition (apply_p_overlap: OVERLAP on and PQINDEX >= 9; the I
+ * plan's mode) stays with the caller. Returns once the flags are copied.
+ */
+int vc1cu_overlap_smooth(vc1cu_ctx* ctx, const vc1cu_params* p, int32_t* d_y, int32_t* d_u, int32_t* d_v,
+                         const uint8_t* flags, int all);
+
+/*
+ * Stores a signed padded reconstruction (the planes of vc1cu_overlap_smooth) as 8-bit samples
+ * clamp(s + bias, 0, 255) into frame slot out_id (src/encoder_filter.cpp reconstruct_i_picture_padded's
+ * store, and the intra write-back after apply_p_overlap, src/encoder_encode.cpp:1425-1449). With
+ * mb_mask NULL the slot becomes the whole padded raster ((mbw*16) x (mbh*16)); with a HOST
+ * mb_mask[mbw*mbh] only the flagged macroblocks are written, into an existing slot (its samples
+ * outside the slot's size are skipped). Returns once the mask is copied.
+ */
+int vc1cu_store_signed(vc1cu_ctx* ctx, const vc1cu_params* p, const int32_t* d_y, const int32_t* d_u,
+                       const int32_t* d_v, int bias, const uint8_t* mb_mask, int out_id);
+
 /* ---- allocation-free whole-frame translation search ------------------------------ */
 
 /*

@@ -36,7 +36,8 @@ EXPORTS = (
     "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
-    "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_fast_transform_types",
+    "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
+    "vc1cu_fast_transform_types",
 )
 
 
@@ -93,6 +94,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_loop_filter_i.argtypes = [vp, PP, i32]
     L.vc1cu_fast_transform_types.argtypes = [vp, PP, i32, i32, vp]
     L.vc1cu_loop_filter_p.argtypes = [vp, PP, i32, vp, vp, vp, vp]
+    L.vc1cu_overlap_smooth.argtypes = [vp, PP, vp, vp, vp, vp, i32]
+    L.vc1cu_store_signed.argtypes = [vp, PP, vp, vp, vp, i32, vp, i32]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
@@ -354,6 +357,20 @@ class CudaComputeContext:
         cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
         self._check(self._L.vc1cu_loop_filter_p(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data,
                                                 t.ctypes.data, i.ctypes.data))
+
+    def overlap_smooth(self, params: Params, d_y: int, d_u: int, d_v: int, flags=None, all_edges: bool = False):
+        """In-place overlap smoothing of DEVICE int32 signed planes (padded raster, rows packed):
+        every 8x8 edge when all_edges, else the edges the per-MB flags enable."""
+        f = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        self._check(self._L.vc1cu_overlap_smooth(self._h, C.byref(params), d_y, d_u, d_v,
+                                                 None if f is None else f.ctypes.data, int(all_edges)))
+
+    def store_signed(self, params: Params, d_y: int, d_u: int, d_v: int, bias: int, out_id: int, mask=None):
+        """Frame slot out_id = clamp(s + bias) of DEVICE int32 signed planes: the whole padded
+        raster, or with a per-MB mask only those macroblocks of an existing slot."""
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self._check(self._L.vc1cu_store_signed(self._h, C.byref(params), d_y, d_u, d_v, int(bias),
+                                               None if m is None else m.ctypes.data, out_id))
 
     def reconstruct(self, params: Params, pred_id: int, d_levels: int, type_mask: int, block_types, out_id: int):
         """Frame slot out_id = pred_id + the inverse-transformed levels of each block's type

@@ -50,6 +50,11 @@ cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y
 cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
                                  cudaStream_t s);
+cudaError_t launch_overlap(int32_t* y, int32_t* u, int32_t* v, int mbw, int mbh, const uint8_t* d_flags, int all,
+                           cudaStream_t s);
+cudaError_t launch_store_signed(const int32_t* y, const int32_t* u, const int32_t* v, int mbw, int mbh, int bias,
+                                const uint8_t* d_mask, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c,
+                                int W, int H, cudaStream_t s);
 void launch_fast_tt(const DevParams& P, const DevFrame& src, const DevFrame& pred, uint8_t* types, cudaStream_t s);
 void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
                   uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
@@ -192,6 +197,8 @@ struct vc1cu_ctx {
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
+    void* d_ovl = nullptr;     // per-macroblock overlap flags / store mask
+    size_t ovl_cap = 0;
     size_t icdesc_cap = 0;
     GState* d_gstates = nullptr;
     int gstates_cap = 0;
@@ -1303,6 +1310,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_icdesc) cudaFree(c->d_icdesc);
     if (c->d_btypes) cudaFree(c->d_btypes);
     if (c->d_lf) cudaFree(c->d_lf);
+    if (c->d_ovl) cudaFree(c->d_ovl);
     for (auto& s : c->cache)
         if (s.d) cudaFree(s.d);
     if (c->d_status) cudaFree(c->d_status);
@@ -1822,6 +1830,52 @@ int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const
         tm.stop(2);
         // the metadata copies read the caller's pageable arrays; finish before returning
         ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        return VC1CU_OK;
+    });
+}
+
+// The per-macroblock byte map of an overlap call on the device (stream-ordered after any launch
+// still reading the previous one).
+static const uint8_t* upload_mb_map(vc1cu_ctx* c, const uint8_t* map, size_t mbs) {
+    uint8_t* d = static_cast<uint8_t*>(ensure(c->d_ovl, c->ovl_cap, mbs, "cudaMalloc(macroblock map)"));
+    ck(cudaMemcpyAsync(d, map, mbs, cudaMemcpyHostToDevice, c->stream), "upload macroblock map");
+    return d;
+}
+
+int vc1cu_overlap_smooth(vc1cu_ctx* c, const vc1cu_params* p, int32_t* d_y, int32_t* d_u, int32_t* d_v,
+                         const uint8_t* flags, int all) {
+    return guarded(c, [&]() -> int {
+        if (!d_y || !d_u || !d_v) throw Fail{VC1CU_ERR_ARG, "null signed plane"};
+        if (!all && !flags) throw Fail{VC1CU_ERR_ARG, "null overlap flags"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const uint8_t* df = all ? nullptr : upload_mb_map(c, flags, (size_t)P.mbw * P.mbh);
+        Timer tm(c, kMc);
+        ck(launch_overlap(d_y, d_u, d_v, P.mbw, P.mbh, df, all ? 1 : 0, c->stream), "overlap launch");
+        tm.stop(2);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_store_signed(vc1cu_ctx* c, const vc1cu_params* p, const int32_t* d_y, const int32_t* d_u, const int32_t* d_v,
+                       int bias, const uint8_t* mb_mask, int out_id) {
+    return guarded(c, [&]() -> int {
+        if (!d_y || !d_u || !d_v) throw Fail{VC1CU_ERR_ARG, "null signed plane"};
+        if (out_id < 0 || out_id >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "invalid output frame slot"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& f = mb_mask ? frame_slot(c, out_id) : alloc_frame(c, out_id, P.mbw * 16, P.mbh * 16);
+        const uint8_t* dm = mb_mask ? upload_mb_map(c, mb_mask, (size_t)P.mbw * P.mbh) : nullptr;
+        const DevFrame o = f.view();
+        Timer tm(c, kMc);
+        ck(launch_store_signed(d_y, d_u, d_v, P.mbw, P.mbh, bias, dm, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v,
+                               f.pitch_y, f.pitch_c, f.w, f.h, c->stream),
+           "signed store launch");
+        tm.stop(1);
         return VC1CU_OK;
     });
 }

@@ -14,6 +14,12 @@
 //   lfp_v_kernel  one thread per 4-row strip: the vertical edges, left to right.
 // The I-like filter has no order between its edges of one direction (8 pixels apart, each reads
 // 4 on either side and writes 1): one thread per 4-line group of every edge.
+//
+// Overlap smoothing (apply_overlap_plane_signed, :217-243) of a signed reconstruction: each
+// edge filter reads and writes the 2 samples on either side along one line, so the lines of
+// one direction's edges (8 apart) touch disjoint samples; one thread per line of every edge,
+// vertical edges in one launch, horizontal edges (which read the first stage's output) in a
+// second.
 #include <cuda_runtime.h>
 
 #include "vc1cu_core.cuh"
@@ -242,6 +248,141 @@ cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y
     const int nh = (W + 3) / 4 + 2 * ((W / 2 + 3) / 4), nv = (H + 3) / 4 + 2 * ((H / 2 + 3) / 4);
     lfp_h_kernel<<<(unsigned)((nh + 63) / 64), 64, 0, s>>>(f, m, pq);
     lfp_v_kernel<<<(unsigned)((nv + 63) / 64), 64, 0, s>>>(f, m, pq);
+    return cudaGetLastError();
+}
+
+// ---- overlap smoothing --------------------------------------------------------------------
+
+struct OvlPlanes {
+    int32_t* p[3];
+    int w[3], h[3];
+    const uint8_t* flags;  // per macroblock, mbw * mbh (unused when all)
+    int mbw, mbh, all;
+};
+
+// overlap_edge_enabled (encoder_filter.cpp:201-215) between 8x8 blocks (bx0, by0), (bx1, by1).
+__device__ __forceinline__ bool ovl_enabled(const OvlPlanes& o, bool luma, int bx0, int by0, int bx1, int by1) {
+    if (o.all) return true;
+    const int mx0 = luma ? bx0 >> 1 : bx0, my0 = luma ? by0 >> 1 : by0;
+    const int mx1 = luma ? bx1 >> 1 : bx1, my1 = luma ? by1 >> 1 : by1;
+    if (mx0 < 0 || my0 < 0 || mx0 >= o.mbw || my0 >= o.mbh) return false;
+    if (mx1 < 0 || my1 < 0 || mx1 >= o.mbw || my1 >= o.mbh) return false;
+    const int a = my0 * o.mbw + mx0, b = my1 * o.mbw + mx1;
+    if (a == b) return o.flags[a] != 0;
+    return o.flags[a] != 0 && o.flags[b] != 0;
+}
+
+// overlap_arshift3 (:162-164): rounds v / 8 toward minus infinity.
+__device__ __forceinline__ int ovl_shift3(int v) { return v >= 0 ? (v >> 3) : -((-v + 7) >> 3); }
+
+// The 4 samples across an edge at line parity i (overlap_vertical_edge :166-180 and
+// overlap_horizontal_edge :182-199 share it); step is the distance between the samples.
+__device__ __forceinline__ void ovl_line(int32_t* c, int step, int i) {
+    const int a = c[-2 * step], b = c[-step], cc = c[0], d = c[step];
+    const int d1 = a - d, d2 = a - d + b - cc;
+    const int r1 = (i & 1) ? 3 : 4, r2 = 7 - r1;
+    c[-2 * step] = ovl_shift3(8 * a - d1 + r1);
+    c[-step] = ovl_shift3(8 * b - d2 + r2);
+    c[0] = ovl_shift3(8 * cc + d2 + r1);
+    c[step] = ovl_shift3(8 * d + d1 + r2);
+}
+
+// Stage one: thread = (row y, vertical edge bx >= 1) of plane blockIdx.y.
+__global__ void ovl_v_kernel(OvlPlanes o) {
+    const int k = blockIdx.y;
+    const int w = o.w[k], h = o.h[k], bw = w / 8;
+    if (w < 8 || h < 8 || bw < 2) return;
+    const long n = (long)(h / 8 * 8) * (bw - 1);
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const int y = (int)(t / (bw - 1)), bx = 1 + (int)(t % (bw - 1));
+        if (!ovl_enabled(o, k == 0, bx - 1, y >> 3, bx, y >> 3)) continue;
+        ovl_line(o.p[k] + (size_t)y * w + bx * 8, 1, y & 7);
+    }
+}
+
+// Stage two: thread = (horizontal edge by >= 1, column x) of plane blockIdx.y.
+__global__ void ovl_h_kernel(OvlPlanes o) {
+    const int k = blockIdx.y;
+    const int w = o.w[k], h = o.h[k], bh = h / 8, bw = w / 8;
+    if (w < 8 || h < 8 || bh < 2) return;
+    const long n = (long)(bh - 1) * (bw * 8);
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const int by = 1 + (int)(t / (bw * 8)), x = (int)(t % (bw * 8));
+        if (!ovl_enabled(o, k == 0, x >> 3, by - 1, x >> 3, by)) continue;
+        ovl_line(o.p[k] + (size_t)(by * 8) * w + x, w, x & 7);
+    }
+}
+
+cudaError_t launch_overlap(int32_t* y, int32_t* u, int32_t* v, int mbw, int mbh, const uint8_t* d_flags, int all,
+                           cudaStream_t s) {
+    OvlPlanes o;
+    o.p[0] = y;
+    o.p[1] = u;
+    o.p[2] = v;
+    o.w[0] = mbw * 16;
+    o.h[0] = mbh * 16;
+    o.w[1] = o.w[2] = mbw * 8;
+    o.h[1] = o.h[2] = mbh * 8;
+    o.flags = d_flags;
+    o.mbw = mbw;
+    o.mbh = mbh;
+    o.all = all;
+    const long lines = (long)o.w[0] * o.h[0] / 8;  // edges per 8 samples, the most of any plane and stage
+    const unsigned blocks = (unsigned)imin(4096, (int)((lines + 255) / 256));
+    ovl_v_kernel<<<dim3(blocks, 3), 256, 0, s>>>(o);
+    ovl_h_kernel<<<dim3(blocks, 3), 256, 0, s>>>(o);
+    return cudaGetLastError();
+}
+
+// clamp(s + bias) of the padded signed planes into a frame (its visible w x h), all macroblocks
+// or the flagged ones; thread = 4 samples of a row.
+struct StoreArgs {
+    const int32_t* s[3];
+    uint8_t* d[3];
+    int sw[3], dpitch[3], dw[3], dh[3];
+    const uint8_t* mask;
+    int mbw, bias;
+};
+
+__global__ void store_signed_kernel(StoreArgs a) {
+    const int k = blockIdx.y;
+    const int w = imin(a.sw[k], a.dw[k]), h = a.dh[k];
+    const int shift = k == 0 ? 4 : 3;
+    const int q = (w + 3) / 4;
+    const long n = (long)q * h;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const int y = (int)(t / q), x0 = (int)(t % q) * 4;
+        if (a.mask && !a.mask[(y >> shift) * a.mbw + (x0 >> shift)]) continue;
+        const int32_t* src = a.s[k] + (size_t)y * a.sw[k];
+        uint8_t* dst = a.d[k] + (size_t)y * a.dpitch[k];
+        for (int x = x0; x < x0 + 4 && x < w; ++x) dst[x] = (uint8_t)iclamp(src[x] + a.bias, 0, 255);
+    }
+}
+
+cudaError_t launch_store_signed(const int32_t* y, const int32_t* u, const int32_t* v, int mbw, int mbh, int bias,
+                                const uint8_t* d_mask, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c,
+                                int W, int H, cudaStream_t s) {
+    StoreArgs a;
+    a.s[0] = y;
+    a.s[1] = u;
+    a.s[2] = v;
+    a.d[0] = dy;
+    a.d[1] = du;
+    a.d[2] = dv;
+    a.sw[0] = mbw * 16;
+    a.sw[1] = a.sw[2] = mbw * 8;
+    a.dpitch[0] = pitch_y;
+    a.dpitch[1] = a.dpitch[2] = pitch_c;
+    a.dw[0] = W;
+    a.dw[1] = a.dw[2] = W / 2;
+    a.dh[0] = imin(H, mbh * 16);
+    a.dh[1] = a.dh[2] = imin(H / 2, mbh * 8);
+    a.mask = d_mask;
+    a.mbw = mbw;
+    a.bias = bias;
+    const long n = (long)((imin(W, mbw * 16) + 3) / 4) * imin(H, mbh * 16);
+    const unsigned blocks = (unsigned)imax(1, imin(4096, (int)((n + 255) / 256)));
+    store_signed_kernel<<<dim3(blocks, 3), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

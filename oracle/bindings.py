@@ -82,6 +82,8 @@ class Oracle:
         L.vo_reconstruct.argtypes = [P, vp, vp, i32, vp, vp, vp, vp]
         L.vo_loop_filter_i.argtypes = [P, vp, vp, vp]
         L.vo_loop_filter_p.argtypes = [P, vp, vp, vp, vp, vp, vp, vp]
+        L.vo_overlap_smooth.argtypes = [i32, i32, vp, vp, vp, vp, i32]
+        L.vo_store_signed.argtypes = [i32, i32, vp, vp, vp, i32, vp, i32, i32, vp, vp, vp]
         L.vo_fast_transform_types.argtypes = [P, vp, vp, vp]
         L.vo_analyze_b.argtypes = [P, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.vo_b_costs.argtypes = [P, vp, vp, vp, i32, i32, Mv, Mv, Mv, Mv, i32, vp]
@@ -189,6 +191,32 @@ class Oracle:
             cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
             self.lib.vo_loop_filter_p(C.byref(p), y.ctypes.data, u.ctypes.data, v.ctypes.data, b.ctypes.data,
                                       cb.ctypes.data, t.ctypes.data, i.ctypes.data)
+        return y, u, v
+
+    def overlap_smooth(self, p, planes, flags=None, all_edges=False):
+        """Overlap-smoothed copies of a signed padded reconstruction (int32 planes
+        (mbh*16, mbw*16), (mbh*8, mbw*8) x 2); flags per MB, or all_edges."""
+        mbw, mbh = mbs_of(p)
+        y, u, v = (np.array(a, np.int32, copy=True, order="C") for a in planes)
+        f = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        self.lib.vo_overlap_smooth(mbw, mbh, y.ctypes.data, u.ctypes.data, v.ctypes.data,
+                                   None if f is None else f.ctypes.data, int(all_edges))
+        return y, u, v
+
+    def store_signed(self, p, planes, bias, mask=None, into=None):
+        """clamp(s + bias) of the signed planes: the padded raster when into is None, else written
+        over a copy of the frame `into` (masked MBs only when mask is given)."""
+        mbw, mbh = mbs_of(p)
+        sy, su, sv = (np.ascontiguousarray(a, np.int32) for a in planes)
+        if into is None:
+            y = np.zeros((mbh * 16, mbw * 16), np.uint8)
+            u, v = np.zeros((mbh * 8, mbw * 8), np.uint8), np.zeros((mbh * 8, mbw * 8), np.uint8)
+        else:
+            y, u, v = (np.array(a, np.uint8, copy=True) for a in _planes(into))
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.lib.vo_store_signed(mbw, mbh, sy.ctypes.data, su.ctypes.data, sv.ctypes.data, int(bias),
+                                 None if m is None else m.ctypes.data, y.shape[1], y.shape[0], y.ctypes.data,
+                                 u.ctypes.data, v.ctypes.data)
         return y, u, v
 
     def fast_transform_types(self, p, src, pred):
@@ -311,6 +339,7 @@ class Reference:
         L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_loop_filter_i.argtypes = [vp, vp]
         L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.ref_overlap.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
         L.ref_fast_transform_types.argtypes = [vp, vp, vp, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
         L.ref_bench_analysis.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i32, i32]
@@ -415,6 +444,15 @@ class Reference:
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)
         self.lib.ref_frame_read(f.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def overlap(self, planes, mode=1, flags=None, p_picture=False):
+        """apply_i_overlap with plan mode (0 None, 1 All, 2 Select with flags), or with p_picture
+        apply_p_overlap with flags as the intra map, on copies of the signed padded planes."""
+        y, u, v = (np.array(a, np.int32, copy=True, order="C") for a in planes)
+        f = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        self.lib.ref_overlap(self.h, int(p_picture), int(mode), None if f is None else f.ctypes.data, y.ctypes.data,
+                             u.ctypes.data, v.ctypes.data)
         return y, u, v
 
     def fast_transform_types(self, src, pred):

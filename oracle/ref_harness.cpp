@@ -391,6 +391,36 @@ void ref_loop_filter_p(void* h, void* frame, const vc1cu_mv* bmv, const uint8_t*
     E(h).apply_p_loop_filter(*static_cast<Frame*>(frame), b, cb, t, in, mbw, mbh);
 }
 
+// Vc1Encoder::apply_i_overlap (mode 0 None, 1 All, 2 Select with flags) or, with p_picture set,
+// apply_p_overlap (flags = the intra map; OVERLAP on), on a signed padded frame held as int32
+// planes (in place).
+void ref_overlap(void* h, int p_picture, int mode, const uint8_t* flags, int32_t* y, int32_t* u, int32_t* v) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.overlap = true;
+    Vc1Encoder enc(c);
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const size_t mbs = static_cast<size_t>(mbw) * mbh;
+    Vc1Encoder::SignedFrame f;
+    f.width = mbw * 16;
+    f.height = mbh * 16;
+    const size_t ny = static_cast<size_t>(f.width) * f.height, nc = ny / 4;
+    f.y.assign(y, y + ny);
+    f.u.assign(u, u + nc);
+    f.v.assign(v, v + nc);
+    if (p_picture) {
+        enc.apply_p_overlap(f, std::vector<uint8_t>(flags, flags + mbs), mbw, mbh);
+    } else {
+        Vc1Encoder::OverlapPlan plan;
+        plan.mode = static_cast<Vc1Encoder::OverlapMode>(mode);
+        plan.flags.assign(mbs, 0);
+        if (flags) plan.flags.assign(flags, flags + mbs);
+        enc.apply_i_overlap(f, plan);
+    }
+    std::copy(f.y.begin(), f.y.end(), y);
+    std::copy(f.u.begin(), f.u.end(), u);
+    std::copy(f.v.begin(), f.v.end(), v);
+}
+
 // The transform type choose_transform_mb picks per MB with the throughput preset
 // (fast_transform_rdo, variable transforms, trellis 0, no DQUANT).
 void ref_fast_transform_types(void* h, void* src, void* pred, uint8_t* types) {

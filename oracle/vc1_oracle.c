@@ -2532,6 +2532,72 @@ static void lf_edge(uint8_t* p, int w, int h, int x, int y, int adx, int ady, in
 static void lf_hborder(uint8_t* p, int w, int h, int x, int y, int len, int pq) { lf_edge(p, w, h, x, y, 1, 0, 0, 1, len, pq); }
 static void lf_vborder(uint8_t* p, int w, int h, int x, int y, int len, int pq) { lf_edge(p, w, h, x, y, 0, 1, 1, 0, len, pq); }
 
+/* overlap_arshift3, encoder_filter.cpp:162-164 */
+static int ovl_arshift3(int v) { return v >= 0 ? (v >> 3) : -((-v + 7) >> 3); }
+
+/* the four samples across one edge along one line, at line parity i
+ * (overlap_vertical_edge :166-180 / overlap_horizontal_edge :182-199) */
+static void ovl_line(int32_t* c, ptrdiff_t step, int i) {
+    const int a = c[-2 * step], b = c[-step], cc = c[0], d = c[step];
+    const int d1 = a - d, d2 = a - d + b - cc;
+    const int r1 = (i & 1) ? 3 : 4, r2 = 7 - r1;
+    c[-2 * step] = ovl_arshift3(8 * a - d1 + r1);
+    c[-step] = ovl_arshift3(8 * b - d2 + r2);
+    c[0] = ovl_arshift3(8 * cc + d2 + r1);
+    c[step] = ovl_arshift3(8 * d + d1 + r2);
+}
+
+/* overlap_edge_enabled, encoder_filter.cpp:201-215 */
+static int ovl_enabled(int luma, int bx0, int by0, int bx1, int by1, const uint8_t* flags, int mbw, int mbh, int all) {
+    if (all) return 1;
+    const int mx0 = luma ? bx0 >> 1 : bx0, my0 = luma ? by0 >> 1 : by0;
+    const int mx1 = luma ? bx1 >> 1 : bx1, my1 = luma ? by1 >> 1 : by1;
+    if (mx0 < 0 || my0 < 0 || mx0 >= mbw || my0 >= mbh || mx1 < 0 || my1 < 0 || mx1 >= mbw || my1 >= mbh) return 0;
+    const int a = my0 * mbw + mx0, b = my1 * mbw + mx1;
+    if (a == b) return flags[a] != 0;
+    return flags[a] != 0 && flags[b] != 0;
+}
+
+/* apply_overlap_plane_signed, encoder_filter.cpp:217-243 */
+static void ovl_plane(int32_t* p, int w, int h, int luma, const uint8_t* flags, int mbw, int mbh, int all) {
+    if (w < 8 || h < 8) return;
+    const int bw = w / 8, bh = h / 8;
+    for (int bx = 1; bx < bw; ++bx)
+        for (int by = 0; by < bh; ++by)
+            if (ovl_enabled(luma, bx - 1, by, bx, by, flags, mbw, mbh, all))
+                for (int i = 0; i < 8; ++i) ovl_line(p + (size_t)(by * 8 + i) * w + bx * 8, 1, i);
+    for (int by = 1; by < bh; ++by)
+        for (int bx = 0; bx < bw; ++bx)
+            if (ovl_enabled(luma, bx, by - 1, bx, by, flags, mbw, mbh, all))
+                for (int i = 0; i < 8; ++i) ovl_line(p + (size_t)(by * 8) * w + bx * 8 + i, w, i);
+}
+
+/* Vc1Encoder::apply_i_overlap / apply_p_overlap, encoder_filter.cpp:344-365 (the plan's
+ * None mode and the picture-level condition are the caller's) */
+void vo_overlap_smooth(int mbw, int mbh, int32_t* y, int32_t* u, int32_t* v, const uint8_t* flags, int all) {
+    ovl_plane(y, mbw * 16, mbh * 16, 1, flags, mbw, mbh, all);
+    ovl_plane(u, mbw * 8, mbh * 8, 0, flags, mbw, mbh, all);
+    ovl_plane(v, mbw * 8, mbh * 8, 0, flags, mbw, mbh, all);
+}
+
+/* the store of reconstruct_i_picture_padded (clamp(s + bias) of every sample) and the intra
+ * write-back after apply_p_overlap (encoder_encode.cpp:1425-1449, bias 128, intra MBs) */
+void vo_store_signed(int mbw, int mbh, const int32_t* sy, const int32_t* su, const int32_t* sv, int bias,
+                     const uint8_t* mask, int w, int h, uint8_t* y, uint8_t* u, uint8_t* v) {
+    for (int k = 0; k < 3; ++k) {
+        const int32_t* s = k == 0 ? sy : (k == 1 ? su : sv);
+        uint8_t* d = k == 0 ? y : (k == 1 ? u : v);
+        const int sw = k == 0 ? mbw * 16 : mbw * 8, sh = k == 0 ? mbh * 16 : mbh * 8;
+        const int dw = k == 0 ? w : w / 2, dh = k == 0 ? h : h / 2, shift = k == 0 ? 4 : 3;
+        for (int yy = 0; yy < dh && yy < sh; ++yy)
+            for (int xx = 0; xx < dw && xx < sw; ++xx) {
+                if (mask && !mask[(yy >> shift) * mbw + (xx >> shift)]) continue;
+                const int t = s[(size_t)yy * sw + xx] + bias;
+                d[(size_t)yy * dw + xx] = (uint8_t)(t < 0 ? 0 : (t > 255 ? 255 : t));
+            }
+    }
+}
+
 /* Vc1Encoder::apply_i_like_loop_filter_plane, encoder_filter.cpp:426-434 */
 static void lf_i_plane(uint8_t* p, int w, int h, int pq) {
     for (int y = 8; y < h; y += 8)

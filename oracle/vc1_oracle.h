@@ -116,6 +116,13 @@ void vo_loop_filter_i(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v)
 void vo_loop_filter_p(const vc1cu_params* p, uint8_t* y, uint8_t* u, uint8_t* v, const vc1cu_mv* block_mvs,
                       const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
 
+/* overlap smoothing of a signed padded reconstruction in place (planes (mbw*16) x (mbh*16) luma,
+ * half chroma, rows packed; flags per MB or all != 0), and its 8-bit store clamp(s + bias) into
+ * a w x h frame (all MBs, or those mask flags) */
+void vo_overlap_smooth(int mbw, int mbh, int32_t* y, int32_t* u, int32_t* v, const uint8_t* flags, int all);
+void vo_store_signed(int mbw, int mbh, const int32_t* sy, const int32_t* su, const int32_t* sv, int bias,
+                     const uint8_t* mask, int w, int h, uint8_t* y, uint8_t* u, uint8_t* v);
+
 /* the throughput preset's transform type per MB (TransformType 1..4) */
 void vo_fast_transform_types(const vc1cu_params* p, const vo_frame* src, const vo_frame* pred, uint8_t* types);
 

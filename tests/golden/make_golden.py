@@ -305,11 +305,31 @@ def make_scene_kat():
     np.savez_compressed(os.path.join(HERE, "scene_kat.npz"), **d)
 
 
+def make_ovl_kat():
+    """Overlap smoothing by the reference: apply_i_overlap with CONDOVER ALL and with a SELECT
+    plan, and apply_p_overlap with an intra map, of tests/ovl_cases.py's signed planes."""
+    from oracle import Reference
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from ovl_cases import OVL_CASES, mb_flags, signed_planes
+
+    d = {}
+    for i, (w, h, pq, seed) in enumerate(OVL_CASES):
+        R = Reference(make_params(w, h, pqindex=pq))
+        planes, flags = signed_planes(w, h, seed), mb_flags(w, h, seed)
+        for tag, out in (("all", R.overlap(planes, 1)), ("sel", R.overlap(planes, 2, flags)),
+                         ("p", R.overlap(planes, 0, flags, p_picture=True))):
+            for c, pl in zip("yuv", out):
+                d[f"c{i}.{tag}.{c}"] = pl.astype(np.int16)
+    np.savez_compressed(os.path.join(HERE, "ovl_kat.npz"), **d)
+
+
 def main(only=()):
     if only:
         for name in only:
             {"b_kat": make_b_kat, "ic_kat": make_ic_kat, "scene_kat": make_scene_kat,
-             "recon_kat": make_recon_kat, "lf_kat": make_lf_kat, "tt_kat": make_tt_kat}[name]()
+             "recon_kat": make_recon_kat, "lf_kat": make_lf_kat, "tt_kat": make_tt_kat,
+             "ovl_kat": make_ovl_kat}[name]()
         return
     from oracle import Reference, ref_available
 
@@ -431,6 +451,7 @@ def main(only=()):
     make_recon_kat()
     make_lf_kat()
     make_tt_kat()
+    make_ovl_kat()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

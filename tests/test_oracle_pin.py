@@ -424,6 +424,59 @@ def test_loop_filter_matches_reference_live(oracle, seed):
         assert np.array_equal(x, y)
 
 
+# ---- overlap smoothing (apply_i_overlap / apply_p_overlap) ----------------------------------
+
+@pytest.mark.parametrize("i", range(6))
+def test_overlap_golden(oracle, i):
+    from ovl_cases import OVL_CASES, mb_flags, signed_planes
+
+    g = load("ovl_kat.npz")
+    w, h, pq, seed = OVL_CASES[i]
+    p = make_params(w, h, pqindex=pq)
+    planes, flags = signed_planes(w, h, seed), mb_flags(w, h, seed)
+    runs = {"all": oracle.overlap_smooth(p, planes, all_edges=True), "sel": oracle.overlap_smooth(p, planes, flags)}
+    # apply_p_overlap runs only at PQINDEX >= 9 (with OVERLAP on)
+    runs["p"] = oracle.overlap_smooth(p, planes, flags) if pq >= 9 else planes
+    for tag, got in runs.items():
+        for x, c in zip(got, "yuv"):
+            assert np.array_equal(x, g[f"c{i}.{tag}.{c}"]), (tag, c)
+    if w >= 32:
+        assert not np.array_equal(g[f"c{i}.all.y"], planes[0])  # the filter does change the picture
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_overlap_matches_reference_live(oracle, seed):
+    from ovl_cases import mb_flags, signed_planes
+
+    Reference = _ref_or_skip()
+    w, h = 322, 242
+    p = make_params(w, h, pqindex=9 + seed)
+    R = Reference(p)
+    planes, flags = signed_planes(w, h, seed), mb_flags(w, h, seed)
+    for got, want in ((oracle.overlap_smooth(p, planes, all_edges=True), R.overlap(planes, 1)),
+                      (oracle.overlap_smooth(p, planes, flags), R.overlap(planes, 2, flags)),
+                      (oracle.overlap_smooth(p, planes, flags), R.overlap(planes, 0, flags, p_picture=True))):
+        for x, y in zip(got, want):
+            assert np.array_equal(x, y)
+
+
+def test_store_signed_clamps_and_masks(oracle):
+    from ovl_cases import mb_flags, signed_planes
+
+    w, h = 98, 66
+    p = make_params(w, h)
+    planes, mask = signed_planes(w, h, 9), mb_flags(w, h, 9)
+    y, u, v = oracle.store_signed(p, planes, 128)
+    assert y.shape == (80, 112) and u.shape == (40, 56)
+    assert np.array_equal(y, np.clip(planes[0] + 128, 0, 255))
+    base = tuple(np.full(s, 7, np.uint8) for s in ((h, w), (h // 2, w // 2), (h // 2, w // 2)))
+    my, mu, _ = oracle.store_signed(p, planes, 128, mask, into=base)
+    m = mask.reshape(5, 7).repeat(16, 0).repeat(16, 1)[:h, :w].astype(bool)
+    assert np.array_equal(my[m], np.clip(planes[0][:h, :w] + 128, 0, 255)[m]) and (my[~m] == 7).all()
+    mc = mask.reshape(5, 7).repeat(8, 0).repeat(8, 1)[:h // 2, :w // 2].astype(bool)
+    assert np.array_equal(mu[mc], np.clip(planes[1][:h // 2, :w // 2] + 128, 0, 255)[mc]) and (mu[~mc] == 7).all()
+
+
 # ---- transform type of the throughput preset (choose_transform_mb, fast transform RDO) ----
 
 TT_CASES = ((98, 66, 4), (130, 98, 12), (322, 242, 6), (16, 16, 1), (354, 290, 3), (98, 66, 10))
