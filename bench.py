@@ -166,49 +166,83 @@ class Runner:
                 y, u, v = pinned[f]
                 self.ctx.upload_frame_ptr(f, y.data_ptr(), u.data_ptr(), v.data_ptr(), W, H)
 
-    def step(self, levels=None, mark=None):
-        """Enqueues one step on the library's stream; levels go to `levels` (default self.levels).
-        mark(stage), when given, is called after each stage (to record a timing event)."""
+    # Result-slot ids of the step's passes; `b` selects one of two sets, so that a pipelined run
+    # can read one step's results while the next step writes the other set.
+    @staticmethod
+    def seed_slot(i, b=0):
+        return 1000 * b + i
+
+    @staticmethod
+    def mode_slot(i, m, b=0):
+        return 1000 * b + 100 + 4 * i + m
+
+    @staticmethod
+    def final_slot(i, b=0):
+        return 1000 * b + 200 + i
+
+    @staticmethod
+    def bpass_slot(k, bil, fut, b=0):
+        return 1000 * b + 300 + 4 * k + 2 * bil + fut
+
+    @staticmethod
+    def bresult_slot(k, j, b=0):
+        return 100 * b + 2 * k + j
+
+    def step(self, levels=None, mark=None, b=0):
+        """Enqueues one step on the library's stream and runs its fade estimates (which wait for
+        the step's device work); levels go to `levels` (default self.levels). mark(stage), when
+        given, is called after each stage (to record a timing event)."""
+        self.launch(levels, mark, b)
+        self.finish(mark, b)
+
+    def launch(self, levels=None, mark=None, b=0):
+        """The step's device work up to the B decisions, enqueued without waiting."""
         levels = self.levels if levels is None else levels
         c, pics = self.ctx, self.pics
         mark = mark or (lambda stage: None)
         # every P picture's quarter-pel seed pass and the four unseeded core passes of every B
         # picture (forward / backward in quarter-pel and in half-pel bilinear mode); the library
         # runs one launch per pass kind
-        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, 1000 + i, pq) for i, (t, r, pq) in enumerate(pics)] +
-                      [(t, ref, m, 0, -1, 3100 + 4 * k + 2 * (m == self.BIL) + (ref == fut), pq)
+        c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, self.seed_slot(i, b), pq) for i, (t, r, pq) in enumerate(pics)] +
+                      [(t, ref, m, 0, -1, self.bpass_slot(k, m == self.BIL, ref == fut, b), pq)
                        for k, (t, past, fut, _n, _d, pq, _a) in enumerate(self.bpics)
                        for m in (self.QPEL, self.BIL) for ref in (past, fut)])
         mark("unseeded passes")
         # the three seeded mode passes of every picture (the library runs one launch per mode)
-        c.core_passes(self.p0, [(t, r, m, 0, 1000 + i, 2000 + 4 * i + m, pq) for i, (t, r, pq) in enumerate(pics)
-                                for m in self.modes])
+        c.core_passes(self.p0, [(t, r, m, 0, self.seed_slot(i, b), self.mode_slot(i, m, b), pq)
+                                for i, (t, r, pq) in enumerate(pics) for m in self.modes])
         mark("seeded mode passes")
         # the final pass (after the host's mode decision over whole passes)
-        c.core_passes(self.p0, [(t, r, self.MIXED, 1, 2000 + 4 * i + self.MIXED, 3000 + i, pq)
+        c.core_passes(self.p0, [(t, r, self.MIXED, 1, self.mode_slot(i, self.MIXED, b), self.final_slot(i, b), pq)
                                 for i, (t, r, pq) in enumerate(pics)])
         mark("final passes")
         for i, (t, r, pq) in enumerate(pics):
             p = params(pq)
-            c.motion_compensate(p, r, 3000 + i, self.MIXED, 3500 + i)
+            c.motion_compensate(p, r, self.final_slot(i, b), self.MIXED, 3500 + i)
             c.forward_quant_device(p, t, 3500 + i, 15, 0, levels[i].data_ptr())
         mark("prediction + transform")
         # the B decisions of both modes against the future anchor's final pass
         if self.bpics:
-            c.b_decide(self.p0, [(t, past, fut, 3100 + 4 * k + 2 * j, 3101 + 4 * k + 2 * j, 3000 + a, num, den, m,
-                                  2 * k + j, pq)
+            c.b_decide(self.p0, [(t, past, fut, self.bpass_slot(k, j, 0, b), self.bpass_slot(k, j, 1, b),
+                                  self.final_slot(a, b), num, den, m, self.bresult_slot(k, j, b), pq)
                                  for k, (t, past, fut, num, den, pq, a) in enumerate(self.bpics)
                                  for j, m in enumerate((self.QPEL, self.BIL))])
         mark("B decisions")
-        # the fade estimate analyze_p_picture runs on its final pass when fade compensation is on
-        # (the default; encoder_motion.cpp:570-573); it waits for the step's device work
-        self.ic = c.estimate_intensity_batch(self.p0, [(t, r, 3000 + i) for i, (t, r, pq) in enumerate(pics)])
+
+    def finish(self, mark=None, b=0):
+        """The fade estimate analyze_p_picture runs on its final pass when fade compensation is on
+        (the default; encoder_motion.cpp:570-573); it waits for the step's device work."""
+        mark = mark or (lambda stage: None)
+        self.ic = self.ctx.estimate_intensity_batch(
+            self.p0, [(t, r, self.final_slot(i, b)) for i, (t, r, pq) in enumerate(self.pics)])
         mark("fade estimates")
 
-    def read_results(self):
-        """D2H of every P picture's final-pass analysis and every B analysis (waits for the step)."""
-        return ([self.ctx.read_result(self.p0, 3000 + i) for i in range(len(self.pics))] +
-                [self.ctx.read_bresult(self.p0, j) for j in range(2 * len(self.bpics))])
+    def read_results(self, b=0):
+        """D2H of every P picture's final-pass analysis and every B analysis of slot set b; each
+        read waits only for the launch that wrote its slot."""
+        return ([self.ctx.read_result(self.p0, self.final_slot(i, b)) for i in range(len(self.pics))] +
+                [self.ctx.read_bresult(self.p0, self.bresult_slot(k, j, b))
+                 for k in range(len(self.bpics)) for j in range(2)])
 
     def mbs_per_step(self):
         return (len(self.pics) + len(self.bpics)) * MBS
@@ -290,43 +324,52 @@ def run_ours(args, rank, world, device):
     for f in run.frames:
         y, u, v = clip.frame(f)
         pinned[f] = tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (y, u, v))
-    # Every step: upload the step's frames from pinned memory, analyse, read the final-pass
-    # analysis back, and copy all levels to pinned host memory. The level copy of step i runs
-    # on a copy stream while step i+1 computes (two level buffers); the timed region ends
-    # when the last step's copy has landed.
+    # Every step: upload the step's frames from pinned memory, analyse, read every P final-pass
+    # and B analysis back, and copy all levels to pinned host memory. Steps are pipelined over
+    # two sets of result slots and level buffers: once step i is enqueued, the host reads step
+    # i-1's results (each read waits only for the launch that wrote its slot) and a copy stream
+    # moves step i-1's levels while step i computes; then step i's fade estimates wait for it.
+    # A run ends when its last step's results are read and its levels have landed.
     lev = [run.levels, torch.empty_like(run.levels)]
     host_levels = [torch.empty(run.levels.shape, dtype=torch.int16).pin_memory() for _ in range(2)]
     copy_stream = torch.cuda.Stream()
     copied = [None, None]
-    e2e_s = []
-    n_e2e = 0 if args.no_e2e else args.warmup + args.steps
-    t0 = None
-    for i in range(n_e2e):
-        if i == args.warmup:
-            copy_stream.synchronize()
-            ctx.synchronize()
-            flush_l2(torch, l2)
-            if world > 1:
-                torch.distributed.barrier()
-            t0 = time.perf_counter()
-        b = i % 2
-        if copied[b] is not None:
-            ext.wait_event(copied[b])  # the previous copy out of this buffer is done
-        with torch.cuda.stream(ext):
-            l2.zero_()  # L2 flush between steps, on the library's stream
-        run.upload_all(pinned)
-        run.step(lev[b])
-        done = torch.cuda.Event()
-        done.record(ext)
-        copy_stream.wait_event(done)
-        with torch.cuda.stream(copy_stream):
-            host_levels[b].copy_(lev[b], non_blocking=True)
-            copied[b] = torch.cuda.Event()
-            copied[b].record(copy_stream)
-        run.read_results()
-    if n_e2e:
+
+    def e2e_run(n):
+        prev = None
+        for i in range(n):
+            b = i % 2
+            if copied[b] is not None:
+                ext.wait_event(copied[b])  # the previous copy out of this level buffer is done
+            with torch.cuda.stream(ext):
+                l2.zero_()  # L2 flush between steps, on the library's stream
+            run.upload_all(pinned)
+            run.launch(lev[b], b=b)
+            done = torch.cuda.Event()
+            done.record(ext)
+            copy_stream.wait_event(done)
+            with torch.cuda.stream(copy_stream):
+                host_levels[b].copy_(lev[b], non_blocking=True)
+                copied[b] = torch.cuda.Event()
+                copied[b].record(copy_stream)
+            if prev is not None:
+                run.read_results(prev)
+            run.finish(b=b)
+            prev = b
+        if prev is not None:
+            run.read_results(prev)
         copy_stream.synchronize()
         ctx.synchronize()
+
+    e2e_s = []
+    if not args.no_e2e:
+        e2e_run(args.warmup)
+        flush_l2(torch, l2)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        e2e_run(args.steps)
         e2e_s.append(time.perf_counter() - t0)
     e2e_worst = slowest(sum(e2e_s), world, "cuda")
     e2e_value = world * mbs_per_step * args.steps / e2e_worst if e2e_s else None

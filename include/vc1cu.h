@@ -27,7 +27,8 @@
  * Frames are 8-bit 4:2:0 planes with tight strides (Y: width, U/V: width/2), the
  * layout of libvc1::Frame (src/encoder_internal.h:68-71).
  *
- * A context is bound to one CUDA device and owns one CUDA stream; calls on one context
+ * A context is bound to one CUDA device and owns one CUDA stream for its work (plus one that
+ * result reads copy on, after the launch that wrote the slot); calls on one context
  * are serialised by an internal mutex (the reference serialises its Vulkan context the
  * same way, src/vulkan_compute.cpp:385).
  */
@@ -255,7 +256,10 @@ typedef struct vc1cu_pass {
 } vc1cu_pass;
 
 int vc1cu_core_passes(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_pass* passes, int n);
-/* Copies a result slot to host arrays (and the scalar totals). Synchronous. */
+/* Copies a result slot to host arrays (and the scalar totals). Synchronous: returns once the
+ * launch that last wrote the slot (as enqueued before this call) has finished and the copies have
+ * landed; work enqueued after that launch keeps running (the copies use a second stream), so a
+ * caller may enqueue its next picture's passes into other slots before reading this one. */
 int vc1cu_read_result(vc1cu_ctx* ctx, int slot, vc1cu_panalysis* out);
 int vc1cu_synchronize(vc1cu_ctx* ctx);
 
@@ -351,7 +355,8 @@ int vc1cu_b_decide(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_bpass* pas
  */
 int vc1cu_b_predict(vc1cu_ctx* ctx, const vc1cu_params* p, int bslot, int cur_id, int past_id, int future_id,
                     int pred_id);
-/* Copies a B-result slot to host arrays (and the scalar totals). Synchronous. */
+/* Copies a B-result slot to host arrays (and the scalar totals). Synchronous, waiting only for
+ * the launch that last wrote the slot, like vc1cu_read_result. */
 int vc1cu_read_bresult(vc1cu_ctx* ctx, int bslot, vc1cu_banalysis* out);
 
 /* ---- intensity compensation (fades) ---------------------------------------------- */

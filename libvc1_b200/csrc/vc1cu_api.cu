@@ -15,6 +15,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -127,8 +128,21 @@ struct FrameSlot {
     }
 };
 
+// The event recorded on the context stream after the work of the API call that last wrote a
+// slot: reads of the slot wait for it alone, on the read stream.
+struct Written {
+    cudaEvent_t e = nullptr;
+    Written() = default;
+    Written(const Written&) = delete;
+    Written& operator=(const Written&) = delete;
+    ~Written() {
+        if (e) cudaEventDestroy(e);
+    }
+};
+
 struct ResultSlot {
     void* d = nullptr;
+    std::shared_ptr<Written> written;
     int mbs = 0;
     DevResult r{};
     bool valid = false;
@@ -139,6 +153,7 @@ struct ResultSlot {
 
 struct BSlot {
     void* d = nullptr;
+    std::shared_ptr<Written> written;
     int mbs = 0;
     DevBResult r{};
     bool valid = false;
@@ -177,6 +192,8 @@ struct vc1cu_ctx {
     int device = 0;
     std::string name;
     cudaStream_t stream = nullptr;
+    cudaStream_t rstream = nullptr;  // result reads (waits on the slot's Written event only)
+    std::vector<int> dirty_results, dirty_bresults;  // slots written by the current call
     std::mutex mu;
     std::string err;
     std::unordered_map<int, FrameSlot> frames;
@@ -241,14 +258,22 @@ int fail(vc1cu_ctx* c, int code, const std::string& msg) {
     return code;
 }
 
+void stamp_written(vc1cu_ctx* c);
+
 template <class F>
 int guarded(vc1cu_ctx* c, F&& f) {
     if (!c) return fail(nullptr, VC1CU_ERR_ARG, "null context");
     std::lock_guard<std::mutex> lock(c->mu);
     try {
         ck(cudaSetDevice(c->device), "cudaSetDevice");
-        return f();
+        const int rc = f();
+        stamp_written(c);
+        return rc;
     } catch (const Fail& e) {
+        try {
+            stamp_written(c);  // slots the failed call wrote before its error
+        } catch (const Fail&) {
+        }
         return fail(c, e.code, e.msg);
     } catch (const std::bad_alloc&) {
         return fail(c, VC1CU_ERR_OOM, "host allocation failed");
@@ -389,6 +414,7 @@ FrameSlot& frame_slot(vc1cu_ctx* c, int id) {
 }
 
 ResultSlot& result_slot(vc1cu_ctx* c, int id, int mbs, bool create) {
+    if (create) c->dirty_results.push_back(id);  // create: the caller writes the slot
     auto& s = c->results[id];
     if (s.valid && s.mbs == mbs) return s;
     if (!create) throw Fail{VC1CU_ERR_STATE, "result slot " + std::to_string(id) + " holds no result of this size"};
@@ -868,6 +894,55 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
     return VC1CU_OK;
 }
 
+// Records one event after the work the current call enqueued and hands it to every slot the
+// call wrote.
+void stamp_written(vc1cu_ctx* c) {
+    if (c->dirty_results.empty() && c->dirty_bresults.empty()) return;
+    auto w = std::make_shared<Written>();
+    ck(cudaEventCreateWithFlags(&w->e, cudaEventDisableTiming), "cudaEventCreate(slot)");
+    ck(cudaEventRecord(w->e, c->stream), "cudaEventRecord(slot)");
+    for (int id : c->dirty_results) {
+        auto it = c->results.find(id);
+        if (it != c->results.end()) it->second.written = w;
+    }
+    for (int id : c->dirty_bresults) {
+        auto it = c->bresults.find(id);
+        if (it != c->bresults.end()) it->second.written = w;
+    }
+    c->dirty_results.clear();
+    c->dirty_bresults.clear();
+}
+
+// Orders the read stream after the work that last wrote a slot (after everything enqueued so far
+// when the slot has no record).
+void read_after(vc1cu_ctx* c, const std::shared_ptr<Written>& w) {
+    if (w) {
+        ck(cudaStreamWaitEvent(c->rstream, w->e, 0), "cudaStreamWaitEvent(read)");
+        return;
+    }
+    cudaEvent_t e = take_event(c);
+    ck(cudaEventRecord(e, c->stream), "cudaEventRecord(read)");
+    ck(cudaStreamWaitEvent(c->rstream, e, 0), "cudaStreamWaitEvent(read)");
+    c->event_pool.push_back(e);
+}
+
+void read_sync(vc1cu_ctx* c) {
+    ck(cudaStreamSynchronize(c->rstream), "cudaStreamSynchronize(read)");
+    ck(cudaGetLastError(), "kernel");
+}
+
+int check_status(vc1cu_ctx* c);
+
+// The launch status as of the slot's writer (later launches may already have added to it); a
+// recorded error is reported and cleared as check_status does.
+void check_status_read(vc1cu_ctx* c, const std::shared_ptr<Written>& w) {
+    read_after(c, w);
+    LaunchStatus st{};
+    ck(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(status)");
+    read_sync(c);
+    if (st.error) check_status(c);
+}
+
 int check_status(vc1cu_ctx* c) {
     LaunchStatus st{};
     ck(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(status)");
@@ -893,8 +968,10 @@ int check_status(vc1cu_ctx* c) {
 
 void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
     const size_t n = (size_t)s.mbs;
+    stamp_written(c);  // slots this call wrote
+    read_after(c, s.written);
     auto cp = [&](void* dst, const void* src, size_t b) {
-        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(result)");
+        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(result)");
     };
     cp(out->mvs, s.r.mvs, 8 * n);
     cp(out->block_mvs, s.r.bmv, 32 * n);
@@ -912,7 +989,7 @@ void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
     cp(it, s.r.itotals, 40);
     cp(g, s.r.global, 8);
     cp(&gsad, s.r.gsad, 8);
-    sync_checked(c);
+    read_sync(c);
     out->mean_abs_residual = tot[0];
     out->rate_complexity = tot[1];
     out->motion_sad = it[0];
@@ -926,6 +1003,7 @@ void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
 }
 
 BSlot& bresult_slot(vc1cu_ctx* c, int id, int mbs) {
+    c->dirty_bresults.push_back(id);
     auto& s = c->bresults[id];
     if (s.d && s.mbs == mbs) {
         s.valid = true;
@@ -1200,8 +1278,10 @@ bool zoom_coherent(const std::vector<vc1cu_mv>& mvs, int mbw, int mbh) {
 
 void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
     const size_t n = (size_t)s.mbs;
+    stamp_written(c);
+    read_after(c, s.written);
     auto cp = [&](void* dst, const void* src, size_t b) {
-        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(B result)");
+        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(B result)");
     };
     cp(out->modes, s.r.modes, n);
     cp(out->forward_mvs, s.r.fmv, 8 * n);
@@ -1217,7 +1297,7 @@ void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
     double tot[2];
     cp(it, s.r.itotals, sizeof it);
     cp(tot, s.r.totals, sizeof tot);
-    sync_checked(c);
+    read_sync(c);
     out->forward_macroblocks = it[kBTotForward];
     out->backward_macroblocks = it[kBTotBackward];
     out->interpolated_macroblocks = it[kBTotInterpolated];
@@ -1280,6 +1360,7 @@ int vc1cu_open(int device, vc1cu_ctx** out) {
     try {
         ck(cudaSetDevice(device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaStreamCreateWithFlags(&c->rstream, cudaStreamNonBlocking), "cudaStreamCreate(read)");
         void* d = nullptr;
         ck(cudaMalloc(&d, sizeof(LaunchStatus)), "cudaMalloc(status)");
         c->d_status = static_cast<LaunchStatus*>(d);
@@ -1327,6 +1408,10 @@ int vc1cu_close(vc1cu_ctx* c) {
     }
     for (auto e : c->event_pool) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->rstream) {
+        cudaStreamSynchronize(c->rstream);
+        cudaStreamDestroy(c->rstream);
+    }
     delete c;
     return VC1CU_OK;
 }
@@ -1473,9 +1558,9 @@ int vc1cu_synchronize(vc1cu_ctx* c) {
 int vc1cu_read_result(vc1cu_ctx* c, int slot, vc1cu_panalysis* out) {
     return guarded(c, [&]() -> int {
         if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
-        check_status(c);
         auto it = c->results.find(slot);
         if (it == c->results.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "empty result slot"};
+        check_status_read(c, it->second.written);
         read_result(c, it->second, out);
         return VC1CU_OK;
     });
@@ -1533,9 +1618,9 @@ int vc1cu_b_decide(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* passe
 int vc1cu_read_bresult(vc1cu_ctx* c, int bslot, vc1cu_banalysis* out) {
     return guarded(c, [&]() -> int {
         if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
-        check_status(c);
         auto it = c->bresults.find(bslot);
         if (it == c->bresults.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "empty B-result slot"};
+        check_status_read(c, it->second.written);
         read_bresult(c, it->second, out);
         return VC1CU_OK;
     });
