@@ -158,13 +158,19 @@ class Runner:
         self.levels = torch.empty((n, 4, MBS, 6, 64), dtype=torch.int16, device="cuda")
         self.frame_bytes = W * H * 3 // 2
 
-    def upload_all(self, pinned=None):
+    @staticmethod
+    def fid(f, b=0):
+        """Frame slot of clip frame f in frame set b (two sets let a pipelined run upload one
+        step's frames while the previous step reads the other set)."""
+        return f + 100 * b
+
+    def upload_all(self, pinned=None, b=0):
         for f in self.frames:
             if pinned is None:
-                self.ctx.upload_frame(f, *self.clip.frame(f))
+                self.ctx.upload_frame(self.fid(f, b), *self.clip.frame(f))
             else:
                 y, u, v = pinned[f]
-                self.ctx.upload_frame_ptr(f, y.data_ptr(), u.data_ptr(), v.data_ptr(), W, H)
+                self.ctx.upload_frame_ptr(self.fid(f, b), y.data_ptr(), u.data_ptr(), v.data_ptr(), W, H)
 
     # Result-slot ids of the step's passes; `b` selects one of two sets, so that a pipelined run
     # can read one step's results while the next step writes the other set.
@@ -198,14 +204,16 @@ class Runner:
     def launch(self, levels=None, mark=None, b=0):
         """The step's device work up to the B decisions, enqueued without waiting."""
         levels = self.levels if levels is None else levels
-        c, pics = self.ctx, self.pics
+        c, F = self.ctx, lambda f: self.fid(f, b)
+        pics = [(F(t), F(r), pq) for t, r, pq in self.pics]
+        bpics = [(F(t), F(past), F(fut), num, den, pq, a) for t, past, fut, num, den, pq, a in self.bpics]
         mark = mark or (lambda stage: None)
         # every P picture's quarter-pel seed pass and the four unseeded core passes of every B
         # picture (forward / backward in quarter-pel and in half-pel bilinear mode); the library
         # runs one launch per pass kind
         c.core_passes(self.p0, [(t, r, self.QPEL, 0, -1, self.seed_slot(i, b), pq) for i, (t, r, pq) in enumerate(pics)] +
                       [(t, ref, m, 0, -1, self.bpass_slot(k, m == self.BIL, ref == fut, b), pq)
-                       for k, (t, past, fut, _n, _d, pq, _a) in enumerate(self.bpics)
+                       for k, (t, past, fut, _n, _d, pq, _a) in enumerate(bpics)
                        for m in (self.QPEL, self.BIL) for ref in (past, fut)])
         mark("unseeded passes")
         # the three seeded mode passes of every picture (the library runs one launch per mode)
@@ -222,10 +230,10 @@ class Runner:
             c.forward_quant_device(p, t, 3500 + i, 15, 0, levels[i].data_ptr())
         mark("prediction + transform")
         # the B decisions of both modes against the future anchor's final pass
-        if self.bpics:
+        if bpics:
             c.b_decide(self.p0, [(t, past, fut, self.bpass_slot(k, j, 0, b), self.bpass_slot(k, j, 1, b),
                                   self.final_slot(a, b), num, den, m, self.bresult_slot(k, j, b), pq)
-                                 for k, (t, past, fut, num, den, pq, a) in enumerate(self.bpics)
+                                 for k, (t, past, fut, num, den, pq, a) in enumerate(bpics)
                                  for j, m in enumerate((self.QPEL, self.BIL))])
         mark("B decisions")
 
@@ -234,8 +242,17 @@ class Runner:
         (the default; encoder_motion.cpp:570-573); it waits for the step's device work."""
         mark = mark or (lambda stage: None)
         self.ic = self.ctx.estimate_intensity_batch(
-            self.p0, [(t, r, self.final_slot(i, b)) for i, (t, r, pq) in enumerate(self.pics)])
+            self.p0, [(self.fid(t, b), self.fid(r, b), self.final_slot(i, b)) for i, (t, r, pq) in enumerate(self.pics)])
         mark("fade estimates")
+
+    def enqueue_ic(self, b=0):
+        """finish() in two phases for a pipelined run: the estimates' device work, enqueued
+        without waiting; returns the ticket collect_ic takes."""
+        return self.ctx.estimate_intensity_enqueue(
+            self.p0, [(self.fid(t, b), self.fid(r, b), self.final_slot(i, b)) for i, (t, r, pq) in enumerate(self.pics)])
+
+    def collect_ic(self, ticket):
+        self.ic = self.ctx.estimate_intensity_collect(ticket)
 
     def read_results(self, b=0):
         """D2H of every P picture's final-pass analysis and every B analysis of slot set b; each
@@ -326,38 +343,51 @@ def run_ours(args, rank, world, device):
         pinned[f] = tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (y, u, v))
     # Every step: upload the step's frames from pinned memory, analyse, read every P final-pass
     # and B analysis back, and copy all levels to pinned host memory. Steps are pipelined over
-    # two sets of result slots and level buffers: once step i is enqueued, the host reads step
-    # i-1's results (each read waits only for the launch that wrote its slot) and a copy stream
-    # moves step i-1's levels while step i computes; then step i's fade estimates wait for it.
-    # A run ends when its last step's results are read and its levels have landed.
+    # two sets of frame slots, result slots and level buffers, so the device always has the
+    # next step queued: while step i computes, the library's upload stream brings step i+1's
+    # frames and step i+1 is enqueued behind it; the host then collects step i's fade
+    # estimates (waiting for step i alone), a copy stream moves step i's levels and the host
+    # reads step i's results (each read waits only for the launch that wrote its slot), all
+    # beside step i+1's compute. A run ends when its last step's results are read and its
+    # levels have landed.
     lev = [run.levels, torch.empty_like(run.levels)]
     host_levels = [torch.empty(run.levels.shape, dtype=torch.int16).pin_memory() for _ in range(2)]
     copy_stream = torch.cuda.Stream()
     copied = [None, None]
 
+    def copy_levels(b, after):
+        copy_stream.wait_event(after)
+        with torch.cuda.stream(copy_stream):
+            host_levels[b].copy_(lev[b], non_blocking=True)
+            copied[b] = torch.cuda.Event()
+            copied[b].record(copy_stream)
+
+    def start(i):
+        """Enqueues step i (frames already uploaded into set i % 2) without waiting."""
+        b = i % 2
+        if copied[b] is not None:
+            ext.wait_event(copied[b])  # the previous copy out of this level buffer is done
+        with torch.cuda.stream(ext):
+            l2.zero_()  # L2 flush between steps, on the library's stream
+        run.launch(lev[b], b=b)  # waits on the device for its frames' uploads
+        ticket = run.enqueue_ic(b)
+        done = torch.cuda.Event()
+        done.record(ext)
+        return b, ticket, done
+
     def e2e_run(n):
-        prev = None
+        if not n:
+            return
+        run.upload_all(pinned, 0)
+        cur = start(0)
         for i in range(n):
-            b = i % 2
-            if copied[b] is not None:
-                ext.wait_event(copied[b])  # the previous copy out of this level buffer is done
-            with torch.cuda.stream(ext):
-                l2.zero_()  # L2 flush between steps, on the library's stream
-            run.upload_all(pinned)
-            run.launch(lev[b], b=b)
-            done = torch.cuda.Event()
-            done.record(ext)
-            copy_stream.wait_event(done)
-            with torch.cuda.stream(copy_stream):
-                host_levels[b].copy_(lev[b], non_blocking=True)
-                copied[b] = torch.cuda.Event()
-                copied[b].record(copy_stream)
-            if prev is not None:
-                run.read_results(prev)
-            run.finish(b=b)
-            prev = b
-        if prev is not None:
-            run.read_results(prev)
+            b, ticket, done = cur
+            if i + 1 < n:
+                run.upload_all(pinned, 1 - b)  # step i+1's frames, beside step i's compute
+                cur = start(i + 1)
+            run.collect_ic(ticket)  # step i's fade estimates (waits for step i alone)
+            copy_levels(b, done)  # step i's levels, beside step i+1's compute
+            run.read_results(b)
         copy_stream.synchronize()
         ctx.synchronize()
 

@@ -27,8 +27,9 @@
  * Frames are 8-bit 4:2:0 planes with tight strides (Y: width, U/V: width/2), the
  * layout of libvc1::Frame (src/encoder_internal.h:68-71).
  *
- * A context is bound to one CUDA device and owns one CUDA stream for its work (plus one that
- * result reads copy on, after the launch that wrote the slot); calls on one context
+ * A context is bound to one CUDA device and owns one CUDA stream for its work, plus one for
+ * frame uploads (each after the last work that used its slot; later work waits for it) and one
+ * for result reads (each after the launch that wrote its slot); calls on one context
  * are serialised by an internal mutex (the reference serialises its Vulkan context the
  * same way, src/vulkan_compute.cpp:385).
  */
@@ -218,7 +219,11 @@ int vc1cu_score_motion_batch_law(vc1cu_ctx* ctx, const vc1cu_params* p, int law,
 /* ---- frames resident in HBM ---------------------------------------------------------- */
 
 /* Copies one 4:2:0 frame (host planes, tight strides) into frame slot frame_id
- * (0 <= frame_id < 4096). u/v may be NULL (chroma then reads as 128). */
+ * (0 <= frame_id < 4096). u/v may be NULL (chroma then reads as 128). The copy runs on the
+ * context's upload stream once the work already enqueued that uses the slot is done, so it
+ * overlaps work on other slots; everything enqueued after this call sees the new frame. From
+ * pinned host memory the call returns at once and the planes must stay unchanged until that
+ * later work has started (or vc1cu_synchronize); from pageable memory it returns once staged. */
 int vc1cu_upload_frame(vc1cu_ctx* ctx, int frame_id, const uint8_t* y, const uint8_t* u,
                        const uint8_t* v, int width, int height);
 /* Reads a frame slot back (for tests). */
@@ -390,6 +395,16 @@ typedef struct vc1cu_icpass {
 
 int vc1cu_estimate_intensity_batch(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
                                    vc1cu_intensity* out);
+
+/* Two-phase form of vc1cu_estimate_intensity_batch for callers that pipeline pictures: _enqueue
+ * puts the batch's device work on the context stream and returns at once with a ticket;
+ * _collect waits for that work alone (not for work enqueued after it) and finishes the n
+ * estimates on the host, with the same results as the batch form. Up to 4 batches may be
+ * outstanding: the fifth enqueue reuses the oldest ticket's buffer, which then reports
+ * VC1CU_ERR_STATE, as does a ticket collected twice. */
+int vc1cu_estimate_intensity_enqueue(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
+                                     int64_t* ticket);
+int vc1cu_estimate_intensity_collect(vc1cu_ctx* ctx, int64_t ticket, vc1cu_intensity* out, int n);
 
 /*
  * Replaces Vc1Encoder::scene_change_score (src/encoder_motion.cpp:599-676), the scene-cut test

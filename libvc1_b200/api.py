@@ -37,6 +37,7 @@ EXPORTS = (
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
+    "vc1cu_estimate_intensity_enqueue", "vc1cu_estimate_intensity_collect",
     "vc1cu_fast_transform_types",
 )
 
@@ -95,6 +96,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_fast_transform_types.argtypes = [vp, PP, i32, i32, vp]
     L.vc1cu_loop_filter_p.argtypes = [vp, PP, i32, vp, vp, vp, vp]
     L.vc1cu_overlap_smooth.argtypes = [vp, PP, vp, vp, vp, vp, i32]
+    L.vc1cu_estimate_intensity_enqueue.argtypes = [vp, PP, vp, i32, C.POINTER(C.c_int64)]
+    L.vc1cu_estimate_intensity_collect.argtypes = [vp, C.c_int64, vp, i32]
     L.vc1cu_store_signed.argtypes = [vp, PP, vp, vp, vp, i32, vp, i32]
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
@@ -278,6 +281,21 @@ class CudaComputeContext:
         out = (Intensity * max(1, len(passes)))()
         self._check(self._L.vc1cu_estimate_intensity_batch(self._h, C.byref(params), arr, len(passes), out))
         return [out[i].as_tuple() for i in range(len(passes))]
+
+    def estimate_intensity_enqueue(self, params: Params, passes) -> tuple:
+        """The batch's device work, enqueued without waiting; returns (ticket, n) for
+        estimate_intensity_collect."""
+        arr = (IcPass * max(1, len(passes)))(*[IcPass(*q) for q in passes])
+        t = C.c_int64()
+        self._check(self._L.vc1cu_estimate_intensity_enqueue(self._h, C.byref(params), arr, len(passes), C.byref(t)))
+        return t.value, len(passes)
+
+    def estimate_intensity_collect(self, ticket) -> list:
+        """Waits for an enqueued batch alone and returns its estimates."""
+        t, n = ticket
+        out = (Intensity * max(1, n))()
+        self._check(self._L.vc1cu_estimate_intensity_collect(self._h, t, out, n))
+        return [out[i].as_tuple() for i in range(n)]
 
     def scene_change_score(self, params: Params, cur_id: int, ref_id: int, fade_compensation: bool = True,
                            scene_threshold: float = 28.0) -> float:

@@ -36,6 +36,7 @@ int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
 size_t gstate_bytes();
 int run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream);
+cudaError_t launch_global_fanout(const GlobalCopy* d_copies, int n, cudaStream_t s);
 void init_gstate(GState* h, const DevFrame& cur, const DevFrame& ref, int range, int* out_global,
                  unsigned long long* out_sad);
 void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const int2* bmv, const uint8_t* use4, int mode,
@@ -112,22 +113,6 @@ inline void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Fail{VC1CU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-struct FrameSlot {
-    uint8_t* d = nullptr;
-    size_t cap = 0;
-    int w = 0, h = 0, pitch_y = 0, pitch_c = 0;
-    bool valid = false;
-    DevFrame view() const {
-        DevFrame f;
-        f.y = d;
-        f.pitch_y = pitch_y;
-        f.pitch_c = pitch_c;
-        f.u = d + (size_t)pitch_y * h;
-        f.v = f.u + (size_t)pitch_c * (h / 2);
-        return f;
-    }
-};
-
 // The event recorded on the context stream after the work of the API call that last wrote a
 // slot: reads of the slot wait for it alone, on the read stream.
 struct Written {
@@ -140,8 +125,27 @@ struct Written {
     }
 };
 
+struct FrameSlot {
+    uint8_t* d = nullptr;
+    size_t cap = 0;
+    int w = 0, h = 0, pitch_y = 0, pitch_c = 0;
+    bool valid = false;
+    std::shared_ptr<Written> last_use;  // after the last call whose work read or wrote the frame
+    cudaEvent_t uploaded = nullptr;     // the last upload into the slot, on the upload stream
+    DevFrame view() const {
+        DevFrame f;
+        f.y = d;
+        f.pitch_y = pitch_y;
+        f.pitch_c = pitch_c;
+        f.u = d + (size_t)pitch_y * h;
+        f.v = f.u + (size_t)pitch_c * (h / 2);
+        return f;
+    }
+};
+
 struct ResultSlot {
     void* d = nullptr;
+    size_t bytes = 0;  // the slot's one allocation, all fields
     std::shared_ptr<Written> written;
     int mbs = 0;
     DevResult r{};
@@ -153,6 +157,7 @@ struct ResultSlot {
 
 struct BSlot {
     void* d = nullptr;
+    size_t bytes = 0;
     std::shared_ptr<Written> written;
     int mbs = 0;
     DevBResult r{};
@@ -193,7 +198,11 @@ struct vc1cu_ctx {
     std::string name;
     cudaStream_t stream = nullptr;
     cudaStream_t rstream = nullptr;  // result reads (waits on the slot's Written event only)
+    void* h_read = nullptr;          // pinned landing buffer of a result read (one slot)
+    size_t read_cap = 0;
     std::vector<int> dirty_results, dirty_bresults;  // slots written by the current call
+    std::vector<int> used_frames;                     // frame slots the current call's work uses
+    cudaStream_t ustream = nullptr;  // frame uploads (each waits for the last use of its slot)
     std::mutex mu;
     std::string err;
     std::unordered_map<int, FrameSlot> frames;
@@ -214,6 +223,19 @@ struct vc1cu_ctx {
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
+    // Outstanding fade-estimate batches (vc1cu_estimate_intensity_enqueue / _collect): each has
+    // a pinned landing buffer for its tables and sums and the event after their copy.
+    static constexpr int kIcTickets = 4;
+    struct IcTicket {
+        void* h = nullptr;
+        size_t cap = 0;
+        cudaEvent_t done = nullptr;
+        int n = 0;
+        int64_t id = 0;  // 0: free
+    } ic_tickets[kIcTickets], ic_sync;  // ic_sync: the synchronous entry points' buffer
+    int64_t ic_next_id = 1;
+    void* d_gcopy = nullptr;   // GlobalCopy list of a launch's passes that share a global search
+    size_t gcopy_cap = 0;
     void* d_ovl = nullptr;     // per-macroblock overlap flags / store mask
     size_t ovl_cap = 0;
     size_t icdesc_cap = 0;
@@ -223,9 +245,16 @@ struct vc1cu_ctx {
     size_t lr_cap = 0;
     void* d_scratch = nullptr;
     size_t scratch_cap = 0;
-    void* h_pinned = nullptr;
-    size_t pinned_cap = 0;
-    cudaEvent_t staging_done = nullptr;  // last H2D copy out of h_pinned
+    // Pinned staging of launch descriptors: a ring, so that the host can enqueue up to
+    // kStagingRing launches ahead of the device (each copy out of a buffer is ordered behind
+    // the launches before it on the stream, and its buffer is reused once that copy is done).
+    static constexpr int kStagingRing = 8;
+    struct StagingBuf {
+        void* h = nullptr;
+        size_t cap = 0;
+        cudaEvent_t done = nullptr;  // the H2D copy out of h
+    } staging_ring[kStagingRing];
+    int staging_next = 0, staging_cur = 0;
     uint32_t epoch = 0;
     int sm_count = 0;
     int max_smem = 0;
@@ -408,6 +437,7 @@ int stage_max(int R) {
 }
 
 FrameSlot& frame_slot(vc1cu_ctx* c, int id) {
+    c->used_frames.push_back(id);
     auto it = c->frames.find(id);
     if (it == c->frames.end() || !it->second.valid) throw Fail{VC1CU_ERR_STATE, "frame slot " + std::to_string(id) + " was never uploaded"};
     return it->second;
@@ -425,6 +455,7 @@ ResultSlot& result_slot(vc1cu_ctx* c, int id, int mbs, bool create) {
     const size_t bytes = al(8 * n) + al(32 * n) + al(n) * 2 + al(8 * n) * 4 + al(n) + al(8 * n) * 2 + al(n) + al(4 * n) +
                          al(8) + al(8) + al(16) + al(40);
     ck(cudaMalloc(&s.d, bytes), "cudaMalloc(result slot)");
+    s.bytes = bytes;
     ck(cudaMemsetAsync(s.d, 0, bytes, c->stream), "cudaMemsetAsync(result slot)");
     uint8_t* p = static_cast<uint8_t*>(s.d);
     auto take = [&](size_t b) { uint8_t* q = p; p += al(b); return q; };
@@ -450,7 +481,10 @@ ResultSlot& result_slot(vc1cu_ctx* c, int id, int mbs, bool create) {
     return s;
 }
 
-FrameSlot& alloc_frame(vc1cu_ctx* c, int id, int w, int h) {
+// by_upload: the caller writes the slot on the upload stream (else work on the context stream
+// writes it, a use of the slot).
+FrameSlot& alloc_frame(vc1cu_ctx* c, int id, int w, int h, bool by_upload = false) {
+    if (!by_upload) c->used_frames.push_back(id);
     auto& f = c->frames[id];
     const int py = (w + 15) & ~15, pc = (w / 2 + 15) & ~15;
     const size_t bytes = (size_t)py * h + 2 * (size_t)pc * (h / 2);
@@ -561,18 +595,28 @@ void collect_timing(vc1cu_ctx* c) {
     c->pending.clear();
 }
 
-// Pinned staging for host->device launch descriptors; waits until its previous copy is done.
+// Pinned staging for host->device launch descriptors: the next buffer of the ring, once its
+// previous copy is done. The caller copies out of it on the context stream, then staging_mark.
 void* staging(vc1cu_ctx* c, size_t bytes) {
-    if (c->staging_done) ck(cudaEventSynchronize(c->staging_done), "cudaEventSynchronize");
-    if (c->pinned_cap < bytes) {
-        if (c->h_pinned) cudaFreeHost(c->h_pinned);
-        c->h_pinned = nullptr;
-        c->pinned_cap = 0;
-        ck(cudaMallocHost(&c->h_pinned, bytes), "cudaMallocHost(staging)");
-        c->pinned_cap = bytes;
+    const int i = c->staging_next;
+    c->staging_next = (i + 1) % vc1cu_ctx::kStagingRing;
+    auto& b = c->staging_ring[i];
+    if (b.done) ck(cudaEventSynchronize(b.done), "cudaEventSynchronize(staging)");
+    if (b.cap < bytes) {
+        if (b.h) cudaFreeHost(b.h);
+        b.h = nullptr;
+        b.cap = 0;
+        ck(cudaMallocHost(&b.h, bytes), "cudaMallocHost(staging)");
+        b.cap = bytes;
     }
-    if (!c->staging_done) ck(cudaEventCreateWithFlags(&c->staging_done, cudaEventDisableTiming), "cudaEventCreate");
-    return c->h_pinned;
+    if (!b.done) ck(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming), "cudaEventCreate(staging)");
+    c->staging_cur = i;
+    return b.h;
+}
+
+// Records the copy out of the buffer the last staging() call handed out.
+void staging_mark(vc1cu_ctx* c) {
+    ck(cudaEventRecord(c->staging_ring[c->staging_cur].done, c->stream), "cudaEventRecord(staging)");
 }
 
 int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1cu_mv* cands, size_t n, uint64_t* costs) {
@@ -696,7 +740,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
             init_gstate(reinterpret_cast<GState*>(hs + gb * k), d.cur, d.ref, grange, d.out.global, d.out.gsad);
         }
         ck(cudaMemcpyAsync(c->d_gstates, hs, gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
-        ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+        staging_mark(c);
         Timer tm(c, kGlobal);
         const int launches = run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
         ck(cudaGetLastError(), "global search launch");
@@ -732,7 +776,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         std::memcpy(hp, h.data(), sizeof(PassDesc) * n);
         ck(cudaMemcpyAsync(c->d_passes, hp, sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
            "cudaMemcpyAsync(pass descriptors)");
-        ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+        staging_mark(c);
     }
     // window / bitset geometry
     WinCfg wc;
@@ -877,16 +921,28 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
                             outs[un[k]]->gsad);
             }
             ck(cudaMemcpyAsync(c->d_gstates, hs, gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
-            ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+            staging_mark(c);
             Timer tm(c, kGlobal);
             const int launches = run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
             ck(cudaGetLastError(), "global search launch");
             tm.stop(launches);
+            // the passes that reuse a search take its result, in one launch (not one copy each)
+            std::vector<GlobalCopy> copies;
             for (size_t k = 0; k < unseeded_idx.size(); ++k) {
                 const int i = unseeded_idx[k], f = first_of[k];
-                if (f == i) continue;
-                ck(cudaMemcpyAsync(outs[i]->global, outs[f]->global, 8, cudaMemcpyDeviceToDevice, c->stream), "copy global");
-                ck(cudaMemcpyAsync(outs[i]->gsad, outs[f]->gsad, 8, cudaMemcpyDeviceToDevice, c->stream), "copy global");
+                if (f != i) copies.push_back(GlobalCopy{outs[f]->global, outs[f]->gsad, outs[i]->global, outs[i]->gsad});
+            }
+            if (!copies.empty()) {
+                const size_t cb = sizeof(GlobalCopy) * copies.size();
+                void* dcp = ensure(c->d_gcopy, c->gcopy_cap, cb, "cudaMalloc(global copies)");
+                void* hc = staging(c, cb);
+                std::memcpy(hc, copies.data(), cb);
+                ck(cudaMemcpyAsync(dcp, hc, cb, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(global copies)");
+                staging_mark(c);
+                Timer tf(c, kGlobal);
+                ck(launch_global_fanout(static_cast<const GlobalCopy*>(dcp), (int)copies.size(), c->stream),
+                   "global copy launch");
+                tf.stop(1);
             }
         }
     }
@@ -897,7 +953,7 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
 // Records one event after the work the current call enqueued and hands it to every slot the
 // call wrote.
 void stamp_written(vc1cu_ctx* c) {
-    if (c->dirty_results.empty() && c->dirty_bresults.empty()) return;
+    if (c->dirty_results.empty() && c->dirty_bresults.empty() && c->used_frames.empty()) return;
     auto w = std::make_shared<Written>();
     ck(cudaEventCreateWithFlags(&w->e, cudaEventDisableTiming), "cudaEventCreate(slot)");
     ck(cudaEventRecord(w->e, c->stream), "cudaEventRecord(slot)");
@@ -909,8 +965,13 @@ void stamp_written(vc1cu_ctx* c) {
         auto it = c->bresults.find(id);
         if (it != c->bresults.end()) it->second.written = w;
     }
+    for (int id : c->used_frames) {
+        auto it = c->frames.find(id);
+        if (it != c->frames.end()) it->second.last_use = w;
+    }
     c->dirty_results.clear();
     c->dirty_bresults.clear();
+    c->used_frames.clear();
 }
 
 // Orders the read stream after the work that last wrote a slot (after everything enqueued so far
@@ -925,6 +986,22 @@ void read_after(vc1cu_ctx* c, const std::shared_ptr<Written>& w) {
     ck(cudaStreamWaitEvent(c->rstream, e, 0), "cudaStreamWaitEvent(read)");
     c->event_pool.push_back(e);
 }
+
+// A whole slot allocation copied to the pinned read buffer in one transfer (on the read stream,
+// after read_after); the fields are then unpacked on the host.
+const uint8_t* read_slot_bytes(vc1cu_ctx* c, const void* d, size_t bytes) {
+    if (c->read_cap < bytes) {
+        if (c->h_read) cudaFreeHost(c->h_read);
+        c->h_read = nullptr;
+        c->read_cap = 0;
+        ck(cudaMallocHost(&c->h_read, bytes), "cudaMallocHost(read buffer)");
+        c->read_cap = bytes;
+    }
+    ck(cudaMemcpyAsync(c->h_read, d, bytes, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(result)");
+    return static_cast<const uint8_t*>(c->h_read);
+}
+
+void read_sync(vc1cu_ctx* c);
 
 void read_sync(vc1cu_ctx* c) {
     ck(cudaStreamSynchronize(c->rstream), "cudaStreamSynchronize(read)");
@@ -970,8 +1047,11 @@ void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
     const size_t n = (size_t)s.mbs;
     stamp_written(c);  // slots this call wrote
     read_after(c, s.written);
+    const uint8_t* hb = read_slot_bytes(c, s.d, s.bytes);
+    read_sync(c);
+    const uint8_t* base = static_cast<const uint8_t*>(s.d);
     auto cp = [&](void* dst, const void* src, size_t b) {
-        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(result)");
+        if (dst) std::memcpy(dst, hb + (static_cast<const uint8_t*>(src) - base), b);
     };
     cp(out->mvs, s.r.mvs, 8 * n);
     cp(out->block_mvs, s.r.bmv, 32 * n);
@@ -989,7 +1069,6 @@ void read_result(vc1cu_ctx* c, const ResultSlot& s, vc1cu_panalysis* out) {
     cp(it, s.r.itotals, 40);
     cp(g, s.r.global, 8);
     cp(&gsad, s.r.gsad, 8);
-    read_sync(c);
     out->mean_abs_residual = tot[0];
     out->rate_complexity = tot[1];
     out->motion_sad = it[0];
@@ -1015,6 +1094,7 @@ BSlot& bresult_slot(vc1cu_ctx* c, int id, int mbs) {
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bytes = al(n) * 3 + al(8 * n) * 7 + al(16 * n) + al(4 * n) + al(8 * kBTotCount) + al(16);
     ck(cudaMalloc(&s.d, bytes), "cudaMalloc(B result slot)");
+    s.bytes = bytes;
     ck(cudaMemsetAsync(s.d, 0, bytes, c->stream), "cudaMemsetAsync(B result slot)");
     uint8_t* p = static_cast<uint8_t*>(s.d);
     auto take = [&](size_t b) { uint8_t* q = p; p += al(b); return q; };
@@ -1118,7 +1198,7 @@ void launch_b(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_bpass* b, int n, 
     void* hp = staging(c, sizeof(BDesc) * n);
     std::memcpy(hp, h.data(), sizeof(BDesc) * n);
     ck(cudaMemcpyAsync(c->d_bdescs, hp, sizeof(BDesc) * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(B descriptors)");
-    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    staging_mark(c);
     Timer tm(c, kB);
     ck(launch_bpictures(P, c->d_bdescs, n, c->stream), "B-picture kernel launch");
     tm.stop(2);
@@ -1167,38 +1247,66 @@ struct IcJob {
     const int2* mvs;
 };
 
-// Device part of the estimate for a batch of pictures (one set of launches), then the host part.
-void ic_estimate(vc1cu_ctx* c, const DevParams& P, const std::vector<IcJob>& jobs, vc1cu_intensity* out) {
+constexpr size_t kIcTable = 63 * 64;                              // SAD of every (LUMSCALE, LUMSHIFT)
+constexpr size_t kIcHostBytes = (kIcTable + 5) * sizeof(unsigned long long);  // one picture's table + sums
+
+// Device part of the estimate for a batch of pictures (one set of launches) on the context
+// stream, its tables and sums copied into ticket t's pinned buffer; t.done follows the copies.
+void ic_enqueue(vc1cu_ctx* c, const DevParams& P, const std::vector<IcJob>& jobs, vc1cu_ctx::IcTicket& t) {
     const int n = (int)jobs.size();
+    t.n = n;
     if (!n) return;
     const size_t sb = ic_scratch_bytes(), db = (ic_desc_bytes() + 15) & ~size_t(15);
     uint8_t* scratch = static_cast<uint8_t*>(ensure(c->d_ic, c->ic_cap, sb * n, "cudaMalloc(intensity scratch)"));
     void* ddesc = ensure(c->d_icdesc, c->icdesc_cap, db * n, "cudaMalloc(intensity descriptors)");
+    if (t.cap < kIcHostBytes * n) {
+        if (t.done) ck(cudaEventSynchronize(t.done), "cudaEventSynchronize(intensity)");
+        if (t.h) cudaFreeHost(t.h);
+        t.h = nullptr;
+        t.cap = 0;
+        ck(cudaMallocHost(&t.h, kIcHostBytes * n), "cudaMallocHost(intensity results)");
+        t.cap = kIcHostBytes * n;
+    }
+    if (!t.done) ck(cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming), "cudaEventCreate(intensity)");
     uint8_t* hp = static_cast<uint8_t*>(staging(c, db * n));
     for (int i = 0; i < n; ++i) ic_fill_desc(hp + db * i, jobs[i].cur, jobs[i].ref, jobs[i].mvs, scratch + sb * i);
     ck(cudaMemcpyAsync(ddesc, hp, db * n, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(intensity descriptors)");
-    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
-    for (int i = 0; i < n; ++i) {
-        ck(cudaMemsetAsync(scratch + sb * i, 0, ic_hist_bytes(), c->stream), "cudaMemsetAsync(histogram)");
-        ck(cudaMemsetAsync(scratch + sb * i + ic_sums_offset(), 0, 5 * sizeof(unsigned long long), c->stream),
-           "cudaMemsetAsync(sums)");
-    }
+    staging_mark(c);
+    // every picture's histogram and sums start at zero (one fill of the whole scratch)
+    ck(cudaMemsetAsync(scratch, 0, sb * n, c->stream), "cudaMemsetAsync(intensity scratch)");
     {
         Timer tm(c, kIc);
         ck(launch_ic_estimate(static_cast<const IcDesc*>(ddesc), n, P.W, P.H, c->stream), "intensity estimate launch");
         tm.stop(3);
     }
-    constexpr size_t kTable = 63 * 64;
-    std::vector<unsigned long long> tables(kTable * n), sums(5 * (size_t)n);
+    uint8_t* hb = static_cast<uint8_t*>(t.h);
     for (int i = 0; i < n; ++i) {
-        ck(cudaMemcpyAsync(tables.data() + kTable * i, scratch + sb * i + ic_table_offset(), kTable * 8,
+        ck(cudaMemcpyAsync(hb + kIcHostBytes * i, scratch + sb * i + ic_table_offset(), kIcTable * 8,
                            cudaMemcpyDeviceToHost, c->stream),
            "cudaMemcpyAsync(intensity table)");
-        ck(cudaMemcpyAsync(sums.data() + 5 * i, scratch + sb * i + ic_sums_offset(), 40, cudaMemcpyDeviceToHost, c->stream),
+        ck(cudaMemcpyAsync(hb + kIcHostBytes * i + kIcTable * 8, scratch + sb * i + ic_sums_offset(), 40,
+                           cudaMemcpyDeviceToHost, c->stream),
            "cudaMemcpyAsync(intensity sums)");
     }
-    sync_checked(c);
-    for (int i = 0; i < n; ++i) out[i] = ic_decide(sums.data() + 5 * i, tables.data() + kTable * i);
+    ck(cudaEventRecord(t.done, c->stream), "cudaEventRecord(intensity)");
+}
+
+// The host part, once ticket t's copies are done: the long double fit and the 7x7 choice.
+void ic_finish(vc1cu_ctx* c, vc1cu_ctx::IcTicket& t, vc1cu_intensity* out) {
+    if (!t.n) return;
+    ck(cudaEventSynchronize(t.done), "cudaEventSynchronize(intensity)");
+    ck(cudaGetLastError(), "kernel");
+    const uint8_t* hb = static_cast<const uint8_t*>(t.h);
+    for (int i = 0; i < t.n; ++i) {
+        const auto* table = reinterpret_cast<const unsigned long long*>(hb + kIcHostBytes * i);
+        out[i] = ic_decide(table + kIcTable, table);
+    }
+}
+
+// Device part of the estimate for a batch of pictures (one set of launches), then the host part.
+void ic_estimate(vc1cu_ctx* c, const DevParams& P, const std::vector<IcJob>& jobs, vc1cu_intensity* out) {
+    ic_enqueue(c, P, jobs, c->ic_sync);  // the call waits for its own copies before returning
+    ic_finish(c, c->ic_sync, out);
 }
 
 // Vc1Encoder::global_motion_search (encoder_motion.cpp:2076-2141) of one picture pair at
@@ -1217,7 +1325,7 @@ void global_search_one(vc1cu_ctx* c, const DevFrame& cur, const DevFrame& ref, i
     const int grange = std::min(range, 32);
     init_gstate(reinterpret_cast<GState*>(hs), cur, ref, grange, s.r.global, s.r.gsad);
     ck(cudaMemcpyAsync(c->d_gstates, hs, gb, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
-    ck(cudaEventRecord(c->staging_done, c->stream), "cudaEventRecord");
+    staging_mark(c);
     {
         Timer tm(c, kGlobal);
         const int launches = run_global_search(c->d_gstates, 1, grange, W, H, c->stream);
@@ -1280,8 +1388,11 @@ void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
     const size_t n = (size_t)s.mbs;
     stamp_written(c);
     read_after(c, s.written);
+    const uint8_t* hb = read_slot_bytes(c, s.d, s.bytes);
+    read_sync(c);
+    const uint8_t* base = static_cast<const uint8_t*>(s.d);
     auto cp = [&](void* dst, const void* src, size_t b) {
-        if (dst) ck(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(B result)");
+        if (dst) std::memcpy(dst, hb + (static_cast<const uint8_t*>(src) - base), b);
     };
     cp(out->modes, s.r.modes, n);
     cp(out->forward_mvs, s.r.fmv, 8 * n);
@@ -1297,7 +1408,6 @@ void read_bresult(vc1cu_ctx* c, const BSlot& s, vc1cu_banalysis* out) {
     double tot[2];
     cp(it, s.r.itotals, sizeof it);
     cp(tot, s.r.totals, sizeof tot);
-    read_sync(c);
     out->forward_macroblocks = it[kBTotForward];
     out->backward_macroblocks = it[kBTotBackward];
     out->interpolated_macroblocks = it[kBTotInterpolated];
@@ -1361,6 +1471,7 @@ int vc1cu_open(int device, vc1cu_ctx** out) {
         ck(cudaSetDevice(device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaStreamCreateWithFlags(&c->rstream, cudaStreamNonBlocking), "cudaStreamCreate(read)");
+        ck(cudaStreamCreateWithFlags(&c->ustream, cudaStreamNonBlocking), "cudaStreamCreate(upload)");
         void* d = nullptr;
         ck(cudaMalloc(&d, sizeof(LaunchStatus)), "cudaMalloc(status)");
         c->d_status = static_cast<LaunchStatus*>(d);
@@ -1380,8 +1491,11 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (!c) return VC1CU_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (auto& kv : c->frames)
+    if (c->ustream) cudaStreamSynchronize(c->ustream);
+    for (auto& kv : c->frames) {
         if (kv.second.d) cudaFree(kv.second.d);
+        if (kv.second.uploaded) cudaEventDestroy(kv.second.uploaded);
+    }
     for (auto& kv : c->results)
         if (kv.second.d) cudaFree(kv.second.d);
     for (auto& kv : c->bresults)
@@ -1392,6 +1506,13 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_btypes) cudaFree(c->d_btypes);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
+    if (c->d_gcopy) cudaFree(c->d_gcopy);
+    auto free_ticket = [](vc1cu_ctx::IcTicket& t) {
+        if (t.h) cudaFreeHost(t.h);
+        if (t.done) cudaEventDestroy(t.done);
+    };
+    for (auto& t : c->ic_tickets) free_ticket(t);
+    free_ticket(c->ic_sync);
     for (auto& s : c->cache)
         if (s.d) cudaFree(s.d);
     if (c->d_status) cudaFree(c->d_status);
@@ -1400,8 +1521,11 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_lr) cudaFree(c->d_lr);
     if (c->d_scratch) cudaFree(c->d_scratch);
     for (auto& kv : c->items) cudaFree(kv.second.first);
-    if (c->h_pinned) cudaFreeHost(c->h_pinned);
-    if (c->staging_done) cudaEventDestroy(c->staging_done);
+    if (c->h_read) cudaFreeHost(c->h_read);
+    for (auto& b : c->staging_ring) {
+        if (b.h) cudaFreeHost(b.h);
+        if (b.done) cudaEventDestroy(b.done);
+    }
     for (auto& t : c->pending) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
@@ -1412,6 +1536,7 @@ int vc1cu_close(vc1cu_ctx* c) {
         cudaStreamSynchronize(c->rstream);
         cudaStreamDestroy(c->rstream);
     }
+    if (c->ustream) cudaStreamDestroy(c->ustream);
     delete c;
     return VC1CU_OK;
 }
@@ -1514,14 +1639,21 @@ int vc1cu_upload_frame(vc1cu_ctx* c, int id, const uint8_t* y, const uint8_t* u,
     return guarded(c, [&]() -> int {
         if (id < 0 || id >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "frame id out of range"};
         if (!y || w <= 0 || h <= 0 || (w & 1) || (h & 1)) throw Fail{VC1CU_ERR_ARG, "invalid frame"};
-        FrameSlot& f = alloc_frame(c, id, w, h);
+        // On the upload stream after the last work that used the slot; work enqueued on the
+        // context stream from here on waits for it, work enqueued before keeps running.
+        FrameSlot& f = alloc_frame(c, id, w, h, true);
+        if (f.last_use) ck(cudaStreamWaitEvent(c->ustream, f.last_use->e, 0), "cudaStreamWaitEvent(upload)");
         const DevFrame d = f.view();
-        ck(cudaMemcpy2DAsync((void*)d.y, f.pitch_y, y, w, w, h, cudaMemcpyHostToDevice, c->stream), "upload Y");
+        cudaStream_t us = c->ustream;
+        ck(cudaMemcpy2DAsync((void*)d.y, f.pitch_y, y, w, w, h, cudaMemcpyHostToDevice, us), "upload Y");
         const int cw = w / 2, ch = h / 2;
-        if (u) ck(cudaMemcpy2DAsync((void*)d.u, f.pitch_c, u, cw, cw, ch, cudaMemcpyHostToDevice, c->stream), "upload U");
-        else ck(cudaMemset2DAsync((void*)d.u, f.pitch_c, 128, cw, ch, c->stream), "fill U");
-        if (v) ck(cudaMemcpy2DAsync((void*)d.v, f.pitch_c, v, cw, cw, ch, cudaMemcpyHostToDevice, c->stream), "upload V");
-        else ck(cudaMemset2DAsync((void*)d.v, f.pitch_c, 128, cw, ch, c->stream), "fill V");
+        if (u) ck(cudaMemcpy2DAsync((void*)d.u, f.pitch_c, u, cw, cw, ch, cudaMemcpyHostToDevice, us), "upload U");
+        else ck(cudaMemset2DAsync((void*)d.u, f.pitch_c, 128, cw, ch, us), "fill U");
+        if (v) ck(cudaMemcpy2DAsync((void*)d.v, f.pitch_c, v, cw, cw, ch, cudaMemcpyHostToDevice, us), "upload V");
+        else ck(cudaMemset2DAsync((void*)d.v, f.pitch_c, 128, cw, ch, us), "fill V");
+        if (!f.uploaded) ck(cudaEventCreateWithFlags(&f.uploaded, cudaEventDisableTiming), "cudaEventCreate(upload)");
+        ck(cudaEventRecord(f.uploaded, us), "cudaEventRecord(upload)");
+        ck(cudaStreamWaitEvent(c->stream, f.uploaded, 0), "cudaStreamWaitEvent(upload)");
         c->counters.frame_uploads++;
         c->counters.frame_upload_bytes += (size_t)w * h + 2 * (size_t)cw * ch;
         return VC1CU_OK;
@@ -1708,6 +1840,21 @@ int vc1cu_estimate_intensity_comp(vc1cu_ctx* c, const vc1cu_params* p, int cur_i
     });
 }
 
+// The jobs of a batch of fade estimates, each along the mvs of its result slot.
+static std::vector<IcJob> ic_jobs(vc1cu_ctx* c, const DevParams& P, const vc1cu_icpass* passes, int n) {
+    const int mbs = P.mbw * P.mbh;
+    std::vector<IcJob> jobs;
+    for (int i = 0; i < n; ++i) {
+        FrameSlot& fc = frame_slot(c, passes[i].cur_id);
+        FrameSlot& fr = frame_slot(c, passes[i].ref_id);
+        if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "intensity estimate frame dimensions do not match the configuration"};
+        if (passes[i].mv_slot < 0 || passes[i].mv_slot >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+        jobs.push_back(IcJob{fc.view(), fr.view(), result_slot(c, passes[i].mv_slot, mbs, false).r.mvs});
+    }
+    return jobs;
+}
+
 int vc1cu_estimate_intensity_batch(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
                                    vc1cu_intensity* out) {
     return guarded(c, [&]() -> int {
@@ -1716,18 +1863,45 @@ int vc1cu_estimate_intensity_batch(vc1cu_ctx* c, const vc1cu_params* p, const vc
         std::string why;
         const int rc = make_dev_params(p, P, why);
         if (rc) throw Fail{rc, why};
-        const int mbs = P.mbw * P.mbh;
         check_status(c);
-        std::vector<IcJob> jobs;
-        for (int i = 0; i < n; ++i) {
-            FrameSlot& fc = frame_slot(c, passes[i].cur_id);
-            FrameSlot& fr = frame_slot(c, passes[i].ref_id);
-            if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
-                throw Fail{VC1CU_ERR_ARG, "intensity estimate frame dimensions do not match the configuration"};
-            if (passes[i].mv_slot < 0 || passes[i].mv_slot >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
-            jobs.push_back(IcJob{fc.view(), fr.view(), result_slot(c, passes[i].mv_slot, mbs, false).r.mvs});
-        }
-        ic_estimate(c, P, jobs, out);
+        ic_estimate(c, P, ic_jobs(c, P, passes, n), out);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_estimate_intensity_enqueue(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_icpass* passes, int n,
+                                     int64_t* ticket) {
+    return guarded(c, [&]() -> int {
+        if (!ticket || n < 0 || (n > 0 && !passes)) throw Fail{VC1CU_ERR_ARG, "invalid intensity batch"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        const std::vector<IcJob> jobs = ic_jobs(c, P, passes, n);
+        const int64_t id = c->ic_next_id++;
+        auto& t = c->ic_tickets[id % vc1cu_ctx::kIcTickets];
+        t.id = 0;  // not collectable until its work is enqueued
+        ic_enqueue(c, P, jobs, t);
+        t.id = id;
+        *ticket = id;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_estimate_intensity_collect(vc1cu_ctx* c, int64_t ticket, vc1cu_intensity* out, int n) {
+    return guarded(c, [&]() -> int {
+        auto& t = c->ic_tickets[(ticket > 0 ? ticket : 0) % vc1cu_ctx::kIcTickets];
+        if (ticket <= 0 || t.id != ticket)
+            throw Fail{VC1CU_ERR_STATE, "intensity ticket unknown, already collected or overwritten"};
+        if (n != t.n || (n > 0 && !out)) throw Fail{VC1CU_ERR_ARG, "collect n differs from the enqueued batch"};
+        // a wavefront timeout recorded by the launches before it is reported here
+        ck(cudaStreamWaitEvent(c->rstream, t.done, 0), "cudaStreamWaitEvent(intensity)");
+        LaunchStatus st{};
+        ck(cudaMemcpyAsync(&st, c->d_status, sizeof st, cudaMemcpyDeviceToHost, c->rstream), "cudaMemcpyAsync(status)");
+        read_sync(c);
+        if (st.error) check_status(c);
+        ic_finish(c, t, out);
+        t.id = 0;
         return VC1CU_OK;
     });
 }

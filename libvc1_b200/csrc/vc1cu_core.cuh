@@ -91,6 +91,14 @@ struct LaunchStatus {
     unsigned int tmask;  // its lanes still waiting (lanes 0-3: left, top-left, top, top-right; lane 0: seed)
 };
 
+// A pass that reuses another pass's whole-frame search (same picture pair) takes its result.
+struct GlobalCopy {
+    const int* src_global;
+    const unsigned long long* src_sad;
+    int* dst_global;
+    unsigned long long* dst_sad;
+};
+
 // One B-result slot (Vc1Encoder::BAnalysis) in HBM, structure of arrays over macroblocks.
 struct DevBResult {
     uint8_t* modes;

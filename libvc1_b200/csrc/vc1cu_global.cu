@@ -312,6 +312,21 @@ size_t gstate_bytes() { return sizeof(GState); }
 // Host driver: runs the staged search for n states already initialised in device memory
 // (cur, ref, range, outputs, phase = 0). Every stage is one scoring launch sized to the
 // stage's largest candidate list and sampling stride, bracketed by plan/fold launches.
+// Passes that share one search take its result: one thread per copy (dx, dy and the SAD).
+__global__ void global_fanout_kernel(const GlobalCopy* copies, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const GlobalCopy c = copies[i];
+    c.dst_global[0] = c.src_global[0];
+    c.dst_global[1] = c.src_global[1];
+    *c.dst_sad = *c.src_sad;
+}
+
+cudaError_t launch_global_fanout(const GlobalCopy* d_copies, int n, cudaStream_t s) {
+    if (n > 0) global_fanout_kernel<<<(n + 127) / 128, 128, 0, s>>>(d_copies, n);
+    return cudaGetLastError();
+}
+
 int run_global_search(GState* d_states, int n, int R, int W, int H, cudaStream_t stream) {
     struct Stage { int maxc, stride; };
     Stage st[4];

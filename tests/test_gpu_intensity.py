@@ -97,3 +97,27 @@ def test_intensity_rejects_bad_arguments(ctx):
     p = make_params(64, 48, search_range=8, local_search_range=8)
     with pytest.raises(Vc1cuError, match="never uploaded"):
         ctx.estimate_intensity_comp(p, 999, 0, np.zeros((12, 2), np.int32))
+
+
+def test_intensity_enqueue_collect_matches_batch(ctx):
+    """The two-phase form gives the batch form's estimates, with two batches outstanding and
+    more work enqueued behind them; a ticket is collectable once."""
+    make, a, b = FADES["cif_darken"]
+    clip = make()
+    w, h = clip.width, clip.height
+    p = make_params(w, h, search_range=16, local_search_range=16)
+    ref, cur = clip.frame(0), synth.fade(clip.frame(1), a, b, 7)
+    ctx.upload_frame(60, *ref)
+    ctx.upload_frame(61, *cur)
+    ctx.core_passes(p, [(61, 60, MV_QPEL, 0, -1, 62), (60, 61, MV_QPEL, 0, -1, 63)])
+    jobs1, jobs2 = [(61, 60, 62)], [(61, 60, 62), (60, 61, 63)]
+    want1, want2 = ctx.estimate_intensity_batch(p, jobs1), ctx.estimate_intensity_batch(p, jobs2)
+    t1 = ctx.estimate_intensity_enqueue(p, jobs1)
+    t2 = ctx.estimate_intensity_enqueue(p, jobs2)
+    ctx.core_passes(p, [(61, 60, MV_QPEL, 0, -1, 64)])  # later work on the stream
+    assert ctx.estimate_intensity_collect(t2) == want2
+    assert ctx.estimate_intensity_collect(t1) == want1
+    with pytest.raises(Vc1cuError, match="ticket"):
+        ctx.estimate_intensity_collect(t1)
+    with pytest.raises(Vc1cuError, match="ticket"):
+        ctx.estimate_intensity_collect((123456, 1))
