@@ -67,3 +67,64 @@ def test_random_configuration_matches_oracle(ctx, oracle, seed):
         g = ctx.analyze_b_picture(p, 1, 0, 2, ef.mvs, ef.use_4mv, 1, 2, mode)
         eb = oracle.analyze_b(p, cur, past, fut, ef.mvs, ef.use_4mv, 1, 2, mode)
         assert g.equal(eb) == [], (seed, "B", mode, kw)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_configuration_reconstruction_matches_oracle(ctx, oracle, seed):
+    """The same random configurations through the rest of the path: a B picture decided from
+    passes in result slots and its prediction, the reconstruction of the P picture's levels with
+    a random transform type per block, the P loop filter with random block metadata, overlap
+    smoothing of a signed picture and the compensated reference of a random fade code."""
+    import torch
+
+    from lf_cases import metadata
+    from ovl_cases import mb_flags, signed_planes
+
+    w, h, kw, motion = random_config(seed)
+    p = make_params(w, h, **kw)
+    mbw, mbh = (w + 15) // 16, (h + 15) // 16
+    clip = synth.generate(w, h, 3, 700 + seed, global_px=motion, n_objects=2, obj_min=8, obj_max=32)
+    past, cur, fut = clip.frame(0), clip.frame(1), clip.frame(2)
+    for fid, fr in ((0, past), (1, cur), (2, fut)):
+        ctx.upload_frame(fid, *fr)
+    ctx.core_passes(p, [(2, 0, MV_QPEL, 0, -1, 230)])
+    ctx.core_passes(p, [(2, 0, MV_MIXED, 1, 230, 231)])
+    q = oracle.analyze_p_core(p, fut, past, MV_QPEL, False)
+    ef = oracle.analyze_p_core(p, fut, past, MV_MIXED, True, seed=q.mvs, seed_distant=q)
+    assert ctx.read_result(p, 231).equal(ef) == [], (seed, kw)
+    # B picture from user slots: forward / backward quarter-pel passes, the decision, the prediction
+    ctx.core_passes(p, [(1, 0, MV_QPEL, 0, -1, 232), (1, 2, MV_QPEL, 0, -1, 233)])
+    ctx.b_decide(p, [(1, 0, 2, 232, 233, 231, 1, 2, MV_QPEL, 7, 0)])
+    eb = oracle.analyze_b(p, cur, past, fut, ef.mvs, ef.use_4mv, 1, 2, MV_QPEL)
+    assert ctx.read_bresult(p, 7).equal(eb) == [], (seed, kw)
+    ctx.b_predict(p, 7, 1, 0, 2, 8)
+    for x, y in zip(ctx.download_frame(8, w, h), oracle.b_predict(p, cur, past, fut, eb, MV_QPEL)):
+        assert np.array_equal(x, y), seed
+    # reconstruction of the P picture from all four types' levels, a random type per block
+    ctx.motion_compensate(p, 0, 231, MV_MIXED, 3)
+    pred = ctx.download_frame(3, w, h)
+    lv = torch.empty((4, mbw * mbh, 6, 64), dtype=torch.int16, device="cuda")
+    ctx.forward_quant_device(p, 2, 3, 15, 0, lv.data_ptr())
+    types = np.random.default_rng(seed).integers(1, 5, (mbw * mbh, 6)).astype(np.uint8)
+    ctx.reconstruct(p, 3, lv.data_ptr(), 15, types, 4)
+    ctx.synchronize()
+    rec = oracle.reconstruct(p, pred, lv.cpu().numpy(), 15, types)
+    assert all(np.array_equal(x, y) for x, y in zip(ctx.download_frame(4, w, h), rec)), seed
+    # the P loop filter of the reconstruction
+    meta = metadata(w, h, seed, seed % 2 == 0)
+    ctx.loop_filter(p, 4, *meta)
+    assert all(np.array_equal(x, y) for x, y in zip(ctx.download_frame(4, w, h), oracle.loop_filter(p, rec, *meta))), seed
+    # overlap smoothing of a signed picture of the padded raster (select flags)
+    planes, flags = signed_planes(w, h, seed), mb_flags(w, h, seed)
+    d = [torch.from_numpy(a).cuda() for a in planes]
+    torch.cuda.synchronize()
+    ctx.overlap_smooth(p, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), flags, False)
+    ctx.synchronize()
+    for x, y in zip(d, oracle.overlap_smooth(p, planes, flags)):
+        assert np.array_equal(x.cpu().numpy(), y), seed
+    # the compensated reference of a random fade code
+    rng = np.random.default_rng(900 + seed)
+    ic = (1, int(rng.integers(0, 64)), int(rng.integers(0, 64)))
+    ctx.intensity_compensate(0, ic, 9)
+    for x, y in zip(ctx.download_frame(9, w, h), oracle.intensity_compensate(past, ic)):
+        assert np.array_equal(x, y), (seed, ic)
