@@ -486,8 +486,10 @@ int vc1cu_reconstruct(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const 
  * (:610-738) of a coded P picture, HOST arrays per macroblock: block_mvs (4 luma block vectors),
  * cbp (6 loop_filter_pattern codes, 4 bits each), tt (6 loop_filter_tt codes: 0, 3, 6, 7) and
  * intra (bit k set when block k is intra). The device result equals the reference's raster
- * order. vc1cu_loop_filter_i is asynchronous; vc1cu_loop_filter_p returns once its metadata
- * copies are done.
+ * order. The frame is the coding raster or the padded raster of whole macroblocks that the
+ * reference's reconstruction holds (vc1cu_store_signed's output); the filter covers the frame's
+ * own extent, as the reference's does. vc1cu_loop_filter_i is asynchronous; vc1cu_loop_filter_p
+ * returns once its metadata copies are done.
  */
 int vc1cu_loop_filter_i(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id);
 int vc1cu_loop_filter_p(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,

@@ -2044,6 +2044,12 @@ int vc1cu_fast_transform_types(vc1cu_ctx* c, const vc1cu_params* p, int src_id, 
     });
 }
 
+// The deblocking filters take the coding raster or the padded raster the reference's
+// reconstruction uses (whole macroblocks); they filter the frame's own extent.
+static bool filter_size_ok(const DevParams& P, const FrameSlot& f) {
+    return (f.w == P.W && f.h == P.H) || (f.w == P.mbw * 16 && f.h == P.mbh * 16);
+}
+
 int vc1cu_loop_filter_i(vc1cu_ctx* c, const vc1cu_params* p, int frame_id) {
     return guarded(c, [&]() -> int {
         DevParams P;
@@ -2051,10 +2057,10 @@ int vc1cu_loop_filter_i(vc1cu_ctx* c, const vc1cu_params* p, int frame_id) {
         const int rc = make_dev_params(p, P, why);
         if (rc) throw Fail{rc, why};
         FrameSlot& f = frame_slot(c, frame_id);
-        if (f.w != P.W || f.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        if (!filter_size_ok(P, f)) throw Fail{VC1CU_ERR_ARG, "frame size is neither the raster nor the padded raster"};
         const DevFrame d = f.view();
         Timer tm(c, kMc);
-        ck(launch_loop_filter_i((uint8_t*)d.y, (uint8_t*)d.u, (uint8_t*)d.v, f.pitch_y, f.pitch_c, P.W, P.H, P.pq, c->stream),
+        ck(launch_loop_filter_i((uint8_t*)d.y, (uint8_t*)d.u, (uint8_t*)d.v, f.pitch_y, f.pitch_c, f.w, f.h, P.pq, c->stream),
            "loop filter launch");
         tm.stop(2);
         return VC1CU_OK;
@@ -2070,7 +2076,7 @@ int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const
         const int rc = make_dev_params(p, P, why);
         if (rc) throw Fail{rc, why};
         FrameSlot& f = frame_slot(c, frame_id);
-        if (f.w != P.W || f.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        if (!filter_size_ok(P, f)) throw Fail{VC1CU_ERR_ARG, "frame size is neither the raster nor the padded raster"};
         const size_t mbs = (size_t)P.mbw * P.mbh;
         for (size_t i = 0; i < mbs * 6; ++i)
             if (cbp[i] > 15 || !(tt[i] == 0 || tt[i] == 3 || tt[i] == 6 || tt[i] == 7))
@@ -2083,7 +2089,7 @@ int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const
         ck(cudaMemcpyAsync(d + al + 12 * mbs, intra, mbs, cudaMemcpyHostToDevice, c->stream), "upload intra bits");
         const DevFrame fr = f.view();
         Timer tm(c, kMc);
-        ck(launch_loop_filter_p((uint8_t*)fr.y, (uint8_t*)fr.u, (uint8_t*)fr.v, f.pitch_y, f.pitch_c, P.W, P.H, P.pq,
+        ck(launch_loop_filter_p((uint8_t*)fr.y, (uint8_t*)fr.u, (uint8_t*)fr.v, f.pitch_y, f.pitch_c, f.w, f.h, P.pq,
                                 reinterpret_cast<const int2*>(d), d + al, d + al + 6 * mbs, d + al + 12 * mbs, c->stream),
            "loop filter launch");
         tm.stop(2);

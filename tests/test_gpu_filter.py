@@ -62,3 +62,39 @@ def test_loop_filter_rejects_bad_codes(ctx):
     tt[0, 0] = 5
     with pytest.raises(Vc1cuError, match="transform kinds"):
         ctx.loop_filter(p, 0, bmv, cbp, tt, intra)
+
+
+def test_loop_filter_of_padded_reconstruction(ctx, oracle):
+    """The padded raster the reference's reconstruction holds (whole macroblocks): both filters
+    cover the frame's own extent, and an I picture stored by vc1cu_store_signed filters in place."""
+    import torch
+
+    from lf_cases import blocky_frame, metadata
+    from ovl_cases import signed_planes
+
+    w, h = 322, 242
+    p = make_params(w, h, pqindex=14)
+    pw, ph = 336, 256
+    pp = make_params(pw, ph, pqindex=14)  # the oracle filters whatever frame it is given
+    fr = blocky_frame(pw, ph, 21)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0)
+    for got, want in zip(ctx.download_frame(0, pw, ph), oracle.loop_filter(pp, fr)):
+        assert np.array_equal(got, want)
+    meta = metadata(w, h, 22, True)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0, *meta)
+    for got, want in zip(ctx.download_frame(0, pw, ph), oracle.loop_filter(pp, fr, *meta)):
+        assert np.array_equal(got, want)
+    planes = signed_planes(w, h, 23)
+    d = [torch.from_numpy(a).cuda() for a in planes]
+    torch.cuda.synchronize()
+    ctx.overlap_smooth(p, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), None, True)
+    ctx.store_signed(p, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), 128, 12)
+    ctx.loop_filter(p, 12)
+    want = oracle.loop_filter(pp, oracle.store_signed(p, oracle.overlap_smooth(p, planes, all_edges=True), 128))
+    for got, x in zip(ctx.download_frame(12, pw, ph), want):
+        assert np.array_equal(got, x)
+    ctx.upload_frame(0, *blocky_frame(330, 250, 24))
+    with pytest.raises(Vc1cuError, match="padded raster"):
+        ctx.loop_filter(p, 0)

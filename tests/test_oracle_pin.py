@@ -494,3 +494,17 @@ def test_fast_transform_types_golden(oracle, i):
 def test_fast_transform_fixture_reaches_every_type():
     g = load("tt_kat.npz")
     assert set(np.concatenate([g[f"c{i}.types"] for i in range(len(TT_CASES))]).tolist()) == {1, 2, 3, 4}
+
+
+def test_loop_filter_padded_frame_matches_reference_live(oracle):
+    """The reference filters the padded reconstruction of its configuration; filtering that frame
+    under the padded raster's dimensions gives the same samples."""
+    from lf_cases import blocky_frame, metadata
+
+    Reference = _ref_or_skip()
+    fr = blocky_frame(336, 256, 25)
+    pp = make_params(336, 256, pqindex=13)
+    R = Reference(pp)
+    meta = metadata(322, 242, 26, True)
+    for x, y in zip(oracle.loop_filter(pp, fr, *meta), R.loop_filter(fr, *meta)):
+        assert np.array_equal(x, y)
