@@ -128,3 +128,22 @@ def test_random_configuration_reconstruction_matches_oracle(ctx, oracle, seed):
     ctx.intensity_compensate(0, ic, 9)
     for x, y in zip(ctx.download_frame(9, w, h), oracle.intensity_compensate(past, ic)):
         assert np.array_equal(x, y), (seed, ic)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_paired_passes_match_oracle(ctx, oracle, seed):
+    """A B picture's four unseeded passes in one call, as an encoder batches them: the two modes
+    run as two launches sharing each picture pair's global search; every pass equals the
+    oracle's."""
+    w, h, kw, motion = random_config(seed)
+    p = make_params(w, h, **kw)
+    clip = synth.generate(w, h, 3, 800 + seed, global_px=motion, n_objects=2, obj_min=8, obj_max=32)
+    frames = [clip.frame(f) for f in range(3)]
+    for f in range(3):
+        ctx.upload_frame(f, *frames[f])
+    passes = [(1, r, m, 0, -1, 260 + 2 * j + (r == 2), 0)
+              for j, m in enumerate((MV_QPEL, MV_HPEL_BILINEAR)) for r in (0, 2)]
+    ctx.core_passes(p, passes)
+    for t, r, m, _a, _s, slot, _q in passes:
+        e = oracle.analyze_p_core(p, frames[t], frames[r], m, False)
+        assert ctx.read_result(p, slot).equal(e) == [], (seed, m, r, kw)
