@@ -2128,9 +2128,11 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 // independent; a pass seeded by another pass of the launch is delayed behind it, so its
 // seed macroblock precedes it too. Items are handed out in order, hence no wait can
 // depend on an item that no running warp holds.
-// Two instantiations: kCoreAny runs any mix of passes; kCoreSeeded runs seeded passes only
-// (no integer-search code, so fewer registers and more resident warps). Four warps per
-// block; at most 65536 / (128 * min blocks) registers per thread.
+// Instantiations: kCoreAny runs any mix of passes; kCoreSeeded runs seeded passes only
+// (no integer-search code, so fewer registers and more resident warps); kCoreUnseeded runs
+// unseeded passes only (no seeded refinement or speculation code: the launches are bound by
+// instruction fetch, so the smaller footprint pays); the Wide forms are compiled for one block
+// per SM. Four warps per block; at most 65536 / (128 * min blocks) registers per thread.
 #ifndef VC1CU_CORE_MIN_BLOCKS
 #define VC1CU_CORE_MIN_BLOCKS 3
 #endif
@@ -2139,7 +2141,9 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #endif
 template <int KIND>
 __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS
-                                                           : (KIND == kCoreAnyWide ? 1 : VC1CU_CORE_MIN_BLOCKS))
+                                                           : (KIND == kCoreAnyWide || KIND == kCoreUnseededWide
+                                                                  ? 1
+                                                                  : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
@@ -2168,7 +2172,8 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         m.lam_m = d.lam_m;
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
-        const int mode = d.mode, seeded = KIND == kCoreSeeded ? 1 : d.seeded;
+        const int mode = d.mode,
+                  seeded = KIND == kCoreSeeded ? 1 : (KIND == kCoreUnseeded || KIND == kCoreUnseededWide ? 0 : d.seeded);
         const bool allow_intra = d.allow_intra && !P.disable_p_intra;
         const bool allow_4mv = mode == VC1CU_MV_MIXED;
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
@@ -2543,6 +2548,8 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
 const void* core_kernel(int kind) {
     if (kind == kCoreSeeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreSeeded>);
     if (kind == kCoreAnyWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAnyWide>);
+    if (kind == kCoreUnseeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseeded>);
+    if (kind == kCoreUnseededWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseededWide>);
     return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
 }
 
@@ -2553,6 +2560,10 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
         core_pass_kernel<kCoreSeeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     else if (kind == kCoreAnyWide)
         core_pass_kernel<kCoreAnyWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else if (kind == kCoreUnseeded)
+        core_pass_kernel<kCoreUnseeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else if (kind == kCoreUnseededWide)
+        core_pass_kernel<kCoreUnseededWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     else
         core_pass_kernel<kCoreAny><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     return cudaGetLastError();

@@ -62,6 +62,9 @@ constexpr int kCoreAny = 0;      // any mix of seeded and unseeded passes
 constexpr int kCoreSeeded = 1;   // seeded passes only
 constexpr int kCoreAnyWide = 2;  // kCoreAny compiled for one block per SM (all 255 registers), for
                                  // launches whose search windows let only one block per SM anyway
+constexpr int kCoreUnseeded = 3;      // unseeded passes only: the seeded refinement and its
+                                      // speculation are compiled out (a smaller instruction footprint)
+constexpr int kCoreUnseededWide = 4;  // kCoreUnseeded for one block per SM, like kCoreAnyWide
 
 // Shared-memory window geometry for one launch.
 struct WinCfg {
