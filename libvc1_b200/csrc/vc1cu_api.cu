@@ -804,10 +804,11 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     if (smem > (size_t)c->max_smem)
         throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
     const bool all_unseeded = (int)unseeded.size() == n;
-    int kind = all_unseeded ? kCoreUnseeded : (any_unseeded ? kCoreAny : kCoreSeeded);
+    const bool umh_local = P.me_algorithm == 0 && P.range == P.local_range;
+    int kind = all_unseeded ? (umh_local ? kCoreUmhLocal : kCoreUnseeded) : (any_unseeded ? kCoreAny : kCoreSeeded);
     // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
     if (kind != kCoreSeeded && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm)
-        kind = kind == kCoreAny ? kCoreAnyWide : kCoreUnseededWide;
+        kind = kind == kCoreAny ? kCoreAnyWide : (kind == kCoreUmhLocal ? kCoreUmhLocalWide : kCoreUnseededWide);
     const void* kern = core_kernel(kind);
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;

@@ -2141,7 +2141,8 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #endif
 template <int KIND>
 __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS
-                                                           : (KIND == kCoreAnyWide || KIND == kCoreUnseededWide
+                                                           : (KIND == kCoreAnyWide || KIND == kCoreUnseededWide ||
+                                                                      KIND == kCoreUmhLocalWide
                                                                   ? 1
                                                                   : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
@@ -2172,8 +2173,9 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         m.lam_m = d.lam_m;
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
-        const int mode = d.mode,
-                  seeded = KIND == kCoreSeeded ? 1 : (KIND == kCoreUnseeded || KIND == kCoreUnseededWide ? 0 : d.seeded);
+        constexpr bool kUmhOnly = KIND == kCoreUmhLocal || KIND == kCoreUmhLocalWide;
+        constexpr bool kUnseededOnly = KIND == kCoreUnseeded || KIND == kCoreUnseededWide || kUmhOnly;
+        const int mode = d.mode, seeded = KIND == kCoreSeeded ? 1 : (kUnseededOnly ? 0 : d.seeded);
         const bool allow_intra = d.allow_intra && !P.disable_p_intra;
         const bool allow_4mv = mode == VC1CU_MV_MIXED;
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
@@ -2307,8 +2309,8 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                 const PInfo pi = predictor_info(P, m);
                 const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
                 auto local_search = [&]() {
-                    return P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
-                                               : umh(P, m, pi, gdx, gdy, local_range, pixels);
+                    return !kUmhOnly && P.me_algorithm == 1 ? diamond(P, m, pi, gdx, gdy, local_range)
+                                                            : umh(P, m, pi, gdx, gdy, local_range, pixels);
                 };
                 // a distant candidate's MAE, kept when it is the least seen (record_distant, :176-183)
                 auto record = [&](uint64_t s, int decision) {
@@ -2319,7 +2321,7 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
                         dd = (uint8_t)decision;
                     }
                 };
-                const bool long_range = range > local_range;
+                const bool long_range = !kUmhOnly && range > local_range;
                 IntRes im{0, 0, UINT64_MAX};
                 if (P.long_range_mode == 2) {
                     // legacy distant-first policy (:144-160)
@@ -2550,6 +2552,8 @@ const void* core_kernel(int kind) {
     if (kind == kCoreAnyWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAnyWide>);
     if (kind == kCoreUnseeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseeded>);
     if (kind == kCoreUnseededWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseededWide>);
+    if (kind == kCoreUmhLocal) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUmhLocal>);
+    if (kind == kCoreUmhLocalWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUmhLocalWide>);
     return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
 }
 
@@ -2564,6 +2568,10 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
         core_pass_kernel<kCoreUnseeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     else if (kind == kCoreUnseededWide)
         core_pass_kernel<kCoreUnseededWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else if (kind == kCoreUmhLocal)
+        core_pass_kernel<kCoreUmhLocal><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    else if (kind == kCoreUmhLocalWide)
+        core_pass_kernel<kCoreUmhLocalWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     else
         core_pass_kernel<kCoreAny><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
     return cudaGetLastError();

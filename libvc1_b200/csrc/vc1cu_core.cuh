@@ -65,6 +65,9 @@ constexpr int kCoreAnyWide = 2;  // kCoreAny compiled for one block per SM (all 
 constexpr int kCoreUnseeded = 3;      // unseeded passes only: the seeded refinement and its
                                       // speculation are compiled out (a smaller instruction footprint)
 constexpr int kCoreUnseededWide = 4;  // kCoreUnseeded for one block per SM, like kCoreAnyWide
+constexpr int kCoreUmhLocal = 5;      // kCoreUnseeded for UMH with the search range equal to the
+                                      // local range: no diamond or long-range code
+constexpr int kCoreUmhLocalWide = 6;  // kCoreUmhLocal for one block per SM
 
 // Shared-memory window geometry for one launch.
 struct WinCfg {
