@@ -803,12 +803,19 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     const size_t smem = (size_t)warps * wc.warp_bytes;
     if (smem > (size_t)c->max_smem)
         throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
-    const bool all_unseeded = (int)unseeded.size() == n;
-    const bool umh_local = P.me_algorithm == 0 && P.range == P.local_range;
-    int kind = all_unseeded ? (umh_local ? kCoreUmhLocal : kCoreUnseeded) : (any_unseeded ? kCoreAny : kCoreSeeded);
+    // the instantiation: the code this launch's passes can reach (the kCore* flags)
+    bool any_mixed_pass = false;
+    for (int i = 0; i < n; ++i) any_mixed_pass |= passes[i].mode == VC1CU_MV_MIXED;
+    int kind = kCoreAny;
+    if (!any_unseeded) {
+        kind = kCoreSeededOnly;
+    } else if ((int)unseeded.size() == n) {
+        kind = kCoreUnseededOnly;
+        if (P.me_algorithm == 0 && P.range == P.local_range) kind |= kCoreUmhLocal;
+    }
+    if (!any_mixed_pass && (kind & (kCoreSeededOnly | kCoreUmhLocal))) kind |= kCoreNoMixed;
     // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
-    if (kind != kCoreSeeded && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm)
-        kind = kind == kCoreAny ? kCoreAnyWide : (kind == kCoreUmhLocal ? kCoreUmhLocalWide : kCoreUnseededWide);
+    if (!(kind & kCoreSeededOnly) && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm) kind |= kCoreWide;
     const void* kern = core_kernel(kind);
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;

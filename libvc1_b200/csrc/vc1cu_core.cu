@@ -2128,11 +2128,9 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 // independent; a pass seeded by another pass of the launch is delayed behind it, so its
 // seed macroblock precedes it too. Items are handed out in order, hence no wait can
 // depend on an item that no running warp holds.
-// Instantiations: kCoreAny runs any mix of passes; kCoreSeeded runs seeded passes only
-// (no integer-search code, so fewer registers and more resident warps); kCoreUnseeded runs
-// unseeded passes only (no seeded refinement or speculation code: the launches are bound by
-// instruction fetch, so the smaller footprint pays); the Wide forms are compiled for one block
-// per SM. Four warps per block; at most 65536 / (128 * min blocks) registers per thread.
+// Instantiations (the kCore* flags): kCoreAny runs any mix of passes; the flags compile out what
+// a launch's passes cannot reach (seeded-only launches also need fewer registers and hold more
+// resident warps). Four warps per block; at most 65536 / (128 * min blocks) registers per thread.
 #ifndef VC1CU_CORE_MIN_BLOCKS
 #define VC1CU_CORE_MIN_BLOCKS 3
 #endif
@@ -2140,11 +2138,8 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #define VC1CU_SEEDED_MIN_BLOCKS 4
 #endif
 template <int KIND>
-__global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BLOCKS
-                                                           : (KIND == kCoreAnyWide || KIND == kCoreUnseededWide ||
-                                                                      KIND == kCoreUmhLocalWide
-                                                                  ? 1
-                                                                  : VC1CU_CORE_MIN_BLOCKS))
+__global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_MIN_BLOCKS
+                                                                : ((KIND & kCoreWide) ? 1 : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
@@ -2173,11 +2168,11 @@ __global__ void __launch_bounds__(128, KIND == kCoreSeeded ? VC1CU_SEEDED_MIN_BL
         m.lam_m = d.lam_m;
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
-        constexpr bool kUmhOnly = KIND == kCoreUmhLocal || KIND == kCoreUmhLocalWide;
-        constexpr bool kUnseededOnly = KIND == kCoreUnseeded || KIND == kCoreUnseededWide || kUmhOnly;
-        const int mode = d.mode, seeded = KIND == kCoreSeeded ? 1 : (kUnseededOnly ? 0 : d.seeded);
+        constexpr bool kUmhOnly = (KIND & kCoreUmhLocal) != 0;
+        const int mode = d.mode,
+                  seeded = (KIND & kCoreSeededOnly) ? 1 : ((KIND & kCoreUnseededOnly) ? 0 : d.seeded);
         const bool allow_intra = d.allow_intra && !P.disable_p_intra;
-        const bool allow_4mv = mode == VC1CU_MV_MIXED;
+        const bool allow_4mv = !(KIND & kCoreNoMixed) && mode == VC1CU_MV_MIXED;
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
         PHASE_START((seeded ? 1 : 0) + (allow_4mv ? 2 : 0));
         bool ok = !*(volatile int*)&st->abort;
@@ -2546,34 +2541,36 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     return cudaGetLastError();
 }
 
-// Host-side handles of the instantiations (attributes, occupancy, launch).
+// Host-side handles of the instantiations (attributes, occupancy, launch): the flag sets the
+// host selects.
+#define VC1CU_CORE_KINDS(X)                                                                      \
+    X(kCoreAny) X(kCoreAny | kCoreWide) X(kCoreSeededOnly) X(kCoreSeededOnly | kCoreNoMixed)     \
+    X(kCoreUnseededOnly) X(kCoreUnseededOnly | kCoreWide) X(kCoreUnseededOnly | kCoreUmhLocal)   \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide) X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed) \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide)
+
 const void* core_kernel(int kind) {
-    if (kind == kCoreSeeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreSeeded>);
-    if (kind == kCoreAnyWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAnyWide>);
-    if (kind == kCoreUnseeded) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseeded>);
-    if (kind == kCoreUnseededWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUnseededWide>);
-    if (kind == kCoreUmhLocal) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUmhLocal>);
-    if (kind == kCoreUmhLocalWide) return reinterpret_cast<const void*>(&core_pass_kernel<kCoreUmhLocalWide>);
-    return reinterpret_cast<const void*>(&core_pass_kernel<kCoreAny>);
+    switch (kind) {
+#define VC1CU_KERNEL_CASE(k) \
+    case (k): return reinterpret_cast<const void*>(&core_pass_kernel<(k)>);
+        VC1CU_CORE_KINDS(VC1CU_KERNEL_CASE)
+#undef VC1CU_KERNEL_CASE
+        default: return nullptr;
+    }
 }
 
 cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,
                         const PassDesc* passes, int npass, const uint32_t* items, unsigned nitems, const WinCfg& wc,
                         uint32_t epoch, LaunchStatus* st) {
-    if (kind == kCoreSeeded)
-        core_pass_kernel<kCoreSeeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else if (kind == kCoreAnyWide)
-        core_pass_kernel<kCoreAnyWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else if (kind == kCoreUnseeded)
-        core_pass_kernel<kCoreUnseeded><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else if (kind == kCoreUnseededWide)
-        core_pass_kernel<kCoreUnseededWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else if (kind == kCoreUmhLocal)
-        core_pass_kernel<kCoreUmhLocal><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else if (kind == kCoreUmhLocalWide)
-        core_pass_kernel<kCoreUmhLocalWide><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
-    else
-        core_pass_kernel<kCoreAny><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st);
+    switch (kind) {
+#define VC1CU_LAUNCH_CASE(k)                                                                              \
+    case (k):                                                                                          \
+        core_pass_kernel<(k)><<<grid, block, smem, s>>>(P, passes, npass, items, nitems, wc, epoch, st); \
+        break;
+        VC1CU_CORE_KINDS(VC1CU_LAUNCH_CASE)
+#undef VC1CU_LAUNCH_CASE
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

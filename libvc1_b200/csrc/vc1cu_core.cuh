@@ -57,17 +57,17 @@ struct PassDesc {
     DevResult out;
 };
 
-// core_pass_kernel instantiations
-constexpr int kCoreAny = 0;      // any mix of seeded and unseeded passes
-constexpr int kCoreSeeded = 1;   // seeded passes only
-constexpr int kCoreAnyWide = 2;  // kCoreAny compiled for one block per SM (all 255 registers), for
-                                 // launches whose search windows let only one block per SM anyway
-constexpr int kCoreUnseeded = 3;      // unseeded passes only: the seeded refinement and its
-                                      // speculation are compiled out (a smaller instruction footprint)
-constexpr int kCoreUnseededWide = 4;  // kCoreUnseeded for one block per SM, like kCoreAnyWide
-constexpr int kCoreUmhLocal = 5;      // kCoreUnseeded for UMH with the search range equal to the
-                                      // local range: no diamond or long-range code
-constexpr int kCoreUmhLocalWide = 6;  // kCoreUmhLocal for one block per SM
+// core_pass_kernel instantiations, as flags: each flag compiles out code that the launch's
+// passes cannot reach (the launches are bound by instruction fetch, so a smaller footprint pays).
+constexpr int kCoreSeededOnly = 1;    // every pass seeded: no integer-search code
+constexpr int kCoreUnseededOnly = 2;  // every pass unseeded: no seeded refinement or speculation
+constexpr int kCoreUmhLocal = 4;      // (with kCoreUnseededOnly) UMH with the search range equal to
+                                      // the local range: no diamond or long-range code
+constexpr int kCoreNoMixed = 8;       // (with kCoreSeededOnly or kCoreUmhLocal) no Mixed-MV pass: no 4-MV code
+constexpr int kCoreWide = 16;         // one block per SM, all 255 registers (search windows that large
+                                      // leave room for one block anyway); not with kCoreSeededOnly
+constexpr int kCoreAny = 0;
+constexpr int kCoreSeeded = kCoreSeededOnly;
 
 // Shared-memory window geometry for one launch.
 struct WinCfg {
