@@ -1617,27 +1617,42 @@ __device__ __forceinline__ void ref_unpack(uint32_t ctx, DevParams& P, Mb& m) {
     m.sm.list_satd.off = r.satd;
 }
 
+// DR: the launch runs the default refinement (me_quality SATD, the full stencils); fixing those
+// parameters lets the compiler drop the other refinements from these hot functions.
+template <bool DR>
+__device__ __forceinline__ void refine_defaults(DevParams& P) {
+    if (DR) {
+        P.me_quality = 2;
+        P.fast_subpel = 0;
+    }
+}
+
+template <bool DR>
 __device__ __noinline__ Shortlist refine_prepare_ool(uint32_t ctx, int bx, int by, int bw, int bh, int2 seed, int range,
                                                      int mode, uint64_t known, bool satd_all) {
     DevParams P;
     Mb m{};
     ref_unpack(ctx, P, m);
+    refine_defaults<DR>(P);
     return refine_prepare(P, m, bx, by, bw, bh, seed, range, mode, known, satd_all);
 }
 
+template <bool DR>
 __device__ __noinline__ RefineOut refine_select_ool(uint32_t ctx, const Shortlist sl, int bx, int by, int bw, int bh,
                                                     int mode, const PInfo pi, bool more) {
     DevParams P;
     Mb m{};
     ref_unpack(ctx, P, m);
+    refine_defaults<DR>(P);
     return refine_select(P, m, sl, bx, by, bw, bh, mode, pi, more);
 }
 
+template <bool DR>
 __device__ __forceinline__ RefineOut refine_staged(const DevParams& P, const Mb& m, int bx, int by, int bw, int bh, int2 seed,
                                                    int range, int mode, const PInfo& pi, bool more, uint64_t known) {
     const uint32_t r = m.sm.ctx.off;
-    const Shortlist sl = refine_prepare_ool(r, bx, by, bw, bh, seed, range, mode, known, false);
-    return refine_select_ool(r, sl, bx, by, bw, bh, mode, pi, more);
+    const Shortlist sl = refine_prepare_ool<DR>(r, bx, by, bw, bh, seed, range, mode, known, false);
+    return refine_select_ool<DR>(r, sl, bx, by, bw, bh, mode, pi, more);
 }
 
 // ---- shortlists parked across the wavefront wait -----------------------------------------
@@ -2169,6 +2184,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
         m.lam_s = d.lam_s;
         const DevResult& o = d.out;
         constexpr bool kUmhOnly = (KIND & kCoreUmhLocal) != 0;
+        constexpr bool kDR = (KIND & kCoreDefaultRefine) != 0;
         const int mode = d.mode,
                   seeded = (KIND & kCoreSeededOnly) ? 1 : ((KIND & kCoreUnseededOnly) ? 0 : d.seeded);
         const bool allow_intra = d.allow_intra && !P.disable_p_intra;
@@ -2229,7 +2245,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                 publish_ctx(P, m);
                 window_wait();
                 PHASE_MARK(2);
-                sl = refine_prepare_ool(m.sm.ctx.off, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
+                sl = refine_prepare_ool<kDR>(m.sm.ctx.off, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
                 PHASE_MARK(3);
                 dl = __ldcg(&d.seed_dl[m.pos]);
                 dc = __ldcg(&d.seed_dc[m.pos]);
@@ -2240,7 +2256,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                     const Field fg{cur4g, m.sm.nb_bmv, m.sm.nb_intra, P.mbw, P.mbh, m.mx, m.my};
                     const PInfo pig = predictor_mixed_1mv(P, fg, m.mx, m.my);
                     shortlist_save(m, 0, sl, seed, 0, 0);
-                    const RefineOut og = refine_select_ool(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, pig, true);
+                    const RefineOut og = refine_select_ool<kDR>(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, pig, true);
                     spec_result_save(m, 0, pig, og);
                     one_g = og.mv;
                     if (hidden_padding(P, m.x0, m.y0, 16, 16, one_g.x, one_g.y, one_mode, true)) one_g = make_int2(0, 0);
@@ -2255,9 +2271,9 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                             const SeedPick b10 = pick_4mv_seed(m, true);
                             const SeedPick bf = pick_4mv_seed(m, false);
                             const uint32_t rc = m.sm.ctx.off;
-                            const Shortlist sk = refine_prepare_ool(rc, bx, by, 8, 8, bf.v, range, VC1CU_MV_MIXED, bf.cost, true);
+                            const Shortlist sk = refine_prepare_ool<kDR>(rc, bx, by, 8, 8, bf.v, range, VC1CU_MV_MIXED, bf.cost, true);
                             shortlist_save(m, k + 1, sk, bf.v, bf.cost, bf.slot);
-                            const RefineOut rk = refine_select_ool(rc, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4g, true);
+                            const RefineOut rk = refine_select_ool<kDR>(rc, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4g, true);
                             if (m.lane == 0) {
                                 SpecBlk& sb = m.sm.spec_blk[k + 1];
                                 sb.b10 = b10.v;
@@ -2298,7 +2314,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                     one = m.sm.spec_blk[0].res;
                 } else {
                     if (spec) shortlist_restore(m, 0);
-                    one = refine_select_ool(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
+                    one = refine_select_ool<kDR>(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
                 }
             } else {
                 const PInfo pi = predictor_info(P, m);
@@ -2362,7 +2378,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                     }
                 }
                 PHASE_MARK(7);
-                one = refine_staged(P, m, m.x0, m.y0, 16, 16, make_int2(im.dx * 4, im.dy * 4), range, one_mode, rate_pi,
+                one = refine_staged<kDR>(P, m, m.x0, m.y0, 16, 16, make_int2(im.dx * 4, im.dy * 4), range, one_mode, rate_pi,
                                     true, im.cost);
             }
             PHASE_MARK(8);
@@ -2412,7 +2428,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                         } else if (sb.seed_slot != 2) {
                             // the parked shortlist was refined from this same seed
                             const Shortlist sk = shortlist_restore(m, k + 1);
-                            r = refine_select_ool(m.sm.ctx.off, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
+                            r = refine_select_ool<kDR>(m.sm.ctx.off, sk, bx, by, 8, 8, VC1CU_MV_MIXED, pi4, true);
                             have = true;
                         } else {
                             best_seed = b.v;
@@ -2426,7 +2442,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                         seed_cost = b.cost;
                     }
                     PHASE_MARK(9);
-                    if (!have) r = refine_staged(P, m, bx, by, 8, 8, best_seed, range, VC1CU_MV_MIXED, pi4, true, seed_cost);
+                    if (!have) r = refine_staged<kDR>(P, m, bx, by, 8, 8, best_seed, range, VC1CU_MV_MIXED, pi4, true, seed_cost);
                     PHASE_MARK(10);
                     four_screen += r.screen_sad;
                     if (m.lane == 0) cur4[k] = r.mv;
@@ -2547,7 +2563,12 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     X(kCoreAny) X(kCoreAny | kCoreWide) X(kCoreSeededOnly) X(kCoreSeededOnly | kCoreNoMixed)     \
     X(kCoreUnseededOnly) X(kCoreUnseededOnly | kCoreWide) X(kCoreUnseededOnly | kCoreUmhLocal)   \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide) X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed) \
-    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide)
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide)                                \
+    X(kCoreSeededOnly | kCoreDefaultRefine) X(kCoreSeededOnly | kCoreNoMixed | kCoreDefaultRefine)   \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreDefaultRefine)                                      \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide | kCoreDefaultRefine)                          \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreDefaultRefine)                       \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine)
 
 const void* core_kernel(int kind) {
     switch (kind) {

@@ -66,6 +66,8 @@ constexpr int kCoreUmhLocal = 4;      // (with kCoreUnseededOnly) UMH with the s
 constexpr int kCoreNoMixed = 8;       // (with kCoreSeededOnly or kCoreUmhLocal) no Mixed-MV pass: no 4-MV code
 constexpr int kCoreWide = 16;         // one block per SM, all 255 registers (search windows that large
                                       // leave room for one block anyway); not with kCoreSeededOnly
+constexpr int kCoreDefaultRefine = 32;  // (with kCoreSeededOnly or kCoreUmhLocal) me_quality SATD and the
+                                        // full sub-pel stencils: no SAD-only, RATE or fast refinement code
 constexpr int kCoreAny = 0;
 constexpr int kCoreSeeded = kCoreSeededOnly;
 
