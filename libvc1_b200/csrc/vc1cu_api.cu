@@ -815,6 +815,9 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     }
     if (!any_mixed_pass && (kind & (kCoreSeededOnly | kCoreUmhLocal))) kind |= kCoreNoMixed;
     if (P.me_quality == 2 && !P.fast_subpel && (kind & (kCoreSeededOnly | kCoreUmhLocal))) kind |= kCoreDefaultRefine;
+    bool any_intra_pass = false;
+    for (int i = 0; i < n; ++i) any_intra_pass |= passes[i].allow_intra != 0;
+    if (!any_intra_pass && (kind & kCoreDefaultRefine)) kind |= kCoreNoIntra;
     // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
     if (!(kind & kCoreSeededOnly) && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm) kind |= kCoreWide;
     const void* kern = core_kernel(kind);

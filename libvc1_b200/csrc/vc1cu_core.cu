@@ -2187,7 +2187,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
         constexpr bool kDR = (KIND & kCoreDefaultRefine) != 0;
         const int mode = d.mode,
                   seeded = (KIND & kCoreSeededOnly) ? 1 : ((KIND & kCoreUnseededOnly) ? 0 : d.seeded);
-        const bool allow_intra = d.allow_intra && !P.disable_p_intra;
+        const bool allow_intra = !(KIND & kCoreNoIntra) && d.allow_intra && !P.disable_p_intra;
         const bool allow_4mv = !(KIND & kCoreNoMixed) && mode == VC1CU_MV_MIXED;
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
         PHASE_START((seeded ? 1 : 0) + (allow_4mv ? 2 : 0));
@@ -2568,7 +2568,13 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreDefaultRefine)                                      \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide | kCoreDefaultRefine)                          \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreDefaultRefine)                       \
-    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine)
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine)                 \
+    X(kCoreSeededOnly | kCoreDefaultRefine | kCoreNoIntra)                                              \
+    X(kCoreSeededOnly | kCoreNoMixed | kCoreDefaultRefine | kCoreNoIntra)                               \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreDefaultRefine | kCoreNoIntra)                            \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)                \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreDefaultRefine | kCoreNoIntra)             \
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)
 
 const void* core_kernel(int kind) {
     switch (kind) {

@@ -68,6 +68,7 @@ constexpr int kCoreWide = 16;         // one block per SM, all 255 registers (se
                                       // leave room for one block anyway); not with kCoreSeededOnly
 constexpr int kCoreDefaultRefine = 32;  // (with kCoreSeededOnly or kCoreUmhLocal) me_quality SATD and the
                                         // full sub-pel stencils: no SAD-only, RATE or fast refinement code
+constexpr int kCoreNoIntra = 64;        // (with kCoreDefaultRefine) no pass allows P-intra: no intra code
 constexpr int kCoreAny = 0;
 constexpr int kCoreSeeded = kCoreSeededOnly;
 
