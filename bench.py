@@ -68,7 +68,7 @@ WORKLOAD = ("1080p IBBP analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP as the
 # DRAM bytes (read + write) of core_pass_kernel per launch on this workload: an ncu capture of the
 # first GOP's six core launches (121.6 MB; profiles/core_pass_kernel_1080p_first_gop.md) scaled by
 # macroblocks to the five GOPs of a step and divided over the step's six launches.
-CORE_DRAM_BYTES_PER_LAUNCH = 119.9e6 * 5 / 6  # ncu, first GOP (6 launches), scaled to the 5 GOPs of a step
+CORE_DRAM_BYTES_PER_LAUNCH = 119.6e6 * 5 / 6  # ncu, first GOP (6 launches), scaled to the 5 GOPs of a step
 P_PASSES = ("unseeded", "seeded_hpel", "seeded_bilinear", "seeded_mixed", "final_mixed_intra")
 B_PASSES = ("b_qpel_forward", "b_qpel_backward", "b_bilinear_forward", "b_bilinear_backward")
 XFORM_FLOPS_PER_MB = 51911.5
