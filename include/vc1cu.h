@@ -177,6 +177,20 @@ const char* vc1cu_last_error(const vc1cu_ctx* ctx);
 int vc1cu_counters_get(const vc1cu_ctx* ctx, vc1cu_counters* out);
 int vc1cu_reset_counters(vc1cu_ctx* ctx);
 
+/*
+ * Test hooks of the wavefront waits' failure path (no counterpart in the reference, whose CPU
+ * loop has no waits). A core-pass macroblock waits for its left, top-left, top and top-right
+ * neighbours' done flags; a wait gives up after 2^log2_polls polls (default 24, a few seconds),
+ * aborts the launch and makes the call that reads its results fail with VC1CU_ERR_TIMEOUT and a
+ * message naming the first waiting work item ("pass P of its launch, macroblock M") and its
+ * lanes still waiting. The context stays usable: the next call starts clean.
+ * vc1cu_debug_set_wait_limit sets the limit (6..24) for every later core launch.
+ * vc1cu_debug_withhold_publish makes the NEXT core launch skip publishing the done flag of one
+ * work item (pass_index within that launch, macroblock index mb); (-1, -1) cancels it.
+ */
+int vc1cu_debug_set_wait_limit(vc1cu_ctx* ctx, int log2_polls);
+int vc1cu_debug_withhold_publish(vc1cu_ctx* ctx, int pass_index, int mb);
+
 /* Turns per-launch event timing on (1) or off (0); vc1cu_timing_get synchronises the
  * context stream and returns the sums; vc1cu_reset_counters clears them. */
 int vc1cu_set_timing(vc1cu_ctx* ctx, int enable);
@@ -550,8 +564,12 @@ int vc1cu_store_signed(vc1cu_ctx* ctx, const vc1cu_params* p, const int32_t* d_y
  * results; calls issued in order on one stream are safe, and devices are independent.
  * Each call resets the state it reads, so nothing carries over from an earlier call.
  *
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture begins.
+ * width and height may be odd (any coding size up to 16384); pitch >= width.
+ *
+ * Every call looks up the array's device address (cudaGetSymbolAddress, with the caller's
+ * device current), so the address always belongs to the module loaded in the current context,
+ * also after a cudaDeviceReset. The first call on a device may load the library's device code
+ * into the context; make that first call before any stream capture begins.
  * On failure a message is written to err (err_len bytes, may be NULL).
  */
 int vc1cu_global_motion_noalloc(const uint8_t* const* cur_y, const uint8_t* const* ref_y, int pitch,

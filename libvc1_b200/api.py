@@ -38,7 +38,7 @@ EXPORTS = (
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
     "vc1cu_estimate_intensity_enqueue", "vc1cu_estimate_intensity_collect",
-    "vc1cu_fast_transform_types",
+    "vc1cu_fast_transform_types", "vc1cu_debug_set_wait_limit", "vc1cu_debug_withhold_publish",
 )
 
 
@@ -80,6 +80,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_forward_quant.argtypes = [vp, PP, i32, i32, i32, vp, vp]
     L.vc1cu_forward_quant_device.argtypes = [vp, PP, i32, i32, i32, vp, vp]
     L.vc1cu_set_timing.argtypes = [vp, i32]
+    L.vc1cu_debug_set_wait_limit.argtypes = [vp, i32]
+    L.vc1cu_debug_withhold_publish.argtypes = [vp, i32, i32]
     L.vc1cu_timing_get.argtypes = [vp, C.POINTER(Timing)]
     L.vc1cu_stream.argtypes = [vp]
     L.vc1cu_stream.restype = vp
@@ -191,6 +193,14 @@ class CudaComputeContext:
 
     def reset_counters(self):
         self._check(self._L.vc1cu_reset_counters(self._h))
+
+    def debug_set_wait_limit(self, log2_polls: int):
+        """Wavefront waits give up after 2**log2_polls polls (6..24) in later core launches."""
+        self._check(self._L.vc1cu_debug_set_wait_limit(self._h, int(log2_polls)))
+
+    def debug_withhold_publish(self, pass_index: int, mb: int):
+        """The next core launch does not publish the done flag of (pass_index, mb)."""
+        self._check(self._L.vc1cu_debug_withhold_publish(self._h, int(pass_index), int(mb)))
 
     def set_timing(self, enable: bool):
         self._check(self._L.vc1cu_set_timing(self._h, int(enable)))

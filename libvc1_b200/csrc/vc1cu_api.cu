@@ -256,6 +256,8 @@ struct vc1cu_ctx {
     } staging_ring[kStagingRing];
     int staging_next = 0, staging_cur = 0;
     uint32_t epoch = 0;
+    int wait_log2 = 24;                  // vc1cu_debug_set_wait_limit
+    uint32_t withhold_next = 0xFFFFFFFFu;  // vc1cu_debug_withhold_publish (next core launch only)
     int sm_count = 0;
     int max_smem = 0;
     int max_smem_sm = 0;  // shared memory per SM
@@ -358,6 +360,8 @@ int make_dev_params(const vc1cu_params* p, DevParams& P, std::string& why) {
     P.disable_b_intra = p->disable_b_intra != 0;
     const int r = p->search_range;
     P.mvrange = r <= 31 ? 0 : (r <= 63 ? 1 : (r <= 127 ? 2 : 3));
+    P.wait_log2 = 24;
+    P.withhold = 0xFFFFFFFFu;
     const double lam = 0.35 * static_cast<double>(p->pqindex);
     P.lambda = std::max(1.0, lam);
     int e = 0;
@@ -837,6 +841,9 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         Timer tm(c, kCore);
         unsigned nitems = 0;
         const uint32_t* items = work_items(c, P.mbw, P.mbh, level, nitems);
+        P.wait_log2 = c->wait_log2;
+        P.withhold = c->withhold_next;
+        c->withhold_next = 0xFFFFFFFFu;
         ck(launch_core(kind, grid, 32 * warps, smem, c->stream, P, c->d_passes, n, items, nitems, wc, c->epoch,
                        c->d_status),
            "core_pass_kernel launch");
@@ -1570,6 +1577,27 @@ int vc1cu_reset_counters(vc1cu_ctx* c) {
         collect_timing(c);
         c->counters = vc1cu_counters{};
         c->tsum = vc1cu_timing{};
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_debug_set_wait_limit(vc1cu_ctx* c, int log2_polls) {
+    return guarded(c, [&]() -> int {
+        if (log2_polls < 6 || log2_polls > 24) throw Fail{VC1CU_ERR_ARG, "log2_polls must be 6..24"};
+        c->wait_log2 = log2_polls;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_debug_withhold_publish(vc1cu_ctx* c, int pass_index, int mb) {
+    return guarded(c, [&]() -> int {
+        if (pass_index < 0 && mb < 0) {
+            c->withhold_next = 0xFFFFFFFFu;
+            return VC1CU_OK;
+        }
+        if (pass_index < 0 || pass_index > 0x7FF || mb < 0 || mb > 0xFFFFF)
+            throw Fail{VC1CU_ERR_ARG, "pass_index must be 0..2047 and mb 0..2^20-1 (or both -1)"};
+        c->withhold_next = ((uint32_t)pass_index << 20) | (uint32_t)mb;
         return VC1CU_OK;
     });
 }

@@ -33,6 +33,8 @@ struct DevParams {
     int mant_bits;       // significand width of the host's long double (64: x87)
     double distant_match_max_mae;
     double inter_intra_threshold;
+    int wait_log2;       // a wavefront wait gives up after 2^wait_log2 polls (default 24)
+    uint32_t withhold;   // work item whose done flag is not published (test hook; 0xFFFFFFFF: none)
 };
 
 __host__ __device__ inline int imin(int a, int b) { return a < b ? a : b; }

@@ -1953,13 +1953,15 @@ __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gp
 // Waits (bounded) until each lane's flag equals epoch (a macroblock of this launch was
 // published; a lane with a null flag waits for nothing). The flags are polled with relaxed
 // loads, all lanes at once, and one acquire fence follows the last poll, so a poll costs
-// no L1 invalidation. Every lane calls it. On timeout it raises the launch's error and
-// abort flags and returns false.
+// no L1 invalidation. Every lane calls it. After 2^log2_limit polls it gives up: it raises
+// the launch's error and abort flags and returns false (a wait that sees the abort flag
+// returns false at once).
 // code: the waiting work item, recorded (with the lanes still waiting) by the first wait
 // that gives up.
-__device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* st, uint32_t code) {
+__device__ bool wait_flags(const uint32_t* flag, uint32_t epoch, LaunchStatus* st, uint32_t code, int log2_limit) {
     bool mine = flag == nullptr;
-    for (long it = 0; it < (1L << 24); ++it) {
+    const long limit = 1L << log2_limit;
+    for (long it = 0; it < limit; ++it) {
         if (!mine) mine = ld_relaxed(flag) == epoch;
         if (__all_sync(FULL, mine)) {
             // the observing lanes acquire; the warp barrier orders the other lanes' reads after it
@@ -1992,7 +1994,7 @@ __device__ bool wait_neighbours(const DevParams& P, const DevResult& o, int mx, 
         const int x = mx + (lane == 3 ? 1 : (lane == 2 ? 0 : -1)), y = my - (lane == 0 ? 0 : 1);
         if (x >= 0 && y >= 0 && x < P.mbw) f = &o.done[y * P.mbw + x];
     }
-    return wait_flags(f, epoch, st, code);
+    return wait_flags(f, epoch, st, code, P.wait_log2);
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
@@ -2194,7 +2196,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
         bool ok = !*(volatile int*)&st->abort;
         // a seed produced by another pass of this launch
         if (ok && d.seed_pass >= 0)
-            ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st, code);
+            ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st, code, P.wait_log2);
         PHASE_MARK(0);
         if (ok) load_cur(P, m, d.cur);
         PHASE_MARK(1);
@@ -2513,7 +2515,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
             }
         }
         __syncwarp();
-        if (m.lane == 0) {
+        if (m.lane == 0 && code != P.withhold) {
             __threadfence();
             st_release(&o.done[m.pos], epoch);
         }

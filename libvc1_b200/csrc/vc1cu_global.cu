@@ -10,7 +10,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "vc1cu_core.cuh"
 
@@ -413,12 +412,6 @@ __global__ void noalloc_init_kernel(GState* states, const __grid_constant__ NoAl
 
 namespace {
 
-// Device address of g_noalloc_states per device ordinal, looked up once per device with
-// that device current (the host-side name of a __device__ array is not a device address).
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-vc1cu::GState* g_noalloc_ptr[kMaxDevices] = {};
-
 int noalloc_fail(char* err, size_t err_len, int code, const char* msg) {
     if (err && err_len) std::snprintf(err, err_len, "%s", msg);
     return code;
@@ -434,9 +427,9 @@ extern "C" int vc1cu_global_motion_noalloc(const uint8_t* const* cur_y, const ui
     if (n < 1 || n > kNoAllocMaxPictures)
         return noalloc_fail(err, err_len, VC1CU_ERR_ARG,
                             "vc1cu_global_motion_noalloc: n must be 1..16 pictures per call (the fixed scratch size)");
-    if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || width > 16384 || height > 16384 || pitch < width)
+    if (width <= 0 || height <= 0 || width > 16384 || height > 16384 || pitch < width)
         return noalloc_fail(err, err_len, VC1CU_ERR_ARG,
-                            "vc1cu_global_motion_noalloc: width/height must be even, 1..16384, pitch >= width");
+                            "vc1cu_global_motion_noalloc: width/height must be 1..16384 and pitch >= width");
     if (range < 0 || range > 32)
         return noalloc_fail(err, err_len, VC1CU_ERR_ARG, "vc1cu_global_motion_noalloc: range must be 0..32");
     if (!cur_y || !ref_y || !d_dxdy || !d_sad)
@@ -452,24 +445,15 @@ extern "C" int vc1cu_global_motion_noalloc(const uint8_t* const* cur_y, const ui
     a.out_sad = reinterpret_cast<unsigned long long*>(d_sad);
     a.range = range;
     a.n = n;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return noalloc_fail(err, err_len, VC1CU_ERR_CUDA, cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices)
-        return noalloc_fail(err, err_len, VC1CU_ERR_UNSUPPORTED, "vc1cu_global_motion_noalloc: device ordinal >= 64");
-    GState* states = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_noalloc_states);
-            if (e != cudaSuccess || !ptr)
-                return noalloc_fail(err, err_len, VC1CU_ERR_CUDA,
-                                    e != cudaSuccess ? cudaGetErrorString(e) : "cudaGetSymbolAddress returned null");
-            g_noalloc_ptr[dev] = static_cast<GState*>(ptr);
-        }
-        states = g_noalloc_ptr[dev];
-    }
+    // The host-side name of a __device__ array is not a device address. The address is looked
+    // up on every call, with the caller's device current, so it is always the one of the module
+    // loaded in the current context (a cached value would dangle after cudaDeviceReset).
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_states);
+    if (e != cudaSuccess || !ptr)
+        return noalloc_fail(err, err_len, VC1CU_ERR_CUDA,
+                            e != cudaSuccess ? cudaGetErrorString(e) : "cudaGetSymbolAddress returned null");
+    GState* states = static_cast<GState*>(ptr);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     noalloc_init_kernel<<<1, 32, 0, s>>>(states, a);
     e = cudaGetLastError();
