@@ -240,6 +240,32 @@ int vc1cu_score_motion_batch_law(vc1cu_ctx* ctx, const vc1cu_params* p, int law,
  * later work has started (or vc1cu_synchronize); from pageable memory it returns once staged. */
 int vc1cu_upload_frame(vc1cu_ctx* ctx, int frame_id, const uint8_t* y, const uint8_t* u,
                        const uint8_t* v, int width, int height);
+/*
+ * Seeded synthetic clip content generated on the device (no counterpart in the reference): the
+ * benchmark workloads' generator, bit-identical to the host generator of this library
+ * (libvc1_b200/csrc/vc1synth.c): 3-octave value-noise background with a per-frame global
+ * translation and zoom, moving textured rectangles, Irwin-Hall sensor noise. Layout mirrors
+ * vc1synth_cfg.
+ */
+typedef struct vc1cu_synth_cfg {
+    int32_t width;             /* even */
+    int32_t height;            /* even */
+    int32_t frames;            /* length of the clip the frames belong to */
+    int32_t n_objects;         /* 0..64 */
+    uint64_t seed;
+    double global_range_x_px;  /* per-frame global translation drawn in [-r, r] at quarter-pel */
+    double global_range_y_px;
+    int32_t obj_min;           /* rectangle side range, pixels */
+    int32_t obj_max;
+    double obj_vel_px;         /* object velocity drawn in [-v, v] px/frame at quarter-pel */
+    double zoom;               /* per-frame zoom about the frame centre, 1.0 = none */
+    double noise_sigma;        /* Gaussian (Irwin-Hall) noise standard deviation */
+} vc1cu_synth_cfg;
+
+/* Frames first .. first+count-1 (count 1..64) of the clip cfg describes into frame slots
+ * frame_id0 .. frame_id0+count-1. Asynchronous on the context stream. */
+int vc1cu_synth_frames(vc1cu_ctx* ctx, const vc1cu_synth_cfg* cfg, int first, int count, int frame_id0);
+
 /* Reads a frame slot back (for tests). */
 int vc1cu_download_frame(vc1cu_ctx* ctx, int frame_id, uint8_t* y, uint8_t* u, uint8_t* v);
 
@@ -534,6 +560,72 @@ int vc1cu_overlap_smooth(vc1cu_ctx* ctx, const vc1cu_params* p, int32_t* d_y, in
  */
 int vc1cu_store_signed(vc1cu_ctx* ctx, const vc1cu_params* p, const int32_t* d_y, const int32_t* d_u,
                        const int32_t* d_v, int bias, const uint8_t* mb_mask, int out_id);
+
+/* ---- learned motion-vector proposals ---------------------------------------------- */
+
+/*
+ * No counterpart in the reference: a small convolutional network that proposes, per macroblock,
+ * K = 4 integer-pixel vectors which replace the integer search (UMH / diamond / long range,
+ * encoder_motion.cpp:1781-2023, :1658-1779) of an unseeded analysis pass; the exact part of the
+ * pass stays: the candidates' full-resolution SADs, a short descent about the best, and the
+ * staged sub-pel refinement of refine_motion_block_staged (encoder_motion.cpp:3271-3594). A
+ * macroblock whose best match is not good (motion_match_good, encoder_motion.cpp:1627-1635: more
+ * than 6 levels of mean absolute error) falls back to the plain search.
+ *
+ * The network reads the current and reference pictures at quarter resolution plus the picture's
+ * dominant translation (found by an exhaustive quarter-resolution search over the search range),
+ * runs four 3x3 convolutions of 32 channels (BF16 weights, FP32 accumulation on the tensor
+ * cores), pools each macroblock and projects to two hypotheses (zero vector, translation), each
+ * with a logit and an offset. It is trained on the device by its own backward kernels on
+ * (picture pair, plain-search vector) samples.
+ *
+ * A vc1cu_lp belongs to one context and one raster (width x height) and search range; it holds
+ * `capacity` samples (features, hint, labels, candidates, fallback flags) and trains or proposes
+ * on up to `max_batch` samples at once. Calls are asynchronous on the context stream unless noted.
+ */
+typedef struct vc1cu_lp vc1cu_lp;
+
+/* Number of fp32 parameters (four conv layers W[32][9][Cin] + b[32], then the 8x32 projection
+ * and its 8 biases, in that order). */
+int vc1cu_lp_param_count(void);
+int vc1cu_lp_create(vc1cu_ctx* ctx, int width, int height, int search_range, int capacity, int max_batch,
+                    uint64_t seed, vc1cu_lp** out);
+int vc1cu_lp_destroy(vc1cu_lp* net);
+/* Synchronous copies of the fp32 parameters; set also restarts the optimiser. */
+int vc1cu_lp_get_params(vc1cu_lp* net, float* out);
+int vc1cu_lp_set_params(vc1cu_lp* net, const float* in);
+/* Sample `sample` := the features and translation hint of the pair (cur_id, ref_id). */
+int vc1cu_lp_prepare(vc1cu_lp* net, int cur_id, int ref_id, int sample);
+/* Its labels := the integer-pixel vectors (nearest pixel) of a plain pass in result slot. */
+int vc1cu_lp_set_labels(vc1cu_lp* net, int sample, int result_slot);
+/* One Adam step (lr; betas 0.9 / 0.999) on the batch; *loss = the batch's mean loss before it.
+ * Synchronous. */
+int vc1cu_lp_train_step(vc1cu_lp* net, const int* samples, int n, float lr, float* loss);
+/* The batch's loss and every parameter's gradient (host, vc1cu_lp_param_count floats), without
+ * an update. Synchronous. */
+int vc1cu_lp_gradients(vc1cu_lp* net, const int* samples, int n, float* grads, float* loss);
+/* Inference on samples first .. first+n-1: their candidates. */
+int vc1cu_lp_propose(vc1cu_lp* net, int first_sample, int n);
+/* Reads a sample back (any pointer may be NULL): features (W4*H4*16 bf16 bit patterns, W4 =
+ * 4*mbw, H4 = 4*mbh, sample-major, channel fastest), hint, candidates (4 per MB), fallback flags.
+ * Synchronous. */
+int vc1cu_lp_read_sample(vc1cu_lp* net, int sample, uint16_t* features, vc1cu_mv* hint, vc1cu_mv* candidates,
+                         uint8_t* fallback);
+
+/* One learned analysis pass (the counterpart of an unseeded 1-MV core pass without P-intra). */
+typedef struct vc1cu_lp_pass {
+    int32_t cur_id;
+    int32_t ref_id;
+    int32_t sample;     /* the sample holding this pair's candidates and hint */
+    int32_t mode;       /* VC1CU_MV_QPEL, _HPEL or _HPEL_BILINEAR */
+    int32_t out_slot;   /* result slot, read with vc1cu_read_result */
+    int32_t pqindex;    /* 0 = params->pqindex */
+} vc1cu_lp_pass;
+
+/* n learned passes in one launch; with fallback != 0 a second launch runs the plain search
+ * (params' algorithm and ranges, the hint as its global vector) on the macroblocks the first
+ * flagged, in wavefront order over the learned field. */
+int vc1cu_lp_analyze(vc1cu_lp* net, const vc1cu_params* p, const vc1cu_lp_pass* passes, int n, int fallback);
 
 /* ---- allocation-free whole-frame translation search ------------------------------ */
 

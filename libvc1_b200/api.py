@@ -39,7 +39,15 @@ EXPORTS = (
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
     "vc1cu_estimate_intensity_enqueue", "vc1cu_estimate_intensity_collect",
     "vc1cu_fast_transform_types", "vc1cu_debug_set_wait_limit", "vc1cu_debug_withhold_publish",
+    "vc1cu_synth_frames", "vc1cu_lp_param_count", "vc1cu_lp_create", "vc1cu_lp_destroy", "vc1cu_lp_get_params",
+    "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
+    "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze",
 )
+
+
+class LpPass(C.Structure):
+    _fields_ = [("cur_id", C.c_int32), ("ref_id", C.c_int32), ("sample", C.c_int32), ("mode", C.c_int32),
+                ("out_slot", C.c_int32), ("pqindex", C.c_int32)]
 
 
 class Pass(C.Structure):
@@ -80,6 +88,19 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_forward_quant.argtypes = [vp, PP, i32, i32, i32, vp, vp]
     L.vc1cu_forward_quant_device.argtypes = [vp, PP, i32, i32, i32, vp, vp]
     L.vc1cu_set_timing.argtypes = [vp, i32]
+    L.vc1cu_synth_frames.argtypes = [vp, vp, i32, i32, i32]
+    L.vc1cu_lp_param_count.argtypes = []
+    L.vc1cu_lp_create.argtypes = [vp, i32, i32, i32, i32, i32, C.c_uint64, C.POINTER(vp)]
+    L.vc1cu_lp_destroy.argtypes = [vp]
+    L.vc1cu_lp_get_params.argtypes = [vp, vp]
+    L.vc1cu_lp_set_params.argtypes = [vp, vp]
+    L.vc1cu_lp_prepare.argtypes = [vp, i32, i32, i32]
+    L.vc1cu_lp_set_labels.argtypes = [vp, i32, i32]
+    L.vc1cu_lp_train_step.argtypes = [vp, vp, i32, C.c_float, C.POINTER(C.c_float)]
+    L.vc1cu_lp_gradients.argtypes = [vp, vp, i32, vp, C.POINTER(C.c_float)]
+    L.vc1cu_lp_propose.argtypes = [vp, i32, i32]
+    L.vc1cu_lp_read_sample.argtypes = [vp, i32, vp, vp, vp, vp]
+    L.vc1cu_lp_analyze.argtypes = [vp, PP, C.POINTER(LpPass), i32, i32]
     L.vc1cu_debug_set_wait_limit.argtypes = [vp, i32]
     L.vc1cu_debug_withhold_publish.argtypes = [vp, i32, i32]
     L.vc1cu_timing_get.argtypes = [vp, C.POINTER(Timing)]
@@ -193,6 +214,11 @@ class CudaComputeContext:
 
     def reset_counters(self):
         self._check(self._L.vc1cu_reset_counters(self._h))
+
+    def synth_frames(self, cfg, first: int, count: int, frame_id0: int):
+        """Frames first..first+count-1 of the synthetic clip `cfg` (libvc1_b200.synth.make_cfg)
+        generated on the device into frame slots frame_id0.. (asynchronous)."""
+        self._check(self._L.vc1cu_synth_frames(self._h, C.byref(cfg), first, count, frame_id0))
 
     def debug_set_wait_limit(self, log2_polls: int):
         """Wavefront waits give up after 2**log2_polls polls (6..24) in later core launches."""
@@ -438,5 +464,85 @@ def global_motion_noalloc(cur_ptrs, ref_ptrs, pitch: int, width: int, height: in
         raise Vc1cuError(rc, err.value.decode())
 
 
+class LearnedProposals:
+    """The learned motion-vector proposals of one context (vc1cu_lp_*, include/vc1cu.h): a
+    network for one raster and search range holding `capacity` samples (a picture pair's
+    features, translation hint, labels, candidates and fallback flags)."""
+
+    def __init__(self, ctx: "CudaComputeContext", width: int, height: int, search_range: int, capacity: int,
+                 max_batch: int = 8, seed: int = 1):
+        self._L = ctx._L
+        self.ctx = ctx
+        self.width, self.height, self.range = width, height, search_range
+        self.mbw, self.mbh = (width + 15) // 16, (height + 15) // 16
+        self.w4, self.h4 = 4 * self.mbw, 4 * self.mbh
+        self.capacity, self.max_batch = capacity, max_batch
+        h = C.c_void_p()
+        ctx._check(self._L.vc1cu_lp_create(ctx._h, width, height, search_range, capacity, max_batch, seed, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            self._L.vc1cu_lp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def param_count() -> int:
+        return int(load_library().vc1cu_lp_param_count())
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.param_count(), np.float32)
+        self.ctx._check(self._L.vc1cu_lp_get_params(self._h, out.ctypes.data))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self.ctx._check(self._L.vc1cu_lp_set_params(self._h, p.ctypes.data))
+
+    def prepare(self, cur_id: int, ref_id: int, sample: int):
+        self.ctx._check(self._L.vc1cu_lp_prepare(self._h, cur_id, ref_id, sample))
+
+    def set_labels(self, sample: int, result_slot: int):
+        self.ctx._check(self._L.vc1cu_lp_set_labels(self._h, sample, result_slot))
+
+    def train_step(self, samples, lr: float) -> float:
+        s = np.ascontiguousarray(samples, np.int32)
+        loss = C.c_float()
+        self.ctx._check(self._L.vc1cu_lp_train_step(self._h, s.ctypes.data, len(s), lr, C.byref(loss)))
+        return float(loss.value)
+
+    def gradients(self, samples):
+        s = np.ascontiguousarray(samples, np.int32)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = C.c_float()
+        self.ctx._check(self._L.vc1cu_lp_gradients(self._h, s.ctypes.data, len(s), g.ctypes.data, C.byref(loss)))
+        return float(loss.value), g
+
+    def propose(self, first_sample: int, n: int = 1):
+        self.ctx._check(self._L.vc1cu_lp_propose(self._h, first_sample, n))
+
+    def read_sample(self, sample: int):
+        """(features (H4, W4, 16) bf16 bit patterns, hint (2,), candidates (mbs, 4, 2), fallback (mbs,))."""
+        mbs = self.mbw * self.mbh
+        f = np.zeros((self.h4, self.w4, 16), np.uint16)
+        h = np.zeros(2, np.int32)
+        c = np.zeros((mbs, 4, 2), np.int32)
+        fb = np.zeros(mbs, np.uint8)
+        self.ctx._check(self._L.vc1cu_lp_read_sample(self._h, sample, f.ctypes.data, h.ctypes.data, c.ctypes.data,
+                                                     fb.ctypes.data))
+        return f, h, c, fb
+
+    def analyze(self, params: Params, passes, fallback: bool = True):
+        """passes: (cur_id, ref_id, sample, mode, out_slot[, pqindex]) tuples."""
+        arr = (LpPass * len(passes))(*[LpPass(*(tuple(q) + (0,) * (6 - len(q)))) for q in passes])
+        self.ctx._check(self._L.vc1cu_lp_analyze(self._h, C.byref(params), arr, len(passes), int(fallback)))
+
+
 __all__ = ["CudaComputeContext", "Vc1cuError", "Pass", "load_library", "EXPORTS", "METRIC_SAD", "METRIC_SATD",
-           "global_motion_noalloc"]
+           "global_motion_noalloc", "LearnedProposals"]

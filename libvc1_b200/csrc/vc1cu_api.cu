@@ -23,6 +23,8 @@
 #include <vector>
 
 #include "vc1cu_core.cuh"
+#include "vc1cu_lp.cuh"
+#include "vc1cu_synth.cuh"
 
 namespace vc1cu {
 // kernels and drivers of the other translation units
@@ -245,6 +247,8 @@ struct vc1cu_ctx {
     size_t lr_cap = 0;
     void* d_scratch = nullptr;
     size_t scratch_cap = 0;
+    void* d_synth = nullptr;   // vc1cu_synth_frames: launch arguments, normalisation terms and sums
+    size_t synth_cap = 0;
     // Pinned staging of launch descriptors: a ring, so that the host can enqueue up to
     // kStagingRing launches ahead of the device (each copy out of a buffer is ordered behind
     // the launches before it on the stream, and its buffer is reused once that copy is done).
@@ -645,7 +649,18 @@ int score_common(vc1cu_ctx* c, const DevParams& P, const ScoreArgs& a, const vc1
 
 // Launches a batch of independent core passes (global search first for unseeded ones).
 // globals_ready: the unseeded passes' global translation results are already in their slots.
-int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false) {
+// Per-pass additions of the learned form (all null for the plain passes): the candidates of a
+// learned pass and where it flags its fallback macroblocks, or the flags a fallback pass
+// computes (only those macroblocks), and the translation hint that replaces the global search.
+struct PassExtra {
+    const int2* cands = nullptr;
+    uint8_t* fallback = nullptr;
+    const uint8_t* only = nullptr;
+    const int2* hint = nullptr;
+};
+
+int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false,
+                 const PassExtra* extra = nullptr) {
     DevParams P;
     std::string why;
     int rc = make_dev_params(p, P, why);
@@ -693,12 +708,34 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
             unseeded.push_back(i);
         }
     }
+    bool learned = false;
     for (int i = 0; i < n; ++i) {
         ResultSlot& o = result_slot(c, passes[i].out_slot, mbs, true);
         o.mode = passes[i].mode;
         o.seeded = passes[i].seed_slot >= 0;
         o.allow_intra = passes[i].allow_intra != 0;
         h[i].out = o.r;
+        h[i].cands = extra ? extra[i].cands : nullptr;
+        h[i].fallback = extra ? extra[i].fallback : nullptr;
+        h[i].only = extra ? extra[i].only : nullptr;
+        learned |= h[i].cands != nullptr;
+    }
+    if (learned) {
+        for (int i = 0; i < n; ++i)
+            if (!h[i].cands || h[i].seeded || h[i].mode == VC1CU_MV_MIXED || h[i].allow_intra)
+                throw Fail{VC1CU_ERR_ARG, "a learned launch takes unseeded 1-MV passes without P-intra only"};
+    }
+    // the translation hint stands in for the global search of passes that carry one
+    if (extra) {
+        bool any_hint = false;
+        for (int i = 0; i < n; ++i)
+            if (extra[i].hint) {
+                any_hint = true;
+                ck(cudaMemcpyAsync(h[i].out.global, extra[i].hint, sizeof(int2), cudaMemcpyDeviceToDevice, c->stream),
+                   "cudaMemcpyAsync(hint)");
+                ck(cudaMemsetAsync(h[i].out.gsad, 0, 8, c->stream), "cudaMemsetAsync(hint sad)");
+            }
+        if (any_hint) globals_ready = true;
     }
     // seed levels of in-launch seeds (a chain, never a cycle)
     std::vector<int> level(n, 0);
@@ -751,7 +788,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         tm.stop(launches);
     }
     // long-range signature index of each long-range pass's reference (build_long_range_index)
-    if (!unseeded.empty() && P.range > P.local_range) {
+    if (!unseeded.empty() && P.range > P.local_range && !learned) {
         const int nx = (P.W + 7) / 8, ny = (P.H + 7) / 8;
         const size_t per = sizeof(uint64_t) * (size_t)nx * ny;
         uint64_t* base = static_cast<uint64_t*>(ensure(c->d_lr, c->lr_cap, per * unseeded.size(), "cudaMalloc(long-range index)"));
@@ -784,7 +821,12 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     }
     // window / bitset geometry
     WinCfg wc;
-    if (any_unseeded) {
+    if (learned) {
+        wc.rw = kLearnRw;
+        wc.seen_r = 0;
+        wc.seen_words = 1;
+        wc.keys_cap = 32;
+    } else if (any_unseeded) {
         wc.rw = P.local_range + 1;
         wc.seen_r = P.local_range;
         wc.seen_words = ((2 * P.local_range + 1) * (2 * P.local_range + 1) + 31) / 32;
@@ -822,6 +864,9 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     bool any_intra_pass = false;
     for (int i = 0; i < n; ++i) any_intra_pass |= passes[i].allow_intra != 0;
     if (!any_intra_pass && (kind & kCoreDefaultRefine)) kind |= kCoreNoIntra;
+    if (learned)
+        kind = kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra |
+               ((P.me_quality == 2 && !P.fast_subpel) ? kCoreDefaultRefine : 0);
     // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
     if (!(kind & kCoreSeededOnly) && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm) kind |= kCoreWide;
     const void* kern = core_kernel(kind);
@@ -1541,6 +1586,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_gstates) cudaFree(c->d_gstates);
     if (c->d_lr) cudaFree(c->d_lr);
     if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->d_synth) cudaFree(c->d_synth);
     for (auto& kv : c->items) cudaFree(kv.second.first);
     if (c->h_read) cudaFreeHost(c->h_read);
     for (auto& b : c->staging_ring) {
@@ -1698,6 +1744,57 @@ int vc1cu_upload_frame(vc1cu_ctx* c, int id, const uint8_t* y, const uint8_t* u,
         ck(cudaStreamWaitEvent(c->stream, f.uploaded, 0), "cudaStreamWaitEvent(upload)");
         c->counters.frame_uploads++;
         c->counters.frame_upload_bytes += (size_t)w * h + 2 * (size_t)cw * ch;
+        return VC1CU_OK;
+    });
+}
+
+static_assert(sizeof(vc1cu_synth_cfg) == sizeof(vc1synth_cfg) &&
+                  offsetof(vc1cu_synth_cfg, noise_sigma) == offsetof(vc1synth_cfg, noise_sigma) &&
+                  offsetof(vc1cu_synth_cfg, seed) == offsetof(vc1synth_cfg, seed),
+              "vc1cu_synth_cfg mirrors vc1synth_cfg");
+
+int vc1cu_synth_frames(vc1cu_ctx* c, const vc1cu_synth_cfg* cfg, int first, int count, int frame_id0) {
+    return guarded(c, [&]() -> int {
+        if (!cfg) throw Fail{VC1CU_ERR_ARG, "null configuration"};
+        vc1synth_cfg s;
+        std::memcpy(&s, cfg, sizeof s);
+        if (s.width <= 0 || s.height <= 0 || (s.width & 1) || (s.height & 1) || s.width > 16384 || s.height > 16384)
+            throw Fail{VC1CU_ERR_ARG, "width/height must be positive, even and <= 16384"};
+        if (s.n_objects < 0 || s.n_objects > 64) throw Fail{VC1CU_ERR_ARG, "n_objects must be 0..64"};
+        if (count < 1 || count > kSynthMaxFrames || first < 0 || first + count > s.frames)
+            throw Fail{VC1CU_ERR_ARG, "count must be 1..64 and first + count <= frames"};
+        if (frame_id0 < 0 || frame_id0 + count > kMaxSlot) throw Fail{VC1CU_ERR_ARG, "frame id out of range"};
+        const size_t nterms = (size_t)((s.width + 1) / 2) * ((s.height + 1) / 2);
+        const size_t args_bytes = (sizeof(SynthArgs) + 255) & ~size_t(255);
+        uint8_t* d = static_cast<uint8_t*>(
+            ensure(c->d_synth, c->synth_cap, args_bytes + 256 + nterms * sizeof(double), "cudaMalloc(synth)"));
+        SynthArgs* da = reinterpret_cast<SynthArgs*>(d);
+        double* d_ms = reinterpret_cast<double*>(d + args_bytes);
+        double* d_terms = reinterpret_cast<double*>(d + args_bytes + 256);
+        SynthArgs* ha = static_cast<SynthArgs*>(staging(c, sizeof(SynthArgs)));
+        std::memset(ha, 0, sizeof(SynthArgs));
+        vs_make_plan(&s, &ha->plan);
+        std::vector<double> gx(first + count), gy(first + count);
+        vs_global_track(&s, first + count, gx.data(), gy.data());
+        ha->first = first;
+        ha->count = count;
+        ha->mean_scale = d_ms;
+        for (int i = 0; i < count; ++i) {
+            const int t = first + i;
+            double zinv = 1.0;
+            for (int k = 0; k < t; ++k) zinv = zinv / s.zoom;
+            ha->zinv[i] = zinv;
+            ha->gx[i] = gx[t];
+            ha->gy[i] = gy[t];
+            FrameSlot& f = alloc_frame(c, frame_id0 + i, s.width, s.height);
+            const DevFrame v = f.view();
+            ha->out[i] = SynthOut{const_cast<uint8_t*>(v.y), const_cast<uint8_t*>(v.u), const_cast<uint8_t*>(v.v),
+                                  f.pitch_y, f.pitch_c};
+        }
+        ck(cudaMemcpyAsync(da, ha, sizeof(SynthArgs), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(synth)");
+        staging_mark(c);
+        ck(launch_synth(s, da, d_terms, d_ms, count, c->sm_count, c->stream), "synth launch");
+        c->counters.kernel_launches += 3;
         return VC1CU_OK;
     });
 }
@@ -2265,6 +2362,467 @@ int vc1cu_forward_quant(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pre
         if (coeffs) ck(cudaMemcpyAsync(coeffs, dco, cb, cudaMemcpyDeviceToHost, c->stream), "download coefficients");
         if (levels) ck(cudaMemcpyAsync(levels, dlv, lb, cudaMemcpyDeviceToHost, c->stream), "download levels");
         sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+
+}  // extern "C"
+
+// ---- learned motion-vector proposals ---------------------------------------------------------
+
+struct vc1cu_lp {
+    vc1cu_ctx* c = nullptr;
+    LpGeom g{};
+    int capacity = 0, max_batch = 0;
+    size_t xelems = 0, aelems = 0;  // bf16 elements of one sample's input / one layer's output
+    float* w = nullptr;             // fp32 master parameters
+    float* gr = nullptr;            // their gradients
+    float* m1 = nullptr;            // Adam moments
+    float* m2 = nullptr;
+    void* fwd_b = nullptr;          // packed bf16 B operands
+    void* dgr_b = nullptr;
+    int step = 0;
+    void* x0 = nullptr;             // dataset: per sample the input features
+    int2* hints = nullptr;          // per sample the translation hint
+    int2* labels = nullptr;         // per sample and MB the plain search's integer vector
+    int2* cands = nullptr;          // per sample and MB the K candidates
+    uint8_t* fallback = nullptr;    // per sample and MB the learned pass's fallback flags
+    void* act[kLpLayers] = {};      // a batch's layer outputs
+    void* dz[2] = {};               // gradient ping-pong
+    void* xb = nullptr;             // a training batch's gathered inputs
+    int2* bhint = nullptr;          // its hints
+    int2* blabel = nullptr;         // its labels
+    uint8_t* cur4 = nullptr;
+    uint8_t* ref4 = nullptr;
+    unsigned long long* hs = nullptr;  // hint search costs
+    float* loss = nullptr;
+    int* err = nullptr;
+    std::vector<void*> owned;
+};
+
+namespace {
+
+size_t lp_off_w(int l) {
+    size_t o = 0;
+    for (int k = 0; k < l; ++k) o += (size_t)lp_wcount(k) + kLpC;
+    return o;
+}
+size_t lp_off_b(int l) { return lp_off_w(l) + (size_t)lp_wcount(l); }
+size_t lp_off_head() { return lp_off_w(kLpLayers); }
+
+template <class T>
+T* lp_alloc(vc1cu_lp* n, size_t bytes, const char* what) {
+    void* d = nullptr;
+    ck(cudaMalloc(&d, bytes ? bytes : 16), what);
+    n->owned.push_back(d);
+    return static_cast<T*>(d);
+}
+
+void lp_check_sample(const vc1cu_lp* n, int s) {
+    if (s < 0 || s >= n->capacity) throw Fail{VC1CU_ERR_ARG, "sample index out of range"};
+}
+
+void lp_pack(vc1cu_lp* n) { ck(lp_launch_pack(n->w, n->fwd_b, n->dgr_b, n->c->stream), "lp pack"); }
+
+size_t lp_fwd_off(int l) {
+    size_t o = 0;
+    for (int k = 0; k < l; ++k) o += lp_fwd_b_elems(k);
+    return o;
+}
+size_t lp_dgr_off(int l) {
+    size_t o = 0;
+    for (int k = 0; k < l; ++k) o += lp_dgrad_b_elems(k);
+    return o;
+}
+
+// The four convolutions of `frames` pictures starting at x (bf16 elements).
+void lp_forward(vc1cu_lp* n, const void* x, int frames) {
+    const auto* bf = static_cast<const uint16_t*>(n->fwd_b);
+    for (int l = 0; l < kLpLayers; ++l) {
+        LpConvArgs a{};
+        a.x = l == 0 ? x : n->act[l - 1];
+        a.wb = bf + lp_fwd_off(l);
+        a.bias = n->w + lp_off_b(l);
+        a.y = n->act[l];
+        a.W4 = n->g.W4;
+        a.H4 = n->g.H4;
+        a.frames = frames;
+        a.err = n->err;
+        ck(lp_launch_conv(lp_cin(l), false, a, n->c->sm_count, n->c->stream), "lp conv forward");
+    }
+    n->c->counters.kernel_launches += kLpLayers;
+}
+
+// Forward, loss and every gradient of a gathered batch (xb, bhint, blabel) into gr; returns the
+// loss (synchronous).
+float lp_backward(vc1cu_lp* n, int frames) {
+    vc1cu_ctx* c = n->c;
+    const int mbs = n->g.mbw * n->g.mbh;
+    ck(cudaMemsetAsync(n->gr, 0, sizeof(float) * lp_param_count(), c->stream), "lp zero grads");
+    ck(cudaMemsetAsync(n->loss, 0, sizeof(float), c->stream), "lp zero loss");
+    lp_forward(n, n->xb, frames);
+    LpHeadArgs h{};
+    h.y4 = n->act[kLpLayers - 1];
+    h.wh = n->w + lp_off_head();
+    h.bh = h.wh + kLpHead * kLpC;
+    h.hint = n->bhint;
+    h.labels = n->blabel;
+    h.cands = nullptr;
+    h.loss = n->loss;
+    h.dwh = n->gr + lp_off_head();
+    h.dbh = h.dwh + kLpHead * kLpC;
+    h.dz4 = n->dz[0];
+    h.db4 = n->gr + lp_off_b(kLpLayers - 1);
+    h.W4 = n->g.W4;
+    h.H4 = n->g.H4;
+    h.mbw = n->g.mbw;
+    h.mbh = n->g.mbh;
+    h.frames = frames;
+    h.range = n->g.range;
+    h.inv_count = 1.0f / (float)(mbs * frames);
+    ck(lp_launch_head(h, c->stream), "lp head");
+    const auto* db = static_cast<const uint16_t*>(n->dgr_b);
+    int cur = 0;  // dz[cur] holds the gradient at layer l's pre-activation
+    for (int l = kLpLayers - 1; l >= 0; --l) {
+        LpWgradArgs wa{};
+        wa.x = l == 0 ? n->xb : n->act[l - 1];
+        wa.dz = n->dz[cur];
+        wa.dw = n->gr + lp_off_w(l);
+        wa.W4 = n->g.W4;
+        wa.H4 = n->g.H4;
+        wa.frames = frames;
+        wa.err = n->err;
+        ck(lp_launch_wgrad(lp_cin(l), wa, c->sm_count, c->stream), "lp wgrad");
+        if (l > 0) {
+            LpConvArgs a{};
+            a.x = n->dz[cur];
+            a.wb = db + lp_dgr_off(l);
+            a.y = n->dz[1 - cur];
+            a.act = n->act[l - 1];
+            a.dbias = n->gr + lp_off_b(l - 1);
+            a.W4 = n->g.W4;
+            a.H4 = n->g.H4;
+            a.frames = frames;
+            a.err = n->err;
+            ck(lp_launch_conv(kLpC, true, a, c->sm_count, c->stream), "lp conv dgrad");
+            cur = 1 - cur;
+        }
+    }
+    c->counters.kernel_launches += 1 + 2 * kLpLayers - 1;
+    float loss = 0.0f;
+    int err = 0;
+    ck(cudaMemcpyAsync(&loss, n->loss, sizeof loss, cudaMemcpyDeviceToHost, c->stream), "lp loss");
+    ck(cudaMemcpyAsync(&err, n->err, sizeof err, cudaMemcpyDeviceToHost, c->stream), "lp err");
+    sync_checked(c);
+    if (err) {
+        ck(cudaMemsetAsync(n->err, 0, sizeof(int), c->stream), "lp err reset");
+        throw Fail{VC1CU_ERR_TIMEOUT, "a tensor-core wait of the proposal network timed out"};
+    }
+    return loss;
+}
+
+void lp_gather(vc1cu_lp* n, const int* samples, int count) {
+    vc1cu_ctx* c = n->c;
+    if (count < 1 || count > n->max_batch) throw Fail{VC1CU_ERR_ARG, "batch must be 1..max_batch samples"};
+    const int mbs = n->g.mbw * n->g.mbh;
+    for (int i = 0; i < count; ++i) {
+        lp_check_sample(n, samples[i]);
+        const size_t s = (size_t)samples[i];
+        ck(cudaMemcpyAsync(static_cast<uint16_t*>(n->xb) + n->xelems * i, static_cast<const uint16_t*>(n->x0) + n->xelems * s,
+                           n->xelems * 2, cudaMemcpyDeviceToDevice, c->stream), "lp gather");
+        ck(cudaMemcpyAsync(n->bhint + i, n->hints + s, sizeof(int2), cudaMemcpyDeviceToDevice, c->stream), "lp gather");
+        ck(cudaMemcpyAsync(n->blabel + (size_t)mbs * i, n->labels + (size_t)mbs * s, sizeof(int2) * mbs,
+                           cudaMemcpyDeviceToDevice, c->stream), "lp gather");
+    }
+}
+
+// He-uniform initial weights from a counter-based hash (no libm), biases zero.
+void lp_init(vc1cu_lp* n, uint64_t seed) {
+    std::vector<float> h(lp_param_count(), 0.0f);
+    auto unit = [&](uint64_t i) {
+        uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    uint64_t k = 0;
+    for (int l = 0; l < kLpLayers; ++l) {
+        const double a = std::sqrt(6.0 / (9.0 * lp_cin(l)));
+        for (int i = 0; i < lp_wcount(l); ++i) h[lp_off_w(l) + i] = (float)(a * unit(k++));
+    }
+    const double ah = 0.1 * std::sqrt(6.0 / kLpC);
+    for (int i = 0; i < kLpHead * kLpC; ++i) h[lp_off_head() + i] = (float)(ah * unit(k++));
+    ck(cudaMemcpyAsync(n->w, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, n->c->stream), "lp init");
+    ck(cudaMemsetAsync(n->m1, 0, sizeof(float) * h.size(), n->c->stream), "lp init");
+    ck(cudaMemsetAsync(n->m2, 0, sizeof(float) * h.size(), n->c->stream), "lp init");
+    n->step = 0;
+    lp_pack(n);
+    sync_checked(n->c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int vc1cu_lp_param_count(void) { return lp_param_count(); }
+
+int vc1cu_lp_create(vc1cu_ctx* c, int width, int height, int search_range, int capacity, int max_batch, uint64_t seed,
+                    vc1cu_lp** out) {
+    return guarded(c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        *out = nullptr;
+        if (width <= 0 || height <= 0 || (width & 1) || (height & 1) || width > 16384 || height > 16384)
+            throw Fail{VC1CU_ERR_ARG, "width/height must be positive, even and <= 16384"};
+        if (search_range < 0 || search_range > 1024) throw Fail{VC1CU_ERR_ARG, "search_range must be 0..1024"};
+        if (capacity < 1 || capacity > (1 << 20) || max_batch < 1 || max_batch > 64)
+            throw Fail{VC1CU_ERR_ARG, "capacity must be >= 1 and max_batch 1..64"};
+        std::unique_ptr<vc1cu_lp> n(new vc1cu_lp);
+        n->c = c;
+        n->g.W = width;
+        n->g.H = height;
+        n->g.mbw = (width + 15) / 16;
+        n->g.mbh = (height + 15) / 16;
+        n->g.W4 = 4 * n->g.mbw;
+        n->g.H4 = 4 * n->g.mbh;
+        n->g.range = search_range;
+        n->capacity = capacity;
+        n->max_batch = max_batch;
+        const size_t px = (size_t)n->g.W4 * n->g.H4, mbs = (size_t)n->g.mbw * n->g.mbh;
+        n->xelems = px * kLpCin0;
+        n->aelems = px * kLpC;
+        try {
+            const size_t np = (size_t)lp_param_count();
+            n->w = lp_alloc<float>(n.get(), 4 * np, "cudaMalloc(lp params)");
+            n->gr = lp_alloc<float>(n.get(), 4 * np, "cudaMalloc(lp grads)");
+            n->m1 = lp_alloc<float>(n.get(), 4 * np, "cudaMalloc(lp adam)");
+            n->m2 = lp_alloc<float>(n.get(), 4 * np, "cudaMalloc(lp adam)");
+            size_t fb = 0, db = 0;
+            for (int l = 0; l < kLpLayers; ++l) {
+                fb += lp_fwd_b_elems(l);
+                db += lp_dgrad_b_elems(l);
+            }
+            n->fwd_b = lp_alloc<void>(n.get(), 2 * fb, "cudaMalloc(lp packed weights)");
+            n->dgr_b = lp_alloc<void>(n.get(), 2 * db, "cudaMalloc(lp packed weights)");
+            n->x0 = lp_alloc<void>(n.get(), 2 * n->xelems * capacity, "cudaMalloc(lp dataset)");
+            n->hints = lp_alloc<int2>(n.get(), sizeof(int2) * capacity, "cudaMalloc(lp hints)");
+            n->labels = lp_alloc<int2>(n.get(), sizeof(int2) * mbs * capacity, "cudaMalloc(lp labels)");
+            n->cands = lp_alloc<int2>(n.get(), sizeof(int2) * kLpK * mbs * capacity, "cudaMalloc(lp candidates)");
+            n->fallback = lp_alloc<uint8_t>(n.get(), mbs * capacity, "cudaMalloc(lp fallback flags)");
+            for (int l = 0; l < kLpLayers; ++l)
+                n->act[l] = lp_alloc<void>(n.get(), 2 * n->aelems * max_batch, "cudaMalloc(lp activations)");
+            for (int k = 0; k < 2; ++k) n->dz[k] = lp_alloc<void>(n.get(), 2 * n->aelems * max_batch, "cudaMalloc(lp grads)");
+            n->xb = lp_alloc<void>(n.get(), 2 * n->xelems * max_batch, "cudaMalloc(lp batch)");
+            n->bhint = lp_alloc<int2>(n.get(), sizeof(int2) * max_batch, "cudaMalloc(lp batch)");
+            n->blabel = lp_alloc<int2>(n.get(), sizeof(int2) * mbs * max_batch, "cudaMalloc(lp batch)");
+            n->cur4 = lp_alloc<uint8_t>(n.get(), px, "cudaMalloc(lp quarter-res)");
+            n->ref4 = lp_alloc<uint8_t>(n.get(), px, "cudaMalloc(lp quarter-res)");
+            n->hs = lp_alloc<unsigned long long>(n.get(), 8 * (65 * 65 + 32), "cudaMalloc(lp hint search)");
+            n->loss = lp_alloc<float>(n.get(), 16, "cudaMalloc(lp loss)");
+            n->err = lp_alloc<int>(n.get(), 16, "cudaMalloc(lp err)");
+            ck(cudaMemsetAsync(n->err, 0, 16, c->stream), "lp err");
+            ck(cudaMemsetAsync(n->labels, 0, sizeof(int2) * mbs * capacity, c->stream), "lp labels");
+            lp_init(n.get(), seed);
+        } catch (...) {
+            for (void* d : n->owned) cudaFree(d);
+            throw;
+        }
+        *out = n.release();
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_destroy(vc1cu_lp* n) {
+    if (!n) return VC1CU_OK;
+    cudaSetDevice(n->c->device);
+    cudaStreamSynchronize(n->c->stream);
+    for (void* d : n->owned) cudaFree(d);
+    delete n;
+    return VC1CU_OK;
+}
+
+int vc1cu_lp_get_params(vc1cu_lp* n, float* out) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    return guarded(n->c, [&]() -> int {
+        if (!out) throw Fail{VC1CU_ERR_ARG, "null output"};
+        ck(cudaMemcpyAsync(out, n->w, sizeof(float) * lp_param_count(), cudaMemcpyDeviceToHost, n->c->stream), "lp params");
+        sync_checked(n->c);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_set_params(vc1cu_lp* n, const float* in) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    return guarded(n->c, [&]() -> int {
+        if (!in) throw Fail{VC1CU_ERR_ARG, "null input"};
+        const size_t b = sizeof(float) * lp_param_count();
+        ck(cudaMemcpyAsync(n->w, in, b, cudaMemcpyHostToDevice, n->c->stream), "lp params");
+        ck(cudaMemsetAsync(n->m1, 0, b, n->c->stream), "lp adam");
+        ck(cudaMemsetAsync(n->m2, 0, b, n->c->stream), "lp adam");
+        n->step = 0;
+        lp_pack(n);
+        sync_checked(n->c);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_prepare(vc1cu_lp* n, int cur_id, int ref_id, int sample) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        lp_check_sample(n, sample);
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fr = frame_slot(c, ref_id);
+        if (fc.w != n->g.W || fc.h != n->g.H || fr.w != n->g.W || fr.h != n->g.H)
+            throw Fail{VC1CU_ERR_ARG, "frame size differs from the network's raster"};
+        c->used_frames.push_back(cur_id);
+        c->used_frames.push_back(ref_id);
+        const DevFrame cf = fc.view(), rf = fr.view();
+        ck(lp_launch_downsample(cf.y, cf.pitch_y, rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, c->stream), "lp downsample");
+        ck(lp_launch_hint(cf.y, cf.pitch_y, rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hs, n->hints + sample, c->stream),
+           "lp hint search");
+        ck(lp_launch_features(rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hints + sample,
+                              static_cast<uint16_t*>(n->x0) + n->xelems * sample, c->stream),
+           "lp features");
+        c->counters.kernel_launches += 5;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_set_labels(vc1cu_lp* n, int sample, int result_slot_id) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        lp_check_sample(n, sample);
+        const int mbs = n->g.mbw * n->g.mbh;
+        ResultSlot& s = result_slot(c, result_slot_id, mbs, false);
+        ck(lp_launch_labels(s.r.mvs, mbs, n->labels + (size_t)mbs * sample, c->stream), "lp labels");
+        c->counters.kernel_launches++;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_train_step(vc1cu_lp* n, const int* samples, int count, float lr, float* loss) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        if (!samples) throw Fail{VC1CU_ERR_ARG, "null sample list"};
+        lp_gather(n, samples, count);
+        const float l = lp_backward(n, count);
+        ++n->step;
+        ck(lp_launch_adam(n->w, n->gr, n->m1, n->m2, lp_param_count(), lr, 0.9f, 0.999f, 1e-8f, n->step, c->stream),
+           "lp adam");
+        lp_pack(n);
+        c->counters.kernel_launches += 1 + kLpLayers;
+        if (loss) *loss = l;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_gradients(vc1cu_lp* n, const int* samples, int count, float* grads, float* loss) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        if (!samples) throw Fail{VC1CU_ERR_ARG, "null sample list"};
+        lp_gather(n, samples, count);
+        const float l = lp_backward(n, count);
+        if (grads) {
+            ck(cudaMemcpyAsync(grads, n->gr, sizeof(float) * lp_param_count(), cudaMemcpyDeviceToHost, c->stream),
+               "lp grads");
+            sync_checked(c);
+        }
+        if (loss) *loss = l;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_propose(vc1cu_lp* n, int first_sample, int count) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        if (count < 1 || count > n->max_batch) throw Fail{VC1CU_ERR_ARG, "count must be 1..max_batch"};
+        lp_check_sample(n, first_sample);
+        lp_check_sample(n, first_sample + count - 1);
+        const int mbs = n->g.mbw * n->g.mbh;
+        lp_forward(n, static_cast<const uint16_t*>(n->x0) + n->xelems * first_sample, count);
+        LpHeadArgs h{};
+        h.y4 = n->act[kLpLayers - 1];
+        h.wh = n->w + lp_off_head();
+        h.bh = h.wh + kLpHead * kLpC;
+        h.hint = n->hints + first_sample;
+        h.cands = n->cands + (size_t)kLpK * mbs * first_sample;
+        h.W4 = n->g.W4;
+        h.H4 = n->g.H4;
+        h.mbw = n->g.mbw;
+        h.mbh = n->g.mbh;
+        h.frames = count;
+        h.range = n->g.range;
+        ck(lp_launch_head(h, c->stream), "lp head");
+        c->counters.kernel_launches++;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_read_sample(vc1cu_lp* n, int sample, uint16_t* features, vc1cu_mv* hint, vc1cu_mv* candidates,
+                         uint8_t* fallback) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        lp_check_sample(n, sample);
+        const size_t mbs = (size_t)n->g.mbw * n->g.mbh;
+        if (features)
+            ck(cudaMemcpyAsync(features, static_cast<const uint16_t*>(n->x0) + n->xelems * sample, 2 * n->xelems,
+                               cudaMemcpyDeviceToHost, c->stream), "lp read");
+        if (hint) ck(cudaMemcpyAsync(hint, n->hints + sample, 8, cudaMemcpyDeviceToHost, c->stream), "lp read");
+        if (candidates)
+            ck(cudaMemcpyAsync(candidates, n->cands + kLpK * mbs * sample, 8 * kLpK * mbs, cudaMemcpyDeviceToHost,
+                               c->stream), "lp read");
+        if (fallback)
+            ck(cudaMemcpyAsync(fallback, n->fallback + mbs * sample, mbs, cudaMemcpyDeviceToHost, c->stream), "lp read");
+        sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_lp_analyze(vc1cu_lp* n, const vc1cu_params* p, const vc1cu_lp_pass* passes, int count, int fallback) {
+    if (!n) return fail(nullptr, VC1CU_ERR_ARG, "null network");
+    vc1cu_ctx* c = n->c;
+    return guarded(c, [&]() -> int {
+        if (count < 1 || !passes) throw Fail{VC1CU_ERR_ARG, "invalid pass list"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        if (P.W != n->g.W || P.H != n->g.H || P.range != n->g.range)
+            throw Fail{VC1CU_ERR_ARG, "params differ from the network's raster or search range"};
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        std::vector<vc1cu_pass> q(count);
+        std::vector<PassExtra> ex(count);
+        for (int i = 0; i < count; ++i) {
+            const vc1cu_lp_pass& a = passes[i];
+            lp_check_sample(n, a.sample);
+            if (a.mode == VC1CU_MV_MIXED) throw Fail{VC1CU_ERR_ARG, "learned passes are 1-MV"};
+            if (a.out_slot < 0 || a.out_slot >= kMaxSlot) throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+            q[i] = vc1cu_pass{a.cur_id, a.ref_id, a.mode, 0, -1, a.out_slot, a.pqindex};
+            ex[i].cands = n->cands + kLpK * mbs * a.sample;
+            ex[i].fallback = n->fallback + mbs * a.sample;
+            ex[i].hint = n->hints + a.sample;
+        }
+        for (int i = 0; i < count; ++i)
+            for (int j = 0; j < i; ++j)
+                if (q[i].out_slot == q[j].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
+        launch_group(c, p, q.data(), count, true, ex.data());
+        if (fallback) {
+            // the macroblocks whose best learned match is not good: the plain search, in
+            // wavefront order, over the learned field
+            for (int i = 0; i < count; ++i) {
+                ex[i].only = ex[i].fallback;
+                ex[i].cands = nullptr;
+                ex[i].fallback = nullptr;
+            }
+            launch_group(c, p, q.data(), count, true, ex.data());
+        }
         return VC1CU_OK;
     });
 }

@@ -1085,6 +1085,86 @@ __device__ IntRes lr_extended(const DevParams& P, const Mb& m, const PassDesc& d
     return best;
 }
 
+// ---- learned passes: candidates and a short integer descent ----------------------------
+
+// (cost, |dx|+|dy|, dy, dx) lexicographic (better_integer, encoder_motion.cpp:127-133).
+__device__ __forceinline__ bool int_better(uint64_t ca, int ax, int ay, uint64_t cb, int bx, int by) {
+    if (ca != cb) return ca < cb;
+    const int ma = iabs(ax) + iabs(ay), mb = iabs(bx) + iabs(by);
+    if (ma != mb) return ma < mb;
+    if (ay != by) return ay < by;
+    return ax < bx;
+}
+
+// Exact full-resolution 16x16 SAD (mb_sad at stride 1, clamped sampling of the reference in
+// HBM) of the pass's kLearnK candidates, clamped to the search bounds; hidden-padding vectors
+// are illegal. Eight lanes per candidate, two rows each. The best by int_better, on every lane.
+__device__ IntRes learned_candidates(const DevParams& P, const Mb& m, const PassDesc& d, int range) {
+    const Bounds b = bounds_px(range);
+    const int k = m.lane >> 3, part = m.lane & 7;
+    int2 c = __ldg(&d.cands[(size_t)m.pos * kLearnK + k]);
+    c.x = iclamp(c.x, b.xmin, b.xmax);
+    c.y = iclamp(c.y, b.ymin, b.ymax);
+    uint32_t s = 0;
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        const int y = 2 * part + rr;
+        if (y < m.ah) {
+            const uint8_t* row = d.ref.y + (size_t)iclamp(m.y0 + y + c.y, 0, P.H - 1) * d.ref.pitch_y;
+            const uint8_t* cur = m.sm.cur.get() + 16 * y;
+#pragma unroll 4
+            for (int x = 0; x < 16; ++x)
+                if (x < m.aw) s += (uint32_t)iabs((int)cur[x] - (int)__ldg(row + iclamp(m.x0 + x + c.x, 0, P.W - 1)));
+        }
+    }
+#pragma unroll
+    for (int o = 4; o; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    uint64_t cost = s;
+    if (hidden_padding(P, m.x0, m.y0, 16, 16, c.x * 4, c.y * 4, VC1CU_MV_QPEL, true)) cost = kBad;
+    IntRes best{c.x, c.y, cost};
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1) {
+        const uint64_t oc = __shfl_xor_sync(FULL, best.cost, o);
+        const int ox = __shfl_xor_sync(FULL, best.dx, o), oy = __shfl_xor_sync(FULL, best.dy, o);
+        if (int_better(oc, ox, oy, best.cost, best.dx, best.dy)) best = IntRes{ox, oy, oc};
+    }
+    return best;
+}
+
+// Small-diamond descent from `best` (window staged about it): the four +-1 neighbours, move
+// while one is int_better, at most 2 * reach steps and never farther than reach from the start.
+__device__ IntRes learned_descent(const DevParams& P, const Mb& m, IntRes best, int range, int reach) {
+    const Bounds b = bounds_px(range);
+    const int cx = best.dx, cy = best.dy;
+#pragma unroll 1
+    for (int step = 0; step < 2 * reach; ++step) {
+        int dx = best.dx + (m.lane == 0 ? 1 : (m.lane == 1 ? -1 : 0));
+        int dy = best.dy + (m.lane == 2 ? 1 : (m.lane == 3 ? -1 : 0));
+        bool valid = m.lane < 4 && dx >= b.xmin && dx <= b.xmax && dy >= b.ymin && dy <= b.ymax &&
+                     iabs(dx - cx) <= reach && iabs(dy - cy) <= reach;
+        uint64_t s = valid ? mb_sad(P, m, dx, dy, 1) : UINT64_MAX;
+#pragma unroll 1
+        for (int o = 1; o < 4; o <<= 1) {
+            const bool ov = __shfl_xor_sync(FULL, valid, o);
+            const uint64_t os = __shfl_xor_sync(FULL, s, o);
+            const int ox = __shfl_xor_sync(FULL, dx, o), oy = __shfl_xor_sync(FULL, dy, o);
+            if (ov && (!valid || int_better(os, ox, oy, s, dx, dy))) {
+                valid = true;
+                s = os;
+                dx = ox;
+                dy = oy;
+            }
+        }
+        valid = __shfl_sync(FULL, valid, 0);
+        s = __shfl_sync(FULL, s, 0);
+        dx = __shfl_sync(FULL, dx, 0);
+        dy = __shfl_sync(FULL, dy, 0);
+        if (!valid || !int_better(s, dx, dy, best.cost, best.dx, best.dy)) break;
+        best = IntRes{dx, dy, s};
+    }
+    return best;
+}
+
 struct RefineOut {
     int2 mv;
     uint64_t screen_sad;
@@ -2155,7 +2235,7 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #define VC1CU_SEEDED_MIN_BLOCKS 4
 #endif
 template <int KIND>
-__global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_MIN_BLOCKS
+__global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned)) ? VC1CU_SEEDED_MIN_BLOCKS
                                                                 : ((KIND & kCoreWide) ? 1 : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
@@ -2194,6 +2274,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
         const int one_mode = allow_4mv ? VC1CU_MV_QPEL : mode;
         PHASE_START((seeded ? 1 : 0) + (allow_4mv ? 2 : 0));
         bool ok = !*(volatile int*)&st->abort;
+        if (d.only && !__ldcg(&d.only[mbi])) ok = false;  // keeps the slot's result, publishes at once
         // a seed produced by another pass of this launch
         if (ok && d.seed_pass >= 0)
             ok = wait_flags(m.lane == 0 ? &passes[d.seed_pass].out.done[mbi] : nullptr, epoch, st, code, P.wait_log2);
@@ -2237,6 +2318,7 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
         const bool spec = seeded && d.seed_pass < 0;
         const bool spec4 = allow_4mv && spec;
         int2 one_g = make_int2(0, 0);
+        IntRes learned{0, 0, UINT64_MAX};  // learned passes: the integer vector before refinement
         if (ok) {
             if (seeded) {
                 int2 seed = __ldcg(&d.seed_mvs[m.pos]);
@@ -2288,6 +2370,16 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                     }
                     PHASE_MARK(12);
                 }
+            } else if constexpr ((KIND & kCoreLearned) != 0) {
+                // the candidates' exact costs on the full-resolution picture, then a short descent
+                // in a small window about the best (neighbour-independent, before the wait)
+                const IntRes best = learned_candidates(P, m, d, range);
+                load_window(P, m, d.ref, best.dx, best.dy, wc);
+                publish_ctx(P, m);
+                window_wait();
+                learned = learned_descent(P, m, best, range, kLearnRw - 4);
+                if (m.lane == 0 && d.fallback) d.fallback[m.pos] = match_good(m, learned.cost) ? 0 : 1;
+                PHASE_MARK(2);
             } else {
                 load_window(P, m, d.ref, 0, 0, wc);
                 publish_ctx(P, m);
@@ -2318,6 +2410,11 @@ __global__ void __launch_bounds__(128, (KIND & kCoreSeededOnly) ? VC1CU_SEEDED_M
                     if (spec) shortlist_restore(m, 0);
                     one = refine_select_ool<kDR>(m.sm.ctx.off, sl, m.x0, m.y0, 16, 16, one_mode, rate_pi, true);
                 }
+            } else if constexpr ((KIND & kCoreLearned) != 0) {
+                if (pixels) dl = (double)learned.cost / (double)pixels;
+                PHASE_MARK(7);
+                one = refine_staged<kDR>(P, m, m.x0, m.y0, 16, 16, make_int2(learned.dx * 4, learned.dy * 4), range,
+                                         one_mode, rate_pi, true, learned.cost);
             } else {
                 const PInfo pi = predictor_info(P, m);
                 const int gdx = __ldcg(&o.global[0]), gdy = __ldcg(&o.global[1]);
@@ -2576,7 +2673,9 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreDefaultRefine | kCoreNoIntra)                            \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)                \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreDefaultRefine | kCoreNoIntra)             \
-    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)
+    X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)    \
+    X(kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra)                                   \
+    X(kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra | kCoreDefaultRefine)
 
 const void* core_kernel(int kind) {
     switch (kind) {

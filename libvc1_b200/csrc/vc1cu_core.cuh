@@ -54,8 +54,14 @@ struct PassDesc {
     const double* seed_dl;
     const double* seed_dc;
     const uint8_t* seed_dd;
+    const int2* cands;           // learned passes: kLearnK integer-pixel candidates per MB
+    uint8_t* fallback;           // learned passes: 1 where the candidates' best match is not good
+    const uint8_t* only;         // non-null: only the MBs flagged here are computed (the others
+                                 // keep the slot's contents and just publish their done flag)
     DevResult out;
 };
+constexpr int kLearnK = 4;       // candidates per macroblock of a learned pass
+constexpr int kLearnRw = 8;      // window radius of a learned pass around its best candidate
 
 // core_pass_kernel instantiations, as flags: each flag compiles out code that the launch's
 // passes cannot reach (the launches are bound by instruction fetch, so a smaller footprint pays).
@@ -69,6 +75,8 @@ constexpr int kCoreWide = 16;         // one block per SM, all 255 registers (se
 constexpr int kCoreDefaultRefine = 32;  // (with kCoreSeededOnly or kCoreUmhLocal) me_quality SATD and the
                                         // full sub-pel stencils: no SAD-only, RATE or fast refinement code
 constexpr int kCoreNoIntra = 64;        // (with kCoreDefaultRefine) no pass allows P-intra: no intra code
+constexpr int kCoreLearned = 128;       // (with kCoreUnseededOnly) the integer search is the learned
+                                        // candidates' exact costs and a short descent about the best
 constexpr int kCoreAny = 0;
 constexpr int kCoreSeeded = kCoreSeededOnly;
 

@@ -25,6 +25,10 @@ typedef struct vc1synth_cfg {
 
 void vc1synth_default(vc1synth_cfg* c, int width, int height, int frames, uint64_t seed);
 
+/* Mean of the background texture over frame 0 and the scale giving it standard deviation 40
+ * (the normalisation every sample uses). */
+void vc1synth_normalisation(const vc1synth_cfg* c, double* mean, double* scale);
+
 /* Writes frames*W*H luma bytes to y and frames*(W/2)*(H/2) bytes to u and v (either may
  * be NULL). Returns 0 on success. */
 int vc1synth_generate(const vc1synth_cfg* c, uint8_t* y, uint8_t* u, uint8_t* v);

@@ -54,8 +54,9 @@ class Clip:
         return self.y[t], self.u[t], self.v[t]
 
 
-def generate(width: int, height: int, frames: int, seed: int, *, global_px=6.75, global_py=None,
-             n_objects=4, obj_min=32, obj_max=96, obj_vel=3.0, zoom=1.0, sigma=2.0) -> Clip:
+def make_cfg(width: int, height: int, frames: int, seed: int, *, global_px=6.75, global_py=None,
+             n_objects=4, obj_min=32, obj_max=96, obj_vel=3.0, zoom=1.0, sigma=2.0) -> SynthCfg:
+    """The generator configuration of a clip (the layout of vc1synth_cfg / vc1cu_synth_cfg)."""
     if width % 2 or height % 2:
         raise ValueError("the internal coding raster is even (libvc1 copy_input_picture)")
     cfg = SynthCfg()
@@ -64,6 +65,11 @@ def generate(width: int, height: int, frames: int, seed: int, *, global_px=6.75,
     cfg.global_range_y_px = global_px if global_py is None else global_py
     cfg.n_objects, cfg.obj_min, cfg.obj_max, cfg.obj_vel_px = n_objects, obj_min, obj_max, obj_vel
     cfg.zoom, cfg.noise_sigma = zoom, sigma
+    return cfg
+
+
+def generate(width: int, height: int, frames: int, seed: int, **kw) -> Clip:
+    cfg = make_cfg(width, height, frames, seed, **kw)
     y = np.empty((frames, height, width), np.uint8)
     u = np.empty((frames, height // 2, width // 2), np.uint8)
     v = np.empty_like(u)
