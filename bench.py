@@ -270,6 +270,81 @@ class Runner:
         return len(self.pics) * (MBS * per_mb) + 2 * len(self.bpics) * MBS * per_b_mb + self.levels.numel() * 2
 
 
+def learned_leg(ctx, torch, l2, steps, warmup, pairs=16):
+    """The learned-proposal form against the plain form on the learned workload (1080p pairs with
+    pans of up to +-128 px, search range 128, local range 32; libvc1_b200/learned.py), both as
+    ME + quarter-pel refinement + prediction + the four transform sizes' forward transform and
+    quantiser, over `pairs` held-out pairs generated on the device. Device time per rep with CUDA
+    events on the library stream, L2 flushed between reps; the exact-SAD cost gap and fallback
+    rate of the same pairs."""
+    from libvc1_b200 import learned as lw
+    from libvc1_b200.abi import MV_QPEL
+    from libvc1_b200.api import LearnedProposals
+
+    if not os.path.exists(lw.WEIGHTS):
+        return {"unavailable": "no trained parameters (libvc1_b200/learned_weights.npy)"}
+    p = lw.params()
+    mbs = ((lw.W + 15) // 16) * ((lw.H + 15) // 16)
+    net = LearnedProposals(ctx, lw.W, lw.H, lw.RANGE, pairs, max_batch=pairs, seed=1)
+    net.set_params(np.load(lw.WEIGHTS))
+    seeds = [lw.HELD_SEED0 + 5000 + i for i in range(pairs)]
+    F0, R0, P0 = 3000, 3000, 3200
+    for k, s in enumerate(seeds):
+        cfg = lw.pair_cfg(s)
+        ctx.synth_frames(cfg, 1, 1, F0 + 2 * k)
+        ctx.synth_frames(cfg, 0, 1, F0 + 2 * k + 1)
+    levels = torch.empty((pairs, 4, mbs, 6, 64), dtype=torch.int16, device="cuda")
+    ext = torch.cuda.ExternalStream(ctx.stream_handle())
+    plain_passes = [(F0 + 2 * k, F0 + 2 * k + 1, MV_QPEL, 0, -1, R0 + k) for k in range(pairs)]
+    learned_passes = [(F0 + 2 * k, F0 + 2 * k + 1, k, MV_QPEL, R0 + 100 + k) for k in range(pairs)]
+
+    def xform(slot0):
+        for k in range(pairs):
+            ctx.motion_compensate(p, F0 + 2 * k + 1, slot0 + k, MV_QPEL, P0 + k)
+            ctx.forward_quant_device(p, F0 + 2 * k, P0 + k, 15, 0, levels[k].data_ptr())
+
+    def plain():
+        ctx.core_passes(p, plain_passes)
+        xform(R0)
+
+    def learned_form():
+        for k in range(pairs):
+            net.prepare(F0 + 2 * k, F0 + 2 * k + 1, k)
+        net.propose(0, pairs)
+        net.analyze(p, learned_passes, fallback=True)
+        xform(R0 + 100)
+
+    ms = {}
+    for name, fn in (("plain", plain), ("learned", learned_form)):
+        for _ in range(warmup):
+            fn()
+        ctx.synchronize()
+        t = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(ext):
+                l2.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ext)
+            fn()
+            b.record(ext)
+            b.synchronize()
+            t += a.elapsed_time(b)
+        ms[name] = t / steps
+    sp = np.array([ctx.read_result(p, R0 + k).screen_sads.astype(np.float64).sum() for k in range(pairs)])
+    sl = np.array([ctx.read_result(p, R0 + 100 + k).screen_sads.astype(np.float64).sum() for k in range(pairs)])
+    gap = (sl - sp) / np.maximum(sp, 1.0)
+    fb = sum(int(net.read_sample(k)[3].sum()) for k in range(pairs))
+    net.close()
+    mb = pairs * mbs
+    return {"workload": f"{pairs} held-out 1080p pairs, pans up to +-128 px, 8 objects, sigma 1-4; search range "
+                        f"{lw.RANGE}, local {lw.LOCAL}; ME + qpel + prediction + 4-size transform/quant, QP {lw.QP}",
+            "mb_per_s_plain": round(mb / (ms["plain"] * 1e-3), 1), "mb_per_s_learned": round(mb / (ms["learned"] * 1e-3), 1),
+            "speedup": round(ms["plain"] / ms["learned"], 3), "ms_per_rep_plain": round(ms["plain"], 3),
+            "ms_per_rep_learned": round(ms["learned"], 3), "cost_gap_mean": round(float(gap.mean()), 5),
+            "cost_gap_p99": round(float(np.percentile(gap, 99)), 5), "fallback_rate": round(fb / mb, 4),
+            "cost_gap_definition": "per pair (sum of the chosen vectors' exact SAD, learned - plain) / plain"}
+
+
 def flush_l2(torch, buf):
     buf.zero_()
     torch.cuda.synchronize()
@@ -412,6 +487,9 @@ def run_ours(args, rank, world, device):
     peak_ops = ctx.measure_int32_peak()
     xform_ms = timing["xform_ms"]
     xform_flops = n * MBS * XFORM_FLOPS_PER_MB * args.steps
+    learned = None
+    if not args.no_learned and world == 1:
+        learned = learned_leg(ctx, torch, l2, args.steps, args.warmup)
     out = None
     if rank == 0:
         cpu = cpu_baseline(args, clip) if (world == 1 and not args.no_cpu_baseline) else None
@@ -451,6 +529,7 @@ def run_ours(args, rank, world, device):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "mpixel_per_s": round(value * 256 / 1e6, 1),
+            "learned": learned,
         }
     ctx.close()
     return out
@@ -548,6 +627,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -11,6 +11,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -33,7 +35,10 @@ public:
         }
         return std::shared_ptr<CudaComputeContext>(new CudaComputeContext(h));
     }
-    ~CudaComputeContext() { vc1cu_close(h_); }
+    ~CudaComputeContext() {
+        if (lp_) vc1cu_lp_destroy(lp_);
+        vc1cu_close(h_);
+    }
     CudaComputeContext(const CudaComputeContext&) = delete;
     CudaComputeContext& operator=(const CudaComputeContext&) = delete;
 
@@ -70,6 +75,25 @@ public:
     // that must not interleave with another worker's: they hold this lock around it.
     std::mutex& mutex() { return mu_; }
     vc1cu_ctx* handle() const { return h_; }
+    // The learned proposals for the encoder's raster, when LIBVC1_CUDA_LEARNED names a file of
+    // vc1cu_lp_param_count() little-endian float32 parameters: unseeded 1-MV analysis passes
+    // without P-intra then use the learned pass (vc1cu_lp_analyze) instead of the plain search.
+    // Created on first use; call with the mutex held.
+    vc1cu_lp* learned(int width, int height, int search_range) {
+        if (lp_tried_) return lp_;
+        lp_tried_ = true;
+        const char* path = std::getenv("LIBVC1_CUDA_LEARNED");
+        if (!path || !*path) return nullptr;
+        std::vector<float> w(static_cast<size_t>(vc1cu_lp_param_count()));
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) throw std::runtime_error(std::string("cannot open learned parameters ") + path);
+        const size_t got = std::fread(w.data(), sizeof(float), w.size(), f);
+        std::fclose(f);
+        if (got != w.size()) throw std::runtime_error(std::string("short learned parameter file ") + path);
+        check(vc1cu_lp_create(h_, width, height, search_range, 1, 1, 1, &lp_), "vc1cu_lp_create");
+        check(vc1cu_lp_set_params(lp_, w.data()), "vc1cu_lp_set_params");
+        return lp_;
+    }
     // Throws with the library's message when rc is not VC1CU_OK.
     void check(int rc, const char* what) const {
         if (rc != VC1CU_OK) throw std::runtime_error(std::string("CUDA analysis backend: ") + what + ": " +
@@ -81,6 +105,8 @@ private:
     vc1cu_ctx* h_;
     std::string name_;
     std::mutex mu_;
+    vc1cu_lp* lp_ = nullptr;
+    bool lp_tried_ = false;
 };
 
 }  // namespace libvc1

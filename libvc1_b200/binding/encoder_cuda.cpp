@@ -51,8 +51,8 @@ vc1cu_params cuda_params(const EncoderConfig& c) {
     return p;
 }
 
-// Frame slots this binding uses for the pictures of one call.
-enum : int { kCur = 0, kRef = 1, kFuture = 2 };
+// Frame slots this binding uses for the pictures of one call, and the result slot of a learned pass.
+enum : int { kCur = 0, kRef = 1, kFuture = 2, kLearnedSlot = 3000 };
 
 void upload(CudaComputeContext& cx, int id, const Frame& f) {
     cx.check(vc1cu_upload_frame(cx.handle(), id, f.y.data(), f.u.data(), f.v.data(), f.width, f.height),
@@ -123,6 +123,17 @@ Vc1Encoder::PAnalysis Vc1Encoder::analyze_p_picture_core_cuda(const Frame& f, co
         std::lock_guard<std::mutex> lock(cx.mutex());
         upload(cx, kCur, f);
         upload(cx, kRef, ref);
+        vc1cu_lp* lp = (!shared_seed && !allow_intra && mode != ProgressiveMvMode::MixedMv && c_.motion_search_range > 0)
+                           ? cx.learned(c_.width, c_.height, c_.motion_search_range)
+                           : nullptr;
+        if (lp) {
+            // the learned proposals replace the integer search of this unseeded pass
+            const vc1cu_lp_pass q{kCur, kRef, 0, static_cast<int>(mode), kLearnedSlot, 0};
+            cx.check(vc1cu_lp_prepare(lp, kCur, kRef, 0), "vc1cu_lp_prepare");
+            cx.check(vc1cu_lp_propose(lp, 0, 1), "vc1cu_lp_propose");
+            cx.check(vc1cu_lp_analyze(lp, &p, &q, 1, 1), "vc1cu_lp_analyze");
+            cx.check(vc1cu_read_result(cx.handle(), kLearnedSlot, &o), "vc1cu_read_result");
+        } else
         cx.check(vc1cu_analyze_p_core(cx.handle(), &p, kCur, kRef, static_cast<int>(mode), allow_intra ? 1 : 0,
                                       shared_seed ? reinterpret_cast<const vc1cu_mv*>(shared_seed->mvs.data())
                                                   : nullptr,

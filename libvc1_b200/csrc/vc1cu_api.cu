@@ -657,6 +657,7 @@ struct PassExtra {
     uint8_t* fallback = nullptr;
     const uint8_t* only = nullptr;
     const int2* hint = nullptr;
+    const unsigned long long* hint_sad = nullptr;  // the frame SAD at the hint (global_full_sad)
 };
 
 int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false,
@@ -733,7 +734,11 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
                 any_hint = true;
                 ck(cudaMemcpyAsync(h[i].out.global, extra[i].hint, sizeof(int2), cudaMemcpyDeviceToDevice, c->stream),
                    "cudaMemcpyAsync(hint)");
-                ck(cudaMemsetAsync(h[i].out.gsad, 0, 8, c->stream), "cudaMemsetAsync(hint sad)");
+                if (extra[i].hint_sad)
+                    ck(cudaMemcpyAsync(h[i].out.gsad, extra[i].hint_sad, 8, cudaMemcpyDeviceToDevice, c->stream),
+                       "cudaMemcpyAsync(hint sad)");
+                else
+                    ck(cudaMemsetAsync(h[i].out.gsad, 0, 8, c->stream), "cudaMemsetAsync(hint sad)");
             }
         if (any_hint) globals_ready = true;
     }
@@ -2385,6 +2390,7 @@ struct vc1cu_lp {
     int step = 0;
     void* x0 = nullptr;             // dataset: per sample the input features
     int2* hints = nullptr;          // per sample the translation hint
+    unsigned long long* hint_sads = nullptr;  // per sample the frame SAD at the hint
     int2* labels = nullptr;         // per sample and MB the plain search's integer vector
     int2* cands = nullptr;          // per sample and MB the K candidates
     uint8_t* fallback = nullptr;    // per sample and MB the learned pass's fallback flags
@@ -2607,6 +2613,7 @@ int vc1cu_lp_create(vc1cu_ctx* c, int width, int height, int search_range, int c
             n->dgr_b = lp_alloc<void>(n.get(), 2 * db, "cudaMalloc(lp packed weights)");
             n->x0 = lp_alloc<void>(n.get(), 2 * n->xelems * capacity, "cudaMalloc(lp dataset)");
             n->hints = lp_alloc<int2>(n.get(), sizeof(int2) * capacity, "cudaMalloc(lp hints)");
+            n->hint_sads = lp_alloc<unsigned long long>(n.get(), 8 * (size_t)capacity, "cudaMalloc(lp hints)");
             n->labels = lp_alloc<int2>(n.get(), sizeof(int2) * mbs * capacity, "cudaMalloc(lp labels)");
             n->cands = lp_alloc<int2>(n.get(), sizeof(int2) * kLpK * mbs * capacity, "cudaMalloc(lp candidates)");
             n->fallback = lp_alloc<uint8_t>(n.get(), mbs * capacity, "cudaMalloc(lp fallback flags)");
@@ -2680,12 +2687,13 @@ int vc1cu_lp_prepare(vc1cu_lp* n, int cur_id, int ref_id, int sample) {
         c->used_frames.push_back(ref_id);
         const DevFrame cf = fc.view(), rf = fr.view();
         ck(lp_launch_downsample(cf.y, cf.pitch_y, rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, c->stream), "lp downsample");
-        ck(lp_launch_hint(cf.y, cf.pitch_y, rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hs, n->hints + sample, c->stream),
+        ck(lp_launch_hint(cf.y, cf.pitch_y, rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hs, n->hints + sample,
+                          n->hint_sads + sample, c->stream),
            "lp hint search");
         ck(lp_launch_features(rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hints + sample,
                               static_cast<uint16_t*>(n->x0) + n->xelems * sample, c->stream),
            "lp features");
-        c->counters.kernel_launches += 5;
+        c->counters.kernel_launches += 6;
         return VC1CU_OK;
     });
 }
@@ -2808,6 +2816,7 @@ int vc1cu_lp_analyze(vc1cu_lp* n, const vc1cu_params* p, const vc1cu_lp_pass* pa
             ex[i].cands = n->cands + kLpK * mbs * a.sample;
             ex[i].fallback = n->fallback + mbs * a.sample;
             ex[i].hint = n->hints + a.sample;
+            ex[i].hint_sad = n->hint_sads + a.sample;
         }
         for (int i = 0; i < count; ++i)
             for (int j = 0; j < i; ++j)

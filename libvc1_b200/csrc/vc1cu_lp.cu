@@ -268,6 +268,22 @@ __global__ void lp_pick_kernel(const unsigned long long* cost, LpGeom g, int2* h
     *hint = b;
 }
 
+// The full-resolution frame SAD at the hint (stride 1, clamped sampling): the analysis pass's
+// global_full_sad when the hint stands in for the global search. `sad` is zeroed by the launcher.
+__global__ void lp_hint_sad_kernel(const uint8_t* cur, int cp, const uint8_t* ref, int rp, LpGeom g, const int2* hint,
+                                   unsigned long long* sad) {
+    __shared__ unsigned long long red[8];
+    const int2 h = *hint;
+    unsigned long long s = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (long)g.W * g.H; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % g.W), y = (int)(i / g.W);
+        const int rx = min(max(x + h.x, 0), g.W - 1), ry = min(max(y + h.y, 0), g.H - 1);
+        s += (unsigned)abs((int)cur[(size_t)y * cp + x] - (int)ref[(size_t)ry * rp + rx]);
+    }
+    s = block_sum_u64(s, red);
+    if (threadIdx.x == 0) atomicAdd(sad, s);
+}
+
 // ---- input features ----------------------------------------------------------------------
 
 // Per quarter-res sample, 16 bf16 channels: cur, ref, ref shifted by the hint, the two
@@ -667,11 +683,16 @@ cudaError_t lp_launch_downsample(const uint8_t* cur, int cur_pitch, const uint8_
 
 cudaError_t lp_launch_hint(const uint8_t* cur, int cur_pitch, const uint8_t* ref, int ref_pitch, const LpGeom& g,
                            const uint8_t* cur4, const uint8_t* ref4, unsigned long long* scratch, int2* hint,
-                           cudaStream_t s) {
+                           unsigned long long* hint_sad, cudaStream_t s) {
     const int R = std::min(32, (g.range + 3) / 4), n = 2 * R + 1;
     lp_coarse_kernel<<<n * n, 256, 0, s>>>(cur4, ref4, g, scratch);
     lp_fine_kernel<<<25, 256, 0, s>>>(cur, cur_pitch, ref, ref_pitch, g, scratch);
     lp_pick_kernel<<<1, 1, 0, s>>>(scratch, g, hint);
+    cudaError_t e = cudaMemsetAsync(hint_sad, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    const long px = (long)g.W * g.H;
+    lp_hint_sad_kernel<<<(int)std::min<long>((px + 255) / 256, 1184L), 256, 0, s>>>(cur, cur_pitch, ref, ref_pitch, g,
+                                                                                  hint, hint_sad);
     return cudaGetLastError();
 }
 

@@ -82,7 +82,7 @@ cudaError_t lp_launch_downsample(const uint8_t* cur, int cur_pitch, const uint8_
                                  const LpGeom& g, uint8_t* cur4, uint8_t* ref4, cudaStream_t s);
 cudaError_t lp_launch_hint(const uint8_t* cur, int cur_pitch, const uint8_t* ref, int ref_pitch, const LpGeom& g,
                            const uint8_t* cur4, const uint8_t* ref4, unsigned long long* scratch, int2* hint,
-                           cudaStream_t s);
+                           unsigned long long* hint_sad, cudaStream_t s);
 cudaError_t lp_launch_features(const uint8_t* ref, int ref_pitch, const LpGeom& g, const uint8_t* cur4,
                                const uint8_t* ref4, const int2* hint, void* x0, cudaStream_t s);
 cudaError_t lp_launch_conv(int ca, bool dgrad, const LpConvArgs& a, int sm_count, cudaStream_t s);

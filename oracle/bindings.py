@@ -65,6 +65,8 @@ class Oracle:
         L.vo_shader_cost.restype = u64
         L.vo_hidden_padding.argtypes = [P, i32, i32, i32, i32, i32, i32, i32, i32]
         L.vo_predict_luma.argtypes = [P, vp, i32, i32, i32, i32, i32, i32, i32, vp, i32]
+        L.vo_analyze_p_learned.argtypes = [P, vp, vp, i32, vp, i32, i32, i32, vp, C.POINTER(PAnalysisC)]
+        L.vo_analyze_p_learned.restype = i32
         L.vo_global_motion.argtypes = [P, vp, vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(u64)]
         L.vo_integer_motion.argtypes = [P, vp, vp, i32, i32, vp, i32, i32, i32, C.POINTER(i32),
                                         C.POINTER(i32), C.POINTER(u64)]
@@ -158,6 +160,20 @@ class Oracle:
         if rc:
             raise RuntimeError("oracle analyze_p_core failed")
         return out.take_totals(oc)
+
+    def analyze_p_learned(self, p, cur, ref, mode, cands, hint, fallback=True):
+        """This library's learned pass (vo_analyze_p_learned): cands (mbs, 4, 2) integer pixels,
+        hint (dx, dy). Returns (Analysis, fallback flags)."""
+        mbw, mbh = mbs_of(p)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        cc = np.ascontiguousarray(cands, np.int32).reshape(-1, 2)
+        flags = np.zeros(mbw * mbh, np.uint8)
+        rc = self.lib.vo_analyze_p_learned(C.byref(p), self._f(cur), self._f(ref), mode, cc.ctypes.data, int(hint[0]),
+                                           int(hint[1]), int(fallback), flags.ctypes.data, C.byref(oc))
+        if rc:
+            raise RuntimeError("oracle analyze_p_learned failed")
+        return out.take_totals(oc), flags
 
     def scene_change_score(self, p, cur, ref, fade_compensation=True, scene_threshold=28.0):
         return self.lib.vo_scene_change_score(C.byref(p), self._f(cur), self._f(ref), int(fade_compensation),

@@ -1448,6 +1448,80 @@ static int median4(int a, int b, int c, int d) {
     return (imin(a, c) + imax(b, d)) / 2;
 }
 
+/* The integer search of an unseeded pass for one macroblock, encoder_motion.cpp:106-225: UMH or
+ * diamond about the predictor / global seeds, the propagated and content-signature long-range
+ * candidates, their distant_* records (dl, dc, dd: this macroblock's entries). The long-range
+ * index is built on first use into *cells. */
+static cand unseeded_integer(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int mx, int my,
+                             const vc1cu_mv* mvs, uint8_t* propagated, int gdx, int gdy, lr_cell** cells, int* ncells,
+                             double* dl, double* dc, uint8_t* dd) {
+    const int mbw = mbw_of(p), mbh = mbh_of(p);
+    const size_t pos = (size_t)my * mbw + mx;
+    const int range = p->search_range;
+    const int local_range = imin(range, imax(0, p->local_search_range));
+    const pinfo pi = predictor_info(mvs, mbw, mbh, mx, my);
+    cand im = {UINT64_MAX, 0, 0};
+    int selected_distant = 0;
+    const uint64_t pixels = active_mb_pixels(p, mx, my);
+    if (p->long_range_mode == 2) {
+        /* VC1_LONG_RANGE_LEGACY_DISTANT_FIRST, encoder_motion.cpp:144-160 */
+        int short_circuit = 0;
+        if (range > local_range) {
+            const cand pr = propagated_long_range(p, f, ref, mx, my, mbw, mvs, propagated, range);
+            if (motion_match_good(p, pr.cost, mx, my)) { im = pr; short_circuit = 1; selected_distant = 1; }
+        }
+        if (!short_circuit)
+            im = p->me_algorithm == 1
+                     ? integer_motion_diamond(p, f, ref, mx, my, &pi, gdx, gdy, local_range)
+                     : integer_motion_umh(p, f, ref, mx, my, &pi, gdx, gdy, local_range);
+    } else {
+        /* encoder_motion.cpp:161-196 */
+        im = p->me_algorithm == 1
+                 ? integer_motion_diamond(p, f, ref, mx, my, &pi, gdx, gdy, local_range)
+                 : integer_motion_umh(p, f, ref, mx, my, &pi, gdx, gdy, local_range);
+        const uint64_t local_sad = im.cost;
+        if (pixels) *dl = (double)local_sad / (double)pixels;
+        const int skip_distant = p->long_range_mode == 1 && motion_match_good(p, im.cost, mx, my);
+        if (range > local_range && !skip_distant) {
+            const cand pr = propagated_long_range(p, f, ref, mx, my, mbw, mvs, propagated, range);
+            const int decision = distant_match_decision(p, pr.cost, local_sad, mx, my);
+            if (pixels && pr.cost < UINT64_MAX / 8) {
+                const double mae = (double)pr.cost / (double)pixels;
+                if (*dc < 0.0 || mae < *dc) { *dc = mae; *dd = (uint8_t)decision; }
+            }
+            if (cand_less(pr.cost, pr.dx, pr.dy, im.cost, im.dx, im.dy) && decision >= 2) {
+                im = pr;
+                selected_distant = 1;
+            }
+        }
+    }
+    if (range > local_range && !motion_match_good(p, im.cost, mx, my)) {
+        /* encoder_motion.cpp:201-225 */
+        if (!*cells) {
+            const int nx = (ref->w + 7) / 8, ny = (ref->h + 7) / 8;
+            *cells = (lr_cell*)malloc(sizeof(lr_cell) * (size_t)nx * ny);
+            *ncells = 0;
+            for (int yy = 0; yy < ref->h; yy += 8)
+                for (int xx = 0; xx < ref->w; xx += 8) {
+                    (*cells)[*ncells].x = xx;
+                    (*cells)[*ncells].y = yy;
+                    (*cells)[*ncells].sig = lr_signature(ref, xx, yy);
+                    ++*ncells;
+                }
+        }
+        uint64_t ext_sad = UINT64_MAX;
+        int ext_dec = 0;
+        const cand ext = extended_content(p, f, ref, mx, my, range, *cells, *ncells, im, &ext_sad, &ext_dec);
+        if (p->long_range_mode != 2 && pixels && ext_sad < UINT64_MAX / 8) {
+            const double mae = (double)ext_sad / (double)pixels;
+            if (*dc < 0.0 || mae < *dc) { *dc = mae; *dd = (uint8_t)ext_dec; }
+        }
+        if (ext.dx != im.dx || ext.dy != im.dy) { im = ext; selected_distant = 1; }
+    }
+    if (selected_distant) propagated[pos] = 1;
+    return im;
+}
+
 /* Vc1Encoder::analyze_p_picture_core, encoder_motion.cpp:47-442 (me_quality != RD) */
 int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int mode, int allow_intra,
                       const vc1cu_mv* shared_seed, const vc1cu_panalysis* seed_distant, vc1cu_panalysis* out) {
@@ -1516,66 +1590,8 @@ int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* f, const vo_frame* 
                     seed.yq = iclamp(seed.yq, qb.ymin, qb.ymax);
                     one = refine_staged(p, f, ref, x0, y0, 16, 16, seed, range, one_mode, &rate_pi, 1, &one_sad, UINT64_MAX);
                 } else {
-                    const pinfo pi = predictor_info(mvs, mbw, mbh, mx, my);
-                    cand im = {UINT64_MAX, 0, 0};
-                    int selected_distant = 0;
-                    const uint64_t pixels = active_mb_pixels(p, mx, my);
-                    if (p->long_range_mode == 2) {
-                        /* VC1_LONG_RANGE_LEGACY_DISTANT_FIRST, encoder_motion.cpp:144-160 */
-                        int short_circuit = 0;
-                        if (range > local_range) {
-                            const cand pr = propagated_long_range(p, f, ref, mx, my, mbw, mvs, propagated, range);
-                            if (motion_match_good(p, pr.cost, mx, my)) { im = pr; short_circuit = 1; selected_distant = 1; }
-                        }
-                        if (!short_circuit)
-                            im = p->me_algorithm == 1
-                                     ? integer_motion_diamond(p, f, ref, mx, my, &pi, gdx, gdy, local_range)
-                                     : integer_motion_umh(p, f, ref, mx, my, &pi, gdx, gdy, local_range);
-                    } else {
-                        /* encoder_motion.cpp:161-196 */
-                        im = p->me_algorithm == 1
-                                 ? integer_motion_diamond(p, f, ref, mx, my, &pi, gdx, gdy, local_range)
-                                 : integer_motion_umh(p, f, ref, mx, my, &pi, gdx, gdy, local_range);
-                        const uint64_t local_sad = im.cost;
-                        if (pixels) dl[pos] = (double)local_sad / (double)pixels;
-                        const int skip_distant = p->long_range_mode == 1 && motion_match_good(p, im.cost, mx, my);
-                        if (range > local_range && !skip_distant) {
-                            const cand pr = propagated_long_range(p, f, ref, mx, my, mbw, mvs, propagated, range);
-                            const int decision = distant_match_decision(p, pr.cost, local_sad, mx, my);
-                            if (pixels && pr.cost < UINT64_MAX / 8) {
-                                const double mae = (double)pr.cost / (double)pixels;
-                                if (dc[pos] < 0.0 || mae < dc[pos]) { dc[pos] = mae; dd[pos] = (uint8_t)decision; }
-                            }
-                            if (cand_less(pr.cost, pr.dx, pr.dy, im.cost, im.dx, im.dy) && decision >= 2) {
-                                im = pr;
-                                selected_distant = 1;
-                            }
-                        }
-                    }
-                    if (range > local_range && !motion_match_good(p, im.cost, mx, my)) {
-                        /* encoder_motion.cpp:201-225 */
-                        if (!cells) {
-                            const int nx = (ref->w + 7) / 8, ny = (ref->h + 7) / 8;
-                            cells = (lr_cell*)malloc(sizeof(lr_cell) * (size_t)nx * ny);
-                            ncells = 0;
-                            for (int yy = 0; yy < ref->h; yy += 8)
-                                for (int xx = 0; xx < ref->w; xx += 8) {
-                                    cells[ncells].x = xx;
-                                    cells[ncells].y = yy;
-                                    cells[ncells].sig = lr_signature(ref, xx, yy);
-                                    ++ncells;
-                                }
-                        }
-                        uint64_t ext_sad = UINT64_MAX;
-                        int ext_dec = 0;
-                        const cand ext = extended_content(p, f, ref, mx, my, range, cells, ncells, im, &ext_sad, &ext_dec);
-                        if (p->long_range_mode != 2 && pixels && ext_sad < UINT64_MAX / 8) {
-                            const double mae = (double)ext_sad / (double)pixels;
-                            if (dc[pos] < 0.0 || mae < dc[pos]) { dc[pos] = mae; dd[pos] = (uint8_t)ext_dec; }
-                        }
-                        if (ext.dx != im.dx || ext.dy != im.dy) { im = ext; selected_distant = 1; }
-                    }
-                    if (selected_distant) propagated[pos] = 1;
+                    const cand im = unseeded_integer(p, f, ref, mx, my, mvs, propagated, gdx, gdy, &cells, &ncells,
+                                                     &dl[pos], &dc[pos], &dd[pos]);
                     const vc1cu_mv s4 = {im.dx * 4, im.dy * 4};
                     one = refine_staged(p, f, ref, x0, y0, 16, 16, s4, range, one_mode, &rate_pi, 1, &one_sad, im.cost);
                 }
@@ -2252,6 +2268,141 @@ int vo_zoom_coherent(const vc1cu_mv* mvs, int mbw, int mbh) {
         }
     const long double az = fabsl(z);
     return inliers * 5 >= samples * 3 && az >= 0.005L && az <= 0.08L;
+}
+
+/* The learned analysis pass of this library (no counterpart in the reference; on the device:
+ * learned_candidates / learned_descent in libvc1_b200/csrc/vc1cu_core.cu and the two launches of
+ * vc1cu_lp_analyze). Pass A, raster order: the best of each macroblock's four integer-pixel
+ * candidates (clamped to the search bounds) by exact mb_sad, a small-diamond descent of at most
+ * 2 * reach steps within reach of it, the fallback flag (motion_match_good fails), then the staged
+ * refinement with the macroblock's real predictor, as an unseeded pass refines its integer vector
+ * (encoder_motion.cpp:226-230). Pass B (fallback != 0), raster order over the flagged macroblocks
+ * only: the unseeded pass's integer search with the hint as its global vector and the current
+ * field as neighbours, then the same refinement. Totals as analyze_p_picture_core's, with the
+ * hint's full-resolution frame SAD standing in for the global search's. */
+int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int mode, const vc1cu_mv* cands,
+                         int hint_dx, int hint_dy, int fallback, uint8_t* flags, vc1cu_panalysis* out) {
+    if (f->w != p->width || f->h != p->height || ref->w != p->width || ref->h != p->height) return 1;
+    if (mode == VC1CU_MV_MIXED || p->search_range == 0) return 2;
+    const int mbw = mbw_of(p), mbh = mbh_of(p);
+    const size_t mbs = (size_t)mbw * mbh;
+    const int range = p->search_range, reach = 4;
+    const bounds b = bounds_px(range);
+    vc1cu_mv* mvs = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    vc1cu_mv* bmv = (vc1cu_mv*)calloc(mbs * 4, sizeof(vc1cu_mv));
+    uint8_t* intra = (uint8_t*)calloc(mbs, 1);
+    uint8_t* propagated = (uint8_t*)calloc(mbs, 1);
+    uint64_t* screen = (uint64_t*)calloc(mbs, sizeof(uint64_t));
+    double* dl = (double*)malloc(mbs * sizeof(double));
+    double* dc = (double*)malloc(mbs * sizeof(double));
+    uint8_t* dd = (uint8_t*)calloc(mbs, 1);
+    lr_cell* cells = NULL;
+    int ncells = 0;
+    for (size_t i = 0; i < mbs; ++i) { dl[i] = -1.0; dc[i] = -1.0; }
+    for (int pass = 0; pass < (fallback ? 2 : 1); ++pass)
+        for (int my = 0; my < mbh; ++my)
+            for (int mx = 0; mx < mbw; ++mx) {
+                const size_t pos = (size_t)my * mbw + mx;
+                if (pass == 1 && !flags[pos]) continue;
+                const int x0 = mx * 16, y0 = my * 16;
+                const uint64_t pixels = active_mb_pixels(p, mx, my);
+                const pinfo rate_pi = predictor_info_mixed_1mv(bmv, intra, mbw, mbh, mx, my);
+                cand best = {UINT64_MAX, 0, 0};
+                if (pass == 0) {
+                    for (int k = 0; k < 4; ++k) {
+                        const int cx = iclamp(cands[pos * 4 + k].xq, b.xmin, b.xmax);
+                        const int cy = iclamp(cands[pos * 4 + k].yq, b.ymin, b.ymax);
+                        const uint64_t c = vo_mb_sad(p, f, ref, mx, my, cx, cy, 1);
+                        if (k == 0 || cand_less(c, cx, cy, best.cost, best.dx, best.dy)) {
+                            best.cost = c;
+                            best.dx = cx;
+                            best.dy = cy;
+                        }
+                    }
+                    const int sx = best.dx, sy = best.dy;
+                    for (int step = 0; step < 2 * reach; ++step) {
+                        cand nb = {UINT64_MAX, 0, 0};
+                        int any = 0;
+                        for (int l = 0; l < 4; ++l) {
+                            const int dx = best.dx + (l == 0) - (l == 1), dy = best.dy + (l == 2) - (l == 3);
+                            if (dx < b.xmin || dx > b.xmax || dy < b.ymin || dy > b.ymax || iabs(dx - sx) > reach ||
+                                iabs(dy - sy) > reach)
+                                continue;
+                            const uint64_t c = vo_mb_sad(p, f, ref, mx, my, dx, dy, 1);
+                            if (!any || cand_less(c, dx, dy, nb.cost, nb.dx, nb.dy)) {
+                                nb.cost = c;
+                                nb.dx = dx;
+                                nb.dy = dy;
+                                any = 1;
+                            }
+                        }
+                        if (!any || !cand_less(nb.cost, nb.dx, nb.dy, best.cost, best.dx, best.dy)) break;
+                        best = nb;
+                    }
+                    if (flags) flags[pos] = motion_match_good(p, best.cost, mx, my) ? 0 : 1;
+                    if (pixels) dl[pos] = (double)best.cost / (double)pixels;
+                } else {
+                    dl[pos] = -1.0;
+                    dc[pos] = -1.0;
+                    dd[pos] = 0;
+                    best = unseeded_integer(p, f, ref, mx, my, mvs, propagated, hint_dx, hint_dy, &cells, &ncells,
+                                            &dl[pos], &dc[pos], &dd[pos]);
+                }
+                uint64_t one_sad = 0;
+                const vc1cu_mv s4 = {best.dx * 4, best.dy * 4};
+                vc1cu_mv one = refine_staged(p, f, ref, x0, y0, 16, 16, s4, range, mode, &rate_pi, 1, &one_sad, best.cost);
+                if (vo_hidden_padding(p, x0, y0, 16, 16, one.xq, one.yq, mode, 1)) {
+                    one.xq = 0;
+                    one.yq = 0;
+                    one_sad = vo_block_sad_motion(p, f, ref, x0, y0, 16, 16, 0, 0, mode);
+                }
+                mvs[pos] = one;
+                for (int k = 0; k < 4; ++k) bmv[pos * 4 + k] = one;
+                screen[pos] = one_sad;
+            }
+    uint64_t total_sad = 0, total_pixels = 0, moved = 0, frac = 0;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = (size_t)my * mbw + mx;
+            total_sad += screen[pos];
+            total_pixels += active_mb_pixels(p, mx, my);
+            moved += mvs[pos].xq != 0 || mvs[pos].yq != 0;
+            frac += (mvs[pos].xq % 8) != 0 || (mvs[pos].yq % 8) != 0;
+        }
+    const uint64_t gsad = vo_frame_sad(f, ref, hint_dx, hint_dy, 1);
+    const double local_mad = total_pixels ? (double)total_sad / (double)total_pixels : 0.0;
+    const double global_mad = (double)gsad / (double)((uint64_t)p->width * p->height);
+    out->mean_abs_residual = local_mad < global_mad ? local_mad : global_mad;
+    out->rate_complexity = out->mean_abs_residual;
+    out->motion_sad = total_sad;
+    for (size_t i = 0; i < mbs; ++i) {
+        if (out->mvs) out->mvs[i] = mvs[i];
+        if (out->block_mvs) for (int k = 0; k < 4; ++k) out->block_mvs[i * 4 + k] = bmv[i * 4 + k];
+        if (out->use_4mv) out->use_4mv[i] = 0;
+        if (out->use_intra) out->use_intra[i] = 0;
+        if (out->screen_sads) out->screen_sads[i] = screen[i];
+        if (out->inter_intra_cost_ratio) out->inter_intra_cost_ratio[i] = -1.0;
+        if (out->distant_local_mae) out->distant_local_mae[i] = dl[i];
+        if (out->distant_candidate_mae) out->distant_candidate_mae[i] = dc[i];
+        if (out->distant_match_decision) out->distant_match_decision[i] = dd[i];
+    }
+    out->moved_macroblocks = moved;
+    out->fractional_chroma_macroblocks = frac;
+    out->four_mv_macroblocks = 0;
+    out->intra_macroblocks = 0;
+    out->global_dx = hint_dx;
+    out->global_dy = hint_dy;
+    out->global_full_sad = gsad;
+    free(mvs);
+    free(bmv);
+    free(intra);
+    free(propagated);
+    free(screen);
+    free(dl);
+    free(dc);
+    free(dd);
+    free(cells);
+    return 0;
 }
 
 /* Vc1Encoder::scene_change_score, encoder_motion.cpp:599-676: the whole-frame translation

@@ -73,6 +73,9 @@ void vo_integer_motion(const vc1cu_params* p, const vo_frame* cur, const vo_fram
 int vo_analyze_p_core(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int mode,
                       int allow_intra, const vc1cu_mv* seed, const vc1cu_panalysis* seed_distant,
                       vc1cu_panalysis* out);
+/* This library's learned analysis pass (candidates, descent, fallback to the plain search). */
+int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* cur, const vo_frame* ref, int mode, const vc1cu_mv* cands,
+                         int hint_dx, int hint_dy, int fallback, uint8_t* flags, vc1cu_panalysis* out);
 
 /* intensity compensation (fades) */
 void vo_intensity_compensate(const vo_frame* ref, const vc1cu_intensity* ic, uint8_t* y, uint8_t* u, uint8_t* v);

@@ -132,6 +132,39 @@ def test_training_on_device_reduces_the_loss(ctx):
     assert last < 0.7 * first, (first, last)
 
 
+LEARNED_CASES = {
+    # (w, h, display, range, local range, mode, fallback, global px)
+    "cif_qpel": (352, 288, None, 64, 32, MV_QPEL, True, 40.0),
+    "odd_hpel": (322, 242, (321, 241), 32, 32, 1, True, 20.0),
+    "longrange_bilinear": (192, 128, None, 128, 16, 2, True, 70.0),
+    "no_fallback": (256, 160, None, 64, 32, MV_QPEL, False, 30.0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(LEARNED_CASES))
+def test_learned_pass_matches_oracle(ctx, oracle, case):
+    """Both launches of the learned pass, bit for bit against the oracle's restatement
+    (oracle/vc1_oracle.c vo_analyze_p_learned) on the device's own candidates and hint."""
+    w, h, disp, rng, local, mode, fallback, gpx = LEARNED_CASES[case]
+    clip = _clip(w, h, 51, gpx)
+    kw = dict(display_width=disp[0], display_height=disp[1]) if disp else {}
+    p = make_params(w, h, search_range=rng, local_search_range=local, **kw)
+    ctx.upload_frame(0, *clip.frame(1))
+    ctx.upload_frame(1, *clip.frame(0))
+    net = LearnedProposals(ctx, w, h, rng, capacity=1, max_batch=1, seed=6)
+    try:
+        net.prepare(0, 1, 0)
+        net.propose(0, 1)
+        net.analyze(p, [(0, 1, 0, mode, 970)], fallback=fallback)
+        got = ctx.read_result(p, 970)
+        _, hint, cands, flags = net.read_sample(0)
+    finally:
+        net.close()
+    want, wflags = oracle.analyze_p_learned(p, clip.frame(1), clip.frame(0), mode, cands, hint, fallback)
+    assert np.array_equal(flags, wflags)
+    assert got.equal(want) == []
+
+
 def test_learned_pass_with_fallback(ctx):
     """Every macroblock gets a legal vector; with the plain search as fallback the mean exact
     cost stays close to the plain pass's."""
