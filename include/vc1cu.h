@@ -301,6 +301,43 @@ typedef struct vc1cu_pass {
 } vc1cu_pass;
 
 int vc1cu_core_passes(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_pass* passes, int n);
+/*
+ * Passes over pictures of different sizes (many clips) in ONE persistent launch: params holds one
+ * parameter block per pass (its raster, display crop, PQINDEX, rounding control); the search
+ * configuration (ranges, algorithm, quality, sub-pel and long-range settings, thresholds) must be
+ * the same in all of them. A pass may be seeded by another pass of the same call (a picture's
+ * seed pass, mode passes and final pass together), as in vc1cu_core_passes. The work queue
+ * interleaves every pass's wavefront, so no picture waits for another. Asynchronous.
+ */
+int vc1cu_core_passes_multi(vc1cu_ctx* ctx, const vc1cu_params* params, const vc1cu_pass* passes, int n);
+
+/*
+ * CUDA graphs of the context's work (no counterpart in the reference, whose GOP workers call the
+ * analysis per picture): vc1cu_graph_begin opens a capture of the context stream; the
+ * asynchronous calls that follow (vc1cu_core_passes[_multi], vc1cu_motion_compensate,
+ * vc1cu_forward_quant_device, vc1cu_reconstruct, vc1cu_synth_frames, ...) are recorded, not run;
+ * vc1cu_graph_end instantiates them as graph *graph_id. vc1cu_graph_launch replays it on the
+ * context stream (the result slots it writes become readable as after the recorded calls), so a
+ * GOP's launches cost one host call. Each launch shape must have run once before it is captured
+ * (the work-item tables and slots are built outside captures); calls that wait for the device
+ * (reads, synchronous calls) fail inside a capture and close it. Core passes in a graph clear their
+ * macroblock done flags at every replay.
+ */
+int vc1cu_graph_begin(vc1cu_ctx* ctx);
+int vc1cu_graph_end(vc1cu_ctx* ctx, int* graph_id);
+int vc1cu_graph_launch(vc1cu_ctx* ctx, int graph_id);
+int vc1cu_graph_destroy(vc1cu_ctx* ctx, int graph_id);
+
+/*
+ * Launch-shape autotuner (no counterpart in the reference): runs the given passes as one launch
+ * (per_pass_params: params holds one block per pass, as vc1cu_core_passes_multi; else one block)
+ * under several shapes of the persistent core kernel - macroblocks (warps) per block 1..4 and
+ * blocks per SM - and keeps the fastest for this raster, search configuration and kernel
+ * instantiation; later launches of that key use it. The passes' result slots are overwritten.
+ * Synchronous; *warps, *blocks (0 = as many as fit) and *ms (one launch) may be NULL.
+ */
+int vc1cu_autotune(vc1cu_ctx* ctx, const vc1cu_params* params, const vc1cu_pass* passes, int n, int per_pass_params,
+                   int* warps, int* blocks, double* ms);
 /* Copies a result slot to host arrays (and the scalar totals). Synchronous: returns once the
  * launch that last wrote the slot (as enqueued before this call) has finished and the copies have
  * landed; work enqueued after that launch keeps running (the copies use a second stream), so a

@@ -41,7 +41,8 @@ EXPORTS = (
     "vc1cu_fast_transform_types", "vc1cu_debug_set_wait_limit", "vc1cu_debug_withhold_publish",
     "vc1cu_synth_frames", "vc1cu_lp_param_count", "vc1cu_lp_create", "vc1cu_lp_destroy", "vc1cu_lp_get_params",
     "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
-    "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze",
+    "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
+    "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
 )
 
 
@@ -82,6 +83,13 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_download_frame.argtypes = [vp, i32, vp, vp, vp]
     L.vc1cu_analyze_p_core.argtypes = [vp, PP, i32, i32, i32, i32, vp, C.POINTER(PAnalysisC), C.POINTER(PAnalysisC)]
     L.vc1cu_core_passes.argtypes = [vp, PP, C.POINTER(Pass), i32]
+    L.vc1cu_core_passes_multi.argtypes = [vp, PP, C.POINTER(Pass), i32]
+    L.vc1cu_graph_begin.argtypes = [vp]
+    L.vc1cu_graph_end.argtypes = [vp, C.POINTER(i32)]
+    L.vc1cu_graph_launch.argtypes = [vp, i32]
+    L.vc1cu_graph_destroy.argtypes = [vp, i32]
+    L.vc1cu_autotune.argtypes = [vp, PP, C.POINTER(Pass), i32, i32, C.POINTER(i32), C.POINTER(i32),
+                                 C.POINTER(C.c_double)]
     L.vc1cu_read_result.argtypes = [vp, i32, C.POINTER(PAnalysisC)]
     L.vc1cu_synchronize.argtypes = [vp]
     L.vc1cu_motion_compensate.argtypes = [vp, PP, i32, i32, i32, i32]
@@ -288,6 +296,38 @@ class CudaComputeContext:
         """passes: iterable of (cur_id, ref_id, mode, allow_intra, seed_slot, out_slot[, pqindex])."""
         arr = (Pass * len(passes))(*[Pass(*p) for p in passes])
         self._check(self._L.vc1cu_core_passes(self._h, C.byref(params), arr, len(passes)))
+
+    def core_passes_multi(self, params_list, passes):
+        """Passes over pictures of different sizes in one launch: params_list[i] is pass i's
+        parameter block; passes as for core_passes."""
+        arr = (Pass * len(passes))(*[Pass(*p) for p in passes])
+        pp = (Params * len(params_list))(*params_list)
+        self._check(self._L.vc1cu_core_passes_multi(self._h, pp, arr, len(passes)))
+
+    def graph_begin(self):
+        self._check(self._L.vc1cu_graph_begin(self._h))
+
+    def graph_end(self) -> int:
+        g = C.c_int()
+        self._check(self._L.vc1cu_graph_end(self._h, C.byref(g)))
+        return g.value
+
+    def graph_launch(self, graph_id: int):
+        self._check(self._L.vc1cu_graph_launch(self._h, graph_id))
+
+    def graph_destroy(self, graph_id: int):
+        self._check(self._L.vc1cu_graph_destroy(self._h, graph_id))
+
+    def autotune(self, params, passes):
+        """params: one Params (one raster) or a list with one per pass (vc1cu_core_passes_multi).
+        Returns (warps per block, blocks per SM or 0, ms per launch) of the fastest shape."""
+        arr = (Pass * len(passes))(*[Pass(*p) for p in passes])
+        multi = isinstance(params, (list, tuple))
+        pp = (Params * len(params))(*params) if multi else C.byref(params)
+        w, b, ms = C.c_int(), C.c_int(), C.c_double()
+        self._check(self._L.vc1cu_autotune(self._h, pp, arr, len(passes), int(multi), C.byref(w), C.byref(b),
+                                           C.byref(ms)))
+        return w.value, b.value, ms.value
 
     def read_result(self, params: Params, slot: int) -> Analysis:
         mbw, mbh = mbs_of(params)

@@ -260,6 +260,25 @@ struct vc1cu_ctx {
     } staging_ring[kStagingRing];
     int staging_next = 0, staging_cur = 0;
     uint32_t epoch = 0;
+    // CUDA-graph capture (vc1cu_graph_begin / _end): while capturing, launch descriptors go to
+    // pinned buffers the graph keeps, core launches clear their done flags and use a fixed epoch,
+    // and the slots the captured work writes are recorded for the graph's launches.
+    bool capturing = false;
+    std::vector<void*> capture_hold;
+    std::vector<int> capture_results, capture_bresults, capture_frames;
+    struct Graph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<void*> hold;
+        std::vector<int> results, bresults, frames;
+    };
+    std::map<int, Graph> graphs;
+    int graph_next = 1;
+    // launch shapes chosen by vc1cu_autotune: key (W, H, range, local range, instantiation) ->
+    // (warps per block, blocks per SM; 0 = the occupancy limit)
+    std::map<std::vector<int>, std::pair<int, int>> tuned;
+    std::pair<int, int> tune_force{0, 0};  // a shape under trial (vc1cu_autotune), (0, 0) otherwise
+    std::vector<int> last_tune_key;        // the key of the last core launch
     int wait_log2 = 24;                  // vc1cu_debug_set_wait_limit
     uint32_t withhold_next = 0xFFFFFFFFu;  // vc1cu_debug_withhold_publish (next core launch only)
     int sm_count = 0;
@@ -295,6 +314,8 @@ int fail(vc1cu_ctx* c, int code, const std::string& msg) {
 
 void stamp_written(vc1cu_ctx* c);
 
+void abort_capture(vc1cu_ctx* c);
+
 template <class F>
 int guarded(vc1cu_ctx* c, F&& f) {
     if (!c) return fail(nullptr, VC1CU_ERR_ARG, "null context");
@@ -309,6 +330,7 @@ int guarded(vc1cu_ctx* c, F&& f) {
             stamp_written(c);  // slots the failed call wrote before its error
         } catch (const Fail&) {
         }
+        abort_capture(c);
         return fail(c, e.code, e.msg);
     } catch (const std::bad_alloc&) {
         return fail(c, VC1CU_ERR_OOM, "host allocation failed");
@@ -393,31 +415,44 @@ void set_lambda(PassDesc& d, int pq) {
 // follow the wavefront order (t = x + 2y, then y); a pass at seed level L (seeded by a pass
 // of the same launch at level L-1) is delayed by L * lag positions, so each item follows all
 // of its dependencies. Cached per (raster, pass levels).
-const uint32_t* work_items(vc1cu_ctx* c, int mbw, int mbh, const std::vector<int>& level, unsigned& nitems) {
-    std::vector<int> key = {mbw, mbh};
-    key.insert(key.end(), level.begin(), level.end());
+const uint32_t* work_items(vc1cu_ctx* c, const std::vector<int>& mbw, const std::vector<int>& mbh,
+                           const std::vector<int>& level, unsigned& nitems) {
+    const int n = (int)level.size();
+    std::vector<int> key;
+    for (int p = 0; p < n; ++p) {
+        key.push_back(mbw[p]);
+        key.push_back(mbh[p]);
+        key.push_back(level[p]);
+    }
     auto it = c->items.find(key);
     if (it != c->items.end()) {
         nitems = it->second.second;
         return it->second.first;
     }
-    std::vector<int> order;
-    order.reserve((size_t)mbw * mbh);
-    for (int t = 0; t <= (mbw - 1) + 2 * (mbh - 1); ++t)
-        for (int y = 0; y < mbh; ++y) {
-            const int x = t - 2 * y;
-            if (x >= 0 && x < mbw) order.push_back(y * mbw + x);
-        }
-    const int mbs = mbw * mbh, n = (int)level.size();
-    const int lag = mbw;  // about two wavefront steps of the raster
-    int maxl = 0;
-    for (int l : level) maxl = std::max(maxl, l);
+    // Each pass's macroblocks in its own wavefront order (t = x + 2y, then y); a seeded pass runs
+    // about two wavefront steps (one raster row of macroblocks) behind its seed pass. The passes'
+    // lists are merged by that step, so every item's dependencies (its neighbours and its seed)
+    // are handed out before it, whatever the passes' raster sizes.
+    std::vector<std::vector<int>> order(n);
+    long steps = 0;
+    for (int p = 0; p < n; ++p) {
+        const int w = mbw[p], hh = mbh[p];
+        order[p].reserve((size_t)w * hh);
+        for (int t = 0; t <= (w - 1) + 2 * (hh - 1); ++t)
+            for (int y = 0; y < hh; ++y) {
+                const int x = t - 2 * y;
+                if (x >= 0 && x < w) order[p].push_back(y * w + x);
+            }
+        steps = std::max(steps, (long)w * hh + (long)w * level[p]);
+    }
+    if (c->capturing)
+        throw Fail{VC1CU_ERR_STATE, "run a launch of this shape once before capturing it (its work-item table is "
+                                    "built and uploaded outside the capture)"};
     std::vector<uint32_t> items;
-    items.reserve((size_t)n * mbs);
-    for (long sstep = 0; sstep < (long)mbs + (long)lag * maxl; ++sstep)
+    for (long sstep = 0; sstep < steps; ++sstep)
         for (int p = 0; p < n; ++p) {
-            const long j = sstep - (long)lag * level[p];
-            if (j >= 0 && j < mbs) items.push_back(((uint32_t)p << 20) | (uint32_t)order[j]);
+            const long j = sstep - (long)mbw[p] * level[p];
+            if (j >= 0 && j < (long)order[p].size()) items.push_back(((uint32_t)p << 20) | (uint32_t)order[p][j]);
         }
     void* d = nullptr;
     ck(cudaMalloc(&d, items.size() * sizeof(uint32_t)), "cudaMalloc(work items)");
@@ -566,7 +601,7 @@ struct Timer {
     int family;
     cudaEvent_t a = nullptr;
     Timer(vc1cu_ctx* cc, int f) : c(cc), family(f) {
-        if (c->timing) {
+        if (c->timing && !c->capturing) {
             a = take_event(c);
             ck(cudaEventRecord(a, c->stream), "cudaEventRecord");
         }
@@ -606,6 +641,13 @@ void collect_timing(vc1cu_ctx* c) {
 // Pinned staging for host->device launch descriptors: the next buffer of the ring, once its
 // previous copy is done. The caller copies out of it on the context stream, then staging_mark.
 void* staging(vc1cu_ctx* c, size_t bytes) {
+    if (c->capturing) {
+        // a captured copy reads its source at every launch of the graph: a buffer of its own
+        void* h = nullptr;
+        ck(cudaMallocHost(&h, bytes), "cudaMallocHost(captured staging)");
+        c->capture_hold.push_back(h);
+        return h;
+    }
     const int i = c->staging_next;
     c->staging_next = (i + 1) % vc1cu_ctx::kStagingRing;
     auto& b = c->staging_ring[i];
@@ -624,6 +666,7 @@ void* staging(vc1cu_ctx* c, size_t bytes) {
 
 // Records the copy out of the buffer the last staging() call handed out.
 void staging_mark(vc1cu_ctx* c) {
+    if (c->capturing) return;
     ck(cudaEventRecord(c->staging_ring[c->staging_cur].done, c->stream), "cudaEventRecord(staging)");
 }
 
@@ -660,14 +703,30 @@ struct PassExtra {
     const unsigned long long* hint_sad = nullptr;  // the frame SAD at the hint (global_full_sad)
 };
 
+// The search configuration every pass of one launch shares (the kernel's window, bitsets and
+// instantiation depend on it); the picture geometry, rounding control and quantiser may differ.
+void same_search_config(const DevParams& a, const DevParams& b) {
+    if (a.range != b.range || a.local_range != b.local_range || a.me_algorithm != b.me_algorithm ||
+        a.me_quality != b.me_quality || a.subpel != b.subpel || a.fast_subpel != b.fast_subpel ||
+        a.subpel_range != b.subpel_range || a.long_range_mode != b.long_range_mode ||
+        a.disable_p_intra != b.disable_p_intra || a.distant_match_max_mae != b.distant_match_max_mae ||
+        a.inter_intra_threshold != b.inter_intra_threshold)
+        throw Fail{VC1CU_ERR_ARG, "passes of one launch must share the search configuration (ranges, algorithm, "
+                                  "quality, sub-pel and long-range settings, thresholds)"};
+}
+
+// The autotuner's cache key of a launch: raster, ranges, algorithm and the instantiation.
+std::vector<int> tune_key(const DevParams& P, int kind) { return {P.W, P.H, P.range, P.local_range, P.me_algorithm, kind}; }
+
+// per_pass: null, or n parameter blocks (pictures of different sizes in one kCoreMulti launch).
 int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false,
-                 const PassExtra* extra = nullptr) {
+                 const PassExtra* extra = nullptr, const vc1cu_params* per_pass = nullptr) {
     DevParams P;
     std::string why;
-    int rc = make_dev_params(p, P, why);
+    int rc = make_dev_params(per_pass ? per_pass : p, P, why);
     if (rc) throw Fail{rc, why};
     if (n <= 0) return VC1CU_OK;
-    const int mbs = P.mbw * P.mbh;
+    const bool multi = per_pass != nullptr;
     bool any_unseeded = false;
     std::vector<PassDesc> h(n);
     std::vector<int> unseeded;
@@ -676,17 +735,24 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         if (q.mode < 0 || q.mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
         if (q.out_slot < 0 || q.out_slot > kInternalLast || q.seed_slot == q.out_slot)
             throw Fail{VC1CU_ERR_ARG, "invalid result slot"};
+        PassDesc& d = h[i];
+        d.geom = P;
+        if (multi) {
+            rc = make_dev_params(per_pass + i, d.geom, why);
+            if (rc) throw Fail{rc, why};
+            same_search_config(P, d.geom);
+        }
+        const int mbs = d.geom.mbw * d.geom.mbh;
         FrameSlot& fc = frame_slot(c, q.cur_id);
         FrameSlot& fr = frame_slot(c, q.ref_id);
-        if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+        if (fc.w != d.geom.W || fc.h != d.geom.H || fr.w != d.geom.W || fr.h != d.geom.H)
             throw Fail{VC1CU_ERR_ARG, "P-picture reference dimensions do not match the configuration"};
-        PassDesc& d = h[i];
         d.cur = fc.view();
         d.ref = fr.view();
         d.mode = q.mode;
         d.allow_intra = q.allow_intra != 0;
         if (q.pqindex < 0 || q.pqindex > 31) throw Fail{VC1CU_ERR_ARG, "pass pqindex must be 0 (params) or 1..31"};
-        set_lambda(d, q.pqindex ? q.pqindex : P.pq);
+        set_lambda(d, q.pqindex ? q.pqindex : d.geom.pq);
         d.seeded = q.seed_slot >= 0;
         d.seed_pass = -1;
         for (int j = 0; j < n; ++j)
@@ -711,7 +777,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     }
     bool learned = false;
     for (int i = 0; i < n; ++i) {
-        ResultSlot& o = result_slot(c, passes[i].out_slot, mbs, true);
+        ResultSlot& o = result_slot(c, passes[i].out_slot, h[i].geom.mbw * h[i].geom.mbh, true);
         o.mode = passes[i].mode;
         o.seeded = passes[i].seed_slot >= 0;
         o.allow_intra = passes[i].allow_intra != 0;
@@ -781,28 +847,45 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         }
         uint8_t* hs = static_cast<uint8_t*>(staging(c, gb * nu));
         const int grange = std::min(P.local_range, 32);
+        // states in raster-size order, so that every size's searches are one contiguous run
+        std::vector<int> order(unseeded);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return h[x].geom.W != h[y].geom.W ? h[x].geom.W < h[y].geom.W : h[x].geom.H < h[y].geom.H;
+        });
         for (int k = 0; k < nu; ++k) {
-            const PassDesc& d = h[unseeded[k]];
+            const PassDesc& d = h[order[k]];
             init_gstate(reinterpret_cast<GState*>(hs + gb * k), d.cur, d.ref, grange, d.out.global, d.out.gsad);
         }
         ck(cudaMemcpyAsync(c->d_gstates, hs, gb * nu, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(gstate)");
         staging_mark(c);
         Timer tm(c, kGlobal);
-        const int launches = run_global_search(c->d_gstates, nu, grange, P.W, P.H, c->stream);
+        int launches = 0;
+        for (int k0 = 0; k0 < nu;) {
+            int k1 = k0 + 1;
+            const DevParams& g0 = h[order[k0]].geom;
+            while (k1 < nu && h[order[k1]].geom.W == g0.W && h[order[k1]].geom.H == g0.H) ++k1;
+            launches += run_global_search(reinterpret_cast<GState*>(reinterpret_cast<uint8_t*>(c->d_gstates) + gb * k0),
+                                          k1 - k0, grange, g0.W, g0.H, c->stream);
+            k0 = k1;
+        }
         ck(cudaGetLastError(), "global search launch");
         tm.stop(launches);
     }
     // long-range signature index of each long-range pass's reference (build_long_range_index)
     if (!unseeded.empty() && P.range > P.local_range && !learned) {
-        const int nx = (P.W + 7) / 8, ny = (P.H + 7) / 8;
-        const size_t per = sizeof(uint64_t) * (size_t)nx * ny;
+        size_t per = 0;
+        for (size_t k = 0; k < unseeded.size(); ++k)
+            per = std::max(per, sizeof(uint64_t) * (size_t)((h[unseeded[k]].geom.W + 7) / 8) *
+                                    (size_t)((h[unseeded[k]].geom.H + 7) / 8));
         uint64_t* base = static_cast<uint64_t*>(ensure(c->d_lr, c->lr_cap, per * unseeded.size(), "cudaMalloc(long-range index)"));
         for (size_t k = 0; k < unseeded.size(); ++k) {
             PassDesc& d = h[unseeded[k]];
-            d.lr_sig = base + (size_t)nx * ny * k;
+            const int nx = (d.geom.W + 7) / 8, ny = (d.geom.H + 7) / 8;
+            d.lr_sig = base + per / sizeof(uint64_t) * k;
             d.lr_nx = nx;
             d.lr_ny = ny;
-            ck(launch_lr_index(d.ref, P.W, P.H, const_cast<uint64_t*>(d.lr_sig), c->stream), "lr_index_kernel launch");
+            ck(launch_lr_index(d.ref, d.geom.W, d.geom.H, const_cast<uint64_t*>(d.lr_sig), c->stream),
+               "lr_index_kernel launch");
             c->counters.kernel_launches++;
         }
     }
@@ -851,7 +934,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     wc.warp_bytes = warp_bytes_for_host(wc);
     int warps = 4;
     while (warps > 1 && (size_t)warps * wc.warp_bytes > (size_t)c->max_smem) --warps;
-    const size_t smem = (size_t)warps * wc.warp_bytes;
+    size_t smem = (size_t)warps * wc.warp_bytes;
     if (smem > (size_t)c->max_smem)
         throw Fail{VC1CU_ERR_UNSUPPORTED, "search window does not fit in shared memory (local range too large)"};
     // the instantiation: the code this launch's passes can reach (the kCore* flags)
@@ -872,17 +955,45 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     if (learned)
         kind = kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra |
                ((P.me_quality == 2 && !P.fast_subpel) ? kCoreDefaultRefine : 0);
+    if (multi) kind = kCoreMulti;
     // windows so large that a second 4-warp block cannot fit: the wide-register build costs no occupancy
     if (!(kind & kCoreSeededOnly) && 2 * 4 * (size_t)wc.warp_bytes > (size_t)c->max_smem_sm) kind |= kCoreWide;
     const void* kern = core_kernel(kind);
+    // a launch shape chosen by vc1cu_autotune for this raster, search configuration and instantiation
+    int tuned_blocks = 0;
+    {
+        c->last_tune_key = tune_key(P, kind);
+        auto t = c->tuned.find(c->last_tune_key);
+        if (c->tune_force.first) {
+            warps = c->tune_force.first;
+            tuned_blocks = c->tune_force.second;
+        } else if (t != c->tuned.end()) {
+            warps = t->second.first;
+            tuned_blocks = t->second.second;
+        }
+        if ((size_t)warps * wc.warp_bytes > (size_t)c->max_smem) throw Fail{VC1CU_ERR_ARG, "tuned warps do not fit"};
+        smem = (size_t)warps * wc.warp_bytes;
+    }
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem), "occupancy");
     per_sm = std::max(per_sm, 1);
-    const long items = (long)n * mbs;
+    if (tuned_blocks > 0) per_sm = std::min(per_sm, tuned_blocks);
+    long items = 0;
+    for (int i = 0; i < n; ++i) items += (long)h[i].geom.mbw * h[i].geom.mbh;
     const long need = (items + warps - 1) / warps;
     const int grid = (int)std::max(1L, std::min<long>((long)per_sm * c->sm_count, need));
-    if (++c->epoch == 0) c->epoch = 1;
+    uint32_t epoch = 0;
+    if (c->capturing) {
+        // a replayed graph cannot count epochs: the flags restart from zero at every launch
+        epoch = 0xFFFFFFFFu;
+        for (int i = 0; i < n; ++i)
+            ck(cudaMemsetAsync(h[i].out.done, 0, sizeof(uint32_t) * h[i].geom.mbw * h[i].geom.mbh, c->stream),
+               "cudaMemsetAsync(done flags)");
+    } else {
+        if (++c->epoch == 0 || c->epoch == 0xFFFFFFFFu) c->epoch = 1;
+        epoch = c->epoch;
+    }
     // only the work counter restarts: an error (and its abort flag) stays until check_status reports it
     ck(cudaMemsetAsync(reinterpret_cast<char*>(c->d_status) + offsetof(LaunchStatus, queue), 0, sizeof(unsigned int),
                        c->stream),
@@ -890,11 +1001,16 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     {
         Timer tm(c, kCore);
         unsigned nitems = 0;
-        const uint32_t* items = work_items(c, P.mbw, P.mbh, level, nitems);
+        std::vector<int> mbw(n), mbh(n);
+        for (int i = 0; i < n; ++i) {
+            mbw[i] = h[i].geom.mbw;
+            mbh[i] = h[i].geom.mbh;
+        }
+        const uint32_t* items = work_items(c, mbw, mbh, level, nitems);
         P.wait_log2 = c->wait_log2;
         P.withhold = c->withhold_next;
         c->withhold_next = 0xFFFFFFFFu;
-        ck(launch_core(kind, grid, 32 * warps, smem, c->stream, P, c->d_passes, n, items, nitems, wc, c->epoch,
+        ck(launch_core(kind, grid, 32 * warps, smem, c->stream, P, c->d_passes, n, items, nitems, wc, epoch,
                        c->d_status),
            "core_pass_kernel launch");
         tm.stop(1);
@@ -1024,6 +1140,17 @@ int launch_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes,
 // Records one event after the work the current call enqueued and hands it to every slot the
 // call wrote.
 void stamp_written(vc1cu_ctx* c) {
+    if (c->capturing) {
+        // the graph's launches stamp these slots (vc1cu_graph_launch)
+        auto add = [](std::vector<int>& to, std::vector<int>& from) {
+            to.insert(to.end(), from.begin(), from.end());
+            from.clear();
+        };
+        add(c->capture_results, c->dirty_results);
+        add(c->capture_bresults, c->dirty_bresults);
+        add(c->capture_frames, c->used_frames);
+        return;
+    }
     if (c->dirty_results.empty() && c->dirty_bresults.empty() && c->used_frames.empty()) return;
     auto w = std::make_shared<Written>();
     ck(cudaEventCreateWithFlags(&w->e, cudaEventDisableTiming), "cudaEventCreate(slot)");
@@ -1043,6 +1170,21 @@ void stamp_written(vc1cu_ctx* c) {
     c->dirty_results.clear();
     c->dirty_bresults.clear();
     c->used_frames.clear();
+}
+
+// Ends an open capture after a failed call and drops what it held, so the stream is usable again.
+void abort_capture(vc1cu_ctx* c) {
+    if (!c || !c->capturing) return;
+    c->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    for (void* h : c->capture_hold) cudaFreeHost(h);
+    c->capture_hold.clear();
+    c->capture_results.clear();
+    c->capture_bresults.clear();
+    c->capture_frames.clear();
 }
 
 // Orders the read stream after the work that last wrote a slot (after everything enqueued so far
@@ -1592,6 +1734,11 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_lr) cudaFree(c->d_lr);
     if (c->d_scratch) cudaFree(c->d_scratch);
     if (c->d_synth) cudaFree(c->d_synth);
+    for (auto& kv : c->graphs) {
+        cudaGraphExecDestroy(kv.second.exec);
+        cudaGraphDestroy(kv.second.g);
+        for (void* h : kv.second.hold) cudaFreeHost(h);
+    }
     for (auto& kv : c->items) cudaFree(kv.second.first);
     if (c->h_read) cudaFreeHost(c->h_read);
     for (auto& b : c->staging_ring) {
@@ -1824,6 +1971,142 @@ int vc1cu_core_passes(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* pas
             if (passes[i].out_slot < 0 || passes[i].out_slot >= kMaxSlot || passes[i].seed_slot >= kMaxSlot)
                 throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
         return launch_passes(c, p, passes, n);
+    });
+}
+
+int vc1cu_core_passes_multi(vc1cu_ctx* c, const vc1cu_params* params, const vc1cu_pass* passes, int n) {
+    return guarded(c, [&]() -> int {
+        if (n <= 0 || !passes || !params) throw Fail{VC1CU_ERR_ARG, "invalid pass list"};
+        for (int i = 0; i < n; ++i) {
+            if (passes[i].out_slot < 0 || passes[i].out_slot >= kMaxSlot || passes[i].seed_slot >= kMaxSlot)
+                throw Fail{VC1CU_ERR_ARG, "result slot out of range"};
+            for (int j = 0; j < i; ++j)
+                if (passes[j].out_slot == passes[i].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
+        }
+        return launch_group(c, params, passes, n, false, nullptr, params);
+    });
+}
+
+int vc1cu_graph_begin(vc1cu_ctx* c) {
+    return guarded(c, [&]() -> int {
+        if (c->capturing) throw Fail{VC1CU_ERR_STATE, "a capture is already open on this context"};
+        if (c->timing) throw Fail{VC1CU_ERR_STATE, "turn per-launch timing off before capturing"};
+        stamp_written(c);
+        ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+        c->capturing = true;
+        c->capture_hold.clear();
+        c->capture_results.clear();
+        c->capture_bresults.clear();
+        c->capture_frames.clear();
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_graph_end(vc1cu_ctx* c, int* graph_id) {
+    return guarded(c, [&]() -> int {
+        if (!c->capturing) throw Fail{VC1CU_ERR_STATE, "no capture is open on this context"};
+        if (!graph_id) throw Fail{VC1CU_ERR_ARG, "null output"};
+        stamp_written(c);
+        vc1cu_ctx::Graph g;
+        c->capturing = false;
+        ck(cudaStreamEndCapture(c->stream, &g.g), "cudaStreamEndCapture");
+        g.hold.swap(c->capture_hold);
+        g.results.swap(c->capture_results);
+        g.bresults.swap(c->capture_bresults);
+        g.frames.swap(c->capture_frames);
+        const cudaError_t e = cudaGraphInstantiate(&g.exec, g.g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g.g);
+            for (void* h : g.hold) cudaFreeHost(h);
+            throw Fail{VC1CU_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+        }
+        const int id = c->graph_next++;
+        c->graphs[id] = std::move(g);
+        *graph_id = id;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_graph_launch(vc1cu_ctx* c, int graph_id) {
+    return guarded(c, [&]() -> int {
+        auto it = c->graphs.find(graph_id);
+        if (it == c->graphs.end()) throw Fail{VC1CU_ERR_ARG, "unknown graph id"};
+        if (c->capturing) throw Fail{VC1CU_ERR_STATE, "a capture is open on this context"};
+        // frames the graph reads may have uploads in flight on the upload stream
+        for (int id : it->second.frames) {
+            auto f = c->frames.find(id);
+            if (f != c->frames.end() && f->second.uploaded)
+                ck(cudaStreamWaitEvent(c->stream, f->second.uploaded, 0), "cudaStreamWaitEvent(upload)");
+        }
+        ck(cudaGraphLaunch(it->second.exec, c->stream), "cudaGraphLaunch");
+        c->dirty_results = it->second.results;
+        c->dirty_bresults = it->second.bresults;
+        c->used_frames = it->second.frames;
+        c->counters.dispatches++;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_graph_destroy(vc1cu_ctx* c, int graph_id) {
+    return guarded(c, [&]() -> int {
+        auto it = c->graphs.find(graph_id);
+        if (it == c->graphs.end()) throw Fail{VC1CU_ERR_ARG, "unknown graph id"};
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        cudaGraphExecDestroy(it->second.exec);
+        cudaGraphDestroy(it->second.g);
+        for (void* h : it->second.hold) cudaFreeHost(h);
+        c->graphs.erase(it);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_autotune(vc1cu_ctx* c, const vc1cu_params* params, const vc1cu_pass* passes, int n, int per_pass_params,
+                   int* warps_out, int* blocks_out, double* ms_out) {
+    return guarded(c, [&]() -> int {
+        if (n <= 0 || !passes || !params) throw Fail{VC1CU_ERR_ARG, "invalid pass list"};
+        if (c->capturing) throw Fail{VC1CU_ERR_STATE, "cannot tune during a capture"};
+        const vc1cu_params* pp = per_pass_params ? params : nullptr;
+        auto run = [&]() { launch_group(c, params, passes, n, false, nullptr, pp); };
+        cudaEvent_t a = take_event(c), b = take_event(c);
+        double best = -1.0;
+        std::pair<int, int> best_shape{0, 0};
+        std::vector<int> key;
+        const std::pair<int, int> shapes[] = {{4, 0}, {4, 1}, {4, 2}, {2, 0}, {2, 2}, {1, 0}, {1, 4}, {3, 0}};
+        for (const auto& s : shapes) {
+            c->tune_force = s;
+            try {
+                run();  // warm-up (and the shape's work-item table)
+                ck(cudaEventRecord(a, c->stream), "cudaEventRecord");
+                run();
+                run();
+                ck(cudaEventRecord(b, c->stream), "cudaEventRecord");
+                check_status(c);
+            } catch (const Fail& f) {
+                if (f.code != VC1CU_ERR_ARG) {  // a shape that does not fit is skipped, anything else fails
+                    c->tune_force = {0, 0};
+                    c->event_pool.push_back(a);
+                    c->event_pool.push_back(b);
+                    throw;
+                }
+                continue;
+            }
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+            key = c->last_tune_key;
+            if (best < 0.0 || ms < best) {
+                best = ms;
+                best_shape = s;
+            }
+        }
+        c->tune_force = {0, 0};
+        c->event_pool.push_back(a);
+        c->event_pool.push_back(b);
+        if (best < 0.0) throw Fail{VC1CU_ERR_UNSUPPORTED, "no launch shape fits"};
+        c->tuned[key] = best_shape;
+        if (warps_out) *warps_out = best_shape.first;
+        if (blocks_out) *blocks_out = best_shape.second;
+        if (ms_out) *ms_out = best / 2.0;
+        return VC1CU_OK;
     });
 }
 

@@ -2237,13 +2237,13 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 template <int KIND>
 __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned)) ? VC1CU_SEEDED_MIN_BLOCKS
                                                                 : ((KIND & kCoreWide) ? 1 : VC1CU_CORE_MIN_BLOCKS))
-    core_pass_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass, const uint32_t* items,
+    core_pass_kernel(const __grid_constant__ DevParams P0, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
     m.lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     carve(m.sm, (uint32_t)(warp * wc.warp_bytes), wc);
-    const int range = P.range, local_range = P.local_range;
+    const int range = P0.range, local_range = P0.local_range;  // one search configuration per launch
     for (;;) {
         unsigned item = 0;
         if (m.lane == 0) item = atomicAdd(&st->queue, 1u);
@@ -2253,6 +2253,8 @@ __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned))
         const int pi_idx = (int)(code >> 20);
         const int mbi = (int)(code & 0xFFFFFu);
         const PassDesc& d = passes[pi_idx];
+        // the picture geometry of this item (every pass of a kCoreMulti launch has its own)
+        const DevParams& P = (KIND & kCoreMulti) ? d.geom : P0;
         m.d = &d;
         m.mx = mbi % P.mbw;
         m.my = mbi / P.mbw;
@@ -2675,7 +2677,8 @@ cudaError_t launch_lr_index(const DevFrame& ref, int W, int H, uint64_t* out, cu
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreDefaultRefine | kCoreNoIntra)             \
     X(kCoreUnseededOnly | kCoreUmhLocal | kCoreNoMixed | kCoreWide | kCoreDefaultRefine | kCoreNoIntra)    \
     X(kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra)                                   \
-    X(kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra | kCoreDefaultRefine)
+    X(kCoreUnseededOnly | kCoreLearned | kCoreNoMixed | kCoreNoIntra | kCoreDefaultRefine)                 \
+    X(kCoreMulti) X(kCoreMulti | kCoreWide)
 
 const void* core_kernel(int kind) {
     switch (kind) {
@@ -2704,8 +2707,10 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
 
 // Picture totals of each pass (encoder_motion.cpp:428-441): integer sums, then the
 // reference's double expressions. One block per pass.
-__global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass) {
+__global__ void totals_kernel(const __grid_constant__ DevParams P0, const PassDesc* passes, int npass) {
     const PassDesc& d = passes[blockIdx.x];
+    const DevParams& P = d.geom;  // every pass carries its own geometry
+    (void)P0;
     const DevResult& o = d.out;
     const int mbs = P.mbw * P.mbh;
     uint64_t ts = 0, rs = 0, mv = 0, fr = 0, f4 = 0, in = 0, px = 0;

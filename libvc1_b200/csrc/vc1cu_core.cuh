@@ -59,6 +59,9 @@ struct PassDesc {
     const uint8_t* only;         // non-null: only the MBs flagged here are computed (the others
                                  // keep the slot's contents and just publish their done flag)
     DevResult out;
+    DevParams geom;              // this pass's picture geometry and configuration (read by the
+                                 // kCoreMulti instantiation and the totals; the others take the
+                                 // launch's parameter block)
 };
 constexpr int kLearnK = 4;       // candidates per macroblock of a learned pass
 constexpr int kLearnRw = 8;      // window radius of a learned pass around its best candidate
@@ -77,6 +80,8 @@ constexpr int kCoreDefaultRefine = 32;  // (with kCoreSeededOnly or kCoreUmhLoca
 constexpr int kCoreNoIntra = 64;        // (with kCoreDefaultRefine) no pass allows P-intra: no intra code
 constexpr int kCoreLearned = 128;       // (with kCoreUnseededOnly) the integer search is the learned
                                         // candidates' exact costs and a short descent about the best
+constexpr int kCoreMulti = 256;         // passes of pictures of different sizes in one launch: each
+                                        // work item takes its pass's own geometry
 constexpr int kCoreAny = 0;
 constexpr int kCoreSeeded = kCoreSeededOnly;
 

@@ -1,6 +1,7 @@
 """ctypes bindings of the two CPU checkers (see oracle/__init__.py)."""
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import os
 
@@ -367,6 +368,7 @@ class Reference:
                                           C.POINTER(i32), i32, i32]
         L.ref_bench_gop_multi.restype = u64
         self.p = p
+        self._recent = collections.deque(maxlen=8)
         self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
 
     def __del__(self):
@@ -379,7 +381,13 @@ class Reference:
         return RefFrame(self.lib, frame)
 
     def _f(self, fr):
-        return (fr if isinstance(fr, RefFrame) else self.frame(fr)).h
+        if isinstance(fr, RefFrame):
+            return fr.h
+        # a frame converted for this call: kept alive for the next few calls (the C++ side reads it
+        # during the call; freeing it as soon as its handle is taken would leave the handle dangling)
+        rf = self.frame(fr)
+        self._recent.append(rf)
+        return rf.h
 
     def mb_sad(self, cur, ref, mx, my, dx, dy, stride=1):
         return self.lib.ref_mb_sad(self.h, self._f(cur), self._f(ref), mx, my, dx, dy, stride)

@@ -19,10 +19,15 @@ pytestmark = pytest.mark.gpu
 _MSG = re.compile(r"pass (\d+) of its launch, macroblock (\d+), lanes still waiting 0x([0-9a-f]+)")
 
 
-def _dependents(mb, mbw):
-    """The macroblocks whose wait reads mb's flag, with the lane (bit) that waits for it:
-    lane 0 left, 1 top-left, 2 top, 3 top-right."""
-    return {mb + 1: 1 << 0, mb + mbw + 1: 1 << 1, mb + mbw: 1 << 2, mb + mbw - 1: 1 << 3}
+def _descends(mb, from_mb, mbw):
+    """Whether macroblock mb waits, directly or through other waits, on from_mb's flag: a
+    macroblock waits for its left, top-left, top and top-right neighbours, so the blocked region
+    is the rest of from_mb's row and, on each row below, everything right of a boundary that moves
+    one macroblock left per row. The first wait to give up can be any of them (each wait counts
+    its own polls)."""
+    x, y = mb % mbw, mb // mbw
+    fx, fy = from_mb % mbw, from_mb // mbw
+    return (y == fy and x > fx) or (y > fy and x >= fx - (y - fy))
 
 
 def test_withheld_done_flag_times_out_and_context_recovers(ctx, oracle):
@@ -43,8 +48,7 @@ def test_withheld_done_flag_times_out_and_context_recovers(ctx, oracle):
         assert m, str(e.value)
         assert int(m.group(1)) == 0
         waiting, mask = int(m.group(2)), int(m.group(3), 16)
-        deps = _dependents(withheld, mbw)
-        assert waiting in deps and mask & deps[waiting], (waiting, hex(mask))
+        assert mask and _descends(waiting, withheld, mbw), (waiting, hex(mask))
     finally:
         ctx.debug_withhold_publish(-1, -1)
         ctx.debug_set_wait_limit(24)
@@ -80,7 +84,7 @@ def test_withheld_seed_flag_in_one_launch_times_out(ctx, oracle):
         # the seeded pass's own macroblock waits for the seed (lane 0); the seed pass's
         # dependents, and the seeded pass's, wait behind it
         assert pas in (0, 1) and mask
-        assert waiting == withheld or waiting in _dependents(withheld, mbw), (pas, waiting, hex(mask))
+        assert waiting == withheld or _descends(waiting, withheld, mbw), (pas, waiting, hex(mask))
     finally:
         ctx.debug_withhold_publish(-1, -1)
         ctx.debug_set_wait_limit(24)
