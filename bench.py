@@ -237,6 +237,30 @@ class Runner:
                                  for j, m in enumerate((self.QPEL, self.BIL))])
         mark("B decisions")
 
+    def tune(self, b=0):
+        """The library's launch-shape autotuner on each of the step's launch kinds (unseeded
+        passes, seeded half-pel modes, seeded Mixed-MV, final passes); later launches of those
+        kinds use the fastest shape. Returns the shapes found."""
+        c, F = self.ctx, lambda f: self.fid(f, b)
+        pics = [(F(t), F(r), pq) for t, r, pq in self.pics]
+        bpics = [(F(t), F(past), F(fut), pq) for t, past, fut, _n, _d, pq, _a in self.bpics]
+        groups = {
+            "unseeded": [(t, r, self.QPEL, 0, -1, self.seed_slot(i, b), pq) for i, (t, r, pq) in enumerate(pics)] +
+                        [(t, ref, m, 0, -1, self.bpass_slot(k, m == self.BIL, ref == fut, b), pq)
+                         for k, (t, past, fut, pq) in enumerate(bpics) for m in (self.QPEL, self.BIL) for ref in (past, fut)],
+            "seeded_hpel": [(t, r, m, 0, self.seed_slot(i, b), self.mode_slot(i, m, b), pq)
+                            for i, (t, r, pq) in enumerate(pics) for m in self.modes[:2]],
+            "seeded_mixed": [(t, r, self.MIXED, 0, self.seed_slot(i, b), self.mode_slot(i, self.MIXED, b), pq)
+                             for i, (t, r, pq) in enumerate(pics)],
+            "final": [(t, r, self.MIXED, 1, self.mode_slot(i, self.MIXED, b), self.final_slot(i, b), pq)
+                      for i, (t, r, pq) in enumerate(pics)],
+        }
+        out = {}
+        for name, passes in groups.items():
+            w, blk, ms = c.autotune(self.p0, passes)
+            out[name] = {"warps_per_block": w, "blocks_per_sm": blk or "occupancy limit", "ms": round(ms, 3)}
+        return out
+
     def finish(self, mark=None, b=0):
         """The fade estimate analyze_p_picture runs on its final pass when fade compensation is on
         (the default; encoder_motion.cpp:570-573); it waits for the step's device work."""
@@ -345,6 +369,86 @@ def learned_leg(ctx, torch, l2, steps, warmup, pairs=16):
             "cost_gap_definition": "per pair (sum of the chosen vectors' exact SAD, learned - plain) / plain"}
 
 
+def batched_clips(n_odd_seed=7):
+    """The batched workload's 48 clips: (coded width, height, display width, height, seed):
+    16 at 640x360, 16 at 1280x720, 8 at 1920x1080 and 8 of odd display sizes with widths in
+    322..1918 and heights in 242..1078 (coded raster rounded up to even)."""
+    rng = np.random.default_rng(n_odd_seed)
+    out = [(640, 360, 640, 360)] * 16 + [(1280, 720, 1280, 720)] * 16 + [(1920, 1080, 1920, 1080)] * 8
+    for _ in range(8):
+        dw, dh = int(rng.integers(161, 960)) * 2 + 1, int(rng.integers(121, 540)) * 2 + 1  # odd, 323..1919
+        dw, dh = min(dw, 1917), min(dh, 1077)
+        out.append((dw + 1, dh + 1, dw, dh))
+    return [c + (500 + k,) for k, c in enumerate(out)]
+
+
+def batched_leg(ctx, torch, reps, frames=31):
+    """The batched plain form: 48 clips of uneven size, every clip's P picture of a frame step
+    analysed (quarter-pel seed pass, three seeded mode passes, final Mixed-MV pass with P-intra,
+    search range 32, QP 8 uniform) in ONE persistent launch per frame step; the 30 frame steps of
+    the GOP captured as one CUDA graph and replayed; the launch shape chosen by the autotuner.
+    Bit-exactness per clip is what tests/test_gpu_multiclip.py checks."""
+    from libvc1_b200 import synth
+    from libvc1_b200.abi import make_params
+
+    clips = batched_clips()
+    params, mbs_step = [], 0
+    for k, (w, h, dw, dh, seed) in enumerate(clips):
+        cfg = synth.make_cfg(w, h, frames, seed, global_px=16.0, n_objects=4, obj_vel=3.0, sigma=2.0)
+        for t0 in range(0, frames, 16):
+            ctx.synth_frames(cfg, t0, min(16, frames - t0), 200 + 64 * k + t0)
+        params.append(make_params(w, h, display_width=dw, display_height=dh, search_range=32, local_search_range=32,
+                                  pqindex=8))
+        mbs_step += ((w + 15) // 16) * ((h + 15) // 16)
+
+    def step(t):
+        ctx.core_passes_multi(*_batched_step_args(params, clips, t))
+
+    ext = torch.cuda.ExternalStream(ctx.stream_handle())
+    step(1)  # builds the launch's tables and slots
+    ctx.synchronize()
+    warps, blocks, tune_ms = ctx.autotune(*_batched_step_args(params, clips))
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        fn()
+        b.record(ext)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    direct_ms = timed(lambda: [step(t) for t in range(1, frames)])
+    ctx.graph_begin()
+    for t in range(1, frames):
+        step(t)
+    g = ctx.graph_end()
+    ctx.graph_launch(g)  # warm-up replay
+    ctx.synchronize()
+    graph_ms = sum(timed(lambda: ctx.graph_launch(g)) for _ in range(reps)) / reps
+    ctx.graph_destroy(g)
+    mb_gop = mbs_step * (frames - 1)
+    return {"workload": "48 clips (16x 640x360, 16x 1280x720, 8x 1920x1080, 8 odd sizes 323-1917 x 243-1077), "
+                        f"{frames - 1} P frames each, global +-16 px; P analysis (5 passes) per picture, range 32, QP 8",
+            "mb_per_gop": mb_gop, "launches_per_frame_step": 1,
+            "mb_per_s_graph": round(mb_gop / (graph_ms * 1e-3), 1), "mb_per_s_direct": round(mb_gop / (direct_ms * 1e-3), 1),
+            "ms_per_gop_graph": round(graph_ms, 2), "ms_per_gop_direct": round(direct_ms, 2),
+            "autotuned_shape": {"warps_per_block": warps, "blocks_per_sm": blocks or "occupancy limit",
+                                "ms_per_launch": round(tune_ms, 3)}}
+
+
+def _batched_step_args(params, clips, t=1):
+    from libvc1_b200.abi import MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED, MV_QPEL
+
+    plist, passes = [], []
+    for k in range(len(clips)):
+        cur, ref, base = 200 + 64 * k + t, 200 + 64 * k + t - 1, 2000 + 5 * k
+        plist += [params[k]] * 5
+        passes += [(cur, ref, MV_QPEL, 0, -1, base)]
+        passes += [(cur, ref, m, 0, base, base + 1 + j) for j, m in enumerate((MV_HPEL, MV_HPEL_BILINEAR, MV_MIXED))]
+        passes += [(cur, ref, MV_MIXED, 1, base + 3, base + 4)]
+    return plist, passes
+
+
 def flush_l2(torch, buf):
     buf.zero_()
     torch.cuda.synchronize()
@@ -367,6 +471,9 @@ def run_ours(args, rank, world, device):
     l2 = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     for _ in range(args.warmup):
         run.step()
+    ctx.synchronize()
+    shapes = None if args.no_autotune else run.tune()
+    run.step()
     ctx.synchronize()
     # ---- value: resident inputs, device time per step, L2 flushed between steps
     ctx.reset_counters()
@@ -485,11 +592,15 @@ def run_ours(args, rank, world, device):
     core_ms = timing["core_ms"]
     achieved_ops = ops_step * args.steps / (core_ms * 1e-3) if core_ms > 0 else 0.0
     peak_ops = ctx.measure_int32_peak()
+    peak_fp64 = ctx.measure_fp64_peak()
     xform_ms = timing["xform_ms"]
     xform_flops = n * MBS * XFORM_FLOPS_PER_MB * args.steps
     learned = None
     if not args.no_learned and world == 1:
         learned = learned_leg(ctx, torch, l2, args.steps, args.warmup)
+    batched = None
+    if not args.no_batched and world == 1:
+        batched = batched_leg(ctx, torch, reps=min(args.steps, 2))
     out = None
     if rank == 0:
         cpu = cpu_baseline(args, clip) if (world == 1 and not args.no_cpu_baseline) else None
@@ -498,10 +609,7 @@ def run_ours(args, rank, world, device):
             "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32 (integer SAD/SATD/interpolation) + f64 transform",
             "data": "synthetic (seeded value-noise clip with the 1080p config's motion, zoom, objects and noise)",
-            "config": {"workload": WORKLOAD,
-                       "mb_per_step_per_gpu": mbs_per_step, "p_pictures": len(run.pics), "b_pictures": len(run.bpics),
-                       "core_passes_per_step": 5 * len(run.pics) + 4 * len(run.bpics),
-                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "config": step_config(len(run.pics), len(run.bpics), world),
             "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
                     "h2d_bytes_per_step": len(run.frames) * run.frame_bytes,
                     "d2h_bytes_per_step": run.result_bytes()},
@@ -516,6 +624,7 @@ def run_ours(args, rank, world, device):
                          "traffic": round(CORE_DRAM_BYTES_PER_LAUNCH) if args.gops is None else None,
                          "traffic_unit": "DRAM bytes per launch (ncu, first GOP scaled by macroblocks)"},
             "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage_ms.items()},
+            "autotuned_shapes": shapes,
             "pass_mb_per_s": {
                 "unseeded (P seed + B forward/backward)": round((len(run.pics) + 4 * len(run.bpics)) * MBS * args.steps
                                                               / (stage_ms["unseeded passes"] * 1e-3), 1),
@@ -524,12 +633,12 @@ def run_ours(args, rank, world, device):
             } if stage_ms else None,
             "kernel_ms_per_step": {k: round(timing[k] / args.steps, 3)
                                    for k in ("core_ms", "global_ms", "totals_ms", "mc_ms", "xform_ms", "b_ms", "ic_ms")},
-            "xform_roofline": {"bound": "fp64", "achieved_gflops": round(xform_flops / (xform_ms * 1e-3) / 1e9, 1)
-                               if xform_ms > 0 else None},
+            "xform_roofline": xform_roofline(xform_flops, xform_ms, peak_fp64),
             "clocks": clocks,
             "cpu_baseline": cpu,
             "mpixel_per_s": round(value * 256 / 1e6, 1),
             "learned": learned,
+            "batched": batched,
         }
     ctx.close()
     return out
@@ -555,9 +664,37 @@ def reference_jobs(clip):
     return any_ref, pjobs, bjobs
 
 
-REF_SAMPLE = ("every picture of the clip once (one step): the 20 P pictures (analyze_p_picture + choose_transform_mb of "
-              "the chosen prediction), then the 35 B pictures (analyze_b_picture against the P analyses), one picture "
-              "per thread, SIMD dispatch auto")
+REF_SAMPLE = ("every picture of the clip once (one step), the same work as the GPU arm on the reference's own "
+              "functions: per P picture the five analyze_p_picture_core passes (qpel seed, hpel, bilinear, Mixed-MV, "
+              "final Mixed-MV + P-intra), estimate_intensity_comp, the prediction and quantize_inter_part of all four "
+              "transform types; per B picture analyze_b_picture_mode in qpel and bilinear mode; P and B pictures in one "
+              "job pool (a B job waits for its anchor), one picture per thread, SIMD dispatch auto")
+REF_FULL_RD = ("the reference's whole picture analysis instead: analyze_p_picture (sampled mode RD, final pass in the "
+               "chosen mode) + choose_transform_mb RD of every MB, then analyze_b_picture (both modes + sampled B mode "
+               "RD), P phase then B phase")
+
+
+def xform_roofline(flops, ms, peak):
+    """The transform kernel against the FP64 peak measured live (FMA kernel, an FMA counted as
+    two flops). The transform rounds every product and sum separately (no contraction, for the
+    reference's bits), so its instruction-rate ceiling is half the FMA peak."""
+    if not ms or ms <= 0:
+        return None
+    achieved = flops / (ms * 1e-3)
+    return {"bound": "fp64", "kernel": "xform_kernel", "achieved_gflops": round(achieved / 1e9, 1),
+            "peak_gflops": round(peak / 1e9, 1) if peak else None,
+            "frac": round(achieved / peak, 4) if peak else None,
+            "frac_of_unfused_ceiling": round(2 * achieved / peak, 4) if peak else None,
+            "peak_source": "measured live: vc1cu_measure_fp64_peak FMA kernel"}
+
+
+def step_config(n_p, n_b, world):
+    """The workload's config block, the same in both arms' lines."""
+    return {"workload": WORKLOAD, "mb_per_step_per_gpu": (n_p + n_b) * MBS, "p_pictures": n_p, "b_pictures": n_b,
+            "core_passes_per_step": 5 * n_p + 4 * n_b,
+            "l2": "inputs larger than L2 (60 frames x 3.1 MB read per step); the GPU arm also flushes L2 (256 MB "
+                  "write) between timed steps",
+            "parallelism": f"replicas x{world}"}
 
 
 def cpu_baseline(args, clip):
@@ -572,9 +709,12 @@ def cpu_baseline(args, clip):
     cores = os.cpu_count() or 1
     anyref, pjobs, bjobs = reference_jobs(clip)
     threads = min(len(pjobs) + len(bjobs), cores)
-    ns = anyref.bench_gop_multi(pjobs, bjobs, threads)
+    ns = anyref.bench_gop_same(pjobs, bjobs, threads)
     out = {"value": round((len(pjobs) + len(bjobs)) * MBS / (ns * 1e-9), 1), "unit": UNIT, "cores": threads,
            "kind": "reference", "sample": REF_SAMPLE}
+    ns_rd = anyref.bench_gop_multi(pjobs, bjobs, threads)
+    out["full_rd"] = {"value": round((len(pjobs) + len(bjobs)) * MBS / (ns_rd * 1e-9), 1), "unit": UNIT,
+                      "sample": REF_FULL_RD}
     # one core: the first P picture and the first B picture anchored on it, with the SIMD dispatch
     # on and with the scalar path (the reference's parity configuration)
     from oracle import Reference
@@ -584,7 +724,7 @@ def cpu_baseline(args, clip):
         R = Reference(params(pjobs[0][0].p.pqindex), simd_auto=simd)
         pj = [(R, pjobs[0][1], pjobs[0][2])]
         bj = [(R,) + tuple(bjobs[0][1:])]
-        ns1 = R.bench_gop_multi(pj, bj, 1)
+        ns1 = R.bench_gop_same(pj, bj, 1)
         one[name] = round(2 * MBS / (ns1 * 1e-9), 1)
     out["one_thread"] = dict(one, sample="P picture 3 and B picture 1 of the clip on one host thread")
     return out
@@ -605,7 +745,7 @@ def run_reference(args, rank, world):
     threads = min(len(pjobs) + len(bjobs), cores)
     per = []
     for i in range(args.warmup + args.steps):
-        ns = anyref.bench_gop_multi(pjobs, bjobs, threads)
+        ns = anyref.bench_gop_same(pjobs, bjobs, threads)
         if i >= args.warmup:
             per.append(ns * 1e-9)
     value = (len(pjobs) + len(bjobs)) * MBS * len(per) / sum(per)
@@ -613,7 +753,7 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(per) / len(per), 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 + f64 (CPU)",
             "data": "synthetic (same seeded clip as ours)",
-            "config": {"workload": WORKLOAD},
+            "config": step_config(len(pjobs), len(bjobs), world),
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": REF_SAMPLE},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -628,6 +768,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-clip leg")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -200,6 +200,9 @@ void* vc1cu_stream(const vc1cu_ctx* ctx);
 /* Measures this device's 32-bit integer lane-op throughput (ops/s) with a dependency-free
  * add/xor kernel: the denominator of the analysis kernels' roofline. */
 int vc1cu_measure_int32_peak(vc1cu_ctx* ctx, double* ops_per_second);
+/* Measures this device's FP64 throughput (flops/s, a fused multiply-add counted as two) with a
+ * dependency-free FMA kernel: the denominator of the transform kernel's roofline. */
+int vc1cu_measure_fp64_peak(vc1cu_ctx* ctx, double* flops_per_second);
 
 /* Fills the defaults of vc1_param_default for a width x height raster. */
 void vc1cu_params_default(vc1cu_params* p, int width, int height);

@@ -33,7 +33,7 @@ EXPORTS = (
     "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
-    "vc1cu_measure_int32_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
+    "vc1cu_measure_int32_peak", "vc1cu_measure_fp64_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
@@ -115,6 +115,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_stream.argtypes = [vp]
     L.vc1cu_stream.restype = vp
     L.vc1cu_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    L.vc1cu_measure_fp64_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
@@ -248,6 +249,12 @@ class CudaComputeContext:
         """32-bit integer lane-ops per second of this device (calibration kernel)."""
         v = C.c_double()
         self._check(self._L.vc1cu_measure_int32_peak(self._h, C.byref(v)))
+        return v.value
+
+    def measure_fp64_peak(self) -> float:
+        """FP64 flops per second of this device (FMA calibration kernel, an FMA counted as two)."""
+        v = C.c_double()
+        self._check(self._L.vc1cu_measure_fp64_peak(self._h, C.byref(v)))
         return v.value
 
     def stream_handle(self) -> int:

@@ -34,6 +34,8 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
                         const PassDesc* passes, int npass, const uint32_t* items, unsigned nitems, const WinCfg& wc,
                         uint32_t epoch, LaunchStatus* st);
 __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
+cudaError_t launch_learned_merge(const DevResult& dst, const DevResult& src, const uint8_t* only, int mbs,
+                                 cudaStream_t s);
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
 size_t gstate_bytes();
@@ -48,6 +50,7 @@ void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred,
 void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int n, unsigned long long* out,
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
+double measure_fp64_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
 cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  cudaStream_t s);
@@ -88,7 +91,9 @@ constexpr int kInternalFwd = kMaxSlot + 3;   // the forward / backward core pass
 constexpr int kInternalBwd = kMaxSlot + 4;   // of vc1cu_analyze_b_picture
 constexpr int kInternalAnchor = kMaxSlot + 5;
 constexpr int kInternalIc = kMaxSlot + 6;     // MV field of vc1cu_estimate_intensity_comp
-constexpr int kInternalLast = kInternalIc;
+constexpr int kInternalLpFb = kMaxSlot + 7;   // + i: the fallback results of vc1cu_lp_analyze's pass i
+constexpr int kMaxLpPasses = 256;
+constexpr int kInternalLast = kInternalLpFb + kMaxLpPasses - 1;
 constexpr int kInternalB = kMaxSlot + 1;     // B-result slot of vc1cu_analyze_b_picture
 constexpr int kInternalFrame = kMaxSlot + 1; // frame slot of the scene score's compensated reference
 constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate limit
@@ -96,6 +101,7 @@ constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate
 #define VC1CU_SEEDED_MIXED_RW 8
 #endif
 constexpr int kSeededMixedRw = VC1CU_SEEDED_MIXED_RW;  // window radius of seeded Mixed-MV launches
+constexpr int kMinUnseededRw = 24;  // smallest window radius a tuned unseeded launch shrinks to
 
 struct Status {
     int code;
@@ -701,6 +707,7 @@ struct PassExtra {
     const uint8_t* only = nullptr;
     const int2* hint = nullptr;
     const unsigned long long* hint_sad = nullptr;  // the frame SAD at the hint (global_full_sad)
+    const DevResult* nb = nullptr;  // no-wait pass: read the neighbours from this finished field
 };
 
 // The search configuration every pass of one launch shares (the kernel's window, bitsets and
@@ -720,7 +727,8 @@ std::vector<int> tune_key(const DevParams& P, int kind) { return {P.W, P.H, P.ra
 
 // per_pass: null, or n parameter blocks (pictures of different sizes in one kCoreMulti launch).
 int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, int n, bool globals_ready = false,
-                 const PassExtra* extra = nullptr, const vc1cu_params* per_pass = nullptr) {
+                 const PassExtra* extra = nullptr, const vc1cu_params* per_pass = nullptr,
+                 std::vector<PassDesc>* descs = nullptr) {
     DevParams P;
     std::string why;
     int rc = make_dev_params(per_pass ? per_pass : p, P, why);
@@ -785,6 +793,8 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         h[i].cands = extra ? extra[i].cands : nullptr;
         h[i].fallback = extra ? extra[i].fallback : nullptr;
         h[i].only = extra ? extra[i].only : nullptr;
+        h[i].no_wait = (extra && extra[i].nb) ? 1 : 0;
+        if (h[i].no_wait) h[i].nb = *extra[i].nb;
         learned |= h[i].cands != nullptr;
     }
     if (learned) {
@@ -971,7 +981,17 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
             warps = t->second.first;
             tuned_blocks = t->second.second;
         }
-        if ((size_t)warps * wc.warp_bytes > (size_t)c->max_smem) throw Fail{VC1CU_ERR_ARG, "tuned warps do not fit"};
+        // a wider block of unseeded passes: their windows shrink until `warps` of them fit; a
+        // candidate outside its window reads the frame in global memory, at the same result
+        if ((kind & kCoreWide) && any_unseeded && !learned)
+            while ((size_t)warps * wc.warp_bytes > (size_t)c->max_smem && wc.rw > kMinUnseededRw) {
+                --wc.rw;
+                wc.wh = 16 + 2 * wc.rw + 3;
+                wc.wp = (wc.wh + 15 + 15) & ~15;
+                wc.warp_bytes = warp_bytes_for_host(wc);
+            }
+        if (warps < 1 || warps > ((kind & kCoreWide) ? 8 : 4) || (size_t)warps * wc.warp_bytes > (size_t)c->max_smem)
+            throw Fail{VC1CU_ERR_ARG, "tuned warps do not fit this instantiation"};
         smem = (size_t)warps * wc.warp_bytes;
     }
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
@@ -1023,6 +1043,7 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
     }
     c->counters.dispatches++;
     c->counters.macroblocks_analysed += (uint64_t)items;
+    if (descs) *descs = h;
     return VC1CU_OK;
 }
 
@@ -1829,6 +1850,16 @@ int vc1cu_measure_int32_peak(vc1cu_ctx* c, double* ops_per_second) {
     });
 }
 
+int vc1cu_measure_fp64_peak(vc1cu_ctx* c, double* flops_per_second) {
+    return guarded(c, [&]() -> int {
+        if (!flops_per_second) throw Fail{VC1CU_ERR_ARG, "null output"};
+        *flops_per_second = measure_fp64_peak(c->stream, c->sm_count);
+        ck(cudaGetLastError(), "fp64_peak_kernel");
+        if (*flops_per_second <= 0.0) throw Fail{VC1CU_ERR_CUDA, "calibration kernel failed"};
+        return VC1CU_OK;
+    });
+}
+
 int vc1cu_score_motion_batch(vc1cu_ctx* c, const uint8_t* cur, const uint8_t* ref, int width, int height, int x0, int y0,
                              int bw, int bh, int sample_stride, int bilinear, int rnd, int metric,
                              const vc1cu_mv* candidates, size_t n, uint64_t* costs) {
@@ -2071,7 +2102,10 @@ int vc1cu_autotune(vc1cu_ctx* c, const vc1cu_params* params, const vc1cu_pass* p
         double best = -1.0;
         std::pair<int, int> best_shape{0, 0};
         std::vector<int> key;
-        const std::pair<int, int> shapes[] = {{4, 0}, {4, 1}, {4, 2}, {2, 0}, {2, 2}, {1, 0}, {1, 4}, {3, 0}};
+        // warps (macroblocks) per block and blocks per SM (0: as many as fit); shapes that do not fit
+        // the launch's instantiation or shared memory are skipped
+        const std::pair<int, int> shapes[] = {{4, 0}, {4, 1}, {4, 2}, {2, 0}, {2, 2}, {1, 0}, {1, 4}, {3, 0},
+                                              {5, 1}, {6, 1}, {7, 1}, {8, 1}};
         for (const auto& s : shapes) {
             c->tune_force = s;
             try {
@@ -2906,8 +2940,9 @@ int vc1cu_lp_create(vc1cu_ctx* c, int width, int height, int search_range, int c
             n->xb = lp_alloc<void>(n.get(), 2 * n->xelems * max_batch, "cudaMalloc(lp batch)");
             n->bhint = lp_alloc<int2>(n.get(), sizeof(int2) * max_batch, "cudaMalloc(lp batch)");
             n->blabel = lp_alloc<int2>(n.get(), sizeof(int2) * mbs * max_batch, "cudaMalloc(lp batch)");
-            n->cur4 = lp_alloc<uint8_t>(n.get(), px, "cudaMalloc(lp quarter-res)");
-            n->ref4 = lp_alloc<uint8_t>(n.get(), px, "cudaMalloc(lp quarter-res)");
+            // quarter-resolution pictures, then their 1/16-resolution level (the hint search's)
+            n->cur4 = lp_alloc<uint8_t>(n.get(), px + mbs, "cudaMalloc(lp quarter-res)");
+            n->ref4 = lp_alloc<uint8_t>(n.get(), px + mbs, "cudaMalloc(lp quarter-res)");
             n->hs = lp_alloc<unsigned long long>(n.get(), 8 * (65 * 65 + 32), "cudaMalloc(lp hint search)");
             n->loss = lp_alloc<float>(n.get(), 16, "cudaMalloc(lp loss)");
             n->err = lp_alloc<int>(n.get(), 16, "cudaMalloc(lp err)");
@@ -2976,7 +3011,7 @@ int vc1cu_lp_prepare(vc1cu_lp* n, int cur_id, int ref_id, int sample) {
         ck(lp_launch_features(rf.y, rf.pitch_y, n->g, n->cur4, n->ref4, n->hints + sample,
                               static_cast<uint16_t*>(n->x0) + n->xelems * sample, c->stream),
            "lp features");
-        c->counters.kernel_launches += 6;
+        c->counters.kernel_launches += 8;
         return VC1CU_OK;
     });
 }
@@ -3104,17 +3139,37 @@ int vc1cu_lp_analyze(vc1cu_lp* n, const vc1cu_params* p, const vc1cu_lp_pass* pa
         for (int i = 0; i < count; ++i)
             for (int j = 0; j < i; ++j)
                 if (q[i].out_slot == q[j].out_slot) throw Fail{VC1CU_ERR_ARG, "two passes write one result slot"};
-        launch_group(c, p, q.data(), count, true, ex.data());
-        if (fallback) {
-            // the macroblocks whose best learned match is not good: the plain search, in
-            // wavefront order, over the learned field
-            for (int i = 0; i < count; ++i) {
-                ex[i].only = ex[i].fallback;
-                ex[i].cands = nullptr;
-                ex[i].fallback = nullptr;
-            }
-            launch_group(c, p, q.data(), count, true, ex.data());
+        if (fallback && count > kMaxLpPasses) throw Fail{VC1CU_ERR_ARG, "too many learned passes in one call"};
+        std::vector<PassDesc> learned;
+        launch_group(c, p, q.data(), count, true, ex.data(), nullptr, &learned);
+        if (!fallback) return VC1CU_OK;
+        // The macroblocks whose best learned match is not good: the plain search, all of them at
+        // once, with the finished learned field as their neighbourhood, into scratch slots; then
+        // their results replace the learned ones and the totals are taken again.
+        std::vector<vc1cu_pass> qb(q);
+        std::vector<PassExtra> eb(count);
+        std::vector<DevResult> snap(count);
+        for (int i = 0; i < count; ++i) {
+            snap[i] = learned[i].out;
+            qb[i].out_slot = kInternalLpFb + i;
+            eb[i].only = ex[i].fallback;
+            eb[i].hint = ex[i].hint;
+            eb[i].hint_sad = ex[i].hint_sad;
+            eb[i].nb = &snap[i];
         }
+        launch_group(c, p, qb.data(), count, true, eb.data());
+        for (int i = 0; i < count; ++i) {
+            const ResultSlot& s = result_slot(c, kInternalLpFb + i, (int)mbs, false);
+            ck(launch_learned_merge(learned[i].out, s.r, ex[i].fallback, (int)mbs, c->stream), "learned merge launch");
+            c->counters.kernel_launches++;
+        }
+        void* hp = staging(c, sizeof(PassDesc) * count);
+        std::memcpy(hp, learned.data(), sizeof(PassDesc) * count);
+        ck(cudaMemcpyAsync(c->d_passes, hp, sizeof(PassDesc) * count, cudaMemcpyHostToDevice, c->stream),
+           "cudaMemcpyAsync(pass descriptors)");
+        staging_mark(c);
+        totals_kernel<<<count, 256, 0, c->stream>>>(learned[0].geom, c->d_passes, count);
+        ck(cudaGetLastError(), "totals_kernel launch");
         return VC1CU_OK;
     });
 }

@@ -306,6 +306,46 @@ __device__ __forceinline__ uint32_t sad_packed(uint32_t cur_off, uint32_t cur2_o
     return acc;
 }
 
+// 16 bytes of a frame row starting at `p` (any alignment), as four little-endian words: five
+// aligned word loads through the read-only path and funnel shifts. The fifth word can reach up
+// to three bytes past the row's 16, which stay inside the frame's allocation (the next row, or
+// the chroma planes after the last luma row).
+__device__ __forceinline__ void glob_load16(const uint8_t* p, uint32_t r[4]) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+    const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8;
+    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+    const uint32_t w4 = sh ? __ldg(w + 4) : 0u;
+    r[0] = __funnelshift_r(w0, w1, sh);
+    r[1] = __funnelshift_r(w1, w2, sh);
+    r[2] = __funnelshift_r(w2, w3, sh);
+    r[3] = __funnelshift_r(w3, w4, sh);
+}
+
+// mb_sad of a full 16x16 MB whose reference block lies inside the frame, read from global
+// memory (the frames stay in L2) with the same packed byte SADs as sad_packed.
+template <int STRIDE>
+__device__ __forceinline__ uint32_t sad_packed_glob(uint32_t cur_off, uint32_t cur2_off, uint32_t cur4_off,
+                                                    const uint8_t* ref, int pitch) {
+    uint32_t acc = 0;
+    const uint32_t c = cur_off >> 2, c2 = cur2_off >> 2, c4 = cur4_off >> 2;
+#pragma unroll 4
+    for (int y = 0; y < 16; y += STRIDE) {
+        uint32_t r[4];
+        glob_load16(ref + (size_t)y * pitch, r);
+        if (STRIDE == 1) {
+            acc += __vsadu4(r[0], g_smem32[c + y * 4 + 0]) + __vsadu4(r[1], g_smem32[c + y * 4 + 1]) +
+                   __vsadu4(r[2], g_smem32[c + y * 4 + 2]) + __vsadu4(r[3], g_smem32[c + y * 4 + 3]);
+        } else if (STRIDE == 2) {
+            acc += __vsadu4(__byte_perm(r[0], r[1], 0x6420), g_smem32[c2 + y * 2 + 0]) +
+                   __vsadu4(__byte_perm(r[2], r[3], 0x6420), g_smem32[c2 + y * 2 + 1]);
+        } else {
+            const uint32_t e = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+            acc += __vsadu4(e, g_smem32[c4 + y]);
+        }
+    }
+    return acc;
+}
+
 // ---- integer SAD of the 16x16 MB, mb_sad (encoder_motion.cpp:2197-2285) ----------------
 
 template <int STRIDE, class S>
@@ -388,6 +428,12 @@ __device__ __noinline__ uint64_t mb_sad_core(uint32_t ctx, int dx, int dy, int s
         if (stride == 1) s = sad_int_loop<1>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
         else if (stride == 2) s = sad_int_loop<2>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
         else s = sad_int_loop<4>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
+    } else if (c.aw == 16 && c.ah == 16 && xa >= 0 && ya >= 0 && xa + 16 <= P.W && ya + 16 <= P.H) {
+        // outside the staged window but inside the frame: no clamping, packed rows from L2
+        const uint8_t* base = c.gref + (size_t)ya * c.gpitch + xa;
+        if (stride == 1) s = sad_packed_glob<1>(c.cur_off, c.cur2_off, c.cur4_off, base, c.gpitch);
+        else if (stride == 2) s = sad_packed_glob<2>(c.cur_off, c.cur2_off, c.cur4_off, base, c.gpitch);
+        else s = sad_packed_glob<4>(c.cur_off, c.cur2_off, c.cur4_off, base, c.gpitch);
     } else {
         const GlobSampler gs{c.gref, c.gpitch, P.W, P.H};
         if (stride == 1) s = sad_int_loop<1>(gs, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
@@ -1165,6 +1211,18 @@ __device__ IntRes learned_descent(const DevParams& P, const Mb& m, IntRes best, 
     return best;
 }
 
+// The learned pass's fallback test: the best match's mean absolute error is above both
+// motion_match_good's six levels and the picture's mean error at the translation hint
+// (global_full_sad / pixels, in o.gsad), so that sensor noise alone sends no macroblock to the
+// plain search. Exact in integers: cost * W * H > px * max(6 * W * H, hint_sad).
+__device__ __forceinline__ bool learned_falls_back(const DevParams& P, const Mb& m, const DevResult& o, uint64_t cost) {
+    const uint64_t px = (uint64_t)m.aw * (uint64_t)m.ah;
+    if (!px || cost >= UINT64_MAX / 8) return true;
+    const uint64_t wh = (uint64_t)P.W * (uint64_t)P.H, hs = __ldcg(o.gsad);
+    const uint64_t a = 6 * wh;
+    return (unsigned __int128)cost * wh > (unsigned __int128)px * (a > hs ? a : hs);
+}
+
 struct RefineOut {
     int2 mv;
     uint64_t screen_sad;
@@ -1869,6 +1927,25 @@ __device__ void load_neighbours(const DevParams& P, const Mb& m, const DevResult
     __syncwarp();
 }
 
+// The neighbourhood a learned pass refines under: each neighbour's first candidate (the
+// network's top proposal, integer pixels) as its 1-MV vector, no P-intra. It is known before any
+// macroblock is analysed, so a learned pass has no wavefront.
+__device__ void load_cand_neighbours(const DevParams& P, const Mb& m, const PassDesc& d) {
+    const int q = m.lane < 16 ? (m.lane >> 2) : (m.lane & 3);
+    const int nx = m.mx + (q == 0 || q == 1 ? -1 : (q == 2 ? 0 : 1)), ny = m.my - (q == 0 ? 0 : 1);
+    const bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
+    const int nb = ny * P.mbw + nx;
+    int2 v = make_int2(0, 0);
+    if (valid && m.lane < 20) {
+        v = __ldg(&d.cands[(size_t)nb * kLearnK]);
+        v = make_int2(4 * v.x, 4 * v.y);
+    }
+    if (m.lane < 16) m.sm.nb_bmv[m.lane] = v;
+    else if (m.lane < 20) m.sm.nb_mv[q] = v;
+    else if (m.lane < 24) m.sm.nb_intra[q] = 0;
+    __syncwarp();
+}
+
 // A stand-in neighbourhood for guessing before the wavefront wait: the seed pass's final
 // vectors and P-intra flags of the same four neighbours (that pass is complete), and a
 // zero current MB.
@@ -2235,8 +2312,11 @@ __device__ uint64_t intra_proxy(const DevParams& P, const Mb& m) {
 #define VC1CU_SEEDED_MIN_BLOCKS 4
 #endif
 template <int KIND>
-__global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned)) ? VC1CU_SEEDED_MIN_BLOCKS
-                                                                : ((KIND & kCoreWide) ? 1 : VC1CU_CORE_MIN_BLOCKS))
+// The wide-register instantiation (one block per SM) takes up to 8 warps per block: 255
+// registers x 256 threads is the SM's register file.
+__global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
+                                  (KIND & (kCoreSeededOnly | kCoreLearned)) ? VC1CU_SEEDED_MIN_BLOCKS
+                                                                           : ((KIND & kCoreWide) ? 1 : VC1CU_CORE_MIN_BLOCKS))
     core_pass_kernel(const __grid_constant__ DevParams P0, const PassDesc* passes, int npass, const uint32_t* items,
                      unsigned nitems, WinCfg wc, uint32_t epoch, LaunchStatus* st) {
     Mb m;
@@ -2380,7 +2460,7 @@ __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned))
                 publish_ctx(P, m);
                 window_wait();
                 learned = learned_descent(P, m, best, range, kLearnRw - 4);
-                if (m.lane == 0 && d.fallback) d.fallback[m.pos] = match_good(m, learned.cost) ? 0 : 1;
+                if (m.lane == 0 && d.fallback) d.fallback[m.pos] = learned_falls_back(P, m, o, learned.cost) ? 1 : 0;
                 PHASE_MARK(2);
             } else {
                 load_window(P, m, d.ref, 0, 0, wc);
@@ -2391,11 +2471,15 @@ __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned))
             PHASE_MARK(4);
         }
         // ---- wavefront: left, top-left, top, top-right of the same pass ----
-        if (ok) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st, code);
+        // learned passes and no_wait passes read a field that is already complete: no wavefront
+        constexpr bool kLearned = (KIND & kCoreLearned) != 0;
+        const bool no_wait = kLearned || d.no_wait;
+        if (ok && !no_wait) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st, code);
         window_wait();  // an unseeded pass's window copies (none pending otherwise)
         PHASE_MARK(5);
         if (ok) {
-            load_neighbours(P, m, o);
+            if constexpr (kLearned) load_cand_neighbours(P, m, d);
+            else load_neighbours(P, m, d.no_wait ? d.nb : o);
             int2* cur4 = m.sm.cur_bmv;
             if (m.lane < 4) cur4[m.lane] = make_int2(0, 0);
             __syncwarp();
@@ -2439,7 +2523,7 @@ __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned))
                     // legacy distant-first policy (:144-160)
                     bool short_circuit = false;
                     if (long_range) {
-                        const IntRes pr = lr_propagated(P, m, o, range);
+                        const IntRes pr = lr_propagated(P, m, d.no_wait ? d.nb : o, range);
                         if (match_good(m, pr.cost)) {
                             im = pr;
                             short_circuit = true;
@@ -2454,7 +2538,7 @@ __global__ void __launch_bounds__(128, (KIND & (kCoreSeededOnly | kCoreLearned))
                     if (pixels) dl = (double)local_sad / (double)pixels;
                     const bool skip = P.long_range_mode == 1 && match_good(m, im.cost);
                     if (long_range && !skip) {
-                        const IntRes pr = lr_propagated(P, m, o, range);
+                        const IntRes pr = lr_propagated(P, m, d.no_wait ? d.nb : o, range);
                         const int decision = distant_decision(P, m, pr.cost, local_sad);
                         record(pr.cost, decision);
                         const bool less = pr.cost != im.cost ? pr.cost < im.cost
@@ -2688,6 +2772,30 @@ const void* core_kernel(int kind) {
 #undef VC1CU_KERNEL_CASE
         default: return nullptr;
     }
+}
+
+// The fallback macroblocks of a learned pass, from the fallback pass's slot into the learned one.
+__global__ void learned_merge_kernel(DevResult dst, DevResult src, const uint8_t* only, int mbs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mbs || !only[i]) return;
+    dst.mvs[i] = src.mvs[i];
+    for (int k = 0; k < 4; ++k) dst.bmv[4 * i + k] = src.bmv[4 * i + k];
+    dst.use4[i] = src.use4[i];
+    dst.intra[i] = src.intra[i];
+    dst.dd[i] = src.dd[i];
+    dst.flags[i] = src.flags[i];
+    dst.screen[i] = src.screen[i];
+    dst.chosen[i] = src.chosen[i];
+    dst.temporal[i] = src.temporal[i];
+    dst.ratio[i] = src.ratio[i];
+    dst.dl[i] = src.dl[i];
+    dst.dc[i] = src.dc[i];
+}
+
+cudaError_t launch_learned_merge(const DevResult& dst, const DevResult& src, const uint8_t* only, int mbs,
+                                 cudaStream_t s) {
+    learned_merge_kernel<<<(mbs + 255) / 256, 256, 0, s>>>(dst, src, only, mbs);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t s, const DevParams& P,

@@ -59,6 +59,8 @@ struct PassDesc {
     const uint8_t* only;         // non-null: only the MBs flagged here are computed (the others
                                  // keep the slot's contents and just publish their done flag)
     DevResult out;
+    DevResult nb;                // no_wait passes: the field the neighbours' vectors are read from
+    int no_wait;                 // 1: no wavefront waits; neighbours from `nb`, a finished field
     DevParams geom;              // this pass's picture geometry and configuration (read by the
                                  // kCoreMulti instantiation and the totals; the others take the
                                  // launch's parameter block)

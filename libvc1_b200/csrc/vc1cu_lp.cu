@@ -123,11 +123,8 @@ constexpr int kHaloW = kLpTile + 2;  // a tile's input row segment with one samp
 // the mbarrier and the tensor-memory address slot.
 __host__ __device__ constexpr int conv_b_bytes(int ca) { return 9 * (ca / 8) * 32 * 16; }
 __host__ __device__ constexpr int conv_a_bytes(int ca) { return (ca / 8) * 3 * kHaloW * 16; }
-// Every descriptor-addressed range stays inside this size under either reading of the two
-// offsets (leading / stride exchanged), so a layout mistake can give wrong numbers but never an
-// out-of-range shared access.
 __host__ __device__ constexpr int conv_smem_bytes(int ca) {
-    return conv_b_bytes(ca) + conv_a_bytes(ca) + 16 * 3 * kHaloW * 16 + 64;
+    return conv_b_bytes(ca) + conv_a_bytes(ca) + 64;
 }
 
 constexpr int kWgK = 64;  // pixels per weight-gradient chunk
@@ -135,16 +132,14 @@ __host__ __device__ constexpr int wg_groups(int cin) { return 9 * cin / 8; }
 __host__ __device__ constexpr int wg_groups_padded(int cin) { return (wg_groups(cin) + 15) / 16 * 16; }
 __host__ __device__ constexpr int wg_a_bytes(int cin) { return (kWgK / 8) * wg_groups_padded(cin) * 128; }
 __host__ __device__ constexpr int wg_b_bytes() { return (kWgK / 8) * 4 * 128; }
-// A, B, then room that keeps every descriptor-addressed range in bounds under either reading of
-// the two offsets (as for the convolutions).
-__host__ __device__ constexpr int wg_smem_bytes(int cin) {
-    return wg_a_bytes(cin) + wg_b_bytes() + 16 * wg_a_bytes(cin) / (kWgK / 8) + 64;
-}
+__host__ __device__ constexpr int wg_smem_bytes(int cin) { return wg_a_bytes(cin) + wg_b_bytes() + 64; }
 
 }  // namespace
 
 size_t lp_conv_smem(int ca) { return (size_t)conv_smem_bytes(ca); }
-size_t lp_wgrad_smem(int cin) { return (size_t)wg_smem_bytes(cin); }
+// At least 50 KB, so that no more than four weight-gradient CTAs share an SM: each holds 128 of
+// the SM's 512 tensor-memory columns.
+size_t lp_wgrad_smem(int cin) { return std::max<size_t>((size_t)wg_smem_bytes(cin), 50 * 1024); }
 size_t lp_fwd_b_elems(int l) { return (size_t)9 * lp_cin(l) * kLpC; }
 size_t lp_dgrad_b_elems(int l) { return l == 0 ? 0 : (size_t)9 * kLpC * kLpC; }
 
@@ -185,23 +180,14 @@ __device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v
     return t;
 }
 
-__device__ __forceinline__ int hint_r4(const LpGeom& g) { return min(32, (g.range + 3) / 4); }
-
-// Coarse stage: every quarter-resolution displacement in [-R4, R4]^2, full quarter-res SAD with
-// clamped reference sampling. One block per displacement.
-__global__ void lp_coarse_kernel(const uint8_t* cur4, const uint8_t* ref4, LpGeom g, unsigned long long* cost) {
-    __shared__ unsigned long long red[8];
-    const int R = hint_r4(g), n = 2 * R + 1;
-    const int dx = (int)(blockIdx.x % n) - R, dy = (int)(blockIdx.x / n) - R;
-    unsigned long long s = 0;
-    for (int i = threadIdx.x; i < g.W4 * g.H4; i += blockDim.x) {
-        const int x = i % g.W4, y = i / g.W4;
-        const int rx = min(max(x + dx, 0), g.W4 - 1), ry = min(max(y + dy, 0), g.H4 - 1);
-        s += (unsigned)abs((int)cur4[i] - (int)ref4[ry * g.W4 + rx]);
-    }
-    s = block_sum_u64(s, red);
-    if (threadIdx.x == 0) cost[blockIdx.x] = s;
-}
+// The translation hint, coarse to fine (each stage's least SAD by hint_less):
+//  A  1/16 resolution (one sample per macroblock, the rounded mean of its 4x4 quarter-res
+//     samples): every displacement in [-R16, R16]^2, R16 = min(16, ceil(range / 16));
+//  B  1/4 resolution: the 7x7 displacements about 4x A's, within +-ceil(range / 4);
+//  C  full resolution, frame SAD at stride 2: the 5x5 vectors about 4x B's, within +-range.
+// Clamped reference sampling at every level; one block per candidate.
+__device__ __forceinline__ int hint_r16(const LpGeom& g) { return min(16, (g.range + 15) / 16); }
+__device__ __forceinline__ int hint_na(const LpGeom& g) { return (2 * hint_r16(g) + 1) * (2 * hint_r16(g) + 1); }
 
 // (cost, |dx|+|dy|, dy, dx) lexicographic order.
 __device__ __forceinline__ bool hint_less(unsigned long long ca, int ax, int ay, unsigned long long cb, int bx, int by) {
@@ -212,36 +198,98 @@ __device__ __forceinline__ bool hint_less(unsigned long long ca, int ax, int ay,
     return ax < bx;
 }
 
-__device__ __forceinline__ int2 coarse_best(const unsigned long long* cost, const LpGeom& g) {
-    const int R = hint_r4(g), n = 2 * R + 1;
+__device__ __forceinline__ int2 vec_a(const LpGeom& g, int i) {
+    const int R = hint_r16(g), n = 2 * R + 1;
+    return make_int2(i % n - R, i / n - R);
+}
+__device__ __forceinline__ int2 vec_b(const LpGeom& g, int2 a, int k) {
+    const int r = (g.range + 3) / 4;
+    return make_int2(min(max(4 * a.x + k % 7 - 3, -r), r), min(max(4 * a.y + k / 7 - 3, -r), r));
+}
+__device__ __forceinline__ int2 vec_c(const LpGeom& g, int2 b, int k) {
+    return make_int2(min(max(4 * b.x + k % 5 - 2, -g.range), g.range), min(max(4 * b.y + k / 5 - 2, -g.range), g.range));
+}
+
+// The winners of the finished stages (cost layout: A's, then B's 49, then C's 25).
+__device__ int2 best_a(const unsigned long long* cost, const LpGeom& g) {
     unsigned long long bc = ~0ull;
-    int bx = 0, by = 0;
-    for (int i = 0; i < n * n; ++i) {
-        const int dx = i % n - R, dy = i / n - R;
-        if (hint_less(cost[i], dx, dy, bc, bx, by)) {
+    int2 b = make_int2(0, 0);
+    for (int i = 0; i < hint_na(g); ++i) {
+        const int2 v = vec_a(g, i);
+        if (hint_less(cost[i], v.x, v.y, bc, b.x, b.y)) {
             bc = cost[i];
-            bx = dx;
-            by = dy;
+            b = v;
         }
     }
-    return make_int2(bx, by);
+    return b;
+}
+__device__ int2 best_b(const unsigned long long* cost, const LpGeom& g, int2 a) {
+    const unsigned long long* cb = cost + hint_na(g);
+    unsigned long long bc = ~0ull;
+    int2 b = make_int2(0, 0);
+    for (int k = 0; k < 49; ++k) {
+        const int2 v = vec_b(g, a, k);
+        if (hint_less(cb[k], v.x, v.y, bc, b.x, b.y)) {
+            bc = cb[k];
+            b = v;
+        }
+    }
+    return b;
 }
 
-__device__ __forceinline__ int2 fine_vec(int2 c, int k, const LpGeom& g) {
-    const int dx = min(max(4 * c.x + k % 5 - 2, -g.range), g.range);
-    const int dy = min(max(4 * c.y + k / 5 - 2, -g.range), g.range);
-    return make_int2(dx, dy);
+// 1/16-resolution pictures: the rounded mean of each macroblock's 4x4 quarter-res samples.
+__global__ void lp_down16_kernel(const uint8_t* cur4, const uint8_t* ref4, LpGeom g, uint8_t* cur16, uint8_t* ref16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mbw * g.mbh) return;
+    const int x = i % g.mbw, y = i / g.mbw;
+    int sc = 0, sr = 0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            sc += cur4[(4 * y + a) * g.W4 + 4 * x + b];
+            sr += ref4[(4 * y + a) * g.W4 + 4 * x + b];
+        }
+    cur16[i] = (uint8_t)((sc + 8) >> 4);
+    ref16[i] = (uint8_t)((sr + 8) >> 4);
 }
 
-// Fine stage: the 5x5 full-resolution vectors about 4x the coarse winner, frame SAD at stride 2.
-__global__ void lp_fine_kernel(const uint8_t* cur, int cp, const uint8_t* ref, int rp, LpGeom g,
-                               unsigned long long* cost) {
+__global__ void lp_hint_a_kernel(const uint8_t* cur16, const uint8_t* ref16, LpGeom g, unsigned long long* cost) {
     __shared__ unsigned long long red[8];
-    __shared__ int2 cbest;
-    const int R = hint_r4(g), n = 2 * R + 1;
-    if (threadIdx.x == 0) cbest = coarse_best(cost, g);
+    const int2 v = vec_a(g, blockIdx.x);
+    unsigned long long s = 0;
+    for (int i = threadIdx.x; i < g.mbw * g.mbh; i += blockDim.x) {
+        const int x = i % g.mbw, y = i / g.mbw;
+        const int rx = min(max(x + v.x, 0), g.mbw - 1), ry = min(max(y + v.y, 0), g.mbh - 1);
+        s += (unsigned)abs((int)cur16[i] - (int)ref16[ry * g.mbw + rx]);
+    }
+    s = block_sum_u64(s, red);
+    if (threadIdx.x == 0) cost[blockIdx.x] = s;
+}
+
+__global__ void lp_hint_b_kernel(const uint8_t* cur4, const uint8_t* ref4, LpGeom g, unsigned long long* cost) {
+    __shared__ unsigned long long red[8];
+    __shared__ int2 a;
+    if (threadIdx.x == 0) a = best_a(cost, g);
     __syncthreads();
-    const int2 v = fine_vec(cbest, blockIdx.x, g);
+    const int2 v = vec_b(g, a, blockIdx.x);
+    unsigned long long s = 0;
+    for (int i = threadIdx.x; i < g.W4 * g.H4; i += blockDim.x) {
+        const int x = i % g.W4, y = i / g.W4;
+        const int rx = min(max(x + v.x, 0), g.W4 - 1), ry = min(max(y + v.y, 0), g.H4 - 1);
+        s += (unsigned)abs((int)cur4[i] - (int)ref4[ry * g.W4 + rx]);
+    }
+    s = block_sum_u64(s, red);
+    if (threadIdx.x == 0) cost[hint_na(g) + blockIdx.x] = s;
+}
+
+__global__ void lp_hint_c_kernel(const uint8_t* cur, int cp, const uint8_t* ref, int rp, LpGeom g,
+                                 unsigned long long* cost) {
+    __shared__ unsigned long long red[8];
+    __shared__ int2 b;
+    if (threadIdx.x == 0) b = best_b(cost, g, best_a(cost, g));
+    __syncthreads();
+    const int2 v = vec_c(g, b, blockIdx.x);
     const int sw = (g.W + 1) / 2, sh = (g.H + 1) / 2;
     unsigned long long s = 0;
     for (int i = threadIdx.x; i < sw * sh; i += blockDim.x) {
@@ -250,22 +298,22 @@ __global__ void lp_fine_kernel(const uint8_t* cur, int cp, const uint8_t* ref, i
         s += (unsigned)abs((int)cur[(size_t)y * cp + x] - (int)ref[(size_t)ry * rp + rx]);
     }
     s = block_sum_u64(s, red);
-    if (threadIdx.x == 0) cost[n * n + blockIdx.x] = s;
+    if (threadIdx.x == 0) cost[hint_na(g) + 49 + blockIdx.x] = s;
 }
 
 __global__ void lp_pick_kernel(const unsigned long long* cost, LpGeom g, int2* hint) {
-    const int R = hint_r4(g), n = 2 * R + 1;
-    const int2 c = coarse_best(cost, g);
+    const int2 b = best_b(cost, g, best_a(cost, g));
+    const unsigned long long* cc = cost + hint_na(g) + 49;
     unsigned long long bc = ~0ull;
-    int2 b = make_int2(0, 0);
+    int2 best = make_int2(0, 0);
     for (int k = 0; k < 25; ++k) {
-        const int2 v = fine_vec(c, k, g);
-        if (hint_less(cost[n * n + k], v.x, v.y, bc, b.x, b.y)) {
-            bc = cost[n * n + k];
-            b = v;
+        const int2 v = vec_c(g, b, k);
+        if (hint_less(cc[k], v.x, v.y, bc, best.x, best.y)) {
+            bc = cc[k];
+            best = v;
         }
     }
-    *hint = b;
+    *hint = best;
 }
 
 // The full-resolution frame SAD at the hint (stride 1, clamped sampling): the analysis pass's
@@ -684,9 +732,13 @@ cudaError_t lp_launch_downsample(const uint8_t* cur, int cur_pitch, const uint8_
 cudaError_t lp_launch_hint(const uint8_t* cur, int cur_pitch, const uint8_t* ref, int ref_pitch, const LpGeom& g,
                            const uint8_t* cur4, const uint8_t* ref4, unsigned long long* scratch, int2* hint,
                            unsigned long long* hint_sad, cudaStream_t s) {
-    const int R = std::min(32, (g.range + 3) / 4), n = 2 * R + 1;
-    lp_coarse_kernel<<<n * n, 256, 0, s>>>(cur4, ref4, g, scratch);
-    lp_fine_kernel<<<25, 256, 0, s>>>(cur, cur_pitch, ref, ref_pitch, g, scratch);
+    const int R = std::min(16, (g.range + 15) / 16), na = (2 * R + 1) * (2 * R + 1);
+    uint8_t* cur16 = const_cast<uint8_t*>(cur4) + (size_t)g.W4 * g.H4;  // the buffers hold both levels
+    uint8_t* ref16 = const_cast<uint8_t*>(ref4) + (size_t)g.W4 * g.H4;
+    lp_down16_kernel<<<(g.mbw * g.mbh + 255) / 256, 256, 0, s>>>(cur4, ref4, g, cur16, ref16);
+    lp_hint_a_kernel<<<na, 256, 0, s>>>(cur16, ref16, g, scratch);
+    lp_hint_b_kernel<<<49, 256, 0, s>>>(cur4, ref4, g, scratch);
+    lp_hint_c_kernel<<<25, 256, 0, s>>>(cur, cur_pitch, ref, ref_pitch, g, scratch);
     lp_pick_kernel<<<1, 1, 0, s>>>(scratch, g, hint);
     cudaError_t e = cudaMemsetAsync(hint_sad, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;

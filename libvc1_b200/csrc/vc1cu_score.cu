@@ -128,4 +128,42 @@ double measure_int32_peak(cudaStream_t s, int sms) {
     return 16.0 * iters * (double)blocks * threads / (ms * 1e-3);
 }
 
+// FP64 throughput calibration: 8 independent chains of fused multiply-adds per thread (two
+// flops each), contracting values that stay normal.
+__global__ void fp64_peak_kernel(double* out, int iters, double k1, double k2) {
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = 1.0 + threadIdx.x * 1e-3 + j * 0.25 + blockIdx.x * 1e-6;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = __fma_rn(a[j], k1, k2);
+    }
+    double r = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r += a[j];
+    if (r == 1234.5) out[0] = r;  // keeps the chains live
+}
+
+// Returns FP64 flops per second (16 per thread per iteration).
+double measure_fp64_peak(cudaStream_t s, int sms) {
+    double* d = nullptr;
+    if (cudaMalloc(&d, 8) != cudaSuccess) return 0.0;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 16;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, 256, 0.999999, 1e-7);  // warm-up
+    cudaEventRecord(a, s);
+    fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, iters, 0.999999, 1e-7);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (ms <= 0.f) return 0.0;
+    return 16.0 * iters * (double)blocks * threads / (ms * 1e-3);
+}
+
 }  // namespace vc1cu

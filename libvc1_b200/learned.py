@@ -111,27 +111,32 @@ def evaluate(ctx, net, seeds, sample0=0, fallback=True, psnr=True):
     levels = torch.empty((mbs, 6, 64), dtype=torch.int16, device="cuda")
     types = np.ones(mbs * 6, np.uint8)
     out = {"sad_plain": [], "sad_learned": [], "psnr_plain": [], "psnr_learned": [], "fallback": [],
-           "ms_plain": 0.0, "ms_learned": 0.0}
+           "ms_plain": 0.0, "ms_learned": 0.0, "ms_prepare": 0.0, "ms_propose": 0.0, "ms_analyze": 0.0}
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     for g in range(0, len(seeds), GROUP):
         grp = seeds[g:g + GROUP]
         n = len(grp)
         make_pairs(ctx, grp)
         ctx.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         e[0].record(stream)
         ctx.core_passes(p, [(_F0 + 2 * k, _F0 + 2 * k + 1, MV_QPEL, 0, -1, _R0 + k) for k in range(n)])
         e[1].record(stream)
         e[2].record(stream)
         for k in range(n):
             net.prepare(_F0 + 2 * k, _F0 + 2 * k + 1, sample0 + k)
+        e[3].record(stream)
         net.propose(sample0, n)
+        e[4].record(stream)
         net.analyze(p, [(_F0 + 2 * k, _F0 + 2 * k + 1, sample0 + k, MV_QPEL, _R0 + 100 + k) for k in range(n)],
                     fallback=fallback)
-        e[3].record(stream)
-        e[3].synchronize()
+        e[5].record(stream)
+        e[5].synchronize()
         out["ms_plain"] += e[0].elapsed_time(e[1])
-        out["ms_learned"] += e[2].elapsed_time(e[3])
+        out["ms_learned"] += e[2].elapsed_time(e[5])
+        out["ms_prepare"] += e[2].elapsed_time(e[3])
+        out["ms_propose"] += e[3].elapsed_time(e[4])
+        out["ms_analyze"] += e[4].elapsed_time(e[5])
         for k in range(n):
             a = ctx.read_result(p, _R0 + k)
             b = ctx.read_result(p, _R0 + 100 + k)
@@ -157,7 +162,11 @@ def summarize(ev, mbs_per_pair):
     s = {"pairs": n, "cost_gap_mean": float(gap.mean()), "cost_gap_p99": float(np.percentile(gap, 99)),
          "fallback_rate": float(np.sum(ev["fallback"]) / (n * mbs_per_pair)),
          "mbs_per_s_plain": n * mbs_per_pair / (ev["ms_plain"] / 1e3) if ev["ms_plain"] else None,
-         "mbs_per_s_learned": n * mbs_per_pair / (ev["ms_learned"] / 1e3) if ev["ms_learned"] else None}
+         "mbs_per_s_learned": n * mbs_per_pair / (ev["ms_learned"] / 1e3) if ev["ms_learned"] else None,
+         "ms_per_pair": {k[3:]: ev[k] / max(n, 1) for k in ("ms_plain", "ms_learned", "ms_prepare", "ms_propose",
+                                                            "ms_analyze")}}
+    if s["mbs_per_s_plain"] and s["mbs_per_s_learned"]:
+        s["speedup"] = s["mbs_per_s_learned"] / s["mbs_per_s_plain"]
     if ev["psnr_plain"]:
         s["psnr_plain"] = float(np.mean(ev["psnr_plain"]))
         s["psnr_learned"] = float(np.mean(ev["psnr_learned"]))

@@ -367,6 +367,8 @@ class Reference:
                                           C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(i32), C.POINTER(i32),
                                           C.POINTER(i32), i32, i32]
         L.ref_bench_gop_multi.restype = u64
+        L.ref_bench_gop_same.argtypes = L.ref_bench_gop_multi.argtypes
+        L.ref_bench_gop_same.restype = u64
         self.p = p
         self._recent = collections.deque(maxlen=8)
         self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
@@ -566,6 +568,18 @@ class Reference:
                                             vpa([j[1].h for j in bjobs]), vpa([j[2].h for j in bjobs]),
                                             vpa([j[3].h for j in bjobs]), ia([j[4] for j in bjobs]),
                                             ia([j[5] for j in bjobs]), ia([j[6] for j in bjobs]), len(bjobs), threads)
+
+    def bench_gop_same(self, pjobs, bjobs, threads):
+        """Wall ns of the GPU arm's work on the reference's functions (ref_bench_gop_same): per P
+        job the five core passes, the fade estimate, the prediction and all four types' levels;
+        per B job analyze_b_picture_mode in quarter-pel and bilinear mode; one pool for both."""
+        vpa = lambda xs: (vp * max(1, len(xs)))(*xs)  # noqa: E731
+        ia = lambda xs: (i32 * max(1, len(xs)))(*xs)  # noqa: E731
+        return self.lib.ref_bench_gop_same(vpa([j[0].h for j in pjobs]), vpa([j[1].h for j in pjobs]),
+                                           vpa([j[2].h for j in pjobs]), len(pjobs), vpa([j[0].h for j in bjobs]),
+                                           vpa([j[1].h for j in bjobs]), vpa([j[2].h for j in bjobs]),
+                                           vpa([j[3].h for j in bjobs]), ia([j[4] for j in bjobs]),
+                                           ia([j[5] for j in bjobs]), ia([j[6] for j in bjobs]), len(bjobs), threads)
 
     def bench_analysis_multi(self, jobs, threads):
         """Wall ns over (Reference, cur RefFrame, ref RefFrame) jobs, each with its own config."""

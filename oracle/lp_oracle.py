@@ -5,9 +5,9 @@ the proposal network (libvc1_b200/csrc/vc1cu_lp.cu) so that the tests can check 
 translation hint, candidates, loss and every gradient:
 
 - quarter-resolution pictures (rounded 4x4 means, clamped at the picture edge);
-- the translation hint: the least quarter-resolution SAD over [-R4, R4]^2 (R4 = min(32,
-  ceil(range/4))), then the least full-resolution SAD at stride 2 over the 5x5 vectors about 4x
-  that, ties by (cost, |dx|+|dy|, dy, dx); the vector is clamped to the search range;
+- the translation hint, coarse to fine: the least 1/16-resolution SAD over [-R16, R16]^2, then
+  the 7x7 quarter-resolution displacements about 4x that, then the 5x5 full-resolution vectors
+  (SAD at stride 2) about 4x that, ties by (cost, |dx|+|dy|, dy, dx), clamped to the search range;
 - the 16 input channels (bf16): cur, ref, ref shifted by the hint, their differences, cur's
   gradients, the hint / 64, zeros;
 - four 3x3 convolutions (zero padding) with bias and ReLU, activations rounded to bf16 where the
@@ -109,28 +109,39 @@ def _hint_less(a, b):
 
 
 def hint_search(cur_y: np.ndarray, ref_y: np.ndarray, search_range: int):
+    """Coarse to fine: 1/16 resolution over [-R16, R16]^2 (R16 = min(16, ceil(range/16))), 1/4
+    resolution over the 7x7 about 4x that (within +-ceil(range/4)), full resolution at stride 2
+    over the 5x5 about 4x that (within +-range)."""
     h, w = cur_y.shape
-    w4, h4, _, _ = geometry(w, h)
+    w4, h4, mbw, mbh = geometry(w, h)
     c4, r4 = downsample(cur_y, w4, h4), downsample(ref_y, w4, h4)
-    R = min(32, (search_range + 3) // 4)
-    best = None
-    for dy in range(-R, R + 1):
-        for dx in range(-R, R + 1):
-            cost = int(np.abs(c4 - _shift_clamped(r4, dx, dy)).sum())
-            if best is None or _hint_less((cost, dx, dy), best):
-                best = (cost, dx, dy)
-    cx, cy = best[1], best[2]
+    c16 = (c4.reshape(mbh, 4, mbw, 4).sum(axis=(1, 3)) + 8) >> 4
+    r16 = (r4.reshape(mbh, 4, mbw, 4).sum(axis=(1, 3)) + 8) >> 4
+
+    def least(cands, cost):
+        best = None
+        for dx, dy in cands:
+            c = cost(dx, dy)
+            if best is None or _hint_less((c, dx, dy), best):
+                best = (c, dx, dy)
+        return best[1], best[2]
+
+    R = min(16, (search_range + 15) // 16)
+    ax, ay = least([(dx, dy) for dy in range(-R, R + 1) for dx in range(-R, R + 1)],
+                   lambda dx, dy: int(np.abs(c16 - _shift_clamped(r16, dx, dy)).sum()))
+    r4r = (search_range + 3) // 4
+    bx, by = least([(min(max(4 * ax + k % 7 - 3, -r4r), r4r), min(max(4 * ay + k // 7 - 3, -r4r), r4r))
+                    for k in range(49)],
+                   lambda dx, dy: int(np.abs(c4 - _shift_clamped(r4, dx, dy)).sum()))
     cur2 = cur_y[::2, ::2].astype(np.int64)
-    fbest = None
-    for k in range(25):
-        dx = min(max(4 * cx + k % 5 - 2, -search_range), search_range)
-        dy = min(max(4 * cy + k // 5 - 2, -search_range), search_range)
+
+    def full(dx, dy):
         ys = np.clip(np.arange(0, h, 2) + dy, 0, h - 1)
         xs = np.clip(np.arange(0, w, 2) + dx, 0, w - 1)
-        cost = int(np.abs(cur2 - ref_y.astype(np.int64)[ys[:, None], xs[None, :]]).sum())
-        if fbest is None or _hint_less((cost, dx, dy), fbest):
-            fbest = (cost, dx, dy)
-    return fbest[1], fbest[2]
+        return int(np.abs(cur2 - ref_y.astype(np.int64)[ys[:, None], xs[None, :]]).sum())
+
+    return least([(min(max(4 * bx + k % 5 - 2, -search_range), search_range),
+                   min(max(4 * by + k // 5 - 2, -search_range), search_range)) for k in range(25)], full)
 
 
 def features(cur_y: np.ndarray, ref_y: np.ndarray, hint) -> np.ndarray:

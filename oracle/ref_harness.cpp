@@ -621,6 +621,104 @@ uint64_t ref_bench_gop_multi(void** p_handles, void** p_curs, void** p_refs, int
     return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
 }
 
+// CPU baseline doing the GPU arm's work with the reference's own functions, one job pool for
+// the P and the B pictures. Per P picture: the five core passes analyze_p_picture chains
+// (quarter-pel seed pass, the half-pel, bilinear and Mixed-MV passes seeded by it, the final
+// Mixed-MV pass with P-intra seeded by the Mixed-MV pass; encoder_motion.cpp:524-597), the fade
+// estimate along the final vectors, the prediction of the final field and quantize_inter_part
+// (forward transform + quantiser) of every partition of all four transform types. Per B picture:
+// analyze_b_picture_mode in quarter-pel and in half-pel bilinear mode against its anchors, with
+// the future anchor's final vectors (intensity compensation off). A B job waits for its anchor's
+// P job; every P job is taken before any B job, so the pool cannot deadlock. Returns wall ns.
+uint64_t ref_bench_gop_same(void** p_handles, void** p_curs, void** p_refs, int n_p, void** b_handles, void** b_curs,
+                            void** b_pasts, void** b_futures, const int* b_anchor, const int* b_num, const int* b_den,
+                            int n_b, int threads) {
+    const size_t np = static_cast<size_t>(std::max(0, n_p));
+    std::vector<Vc1Encoder::PAnalysis> finals(np);
+    std::unique_ptr<std::atomic<int>[]> done(new std::atomic<int>[np > 0 ? np : 1]);
+    for (size_t i = 0; i < np; ++i) done[i].store(0);
+    std::atomic<long long> sink{0};
+    std::atomic<int> next{0};
+    auto p_job = [&](int i) {
+        const auto& c = static_cast<RefEncoder*>(p_handles[i])->cfg;
+        const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+        Vc1Encoder enc(c);
+        const Frame& cur = F(p_curs[i]);
+        const Frame& ref = F(p_refs[i]);
+        const auto seed = enc.analyze_p_picture_core(cur, ref, Mode::OneMvQpel, false, nullptr);
+        (void)enc.analyze_p_picture_core(cur, ref, Mode::OneMvHpel, false, &seed);
+        (void)enc.analyze_p_picture_core(cur, ref, Mode::OneMvHpelBilinear, false, &seed);
+        const auto mixed = enc.analyze_p_picture_core(cur, ref, Mode::MixedMv, false, &seed);
+        finals[i] = enc.analyze_p_picture_core(cur, ref, Mode::MixedMv, true, &mixed);
+        const auto& a = finals[i];
+        const auto ic = enc.estimate_intensity_comp(cur, ref, a.mvs);
+        Frame pred;
+        pred.width = c.width;
+        pred.height = c.height;
+        pred.y.assign(static_cast<size_t>(c.width) * c.height, 0);
+        pred.u.assign(static_cast<size_t>(c.width / 2) * (c.height / 2), 128);
+        pred.v = pred.u;
+        for (int my = 0; my < mbh; ++my)
+            for (int mx = 0; mx < mbw; ++mx) {
+                const size_t pos = static_cast<size_t>(my) * mbw + mx;
+                if (a.use_4mv[pos]) enc.motion_compensate_4mv(pred, ref, mx, my, a.block_mvs[pos]);
+                else enc.motion_compensate_mb(pred, ref, mx, my, a.mvs[pos], Mode::MixedMv);
+            }
+        long long acc = ic.enabled ? 1 : 0;
+        for (int t = 1; t <= 4; ++t) {
+            const auto type = static_cast<Vc1Encoder::TransformType>(t);
+            for (int my = 0; my < mbh; ++my)
+                for (int mx = 0; mx < mbw; ++mx)
+                    for (int k = 0; k < 6; ++k) {
+                        const bool chroma = k >= 4;
+                        const auto& sp = chroma ? (k == 4 ? cur.u : cur.v) : cur.y;
+                        const auto& pp = chroma ? (k == 4 ? pred.u : pred.v) : pred.y;
+                        const int w = chroma ? c.width / 2 : c.width, hh = chroma ? c.height / 2 : c.height;
+                        const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
+                        for (int part = 0; part < Vc1Encoder::transform_part_count(type); ++part) {
+                            int ox, oy, bw, bh;
+                            Vc1Encoder::transform_part_geometry(type, part, ox, oy, bw, bh);
+                            const auto q = enc.quantize_inter_part(sp, pp, w, hh, bx * 8 + ox, by * 8 + oy, bw, bh, false);
+                            acc += q[0];
+                        }
+                    }
+        }
+        sink.fetch_add(acc);
+        done[i].store(1, std::memory_order_release);
+    };
+    auto b_job = [&](int i) {
+        const auto& c = static_cast<RefEncoder*>(b_handles[i])->cfg;
+        const size_t a_idx = static_cast<size_t>(b_anchor[i]);
+        while (!done[a_idx].load(std::memory_order_acquire)) std::this_thread::yield();
+        const auto& a = finals[a_idx];
+        Vc1Encoder enc(c);
+        for (const Mode m : {Mode::OneMvQpel, Mode::OneMvHpelBilinear}) {
+            const auto r = enc.analyze_b_picture_mode(F(b_curs[i]), F(b_pasts[i]), F(b_futures[i]), a.mvs, a.use_4mv,
+                                                      Vc1Encoder::IntensityComp{}, b_num[i], b_den[i], m, nullptr,
+                                                      nullptr, nullptr);
+            sink.fetch_add(static_cast<long long>(r.motion_sad));
+        }
+    };
+    auto worker = [&]() {
+        for (;;) {
+            const int j = next.fetch_add(1);
+            if (j >= n_p + n_b) break;
+            if (j < n_p) p_job(j);
+            else b_job(j - n_p);
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < std::max(1, threads); ++t) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    static std::atomic<long long> keep{0};
+    keep.fetch_add(sink.load());
+    return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+}
+
 // CPU baseline: analyze_p_picture + choose_transform_mb of the chosen prediction for every
 // MB of every (cur, ref) pair, one pair per worker thread at a time. Returns wall ns.
 uint64_t ref_bench_analysis(void* h, void** curs, void** refs, int n_pairs, int threads) {

@@ -2271,14 +2271,16 @@ int vo_zoom_coherent(const vc1cu_mv* mvs, int mbw, int mbh) {
 }
 
 /* The learned analysis pass of this library (no counterpart in the reference; on the device:
- * learned_candidates / learned_descent in libvc1_b200/csrc/vc1cu_core.cu and the two launches of
- * vc1cu_lp_analyze). Pass A, raster order: the best of each macroblock's four integer-pixel
+ * learned_candidates / learned_descent in libvc1_b200/csrc/vc1cu_core.cu and the launches of
+ * vc1cu_lp_analyze). Pass A, every macroblock independently: the best of its four integer-pixel
  * candidates (clamped to the search bounds) by exact mb_sad, a small-diamond descent of at most
- * 2 * reach steps within reach of it, the fallback flag (motion_match_good fails), then the staged
- * refinement with the macroblock's real predictor, as an unseeded pass refines its integer vector
- * (encoder_motion.cpp:226-230). Pass B (fallback != 0), raster order over the flagged macroblocks
- * only: the unseeded pass's integer search with the hint as its global vector and the current
- * field as neighbours, then the same refinement. Totals as analyze_p_picture_core's, with the
+ * 2 * reach steps within reach of it, the fallback flag (the match's mean absolute error is above
+ * six levels and above the picture's mean error at the hint), then the staged
+ * refinement, whose rate predictor takes the neighbours' first candidates as their vectors, as an
+ * unseeded pass refines its integer vector (encoder_motion.cpp:226-230). Pass B (fallback != 0),
+ * the flagged macroblocks independently: the unseeded pass's integer search with the hint as its
+ * global vector and the finished pass-A field as neighbours, then the same refinement with that
+ * field's predictor; its results replace pass A's. Totals as analyze_p_picture_core's, with the
  * hint's full-resolution frame SAD standing in for the global search's. */
 int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_frame* ref, int mode, const vc1cu_mv* cands,
                          int hint_dx, int hint_dy, int fallback, uint8_t* flags, vc1cu_panalysis* out) {
@@ -2298,15 +2300,32 @@ int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_fram
     uint8_t* dd = (uint8_t*)calloc(mbs, 1);
     lr_cell* cells = NULL;
     int ncells = 0;
-    for (size_t i = 0; i < mbs; ++i) { dl[i] = -1.0; dc[i] = -1.0; }
-    for (int pass = 0; pass < (fallback ? 2 : 1); ++pass)
+    /* the learned pass's neighbourhood: every macroblock's first candidate as its 1-MV vector
+       (no wavefront); the fallback pass's: the finished learned field (smvs, sbmv), in which no
+       macroblock took a distant match */
+    vc1cu_mv* cbmv = (vc1cu_mv*)calloc(mbs * 4, sizeof(vc1cu_mv));
+    vc1cu_mv* smvs = (vc1cu_mv*)calloc(mbs, sizeof(vc1cu_mv));
+    vc1cu_mv* sbmv = (vc1cu_mv*)calloc(mbs * 4, sizeof(vc1cu_mv));
+    for (size_t i = 0; i < mbs; ++i) {
+        dl[i] = -1.0;
+        dc[i] = -1.0;
+        const vc1cu_mv c0 = {cands[i * 4].xq * 4, cands[i * 4].yq * 4};
+        for (int k = 0; k < 4; ++k) cbmv[i * 4 + k] = c0;
+    }
+    const uint64_t hint_sad = vo_frame_sad(f, ref, hint_dx, hint_dy, 1);
+    const uint64_t wh = (uint64_t)p->width * (uint64_t)p->height;
+    for (int pass = 0; pass < (fallback ? 2 : 1); ++pass) {
+        if (pass == 1) {
+            memcpy(smvs, mvs, mbs * sizeof(vc1cu_mv));
+            memcpy(sbmv, bmv, mbs * 4 * sizeof(vc1cu_mv));
+        }
         for (int my = 0; my < mbh; ++my)
             for (int mx = 0; mx < mbw; ++mx) {
                 const size_t pos = (size_t)my * mbw + mx;
                 if (pass == 1 && !flags[pos]) continue;
                 const int x0 = mx * 16, y0 = my * 16;
                 const uint64_t pixels = active_mb_pixels(p, mx, my);
-                const pinfo rate_pi = predictor_info_mixed_1mv(bmv, intra, mbw, mbh, mx, my);
+                const pinfo rate_pi = predictor_info_mixed_1mv(pass == 0 ? cbmv : sbmv, intra, mbw, mbh, mx, my);
                 cand best = {UINT64_MAX, 0, 0};
                 if (pass == 0) {
                     for (int k = 0; k < 4; ++k) {
@@ -2339,14 +2358,25 @@ int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_fram
                         if (!any || !cand_less(nb.cost, nb.dx, nb.dy, best.cost, best.dx, best.dy)) break;
                         best = nb;
                     }
-                    if (flags) flags[pos] = motion_match_good(p, best.cost, mx, my) ? 0 : 1;
+                    if (flags) {
+                        /* fallback when the match's mean absolute error is above both six levels
+                           and the picture's mean error at the hint:
+                           cost * W * H > pixels * max(6 * W * H, hint_sad) */
+                        int fb = 1;
+                        if (pixels && best.cost < UINT64_MAX / 8) {
+                            const uint64_t a = 6 * wh;
+                            fb = (unsigned __int128)best.cost * wh > (unsigned __int128)pixels * (a > hint_sad ? a : hint_sad);
+                        }
+                        flags[pos] = (uint8_t)fb;
+                    }
                     if (pixels) dl[pos] = (double)best.cost / (double)pixels;
                 } else {
                     dl[pos] = -1.0;
                     dc[pos] = -1.0;
                     dd[pos] = 0;
-                    best = unseeded_integer(p, f, ref, mx, my, mvs, propagated, hint_dx, hint_dy, &cells, &ncells,
+                    best = unseeded_integer(p, f, ref, mx, my, smvs, propagated, hint_dx, hint_dy, &cells, &ncells,
                                             &dl[pos], &dc[pos], &dd[pos]);
+                    propagated[pos] = 0; /* the learned field holds no distant matches */
                 }
                 uint64_t one_sad = 0;
                 const vc1cu_mv s4 = {best.dx * 4, best.dy * 4};
@@ -2360,6 +2390,10 @@ int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_fram
                 for (int k = 0; k < 4; ++k) bmv[pos * 4 + k] = one;
                 screen[pos] = one_sad;
             }
+    }
+    free(cbmv);
+    free(smvs);
+    free(sbmv);
     uint64_t total_sad = 0, total_pixels = 0, moved = 0, frac = 0;
     for (int my = 0; my < mbh; ++my)
         for (int mx = 0; mx < mbw; ++mx) {
@@ -2369,7 +2403,7 @@ int vo_analyze_p_learned(const vc1cu_params* p, const vo_frame* f, const vo_fram
             moved += mvs[pos].xq != 0 || mvs[pos].yq != 0;
             frac += (mvs[pos].xq % 8) != 0 || (mvs[pos].yq % 8) != 0;
         }
-    const uint64_t gsad = vo_frame_sad(f, ref, hint_dx, hint_dy, 1);
+    const uint64_t gsad = hint_sad;
     const double local_mad = total_pixels ? (double)total_sad / (double)total_pixels : 0.0;
     const double global_mad = (double)gsad / (double)((uint64_t)p->width * p->height);
     out->mean_abs_residual = local_mad < global_mad ? local_mad : global_mad;
