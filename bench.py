@@ -369,6 +369,102 @@ def learned_leg(ctx, torch, l2, steps, warmup, pairs=16):
             "cost_gap_definition": "per pair (sum of the chosen vectors' exact SAD, learned - plain) / plain"}
 
 
+def longrange_leg(ctx, torch, reps, clips=8, frames=12):
+    """Long-range pans (1920x1080, pans up to 200 px/frame horizontal and 60 vertical, 4 objects;
+    search range 1024 = MVRANGE 3, local 32, QP 6): `clips` clips of `frames` frames, every frame
+    step's P pictures of all clips as one batch. The plain batched form (one launch of the
+    unseeded quarter-pel passes per frame step) against the learned form (hint + features +
+    network for every clip, one learned launch and one fallback launch per frame step), each GOP
+    captured as one CUDA graph and replayed; then the exact-SAD cost gap, fallback rate and the
+    luma PSNR of the QP-6 reconstruction of every pair."""
+    from libvc1_b200 import learned as lw
+    from libvc1_b200 import synth
+    from libvc1_b200.abi import MV_QPEL, make_params
+    from libvc1_b200.api import LearnedProposals
+
+    if not os.path.exists(lw.WEIGHTS):
+        return {"unavailable": "no trained parameters (libvc1_b200/learned_weights.npy)"}
+    p = make_params(W, H, search_range=1024, local_search_range=32, pqindex=lw.QP)
+    F0, R0 = 200, 2000
+    fid = lambda k, t: F0 + 64 * k + t  # noqa: E731
+    for k in range(clips):
+        cfg = synth.make_cfg(W, H, frames, 700 + k, global_px=200.0, global_py=60.0, n_objects=4, obj_vel=8.0,
+                             sigma=2.0)
+        ctx.synth_frames(cfg, 0, frames, fid(k, 0))
+    net = LearnedProposals(ctx, W, H, 1024, clips, max_batch=clips, seed=1)
+    net.set_params(np.load(lw.WEIGHTS))
+    steps = range(1, frames)
+    pslot = lambda k, t: R0 + 2 * (frames * k + t)  # noqa: E731
+    lslot = lambda k, t: pslot(k, t) + 1  # noqa: E731
+
+    def plain_gop():
+        for t in steps:
+            ctx.core_passes(p, [(fid(k, t), fid(k, t - 1), MV_QPEL, 0, -1, pslot(k, t)) for k in range(clips)])
+
+    def learned_gop():
+        for t in steps:
+            for k in range(clips):
+                net.prepare(fid(k, t), fid(k, t - 1), k)
+            net.propose(0, clips)
+            net.analyze(p, [(fid(k, t), fid(k, t - 1), k, MV_QPEL, lslot(k, t)) for k in range(clips)], fallback=True)
+
+    ext = torch.cuda.ExternalStream(ctx.stream_handle())
+    out = {}
+    for name, gop in (("plain", plain_gop), ("learned", learned_gop)):
+        gop()  # direct: builds the launches' tables and slots
+        ctx.synchronize()
+        ctx.graph_begin()
+        gop()
+        g = ctx.graph_end()
+        ctx.graph_launch(g)
+        ctx.synchronize()
+        t = 0.0
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ext)
+            ctx.graph_launch(g)
+            b.record(ext)
+            b.synchronize()
+            t += a.elapsed_time(b)
+        ctx.graph_destroy(g)
+        out[name] = t / reps
+    # quality of every pair (the last replay's results)
+    gaps, psnr_p, psnr_l = [], [], []
+    levels = torch.empty((MBS, 6, 64), dtype=torch.int16, device="cuda")
+    types = np.ones(MBS * 6, np.uint8)
+    for k in range(clips):
+        for t in steps:
+            a, b = ctx.read_result(p, pslot(k, t)), ctx.read_result(p, lslot(k, t))
+            sp, sl = float(a.screen_sads.astype(np.float64).sum()), float(b.screen_sads.astype(np.float64).sum())
+            gaps.append((sl - sp) / max(sp, 1.0))
+        for t in (1, frames - 1):
+            cur = ctx.download_frame(fid(k, t), W, H)[0]
+            for acc, slot in ((psnr_p, pslot(k, t)), (psnr_l, lslot(k, t))):
+                ctx.motion_compensate(p, fid(k, t - 1), slot, MV_QPEL, 3900)
+                ctx.forward_quant_device(p, fid(k, t), 3900, 1, 0, levels.data_ptr())
+                ctx.reconstruct(p, 3900, levels.data_ptr(), 1, types, 3901)
+                rec = ctx.download_frame(3901, W, H)[0]
+                mse = np.mean((rec.astype(np.float64) - cur.astype(np.float64)) ** 2)
+                acc.append(99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse))
+    # fallback share of the last frame step (the network's per-sample flags)
+    fb = sum(int(net.read_sample(k)[3].sum()) for k in range(clips))
+    net.close()
+    gaps = np.array(gaps)
+    mb_gop = clips * len(steps) * MBS
+    return {"workload": f"{clips} clips x {frames} frames 1920x1080, pans up to 200 px/frame horizontal and 60 vertical, "
+                        "4 objects, sigma 2; search range 1024 (MVRANGE 3), local 32; ME + qpel per P picture; "
+                        "every frame step's pictures of all clips in one batch; a CUDA graph per GOP",
+            "mb_per_s_plain": round(mb_gop / (out["plain"] * 1e-3), 1),
+            "mb_per_s_learned": round(mb_gop / (out["learned"] * 1e-3), 1),
+            "speedup": round(out["plain"] / out["learned"], 3), "ms_per_gop_plain": round(out["plain"], 2),
+            "ms_per_gop_learned": round(out["learned"], 2), "cost_gap_mean": round(float(gaps.mean()), 5),
+            "cost_gap_p99": round(float(np.percentile(gaps, 99)), 5),
+            "fallback_rate_last_step": round(fb / (clips * MBS), 4),
+            "psnr_plain": round(float(np.mean(psnr_p)), 4), "psnr_learned": round(float(np.mean(psnr_l)), 4),
+            "psnr_delta_db": round(float(np.mean(psnr_l) - np.mean(psnr_p)), 4),
+            "psnr_sample": "QP-6 luma reconstruction of frame steps 1 and last of every clip"}
+
+
 def batched_clips(n_odd_seed=7):
     """The batched workload's 48 clips: (coded width, height, display width, height, seed):
     16 at 640x360, 16 at 1280x720, 8 at 1920x1080 and 8 of odd display sizes with widths in
@@ -601,6 +697,9 @@ def run_ours(args, rank, world, device):
     batched = None
     if not args.no_batched and world == 1:
         batched = batched_leg(ctx, torch, reps=min(args.steps, 2))
+    longrange = None
+    if not args.no_longrange and world == 1:
+        longrange = longrange_leg(ctx, torch, reps=min(args.steps, 2))
     out = None
     if rank == 0:
         cpu = cpu_baseline(args, clip) if (world == 1 and not args.no_cpu_baseline) else None
@@ -639,6 +738,7 @@ def run_ours(args, rank, world, device):
             "mpixel_per_s": round(value * 256 / 1e6, 1),
             "learned": learned,
             "batched": batched,
+            "longrange": longrange,
         }
     ctx.close()
     return out
@@ -769,6 +869,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-clip leg")
+    ap.add_argument("--no-longrange", action="store_true", help="skip the long-range pan leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()

@@ -203,6 +203,14 @@ int vc1cu_measure_int32_peak(vc1cu_ctx* ctx, double* ops_per_second);
 /* Measures this device's FP64 throughput (flops/s, a fused multiply-add counted as two) with a
  * dependency-free FMA kernel: the denominator of the transform kernel's roofline. */
 int vc1cu_measure_fp64_peak(vc1cu_ctx* ctx, double* flops_per_second);
+/* The index-checked build of this library (libvc1cu_checked.so, compiled with
+ * -DVC1CU_INDEX_CHECK) tests every guarded access of the analysis kernels against its buffer
+ * (search window, stage key array, first-visit bitset, neighbour, candidate and signature
+ * tables, work items, window staging), counts violations and skips them. This returns the count
+ * and the first violation (site << 40 | index, sites as in vc1cu_core.cu's IndexSite) since the
+ * last reset, process-wide; with reset != 0 it clears them. Other builds return
+ * VC1CU_ERR_UNSUPPORTED. */
+int vc1cu_debug_index_faults(unsigned int* count, unsigned long long* first, int reset);
 
 /* Fills the defaults of vc1_param_default for a width x height raster. */
 void vc1cu_params_default(vc1cu_params* p, int width, int height);

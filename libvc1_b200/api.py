@@ -24,7 +24,8 @@ from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, IcPa
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
-_LIB = None
+CHECKED_LIB_PATH = os.path.join(_HERE, "libvc1cu_checked.so")  # the index-checked build
+_LIBS = {}
 
 # Every entry point declared in include/vc1cu.h.
 EXPORTS = (
@@ -33,7 +34,7 @@ EXPORTS = (
     "vc1cu_score_motion_batch_law", "vc1cu_upload_frame", "vc1cu_download_frame", "vc1cu_analyze_p_core",
     "vc1cu_core_passes", "vc1cu_read_result", "vc1cu_synchronize", "vc1cu_motion_compensate",
     "vc1cu_forward_quant", "vc1cu_forward_quant_device", "vc1cu_set_timing", "vc1cu_timing_get", "vc1cu_stream",
-    "vc1cu_measure_int32_peak", "vc1cu_measure_fp64_peak", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
+    "vc1cu_measure_int32_peak", "vc1cu_measure_fp64_peak", "vc1cu_debug_index_faults", "vc1cu_global_motion_noalloc", "vc1cu_analyze_b_picture", "vc1cu_b_decide",
     "vc1cu_read_bresult", "vc1cu_estimate_intensity_comp", "vc1cu_estimate_intensity_batch",
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
@@ -57,10 +58,10 @@ class Pass(C.Structure):
 
 
 def load_library(path: str = LIB_PATH):
-    """Loads libvc1cu.so and declares its C signatures (no device work)."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
+    """Loads libvc1cu.so (or another build of it, e.g. CHECKED_LIB_PATH) and declares its C
+    signatures (no device work)."""
+    if path in _LIBS:
+        return _LIBS[path]
     if not os.path.exists(path):
         raise RuntimeError(f"{path} is missing: the CUDA backend must be built (__graft_entry__.build())")
     L = C.CDLL(path)
@@ -116,6 +117,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_stream.restype = vp
     L.vc1cu_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_measure_fp64_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
@@ -134,7 +136,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_scene_change_score.argtypes = [vp, PP, i32, i32, i32, C.c_double, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name)  # AttributeError if the library lacks a declared entry point
-    _LIB = L
+    _LIBS[path] = L
     return L
 
 
@@ -157,9 +159,10 @@ class CudaComputeContext:
 
     # --- VulkanComputeContext::create / device_name / device_index -----------------------
     @staticmethod
-    def create(requested_device: int = -1):
-        """Returns (context, "") or (None, error) like VulkanComputeContext::create."""
-        L = load_library()
+    def create(requested_device: int = -1, library: str | None = None):
+        """Returns (context, "") or (None, error) like VulkanComputeContext::create. `library`
+        selects another build of the backend (e.g. CHECKED_LIB_PATH)."""
+        L = load_library(library or LIB_PATH)
         h = C.c_void_p()
         rc = L.vc1cu_open(requested_device, C.byref(h))
         if rc:
@@ -250,6 +253,15 @@ class CudaComputeContext:
         v = C.c_double()
         self._check(self._L.vc1cu_measure_int32_peak(self._h, C.byref(v)))
         return v.value
+
+    def index_faults(self, reset: bool = True):
+        """(count, first site, first index) of the index-checked build's record; raises
+        Vc1cuError (VC1CU_ERR_UNSUPPORTED) on other builds."""
+        n, first = C.c_uint(), C.c_ulonglong()
+        rc = self._L.vc1cu_debug_index_faults(C.byref(n), C.byref(first), int(reset))
+        if rc:
+            raise Vc1cuError(rc, self._L.vc1cu_last_error(None).decode())
+        return n.value, first.value >> 40, first.value & ((1 << 40) - 1)
 
     def measure_fp64_peak(self) -> float:
         """FP64 flops per second of this device (FMA calibration kernel, an FMA counted as two)."""

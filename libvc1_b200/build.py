@@ -32,17 +32,27 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_cuda(force: bool = False, verbose: bool = False) -> str:
-    out = os.path.join(HERE, "libvc1cu.so")
+# Library variants: name -> (file, extra nvcc defines). "checked" is the index-checked build:
+# every guarded shared-memory, frame and table access of the analysis kernels is bounds-checked,
+# a violation is counted with its site and skipped (vc1cu_debug_index_faults reads the record).
+VARIANTS = {"default": ("libvc1cu.so", ()), "checked": ("libvc1cu_checked.so", ("-DVC1CU_INDEX_CHECK",))}
+
+
+def build_cuda(force: bool = False, verbose: bool = False, variant: str = "default", out: str | None = None,
+               defines=()) -> str:
+    name, vdefs = VARIANTS[variant]
+    out = out or os.path.join(HERE, name)
+    defines = tuple(vdefs) + tuple(defines)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))]
     deps.append(os.path.join(HERE, "..", "include", "vc1cu.h"))
     if not force and not _stale(out, deps):
         return out
     objs = []
     procs = []
+    tag = os.path.splitext(os.path.basename(out))[0]
     for src in CU_SOURCES:
-        obj = os.path.join(CSRC, "_" + src.replace(".cu", ".o"))
-        cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+        obj = os.path.join(CSRC, f"_{tag}_" + src.replace(".cu", ".o"))
+        cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", *defines,
                "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(-4, "-Xptxas=-v")
@@ -73,6 +83,7 @@ def build_synth(force: bool = False) -> str:
 def build_all(force: bool = False, verbose: bool = False):
     build_synth(force)
     build_cuda(force, verbose)
+    build_cuda(force, verbose, variant="checked")
 
 
 if __name__ == "__main__":

@@ -50,6 +50,7 @@ void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred,
 void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int n, unsigned long long* out,
                   cudaStream_t s);
 double measure_int32_peak(cudaStream_t s, int sms);
+int index_fault_record(unsigned int* count, unsigned long long* first, int reset);
 double measure_fp64_peak(cudaStream_t s, int sms);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
 cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
@@ -1848,6 +1849,13 @@ int vc1cu_measure_int32_peak(vc1cu_ctx* c, double* ops_per_second) {
         if (*ops_per_second <= 0.0) throw Fail{VC1CU_ERR_CUDA, "calibration kernel failed"};
         return VC1CU_OK;
     });
+}
+
+int vc1cu_debug_index_faults(unsigned int* count, unsigned long long* first, int reset) {
+    const int rc = index_fault_record(count, first, reset);
+    if (rc < 0) return fail(nullptr, VC1CU_ERR_UNSUPPORTED, "not an index-checked build (libvc1cu_checked.so)");
+    if (rc > 0) return fail(nullptr, VC1CU_ERR_CUDA, "reading the index-check record failed");
+    return VC1CU_OK;
 }
 
 int vc1cu_measure_fp64_peak(vc1cu_ctx* c, double* flops_per_second) {

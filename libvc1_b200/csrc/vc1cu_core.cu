@@ -54,11 +54,41 @@ extern __shared__ __align__(16) uint32_t g_smem32[];  // the same memory, 32-bit
 
 // Reference-window sampler: bytes read by direct index into the shared array (so always
 // shared-space loads). off: byte offset of the window; ww: row pitch; (wx0, wy0): origin.
+// ---- the index-checked build (-DVC1CU_INDEX_CHECK) ----------------------------------------
+// Every guarded access tests its index against the buffer it addresses. A violation is counted
+// with its site and index (the first one is kept) and the access is skipped: a read returns 0,
+// a write is dropped, a work item is abandoned. vc1cu_debug_index_faults reads the record. In
+// the default build the guards are the constant true.
+enum IndexSite : int {
+    kSiteWorkItem = 1,   // work item: pass index < npass, macroblock < the pass's raster
+    kSiteWindow = 2,     // search-window read (x, y) inside the staged window
+    kSiteKeys = 3,       // a stage's key slot < the key array's capacity
+    kSiteSeen = 4,       // first-visit bitset: (dx, dy) inside the bitset's square
+    kSiteNeighbour = 5,  // neighbour macroblock inside the raster
+    kSiteCands = 6,      // learned candidate of a macroblock inside the raster
+    kSiteSignature = 7,  // long-range signature cell inside the reference's lattice
+    kSiteStage = 8,      // window staging write inside the window
+};
+#ifdef VC1CU_INDEX_CHECK
+__device__ unsigned int g_index_faults;
+__device__ unsigned long long g_index_first;  // site << 40 | (index & (2^40 - 1)) of the first violation
+__device__ __noinline__ void index_fault(int site, long long index) {
+    if (atomicAdd(&g_index_faults, 1u) == 0)
+        atomicExch(&g_index_first, ((unsigned long long)site << 40) | ((unsigned long long)index & 0xFFFFFFFFFFull));
+}
+#define IDX_OK(cond, site, index) ((cond) || (index_fault((site), (long long)(index)), false))
+#else
+#define IDX_OK(cond, site, index) true
+#endif
+
 struct WinSampler {
     uint32_t off;
     int ww, wx0, wy0;
+    int wh = 1 << 30;  // rows staged (checked builds test reads against it)
     __device__ __forceinline__ int operator()(int x, int y) const {
-        return g_smem[off + (uint32_t)((y - wy0) * ww + (x - wx0))];
+        const int rx = x - wx0, ry = y - wy0;
+        if (!IDX_OK(rx >= 0 && ry >= 0 && rx < ww && ry < wh, kSiteWindow, (long long)ry * 65536 + rx)) return 0;
+        return g_smem[off + (uint32_t)(ry * ww + rx)];
     }
 };
 
@@ -111,6 +141,9 @@ struct Mb {
     WarpMem sm;
     int wx0, wy0, wp, wh;  // window origin (wx0 a multiple of 16), row pitch = width, height
     GlobSampler gref;
+#ifdef VC1CU_INDEX_CHECK
+    int keys_cap;  // capacity of m.sm.keys
+#endif
 };
 
 __device__ __forceinline__ bool win_inside(const Mb& m, int xa, int ya, int xb, int yb) {
@@ -424,7 +457,7 @@ __device__ __noinline__ uint64_t mb_sad_core(uint32_t ctx, int dx, int dy, int s
         else if (stride == 2) s = sad_packed<2>(c.cur_off, c.cur2_off, c.cur4_off, c.wp, base);
         else s = sad_packed<4>(c.cur_off, c.cur2_off, c.cur4_off, c.wp, base);
     } else if (fast) {
-        const WinSampler ws{c.win_off, c.wp, c.wx0, c.wy0};
+        const WinSampler ws{c.win_off, c.wp, c.wx0, c.wy0, c.wh};
         if (stride == 1) s = sad_int_loop<1>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
         else if (stride == 2) s = sad_int_loop<2>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
         else s = sad_int_loop<4>(ws, c.cur_off, c.x0, c.y0, dx, dy, c.aw, c.ah);
@@ -489,7 +522,7 @@ __device__ __noinline__ void sad_batch_core(uint32_t ctx, uint32_t mvs_off, int 
                 const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
                 const int nvis = imin(8, aw - c0);
                 if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1)) {
-                    part = sad_row8(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, cp, nvis);
+                    part = sad_row8(WinSampler{c.win_off, c.wp, c.wx0, c.wy0, c.wh}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, cp, nvis);
                 } else {
                     const PredRow<8> g8 = predict_row_glob<8>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + c0, by + r);
 #pragma unroll
@@ -536,7 +569,7 @@ __device__ __noinline__ void satd_batch_core(uint32_t ctx, uint32_t mvs_off, int
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
                 if (fast) {
-                    const int4 w4 = pred_row4(WinSampler{c.win_off, c.wp, c.wx0, c.wy0}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy);
+                    const int4 w4 = pred_row4(WinSampler{c.win_off, c.wp, c.wx0, c.wy0, c.wh}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy);
                     pred[0] = w4.x;
                     pred[1] = w4.y;
                     pred[2] = w4.z;
@@ -579,6 +612,7 @@ __device__ __forceinline__ void satd_batch(const DevParams& P, const Mb& m, cons
 
 __device__ __forceinline__ bool seen_test_set(uint32_t* bits, int r, int dx, int dy) {
     const int side = 2 * r + 1;
+    if (!IDX_OK(dx >= -r && dx <= r && dy >= -r && dy <= r, kSiteSeen, (long long)dy * 65536 + dx)) return true;
     const int bit = (dy + r) * side + (dx + r);
     const uint32_t mask = 1u << (bit & 31);
     return (atomicOr(&bits[bit >> 5], mask) & mask) != 0;
@@ -668,7 +702,7 @@ __device__ void umh_stage(const DevParams& P, const Mb& m, int n, int range, Gen
         c.y = iclamp(c.y, -range, range);
         uint64_t key = UINT64_MAX;
         if (!seen_test_set(m.sm.seen, range, c.x, c.y)) key = int_key(mb_sad(P, m, c.x, c.y, 2), c.x, c.y);
-        m.sm.keys[i] = key;
+        if (IDX_OK(i < m.keys_cap, kSiteKeys, i)) m.sm.keys[i] = key;
     }
     __syncwarp();
     top8_merge(m, n);
@@ -1055,7 +1089,8 @@ __device__ IntRes lr_extended(const DevParams& P, const Mb& m, const PassDesc& d
         uint64_t key = UINT64_MAX;
         if (i < n) {
             const int dx = (i % d.lr_nx) * 8 - m.x0, dy = (i / d.lr_nx) * 8 - m.y0;
-            if (dx >= b.xmin && dx <= b.xmax && dy >= b.ymin && dy <= b.ymax && !(iabs(dx) <= 32 && iabs(dy) <= 32)) {
+            if (dx >= b.xmin && dx <= b.xmax && dy >= b.ymin && dy <= b.ymax && !(iabs(dx) <= 32 && iabs(dy) <= 32) &&
+                IDX_OK(d.lr_sig != nullptr, kSiteSignature, i)) {
                 const uint64_t dist = sig_distance(want, __ldg(&d.lr_sig[i]));
                 key = (dist << 36) | ((uint64_t)(iabs(dx) + iabs(dy)) << 24) | ((uint64_t)(dy + 2048) << 12) |
                       (uint64_t)(dx + 2048);
@@ -1148,7 +1183,8 @@ __device__ __forceinline__ bool int_better(uint64_t ca, int ax, int ay, uint64_t
 __device__ IntRes learned_candidates(const DevParams& P, const Mb& m, const PassDesc& d, int range) {
     const Bounds b = bounds_px(range);
     const int k = m.lane >> 3, part = m.lane & 7;
-    int2 c = __ldg(&d.cands[(size_t)m.pos * kLearnK + k]);
+    int2 c = make_int2(0, 0);
+    if (IDX_OK(m.pos >= 0 && m.pos < P.mbw * P.mbh, kSiteCands, m.pos)) c = __ldg(&d.cands[(size_t)m.pos * kLearnK + k]);
     c.x = iclamp(c.x, b.xmin, b.xmax);
     c.y = iclamp(c.y, b.ymin, b.ymax);
     uint32_t s = 0;
@@ -1919,8 +1955,9 @@ __device__ __forceinline__ bool seed_before(int2 v, uint64_t c, int slot, const 
 __device__ void load_neighbours(const DevParams& P, const Mb& m, const DevResult& o) {
     const int q = m.lane < 16 ? (m.lane >> 2) : (m.lane & 3);
     const int nx = m.mx + (q == 0 || q == 1 ? -1 : (q == 2 ? 0 : 1)), ny = m.my - (q == 0 ? 0 : 1);
-    const bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
+    bool valid = nx >= 0 && ny >= 0 && nx < P.mbw;
     const int nb = ny * P.mbw + nx;
+    valid = valid && IDX_OK(nb >= 0 && nb < P.mbw * P.mbh, kSiteNeighbour, nb);
     if (m.lane < 16) m.sm.nb_bmv[m.lane] = valid ? __ldcg(&o.bmv[nb * 4 + (m.lane & 3)]) : make_int2(0, 0);
     else if (m.lane < 20) m.sm.nb_mv[q] = valid ? __ldcg(&o.mvs[nb]) : make_int2(0, 0);
     else if (m.lane < 24) m.sm.nb_intra[q] = valid ? (int)__ldcg(&o.intra[nb]) : 0;
@@ -2234,6 +2271,7 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
         const int gy = iclamp(m.wy0 + r, 0, P.H - 1), gx = m.wx0 + 16 * c;
         const uint8_t* row = ref.y + (size_t)gy * ref.pitch_y;
         uint8_t* dst = m.sm.win.get() + r * m.wp + 16 * c;
+        if (!IDX_OK(r < m.wh && 16 * c + 16 <= m.wp, kSiteStage, j)) continue;
         if (gx >= 0 && gx + 16 <= P.W) {
             cp_async16(dst, row + gx);
         } else {
@@ -2323,6 +2361,9 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
     m.lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     carve(m.sm, (uint32_t)(warp * wc.warp_bytes), wc);
+#ifdef VC1CU_INDEX_CHECK
+    m.keys_cap = wc.keys_cap;
+#endif
     const int range = P0.range, local_range = P0.local_range;  // one search configuration per launch
     for (;;) {
         unsigned item = 0;
@@ -2332,9 +2373,11 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
         const uint32_t code = __ldg(&items[item]);
         const int pi_idx = (int)(code >> 20);
         const int mbi = (int)(code & 0xFFFFFu);
+        if (!IDX_OK(pi_idx < npass, kSiteWorkItem, code)) continue;
         const PassDesc& d = passes[pi_idx];
         // the picture geometry of this item (every pass of a kCoreMulti launch has its own)
         const DevParams& P = (KIND & kCoreMulti) ? d.geom : P0;
+        if (!IDX_OK(mbi < P.mbw * P.mbh, kSiteWorkItem, code)) continue;
         m.d = &d;
         m.mx = mbi % P.mbw;
         m.my = mbi / P.mbw;
@@ -2864,6 +2907,32 @@ __global__ void totals_kernel(const __grid_constant__ DevParams P0, const PassDe
     }
 }
 
+}  // namespace vc1cu
+
+namespace vc1cu {
+// The index-checked build's record (count, first site << 40 | index); -1 in other builds.
+int index_fault_record(unsigned int* count, unsigned long long* first, int reset) {
+#ifdef VC1CU_INDEX_CHECK
+    unsigned int n = 0;
+    unsigned long long f = 0;
+    if (cudaMemcpyFromSymbol(&n, g_index_faults, sizeof n) != cudaSuccess) return 1;
+    if (cudaMemcpyFromSymbol(&f, g_index_first, sizeof f) != cudaSuccess) return 1;
+    if (count) *count = n;
+    if (first) *first = f;
+    if (reset) {
+        const unsigned int z = 0;
+        const unsigned long long zf = 0;
+        if (cudaMemcpyToSymbol(g_index_faults, &z, sizeof z) != cudaSuccess) return 1;
+        if (cudaMemcpyToSymbol(g_index_first, &zf, sizeof zf) != cudaSuccess) return 1;
+    }
+    return 0;
+#else
+    (void)count;
+    (void)first;
+    (void)reset;
+    return -1;
+#endif
+}
 }  // namespace vc1cu
 
 #ifdef VC1CU_PHASE_CLOCKS

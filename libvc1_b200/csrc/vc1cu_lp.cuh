@@ -2,8 +2,8 @@
 //
 // The network reads the current and reference pictures at quarter resolution (one sample per
 // 4x4 luma block, so a macroblock is 4x4 samples) together with the picture's dominant
-// translation g (found by an exhaustive search of the quarter-resolution pictures over the
-// search range), runs four 3x3 convolutions of 32 channels with ReLU (BF16 operands, FP32
+// translation g (a coarse-to-fine search: 1/16 resolution, then quarter resolution, then full
+// resolution at stride 2, each about 4x the previous level's answer), runs four 3x3 convolutions of 32 channels with ReLU (BF16 operands, FP32
 // accumulation in tensor memory, tcgen05.mma), mean-pools each macroblock's 16 samples and
 // maps them (a 32 -> 8 projection) to two hypotheses: "the block moves with the zero vector"
 // and "the block moves with g", each with a logit and a regressed offset. The K = 4

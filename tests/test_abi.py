@@ -75,3 +75,17 @@ def test_open_without_device_reports_error_not_crash():
         return
     ctx, err = api.CudaComputeContext.create(0)
     assert ctx is None and err
+
+
+def test_checked_build_exports_the_same_symbols():
+    """The index-checked build is a full copy of the library."""
+    lib = C.CDLL(api.CHECKED_LIB_PATH)
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_index_fault_record_only_in_the_checked_build():
+    lib = api.load_library()
+    n, first = C.c_uint(), C.c_ulonglong()
+    assert lib.vc1cu_debug_index_faults(C.byref(n), C.byref(first), 0) == 6  # VC1CU_ERR_UNSUPPORTED
+    assert b"index-checked" in lib.vc1cu_last_error(None)
