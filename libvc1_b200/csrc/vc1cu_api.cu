@@ -5,6 +5,7 @@
 // (src/vulkan_compute.cpp:30-45, :194-231), launch descriptors and counters. Every entry
 // point returns a status code and never throws; failures are reported, never replaced by a
 // CPU computation.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is reached through the runtime's entry point)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -103,6 +104,49 @@ constexpr size_t kMaxBatch = 64u * 65535u;   // VulkanComputeContext's candidate
 #endif
 constexpr int kSeededMixedRw = VC1CU_SEEDED_MIXED_RW;  // window radius of seeded Mixed-MV launches
 constexpr int kMinUnseededRw = 24;  // smallest window radius a tuned unseeded launch shrinks to
+#ifndef VC1CU_WINDOW_TMA
+#define VC1CU_WINDOW_TMA 1
+#endif
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// The tensor map of a frame's luma plane (W x H bytes, row pitch `pitch`) with a box of one
+// search window (wp x wh bytes). Requirements checked here: base 16-byte aligned, pitch a
+// multiple of 16, box sides 1..256, box width a multiple of 16 bytes; the kernel only issues a
+// copy whose x is a multiple of 16 and whose box lies inside the plane.
+bool encode_window_map(void* out128, const uint8_t* luma, int W, int H, int pitch, int wp, int wh) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || (reinterpret_cast<uintptr_t>(luma) & 15) || (pitch & 15) || wp < 16 || wp > 256 || (wp & 15) ||
+        wh < 1 || wh > 256 || W < wp || H < wh)
+        return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch};
+    const cuuint32_t box[2] = {(cuuint32_t)wp, (cuuint32_t)wh};
+    const cuuint32_t estr[2] = {1, 1};
+    CUtensorMap map;
+    const CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(luma), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    static_assert(sizeof(CUtensorMap) == 128, "CUtensorMap size");
+    std::memcpy(out128, &map, 128);
+    return true;
+}
 
 struct Status {
     int code;
@@ -900,24 +944,6 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
             c->counters.kernel_launches++;
         }
     }
-    // pass descriptors
-    if (c->passes_cap < n) {
-        if (c->d_passes) cudaFree(c->d_passes);
-        c->d_passes = nullptr;
-        c->passes_cap = 0;
-        void* d = nullptr;
-        ck(cudaMalloc(&d, sizeof(PassDesc) * n), "cudaMalloc(pass descriptors)");
-        c->d_passes = static_cast<PassDesc*>(d);
-        c->passes_cap = n;
-    }
-    // ordered on the context stream after any launch still reading the previous descriptors
-    {
-        void* hp = staging(c, sizeof(PassDesc) * n);
-        std::memcpy(hp, h.data(), sizeof(PassDesc) * n);
-        ck(cudaMemcpyAsync(c->d_passes, hp, sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
-           "cudaMemcpyAsync(pass descriptors)");
-        staging_mark(c);
-    }
     // window / bitset geometry
     WinCfg wc;
     if (learned) {
@@ -994,6 +1020,34 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
         if (warps < 1 || warps > ((kind & kCoreWide) ? 8 : 4) || (size_t)warps * wc.warp_bytes > (size_t)c->max_smem)
             throw Fail{VC1CU_ERR_ARG, "tuned warps do not fit this instantiation"};
         smem = (size_t)warps * wc.warp_bytes;
+    }
+    // the windows' tensor maps (the box is this launch's final window)
+    wc.tma = 0;
+    if (VC1CU_WINDOW_TMA && wc.wp <= 256 && wc.wh <= 256) {
+        wc.tma = 1;
+        for (int i = 0; i < n; ++i)
+            h[i].ref_tma = encode_window_map(h[i].ref_tmap, h[i].ref.y, h[i].geom.W, h[i].geom.H, h[i].ref.pitch_y, wc.wp,
+                                             wc.wh)
+                               ? 1
+                               : 0;
+    }
+    // pass descriptors, ordered on the context stream after any launch still reading the
+    // previous ones
+    if (c->passes_cap < n) {
+        if (c->d_passes) cudaFree(c->d_passes);
+        c->d_passes = nullptr;
+        c->passes_cap = 0;
+        void* d = nullptr;
+        ck(cudaMalloc(&d, sizeof(PassDesc) * n), "cudaMalloc(pass descriptors)");
+        c->d_passes = static_cast<PassDesc*>(d);
+        c->passes_cap = n;
+    }
+    {
+        void* hp = staging(c, sizeof(PassDesc) * n);
+        std::memcpy(hp, h.data(), sizeof(PassDesc) * n);
+        ck(cudaMemcpyAsync(c->d_passes, hp, sizeof(PassDesc) * n, cudaMemcpyHostToDevice, c->stream),
+           "cudaMemcpyAsync(pass descriptors)");
+        staging_mark(c);
     }
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "cudaFuncSetAttribute");
     int per_sm = 0;

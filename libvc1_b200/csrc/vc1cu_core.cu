@@ -130,6 +130,7 @@ struct WarpMem {
     SPtr<uint64_t> spec_satd;
     SPtr<SpecBlk> spec_blk;     // [5]
     SPtr<uint8_t> ctx;          // the macroblock's MbCtx
+    SPtr<uint64_t> tma_bar;     // mbarrier of the window's TMA copy
 };
 
 struct Mb {
@@ -141,6 +142,8 @@ struct Mb {
     WarpMem sm;
     int wx0, wy0, wp, wh;  // window origin (wx0 a multiple of 16), row pitch = width, height
     GlobSampler gref;
+    uint32_t tma_phase;    // parity of the window mbarrier's next phase
+    bool tma_pending;      // a TMA window copy is in flight
 #ifdef VC1CU_INDEX_CHECK
     int keys_cap;  // capacity of m.sm.keys
 #endif
@@ -2226,6 +2229,10 @@ __device__ void carve(WarpMem& s, uint32_t base, const WinCfg& wc) {
     s.seen.off = take(4 * (uint32_t)wc.seen_words);
     s.seen_full.off = take(4 * (uint32_t)wc.seen_words);
     s.cur.off = take(256);
+    s.tma_bar.off = take(8);
+    // the window starts on a 128-byte boundary of the shared address space (a TMA destination)
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(g_smem);
+    p = ((sbase + p + 127) & ~127u) - sbase;
     s.win.off = take((uint32_t)(wc.wp * wc.wh + 32));
 }
 
@@ -2234,7 +2241,7 @@ __host__ __device__ inline int warp_bytes_for(const WinCfg& wc) {
     return r(16 * kListCap) + r(8 * kListCap) * 2 + r(8 * 32) + r(8 * wc.keys_cap) + r(64) + r(8 * kListCap) +
            r(8 * 32) + r(128) + r(4 * kListCap) + r(128) + r(64) + r(64) + r(32) + r(32) + r(128) + r(16) +
            3 * r(8 * 40) + r(kSpecBlkBytes * 5) + r(kMbCtxBytes) +
-           2 * r(4 * wc.seen_words) + r(256) +
+           2 * r(4 * wc.seen_words) + r(256) + r(8) + 128 +
            r(wc.wp * wc.wh + 32);
 }
 
@@ -2247,9 +2254,62 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
 
+// ---- the window's TMA copy (cp.async.bulk.tensor on the reference's tensor map) ----------
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_bar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// Lane 0: orders the warp's earlier generic reads of the window before the async write, arms
+// the barrier with the box's bytes and issues the 2-D tensor copy of the box at (x, y).
+__device__ __forceinline__ void tma_window(uint32_t dst, const void* tmap, int x, int y, uint32_t bar, uint32_t bytes) {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ bool tma_bar_test(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Waits (bounded) for the window's TMA copy; on timeout records VC1CU_ERR_TIMEOUT with the work
+// item, aborts the launch and leaves the copy marked pending (drained before the kernel exits).
+__device__ void tma_wait(Mb& m, LaunchStatus* st, uint32_t code, int log2_limit) {
+    if (!m.tma_pending) return;
+    const uint32_t bar = m.sm.tma_bar.off + sh_addr(g_smem);
+    const long limit = 1L << log2_limit;
+    for (long it = 0; it < limit; ++it) {
+        if (tma_bar_test(bar, m.tma_phase)) {
+            m.tma_phase ^= 1u;
+            m.tma_pending = false;
+            __syncwarp();
+            return;
+        }
+        if (it > 64) __nanosleep(32);
+    }
+    if (m.lane == 0 && st) {
+        if (atomicCAS(&st->tcode, 0u, code + 1u) == 0u) st->tmask = 0x100u;  // 0x100: the window copy
+        atomicExch(&st->error, (int)VC1CU_ERR_TIMEOUT);
+        atomicExch(&st->abort, 1);
+        atomicAdd(&st->timeouts, 1u);
+    }
+}
+
 // Completes this thread's cp.async copies; the warp barrier makes every lane's copies
 // visible to the whole warp.
-__device__ __forceinline__ void window_wait() {
+__device__ __forceinline__ void window_wait(Mb& m, LaunchStatus* st, uint32_t code, int log2_limit) {
+    tma_wait(m, st, code, log2_limit);
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
 }
@@ -2263,6 +2323,16 @@ __device__ void load_window(const DevParams& P, Mb& m, const DevFrame& ref, int 
     m.wp = wc.wp;
     m.wx0 = (m.x0 + cdx - wc.rw - 1) & ~15;
     m.wy0 = m.y0 + cdy - wc.rw - 1;
+    // a window wholly inside the picture: one tensor copy (its x is a multiple of 16 bytes)
+    if (wc.tma && m.d->ref_tma && m.wx0 >= 0 && m.wy0 >= 0 && m.wx0 + m.wp <= P.W && m.wy0 + m.wh <= P.H &&
+        !m.tma_pending) {
+        __syncwarp();  // every lane's reads of the previous window are done
+        if (m.lane == 0)
+            tma_window(sh_addr(m.sm.win.get()), m.d->ref_tmap, m.wx0, m.wy0, sh_addr(m.sm.tma_bar.get()),
+                       (uint32_t)(m.wp * m.wh));
+        m.tma_pending = true;
+        return;
+    }
     const int cpr = m.wp >> 4;
     const int total = m.wh * cpr;
 #pragma unroll 4
@@ -2364,6 +2434,10 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
 #ifdef VC1CU_INDEX_CHECK
     m.keys_cap = wc.keys_cap;
 #endif
+    m.tma_phase = 0;
+    m.tma_pending = false;
+    if (wc.tma && m.lane == 0) tma_bar_init(sh_addr(m.sm.tma_bar.get()));
+    __syncwarp();
     const int range = P0.range, local_range = P0.local_range;  // one search configuration per launch
     for (;;) {
         unsigned item = 0;
@@ -2452,7 +2526,7 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
                 seed.y = iclamp(seed.y, qb.ymin, qb.ymax);
                 load_window(P, m, d.ref, floor_div4(seed.x), floor_div4(seed.y), wc);
                 publish_ctx(P, m);
-                window_wait();
+                window_wait(m, st, code, P.wait_log2);
                 PHASE_MARK(2);
                 sl = refine_prepare_ool<kDR>(m.sm.ctx.off, m.x0, m.y0, 16, 16, seed, range, one_mode, UINT64_MAX, true);
                 PHASE_MARK(3);
@@ -2501,7 +2575,7 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
                 const IntRes best = learned_candidates(P, m, d, range);
                 load_window(P, m, d.ref, best.dx, best.dy, wc);
                 publish_ctx(P, m);
-                window_wait();
+                window_wait(m, st, code, P.wait_log2);
                 learned = learned_descent(P, m, best, range, kLearnRw - 4);
                 if (m.lane == 0 && d.fallback) d.fallback[m.pos] = learned_falls_back(P, m, o, learned.cost) ? 1 : 0;
                 PHASE_MARK(2);
@@ -2518,7 +2592,7 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
         constexpr bool kLearned = (KIND & kCoreLearned) != 0;
         const bool no_wait = kLearned || d.no_wait;
         if (ok && !no_wait) ok = wait_neighbours(P, o, m.mx, m.my, m.lane, epoch, st, code);
-        window_wait();  // an unseeded pass's window copies (none pending otherwise)
+        window_wait(m, st, code, P.wait_log2);  // an unseeded pass's window copies (none pending otherwise)
         PHASE_MARK(5);
         if (ok) {
             if constexpr (kLearned) load_cand_neighbours(P, m, d);
@@ -2748,6 +2822,9 @@ __global__ void __launch_bounds__((KIND & kCoreWide) ? 256 : 128,
         __syncwarp();
         PHASE_MARK(11);
     }
+    // a window copy still in flight after a timed-out wait lands before the block's shared
+    // memory is released (bounded again)
+    if (m.tma_pending) tma_wait(m, nullptr, 0, 22);
 }
 
 // mean_region (:1578-1590) of one 8x8 region, by one thread.

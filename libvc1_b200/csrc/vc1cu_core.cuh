@@ -37,7 +37,10 @@ struct DevResult {
     unsigned long long* itotals;  // motion_sad, moved, frac, four, intra
 };
 
-struct PassDesc {
+struct alignas(64) PassDesc {
+    unsigned char ref_tmap[128];  // TMA descriptor (CUtensorMap) of ref's luma plane, box = the
+                                  // launch's window (wp x wh bytes); valid when ref_tma != 0
+    int ref_tma;
     DevFrame cur, ref;
     int mode, allow_intra;
     int pq;                // this picture's PQINDEX
@@ -96,6 +99,7 @@ struct WinCfg {
     int seen_words;
     int keys_cap;  // capacity of the per-stage key array
     int warp_bytes;
+    int tma;       // 1: windows wholly inside the picture are staged by one TMA tensor copy
 };
 
 // Arguments of one candidate-scoring launch (vc1cu_score_motion_batch[_law]).
