@@ -554,6 +554,51 @@ int vc1cu_forward_quant_device(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id
  */
 int vc1cu_fast_transform_types(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int pred_id, uint8_t* types);
 
+/* Configuration of the transform RD (the EncoderConfig fields and picture-level choices
+ * Vc1Encoder::choose_transform_mb reads, src/encoder_internal.h:258-266). */
+typedef struct {
+    int32_t trellis;                      /* 0 scalar, 1 fast bounded trellis (beam 4), 2 wide (beam 8) */
+    int32_t adaptive_quality;             /* perceptual lambda scale (src/encoder_aq.cpp:405-653) */
+    double aq_strength;
+    int32_t variable_transforms;          /* 0: every MB 8x8 */
+    int32_t extended_transform_signaling; /* 0: macroblock signaling only (no TTBLK choice) */
+    int32_t coding_set;                   /* the picture's inter AC coding set, 0..7 */
+    int32_t use_vlc;                      /* 0: every AC coefficient as Escape-3 */
+    int32_t dquantfrm;                    /* DQUANTFRM of the picture */
+    int32_t hrd_enabled;                  /* keeps scalar levels at MQUANT 1 */
+    int32_t frame_type;                   /* 0: per-MB choice; 1..4: frame-level TTFRM type */
+} vc1cu_trd_cfg;
+
+/* One macroblock's MbTransformDecision (src/encoder_internal.h:1013-1033). */
+typedef struct {
+    uint8_t type;                 /* 1 8x8, 2 8x4, 3 4x8, 4 4x4: the common type, or the first coded
+                                     parent's at block signaling */
+    uint8_t signal_level;         /* 0 macroblock (TTMB), 1 block (TTBLK), 2 frame (TTFRM) */
+    uint8_t cbp;                  /* Y0 Y1 Y2 Y3 U V, bit 5 = Y0 */
+    uint8_t parent_type[6];
+    uint8_t skip_mask[6];
+    uint8_t reserved;
+    uint32_t estimated_bits;      /* CBPCY + transform syntax + coefficients */
+    uint32_t parent_bits[6];      /* each parent's payload estimate (estimate_parent_payload_bits) */
+    double distortion;            /* sum of the parents' reconstruction SSE */
+    double parent_distortion[6];
+} vc1cu_tdecision;
+
+/*
+ * The transform RD of the default presets (Vc1Encoder::choose_transform_mb without the
+ * throughput shortcut, src/encoder_transform.cpp:1605-1780): for every MB of src_id against the
+ * prediction pred_id, the candidate transform types from the residual metrics, each evaluated on
+ * all six parents (forward transform, scalar or trellis quantisation (trellis_quantize,
+ * :1873-2088) with the perceptual lambda scale, inverse transform, reconstruction SSE and the
+ * coefficient/subblock bit estimate of the VC-1 VLC tables), the macroblock- against block-level
+ * signaling decision by D + lambda R, and the trellis re-evaluation of the winners. mquant: HOST
+ * array of mbw*mbh MQUANT values (NULL: PQINDEX everywhere). out: HOST array of mbw*mbh
+ * decisions; levels: HOST int16 [mbw*mbh][6][64] of the chosen quantised coefficients (each
+ * parent's partitions in their natural sub-rectangles of the 8x8 grid), or NULL. Synchronous.
+ */
+int vc1cu_choose_transform(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id, int pred_id,
+                           const uint8_t* mquant, vc1cu_tdecision* out, int16_t* levels);
+
 /*
  * The reconstruction a transform decision implies (evaluate_transform_parent,
  * src/encoder_transform.cpp:1569-1585): for every MB and parent block (Y0..Y3, U, V), the levels

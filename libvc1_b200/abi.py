@@ -243,3 +243,60 @@ class Intensity(C.Structure):
 
 class IcPass(C.Structure):
     _fields_ = [("cur_id", C.c_int32), ("ref_id", C.c_int32), ("mv_slot", C.c_int32)]
+
+
+class TrdCfg(C.Structure):
+    """vc1cu_trd_cfg: the transform RD's configuration (EncoderConfig fields and picture choices)."""
+    _fields_ = [("trellis", C.c_int32), ("adaptive_quality", C.c_int32), ("aq_strength", C.c_double),
+                ("variable_transforms", C.c_int32), ("extended_transform_signaling", C.c_int32),
+                ("coding_set", C.c_int32), ("use_vlc", C.c_int32), ("dquantfrm", C.c_int32), ("hrd_enabled", C.c_int32),
+                ("frame_type", C.c_int32)]
+
+
+def make_trd_cfg(**kw) -> TrdCfg:
+    """The default presets' values (trellis 1, AQ on at strength 1, variable transforms with
+    extended signaling, VLC coding) unless overridden; coding set 1 (high-motion inter)."""
+    c = TrdCfg()
+    c.trellis, c.adaptive_quality, c.aq_strength = 1, 1, 1.0
+    c.variable_transforms, c.extended_transform_signaling = 1, 1
+    c.coding_set, c.use_vlc, c.dquantfrm, c.hrd_enabled, c.frame_type = 1, 1, 0, 0, 0
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    return c
+
+
+class TDecisionC(C.Structure):
+    """vc1cu_tdecision: one macroblock's MbTransformDecision."""
+    _fields_ = [("type", C.c_uint8), ("signal_level", C.c_uint8), ("cbp", C.c_uint8), ("parent_type", C.c_uint8 * 6),
+                ("skip_mask", C.c_uint8 * 6), ("reserved", C.c_uint8), ("estimated_bits", C.c_uint32),
+                ("parent_bits", C.c_uint32 * 6), ("distortion", C.c_double), ("parent_distortion", C.c_double * 6)]
+
+
+# numpy view of an array of vc1cu_tdecision
+TDECISION_DTYPE = np.dtype({"names": ["type", "signal_level", "cbp", "parent_type", "skip_mask", "reserved",
+                                      "estimated_bits", "parent_bits", "distortion", "parent_distortion"],
+                            "formats": [np.uint8, np.uint8, np.uint8, (np.uint8, 6), (np.uint8, 6), np.uint8, np.uint32,
+                                        (np.uint32, 6), np.float64, (np.float64, 6)],
+                            "offsets": [TDecisionC.type.offset, TDecisionC.signal_level.offset, TDecisionC.cbp.offset,
+                                        TDecisionC.parent_type.offset, TDecisionC.skip_mask.offset,
+                                        TDecisionC.reserved.offset, TDecisionC.estimated_bits.offset,
+                                        TDecisionC.parent_bits.offset, TDecisionC.distortion.offset,
+                                        TDecisionC.parent_distortion.offset],
+                            "itemsize": C.sizeof(TDecisionC)})
+
+
+def tdecisions_differ(a: np.ndarray, b: np.ndarray) -> list[str]:
+    """Fields of two decision arrays that differ (doubles by bit pattern)."""
+    bad = []
+    for name in TDECISION_DTYPE.names:
+        if name == "reserved":
+            continue
+        x, y = a[name], b[name]
+        if x.dtype == np.float64:
+            if not np.array_equal(np.ascontiguousarray(x).view(np.uint64), np.ascontiguousarray(y).view(np.uint64)):
+                bad.append(name)
+        elif not np.array_equal(x, y):
+            bad.append(name)
+    return bad

@@ -20,7 +20,7 @@ import os
 import numpy as np
 
 from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, IcPass, Intensity, Timing, MV_QPEL,
-                  METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params, mbs_of)
+                  METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params, TDECISION_DTYPE, TrdCfg, mbs_of)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
@@ -39,7 +39,7 @@ EXPORTS = (
     "vc1cu_intensity_compensate", "vc1cu_scene_change_score", "vc1cu_b_predict", "vc1cu_reconstruct",
     "vc1cu_loop_filter_i", "vc1cu_loop_filter_p", "vc1cu_overlap_smooth", "vc1cu_store_signed",
     "vc1cu_estimate_intensity_enqueue", "vc1cu_estimate_intensity_collect",
-    "vc1cu_fast_transform_types", "vc1cu_debug_set_wait_limit", "vc1cu_debug_withhold_publish",
+    "vc1cu_fast_transform_types", "vc1cu_choose_transform", "vc1cu_debug_set_wait_limit", "vc1cu_debug_withhold_publish",
     "vc1cu_synth_frames", "vc1cu_lp_param_count", "vc1cu_lp_create", "vc1cu_lp_destroy", "vc1cu_lp_get_params",
     "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
@@ -118,6 +118,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_measure_int32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_measure_fp64_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
+    L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
@@ -452,6 +453,20 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_forward_quant(self._h, C.byref(params), src_id, pred_id, type_mask,
                                                 co.ctypes.data, lv.ctypes.data))
         return co, lv
+
+    def choose_transform(self, params: Params, cfg: TrdCfg, src_id: int, pred_id: int, mquant=None, levels=True):
+        """Vc1Encoder::choose_transform_mb for every MB (vc1cu_choose_transform): a structured array of
+        TDECISION_DTYPE per MB and, with levels, the chosen levels int16 [mb][6][64]."""
+        mbw, mbh = mbs_of(params)
+        out = np.zeros(mbw * mbh, TDECISION_DTYPE)
+        lv = np.zeros((mbw * mbh, 6, 64), np.int16) if levels else None
+        mq = None if mquant is None else np.ascontiguousarray(mquant, np.uint8).reshape(-1)
+        if mq is not None and mq.size != mbw * mbh:
+            raise ValueError("mquant needs one value per macroblock")
+        self._check(self._L.vc1cu_choose_transform(self._h, C.byref(params), C.byref(cfg), src_id, pred_id,
+                                                   None if mq is None else mq.ctypes.data, out.ctypes.data,
+                                                   None if lv is None else lv.ctypes.data))
+        return out, lv
 
     def fast_transform_types(self, params: Params, src_id: int, pred_id: int):
         """The throughput preset's transform type (1..4) of every MB of src_id against pred_id."""

@@ -53,6 +53,11 @@ void launch_score(const DevParams& P, const ScoreArgs& a, const int2* cands, int
 double measure_int32_peak(cudaStream_t s, int sms);
 int index_fault_record(unsigned int* count, unsigned long long* first, int reset);
 double measure_fp64_peak(cudaStream_t s, int sms);
+size_t trd_tables_bytes();
+void trd_fill_tables(void* host);
+cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
+                       const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
+                       int16_t* levels, cudaStream_t s);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
 cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  cudaStream_t s);
@@ -273,6 +278,9 @@ struct vc1cu_ctx {
     size_t lf_cap = 0;
     void* d_btypes = nullptr;  // per-block transform types of vc1cu_reconstruct
     size_t btypes_cap = 0;
+    void* d_trd_tab = nullptr;  // the transform RD's dense rate tables (built once)
+    void* d_trd = nullptr;      // its per-call buffers: MQUANT, decisions, levels, luma sum
+    size_t trd_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -1793,6 +1801,8 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_ic) cudaFree(c->d_ic);
     if (c->d_icdesc) cudaFree(c->d_icdesc);
     if (c->d_btypes) cudaFree(c->d_btypes);
+    if (c->d_trd_tab) cudaFree(c->d_trd_tab);
+    if (c->d_trd) cudaFree(c->d_trd);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
     if (c->d_gcopy) cudaFree(c->d_gcopy);
@@ -2562,6 +2572,57 @@ int vc1cu_fast_transform_types(vc1cu_ctx* c, const vc1cu_params* p, int src_id, 
         ck(cudaGetLastError(), "transform type launch");
         tm.stop(1);
         ck(cudaMemcpyAsync(types, d, mbs, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(types)");
+        sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id, int pred_id,
+                           const uint8_t* mquant, vc1cu_tdecision* out, int16_t* levels) {
+    return guarded(c, [&]() -> int {
+        if (!cfg || !out) throw Fail{VC1CU_ERR_ARG, "null configuration or output"};
+        if (cfg->trellis < 0 || cfg->trellis > 2 || cfg->coding_set < 0 || cfg->coding_set > 7 || cfg->frame_type < 0 ||
+            cfg->frame_type > 4)
+            throw Fail{VC1CU_ERR_ARG, "invalid transform RD configuration"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& fs = frame_slot(c, src_id);
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        if (mquant)
+            for (size_t i = 0; i < mbs; ++i)
+                if (mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 0 (PQINDEX) or 1..31"};
+        if (!c->d_trd_tab) {
+            std::vector<uint8_t> h(trd_tables_bytes());
+            trd_fill_tables(h.data());
+            void* d = nullptr;
+            ck(cudaMalloc(&d, h.size()), "cudaMalloc(transform RD tables)");
+            c->d_trd_tab = d;
+            ck(cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(tables)");
+            ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize(tables)");  // h is freed on return
+        }
+        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t b_sum = 256, b_mq = al(mbs), b_out = al(mbs * sizeof(vc1cu_tdecision)), b_lv = al(mbs * 384 * 2);
+        uint8_t* base = static_cast<uint8_t*>(ensure(c->d_trd, c->trd_cap, b_sum + b_mq + b_out + b_lv,
+                                                     "cudaMalloc(transform RD buffers)"));
+        auto* d_sum = reinterpret_cast<unsigned long long*>(base);
+        uint8_t* d_mq = base + b_sum;
+        auto* d_out = reinterpret_cast<vc1cu_tdecision*>(base + b_sum + b_mq);
+        auto* d_lv = reinterpret_cast<int16_t*>(base + b_sum + b_mq + b_out);
+        if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(mquant)");
+        Timer tm(c, kXform);
+        ck(launch_trd(P, fs.view(), fp.view(), c->d_trd_tab, mquant ? d_mq : nullptr, *cfg, d_sum, d_out,
+                      levels ? d_lv : nullptr, c->stream),
+           "transform RD launch");
+        tm.stop(2);
+        ck(cudaMemcpyAsync(out, d_out, mbs * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
+           "cudaMemcpyAsync(decisions)");
+        if (levels)
+            ck(cudaMemcpyAsync(levels, d_lv, mbs * 384 * 2, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(levels)");
         sync_checked(c);
         return VC1CU_OK;
     });

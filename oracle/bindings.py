@@ -369,6 +369,12 @@ class Reference:
         L.ref_bench_gop_multi.restype = u64
         L.ref_bench_gop_same.argtypes = L.ref_bench_gop_multi.argtypes
         L.ref_bench_gop_same.restype = u64
+        L.ref_choose_transform.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.ref_choose_transform.restype = None
+        L.ref_ac_direct_bits.argtypes = [i32, i32, i32, i32]
+        L.ref_ac_direct_bits.restype = i32
+        L.ref_ac_rate_bits.argtypes = [vp, i32, i32, i32, i32]
+        L.ref_ac_rate_bits.restype = i32
         self.p = p
         self._recent = collections.deque(maxlen=8)
         self.h = L.ref_encoder_new(C.byref(p), int(simd_auto))
@@ -568,6 +574,25 @@ class Reference:
                                             vpa([j[1].h for j in bjobs]), vpa([j[2].h for j in bjobs]),
                                             vpa([j[3].h for j in bjobs]), ia([j[4] for j in bjobs]),
                                             ia([j[5] for j in bjobs]), ia([j[6] for j in bjobs]), len(bjobs), threads)
+
+    def choose_transform(self, cfg, src, pred, mquant=None):
+        """Vc1Encoder::choose_transform_mb of every MB (ref_choose_transform): decisions as a
+        TDECISION_DTYPE array and the chosen levels int16 [mb][6][64]. cfg: abi.TrdCfg."""
+        from libvc1_b200.abi import TDECISION_DTYPE
+
+        mbw, mbh = mbs_of(self.p)
+        out = np.zeros(mbw * mbh, TDECISION_DTYPE)
+        lv = np.zeros((mbw * mbh, 6, 64), np.int16)
+        mq = None if mquant is None else np.ascontiguousarray(mquant, np.uint8).reshape(-1)
+        self.lib.ref_choose_transform(self.h, C.addressof(cfg), self._f(src), self._f(pred),
+                                      None if mq is None else mq.ctypes.data, out.ctypes.data, lv.ctypes.data)
+        return out, lv
+
+    def ac_direct_bits(self, coding_set, run, level, last):
+        return self.lib.ref_ac_direct_bits(coding_set, run, level, int(last))
+
+    def ac_rate_bits(self, coding_set, run, level, last):
+        return self.lib.ref_ac_rate_bits(self.h, coding_set, run, level, int(last))
 
     def bench_gop_same(self, pjobs, bjobs, threads):
         """Wall ns of the GPU arm's work on the reference's functions (ref_bench_gop_same): per P

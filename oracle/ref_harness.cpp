@@ -519,6 +519,62 @@ void ref_forward_quant(void* h, void* src, void* pred, int type_mask, double* co
 
 int ref_scalar_quantize_level(void* h, double coeff) { return E(h).scalar_quantize_level(coeff); }
 
+// Vc1Encoder::choose_transform_mb (encoder_transform.cpp:1605-1780) for every MB of src against
+// pred, with the handle's configuration and the transform RD fields of t (trellis, AQ, variable
+// transforms, extended signaling, HRD; the throughput shortcut off); mquant per MB (NULL: PQINDEX).
+void ref_choose_transform(void* h, const vc1cu_trd_cfg* t, void* src, void* pred, const uint8_t* mquant,
+                          vc1cu_tdecision* out, int16_t* levels) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.trellis = t->trellis;
+    c.adaptive_quality = t->adaptive_quality != 0;
+    c.aq_strength = t->aq_strength;
+    c.variable_transforms = t->variable_transforms != 0;
+    c.extended_transform_signaling = t->extended_transform_signaling != 0;
+    c.hrd_enabled = t->hrd_enabled != 0;
+    c.fast_transform_rdo = false;
+    Vc1Encoder e(c);
+    Vc1Encoder::TransformPicturePlan plan;
+    plan.frame_level = t->frame_type > 0;
+    plan.frame_type = static_cast<Vc1Encoder::TransformType>(t->frame_type > 0 ? t->frame_type : 1);
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            const auto d = e.choose_transform_mb(F(src), F(pred), mx, my, t->coding_set, t->use_vlc != 0,
+                                                 mquant ? mquant[pos] : 0, t->dquantfrm != 0,
+                                                 t->frame_type > 0 ? &plan : nullptr);
+            vc1cu_tdecision& o = out[pos];
+            std::memset(&o, 0, sizeof o);
+            o.type = static_cast<uint8_t>(d.type);
+            o.signal_level = static_cast<uint8_t>(d.signal_level == Vc1Encoder::TransformSignalLevel::Macroblock
+                                                      ? 0
+                                                      : (d.signal_level == Vc1Encoder::TransformSignalLevel::Block ? 1 : 2));
+            o.cbp = d.cbp;
+            o.estimated_bits = static_cast<uint32_t>(d.estimated_bits);
+            o.distortion = d.distortion;
+            for (int k = 0; k < 6; ++k) {
+                const auto& p = d.parents[static_cast<size_t>(k)];
+                o.parent_type[k] = static_cast<uint8_t>(p.type);
+                o.skip_mask[k] = p.skip_mask;
+                o.parent_bits[k] = static_cast<uint32_t>(p.estimated_bits);
+                o.parent_distortion[k] = p.distortion;
+                if (levels)
+                    for (int i = 0; i < 64; ++i) levels[(pos * 6 + k) * 64 + i] = p.qcoeff[static_cast<size_t>(i)];
+            }
+        }
+}
+
+// The direct AC code length (0: none) of (run, level, last) in coding set `set`
+// (Vc1Encoder::find_ac_vlc, encoder_entropy.cpp:182-192), and write_ac_coeff's lower envelope
+// used by the trellis (trellis_rate_bits_for_set, encoder_transform.cpp:1811-1841).
+int ref_ac_direct_bits(int set, int run, int level, int last) {
+    const auto* e = Vc1Encoder::find_ac_vlc(set, run, level, last != 0);
+    return e ? e->bits : 0;
+}
+int ref_ac_rate_bits(void* h, int set, int run, int level, int last) {
+    return E(h).trellis_rate_bits_for_set(run, level, last != 0, set);
+}
+
 // CPU baseline over pairs that each carry their own encoder configuration (e.g. per-picture
 // PQINDEX): analyze_p_picture + choose_transform_mb of the chosen prediction for every MB,
 // one pair per worker thread at a time. Returns wall ns.

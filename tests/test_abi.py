@@ -28,7 +28,8 @@ STRUCTS = {"Params": (abi.Params, "vc1cu_params"), "Mv": (abi.Mv, "vc1cu_mv"),
            "PAnalysisC": (abi.PAnalysisC, "vc1cu_panalysis"), "Counters": (abi.Counters, "vc1cu_counters"),
            "Timing": (abi.Timing, "vc1cu_timing"), "Pass": (api.Pass, "vc1cu_pass"),
            "BAnalysisC": (abi.BAnalysisC, "vc1cu_banalysis"), "BPass": (abi.BPass, "vc1cu_bpass"),
-           "Intensity": (abi.Intensity, "vc1cu_intensity"), "IcPass": (abi.IcPass, "vc1cu_icpass")}
+           "Intensity": (abi.Intensity, "vc1cu_intensity"), "IcPass": (abi.IcPass, "vc1cu_icpass"),
+           "TrdCfg": (abi.TrdCfg, "vc1cu_trd_cfg"), "TDecisionC": (abi.TDecisionC, "vc1cu_tdecision")}
 
 
 def test_struct_layouts_match_header(tmp_path):
