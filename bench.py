@@ -465,6 +465,44 @@ def longrange_leg(ctx, torch, reps, clips=8, frames=12):
             "psnr_sample": "QP-6 luma reconstruction of frame steps 1 and last of every clip"}
 
 
+def transform_rd_leg(ctx, run, clip, pictures=4):
+    """The default presets' transform RD (vc1cu_choose_transform: candidate types, trellis with
+    the perceptual lambda scale, bit estimates, macroblock/block signaling) on the step's first
+    P pictures against their final Mixed-MV predictions (frame slots the step left), through the
+    C ABI with the decisions and levels copied back; and the reference's choose_transform_mb on
+    one of those pictures on one host thread, compared bit for bit."""
+    import time
+
+    from libvc1_b200.abi import make_trd_cfg, tdecisions_differ
+
+    cfg = make_trd_cfg()
+    pics = run.pics[:pictures]
+    ctx.choose_transform(params(pics[0][2]), cfg, pics[0][0], 3500)  # tables and buffers
+    t0 = time.perf_counter()
+    results = [ctx.choose_transform(params(pq), cfg, t, 3500 + i) for i, (t, _r, pq) in enumerate(pics)]
+    dt = time.perf_counter() - t0
+    out = {"workload": f"{len(pics)} 1080p P pictures of the step against their Mixed-MV predictions; trellis 1, "
+                       "AQ strength 1, variable transforms with TTBLK signaling, coding set 1",
+           "mb_per_s": round(len(pics) * MBS / dt, 1), "ms_per_picture": round(1e3 * dt / len(pics), 2),
+           "timing": "wall clock of synchronous C-ABI calls, decisions and levels copied to the host"}
+    try:
+        from oracle import Reference, ref_available
+    except Exception:  # pragma: no cover
+        return out
+    if not ref_available():
+        return out
+    t, _r, pq = pics[0]
+    pred = ctx.download_frame(3500, W, H)
+    R = Reference(params(pq), simd_auto=True)
+    t0 = time.perf_counter()
+    want, wlv = R.choose_transform(cfg, clip.frame(t), pred)
+    dt_ref = time.perf_counter() - t0
+    got, glv = results[0]
+    out["reference_one_thread_mb_per_s"] = round(MBS / dt_ref, 1)
+    out["matches_reference"] = tdecisions_differ(got, want) == [] and bool(np.array_equal(glv, wlv))
+    return out
+
+
 def batched_clips(n_odd_seed=7):
     """The batched workload's 48 clips: (coded width, height, display width, height, seed):
     16 at 640x360, 16 at 1280x720, 8 at 1920x1080 and 8 of odd display sizes with widths in
@@ -700,6 +738,11 @@ def run_ours(args, rank, world, device):
     longrange = None
     if not args.no_longrange and world == 1:
         longrange = longrange_leg(ctx, torch, reps=min(args.steps, 2))
+    transform_rd = None
+    if not args.no_transform_rd and world == 1:
+        run.step()  # the step's predictions back in their frame slots
+        ctx.synchronize()
+        transform_rd = transform_rd_leg(ctx, run, clip)
     out = None
     if rank == 0:
         cpu = cpu_baseline(args, clip) if (world == 1 and not args.no_cpu_baseline) else None
@@ -739,6 +782,7 @@ def run_ours(args, rank, world, device):
             "learned": learned,
             "batched": batched,
             "longrange": longrange,
+            "transform_rd": transform_rd,
         }
     ctx.close()
     return out
@@ -870,6 +914,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-clip leg")
     ap.add_argument("--no-longrange", action="store_true", help="skip the long-range pan leg")
+    ap.add_argument("--no-transform-rd", action="store_true", help="skip the transform RD leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()
