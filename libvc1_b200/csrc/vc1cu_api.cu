@@ -37,6 +37,8 @@ cudaError_t launch_core(int kind, int grid, int block, size_t smem, cudaStream_t
 __global__ void totals_kernel(const __grid_constant__ DevParams P, const PassDesc* passes, int npass);
 cudaError_t launch_learned_merge(const DevResult& dst, const DevResult& src, const uint8_t* only, int mbs,
                                  cudaStream_t s);
+cudaError_t launch_subpel_planes(const uint8_t* ref, int pitch, int W, int H, int rnd, int bilinear, uint32_t phase_mask,
+                                 uint8_t* out, int opitch, int border, long long stride, cudaStream_t s);
 int warp_bytes_for_host(const WinCfg& wc);
 struct GState;
 size_t gstate_bytes();
@@ -112,6 +114,10 @@ constexpr int kMinUnseededRw = 24;  // smallest window radius a tuned unseeded l
 #ifndef VC1CU_WINDOW_TMA
 #define VC1CU_WINDOW_TMA 1
 #endif
+#ifndef VC1CU_SUBPEL_PLANES
+#define VC1CU_SUBPEL_PLANES 1
+#endif
+constexpr int kSubpelBorder = 32;  // sub-pel planes extend this far beyond the picture
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -278,6 +284,8 @@ struct vc1cu_ctx {
     size_t lf_cap = 0;
     void* d_btypes = nullptr;  // per-block transform types of vc1cu_reconstruct
     size_t btypes_cap = 0;
+    void* d_sp = nullptr;       // sub-pel prediction planes of the current launch's references
+    size_t sp_cap = 0;
     void* d_trd_tab = nullptr;  // the transform RD's dense rate tables (built once)
     void* d_trd = nullptr;      // its per-call buffers: MQUANT, decisions, levels, luma sum
     size_t trd_cap = 0;
@@ -1038,6 +1046,56 @@ int launch_group(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_pass* passes, 
                                              wc.wh)
                                ? 1
                                : 0;
+    }
+    // Sub-pel prediction planes, one set per (reference, rounding, filter) of the launch, built
+    // before it on the context stream: every candidate's interpolated rows are then read, not
+    // recomputed per candidate and macroblock (the phases each set needs: all 15 for the bicubic
+    // modes, whose SAD batches may score odd seeds; the three half-pel ones for the bilinear mode,
+    // which rejects odd vectors).
+    if (VC1CU_SUBPEL_PLANES && P.subpel) {
+        struct Key {
+            const uint8_t* ref;
+            int W, H, pitch, rnd, bil;
+            uint32_t mask;
+            size_t off, stride;
+            int opitch;
+        };
+        std::vector<Key> keys;
+        std::vector<int> key_of(n);
+        for (int i = 0; i < n; ++i) {
+            const int bil = h[i].mode == VC1CU_MV_HPEL_BILINEAR ? 1 : 0;
+            const uint32_t mask = bil ? 0x504u : 0xFFFEu;
+            int k = 0;
+            while (k < (int)keys.size() && !(keys[k].ref == h[i].ref.y && keys[k].rnd == h[i].geom.rnd && keys[k].bil == bil))
+                ++k;
+            if (k == (int)keys.size())
+                keys.push_back(Key{h[i].ref.y, h[i].geom.W, h[i].geom.H, h[i].ref.pitch_y, h[i].geom.rnd, bil, 0u, 0, 0, 0});
+            keys[k].mask |= mask;
+            key_of[i] = k;
+        }
+        size_t total = 0;
+        for (auto& k : keys) {
+            k.opitch = ((k.W + 2 * kSubpelBorder + 15) & ~15) + 16;
+            k.stride = (size_t)k.opitch * (size_t)(k.H + 2 * kSubpelBorder);
+            k.off = total;
+            total += 16 * k.stride;
+        }
+        if (c->capturing && c->sp_cap < total)
+            throw Fail{VC1CU_ERR_STATE, "run this launch once before capturing it (sub-pel plane pool too small)"};
+        uint8_t* pool = static_cast<uint8_t*>(ensure(c->d_sp, c->sp_cap, total, "cudaMalloc(sub-pel planes)"));
+        for (const auto& k : keys) {
+            ck(launch_subpel_planes(k.ref, k.pitch, k.W, k.H, k.rnd, k.bil, k.mask, pool + k.off, k.opitch, kSubpelBorder,
+                                    (long long)k.stride, c->stream),
+               "subpel_plane_kernel launch");
+            c->counters.kernel_launches++;
+        }
+        for (int i = 0; i < n; ++i) {
+            const Key& k = keys[key_of[i]];
+            h[i].sp_planes = pool + k.off;
+            h[i].sp_pitch = k.opitch;
+            h[i].sp_border = kSubpelBorder;
+            h[i].sp_stride = (long long)k.stride;
+        }
     }
     // pass descriptors, ordered on the context stream after any launch still reading the
     // previous ones
@@ -1802,6 +1860,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_icdesc) cudaFree(c->d_icdesc);
     if (c->d_btypes) cudaFree(c->d_btypes);
     if (c->d_trd_tab) cudaFree(c->d_trd_tab);
+    if (c->d_sp) cudaFree(c->d_sp);
     if (c->d_trd) cudaFree(c->d_trd);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);

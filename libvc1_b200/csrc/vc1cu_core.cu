@@ -439,6 +439,9 @@ struct MbCtx {
     int subpel, fast_subpel, subpel_range, me_quality, mvrange, mant_bits, lam_s;
     uint64_t lam_m;
     uint32_t batch, cost, satd;  // the warp's shortlist buffers
+    const uint8_t* sp;           // the pass's sub-pel prediction planes (nullptr: none)
+    int sp_pitch, sp_border;
+    long long sp_stride;
 };
 constexpr int kMbCtxBytes = 192;
 static_assert(sizeof(MbCtx) <= kMbCtxBytes, "MbCtx layout");
@@ -493,9 +496,29 @@ __device__ __forceinline__ bool ctx_inside(const MbCtx& c, int xa, int ya, int x
     return xa >= c.wx0 && ya >= c.wy0 && xb < c.wx0 + c.wp && yb < c.wy0 + c.wh;
 }
 
+// The sub-pel plane row of phase (hm, vm) at integer origin (sx, sy), when its n samples lie in
+// the planes (nullptr otherwise).
+__device__ __forceinline__ const uint8_t* sp_row(const MbCtx& c, int hm, int vm, int sx, int sy, int n) {
+    if (!c.sp || !(hm | vm)) return nullptr;
+    const int b = c.sp_border;
+    if (sx < -b || sx + n > c.g.W + b || sy < -b || sy >= c.g.H + b) return nullptr;
+    return c.sp + (long long)(vm * 4 + hm) * c.sp_stride + (long long)(sy + b) * c.sp_pitch + (sx + b);
+}
+
+// n <= 8 bytes of a plane row as two little-endian words (aligned loads and funnel shifts; the
+// row continues at least 3 bytes past any origin sp_row accepts)
+__device__ __forceinline__ void sp_load8(const uint8_t* p, uint32_t& lo, uint32_t& hi) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3));
+    const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8;
+    const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = sh ? __ldg(w + 2) : 0u;
+    lo = __funnelshift_r(w0, w1, sh);
+    hi = __funnelshift_r(w1, w2, sh);
+}
+
 // SAD of n candidates of block (bx,by,bw,bh) (bw,bh in {8,16}) under the CPU law, written
 // to out[]. Each candidate's block is split into 8-pixel row segments over bh*bw/8 lanes.
-// One out-of-line copy serves every call site.
+// One out-of-line copy serves every call site. Sub-pel rows come from the pass's prediction
+// planes where they cover them, else are interpolated from the window or the frame.
 __device__ __noinline__ void sad_batch_core(uint32_t ctx, uint32_t mvs_off, int n, int bx, int by,
                                             int bw, int bh, int mode, uint32_t out_off) {
     const MbCtx& c = mbctx(ctx);
@@ -524,7 +547,12 @@ __device__ __noinline__ void sad_batch_core(uint32_t ctx, uint32_t mvs_off, int 
                 const int ix = floor_div4(mv.x), iy = floor_div4(mv.y);
                 const uint32_t cp = c.cur_off + (uint32_t)((cy + r) * 16 + cx + c0);
                 const int nvis = imin(8, aw - c0);
-                if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1)) {
+                const uint8_t* pr = nvis == 8 ? sp_row(c, mv.x - 4 * ix, mv.y - 4 * iy, bx + c0 + ix, by + r + iy, 8) : nullptr;
+                if (pr) {
+                    uint32_t lo, hi;
+                    sp_load8(pr, lo, hi);
+                    part = __vsadu4(lo, g_smem32[cp >> 2]) + __vsadu4(hi, g_smem32[(cp >> 2) + 1]);
+                } else if (ctx_inside(c, bx + ix - 1, by + iy - 1, bx + ix + bw + 1, by + iy + bh + 1)) {
                     part = sad_row8(WinSampler{c.win_off, c.wp, c.wx0, c.wy0, c.wh}, bil, P.rnd, mv.x, mv.y, bx + c0, by + r, cp, nvis);
                 } else {
                     const PredRow<8> g8 = predict_row_glob<8>(c.gref, c.gpitch, P.W, P.H, bil, P.rnd, mv.x, mv.y, bx + c0, by + r);
@@ -568,10 +596,19 @@ __device__ __noinline__ void satd_batch_core(uint32_t ctx, uint32_t mvs_off, int
             // rows one at a time (one copy of the interpolation code), row-transformed and
             // rotated through four registers for the column stage
             int4 r0 = make_int4(0, 0, 0, 0), r1 = r0, r2 = r0, r3 = r0;
+            const uint8_t* pr = sp_row(c, mv.x - 4 * ix, mv.y - 4 * iy, bx + tx + ix, by + ty + iy, 4);
+            if (pr && !sp_row(c, mv.x - 4 * ix, mv.y - 4 * iy, bx + tx + ix, by + ty + iy + 3, 4)) pr = nullptr;
 #pragma unroll 1
             for (int yy = 0; yy < 4; ++yy) {
                 int pred[4];
-                if (fast) {
+                if (pr) {
+                    uint32_t lo, hi;
+                    sp_load8(pr + (long long)yy * c.sp_pitch, lo, hi);
+                    pred[0] = lo & 255;
+                    pred[1] = (lo >> 8) & 255;
+                    pred[2] = (lo >> 16) & 255;
+                    pred[3] = lo >> 24;
+                } else if (fast) {
                     const int4 w4 = pred_row4(WinSampler{c.win_off, c.wp, c.wx0, c.wy0, c.wh}, bil, P.rnd, mv.x, mv.y, bx + tx, by + ty + yy);
                     pred[0] = w4.x;
                     pred[1] = w4.y;
@@ -1758,6 +1795,10 @@ __device__ void publish_ctx(const DevParams& P, const Mb& m) {
         r.batch = m.sm.batch.off;
         r.cost = m.sm.batch_cost.off;
         r.satd = m.sm.list_satd.off;
+        r.sp = m.d->sp_planes;
+        r.sp_pitch = m.d->sp_pitch;
+        r.sp_border = m.d->sp_border;
+        r.sp_stride = m.d->sp_stride;
     }
     __syncwarp();
 }
@@ -2910,6 +2951,26 @@ __global__ void learned_merge_kernel(DevResult dst, DevResult src, const uint8_t
     dst.ratio[i] = src.ratio[i];
     dst.dl[i] = src.dl[i];
     dst.dc[i] = src.dc[i];
+}
+
+// The sub-pel prediction planes of a reference picture: plane (vm * 4 + hm) holds, at (y + border)
+// * opitch + x + border, the prediction of phase (hm, vm) whose integer origin is (x, y) (predict_row,
+// clamped sampling), for the phases in phase_mask.
+__global__ void subpel_plane_kernel(const uint8_t* ref, int pitch, int W, int H, int rnd, int bilinear,
+                                    uint32_t phase_mask, uint8_t* out, int opitch, int border, long long stride) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, ph = blockIdx.z;
+    if (!((phase_mask >> ph) & 1) || x >= W + 2 * border) return;
+    const GlobSampler gs{ref, pitch, W, H};
+    int v[1];
+    predict_row<1>(gs, bilinear != 0, rnd, ph & 3, ph >> 2, x - border, y - border, v);
+    out[ph * stride + (long long)y * opitch + x] = (uint8_t)v[0];
+}
+
+cudaError_t launch_subpel_planes(const uint8_t* ref, int pitch, int W, int H, int rnd, int bilinear, uint32_t phase_mask,
+                                 uint8_t* out, int opitch, int border, long long stride, cudaStream_t s) {
+    const dim3 grid((unsigned)((W + 2 * border + 127) / 128), (unsigned)(H + 2 * border), 16);
+    subpel_plane_kernel<<<grid, 128, 0, s>>>(ref, pitch, W, H, rnd, bilinear, phase_mask, out, opitch, border, stride);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_learned_merge(const DevResult& dst, const DevResult& src, const uint8_t* only, int mbs,

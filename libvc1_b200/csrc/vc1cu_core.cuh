@@ -41,6 +41,13 @@ struct alignas(64) PassDesc {
     unsigned char ref_tmap[128];  // TMA descriptor (CUtensorMap) of ref's luma plane, box = the
                                   // launch's window (wp x wh bytes); valid when ref_tma != 0
     int ref_tma;
+    // Sub-pel prediction planes of ref for this pass's filter and rounding (nullptr: none): the
+    // prediction of phase (hm, vm) whose integer origin is (x, y), for x in [-sp_border, W +
+    // sp_border) and y likewise, at sp_planes + (vm * 4 + hm) * sp_stride + (y + sp_border) *
+    // sp_pitch + x + sp_border.
+    const uint8_t* sp_planes;
+    int sp_pitch, sp_border;
+    long long sp_stride;
     DevFrame cur, ref;
     int mode, allow_intra;
     int pq;                // this picture's PQINDEX
