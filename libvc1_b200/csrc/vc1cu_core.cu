@@ -2953,23 +2953,48 @@ __global__ void learned_merge_kernel(DevResult dst, DevResult src, const uint8_t
     dst.dc[i] = src.dc[i];
 }
 
+// The 4x4 clamped neighbourhood of an integer origin (columns x-1..x+2, rows y-1..y+2), which
+// holds every tap any phase of predict_row<1> reads there.
+struct NbrSampler {
+    int v[4][4];
+    int x0, y0;
+    __device__ __forceinline__ int operator()(int x, int y) const { return v[y - y0][x - x0]; }
+};
+
 // The sub-pel prediction planes of a reference picture: plane (vm * 4 + hm) holds, at (y + border)
 // * opitch + x + border, the prediction of phase (hm, vm) whose integer origin is (x, y) (predict_row,
-// clamped sampling), for the phases in phase_mask.
-__global__ void subpel_plane_kernel(const uint8_t* ref, int pitch, int W, int H, int rnd, int bilinear,
-                                    uint32_t phase_mask, uint8_t* out, int opitch, int border, long long stride) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, ph = blockIdx.z;
-    if (!((phase_mask >> ph) & 1) || x >= W + 2 * border) return;
-    const GlobSampler gs{ref, pitch, W, H};
-    int v[1];
-    predict_row<1>(gs, bilinear != 0, rnd, ph & 3, ph >> 2, x - border, y - border, v);
-    out[ph * stride + (long long)y * opitch + x] = (uint8_t)v[0];
+// clamped sampling), for the phases in phase_mask. One thread per origin loads its neighbourhood
+// once and evaluates every phase from it.
+template <bool BILINEAR>
+__global__ void subpel_plane_kernel(const uint8_t* ref, int pitch, int W, int H, int rnd, uint32_t phase_mask,
+                                    uint8_t* out, int opitch, int border, long long stride) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= W + 2 * border) return;
+    const int x = px - border, y = py - border;
+    NbrSampler n;
+    n.x0 = x - 1;
+    n.y0 = y - 1;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const uint8_t* row = ref + (size_t)iclamp(y - 1 + r, 0, H - 1) * pitch;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) n.v[r][k] = __ldg(row + iclamp(x - 1 + k, 0, W - 1));
+    }
+    uint8_t* o = out + (long long)py * opitch + px;
+#pragma unroll
+    for (int ph = 1; ph < 16; ++ph) {
+        if (!((phase_mask >> ph) & 1)) continue;
+        int v[1];
+        predict_row<1>(n, BILINEAR, rnd, ph & 3, ph >> 2, x, y, v);
+        o[ph * stride] = (uint8_t)v[0];
+    }
 }
 
 cudaError_t launch_subpel_planes(const uint8_t* ref, int pitch, int W, int H, int rnd, int bilinear, uint32_t phase_mask,
                                  uint8_t* out, int opitch, int border, long long stride, cudaStream_t s) {
-    const dim3 grid((unsigned)((W + 2 * border + 127) / 128), (unsigned)(H + 2 * border), 16);
-    subpel_plane_kernel<<<grid, 128, 0, s>>>(ref, pitch, W, H, rnd, bilinear, phase_mask, out, opitch, border, stride);
+    const dim3 grid((unsigned)((W + 2 * border + 127) / 128), (unsigned)(H + 2 * border));
+    if (bilinear) subpel_plane_kernel<true><<<grid, 128, 0, s>>>(ref, pitch, W, H, rnd, phase_mask, out, opitch, border, stride);
+    else subpel_plane_kernel<false><<<grid, 128, 0, s>>>(ref, pitch, W, H, rnd, phase_mask, out, opitch, border, stride);
     return cudaGetLastError();
 }
 
