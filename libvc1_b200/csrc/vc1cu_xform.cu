@@ -114,29 +114,41 @@ __device__ __forceinline__ int quantize_level(const DevParams& P, double coeff) 
     return sign * best;
 }
 
-// One thread per (type, MB, parent, partition). Output layout [type][mb][parent][64].
+// Threads per (MB, parent) of transform type t: one per partition row (partitions x rows).
+__device__ __forceinline__ int xform_threads(int t) { return t == 1 || t == 2 ? 8 : 16; }
+
+// One thread per (type, MB, parent, partition, transform row a): the row of the vertical stage
+// and the outputs of frequency a (an 8x8 output column, transposed; a rectangle's row). Every
+// product and sum is the reference's, in its order. Output layout [type][mb][parent][64].
 __global__ void xform_kernel(const __grid_constant__ DevParams P, DevFrame src, DevFrame pred, int type_mask, double* coeffs,
                              int16_t* levels) {
     const int mbs = P.mbw * P.mbh;
-    // partitions per parent for each of the up-to-4 types, in type order
-    int types[4], nt = 0;
-    for (int t = 1; t <= 4; ++t)
-        if (type_mask & (1 << (t - 1))) types[nt++] = t;
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long per_type = (long)mbs * 6 * 4;  // up to 4 partitions
-    if (idx >= per_type * nt) return;
-    const int ti = (int)(idx / per_type);
-    const long rem = idx % per_type;
-    const int part = (int)(rem & 3);
-    const int k = (int)((rem >> 2) % 6);
-    const int mb = (int)((rem >> 2) / 6);
-    const int t = types[ti];
-    const int np = t == 1 ? 1 : (t == 4 ? 4 : 2);
-    if (part >= np) return;
-    int ox = 0, oy = 0, bw = 8, bh = 8;
-    if (t == 2) { bh = 4; oy = part * 4; }
-    else if (t == 3) { bw = 4; ox = part * 4; }
-    else if (t == 4) { bw = 4; bh = 4; ox = (part & 1) * 4; oy = (part >> 1) * 4; }
+    long off = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int ti = -1, t = 0, nt = 0;
+    for (int tt = 1; tt <= 4; ++tt) {
+        if (!(type_mask & (1 << (tt - 1)))) continue;
+        const long n = (long)mbs * 6 * xform_threads(tt);
+        if (ti < 0) {
+            if (off < n) {
+                ti = nt;
+                t = tt;
+            } else {
+                off -= n;
+            }
+        }
+        ++nt;
+    }
+    if (ti < 0) return;
+    const int per = xform_threads(t);
+    const int sub = (int)(off % per);
+    const long pk = off / per;
+    const int k = (int)(pk % 6), mb = (int)(pk / 6);
+    const int bh = (t == 2 || t == 4) ? 4 : 8, bw = (t == 3 || t == 4) ? 4 : 8;
+    const int part = sub / bh, a = sub % bh;
+    int ox = 0, oy = 0;
+    if (t == 2) oy = part * 4;
+    else if (t == 3) ox = part * 4;
+    else if (t == 4) { ox = (part & 1) * 4; oy = (part >> 1) * 4; }
     const int mx = mb % P.mbw, my = mb / P.mbw;
     const bool chroma = k >= 4;
     const uint8_t* sp = chroma ? (k == 4 ? src.u : src.v) : src.y;
@@ -146,43 +158,37 @@ __global__ void xform_kernel(const __grid_constant__ DevParams P, DevFrame src, 
     const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
     const int x0 = bx * 8 + ox, y0 = by * 8 + oy;
     const size_t base = (((size_t)ti * mbs + mb) * 6 + k) * 64;
+    // output b of this thread's frequency a: transposed for 8x8, row-major for rectangles
+    auto out_pos = [&](int b) {
+        return (bw == 8 && bh == 8) ? base + (size_t)(oy + b) * 8 + ox + a : base + (size_t)(oy + a) * 8 + ox + b;
+    };
     if (x0 >= w || y0 >= h || x0 + bw <= 0 || y0 + bh <= 0) {
         // a partition wholly outside the crop codes nothing (encoder_transform.cpp:1097)
-        for (int y = 0; y < bh; ++y)
-            for (int x = 0; x < bw; ++x) {
-                if (coeffs) coeffs[base + (oy + y) * 8 + ox + x] = 0.0;
-                if (levels) levels[base + (oy + y) * 8 + ox + x] = 0;
-            }
+        for (int b = 0; b < bw; ++b) {
+            if (coeffs) coeffs[out_pos(b)] = 0.0;
+            if (levels) levels[out_pos(b)] = 0;
+        }
         return;
     }
-    double r[8][8];
-    for (int y = 0; y < bh; ++y)
-        for (int x = 0; x < bw; ++x) {
+    double trow[8];
+    for (int x = 0; x < bw; ++x) {
+        double acc = 0.0;
+        for (int y = 0; y < bh; ++y) {
             const int sx = x0 + x, sy = y0 + y;
-            r[y][x] = (sx < 0 || sy < 0 || sx >= w || sy >= h)
-                          ? 0.0
-                          : (double)((int)__ldg(sp + (size_t)sy * spitch + sx) - (int)__ldg(pp + (size_t)sy * ppitch + sx));
+            const double r = (sx < 0 || sy < 0 || sx >= w || sy >= h)
+                                 ? 0.0
+                                 : (double)((int)__ldg(sp + (size_t)sy * spitch + sx) - (int)__ldg(pp + (size_t)sy * ppitch + sx));
+            acc = __dadd_rn(acc, __dmul_rn(bh == 8 ? c_k8[a][y] : c_k4[a][y], r));
         }
-    double tmp[8][8];
-    for (int a = 0; a < bh; ++a)
-        for (int x = 0; x < bw; ++x) {
-            double acc = 0.0;
-            for (int y = 0; y < bh; ++y) acc = __dadd_rn(acc, __dmul_rn(bh == 8 ? c_k8[a][y] : c_k4[a][y], r[y][x]));
-            tmp[a][x] = acc;
-        }
-    for (int a = 0; a < bh; ++a)
-        for (int b = 0; b < bw; ++b) {
-            double acc = 0.0;
-            for (int x = 0; x < bw; ++x) acc = __dadd_rn(acc, __dmul_rn(tmp[a][x], bw == 8 ? c_k8[b][x] : c_k4[b][x]));
-            // 8x8 output is transposed (c[row*8+col] = 1024*xform[col][row]), rectangles are not
-            const double c = __dmul_rn(1024.0, acc);
-            int row, col;
-            if (bw == 8 && bh == 8) { row = b; col = a; }
-            else { row = a; col = b; }
-            const size_t o = base + (size_t)(oy + row) * 8 + ox + col;
-            if (coeffs) coeffs[o] = c;
-            if (levels) levels[o] = (int16_t)quantize_level(P, c);
-        }
+        trow[x] = acc;
+    }
+    for (int b = 0; b < bw; ++b) {
+        double acc = 0.0;
+        for (int x = 0; x < bw; ++x) acc = __dadd_rn(acc, __dmul_rn(trow[x], bw == 8 ? c_k8[b][x] : c_k4[b][x]));
+        const double c = __dmul_rn(1024.0, acc);
+        if (coeffs) coeffs[out_pos(b)] = c;
+        if (levels) levels[out_pos(b)] = (int16_t)quantize_level(P, c);
+    }
 }
 
 // ---- inverse transform and reconstruction (encoder_transform.cpp:1058-1274, :1569-1585) ----
@@ -374,9 +380,9 @@ void launch_mc(const DevParams& P, const DevFrame& ref, const int2* mvs, const i
 
 void launch_xform(const DevParams& P, const DevFrame& src, const DevFrame& pred, int type_mask, double* coeffs,
                   int16_t* levels, cudaStream_t s) {
-    int nt = 0;
-    for (int t = 0; t < 4; ++t) nt += (type_mask >> t) & 1;
-    const long n = (long)P.mbw * P.mbh * 6 * 4 * nt;
+    long n = 0;
+    for (int t = 1; t <= 4; ++t)
+        if (type_mask & (1 << (t - 1))) n += (long)P.mbw * P.mbh * 6 * (t == 1 || t == 2 ? 8 : 16);
     if (!n) return;
     xform_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, src, pred, type_mask, coeffs, levels);
 }
