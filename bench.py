@@ -65,10 +65,12 @@ WORKLOAD = ("1080p IBBP analysis: 1920x1080 4:2:0, 60 frames, GOP 12 IBBP as the
             "pictures/step; P: 5 core passes + fade estimate + prediction + 4-size transform/quant; B: forward+backward "
             "core passes and "
             "the MB decision in qpel and hpel-bilinear mode; search +/-64, Mixed-MV, nonuniform QP 4-12")
-# DRAM bytes (read + write) of core_pass_kernel per launch on this workload: an ncu capture of the
-# first GOP's six core launches (119.6 MB in all) scaled by macroblocks to the five GOPs of a step
-# and divided over the step's six launches.
-CORE_DRAM_BYTES_PER_LAUNCH = 119.6e6 * 5 / 6  # ncu, first GOP (6 launches), scaled to the 5 GOPs of a step
+# DRAM bytes (read + write) of core_pass_kernel per launch on this workload, with the sub-pel
+# plane builds that precede each launch: an ncu capture of the first GOP's six core launches and
+# their plane builds (709.7 MB in all; the core launches re-read the 15 phase planes of each
+# reference) scaled by macroblocks to the five GOPs of a step and divided over the step's six
+# launches.
+CORE_DRAM_BYTES_PER_LAUNCH = 709.7e6 * 5 / 6  # ncu, first GOP (6 launches + planes), scaled to the 5 GOPs of a step
 P_PASSES = ("unseeded", "seeded_hpel", "seeded_bilinear", "seeded_mixed", "final_mixed_intra")
 B_PASSES = ("b_qpel_forward", "b_qpel_backward", "b_bilinear_forward", "b_bilinear_backward")
 XFORM_FLOPS_PER_MB = 51911.5
