@@ -505,6 +505,46 @@ def transform_rd_leg(ctx, run, clip, pictures=4):
     return out
 
 
+def mode_decision_leg(ctx, run, clip, pictures=4):
+    """The P picture's whole motion-mode decision (vc1cu_analyze_p_picture: quarter-pel seed pass,
+    three seeded mode passes, each candidate's motion bits and sampled transform RD, the final
+    pass in the chosen mode, the fade estimate and, when it is enabled, the compensated candidates)
+    on the step's first P pictures with the reference's default presets, through the C ABI; and
+    the reference's analyze_p_picture on one of those pictures on one host thread, compared."""
+    import time
+
+    from libvc1_b200.abi import make_ppic_cfg
+
+    cfg = make_ppic_cfg()
+    pics = run.pics[:pictures]
+    t, r, pq = pics[0]
+    ctx.analyze_p_picture(params(pq), cfg, t, r, 3600, 3610, 3600)  # buffers and tuned shapes
+    t0 = time.perf_counter()
+    infos = [ctx.analyze_p_picture(params(pq), cfg, t, r, 3600 + i, 3610, 3600) for i, (t, r, pq) in enumerate(pics)]
+    dt = time.perf_counter() - t0
+    out = {"workload": f"{len(pics)} 1080p P pictures of the step against their references; the reference's default "
+                       "presets (trellis 1, DQUANT on, variable transforms with TTBLK signaling, fade compensation)",
+           "mb_per_s": round(len(pics) * MBS / dt, 1), "ms_per_picture": round(1e3 * dt / len(pics), 2),
+           "modes": [int(i.mode) for i in infos], "weighted": [int(i.weighted) for i in infos],
+           "timing": "wall clock of synchronous C-ABI calls (every pass, score and decision of the picture)"}
+    try:
+        from oracle import Reference, ref_available
+    except Exception:  # pragma: no cover
+        return out
+    if not ref_available():
+        return out
+    t, r, pq = pics[0]
+    R = Reference(params(pq), simd_auto=True)
+    t0 = time.perf_counter()
+    want, mode, ic, bits = R.analyze_p_picture_cfg(cfg, clip.frame(t), clip.frame(r))
+    dt_ref = time.perf_counter() - t0
+    got = ctx.read_result(params(pq), 3600)
+    out["reference_one_thread_mb_per_s"] = round(MBS / dt_ref, 1)
+    out["matches_reference"] = (got.equal(want) == [] and infos[0].mode == mode and bool(infos[0].weighted) == ic
+                                and infos[0].motion_bits == bits)
+    return out
+
+
 def batched_clips(n_odd_seed=7):
     """The batched workload's 48 clips: (coded width, height, display width, height, seed):
     16 at 640x360, 16 at 1280x720, 8 at 1920x1080 and 8 of odd display sizes with widths in
@@ -745,6 +785,9 @@ def run_ours(args, rank, world, device):
         run.step()  # the step's predictions back in their frame slots
         ctx.synchronize()
         transform_rd = transform_rd_leg(ctx, run, clip)
+    mode_decision = None
+    if not args.no_mode_decision and world == 1:
+        mode_decision = mode_decision_leg(ctx, run, clip)
     out = None
     if rank == 0:
         cpu = cpu_baseline(args, clip) if (world == 1 and not args.no_cpu_baseline) else None
@@ -786,6 +829,7 @@ def run_ours(args, rank, world, device):
             "batched": batched,
             "longrange": longrange,
             "transform_rd": transform_rd,
+            "mode_decision": mode_decision,
         }
     ctx.close()
     return out
@@ -918,6 +962,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-clip leg")
     ap.add_argument("--no-longrange", action="store_true", help="skip the long-range pan leg")
     ap.add_argument("--no-transform-rd", action="store_true", help="skip the transform RD leg")
+    ap.add_argument("--no-mode-decision", action="store_true", help="skip the P motion-mode decision leg")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--gops", type=int, default=None, help="analyse only the pictures of the first N GOPs (profiling)")
     args = ap.parse_args()

@@ -612,6 +612,61 @@ int vc1cu_choose_transform(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_tr
 int vc1cu_reconstruct(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
                       const uint8_t* block_types, int out_id);
 
+/* ---- the P picture's motion-mode decision (Vc1Encoder::analyze_p_picture) ---------- */
+
+/*
+ * Replaces Vc1Encoder::estimate_p_motion_bits (src/encoder_motion.cpp:444-486) for the analysis
+ * in result slot `slot`, made in mv_mode: the MVTAB selector, MVMODE (with the
+ * intensity-compensation fields when intensity != 0), the MVTYPEMB bitplane of a Mixed-MV
+ * picture (choose_bitplane, src/encoder_entropy.cpp:37-61) and every macroblock's MVDATA under
+ * the cheapest of the four MV tables (choose_mv_table, :1223-1234) with one bit per
+ * hybrid-predicted vector. A half-pel differential the syntax cannot represent (the reference
+ * throws) fails with VC1CU_ERR_STATE. Synchronous.
+ */
+int vc1cu_p_motion_bits(vc1cu_ctx* ctx, const vc1cu_params* p, int slot, int mv_mode, int intensity, uint64_t* bits);
+
+/* The EncoderConfig fields analyze_p_picture reads beyond vc1cu_params. */
+typedef struct {
+    vc1cu_trd_cfg trd;           /* the encoder's trellis, variable_transforms,
+                                    extended_transform_signaling, use_vlc and hrd_enabled; the mode
+                                    RD evaluates AQ-neutrally at PQINDEX with the picture's decision
+                                    coding set, per-MB types and no DQUANT (the other fields are
+                                    ignored) */
+    int32_t fast_transform_rdo;  /* EncoderConfig::fast_transform_rdo */
+    int32_t dquant;              /* EncoderConfig::dquant */
+    int32_t n_modes;             /* candidate modes in order qpel, half-pel, bilinear, Mixed-MV: 4 in
+                                    Advanced Profile (1 or 3 in Main Profile) */
+    int32_t fade_compensation;   /* EncoderConfig::fade_compensation */
+    double fade_min_gain;        /* EncoderConfig::fade_min_gain */
+} vc1cu_ppic_cfg;
+
+/* What vc1cu_analyze_p_picture decided. Candidate i < n_modes is the plain analysis in mode i,
+ * candidate 4 + i the fade-compensated one (when an estimate was enabled). */
+typedef struct {
+    int32_t mode;                /* the final pass's MV mode */
+    int32_t weighted;            /* 1: the fade-compensated analysis was kept */
+    vc1cu_intensity ic;          /* the fade estimate on the plain choice (enabled 0: none) */
+    uint64_t motion_bits;        /* estimate_p_motion_bits of the returned analysis */
+    uint64_t cand_bits[8];       /* the candidates' motion bits */
+    double cand_score[8];        /* their sampled mode-RD scores (compared in long double; reported
+                                    rounded to double) */
+} vc1cu_ppic_info;
+
+/*
+ * The whole of Vc1Encoder::analyze_p_picture (src/encoder_motion.cpp:524-597) on the device: the
+ * quarter-pel seed pass and the seeded mode passes, each candidate's motion bits and
+ * sampled_p_mode_rd (:488-522: the prediction and the AQ-neutral transform RD of 32 evenly spaced
+ * macroblocks, residual RD per MB plus lambda times motion bits per MB with lambda = 0.75 * (2 *
+ * PQ + HALFQP)^2, in the host's long double), the final pass in the least-scoring mode into
+ * out_slot, and with fade compensation the intensity estimate on it, the compensated reference,
+ * the weighted seed and mode passes, their scores and the reference's acceptance test, the
+ * weighted final pass replacing out_slot when it wins. scratch_slot .. scratch_slot + 7 are
+ * result slots and scratch_frame, scratch_frame + 1 frame slots the call overwrites (the
+ * prediction scratch and the compensated reference). info may be NULL. Synchronous.
+ */
+int vc1cu_analyze_p_picture(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_ppic_cfg* cfg, int cur_id, int ref_id,
+                            int out_slot, int scratch_slot, int scratch_frame, vc1cu_ppic_info* info);
+
 /*
  * In-loop deblocking of frame slot frame_id in place, at params->pqindex.
  * vc1cu_loop_filter_i: Vc1Encoder::apply_i_like_loop_filter (src/encoder_filter.cpp:426-441),

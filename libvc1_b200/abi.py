@@ -267,6 +267,38 @@ def make_trd_cfg(**kw) -> TrdCfg:
     return c
 
 
+class PpicCfg(C.Structure):
+    """vc1cu_ppic_cfg: the EncoderConfig fields analyze_p_picture reads beyond the parameters."""
+    _fields_ = [("trd", TrdCfg), ("fast_transform_rdo", C.c_int32), ("dquant", C.c_int32), ("n_modes", C.c_int32),
+                ("fade_compensation", C.c_int32), ("fade_min_gain", C.c_double)]
+
+
+def make_ppic_cfg(**kw) -> PpicCfg:
+    """The reference's EncoderConfig defaults (trellis 1, variable transforms with extended
+    signaling, VLC coding, DQUANT on, fast transform RDO off, fade compensation on with a 0.04
+    minimum gain) and the four Advanced Profile candidate modes, unless overridden; trd_* keys set
+    fields of the transform RD configuration."""
+    c = PpicCfg()
+    c.trd = make_trd_cfg(adaptive_quality=0, aq_strength=0.0)
+    c.fast_transform_rdo, c.dquant, c.n_modes, c.fade_compensation, c.fade_min_gain = 0, 1, 4, 1, 0.04
+    for k, v in kw.items():
+        if k.startswith("trd_"):
+            if not hasattr(c.trd, k[4:]):
+                raise KeyError(k)
+            setattr(c.trd, k[4:], v)
+        elif hasattr(c, k):
+            setattr(c, k, v)
+        else:
+            raise KeyError(k)
+    return c
+
+
+class PpicInfo(C.Structure):
+    """vc1cu_ppic_info: what analyze_p_picture decided (mode, fade use, motion bits, candidates)."""
+    _fields_ = [("mode", C.c_int32), ("weighted", C.c_int32), ("ic", Intensity), ("motion_bits", C.c_uint64),
+                ("cand_bits", C.c_uint64 * 8), ("cand_score", C.c_double * 8)]
+
+
 class TDecisionC(C.Structure):
     """vc1cu_tdecision: one macroblock's MbTransformDecision."""
     _fields_ = [("type", C.c_uint8), ("signal_level", C.c_uint8), ("cbp", C.c_uint8), ("parent_type", C.c_uint8 * 6),

@@ -20,7 +20,8 @@ import os
 import numpy as np
 
 from .abi import (Analysis, BAnalysis, BAnalysisC, BPass, Counters, ERRORS, IcPass, Intensity, Timing, MV_QPEL,
-                  METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params, TDECISION_DTYPE, TrdCfg, mbs_of)
+                  METRIC_SAD, METRIC_SATD, Mv, PAnalysisC, Params, PpicCfg, PpicInfo, TDECISION_DTYPE, TrdCfg,
+                  mbs_of)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvc1cu.so")
@@ -44,6 +45,7 @@ EXPORTS = (
     "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
+    "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture",
 )
 
 
@@ -119,6 +121,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_measure_fp64_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
+    L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
+    L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
@@ -467,6 +471,21 @@ class CudaComputeContext:
                                                    None if mq is None else mq.ctypes.data, out.ctypes.data,
                                                    None if lv is None else lv.ctypes.data))
         return out, lv
+
+    def p_motion_bits(self, params: Params, slot: int, mode: int, intensity: bool = False) -> int:
+        """Vc1Encoder::estimate_p_motion_bits of the analysis in result slot `slot` (made in mode)."""
+        out = C.c_uint64()
+        self._check(self._L.vc1cu_p_motion_bits(self._h, C.byref(params), slot, mode, int(intensity), C.byref(out)))
+        return out.value
+
+    def analyze_p_picture(self, params: Params, cfg: PpicCfg, cur_id: int, ref_id: int, out_slot: int,
+                          scratch_slot: int, scratch_frame: int) -> PpicInfo:
+        """Vc1Encoder::analyze_p_picture on the device (vc1cu_analyze_p_picture): the final analysis
+        lands in out_slot (read it with read_result); returns the decision record."""
+        info = PpicInfo()
+        self._check(self._L.vc1cu_analyze_p_picture(self._h, C.byref(params), C.byref(cfg), cur_id, ref_id, out_slot,
+                                                    scratch_slot, scratch_frame, C.byref(info)))
+        return info
 
     def fast_transform_types(self, params: Params, src_id: int, pred_id: int):
         """The throughput preset's transform type (1..4) of every MB of src_id against pred_id."""

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 CU_SOURCES = ["vc1cu_api.cu", "vc1cu_core.cu", "vc1cu_global.cu", "vc1cu_xform.cu", "vc1cu_score.cu", "vc1cu_bpic.cu", "vc1cu_ic.cu", "vc1cu_filter.cu",
-              "vc1cu_synth.cu", "vc1cu_lp.cu"]
+              "vc1cu_synth.cu", "vc1cu_lp.cu", "vc1cu_moderd.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

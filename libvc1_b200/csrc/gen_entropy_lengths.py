@@ -1,8 +1,8 @@
 """Writes vc1cu_entropy_lengths.h: the VC-1 code lengths the transform RD's bit estimates need.
 
 The lengths are bitstream-format data (SMPTE ST 421: the eight progressive AC run/level VLC
-tables and their escape codes, the P-picture CBPCY table, TTMB / TTBLK / SUBBLKPAT and the
-progressive inter scans). They are read from the reference tree, whose tables state them, and
+tables and their escape codes, the P-picture CBPCY table, TTMB / TTBLK / SUBBLKPAT, the
+progressive inter scans, the four MVDATA tables and the bitplane IMODE / NORM-2 / NORM-6 codes). They are read from the reference tree, whose tables state them, and
 only the lengths (never the code words) are kept. Run it where the reference tree is present:
 
     python libvc1_b200/csrc/gen_entropy_lengths.py [reference tree]    (default $LIBVC1_REFERENCE
@@ -31,14 +31,24 @@ def _block(text, name):
     return m.group(1)
 
 
+def _gblock(text, name):
+    """A std::array initialiser of the group-A tables (`name{{...}};` or `name = {{...}};`)."""
+    m = re.search(r"\b" + re.escape(name) + r"\s*=?\s*\{\{(.*?)\}\};", text, re.S)
+    if not m:
+        raise SystemExit(f"{name} not found")
+    return m.group(1)
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIBVC1_REFERENCE", "/root/reference")
     ent = open(os.path.join(ref, "src", "vc1_entropy_tables.h")).read()
     inh = open(os.path.join(ref, "src", "encoder_internal.h")).read()
+    grp = open(os.path.join(ref, "src", "vc1_groupa_tables.h")).read()
     out = ["// vc1cu_entropy_lengths.h - VC-1 code lengths of the transform RD's bit estimates.",
            "// Generated by gen_entropy_lengths.py (do not edit): bitstream-format data of SMPTE ST 421",
            "// (AC run/level tables and escapes of the eight progressive coding sets, P CBPCY, TTMB,",
-           "// TTBLK, SUBBLKPAT, the progressive inter scans); lengths only, no code words.",
+           "// TTBLK, SUBBLKPAT, the progressive inter scans, MVDATA, IMODE, NORM-2, NORM-6); lengths only,",
+           "// no code words.",
            "// The small tables' storage is VC1CU_ENT_TABLE (constexpr unless the includer puts them in",
            "// device constant memory); the AC entries are host data (dense tables are built from them).",
            "#pragma once", "", "#include <cstdint>", "", "#ifndef VC1CU_ENT_TABLE", "#define VC1CU_ENT_TABLE constexpr",
@@ -72,6 +82,18 @@ def main():
                    ", ".join("{" + ", ".join(map(str, v[r * n:(r + 1) * n])) + "}" for r in range(3)) + "};")
     for name, n in (("kInterScan", 64), ("kInterScan8x4", 32), ("kInterScan4x8", 32), ("kInterScan4x4", 16)):
         v = _ints(_block(inh, name))
+        assert len(v) == n, name
+        out.append(f"VC1CU_ENT_TABLE uint8_t {name}[{n}] = {{" + ", ".join(map(str, v)) + "};")
+    # picture-layer lengths of the P motion-bit estimate: MVDATA of the four MV tables, IMODE,
+    # NORM-2 and NORM-6 bitplane symbols
+    out.append("// MVDATA lengths of MV tables 0..3 by symbol (0..72)")
+    v = _ints(_gblock(grp, "kMvDiffBits"))
+    assert len(v) == 4 * 73, "kMvDiffBits"
+    out.append("VC1CU_ENT_TABLE uint8_t kMvDiffBits[4][73] = {" +
+               ", ".join("{" + ", ".join(map(str, v[r * 73:(r + 1) * 73])) + "}" for r in range(4)) + "};")
+    out.append("// bitplane IMODE, NORM-2 and NORM-6 symbol lengths")
+    for name, n in (("kImodeBits", 7), ("kNorm2Bits", 4), ("kNorm6Bits", 64)):
+        v = _ints(_gblock(grp, name))
         assert len(v) == n, name
         out.append(f"VC1CU_ENT_TABLE uint8_t {name}[{n}] = {{" + ", ".join(map(str, v)) + "};")
     out += ["", "}  // namespace ent", "}  // namespace vc1cu", ""]

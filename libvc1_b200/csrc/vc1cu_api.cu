@@ -59,8 +59,9 @@ size_t trd_tables_bytes();
 void trd_fill_tables(void* host);
 cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
                        const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
-                       int16_t* levels, cudaStream_t s);
+                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
+cudaError_t launch_p_motion_bits(const DevParams& P, const DevResult& r, int mode, unsigned long long* acc, cudaStream_t s);
 cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  cudaStream_t s);
 cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
@@ -289,6 +290,8 @@ struct vc1cu_ctx {
     void* d_trd_tab = nullptr;  // the transform RD's dense rate tables (built once)
     void* d_trd = nullptr;      // its per-call buffers: MQUANT, decisions, levels, luma sum
     size_t trd_cap = 0;
+    void* d_mrd = nullptr;      // the P mode decision's counters, sampled MB list and decisions
+    size_t mrd_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -1866,6 +1869,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_trd_tab) cudaFree(c->d_trd_tab);
     if (c->d_sp) cudaFree(c->d_sp);
     if (c->d_trd) cudaFree(c->d_trd);
+    if (c->d_mrd) cudaFree(c->d_mrd);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
     if (c->d_gcopy) cudaFree(c->d_gcopy);
@@ -2562,34 +2566,40 @@ int vc1cu_scene_change_score(vc1cu_ctx* c, const vc1cu_params* p, int cur_id, in
     });
 }
 
+// intensity_compensated_reference (encoder_motion_compensation.cpp:175-193, :195-294) of frame
+// slot ref_id into out_id, on the context stream.
+static void ic_compensate(vc1cu_ctx* c, int ref_id, const vc1cu_intensity* ic, int out_id) {
+    FrameSlot& fr = frame_slot(c, ref_id);
+    const int W = fr.w, H = fr.h;
+    const DevFrame ref = fr.view();
+    FrameSlot& fo = alloc_frame(c, out_id, W, H);
+    const DevFrame o = fo.view();
+    // the luma law of intensity_map_y and the chroma scale of intensity_map_uv
+    // (encoder_motion_compensation.cpp:175-193)
+    int scale, shift;
+    if (ic->lumscale == 0) {
+        scale = -64;
+        shift = (255 - ic->lumshift * 2) * 64;
+        if (ic->lumshift > 31) shift += 128 * 64;
+    } else {
+        scale = ic->lumscale + 32;
+        shift = (ic->lumshift > 31 ? ic->lumshift - 64 : ic->lumshift) * 64;
+    }
+    const int cscale = ic->lumscale == 0 ? -64 : ic->lumscale + 32;
+    Timer tm(c, kMc);
+    ck(launch_ic_map(ref, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v, fo.pitch_y, fo.pitch_c, W, H, ic->enabled != 0, scale,
+                     shift, cscale, c->stream),
+       "intensity map launch");
+    tm.stop(1);
+}
+
 int vc1cu_intensity_compensate(vc1cu_ctx* c, int ref_id, const vc1cu_intensity* ic, int out_id) {
     return guarded(c, [&]() -> int {
         if (!ic) throw Fail{VC1CU_ERR_ARG, "null intensity parameters"};
         if (ic->lumscale < 0 || ic->lumscale > 63 || ic->lumshift < 0 || ic->lumshift > 63)
             throw Fail{VC1CU_ERR_ARG, "LUMSCALE and LUMSHIFT are 6-bit codes (0..63)"};
         if (out_id < 0 || out_id >= kMaxSlot || out_id == ref_id) throw Fail{VC1CU_ERR_ARG, "invalid output frame slot"};
-        FrameSlot& fr = frame_slot(c, ref_id);
-        const int W = fr.w, H = fr.h;
-        const DevFrame ref = fr.view();
-        FrameSlot& fo = alloc_frame(c, out_id, W, H);
-        const DevFrame o = fo.view();
-        // the luma law of intensity_map_y and the chroma scale of intensity_map_uv
-        // (encoder_motion_compensation.cpp:175-193)
-        int scale, shift;
-        if (ic->lumscale == 0) {
-            scale = -64;
-            shift = (255 - ic->lumshift * 2) * 64;
-            if (ic->lumshift > 31) shift += 128 * 64;
-        } else {
-            scale = ic->lumscale + 32;
-            shift = (ic->lumshift > 31 ? ic->lumshift - 64 : ic->lumshift) * 64;
-        }
-        const int cscale = ic->lumscale == 0 ? -64 : ic->lumscale + 32;
-        Timer tm(c, kMc);
-        ck(launch_ic_map(ref, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v, fo.pitch_y, fo.pitch_c, W, H, ic->enabled != 0, scale,
-                         shift, cscale, c->stream),
-           "intensity map launch");
-        tm.stop(1);
+        ic_compensate(c, ref_id, ic, out_id);
         return VC1CU_OK;
     });
 }
@@ -2640,6 +2650,20 @@ int vc1cu_fast_transform_types(vc1cu_ctx* c, const vc1cu_params* p, int src_id, 
     });
 }
 
+// The transform RD's dense rate tables on the device, built once per context.
+static const void* trd_tables(vc1cu_ctx* c) {
+    if (!c->d_trd_tab) {
+        std::vector<uint8_t> h(trd_tables_bytes());
+        trd_fill_tables(h.data());
+        void* d = nullptr;
+        ck(cudaMalloc(&d, h.size()), "cudaMalloc(transform RD tables)");
+        c->d_trd_tab = d;
+        ck(cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(tables)");
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize(tables)");  // h is freed on return
+    }
+    return c->d_trd_tab;
+}
+
 int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id, int pred_id,
                            const uint8_t* mquant, vc1cu_tdecision* out, int16_t* levels) {
     return guarded(c, [&]() -> int {
@@ -2659,15 +2683,7 @@ int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_
         if (mquant)
             for (size_t i = 0; i < mbs; ++i)
                 if (mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 0 (PQINDEX) or 1..31"};
-        if (!c->d_trd_tab) {
-            std::vector<uint8_t> h(trd_tables_bytes());
-            trd_fill_tables(h.data());
-            void* d = nullptr;
-            ck(cudaMalloc(&d, h.size()), "cudaMalloc(transform RD tables)");
-            c->d_trd_tab = d;
-            ck(cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(tables)");
-            ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize(tables)");  // h is freed on return
-        }
+        trd_tables(c);
         auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
         const size_t b_sum = 256, b_mq = al(mbs), b_out = al(mbs * sizeof(vc1cu_tdecision)), b_lv = al(mbs * 384 * 2);
         uint8_t* base = static_cast<uint8_t*>(ensure(c->d_trd, c->trd_cap, b_sum + b_mq + b_out + b_lv,
@@ -2679,7 +2695,7 @@ int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_
         if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(mquant)");
         Timer tm(c, kXform);
         ck(launch_trd(P, fs.view(), fp.view(), c->d_trd_tab, mquant ? d_mq : nullptr, *cfg, d_sum, d_out,
-                      levels ? d_lv : nullptr, c->stream),
+                      levels ? d_lv : nullptr, c->stream, nullptr, 0),
            "transform RD launch");
         tm.stop(2);
         ck(cudaMemcpyAsync(out, d_out, mbs * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
@@ -2687,6 +2703,224 @@ int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_
         if (levels)
             ck(cudaMemcpyAsync(levels, d_lv, mbs * 384 * 2, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(levels)");
         sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+// ---- the P picture's motion-mode decision (analyze_p_picture, encoder_motion.cpp:524-597) ----
+
+// unary_mode_bits and p_mv_mode_index (encoder_motion.cpp:1116-1143): the MVMODE (and, with
+// intensity compensation, MVMODE2) unary codes of a progressive P picture.
+static int unary_mode_bits(int index, int maximum) { return index < maximum ? index + 1 : maximum; }
+static int p_mv_mode_index(int mode, int pq, bool secondary) {
+    if (secondary) {
+        if (pq <= 12) return mode == VC1CU_MV_QPEL ? 0 : mode == VC1CU_MV_MIXED ? 1 : mode == VC1CU_MV_HPEL ? 2 : 3;
+        return mode == VC1CU_MV_HPEL_BILINEAR ? 0 : mode == VC1CU_MV_QPEL ? 1 : mode == VC1CU_MV_HPEL ? 2 : 3;
+    }
+    if (pq <= 12) {
+        if (mode == VC1CU_MV_QPEL) return 0;
+        if (mode == VC1CU_MV_MIXED) return 1;
+        if (mode == VC1CU_MV_HPEL) return 2;
+        if (mode == VC1CU_MV_HPEL_BILINEAR) return 4;
+    } else {
+        if (mode == VC1CU_MV_HPEL_BILINEAR) return 0;
+        if (mode == VC1CU_MV_QPEL) return 1;
+        if (mode == VC1CU_MV_HPEL) return 2;
+        if (mode == VC1CU_MV_MIXED) return 4;
+    }
+    return 3;
+}
+
+// The mode decision's device buffer: 7 counters, the sampled MB list, their decisions.
+constexpr int kModeRdSamples = 32;
+static uint8_t* mrd_buffer(vc1cu_ctx* c) {
+    return static_cast<uint8_t*>(ensure(c->d_mrd, c->mrd_cap, 256 + 256 + kModeRdSamples * sizeof(vc1cu_tdecision),
+                                        "cudaMalloc(mode decision buffers)"));
+}
+
+// estimate_p_motion_bits (encoder_motion.cpp:444-486) of result slot s, analysed in `mode`.
+static uint64_t p_motion_bits(vc1cu_ctx* c, const DevParams& P, const ResultSlot& s, int mode, bool intensity) {
+    auto* acc = reinterpret_cast<unsigned long long*>(mrd_buffer(c));
+    Timer tm(c, kMc);
+    ck(launch_p_motion_bits(P, s.r, mode, acc, c->stream), "motion-bit launch");
+    tm.stop(mode == VC1CU_MV_MIXED ? 2 : 1);
+    unsigned long long h[7];
+    ck(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(motion bits)");
+    sync_checked(c);
+    if (h[5]) throw Fail{VC1CU_ERR_STATE, "a half-pel MV differential is not representable from its predictor"};
+    uint64_t bits = 2;  // MVTAB
+    if (intensity)
+        bits += (uint64_t)unary_mode_bits(3, 4) + (uint64_t)unary_mode_bits(p_mv_mode_index(mode, P.pq, true), 3) + 12;
+    else
+        bits += (uint64_t)unary_mode_bits(p_mv_mode_index(mode, P.pq, false), 4);
+    if (mode == VC1CU_MV_MIXED) bits += h[6];  // MVTYPEMB
+    bits += h[4];                              // hybrid-predictor flags
+    uint64_t table = h[0];                     // choose_mv_table: the least of the four
+    for (int t = 1; t < 4; ++t) table = h[t] < table ? h[t] : table;
+    return bits + table;
+}
+
+// sampled_p_mode_rd (encoder_motion.cpp:488-522): the prediction of slot s against pred_ref and
+// the AQ-neutral transform RD of up to 32 evenly spaced macroblocks, combined with the motion
+// bits in long double exactly as the reference does.
+static long double sampled_mode_rd(vc1cu_ctx* c, const DevParams& P, const vc1cu_ppic_cfg& cfg, int cur_id, int pred_ref_id,
+                                   const ResultSlot& s, int mode, uint64_t motion_bits, int pred_id) {
+    const int total = P.mbw * P.mbh;
+    if (total <= 0) return 0.0L;
+    const int wanted = std::min(kModeRdSamples, total);
+    const int stride = std::max(1, total / wanted);
+    std::vector<int> list;
+    for (int linear = 0; linear < total && (int)list.size() < wanted; linear += stride) list.push_back(linear);
+    const int n = (int)list.size();
+    const int q = 2 * P.pq + (P.halfqp ? 1 : 0);  // picture_double_quant(PQINDEX, false)
+    const double lambda = 0.75 * static_cast<double>(q) * static_cast<double>(q);
+    long double rd = 0.0L;
+    // the fixed-8x8 shortcut of choose_transform_mb (encoder_transform.cpp:1610-1634) returns an
+    // empty decision: no distortion, no bits
+    const bool shortcut = !cfg.trd.variable_transforms && cfg.fast_transform_rdo && !cfg.dquant && cfg.trd.trellis == 0;
+    if (!shortcut) {
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fr = frame_slot(c, pred_ref_id);
+        FrameSlot& fp = alloc_frame(c, pred_id, P.W, P.H);
+        {
+            Timer tm(c, kMc);
+            launch_mc(P, fr.view(), s.r.mvs, s.r.bmv, s.r.use4, mode, (uint8_t*)fp.view().y, (uint8_t*)fp.view().u,
+                      (uint8_t*)fp.view().v, fp.pitch_y, fp.pitch_c, c->stream);
+            ck(cudaGetLastError(), "mc_kernel launch");
+            tm.stop(1);
+        }
+        uint8_t* base = mrd_buffer(c);
+        auto* d_list = reinterpret_cast<int*>(base + 256);
+        auto* d_out = reinterpret_cast<vc1cu_tdecision*>(base + 512);
+        ck(cudaMemcpyAsync(d_list, list.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(list)");
+        vc1cu_trd_cfg t = cfg.trd;  // the AQ-neutral evaluator at PQINDEX, no DQUANT, per-MB types
+        t.adaptive_quality = 0;
+        t.aq_strength = 0.0;
+        t.coding_set = P.pq <= 8 ? 1 : 3;  // chroma_coding_set(PQINDEX <= 8 ? 1 : 0, PQINDEX)
+        t.dquantfrm = 0;
+        t.frame_type = 0;
+        {
+            Timer tm(c, kXform);
+            ck(launch_trd(P, fc.view(), fp.view(), trd_tables(c), nullptr, t, nullptr, d_out, nullptr, c->stream, d_list, n),
+               "transform RD launch");
+            tm.stop(1);
+        }
+        std::vector<vc1cu_tdecision> dec(n);
+        ck(cudaMemcpyAsync(dec.data(), d_out, n * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
+           "cudaMemcpyAsync(decisions)");
+        sync_checked(c);
+        for (int i = 0; i < n; ++i)
+            rd += static_cast<long double>(dec[i].distortion) + lambda * static_cast<long double>(dec[i].estimated_bits);
+    }
+    const long double residual_per_mb = rd / static_cast<long double>(n);
+    const long double motion_per_mb = static_cast<long double>(motion_bits) / static_cast<long double>(total);
+    return residual_per_mb + lambda * motion_per_mb;
+}
+
+int vc1cu_p_motion_bits(vc1cu_ctx* c, const vc1cu_params* p, int slot, int mv_mode, int intensity, uint64_t* bits) {
+    return guarded(c, [&]() -> int {
+        if (!bits) throw Fail{VC1CU_ERR_ARG, "null output"};
+        if (mv_mode < 0 || mv_mode > 3) throw Fail{VC1CU_ERR_ARG, "invalid MV mode"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        ResultSlot& s = result_slot(c, slot, P.mbw * P.mbh, false);
+        check_status(c);
+        *bits = p_motion_bits(c, P, s, mv_mode, intensity != 0);
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_analyze_p_picture(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_ppic_cfg* cfg, int cur_id, int ref_id,
+                            int out_slot, int scratch_slot, int scratch_frame, vc1cu_ppic_info* info) {
+    return guarded(c, [&]() -> int {
+        if (!cfg) throw Fail{VC1CU_ERR_ARG, "null configuration"};
+        const int n = cfg->n_modes;
+        if (n != 1 && n != 3 && n != 4) throw Fail{VC1CU_ERR_ARG, "n_modes must be 1, 3 or 4"};
+        if (cfg->trd.trellis < 0 || cfg->trd.trellis > 2) throw Fail{VC1CU_ERR_ARG, "invalid trellis"};
+        if (out_slot < 0 || out_slot >= kMaxSlot || scratch_slot < 0 || scratch_slot + 8 > kMaxSlot ||
+            (out_slot >= scratch_slot && out_slot < scratch_slot + 8))
+            throw Fail{VC1CU_ERR_ARG, "result slots out of range or overlapping"};
+        if (scratch_frame < 0 || scratch_frame + 2 > kMaxSlot || cur_id == scratch_frame || cur_id == scratch_frame + 1 ||
+            ref_id == scratch_frame || ref_id == scratch_frame + 1)
+            throw Fail{VC1CU_ERR_ARG, "scratch frame slots out of range or overlapping the pictures"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        {
+            FrameSlot& fc = frame_slot(c, cur_id);
+            FrameSlot& fr = frame_slot(c, ref_id);
+            if (fc.w != P.W || fc.h != P.H || fr.w != P.W || fr.h != P.H)
+                throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        }
+        const int mbs = P.mbw * P.mbh;
+        const int modes[4] = {VC1CU_MV_QPEL, VC1CU_MV_HPEL, VC1CU_MV_HPEL_BILINEAR, VC1CU_MV_MIXED};
+        const int pred_id = scratch_frame, comp_id = scratch_frame + 1;
+        vc1cu_ppic_info inf{};
+        auto mean_abs_residual = [&](int slot) {
+            vc1cu_panalysis a{};
+            ResultSlot& s = result_slot(c, slot, mbs, false);
+            check_status_read(c, s.written);
+            read_result(c, s, &a);
+            return a.mean_abs_residual;
+        };
+        // the seed pass and the seeded mode passes over reference r into slots base..base+n-1,
+        // each scored; returns the candidate index with the strictly least score
+        auto candidates = [&](int r, int base, bool intensity, long double& best_score) {
+            std::vector<vc1cu_pass> passes;
+            passes.push_back(vc1cu_pass{cur_id, r, VC1CU_MV_QPEL, 0, -1, base, 0});
+            for (int i = 1; i < n; ++i) passes.push_back(vc1cu_pass{cur_id, r, modes[i], 0, base, base + i, 0});
+            launch_passes(c, p, passes.data(), n);
+            stamp_written(c);
+            check_status(c);
+            int best = 0;
+            best_score = std::numeric_limits<long double>::infinity();
+            for (int i = 0; i < n; ++i) {
+                ResultSlot& s = result_slot(c, base + i, mbs, false);
+                const uint64_t bits = p_motion_bits(c, P, s, modes[i], intensity);
+                const long double sc = sampled_mode_rd(c, P, *cfg, cur_id, r, s, modes[i], bits, pred_id);
+                const int k = (intensity ? 4 : 0) + i;
+                inf.cand_bits[k] = bits;
+                inf.cand_score[k] = static_cast<double>(sc);
+                if (sc < best_score) {
+                    best_score = sc;
+                    best = i;
+                }
+            }
+            return best;
+        };
+        long double best_score;
+        const int best = candidates(ref_id, scratch_slot, false, best_score);
+        const vc1cu_pass fin{cur_id, ref_id, modes[best], 1, scratch_slot + best, out_slot, 0};
+        launch_passes(c, p, &fin, 1);
+        stamp_written(c);
+        check_status(c);
+        inf.mode = modes[best];
+        inf.motion_bits = p_motion_bits(c, P, result_slot(c, out_slot, mbs, false), modes[best], false);
+        if (cfg->fade_compensation) {
+            // estimate_intensity_comp on the chosen analysis, then the weighted candidates
+            const vc1cu_icpass icp{cur_id, ref_id, out_slot};
+            ic_estimate(c, P, ic_jobs(c, P, &icp, 1), &inf.ic);
+            if (inf.ic.enabled) {
+                ic_compensate(c, ref_id, &inf.ic, comp_id);
+                long double w_score;
+                const int wbest = candidates(comp_id, scratch_slot + 4, true, w_score);
+                const double mar = mean_abs_residual(out_slot);
+                const double need = std::max(0.25, mar * cfg->fade_min_gain);
+                if (!(mean_abs_residual(scratch_slot + 4 + wbest) + need >= mar || w_score >= best_score)) {
+                    const vc1cu_pass wfin{cur_id, comp_id, modes[wbest], 1, scratch_slot + 4 + wbest, out_slot, 0};
+                    launch_passes(c, p, &wfin, 1);
+                    stamp_written(c);
+                    check_status(c);
+                    inf.mode = modes[wbest];
+                    inf.weighted = 1;
+                    inf.motion_bits = p_motion_bits(c, P, result_slot(c, out_slot, mbs, false), modes[wbest], true);
+                }
+            }
+        }
+        if (info) *info = inf;
         return VC1CU_OK;
     });
 }

@@ -166,9 +166,10 @@ __device__ __forceinline__ int mv_component_bits(int cat, bool halfpel) {
     return sz - ((halfpel && cat == 5) ? 1 : 0);
 }
 
-// Vc1Encoder::motion_vector_rate_bits, encoder_motion.cpp:3214-3225, with mvdata_for_mode
-// (:1099-1114), mv_symbol (:1164-1171) and mv_suffix_bits (:1178-1197). Table 0 proxy.
-__device__ inline uint32_t mv_rate_bits(const DevParams& p, int2 desired, int2 pred, int mode, bool more) {
+// mvdata_for_mode (:1099-1114), mv_symbol (:1164-1171) and mv_suffix_bits (:1178-1197) of a
+// non-intra MVDATA: the symbol (0..72), and in `suffix` the escape or category suffix bits. A
+// half-pel mode codes the differential in half-pel units (callers keep it even).
+__device__ inline int mv_symbol_suffix(const DevParams& p, int2 desired, int2 pred, int mode, bool more, int& suffix) {
     const bool hp = mode_halfpel(mode);
     int dx = desired.x - pred.x, dy = desired.y - pred.y;
     if (hp) { dx /= 2; dy /= 2; }
@@ -179,7 +180,6 @@ __device__ inline uint32_t mv_rate_bits(const DevParams& p, int2 desired, int2 p
         const int idx = yc * 6 + xc;
         sym = (!more && idx == 0) ? 34 : (more ? idx + 36 : idx - 1);
     }
-    int suffix;
     if (sym == 34 || sym == 71) {
         // mvrange_kx {9,10,12,13} / mvrange_ky {8,9,10,11} (:1273-1281)
         const int kx = p.mvrange < 2 ? 9 + p.mvrange : 10 + p.mvrange, ky = 8 + p.mvrange;
@@ -188,6 +188,14 @@ __device__ inline uint32_t mv_rate_bits(const DevParams& p, int2 desired, int2 p
     } else {
         suffix = mv_component_bits(xc, hp) + mv_component_bits(yc, hp);
     }
+    return sym;
+}
+
+// Vc1Encoder::motion_vector_rate_bits, encoder_motion.cpp:3214-3225: the MVDATA length under
+// table 0 (the reference's local proxy) plus the suffix.
+__device__ inline uint32_t mv_rate_bits(const DevParams& p, int2 desired, int2 pred, int mode, bool more) {
+    int suffix;
+    const int sym = mv_symbol_suffix(p, desired, pred, mode, more, suffix);
     return (uint32_t)kMvDiffBits0[sym] + (uint32_t)suffix;
 }
 
@@ -207,6 +215,68 @@ __device__ inline bool hybrid_of(int2 pre, int2 A, int2 C, bool a_intra, bool c_
     if (suma > 32) return true;
     const int sumc = c_intra ? iabs(pre.x) + iabs(pre.y) : iabs(pre.x - C.x) + iabs(pre.y - C.y);
     return sumc > 32;
+}
+
+// Vc1Encoder::predictor_info_mixed_1mv, encoder_motion.cpp:1354-1406. F reads the block-MV field:
+// get(x, y) the vector of 8x8 block (x, y) (zero outside the raster), intra(x, y) its MB's intra flag.
+template <class F>
+__device__ PInfo predictor_mixed_1mv(const DevParams& P, const F& f, int mx, int my) {
+    PInfo r;
+    const int bx = mx * 2, by = my * 2, mbw = P.mbw;
+    const bool a_valid = my > 0, c_valid = mx > 0, b_valid = my > 0 && mbw > 1;
+    const int2 z = make_int2(0, 0);
+    const int2 A = a_valid ? f.get(bx, by - 1) : z;
+    const int2 C = c_valid ? f.get(bx - 1, by) : z;
+    int2 B = z;
+    if (b_valid) B = f.get(bx + ((mx == mbw - 1) ? -1 : 2), by - 1);
+    int2 pre = z;
+    if (a_valid) pre = A;
+    else if (c_valid) pre = C;
+    else if (b_valid) pre = B;
+    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
+        pre.x = median3(A.x, B.x, C.x);
+        pre.y = median3(A.y, B.y, C.y);
+    }
+    pullback(pre, mx * 64, my * 64, mbw * 64 - 4, P.mbh * 64 - 4, -60);
+    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
+    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
+    return r;
+}
+
+// Vc1Encoder::predictor_info_4mv, encoder_motion.cpp:1408-1466
+template <class F>
+__device__ PInfo predictor_4mv(const DevParams& P, const F& f, int mx, int my, int n) {
+    PInfo r;
+    const int mbw = P.mbw;
+    const int bx = mx * 2 + (n & 1), by = my * 2 + ((n >> 1) & 1);
+    const bool a_valid = my > 0 || n == 2 || n == 3;
+    const bool c_valid = mx > 0 || n == 1 || n == 3;
+    const bool b_valid = a_valid;
+    const int2 z = make_int2(0, 0);
+    const int2 A = a_valid ? f.get(bx, by - 1) : z;
+    const int2 C = c_valid ? f.get(bx - 1, by) : z;
+    int2 B = z;
+    if (b_valid) {
+        int bxx = bx;
+        if (n == 0) bxx += mx ? -1 : 1;
+        else if (n == 1) bxx += (mx == mbw - 1) ? -1 : 1;
+        else if (n == 2) bxx += 1;
+        else bxx -= 1;
+        B = f.get(bxx, by - 1);
+    }
+    int2 pre = z;
+    if (a_valid) pre = A;
+    else if (c_valid) pre = C;
+    else if (b_valid) pre = B;
+    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
+        pre.x = median3(A.x, B.x, C.x);
+        pre.y = median3(A.y, B.y, C.y);
+    }
+    pullback(pre, mx * 64 + ((n == 1 || n == 3) ? 32 : 0), my * 64 + ((n == 2 || n == 3) ? 32 : 0), mbw * 64 - 4,
+             P.mbh * 64 - 4, -28);
+    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
+    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
+    return r;
 }
 
 // ---- the x87 long double score (encoder_motion.cpp:3458-3476, :3518-3524) -------------

@@ -2107,65 +2107,6 @@ struct Field {
     }
 };
 
-// Vc1Encoder::predictor_info_mixed_1mv, encoder_motion.cpp:1354-1406
-__device__ PInfo predictor_mixed_1mv(const DevParams& P, const Field& f, int mx, int my) {
-    PInfo r;
-    const int bx = mx * 2, by = my * 2, mbw = P.mbw;
-    const bool a_valid = my > 0, c_valid = mx > 0, b_valid = my > 0 && mbw > 1;
-    const int2 z = make_int2(0, 0);
-    const int2 A = a_valid ? f.get(bx, by - 1) : z;
-    const int2 C = c_valid ? f.get(bx - 1, by) : z;
-    int2 B = z;
-    if (b_valid) B = f.get(bx + ((mx == mbw - 1) ? -1 : 2), by - 1);
-    int2 pre = z;
-    if (a_valid) pre = A;
-    else if (c_valid) pre = C;
-    else if (b_valid) pre = B;
-    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
-        pre.x = median3(A.x, B.x, C.x);
-        pre.y = median3(A.y, B.y, C.y);
-    }
-    pullback(pre, mx * 64, my * 64, mbw * 64 - 4, P.mbh * 64 - 4, -60);
-    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
-    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
-    return r;
-}
-
-// Vc1Encoder::predictor_info_4mv, encoder_motion.cpp:1408-1466
-__device__ PInfo predictor_4mv(const DevParams& P, const Field& f, int mx, int my, int n) {
-    PInfo r;
-    const int mbw = P.mbw;
-    const int bx = mx * 2 + (n & 1), by = my * 2 + ((n >> 1) & 1);
-    const bool a_valid = my > 0 || n == 2 || n == 3;
-    const bool c_valid = mx > 0 || n == 1 || n == 3;
-    const bool b_valid = a_valid;
-    const int2 z = make_int2(0, 0);
-    const int2 A = a_valid ? f.get(bx, by - 1) : z;
-    const int2 C = c_valid ? f.get(bx - 1, by) : z;
-    int2 B = z;
-    if (b_valid) {
-        int bxx = bx;
-        if (n == 0) bxx += mx ? -1 : 1;
-        else if (n == 1) bxx += (mx == mbw - 1) ? -1 : 1;
-        else if (n == 2) bxx += 1;
-        else bxx -= 1;
-        B = f.get(bxx, by - 1);
-    }
-    int2 pre = z;
-    if (a_valid) pre = A;
-    else if (c_valid) pre = C;
-    else if (b_valid) pre = B;
-    if ((int)a_valid + (int)b_valid + (int)c_valid > 1) {
-        pre.x = median3(A.x, B.x, C.x);
-        pre.y = median3(A.y, B.y, C.y);
-    }
-    pullback(pre, mx * 64 + ((n == 1 || n == 3) ? 32 : 0), my * 64 + ((n == 2 || n == 3) ? 32 : 0), mbw * 64 - 4,
-             P.mbh * 64 - 4, -28);
-    const bool hybrid = a_valid && c_valid && hybrid_of(pre, A, C, f.intra(bx, by - 1), f.intra(bx - 1, by));
-    r.pre = pre; r.a = A; r.c = C; r.a_valid = a_valid; r.c_valid = c_valid; r.hybrid = hybrid;
-    return r;
-}
-
 __device__ __forceinline__ int median4(int a, int b, int c, int d) {
     if (a < b) {
         if (c < d) return (imin(b, d) + imax(a, c)) / 2;

@@ -414,6 +414,8 @@ struct TrdArgs {
     double frame_mean;      // mean of the source luma plane (cached_luma_mean)
     vc1cu_tdecision* out;
     int16_t* levels;        // [mb][6][64] or nullptr
+    const int* mb_list;     // nullptr: every MB; else entry i of out / levels is MB mb_list[i]
+    int n_list;
 };
 
 __device__ __forceinline__ double dclamp(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
@@ -1118,9 +1120,10 @@ __global__ void __launch_bounds__(32 * kTrdWarps) trd_kernel(const __grid_consta
     __shared__ int list_all[kTrdWarps][8];  // [0..3] candidate types, [4] count, [5] macro type, [6..] scratch
     __shared__ uint8_t need_all[kTrdWarps][6];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mb = blockIdx.x * kTrdWarps + warp;
+    const int item = blockIdx.x * kTrdWarps + warp;
     const DevParams& P = A.P;
-    if (mb >= P.mbw * P.mbh) return;
+    if (item >= (A.mb_list ? A.n_list : P.mbw * P.mbh)) return;
+    const int mb = A.mb_list ? A.mb_list[item] : item;
     TParent* pool = pool_all[warp];
     int* list = list_all[warp];
     uint8_t* need = need_all[warp];
@@ -1280,12 +1283,12 @@ __global__ void __launch_bounds__(32 * kTrdWarps) trd_kernel(const __grid_consta
             o.parent_distortion[k] = p.distortion;
             chosen_all[warp][k] = d.parent[k];
         }
-        A.out[mb] = o;
+        A.out[item] = o;
     }
     __syncwarp();
     if (A.levels)
         for (int i = lane; i < 6 * 64; i += 32)
-            A.levels[(size_t)mb * 384 + i] = pool[chosen_all[warp][i >> 6]].q[i & 63];
+            A.levels[(size_t)item * 384 + i] = pool[chosen_all[warp][i >> 6]].q[i & 63];
 }
 
 // mean of the source luma plane (cached_luma_mean, encoder_aq.cpp:506-545): one block's partial sums
@@ -1316,14 +1319,17 @@ void trd_fill_tables(void* host) {
 
 cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
                        const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
-                       int16_t* levels, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s);
-    if (e != cudaSuccess) return e;
-    luma_sum_kernel<<<148, 256, 0, s>>>(src.y, src.pitch_y, P.W, P.H, d_sum);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list) {
+    cudaError_t e;
     unsigned long long sum = 0;
-    if ((e = cudaMemcpyAsync(&sum, d_sum, sizeof sum, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    if (cfg.adaptive_quality && cfg.aq_strength > 0.0) {
+        // the frame mean only enters the perceptual lambda scale
+        if ((e = cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        luma_sum_kernel<<<148, 256, 0, s>>>(src.y, src.pitch_y, P.W, P.H, d_sum);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(&sum, d_sum, sizeof sum, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    }
     TrdArgs a;
     a.P = P;
     a.src = src;
@@ -1334,8 +1340,11 @@ cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& 
     a.frame_mean = (P.W > 0 && P.H > 0) ? (double)sum / (double)((size_t)P.W * P.H) : 0.0;
     a.out = out;
     a.levels = levels;
-    const int mbs = P.mbw * P.mbh;
-    trd_kernel<<<(mbs + kTrdWarps - 1) / kTrdWarps, 32 * kTrdWarps, 0, s>>>(a);
+    a.mb_list = mb_list;
+    a.n_list = n_list;
+    const int items = mb_list ? n_list : P.mbw * P.mbh;
+    if (items <= 0) return cudaSuccess;
+    trd_kernel<<<(items + kTrdWarps - 1) / kTrdWarps, 32 * kTrdWarps, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -7,7 +7,7 @@ import os
 
 import numpy as np
 
-from libvc1_b200.abi import Analysis, BAnalysis, BAnalysisC, Intensity, Mv, PAnalysisC, Params, mbs_of
+from libvc1_b200.abi import Analysis, BAnalysis, BAnalysisC, Intensity, Mv, PAnalysisC, Params, PpicCfg, mbs_of
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_oracle", "libvc1oracle.so")
@@ -345,6 +345,13 @@ class Reference:
         L.ref_analyze_p_core.restype = i32
         L.ref_analyze_p_picture.argtypes = [vp, vp, vp, C.POINTER(PAnalysisC), C.POINTER(i32), C.POINTER(i32)]
         L.ref_analyze_p_picture.restype = i32
+        L.ref_analyze_p_picture_cfg.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, C.POINTER(PAnalysisC), C.POINTER(i32),
+                                                C.POINTER(i32), C.POINTER(u64)]
+        L.ref_analyze_p_picture_cfg.restype = i32
+        L.ref_p_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp]
+        L.ref_p_mode_scores.restype = i32
+        L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
+        L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
         L.ref_forward_quant.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
@@ -540,6 +547,39 @@ class Reference:
             raise RuntimeError("reference analyze_p_picture threw")
         out.take_totals(oc)
         return out, mode.value, bool(ic.value)
+
+    def analyze_p_picture_cfg(self, cfg: PpicCfg, cur, ref):
+        """analyze_p_picture under cfg: (analysis, chosen mode, IC enabled, motion bits)."""
+        mbw, mbh = mbs_of(self.p)
+        out = Analysis.empty(mbw * mbh)
+        oc = out.as_c()
+        mode, ic, bits = i32(), i32(), u64()
+        rc = self.lib.ref_analyze_p_picture_cfg(self.h, C.byref(cfg), self._f(cur), self._f(ref), C.byref(oc),
+                                                C.byref(mode), C.byref(ic), C.byref(bits))
+        if rc:
+            raise RuntimeError("reference analyze_p_picture threw")
+        out.take_totals(oc)
+        return out, mode.value, bool(ic.value), bits.value
+
+    def p_mode_scores(self, cfg: PpicCfg, cur, ref):
+        """The four plain candidates' motion bits and sampled mode-RD scores (long double values,
+        returned as numpy longdouble)."""
+        bits = np.zeros(4, np.uint64)
+        scores = np.zeros(4, np.longdouble)
+        assert C.sizeof(C.c_longdouble) == scores.itemsize
+        rc = self.lib.ref_p_mode_scores(self.h, C.byref(cfg), self._f(cur), self._f(ref), bits.ctypes.data,
+                                        scores.ctypes.data)
+        if rc:
+            raise RuntimeError("reference mode scoring threw")
+        return bits, scores
+
+    def estimate_p_motion_bits(self, a: Analysis, mode: int, intensity: bool = False) -> int:
+        """estimate_p_motion_bits of analysis a made in mode (None when the reference throws)."""
+        v = self.lib.ref_estimate_p_motion_bits(self.h, a.mvs.ctypes.data, a.block_mvs.ctypes.data,
+                                                np.ascontiguousarray(a.use_4mv, np.uint8).ctypes.data,
+                                                np.ascontiguousarray(a.use_intra, np.uint8).ctypes.data, mode,
+                                                int(intensity))
+        return None if v == 2 ** 64 - 1 else int(v)
 
     def motion_compensate(self, ref, a: Analysis, mode):
         h, w = self.p.height, self.p.width

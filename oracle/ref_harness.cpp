@@ -451,6 +451,86 @@ int ref_analyze_p_picture(void* h, void* cur, void* ref, vc1cu_panalysis* out, i
     }
 }
 
+// The harness encoder's configuration with the mode decision's fields of a vc1cu_ppic_cfg.
+static EncoderConfig ppic_config(void* h, const vc1cu_ppic_cfg* pc) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.trellis = pc->trd.trellis;
+    c.variable_transforms = pc->trd.variable_transforms != 0;
+    c.extended_transform_signaling = pc->trd.extended_transform_signaling != 0;
+    c.ac_mode = pc->trd.use_vlc ? libvc1::AcMode::Auto : libvc1::AcMode::Esc3;
+    c.hrd_enabled = pc->trd.hrd_enabled != 0;
+    c.fast_transform_rdo = pc->fast_transform_rdo != 0;
+    c.dquant = pc->dquant != 0;
+    c.fade_compensation = pc->fade_compensation != 0;
+    c.fade_min_gain = pc->fade_min_gain;
+    return c;
+}
+
+// analyze_p_picture under a vc1cu_ppic_cfg, with the returned analysis's motion bits.
+int ref_analyze_p_picture_cfg(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* ref, vc1cu_panalysis* out,
+                              int* chosen_mode, int* ic_enabled, uint64_t* motion_bits) {
+    try {
+        const Vc1Encoder e(ppic_config(h, pc));
+        const auto a = e.analyze_p_picture(F(cur), F(ref));
+        fill_out(a, out);
+        *chosen_mode = static_cast<int>(a.mv_mode);
+        *ic_enabled = a.intensity.enabled ? 1 : 0;
+        *motion_bits = a.motion_bits;
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// The plain candidates of analyze_p_picture (encoder_motion.cpp:541-566): each of the four modes'
+// analysis, its estimate_p_motion_bits and its sampled_p_mode_rd score, as the reference computes
+// them (scores in long double).
+int ref_p_mode_scores(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* ref, uint64_t* bits, long double* scores) {
+    try {
+        const EncoderConfig c = ppic_config(h, pc);
+        const Vc1Encoder e(c);
+        EncoderConfig nc = c;
+        nc.adaptive_quality = false;
+        nc.aq_strength = 0.0;
+        const Vc1Encoder neutral(nc);
+        const Mode modes[4] = {Mode::OneMvQpel, Mode::OneMvHpel, Mode::OneMvHpelBilinear, Mode::MixedMv};
+        Frame pred = e.empty_frame();
+        const auto qseed = e.analyze_p_picture_core(F(cur), F(ref), Mode::OneMvQpel, false, nullptr);
+        for (int i = 0; i < 4; ++i) {
+            auto cand = i == 0 ? qseed : e.analyze_p_picture_core(F(cur), F(ref), modes[i], false, &qseed);
+            cand.motion_bits = e.estimate_p_motion_bits(cand, false);
+            bits[i] = cand.motion_bits;
+            scores[i] = e.sampled_p_mode_rd(F(cur), F(ref), cand, cand.motion_bits, pred, neutral);
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+// estimate_p_motion_bits of an analysis given as host arrays (mbw*mbh vectors, 4 block vectors
+// per MB, the 4-MV and intra flags) made in `mode`; UINT64_MAX when the reference throws.
+uint64_t ref_estimate_p_motion_bits(void* h, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs, const uint8_t* use_4mv,
+                                    const uint8_t* use_intra, int mode, int intensity) {
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const size_t mbs = static_cast<size_t>((c.width + 15) / 16) * ((c.height + 15) / 16);
+    Vc1Encoder::PAnalysis a;
+    a.mv_mode = to_mode(mode);
+    a.mvs.resize(mbs);
+    a.block_mvs.resize(mbs);
+    a.use_4mv.assign(use_4mv, use_4mv + mbs);
+    a.use_intra.assign(use_intra, use_intra + mbs);
+    for (size_t i = 0; i < mbs; ++i) {
+        a.mvs[i] = MV{mvs[i].xq, mvs[i].yq};
+        for (int k = 0; k < 4; ++k) a.block_mvs[i][k] = MV{block_mvs[i * 4 + k].xq, block_mvs[i * 4 + k].yq};
+    }
+    try {
+        return E(h).estimate_p_motion_bits(a, intensity != 0);
+    } catch (const std::exception&) {
+        return UINT64_MAX;
+    }
+}
+
 // Prediction of a PAnalysis-like MV field (motion_compensate_mb / _4mv), intra MBs at zero
 // motion, into dst (a frame handle of the same size).
 void ref_motion_compensate(void* h, void* ref, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs,

@@ -29,7 +29,8 @@ STRUCTS = {"Params": (abi.Params, "vc1cu_params"), "Mv": (abi.Mv, "vc1cu_mv"),
            "Timing": (abi.Timing, "vc1cu_timing"), "Pass": (api.Pass, "vc1cu_pass"),
            "BAnalysisC": (abi.BAnalysisC, "vc1cu_banalysis"), "BPass": (abi.BPass, "vc1cu_bpass"),
            "Intensity": (abi.Intensity, "vc1cu_intensity"), "IcPass": (abi.IcPass, "vc1cu_icpass"),
-           "TrdCfg": (abi.TrdCfg, "vc1cu_trd_cfg"), "TDecisionC": (abi.TDecisionC, "vc1cu_tdecision")}
+           "TrdCfg": (abi.TrdCfg, "vc1cu_trd_cfg"), "TDecisionC": (abi.TDecisionC, "vc1cu_tdecision"),
+           "PpicCfg": (abi.PpicCfg, "vc1cu_ppic_cfg"), "PpicInfo": (abi.PpicInfo, "vc1cu_ppic_info")}
 
 
 def test_struct_layouts_match_header(tmp_path):
