@@ -17,7 +17,13 @@
  *      as vc1cu_analyze_b_picture / vc1cu_b_decide;
  *   5. the fade and scene-cut analysis: estimate_intensity_comp and
  *      intensity_compensated_reference (encoder_motion_compensation.cpp:175-348) and
- *      scene_change_score (encoder_motion.cpp:599-676).
+ *      scene_change_score (encoder_motion.cpp:599-676);
+ *   6. the transform RD, Vc1Encoder::choose_transform_mb (encoder_transform.cpp:1605-1780), as
+ *      vc1cu_fast_transform_types / vc1cu_choose_transform;
+ *   7. the picture-level motion-mode decisions, analyze_p_picture (encoder_motion.cpp:524-597)
+ *      with estimate_p_motion_bits and sampled_p_mode_rd, and the quarter-pel versus bilinear
+ *      choice of analyze_b_picture (:1006-1095), as vc1cu_analyze_p_picture /
+ *      vc1cu_p_motion_bits / vc1cu_b_mode_rd.
  *
  * Conventions: every function is extern "C", returns an int status (VC1CU_OK on
  * success), never throws, and records a message retrievable with vc1cu_last_error().
@@ -666,6 +672,22 @@ typedef struct {
  */
 int vc1cu_analyze_p_picture(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_ppic_cfg* cfg, int cur_id, int ref_id,
                             int out_slot, int scratch_slot, int scratch_frame, vc1cu_ppic_info* info);
+
+/*
+ * The quarter-pel versus half-pel bilinear choice of Vc1Encoder::analyze_b_picture
+ * (src/encoder_motion.cpp:1062-1095) for two analyses of one B picture already in B-result slots
+ * (vc1cu_b_decide in quarter-pel and in bilinear mode): sampled_b_mode_rd (:1006-1060) of each,
+ * the prediction of 32 evenly spaced macroblocks (B-intra ones from their blocks' visible means,
+ * plus 72 bits of intra syntax) and their AQ-neutral transform RD, residual RD per MB plus lambda
+ * times the analysis's motion bits per MB, in the host's long double. *choice = 1 when the
+ * bilinear analysis scores strictly less, else 0. past_id is the forward reference the analyses
+ * used (the compensated one under forward intensity compensation). cfg: the transform RD fields,
+ * fast_transform_rdo and dquant of a vc1cu_ppic_cfg; the rest is ignored. pred_id is a frame slot
+ * the call overwrites; scores (2 entries: quarter-pel, bilinear; rounded to double) may be NULL.
+ * Synchronous.
+ */
+int vc1cu_b_mode_rd(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_ppic_cfg* cfg, int cur_id, int past_id,
+                    int future_id, int bslot_qpel, int bslot_bilinear, int pred_id, int* choice, double* scores);
 
 /*
  * In-loop deblocking of frame slot frame_id in place, at params->pqindex.

@@ -45,7 +45,7 @@ EXPORTS = (
     "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
-    "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture",
+    "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd",
 )
 
 
@@ -123,6 +123,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
     L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
+    L.vc1cu_b_mode_rd.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
+                                  C.POINTER(C.c_double)]
     L.vc1cu_analyze_b_picture.argtypes = [vp, PP, i32, i32, i32, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
     L.vc1cu_b_decide.argtypes = [vp, PP, C.POINTER(BPass), i32]
     L.vc1cu_read_bresult.argtypes = [vp, i32, C.POINTER(BAnalysisC)]
@@ -486,6 +488,16 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_analyze_p_picture(self._h, C.byref(params), C.byref(cfg), cur_id, ref_id, out_slot,
                                                     scratch_slot, scratch_frame, C.byref(info)))
         return info
+
+    def b_mode_rd(self, params: Params, cfg: PpicCfg, cur_id: int, past_id: int, future_id: int, bslot_qpel: int,
+                  bslot_bilinear: int, pred_id: int):
+        """analyze_b_picture's quarter-pel versus bilinear choice (vc1cu_b_mode_rd) for two B-result
+        slots: (1 when the bilinear analysis wins else 0, (quarter-pel score, bilinear score))."""
+        choice = C.c_int32()
+        scores = (C.c_double * 2)()
+        self._check(self._L.vc1cu_b_mode_rd(self._h, C.byref(params), C.byref(cfg), cur_id, past_id, future_id,
+                                            bslot_qpel, bslot_bilinear, pred_id, C.byref(choice), scores))
+        return choice.value, (scores[0], scores[1])
 
     def fast_transform_types(self, params: Params, src_id: int, pred_id: int):
         """The throughput preset's transform type (1..4) of every MB of src_id against pred_id."""

@@ -2760,26 +2760,71 @@ static uint64_t p_motion_bits(vc1cu_ctx* c, const DevParams& P, const ResultSlot
     return bits + table;
 }
 
+// The mode RD's sample (sampled_p_mode_rd :504-508, sampled_b_mode_rd :1024-1028): up to 32
+// macroblocks evenly spaced in raster order.
+static std::vector<int> mode_rd_sample(const DevParams& P) {
+    const int total = P.mbw * P.mbh;
+    std::vector<int> list;
+    if (total <= 0) return list;
+    const int wanted = std::min(kModeRdSamples, total);
+    const int stride = std::max(1, total / wanted);
+    for (int linear = 0; linear < total && (int)list.size() < wanted; linear += stride) list.push_back(linear);
+    return list;
+}
+
+// lambda = 0.75 * q^2 with q = picture_double_quant(PQINDEX, false)
+static double mode_rd_lambda(const DevParams& P) {
+    const int q = 2 * P.pq + (P.halfqp ? 1 : 0);
+    return 0.75 * static_cast<double>(q) * static_cast<double>(q);
+}
+
+// The fixed-8x8 shortcut of choose_transform_mb (encoder_transform.cpp:1610-1634): an empty
+// decision, no distortion and no bits.
+static bool fixed_8x8_shortcut(const vc1cu_ppic_cfg& cfg) {
+    return !cfg.trd.variable_transforms && cfg.fast_transform_rdo && !cfg.dquant && cfg.trd.trellis == 0;
+}
+
+// The AQ-neutral transform RD (at PQINDEX, no DQUANT, per-MB types, the picture's decision
+// coding set) of the listed macroblocks of cur_id against the prediction in frame slot pred_id.
+static std::vector<vc1cu_tdecision> sampled_decisions(vc1cu_ctx* c, const DevParams& P, const vc1cu_ppic_cfg& cfg,
+                                                      int cur_id, int pred_id, const std::vector<int>& list) {
+    const int n = (int)list.size();
+    FrameSlot& fc = frame_slot(c, cur_id);
+    FrameSlot& fp = frame_slot(c, pred_id);
+    uint8_t* base = mrd_buffer(c);
+    auto* d_list = reinterpret_cast<int*>(base + 256);
+    auto* d_out = reinterpret_cast<vc1cu_tdecision*>(base + 512);
+    ck(cudaMemcpyAsync(d_list, list.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(list)");
+    vc1cu_trd_cfg t = cfg.trd;
+    t.adaptive_quality = 0;
+    t.aq_strength = 0.0;
+    t.coding_set = P.pq <= 8 ? 1 : 3;  // chroma_coding_set(PQINDEX <= 8 ? 1 : 0, PQINDEX)
+    t.dquantfrm = 0;
+    t.frame_type = 0;
+    {
+        Timer tm(c, kXform);
+        ck(launch_trd(P, fc.view(), fp.view(), trd_tables(c), nullptr, t, nullptr, d_out, nullptr, c->stream, d_list, n),
+           "transform RD launch");
+        tm.stop(1);
+    }
+    std::vector<vc1cu_tdecision> dec(n);
+    ck(cudaMemcpyAsync(dec.data(), d_out, n * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
+       "cudaMemcpyAsync(decisions)");
+    sync_checked(c);
+    return dec;
+}
+
 // sampled_p_mode_rd (encoder_motion.cpp:488-522): the prediction of slot s against pred_ref and
-// the AQ-neutral transform RD of up to 32 evenly spaced macroblocks, combined with the motion
-// bits in long double exactly as the reference does.
+// the AQ-neutral transform RD of the sampled macroblocks, combined with the motion bits in long
+// double exactly as the reference does.
 static long double sampled_mode_rd(vc1cu_ctx* c, const DevParams& P, const vc1cu_ppic_cfg& cfg, int cur_id, int pred_ref_id,
                                    const ResultSlot& s, int mode, uint64_t motion_bits, int pred_id) {
     const int total = P.mbw * P.mbh;
-    if (total <= 0) return 0.0L;
-    const int wanted = std::min(kModeRdSamples, total);
-    const int stride = std::max(1, total / wanted);
-    std::vector<int> list;
-    for (int linear = 0; linear < total && (int)list.size() < wanted; linear += stride) list.push_back(linear);
-    const int n = (int)list.size();
-    const int q = 2 * P.pq + (P.halfqp ? 1 : 0);  // picture_double_quant(PQINDEX, false)
-    const double lambda = 0.75 * static_cast<double>(q) * static_cast<double>(q);
+    const std::vector<int> list = mode_rd_sample(P);
+    if (list.empty()) return 0.0L;
+    const double lambda = mode_rd_lambda(P);
     long double rd = 0.0L;
-    // the fixed-8x8 shortcut of choose_transform_mb (encoder_transform.cpp:1610-1634) returns an
-    // empty decision: no distortion, no bits
-    const bool shortcut = !cfg.trd.variable_transforms && cfg.fast_transform_rdo && !cfg.dquant && cfg.trd.trellis == 0;
-    if (!shortcut) {
-        FrameSlot& fc = frame_slot(c, cur_id);
+    if (!fixed_8x8_shortcut(cfg)) {
         FrameSlot& fr = frame_slot(c, pred_ref_id);
         FrameSlot& fp = alloc_frame(c, pred_id, P.W, P.H);
         {
@@ -2789,31 +2834,49 @@ static long double sampled_mode_rd(vc1cu_ctx* c, const DevParams& P, const vc1cu
             ck(cudaGetLastError(), "mc_kernel launch");
             tm.stop(1);
         }
-        uint8_t* base = mrd_buffer(c);
-        auto* d_list = reinterpret_cast<int*>(base + 256);
-        auto* d_out = reinterpret_cast<vc1cu_tdecision*>(base + 512);
-        ck(cudaMemcpyAsync(d_list, list.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(list)");
-        vc1cu_trd_cfg t = cfg.trd;  // the AQ-neutral evaluator at PQINDEX, no DQUANT, per-MB types
-        t.adaptive_quality = 0;
-        t.aq_strength = 0.0;
-        t.coding_set = P.pq <= 8 ? 1 : 3;  // chroma_coding_set(PQINDEX <= 8 ? 1 : 0, PQINDEX)
-        t.dquantfrm = 0;
-        t.frame_type = 0;
+        for (const vc1cu_tdecision& d : sampled_decisions(c, P, cfg, cur_id, pred_id, list))
+            rd += static_cast<long double>(d.distortion) + lambda * static_cast<long double>(d.estimated_bits);
+    }
+    const long double residual_per_mb = rd / static_cast<long double>(list.size());
+    const long double motion_per_mb = static_cast<long double>(motion_bits) / static_cast<long double>(total);
+    return residual_per_mb + lambda * motion_per_mb;
+}
+
+// sampled_b_mode_rd (encoder_motion.cpp:1006-1060) of the B analysis in b: the B prediction of
+// the sampled macroblocks (B-intra ones from their blocks' visible means), their AQ-neutral
+// transform RD, 72 bits of intra syntax per B-intra sample, and the analysis's motion bits.
+static long double sampled_b_rd(vc1cu_ctx* c, const DevParams& P, const vc1cu_ppic_cfg& cfg, int cur_id, int past_id,
+                                int future_id, const BSlot& b, int pred_id) {
+    const int total = P.mbw * P.mbh;
+    const std::vector<int> list = mode_rd_sample(P);
+    if (list.empty()) return 0.0L;
+    std::vector<uint8_t> modes((size_t)total);
+    vc1cu_banalysis ba{};
+    ba.modes = modes.data();
+    read_bresult(c, b, &ba);
+    const double lambda = mode_rd_lambda(P);
+    std::vector<vc1cu_tdecision> dec(list.size());  // the shortcut's empty decisions
+    if (!fixed_8x8_shortcut(cfg)) {
+        FrameSlot& fc = frame_slot(c, cur_id);
+        FrameSlot& fp = frame_slot(c, past_id);
+        FrameSlot& ff = frame_slot(c, future_id);
+        FrameSlot& fo = alloc_frame(c, pred_id, P.W, P.H);
         {
-            Timer tm(c, kXform);
-            ck(launch_trd(P, fc.view(), fp.view(), trd_tables(c), nullptr, t, nullptr, d_out, nullptr, c->stream, d_list, n),
-               "transform RD launch");
+            Timer tm(c, kMc);
+            ck(launch_b_mc(P, fc.view(), fp.view(), ff.view(), b.r.modes, b.r.fmv, b.r.bmv, b.mode, (uint8_t*)fo.view().y,
+                           (uint8_t*)fo.view().u, (uint8_t*)fo.view().v, fo.pitch_y, fo.pitch_c, c->stream),
+               "B prediction launch");
             tm.stop(1);
         }
-        std::vector<vc1cu_tdecision> dec(n);
-        ck(cudaMemcpyAsync(dec.data(), d_out, n * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
-           "cudaMemcpyAsync(decisions)");
-        sync_checked(c);
-        for (int i = 0; i < n; ++i)
-            rd += static_cast<long double>(dec[i].distortion) + lambda * static_cast<long double>(dec[i].estimated_bits);
+        dec = sampled_decisions(c, P, cfg, cur_id, pred_id, list);
     }
-    const long double residual_per_mb = rd / static_cast<long double>(n);
-    const long double motion_per_mb = static_cast<long double>(motion_bits) / static_cast<long double>(total);
+    long double rd = 0.0L;
+    for (size_t i = 0; i < list.size(); ++i) {
+        rd += static_cast<long double>(dec[i].distortion) + lambda * static_cast<long double>(dec[i].estimated_bits);
+        if (modes[(size_t)list[i]] == VC1CU_BMB_INTRA) rd += lambda * 72.0L;
+    }
+    const long double residual_per_mb = rd / static_cast<long double>(list.size());
+    const long double motion_per_mb = static_cast<long double>(ba.motion_bits) / static_cast<long double>(total);
     return residual_per_mb + lambda * motion_per_mb;
 }
 
@@ -2921,6 +2984,42 @@ int vc1cu_analyze_p_picture(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_ppi
             }
         }
         if (info) *info = inf;
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_b_mode_rd(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_ppic_cfg* cfg, int cur_id, int past_id,
+                    int future_id, int bslot_qpel, int bslot_bilinear, int pred_id, int* choice, double* scores) {
+    return guarded(c, [&]() -> int {
+        if (!cfg || !choice) throw Fail{VC1CU_ERR_ARG, "null configuration or output"};
+        if (cfg->trd.trellis < 0 || cfg->trd.trellis > 2) throw Fail{VC1CU_ERR_ARG, "invalid trellis"};
+        if (pred_id < 0 || pred_id >= kMaxSlot || pred_id == cur_id || pred_id == past_id || pred_id == future_id)
+            throw Fail{VC1CU_ERR_ARG, "invalid prediction slot"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        auto slot = [&](int id, int mode) -> const BSlot& {
+            auto it = c->bresults.find(id);
+            if (it == c->bresults.end() || !it->second.valid || it->second.mbs != P.mbw * P.mbh)
+                throw Fail{VC1CU_ERR_STATE, "B-result slot holds no analysis of this size"};
+            if (it->second.mode != mode) throw Fail{VC1CU_ERR_ARG, "B-result slot analysed in another mode"};
+            return it->second;
+        };
+        const BSlot& q = slot(bslot_qpel, VC1CU_MV_QPEL);
+        const BSlot& h = slot(bslot_bilinear, VC1CU_MV_HPEL_BILINEAR);
+        for (int id : {cur_id, past_id, future_id}) {
+            FrameSlot& f = frame_slot(c, id);
+            if (f.w != P.W || f.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        }
+        check_status(c);
+        const long double qs = sampled_b_rd(c, P, *cfg, cur_id, past_id, future_id, q, pred_id);
+        const long double hs = sampled_b_rd(c, P, *cfg, cur_id, past_id, future_id, h, pred_id);
+        *choice = hs < qs ? 1 : 0;
+        if (scores) {
+            scores[0] = static_cast<double>(qs);
+            scores[1] = static_cast<double>(hs);
+        }
         return VC1CU_OK;
     });
 }

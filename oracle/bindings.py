@@ -350,6 +350,8 @@ class Reference:
         L.ref_analyze_p_picture_cfg.restype = i32
         L.ref_p_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp]
         L.ref_p_mode_scores.restype = i32
+        L.ref_b_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp, vp, i32, i32, vp, C.POINTER(i32)]
+        L.ref_b_mode_scores.restype = i32
         L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
@@ -572,6 +574,19 @@ class Reference:
         if rc:
             raise RuntimeError("reference mode scoring threw")
         return bits, scores
+
+    def b_mode_scores(self, cfg: PpicCfg, cur, past, future, anchor_mvs, anchor_4mv, num, den):
+        """analyze_b_picture's quarter-pel and bilinear sampled_b_mode_rd scores (numpy longdouble)
+        and its choice (1: bilinear)."""
+        am = np.ascontiguousarray(anchor_mvs, np.int32).reshape(-1, 2)
+        a4 = np.ascontiguousarray(anchor_4mv, np.uint8)
+        scores = np.zeros(2, np.longdouble)
+        chosen = i32()
+        rc = self.lib.ref_b_mode_scores(self.h, C.byref(cfg), self._f(cur), self._f(past), self._f(future),
+                                        am.ctypes.data, a4.ctypes.data, num, den, scores.ctypes.data, C.byref(chosen))
+        if rc:
+            raise RuntimeError("reference B mode scoring threw")
+        return scores, chosen.value
 
     def estimate_p_motion_bits(self, a: Analysis, mode: int, intensity: bool = False) -> int:
         """estimate_p_motion_bits of analysis a made in mode (None when the reference throws)."""

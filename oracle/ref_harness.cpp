@@ -508,6 +508,38 @@ int ref_p_mode_scores(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* ref, u
     }
 }
 
+// analyze_b_picture's two analyses (encoder_motion.cpp:1066-1088) and their sampled_b_mode_rd
+// scores (:1089-1094) in long double, no forward intensity compensation; *chosen = 1 when the
+// bilinear analysis wins.
+int ref_b_mode_scores(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* past, void* future, const vc1cu_mv* anchor_mvs,
+                      const uint8_t* anchor_4mv, int fraction_num, int fraction_den, long double* scores, int* chosen) {
+    try {
+        const EncoderConfig c = ppic_config(h, pc);
+        const Vc1Encoder e(c);
+        EncoderConfig nc = c;
+        nc.adaptive_quality = false;
+        nc.aq_strength = 0.0;
+        const Vc1Encoder neutral(nc);
+        const size_t mbs = static_cast<size_t>((c.width + 15) / 16) * ((c.height + 15) / 16);
+        std::vector<MV> amv(mbs);
+        std::vector<uint8_t> a4(anchor_4mv, anchor_4mv + mbs);
+        for (size_t i = 0; i < mbs; ++i) amv[i] = MV{anchor_mvs[i].xq, anchor_mvs[i].yq};
+        const Vc1Encoder::IntensityComp none{};
+        auto q = e.analyze_b_picture_mode(F(cur), F(past), F(future), amv, a4, none, fraction_num, fraction_den,
+                                          Mode::OneMvQpel, nullptr, nullptr, nullptr);
+        auto hh = e.analyze_b_picture_mode(F(cur), F(past), F(future), amv, a4, none, fraction_num, fraction_den,
+                                           Mode::OneMvHpelBilinear, nullptr, nullptr, &q.compensated_past);
+        Frame pred = e.empty_frame();
+        scores[0] = e.sampled_b_mode_rd(F(cur), F(past), F(future), q, pred, neutral);
+        scores[1] = e.sampled_b_mode_rd(F(cur), F(past), F(future), hh, pred, neutral);
+        const auto whole = e.analyze_b_picture(F(cur), F(past), F(future), amv, a4, none, fraction_num, fraction_den);
+        *chosen = whole.mv_mode == Mode::OneMvHpelBilinear ? 1 : 0;
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
 // estimate_p_motion_bits of an analysis given as host arrays (mbw*mbh vectors, 4 block vectors
 // per MB, the 4-MV and intra flags) made in `mode`; UINT64_MAX when the reference throws.
 uint64_t ref_estimate_p_motion_bits(void* h, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs, const uint8_t* use_4mv,

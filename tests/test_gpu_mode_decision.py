@@ -9,7 +9,10 @@ against the reference's own Vc1Encoder::analyze_p_picture (oracle/_ref, scalar p
   rounded to double on both sides);
 - the whole picture: the chosen mode, the fade-compensation decision, the returned analysis bit
   for bit and its motion bits, under the default presets, scalar quantisation, 8x8-only
-  transforms, the fixed-8x8 shortcut and a faded picture whose compensated analysis wins."""
+  transforms, the fixed-8x8 shortcut and a faded picture whose compensated analysis wins;
+- the B picture's quarter-pel versus bilinear choice of analyze_b_picture: both analyses'
+  sampled_b_mode_rd scores (B-intra samples included) and the choice, at fractions 1/2, 1/3 and
+  2/3, with the same transform configurations."""
 import numpy as np
 import pytest
 
@@ -103,3 +106,40 @@ def test_picture_matches_reference(ctx, case):
     assert ctx.read_result(p, 850).equal(want) == []
     if fade is not None:
         assert info.ic.enabled and info.weighted  # the compensated analysis was kept
+
+
+B_PICTURES = {
+    # (w, h, display, pq, fraction, cfg overrides)
+    "cif_half": (176, 144, None, 8, (1, 2), {}),
+    "cropped_third_scalar": (208, 128, (203, 121), 11, (1, 3), dict(trd_trellis=0, dquant=0)),
+    "two_thirds_8x8": (160, 96, None, 5, (2, 3), dict(trd_variable_transforms=0)),
+    "fixed_8x8_shortcut": (160, 96, None, 6, (1, 2), dict(trd_variable_transforms=0, fast_transform_rdo=1, dquant=0,
+                                                          trd_trellis=0)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(B_PICTURES))
+def test_b_mode_choice_matches_reference(ctx, case):
+    """analyze_b_picture's quarter-pel versus bilinear choice (vc1cu_b_mode_rd on two vc1cu_b_decide
+    results) against the reference's own two analyses and sampled_b_mode_rd scores."""
+    w, h, disp, pq, (num, den), over = B_PICTURES[case]
+    kw = dict(display_width=disp[0], display_height=disp[1]) if disp else {}
+    p = make_params(w, h, search_range=16, local_search_range=16, pqindex=pq, **kw)
+    clip = synth.generate(w, h, 3, 470 + pq, global_px=4.0, n_objects=4, obj_min=12, obj_max=40, obj_vel=4.0, sigma=2.0)
+    for t in range(3):
+        ctx.upload_frame(t, *clip.frame(t))
+    # the future anchor (picture 2 against picture 0), then both modes' B passes and decisions
+    ctx.core_passes(p, [(2, 0, MV_QPEL, 0, -1, 870)])
+    ctx.core_passes(p, [(2, 0, MV_MIXED, 1, 870, 871)])
+    ctx.core_passes(p, [(1, 0, MV_QPEL, 0, -1, 872), (1, 2, MV_QPEL, 0, -1, 873),
+                        (1, 0, MV_HPEL_BILINEAR, 0, -1, 874), (1, 2, MV_HPEL_BILINEAR, 0, -1, 875)])
+    ctx.b_decide(p, [(1, 0, 2, 872, 873, 871, num, den, MV_QPEL, 60),
+                     (1, 0, 2, 874, 875, 871, num, den, MV_HPEL_BILINEAR, 61)])
+    cfg = make_ppic_cfg(**over)
+    choice, (qs, hs) = ctx.b_mode_rd(p, cfg, 1, 0, 2, 60, 61, 62)
+    anc = ctx.read_result(p, 871)
+    scores, chosen = Reference(p).b_mode_scores(cfg, clip.frame(1), clip.frame(0), clip.frame(2), anc.mvs,
+                                                anc.use_4mv, num, den)
+    got = np.array([qs, hs], np.float64)
+    assert np.array_equal(got.view(np.uint64), scores.astype(np.float64).view(np.uint64)), (got, scores)
+    assert choice == chosen
