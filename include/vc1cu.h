@@ -706,6 +706,18 @@ int vc1cu_loop_filter_p(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, con
                         const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
 
 /*
+ * The Main Profile P-picture deblocking (apply_p_loop_filter_plane_main,
+ * src/encoder_filter.cpp:465-608, what apply_p_loop_filter runs for WMV9 Main syntax): the
+ * filter of vc1cu_loop_filter_p with SMPTE 421M 8.6.4.1's four Main Profile exceptions - block 0
+ * of the first macroblock intra forces whole top and left borders of every inter macroblock; the
+ * luma edge between blocks 2 and 3 decides with block 1's pattern and kind; a 4x4-transformed
+ * side forces the whole border; chroma vectors compared after FASTUVMC rounding and the 8.3.6.5
+ * range limit. Same arguments and return as vc1cu_loop_filter_p.
+ */
+int vc1cu_loop_filter_p_main(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
+                             const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
+
+/*
  * Overlap smoothing of a signed (unclamped, unbiased) reconstruction in place:
  * apply_overlap_plane_signed (src/encoder_filter.cpp:217-243) on each plane, as
  * Vc1Encoder::apply_i_overlap (:344-352) and apply_p_overlap (:354-365) call it. d_y, d_u, d_v

@@ -45,7 +45,7 @@ EXPORTS = (
     "vc1cu_lp_set_params", "vc1cu_lp_prepare", "vc1cu_lp_set_labels", "vc1cu_lp_train_step", "vc1cu_lp_gradients",
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
-    "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd",
+    "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd", "vc1cu_loop_filter_p_main",
 )
 
 
@@ -136,6 +136,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_loop_filter_i.argtypes = [vp, PP, i32]
     L.vc1cu_fast_transform_types.argtypes = [vp, PP, i32, i32, vp]
     L.vc1cu_loop_filter_p.argtypes = [vp, PP, i32, vp, vp, vp, vp]
+    L.vc1cu_loop_filter_p_main.argtypes = [vp, PP, i32, vp, vp, vp, vp]
     L.vc1cu_overlap_smooth.argtypes = [vp, PP, vp, vp, vp, vp, i32]
     L.vc1cu_estimate_intensity_enqueue.argtypes = [vp, PP, vp, i32, C.POINTER(C.c_int64)]
     L.vc1cu_estimate_intensity_collect.argtypes = [vp, C.c_int64, vp, i32]
@@ -506,16 +507,18 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_fast_transform_types(self._h, C.byref(params), src_id, pred_id, out.ctypes.data))
         return out
 
-    def loop_filter(self, params: Params, frame_id: int, block_mvs=None, cbp=None, tt=None, intra=None):
+    def loop_filter(self, params: Params, frame_id: int, block_mvs=None, cbp=None, tt=None, intra=None,
+                    main_profile: bool = False):
         """In-place deblocking of frame slot frame_id: the I-like filter when block_mvs is None, else
-        the P filter of the coded blocks (per MB: 4 block vectors, 6 patterns, 6 kinds, intra bits)."""
+        the P filter of the coded blocks (per MB: 4 block vectors, 6 patterns, 6 kinds, intra bits),
+        with the Main Profile exceptions when main_profile."""
         if block_mvs is None:
             self._check(self._L.vc1cu_loop_filter_i(self._h, C.byref(params), frame_id))
             return
         b = np.ascontiguousarray(block_mvs, np.int32)
         cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
-        self._check(self._L.vc1cu_loop_filter_p(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data,
-                                                t.ctypes.data, i.ctypes.data))
+        fn = self._L.vc1cu_loop_filter_p_main if main_profile else self._L.vc1cu_loop_filter_p
+        self._check(fn(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data))
 
     def overlap_smooth(self, params: Params, d_y: int, d_u: int, d_v: int, flags=None, all_edges: bool = False):
         """In-place overlap smoothing of DEVICE int32 signed planes (padded raster, rows packed):

@@ -66,7 +66,7 @@ cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y
                                  cudaStream_t s);
 cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
-                                 cudaStream_t s);
+                                 cudaStream_t s, int main_profile);
 cudaError_t launch_overlap(int32_t* y, int32_t* u, int32_t* v, int mbw, int mbh, const uint8_t* d_flags, int all,
                            cudaStream_t s);
 cudaError_t launch_store_signed(const int32_t* y, const int32_t* u, const int32_t* v, int mbw, int mbh, int bias,
@@ -3047,8 +3047,10 @@ int vc1cu_loop_filter_i(vc1cu_ctx* c, const vc1cu_params* p, int frame_id) {
     });
 }
 
-int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs, const uint8_t* cbp,
-                        const uint8_t* tt, const uint8_t* intra) {
+// The P-picture deblocking of vc1cu_loop_filter_p (main_profile 0) and
+// vc1cu_loop_filter_p_main (1).
+static int loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs, const uint8_t* cbp,
+                         const uint8_t* tt, const uint8_t* intra, int main_profile) {
     return guarded(c, [&]() -> int {
         if (!block_mvs || !cbp || !tt || !intra) throw Fail{VC1CU_ERR_ARG, "null block metadata"};
         DevParams P;
@@ -3070,13 +3072,24 @@ int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const
         const DevFrame fr = f.view();
         Timer tm(c, kMc);
         ck(launch_loop_filter_p((uint8_t*)fr.y, (uint8_t*)fr.u, (uint8_t*)fr.v, f.pitch_y, f.pitch_c, f.w, f.h, P.pq,
-                                reinterpret_cast<const int2*>(d), d + al, d + al + 6 * mbs, d + al + 12 * mbs, c->stream),
+                                reinterpret_cast<const int2*>(d), d + al, d + al + 6 * mbs, d + al + 12 * mbs, c->stream,
+                                main_profile),
            "loop filter launch");
         tm.stop(2);
         // the metadata copies read the caller's pageable arrays; finish before returning
         ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
         return VC1CU_OK;
     });
+}
+
+int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs, const uint8_t* cbp,
+                        const uint8_t* tt, const uint8_t* intra) {
+    return loop_filter_p(c, p, frame_id, block_mvs, cbp, tt, intra, 0);
+}
+
+int vc1cu_loop_filter_p_main(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
+                             const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra) {
+    return loop_filter_p(c, p, frame_id, block_mvs, cbp, tt, intra, 1);
 }
 
 // The per-macroblock byte map of an overlap call on the device (stream-ordered after any launch

@@ -112,11 +112,12 @@ struct LfMeta {
     const uint8_t* tt;
     const uint8_t* intra;
     int mbw, mbh;
+    int main_profile;  // the Main Profile rules (apply_p_loop_filter_plane_main, encoder_filter.cpp:465-608)
 };
 
 struct LfBlock {
     int cbp, tt;
-    bool intra;
+    bool intra, mb_intra;  // this block intra; any block of its macroblock intra
     int2 mv;
 };
 
@@ -132,6 +133,7 @@ __device__ LfBlock lf_block(const LfMeta& m, int k, int bx, int by) {
     b.cbp = m.cbp[mb * 6 + bk];
     b.tt = m.tt[mb * 6 + bk];
     b.intra = (m.intra[mb] >> bk) & 1;
+    b.mb_intra = m.intra[mb] != 0;
     const int2* v = m.bmv + mb * 4;
     if (luma) {
         b.mv = v[bk];
@@ -145,7 +147,20 @@ __device__ LfBlock lf_block(const LfMeta& m, int k, int bx, int by) {
             return (imin(a, c) + imax(b2, d)) / 2;
         };
         const int cx = med4(v[0].x, v[1].x, v[2].x, v[3].x), cy = med4(v[0].y, v[1].y, v[2].y, v[3].y);
-        b.mv = make_int2(arshift(cx + ((cx & 3) == 3), 1), arshift(cy + ((cy & 3) == 3), 1));
+        int x = arshift(cx + ((cx & 3) == 3), 1), y = arshift(cy + ((cy & 3) == 3), 1);
+        if (m.main_profile) {
+            // Main Profile exception 4 (:502-523): the FASTUVMC rounding towards zero and the
+            // 8.3.6.5 range limit of the chroma vector that the decoder compares
+            x = x < 0 ? x + (x & 1) : x - (x & 1);
+            y = y < 0 ? y + (y & 1) : y - (y & 1);
+            const int ox = mx * 8, oy = my * 8;
+            const int px = ox + arshift(x, 2), py = oy + arshift(y, 2);
+            if (px < -8) x = 4 * (-8 - ox) + (x & 3);
+            else if (px > m.mbw * 8) x = 4 * (m.mbw * 8 - ox) + (x & 3);
+            if (py < -8) y = 4 * (-8 - oy) + (y & 3);
+            else if (py > m.mbh * 8) y = 4 * (m.mbh * 8 - oy) + (y & 3);
+        }
+        b.mv = make_int2(x, y);
     }
     return b;
 }
@@ -169,7 +184,10 @@ __global__ void lfp_h_kernel(LfFrame f, LfMeta m, int pq) {
             const LfBlock b = lf_block(m, k, bx, by);
             if (by + 1 < grid_h && y0 + 8 < pl.h) {
                 const LfBlock n = lf_block(m, k, bx, by + 1);
-                if (b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
+                // Main Profile exceptions 1 (block 0 of the first MB intra: every inter MB's top
+                // border filtered whole) and 3 (a 4x4-transformed side: the whole border, :547-553)
+                const bool ex = m.main_profile && (((m.intra[0] & 1) && !n.mb_intra) || b.tt == 7 || n.tt == 7);
+                if (ex || b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
                     if (half * 4 < imin(8, pl.w - x0)) lf_hgroup(pl, cx, y0 + 8, pq);
                 } else {
                     const int mask = (b.cbp | (n.cbp >> 2)) & 3;
@@ -203,10 +221,14 @@ __global__ void lfp_v_kernel(LfFrame f, LfMeta m, int pq) {
             const LfBlock b = lf_block(m, k, bx, by);
             if (bx + 1 < grid_w && x0 + 8 < pl.w) {
                 const LfBlock n = lf_block(m, k, bx + 1, by);
-                if (b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
+                // Main Profile exceptions 1 and 3, and 2: the luma edge between blocks 2 and 3
+                // decides with block 1's pattern and kind on its left (:563-581)
+                const LfBlock d = (m.main_profile && k == 0 && !(bx & 1) && (by & 1)) ? lf_block(m, k, bx + 1, by - 1) : b;
+                const bool ex = m.main_profile && (((m.intra[0] & 1) && !n.mb_intra) || d.tt == 7 || n.tt == 7);
+                if (ex || b.intra || n.intra || b.mv.x != n.mv.x || b.mv.y != n.mv.y) {
                     if (half * 4 < imin(8, pl.h - y0)) lf_vgroup(pl, x0 + 8, ry, pq);
                 } else {
-                    const int mask = (b.cbp | (n.cbp >> 1)) & 5;
+                    const int mask = (d.cbp | (n.cbp >> 1)) & 5;
                     if (half == 0 ? (mask & 4) != 0 : ((mask & 1) && y0 + 4 < pl.h)) lf_vgroup(pl, x0 + 8, ry, pq);
                 }
             }
@@ -242,9 +264,9 @@ cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y
 
 cudaError_t launch_loop_filter_p(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
                                  const int2* bmv, const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, int main_profile) {
     const LfFrame f = lf_frame(y, u, v, pitch_y, pitch_c, W, H);
-    const LfMeta m{bmv, cbp, tt, intra, (W + 15) / 16, (H + 15) / 16};
+    const LfMeta m{bmv, cbp, tt, intra, (W + 15) / 16, (H + 15) / 16, main_profile};
     const int nh = (W + 3) / 4 + 2 * ((W / 2 + 3) / 4), nv = (H + 3) / 4 + 2 * ((H / 2 + 3) / 4);
     lfp_h_kernel<<<(unsigned)((nh + 63) / 64), 64, 0, s>>>(f, m, pq);
     lfp_v_kernel<<<(unsigned)((nv + 63) / 64), 64, 0, s>>>(f, m, pq);

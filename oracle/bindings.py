@@ -355,6 +355,8 @@ class Reference:
         L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+        L.ref_motion_compensate_padded.argtypes = [vp, vp, vp, vp, vp, i32, vp]
+        L.ref_b_predict_padded.argtypes = [vp, vp, vp, vp, vp, vp, i32, vp]
         L.ref_forward_quant.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_scalar_quantize_level.argtypes = [vp, C.c_double]
         L.ref_estimate_ic.argtypes = [vp, vp, vp, vp, C.POINTER(Intensity)]
@@ -364,7 +366,7 @@ class Reference:
         L.ref_b_predict.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, vp]
         L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
         L.ref_loop_filter_i.argtypes = [vp, vp]
-        L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp, i32]
         L.ref_overlap.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
         L.ref_fast_transform_types.argtypes = [vp, vp, vp, vp]
         L.ref_analyze_b.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, C.POINTER(BAnalysisC)]
@@ -472,7 +474,7 @@ class Reference:
         self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
         return y, u, v
 
-    def loop_filter(self, frame, block_mvs=None, cbp=None, tt=None, intra=None):
+    def loop_filter(self, frame, block_mvs=None, cbp=None, tt=None, intra=None, main_profile=False):
         h, w = self.p.height, self.p.width
         f = self.frame(frame)
         if block_mvs is None:
@@ -480,7 +482,8 @@ class Reference:
         else:
             b = np.ascontiguousarray(block_mvs, np.int32)
             cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
-            self.lib.ref_loop_filter_p(self.h, f.h, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data)
+            self.lib.ref_loop_filter_p(self.h, f.h, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data,
+                                       int(main_profile))
         y = np.zeros((h, w), np.uint8)
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)
@@ -607,6 +610,33 @@ class Reference:
         v = np.zeros_like(u)
         self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
         return y, u, v
+
+    def _padded_call(self, fn):
+        mbw, mbh = mbs_of(self.p)
+        pw, ph = mbw * 16, mbh * 16
+        dst = self.frame((np.zeros((ph, pw), np.uint8), np.full((ph // 2, pw // 2), 128, np.uint8),
+                          np.full((ph // 2, pw // 2), 128, np.uint8)))
+        fn(dst)
+        y = np.zeros((ph, pw), np.uint8)
+        u = np.zeros((ph // 2, pw // 2), np.uint8)
+        v = np.zeros_like(u)
+        self.lib.ref_frame_read(dst.h, y.ctypes.data, u.ctypes.data, v.ctypes.data)
+        return y, u, v
+
+    def motion_compensate_padded(self, ref, a: Analysis, mode):
+        """motion_compensate_{mb,4mv}_padded of every macroblock from the padded reference frame
+        `ref` (mbw*16 x mbh*16 planes) into a padded destination."""
+        r = self.frame(ref)
+        return self._padded_call(lambda dst: self.lib.ref_motion_compensate_padded(
+            self.h, r.h, a.mvs.ctypes.data, a.block_mvs.ctypes.data, a.use_4mv.ctypes.data, mode, dst.h))
+
+    def b_predict_padded(self, past, future, b, mode):
+        """The B picture's padded prediction (Backward / Forward / bi) from padded references;
+        B-intra macroblocks stay zero (luma) and 128 (chroma)."""
+        pa, fu = self.frame(past), self.frame(future)
+        return self._padded_call(lambda dst: self.lib.ref_b_predict_padded(
+            self.h, pa.h, fu.h, np.ascontiguousarray(b.modes, np.uint8).ctypes.data, b.forward_mvs.ctypes.data,
+            b.backward_mvs.ctypes.data, mode, dst.h))
 
     def forward_quant(self, src, pred, type_mask=1):
         mbw, mbh = mbs_of(self.p)

@@ -374,7 +374,7 @@ void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, 
 void ref_loop_filter_i(void* h, void* frame) { E(h).apply_i_like_loop_filter(*static_cast<Frame*>(frame)); }
 
 void ref_loop_filter_p(void* h, void* frame, const vc1cu_mv* bmv, const uint8_t* cbp, const uint8_t* tt,
-                       const uint8_t* intra) {
+                       const uint8_t* intra, int main_profile) {
     const auto& c = static_cast<RefEncoder*>(h)->cfg;
     const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
     const size_t mbs = static_cast<size_t>(mbw) * mbh;
@@ -387,6 +387,13 @@ void ref_loop_filter_p(void* h, void* frame, const vc1cu_mv* bmv, const uint8_t*
             cb[i][k] = cbp[i * 6 + k];
             t[i][k] = tt[i * 6 + k];
         }
+    }
+    if (main_profile) {
+        // the Main Profile branch of apply_p_loop_filter_plane (encoder_filter.cpp:616-619)
+        EncoderConfig mc = c;
+        mc.syntax = libvc1::StreamSyntax::Wmv9Main;
+        Vc1Encoder(mc).apply_p_loop_filter(*static_cast<Frame*>(frame), b, cb, t, in, mbw, mbh);
+        return;
     }
     E(h).apply_p_loop_filter(*static_cast<Frame*>(frame), b, cb, t, in, mbw, mbh);
 }
@@ -580,6 +587,51 @@ void ref_motion_compensate(void* h, void* ref, const vc1cu_mv* mvs, const vc1cu_
                 e.motion_compensate_4mv(d, F(ref), mx, my, four);
             } else {
                 e.motion_compensate_mb(d, F(ref), mx, my, MV{mvs[pos].xq, mvs[pos].yq}, to_mode(mode));
+            }
+        }
+}
+
+// The padded-raster prediction of the picture coder's reconstruction loop
+// (motion_compensate_mb_padded / motion_compensate_4mv_padded, encoder_motion_compensation.cpp:573-660;
+// encoder_encode.cpp:1183-1195): every whole macroblock of a (mbw*16) x (mbh*16) destination from
+// a padded reference, intra MBs at zero motion.
+void ref_motion_compensate_padded(void* h, void* ref, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs,
+                                  const uint8_t* use_4mv, int mode, void* dst) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    Frame& d = *static_cast<Frame*>(dst);
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            if (use_4mv && use_4mv[pos]) {
+                std::array<MV, 4> four;
+                for (int k = 0; k < 4; ++k) four[k] = MV{block_mvs[pos * 4 + k].xq, block_mvs[pos * 4 + k].yq};
+                e.motion_compensate_4mv_padded(d, F(ref), mx, my, four);
+            } else {
+                e.motion_compensate_mb_padded(d, F(ref), mx, my, MV{mvs[pos].xq, mvs[pos].yq}, to_mode(mode));
+            }
+        }
+}
+
+// The B picture's padded-raster prediction (encoder_encode.cpp:1679-1688): Backward from the
+// future reference, Forward from the past, Direct and Interpolated with
+// motion_compensate_bi_mb_padded (:712-763); B-intra macroblocks are left as they are.
+void ref_b_predict_padded(void* h, void* past, void* future, const uint8_t* modes, const vc1cu_mv* fmv,
+                          const vc1cu_mv* bmv, int mode, void* dst) {
+    auto& e = E(h);
+    const auto& c = static_cast<RefEncoder*>(h)->cfg;
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    Frame& d = *static_cast<Frame*>(dst);
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            const MV f{fmv[pos].xq, fmv[pos].yq}, b{bmv[pos].xq, bmv[pos].yq};
+            switch (modes[pos]) {
+                case VC1CU_BMB_INTRA: break;
+                case VC1CU_BMB_BACKWARD: e.motion_compensate_mb_padded(d, F(future), mx, my, b, to_mode(mode)); break;
+                case VC1CU_BMB_FORWARD: e.motion_compensate_mb_padded(d, F(past), mx, my, f, to_mode(mode)); break;
+                default: e.motion_compensate_bi_mb_padded(d, F(past), F(future), mx, my, f, b, to_mode(mode)); break;
             }
         }
 }

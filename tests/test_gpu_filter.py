@@ -98,3 +98,37 @@ def test_loop_filter_of_padded_reconstruction(ctx, oracle):
     ctx.upload_frame(0, *blocky_frame(330, 250, 24))
     with pytest.raises(Vc1cuError, match="padded raster"):
         ctx.loop_filter(p, 0)
+
+
+@pytest.mark.parametrize("case", [(98, 66, 21, 8, False, False), (322, 242, 22, 12, True, False),
+                                  (130, 98, 23, 25, True, True), (354, 290, 24, 4, False, True)])
+def test_main_profile_p_filter_matches_reference(ctx, case):
+    """vc1cu_loop_filter_p_main against the reference's own apply_p_loop_filter under WMV9 Main
+    syntax (oracle/_ref): block 0 of the first macroblock intra or not (exception 1), every
+    transform kind (exceptions 2 and 3), and block vectors long enough to hit the chroma range
+    limit of exception 4."""
+    from lf_cases import blocky_frame, metadata
+    from oracle.bindings import Reference, ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    w, h, seed, pq, first_intra, long_mvs = case
+    p = make_params(w, h, pqindex=pq)
+    fr = blocky_frame(w, h, seed)
+    bmv, cbp, tt, intra = metadata(w, h, seed, True)
+    intra[0] = (int(intra[0]) | 1) if first_intra else (int(intra[0]) & 0xFE)
+    if long_mvs:
+        # one vector per 2x2 macroblocks, many pointing far outside the picture: neighbours share
+        # a luma vector while their range-limited chroma vectors differ
+        mbw, mbh = (w + 15) // 16, (h + 15) // 16
+        rng = np.random.default_rng(seed)
+        g = rng.integers(-4 * (w + 40), 4 * (w + 40), ((mbh + 1) // 2, (mbw + 1) // 2, 2))
+        bmv = np.repeat(np.repeat(g, 2, 0), 2, 1)[:mbh, :mbw].reshape(-1, 1, 2).repeat(4, 1).astype(np.int32)
+    ctx.upload_frame(0, *fr)
+    ctx.loop_filter(p, 0, bmv, cbp, tt, intra, main_profile=True)
+    want = Reference(p).loop_filter(fr, bmv, cbp, tt, intra, main_profile=True)
+    for got, exp, c in zip(ctx.download_frame(0, w, h), want, "yuv"):
+        assert np.array_equal(got, exp), c
+    # the Main rules change the picture against the Advanced filter on these inputs
+    adv = Reference(p).loop_filter(fr, bmv, cbp, tt, intra)
+    assert any(not np.array_equal(a, b) for a, b in zip(adv, want))
