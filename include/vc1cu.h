@@ -606,6 +606,24 @@ int vc1cu_choose_transform(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_tr
                            const uint8_t* mquant, vc1cu_tdecision* out, int16_t* levels);
 
 /*
+ * Replaces Vc1Encoder::choose_dquant_transform_mb (src/encoder_aq.cpp:280-404) for every MB: the
+ * transform RD at the MB's base MQUANT rate_base[mb] (HOST array of mbw*mbh values 1..31: the
+ * caller's rate-control base, that is rate_weighted_mquant with the residual-priority adjustment
+ * and the perceptual priority's boost, :284-310), then, with DQUANT and the perceptual scale on,
+ * the finer absolute MQUANT of a quiet block next to detail, of bright detail on dark or of
+ * predictable texture, kept when either decision codes coefficients (:318-370), else the up to
+ * three coarser MQUANTs of an unprotected coded MB, each kept when its D + lambda R beats the
+ * best so far by 0.05% (:372-403). cfg: as for vc1cu_choose_transform (dquantfrm is set per
+ * evaluation as the reference does; the fixed-8x8 shortcut of the throughput preset is
+ * vc1cu_fast_transform_types); dquant: EncoderConfig::dquant; predictable_texture:
+ * EncoderConfig::aq_predictable_texture. out, mquant (HOST mbw*mbh) and levels (HOST int16
+ * [mb][6][64] or NULL) take each MB's decision, MQUANT and levels. Synchronous.
+ */
+int vc1cu_choose_dquant(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int dquant,
+                        int predictable_texture, int src_id, int pred_id, const uint8_t* rate_base, vc1cu_tdecision* out,
+                        uint8_t* mquant, int16_t* levels);
+
+/*
  * The reconstruction a transform decision implies (evaluate_transform_parent,
  * src/encoder_transform.cpp:1569-1585): for every MB and parent block (Y0..Y3, U, V), the levels
  * of its chosen type dequantised (dequant_level at PQINDEX, :1058-1065), inverse-transformed

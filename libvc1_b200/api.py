@@ -46,6 +46,7 @@ EXPORTS = (
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
     "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd", "vc1cu_loop_filter_p_main",
+    "vc1cu_choose_dquant",
 )
 
 
@@ -121,6 +122,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_measure_fp64_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
+    L.vc1cu_choose_dquant.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, i32, i32, vp, vp, vp, vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
     L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
     L.vc1cu_b_mode_rd.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
@@ -474,6 +476,23 @@ class CudaComputeContext:
                                                    None if mq is None else mq.ctypes.data, out.ctypes.data,
                                                    None if lv is None else lv.ctypes.data))
         return out, lv
+
+    def choose_dquant(self, params: Params, cfg: TrdCfg, src_id: int, pred_id: int, rate_base, dquant: bool = True,
+                      predictable_texture: bool = False, levels: bool = True):
+        """Vc1Encoder::choose_dquant_transform_mb for every MB (vc1cu_choose_dquant) from the base
+        MQUANTs rate_base: (decisions as TDECISION_DTYPE, chosen MQUANT, levels [mb][6][64] or None)."""
+        mbw, mbh = mbs_of(params)
+        n = mbw * mbh
+        rb = np.ascontiguousarray(rate_base, np.uint8).reshape(-1)
+        if rb.size != n:
+            raise ValueError("rate_base needs one value per macroblock")
+        out = np.zeros(n, TDECISION_DTYPE)
+        mq = np.zeros(n, np.uint8)
+        lv = np.zeros((n, 6, 64), np.int16) if levels else None
+        self._check(self._L.vc1cu_choose_dquant(self._h, C.byref(params), C.byref(cfg), int(dquant),
+                                                int(predictable_texture), src_id, pred_id, rb.ctypes.data,
+                                                out.ctypes.data, mq.ctypes.data, None if lv is None else lv.ctypes.data))
+        return out, mq, lv
 
     def p_motion_bits(self, params: Params, slot: int, mode: int, intensity: bool = False) -> int:
         """Vc1Encoder::estimate_p_motion_bits of the analysis in result slot `slot` (made in mode)."""

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstddef>
 #include <chrono>
 #include <cmath>
@@ -59,7 +60,11 @@ size_t trd_tables_bytes();
 void trd_fill_tables(void* host);
 cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
                        const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
-                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list);
+                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list, double frame_mean);
+cudaError_t trd_frame_mean(const DevParams& P, const DevFrame& src, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum,
+                           cudaStream_t s, double* mean);
+cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const DevFrame& pred, const vc1cu_trd_cfg& cfg,
+                                double frame_mean, double* lscale, double* adjacency, uint8_t* bright, cudaStream_t s);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
 cudaError_t launch_p_motion_bits(const DevParams& P, const DevResult& r, int mode, unsigned long long* acc, cudaStream_t s);
 cudaError_t launch_loop_filter_i(uint8_t* y, uint8_t* u, uint8_t* v, int pitch_y, int pitch_c, int W, int H, int pq,
@@ -292,6 +297,8 @@ struct vc1cu_ctx {
     size_t trd_cap = 0;
     void* d_mrd = nullptr;      // the P mode decision's counters, sampled MB list and decisions
     size_t mrd_cap = 0;
+    void* d_dq = nullptr;       // the DQUANT search's rounds (MB lists, MQUANTs, decisions, levels, statistics)
+    size_t dq_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -1870,6 +1877,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_sp) cudaFree(c->d_sp);
     if (c->d_trd) cudaFree(c->d_trd);
     if (c->d_mrd) cudaFree(c->d_mrd);
+    if (c->d_dq) cudaFree(c->d_dq);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
     if (c->d_gcopy) cudaFree(c->d_gcopy);
@@ -2695,7 +2703,7 @@ int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_
         if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "cudaMemcpyAsync(mquant)");
         Timer tm(c, kXform);
         ck(launch_trd(P, fs.view(), fp.view(), c->d_trd_tab, mquant ? d_mq : nullptr, *cfg, d_sum, d_out,
-                      levels ? d_lv : nullptr, c->stream, nullptr, 0),
+                      levels ? d_lv : nullptr, c->stream, nullptr, 0, -1.0),
            "transform RD launch");
         tm.stop(2);
         ck(cudaMemcpyAsync(out, d_out, mbs * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
@@ -2703,6 +2711,205 @@ int vc1cu_choose_transform(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_
         if (levels)
             ck(cudaMemcpyAsync(levels, d_lv, mbs * 384 * 2, cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync(levels)");
         sync_checked(c);
+        return VC1CU_OK;
+    });
+}
+
+// ---- the DQUANT MQUANT search (choose_dquant_transform_mb, encoder_aq.cpp:280-404) ----------
+
+// Evaluation rounds of the search: the base MQUANT at PQINDEX (DQUANTFRM 0) and elsewhere
+// (DQUANTFRM 1), the finer adjacency candidate, the three coarser candidates.
+constexpr int kDqRounds = 6;
+
+int vc1cu_choose_dquant(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int dquant, int predictable_texture,
+                        int src_id, int pred_id, const uint8_t* rate_base, vc1cu_tdecision* out, uint8_t* mquant_out,
+                        int16_t* levels) {
+    return guarded(c, [&]() -> int {
+        if (!cfg || !rate_base || !out || !mquant_out) throw Fail{VC1CU_ERR_ARG, "null configuration, base MQUANT or output"};
+        if (cfg->trellis < 0 || cfg->trellis > 2 || cfg->coding_set < 0 || cfg->coding_set > 7 || cfg->frame_type < 0 ||
+            cfg->frame_type > 4)
+            throw Fail{VC1CU_ERR_ARG, "invalid transform RD configuration"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& fs = frame_slot(c, src_id);
+        FrameSlot& fp = frame_slot(c, pred_id);
+        if (fs.w != P.W || fs.h != P.H || fp.w != P.W || fp.h != P.H)
+            throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const int mbs = P.mbw * P.mbh;
+        for (int i = 0; i < mbs; ++i)
+            if (rate_base[i] < 1 || rate_base[i] > 31) throw Fail{VC1CU_ERR_ARG, "base MQUANT must be 1..31"};
+        const void* tab = trd_tables(c);
+        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t b_mq = al(mbs), b_list = al(4 * (size_t)mbs), b_out = al(mbs * sizeof(vc1cu_tdecision)),
+                     b_lv = levels ? al((size_t)mbs * 768) : 0, b_stat = al(8 * (size_t)mbs);
+        const size_t round_bytes = b_mq + b_list + b_out + b_lv;
+        uint8_t* base = static_cast<uint8_t*>(
+            ensure(c->d_dq, c->dq_cap, 256 + kDqRounds * round_bytes + 2 * b_stat + al(mbs), "cudaMalloc(DQUANT search)"));
+        auto* d_sum = reinterpret_cast<unsigned long long*>(base);
+        auto rb_at = [&](int r) { return base + 256 + (size_t)r * round_bytes; };
+        auto* d_lscale = reinterpret_cast<double*>(base + 256 + kDqRounds * round_bytes);
+        auto* d_adj = reinterpret_cast<double*>(base + 256 + kDqRounds * round_bytes + b_stat);
+        uint8_t* d_bright = base + 256 + kDqRounds * round_bytes + 2 * b_stat;
+        double frame_mean = 0.0;
+        ck(trd_frame_mean(P, fs.view(), *cfg, d_sum, c->stream, &frame_mean), "frame mean");
+        std::vector<std::vector<int>> lists(kDqRounds);
+        std::vector<std::vector<uint8_t>> mqs(kDqRounds, std::vector<uint8_t>((size_t)mbs, 0));
+        std::vector<std::vector<vc1cu_tdecision>> res(kDqRounds);
+        // round r: the transform RD of lists[r] at MQUANT mqs[r] with DQUANTFRM dqf, decisions back
+        auto run = [&](int r, int dqf) {
+            const int n = (int)lists[r].size();
+            if (!n) return;
+            uint8_t* b = rb_at(r);
+            auto* d_list = reinterpret_cast<int*>(b + b_mq);
+            auto* d_out = reinterpret_cast<vc1cu_tdecision*>(b + b_mq + b_list);
+            auto* d_lv = levels ? reinterpret_cast<int16_t*>(b + b_mq + b_list + b_out) : nullptr;
+            ck(cudaMemcpyAsync(b, mqs[r].data(), (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload MQUANT");
+            ck(cudaMemcpyAsync(d_list, lists[r].data(), 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "upload MB list");
+            vc1cu_trd_cfg t = *cfg;
+            t.dquantfrm = dqf;
+            {
+                Timer tm(c, kXform);
+                ck(launch_trd(P, fs.view(), fp.view(), tab, b, t, d_sum, d_out, d_lv, c->stream, d_list, n, frame_mean),
+                   "transform RD launch");
+                tm.stop(1);
+            }
+            res[r].resize(n);
+            ck(cudaMemcpyAsync(res[r].data(), d_out, n * sizeof(vc1cu_tdecision), cudaMemcpyDeviceToHost, c->stream),
+               "cudaMemcpyAsync(decisions)");
+            sync_checked(c);
+        };
+        // the base decision (:308-309): DQUANTFRM set where the base MQUANT is not PQINDEX
+        std::vector<vc1cu_tdecision> dec((size_t)mbs);
+        std::vector<int> mq_out((size_t)mbs), src_round((size_t)mbs), src_pos((size_t)mbs);
+        for (int mb = 0; mb < mbs; ++mb) {
+            const int r = rate_base[mb] == P.pq ? 0 : 1;
+            lists[r].push_back(mb);
+            mqs[r][mb] = rate_base[mb];
+        }
+        run(0, 0);
+        run(1, 1);
+        for (int r = 0; r < 2; ++r)
+            for (size_t i = 0; i < lists[r].size(); ++i) {
+                const int mb = lists[r][i];
+                dec[mb] = res[r][i];
+                mq_out[mb] = rate_base[mb];
+                src_round[mb] = r;
+                src_pos[mb] = (int)i;
+            }
+        if (dquant && cfg->adaptive_quality && cfg->aq_strength > 0.0) {
+            ck(launch_dquant_stats(P, fs.view(), fp.view(), *cfg, frame_mean, d_lscale, d_adj, d_bright, c->stream),
+               "DQUANT statistics launch");
+            std::vector<double> lscale((size_t)mbs), adj((size_t)mbs);
+            std::vector<uint8_t> bright((size_t)mbs);
+            ck(cudaMemcpyAsync(lscale.data(), d_lscale, 8 * (size_t)mbs, cudaMemcpyDeviceToHost, c->stream), "read scales");
+            ck(cudaMemcpyAsync(adj.data(), d_adj, 8 * (size_t)mbs, cudaMemcpyDeviceToHost, c->stream), "read adjacency");
+            ck(cudaMemcpyAsync(bright.data(), d_bright, (size_t)mbs, cudaMemcpyDeviceToHost, c->stream), "read flags");
+            sync_checked(c);
+            // the finer absolute MQUANT (:318-370)
+            std::vector<uint8_t> done((size_t)mbs, 0);
+            for (int mb = 0; mb < mbs; ++mb) {
+                const int rb = rate_base[mb];
+                if (rb <= 2 || rb < 12 || !(adj[mb] >= 0.80 || bright[mb] || predictable_texture)) continue;
+                const int implied = std::clamp(
+                    static_cast<int>(std::lround(static_cast<double>(rb) * std::sqrt(std::clamp(lscale[mb], 0.18, 1.0)))), 1, rb);
+                const int cap = adj[mb] >= 0.80 ? 16 : (bright[mb] ? 2 : 1);
+                const int protected_implied = adj[mb] >= 0.80 ? std::max(1, implied - 4) : implied;
+                const int mq = predictable_texture ? std::max(1, rb - 1) : std::max(protected_implied, rb - cap);
+                if (mq < rb) {
+                    lists[2].push_back(mb);
+                    mqs[2][mb] = (uint8_t)mq;
+                }
+            }
+            run(2, 1);
+            for (size_t i = 0; i < lists[2].size(); ++i) {
+                const int mb = lists[2][i];
+                if (res[2][i].cbp || dec[mb].cbp) {
+                    dec[mb] = res[2][i];
+                    mq_out[mb] = mqs[2][mb];
+                    src_round[mb] = 2;
+                    src_pos[mb] = (int)i;
+                    done[mb] = 1;
+                }
+            }
+            // the coarser candidates of an unprotected coded MB (:372-403), each MQUANT evaluated
+            // once; the acceptance below keeps the reference's order and 0.9995 rule
+            std::vector<int> eligible;
+            std::vector<std::array<int, 3>> cand_mq;
+            std::vector<std::array<int, 3>> cand_pos;
+            for (int mb = 0; mb < mbs; ++mb) {
+                const int rb = rate_base[mb];
+                if (rb <= 2 || done[mb] || !dec[mb].cbp || rb >= 31 || lscale[mb] < 1.0 - 1e-12) continue;
+                const int md = std::min(4, 31 - rb);
+                const std::array<int, 3> deltas = P.halfqp ? std::array<int, 3>{1, 1, 1}
+                                                           : std::array<int, 3>{std::max(1, md / 2), md, std::max(1, md - 1)};
+                std::array<int, 3> mq{}, pos{-1, -1, -1};
+                for (int k = 0; k < 3; ++k) {
+                    mq[k] = std::min(31, rb + deltas[k]);
+                    bool dup = false;
+                    for (int j = 0; j < k; ++j) dup |= mq[j] == mq[k];
+                    if (dup) continue;
+                    pos[k] = (int)lists[3 + k].size();
+                    lists[3 + k].push_back(mb);
+                    mqs[3 + k][mb] = (uint8_t)mq[k];
+                }
+                eligible.push_back(mb);
+                cand_mq.push_back(mq);
+                cand_pos.push_back(pos);
+            }
+            for (int k = 0; k < 3; ++k) run(3 + k, 1);
+            for (size_t e = 0; e < eligible.size(); ++e) {
+                const int mb = eligible[e], rb = rate_base[mb];
+                const double base_q = static_cast<double>(2 * rb + ((rb == P.pq && P.halfqp) ? 1 : 0));
+                const double lambda = 0.75 * base_q * base_q * lscale[mb];
+                auto rd = [&](const vc1cu_tdecision& t) {
+                    return t.distortion + lambda * static_cast<double>(static_cast<uint64_t>(t.estimated_bits) + (t.cbp ? 3u : 0u));
+                };
+                double best_rd = rd(dec[mb]);
+                int tried[3], n_tried = 0;
+                for (int k = 0; k < 3; ++k) {
+                    const int mq = cand_mq[e][k];
+                    if (mq <= mq_out[mb]) continue;
+                    bool again = false;
+                    for (int i = 0; i < n_tried; ++i) again |= tried[i] == mq;
+                    if (again) continue;
+                    tried[n_tried++] = mq;
+                    int r = 3 + k, pos = cand_pos[e][k];
+                    for (int j = 0; pos < 0 && j < k; ++j)  // a repeated MQUANT was evaluated at its first index
+                        if (cand_mq[e][j] == mq) {
+                            r = 3 + j;
+                            pos = cand_pos[e][j];
+                        }
+                    const double crd = rd(res[r][pos]);
+                    if (crd < best_rd * 0.9995) {
+                        dec[mb] = res[r][pos];
+                        mq_out[mb] = mq;
+                        best_rd = crd;
+                        src_round[mb] = r;
+                        src_pos[mb] = pos;
+                    }
+                }
+            }
+        }
+        for (int mb = 0; mb < mbs; ++mb) {
+            out[mb] = dec[mb];
+            mquant_out[mb] = (uint8_t)mq_out[mb];
+        }
+        if (levels) {
+            std::vector<int16_t> lv;
+            for (int r = 0; r < kDqRounds; ++r) {
+                const int n = (int)lists[r].size();
+                if (!n) continue;
+                lv.resize((size_t)n * 384);
+                ck(cudaMemcpyAsync(lv.data(), rb_at(r) + b_mq + b_list + b_out, (size_t)n * 768, cudaMemcpyDeviceToHost,
+                                   c->stream),
+                   "cudaMemcpyAsync(levels)");
+                sync_checked(c);
+                for (int mb = 0; mb < mbs; ++mb)
+                    if (src_round[mb] == r) std::memcpy(levels + (size_t)mb * 384, lv.data() + (size_t)src_pos[mb] * 384, 768);
+            }
+        }
         return VC1CU_OK;
     });
 }
@@ -2803,7 +3010,7 @@ static std::vector<vc1cu_tdecision> sampled_decisions(vc1cu_ctx* c, const DevPar
     t.frame_type = 0;
     {
         Timer tm(c, kXform);
-        ck(launch_trd(P, fc.view(), fp.view(), trd_tables(c), nullptr, t, nullptr, d_out, nullptr, c->stream, d_list, n),
+        ck(launch_trd(P, fc.view(), fp.view(), trd_tables(c), nullptr, t, nullptr, d_out, nullptr, c->stream, d_list, n, -1.0),
            "transform RD launch");
         tm.stop(1);
     }

@@ -578,9 +578,12 @@ __device__ __forceinline__ double aq_activity(const AqStats& st) {
 
 // plane (pitch) of w x h; pp the prediction (or nullptr); luma: the picture's luma plane when the
 // block is chroma (the luma context), else nullptr
+// adjacency_out (luma blocks): the quiet-block-next-to-detail term, 0 when the scale is not
+// computed (perceptual_lambda_scale's adjacency_out, encoder_aq.cpp:410, :641)
 __device__ double aq_scale(const TrdArgs& A, const uint8_t* plane, int pitch, int w, int h, int x0, int y0, int bw, int bh,
-                           const uint8_t* pp, int ppitch, const uint8_t* luma, int lpitch) {
+                           const uint8_t* pp, int ppitch, const uint8_t* luma, int lpitch, double* adjacency_out = nullptr) {
     const vc1cu_trd_cfg& c = A.cfg;
+    if (adjacency_out) *adjacency_out = 0.0;
     if (!c.adaptive_quality || c.aq_strength <= 0.0) return 1.0;
     const AqStats st = aq_stats(plane, pitch, w, h, x0, y0, bw, bh, pp, ppitch);
     if (!st.n) return 1.0;
@@ -657,6 +660,7 @@ __device__ double aq_scale(const TrdArgs& A, const uint8_t* plane, int pitch, in
     const double quietness = dclamp((18.0 - st.grad_avg) / 14.0, 0.0, 1.0);
     const double neutral_window = dclamp((190.0 - st.mean) / 120.0, 0.0, 1.0) * dclamp((st.mean - 6.0) / 30.0, 0.0, 1.0);
     const double adjacency = quietness * neutral_window * dclamp(context_activity, 0.0, 1.5);
+    if (adjacency_out) *adjacency_out = adjacency;
     double bright_field_detail = 0.0;
     if ((contrast > 0.15 || edge_density > 0.25) && w == A.P.W && h == A.P.H) {
         const double bright_field = dclamp((frame_mean - 165.0) / 55.0, 0.0, 1.0);
@@ -1291,6 +1295,31 @@ __global__ void __launch_bounds__(32 * kTrdWarps) trd_kernel(const __grid_consta
             A.levels[(size_t)item * 384 + i] = pool[chosen_all[warp][i >> 6]].q[i & 63];
 }
 
+// The DQUANT search's per-macroblock inputs (choose_dquant_transform_mb, encoder_aq.cpp:318-336):
+// the perceptual lambda scale of the MB's luma against its prediction with its adjacency term,
+// and the bright-detail-on-dark test of the source MB. One thread per MB.
+__global__ void dquant_stats_kernel(const __grid_constant__ TrdArgs A, double* lscale, double* adjacency, uint8_t* bright) {
+    const DevParams& P = A.P;
+    const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mb >= P.mbw * P.mbh) return;
+    const int x0 = (mb % P.mbw) * 16, y0 = (mb / P.mbw) * 16;
+    double adj = 0.0;
+    lscale[mb] = aq_scale(A, A.src.y, A.src.pitch_y, P.W, P.H, x0, y0, 16, 16, A.pred.y, A.pred.pitch_y, nullptr, 0, &adj);
+    adjacency[mb] = adj;
+    unsigned long long sum = 0;
+    int n = 0, hi = 0, lo = 0;
+    for (int y = 0; y < 16 && y0 + y < P.H; ++y)
+        for (int x = 0; x < 16 && x0 + x < P.W; ++x) {
+            const int v = A.src.y[(size_t)(y0 + y) * A.src.pitch_y + x0 + x];
+            sum += (unsigned long long)v;
+            ++n;
+            hi += v >= 180;
+            lo += v <= 48;
+        }
+    const double mean = n ? (double)sum / n : 128.0;
+    bright[mb] = (n && mean < 90.0 && hi >= imax(2, n / 32) && lo >= n / 2) ? 1 : 0;
+}
+
 // mean of the source luma plane (cached_luma_mean, encoder_aq.cpp:506-545): one block's partial sums
 __global__ void luma_sum_kernel(const uint8_t* y, int pitch, int W, int H, unsigned long long* sum) {
     unsigned long long s = 0;
@@ -1317,19 +1346,27 @@ void trd_fill_tables(void* host) {
     }
 }
 
-cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
-                       const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
-                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list) {
+// The source luma mean the perceptual lambda scale reads (0 when the scale is off).
+static cudaError_t frame_mean_for(const DevParams& P, const DevFrame& src, const vc1cu_trd_cfg& cfg,
+                                  unsigned long long* d_sum, cudaStream_t s, double& mean) {
+    mean = 0.0;
+    if (!cfg.adaptive_quality || cfg.aq_strength <= 0.0 || P.W <= 0 || P.H <= 0) return cudaSuccess;
     cudaError_t e;
     unsigned long long sum = 0;
-    if (cfg.adaptive_quality && cfg.aq_strength > 0.0) {
-        // the frame mean only enters the perceptual lambda scale
-        if ((e = cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
-        luma_sum_kernel<<<148, 256, 0, s>>>(src.y, src.pitch_y, P.W, P.H, d_sum);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync(&sum, d_sum, sizeof sum, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    }
+    if ((e = cudaMemsetAsync(d_sum, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+    luma_sum_kernel<<<148, 256, 0, s>>>(src.y, src.pitch_y, P.W, P.H, d_sum);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(&sum, d_sum, sizeof sum, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    mean = (double)sum / (double)((size_t)P.W * P.H);
+    return cudaSuccess;
+}
+
+cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& pred, const void* tables,
+                       const uint8_t* mquant, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum, vc1cu_tdecision* out,
+                       int16_t* levels, cudaStream_t s, const int* mb_list, int n_list, double frame_mean) {
+    cudaError_t e;
+    if (frame_mean < 0.0 && (e = frame_mean_for(P, src, cfg, d_sum, s, frame_mean)) != cudaSuccess) return e;
     TrdArgs a;
     a.P = P;
     a.src = src;
@@ -1337,7 +1374,7 @@ cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& 
     a.tab = static_cast<const TrdTables*>(tables);
     a.mquant = mquant;
     a.cfg = cfg;
-    a.frame_mean = (P.W > 0 && P.H > 0) ? (double)sum / (double)((size_t)P.W * P.H) : 0.0;
+    a.frame_mean = frame_mean < 0.0 ? 0.0 : frame_mean;
     a.out = out;
     a.levels = levels;
     a.mb_list = mb_list;
@@ -1345,6 +1382,27 @@ cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& 
     const int items = mb_list ? n_list : P.mbw * P.mbh;
     if (items <= 0) return cudaSuccess;
     trd_kernel<<<(items + kTrdWarps - 1) / kTrdWarps, 32 * kTrdWarps, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// The source luma mean of the perceptual lambda scale (for launches that share it).
+cudaError_t trd_frame_mean(const DevParams& P, const DevFrame& src, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum,
+                           cudaStream_t s, double* mean) {
+    return frame_mean_for(P, src, cfg, d_sum, s, *mean);
+}
+
+// The DQUANT search's per-MB scale, adjacency and bright-on-dark flags.
+cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const DevFrame& pred, const vc1cu_trd_cfg& cfg,
+                                double frame_mean, double* lscale, double* adjacency, uint8_t* bright, cudaStream_t s) {
+    TrdArgs a{};
+    a.P = P;
+    a.src = src;
+    a.pred = pred;
+    a.cfg = cfg;
+    a.frame_mean = frame_mean;
+    const int mbs = P.mbw * P.mbh;
+    if (mbs <= 0) return cudaSuccess;
+    dquant_stats_kernel<<<(mbs + 127) / 128, 128, 0, s>>>(a, lscale, adjacency, bright);
     return cudaGetLastError();
 }
 

@@ -381,6 +381,7 @@ class Reference:
         L.ref_bench_gop_same.argtypes = L.ref_bench_gop_multi.argtypes
         L.ref_bench_gop_same.restype = u64
         L.ref_choose_transform.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.ref_choose_dquant.argtypes = [vp, vp, i32, i32, C.c_double, C.c_double, vp, vp, vp, vp, vp, vp]
         L.ref_choose_transform.restype = None
         L.ref_ac_direct_bits.argtypes = [i32, i32, i32, i32]
         L.ref_ac_direct_bits.restype = i32
@@ -672,6 +673,22 @@ class Reference:
         self.lib.ref_choose_transform(self.h, C.addressof(cfg), self._f(src), self._f(pred),
                                       None if mq is None else mq.ctypes.data, out.ctypes.data, lv.ctypes.data)
         return out, lv
+
+    def choose_dquant(self, cfg, src, pred, dquant=True, predictable=False, block_weight=1.0, residual_mean=0.0):
+        """Vc1Encoder::choose_dquant_transform_mb of every MB (ref_choose_dquant): (base MQUANT the
+        function starts from, decisions, chosen MQUANT, levels)."""
+        from libvc1_b200.abi import TDECISION_DTYPE
+
+        mbw, mbh = mbs_of(self.p)
+        n = mbw * mbh
+        rb = np.zeros(n, np.uint8)
+        out = np.zeros(n, TDECISION_DTYPE)
+        mq = np.zeros(n, np.uint8)
+        lv = np.zeros((n, 6, 64), np.int16)
+        self.lib.ref_choose_dquant(self.h, C.addressof(cfg), int(dquant), int(predictable), block_weight, residual_mean,
+                                   self._f(src), self._f(pred), rb.ctypes.data, out.ctypes.data, mq.ctypes.data,
+                                   lv.ctypes.data)
+        return rb, out, mq, lv
 
     def ac_direct_bits(self, coding_set, run, level, last):
         return self.lib.ref_ac_direct_bits(coding_set, run, level, int(last))

@@ -686,8 +686,8 @@ int ref_scalar_quantize_level(void* h, double coeff) { return E(h).scalar_quanti
 // Vc1Encoder::choose_transform_mb (encoder_transform.cpp:1605-1780) for every MB of src against
 // pred, with the handle's configuration and the transform RD fields of t (trellis, AQ, variable
 // transforms, extended signaling, HRD; the throughput shortcut off); mquant per MB (NULL: PQINDEX).
-void ref_choose_transform(void* h, const vc1cu_trd_cfg* t, void* src, void* pred, const uint8_t* mquant,
-                          vc1cu_tdecision* out, int16_t* levels) {
+// The harness encoder's configuration with a vc1cu_trd_cfg's EncoderConfig fields.
+static EncoderConfig trd_config(void* h, const vc1cu_trd_cfg* t) {
     EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
     c.trellis = t->trellis;
     c.adaptive_quality = t->adaptive_quality != 0;
@@ -696,6 +696,34 @@ void ref_choose_transform(void* h, const vc1cu_trd_cfg* t, void* src, void* pred
     c.extended_transform_signaling = t->extended_transform_signaling != 0;
     c.hrd_enabled = t->hrd_enabled != 0;
     c.fast_transform_rdo = false;
+    return c;
+}
+
+// An MbTransformDecision as a vc1cu_tdecision (and its 6 x 64 levels when levels is set).
+static void fill_tdecision(const Vc1Encoder::MbTransformDecision& d, vc1cu_tdecision* out, int16_t* levels) {
+    vc1cu_tdecision& o = *out;
+    std::memset(&o, 0, sizeof o);
+    o.type = static_cast<uint8_t>(d.type);
+    o.signal_level = static_cast<uint8_t>(d.signal_level == Vc1Encoder::TransformSignalLevel::Macroblock
+                                              ? 0
+                                              : (d.signal_level == Vc1Encoder::TransformSignalLevel::Block ? 1 : 2));
+    o.cbp = d.cbp;
+    o.estimated_bits = static_cast<uint32_t>(d.estimated_bits);
+    o.distortion = d.distortion;
+    for (int k = 0; k < 6; ++k) {
+        const auto& p = d.parents[static_cast<size_t>(k)];
+        o.parent_type[k] = static_cast<uint8_t>(p.type);
+        o.skip_mask[k] = p.skip_mask;
+        o.parent_bits[k] = static_cast<uint32_t>(p.estimated_bits);
+        o.parent_distortion[k] = p.distortion;
+        if (levels)
+            for (int i = 0; i < 64; ++i) levels[k * 64 + i] = p.qcoeff[static_cast<size_t>(i)];
+    }
+}
+
+void ref_choose_transform(void* h, const vc1cu_trd_cfg* t, void* src, void* pred, const uint8_t* mquant,
+                          vc1cu_tdecision* out, int16_t* levels) {
+    const EncoderConfig c = trd_config(h, t);
     Vc1Encoder e(c);
     Vc1Encoder::TransformPicturePlan plan;
     plan.frame_level = t->frame_type > 0;
@@ -707,24 +735,57 @@ void ref_choose_transform(void* h, const vc1cu_trd_cfg* t, void* src, void* pred
             const auto d = e.choose_transform_mb(F(src), F(pred), mx, my, t->coding_set, t->use_vlc != 0,
                                                  mquant ? mquant[pos] : 0, t->dquantfrm != 0,
                                                  t->frame_type > 0 ? &plan : nullptr);
-            vc1cu_tdecision& o = out[pos];
-            std::memset(&o, 0, sizeof o);
-            o.type = static_cast<uint8_t>(d.type);
-            o.signal_level = static_cast<uint8_t>(d.signal_level == Vc1Encoder::TransformSignalLevel::Macroblock
-                                                      ? 0
-                                                      : (d.signal_level == Vc1Encoder::TransformSignalLevel::Block ? 1 : 2));
-            o.cbp = d.cbp;
-            o.estimated_bits = static_cast<uint32_t>(d.estimated_bits);
-            o.distortion = d.distortion;
-            for (int k = 0; k < 6; ++k) {
-                const auto& p = d.parents[static_cast<size_t>(k)];
-                o.parent_type[k] = static_cast<uint8_t>(p.type);
-                o.skip_mask[k] = p.skip_mask;
-                o.parent_bits[k] = static_cast<uint32_t>(p.estimated_bits);
-                o.parent_distortion[k] = p.distortion;
-                if (levels)
-                    for (int i = 0; i < 64; ++i) levels[(pos * 6 + k) * 64 + i] = p.qcoeff[static_cast<size_t>(i)];
+            fill_tdecision(d, out + pos, levels ? levels + pos * 384 : nullptr);
+        }
+}
+
+
+// choose_dquant_transform_mb (encoder_aq.cpp:280-404) of every MB under a transform configuration,
+// the DQUANT switches and the rate-control hooks it reads (rc_inter_block_weight,
+// rc_prediction_residual_mean). rate_base receives each MB's base MQUANT as the function forms it
+// (:284-310, restated here from the same member functions) for the device search to start from.
+void ref_choose_dquant(void* h, const vc1cu_trd_cfg* t, int dquant, int predictable, double block_weight,
+                       double residual_mean, void* src, void* pred, uint8_t* rate_base, vc1cu_tdecision* out,
+                       uint8_t* mquant, int16_t* levels) {
+    EncoderConfig c = trd_config(h, t);
+    c.dquant = dquant != 0;
+    c.aq_predictable_texture = predictable != 0;
+    c.rc_inter_block_weight = block_weight;
+    c.rc_prediction_residual_mean = residual_mean;
+    const Vc1Encoder e(c);
+    Vc1Encoder::TransformPicturePlan plan;
+    plan.frame_level = t->frame_type > 0;
+    plan.frame_type = static_cast<Vc1Encoder::TransformType>(t->frame_type > 0 ? t->frame_type : 1);
+    const Frame& s = F(src);
+    const Frame& pr = F(pred);
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    for (int my = 0; my < mbh; ++my)
+        for (int mx = 0; mx < mbw; ++mx) {
+            const size_t pos = static_cast<size_t>(my) * mbw + mx;
+            int rb = e.rate_weighted_mquant(c.rc_inter_block_weight);
+            if (c.rc_prediction_residual_mean > 0.0) {
+                const int x0 = mx * 16, y0 = my * 16;
+                const int bw = std::max(0, std::min(16, c.visible_width() - x0));
+                const int bh = std::max(0, std::min(16, c.visible_height() - y0));
+                uint64_t sad = 0;
+                for (int y = 0; y < bh; ++y)
+                    for (int x = 0; x < bw; ++x) {
+                        const size_t o = static_cast<size_t>(y0 + y) * c.width + x0 + x;
+                        sad += static_cast<uint64_t>(std::abs(static_cast<int>(s.y[o]) - static_cast<int>(pr.y[o])));
+                    }
+                const double local_mae = (bw > 0 && bh > 0) ? static_cast<double>(sad) / static_cast<double>(bw * bh) : 0.0;
+                rb = e.residual_priority_mquant(rb, local_mae, c.rc_prediction_residual_mean);
             }
+            if (c.adaptive_quality && c.aq_strength > 0.0 && c.dquant && rb > 1) {
+                const auto priority = e.perceptual_mb_priority(s, mx, my, false);
+                const int delta = std::clamp(static_cast<int>(std::lround(priority.requested_q_boost)), 0, std::min(2, rb - 1));
+                rb = std::max(1, rb - delta);
+            }
+            rate_base[pos] = static_cast<uint8_t>(rb);
+            const auto q = e.choose_dquant_transform_mb(s, pr, mx, my, t->coding_set, t->use_vlc != 0,
+                                                        t->frame_type > 0 ? &plan : nullptr);
+            mquant[pos] = static_cast<uint8_t>(q.mquant);
+            fill_tdecision(q.tx, out + pos, levels ? levels + pos * 384 : nullptr);
         }
 }
 
