@@ -18,12 +18,18 @@
  *   5. the fade and scene-cut analysis: estimate_intensity_comp and
  *      intensity_compensated_reference (encoder_motion_compensation.cpp:175-348) and
  *      scene_change_score (encoder_motion.cpp:599-676);
- *   6. the transform RD, Vc1Encoder::choose_transform_mb (encoder_transform.cpp:1605-1780), as
- *      vc1cu_fast_transform_types / vc1cu_choose_transform;
+ *   6. the transform RD, Vc1Encoder::choose_transform_mb (encoder_transform.cpp:1605-1780), and
+ *      its DQUANT search, choose_dquant_transform_mb (encoder_aq.cpp:280-404), as
+ *      vc1cu_fast_transform_types / vc1cu_choose_transform / vc1cu_choose_dquant;
  *   7. the picture-level motion-mode decisions, analyze_p_picture (encoder_motion.cpp:524-597)
  *      with estimate_p_motion_bits and sampled_p_mode_rd, and the quarter-pel versus bilinear
  *      choice of analyze_b_picture (:1006-1095), as vc1cu_analyze_p_picture /
- *      vc1cu_p_motion_bits / vc1cu_b_mode_rd.
+ *      vc1cu_p_motion_bits / vc1cu_b_mode_rd;
+ *   8. the reconstruction side: the B prediction, the inverse transforms, the I picture's intra
+ *      reconstruction (reconstruct_i_signed_padded, encoder_encode.cpp:814-887), the in-loop
+ *      deblocking (Advanced and Main Profile) and overlap smoothing, as vc1cu_b_predict /
+ *      vc1cu_reconstruct / vc1cu_reconstruct_intra / vc1cu_loop_filter_i / _p / _p_main /
+ *      vc1cu_overlap_smooth / vc1cu_store_signed.
  *
  * Conventions: every function is extern "C", returns an int status (VC1CU_OK on
  * success), never throws, and records a message retrievable with vc1cu_last_error().
@@ -734,6 +740,23 @@ int vc1cu_loop_filter_p(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, con
  */
 int vc1cu_loop_filter_p_main(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
                              const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra);
+
+/*
+ * The signed intra reconstruction of an I picture, Vc1Encoder::reconstruct_i_signed_padded
+ * (src/encoder_encode.cpp:814-887) with scalar AC quantisation (trellis 0) and AC coding: for every
+ * 8x8 block of frame slot src_id the intra forward transform (forward_transform, samples outside
+ * the source read 0 luma / 128 chroma), the AC levels at the MB's MQUANT, the DC level whose
+ * reconstruction is nearest the padded block mean, predicted from its neighbours and clamped to
+ * the DC range (predict_dc_dquant with the DQUANT scaling, clamp_dc_target_for_diff), the
+ * dequantised coefficients and the 8x8 inverse transform, into the DEVICE int32 planes d_y, d_u,
+ * d_v of the padded raster, rows packed (the layout vc1cu_overlap_smooth and vc1cu_store_signed
+ * take). overlap: 0 none, 1 all, 2 select with the HOST per-MB flags: the overlap plan whose edge
+ * source (make_overlap_edge_source, :13-63) the transform reads. mquant / derived: HOST per-MB
+ * MQUANT (1..31) and DQUANT-derived flags of the picture's DQUANT plan, or NULL for PQINDEX and
+ * none. Returns once its inputs are copied.
+ */
+int vc1cu_reconstruct_intra(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int overlap, const uint8_t* flags,
+                            const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v);
 
 /*
  * Overlap smoothing of a signed (unclamped, unbiased) reconstruction in place:

@@ -46,7 +46,7 @@ EXPORTS = (
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
     "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd", "vc1cu_loop_filter_p_main",
-    "vc1cu_choose_dquant",
+    "vc1cu_choose_dquant", "vc1cu_reconstruct_intra",
 )
 
 
@@ -123,6 +123,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_choose_dquant.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, i32, i32, vp, vp, vp, vp]
+    L.vc1cu_reconstruct_intra.argtypes = [vp, PP, i32, i32, vp, vp, vp, vp, vp, vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
     L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
     L.vc1cu_b_mode_rd.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
@@ -538,6 +539,16 @@ class CudaComputeContext:
         cb, t, i = (np.ascontiguousarray(a, np.uint8) for a in (cbp, tt, intra))
         fn = self._L.vc1cu_loop_filter_p_main if main_profile else self._L.vc1cu_loop_filter_p
         self._check(fn(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data))
+
+    def reconstruct_intra(self, params: Params, src_id: int, d_y: int, d_u: int, d_v: int, overlap: int = 0,
+                          flags=None, mquant=None, derived=None):
+        """The signed intra reconstruction of I picture src_id into DEVICE int32 planes of the padded
+        raster (vc1cu_reconstruct_intra): overlap 0 none / 1 all / 2 select with per-MB flags; the
+        DQUANT plan's per-MB MQUANT and derived flags, or None for PQINDEX."""
+        arrs = [None if a is None else np.ascontiguousarray(a, np.uint8) for a in (flags, mquant, derived)]
+        self._check(self._L.vc1cu_reconstruct_intra(self._h, C.byref(params), src_id, overlap,
+                                                    *[None if a is None else a.ctypes.data for a in arrs], d_y, d_u,
+                                                    d_v))
 
     def overlap_smooth(self, params: Params, d_y: int, d_u: int, d_v: int, flags=None, all_edges: bool = False):
         """In-place overlap smoothing of DEVICE int32 signed planes (padded raster, rows packed):

@@ -63,6 +63,10 @@ cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& 
                        int16_t* levels, cudaStream_t s, const int* mb_list, int n_list, double frame_mean);
 cudaError_t trd_frame_mean(const DevParams& P, const DevFrame& src, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum,
                            cudaStream_t s, double* mean);
+size_t intra_scratch_bytes(const DevParams& P);
+cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int overlap, const uint8_t* d_flags,
+                               const uint8_t* d_mquant, const uint8_t* d_derived, void* scratch, uint8_t* edge,
+                               int32_t* oy, int32_t* ou, int32_t* ov, cudaStream_t s);
 cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const DevFrame& pred, const vc1cu_trd_cfg& cfg,
                                 double frame_mean, double* lscale, double* adjacency, uint8_t* bright, cudaStream_t s);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
@@ -299,6 +303,8 @@ struct vc1cu_ctx {
     size_t mrd_cap = 0;
     void* d_dq = nullptr;       // the DQUANT search's rounds (MB lists, MQUANTs, decisions, levels, statistics)
     size_t dq_cap = 0;
+    void* d_intra = nullptr;    // the intra reconstruction's levels, DC grids, maps and edge source
+    size_t intra_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -1878,6 +1884,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_trd) cudaFree(c->d_trd);
     if (c->d_mrd) cudaFree(c->d_mrd);
     if (c->d_dq) cudaFree(c->d_dq);
+    if (c->d_intra) cudaFree(c->d_intra);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
     if (c->d_gcopy) cudaFree(c->d_gcopy);
@@ -3297,6 +3304,42 @@ int vc1cu_loop_filter_p(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const
 int vc1cu_loop_filter_p_main(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, const vc1cu_mv* block_mvs,
                              const uint8_t* cbp, const uint8_t* tt, const uint8_t* intra) {
     return loop_filter_p(c, p, frame_id, block_mvs, cbp, tt, intra, 1);
+}
+
+int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int overlap, const uint8_t* flags,
+                            const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v) {
+    return guarded(c, [&]() -> int {
+        if (!d_y || !d_u || !d_v) throw Fail{VC1CU_ERR_ARG, "null signed plane"};
+        if (overlap < 0 || overlap > 2) throw Fail{VC1CU_ERR_ARG, "overlap is 0 none, 1 all or 2 select"};
+        if (overlap == 2 && !flags) throw Fail{VC1CU_ERR_ARG, "null overlap flags"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& fs = frame_slot(c, src_id);
+        if (fs.w != P.W || fs.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        if (mquant)
+            for (size_t i = 0; i < mbs; ++i)
+                if (mquant[i] < 1 || mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 1..31"};
+        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t b_scr = al(intra_scratch_bytes(P)), b_edge = al(mbs * 256 * 3 / 2), b_map = al(mbs);
+        uint8_t* base = static_cast<uint8_t*>(
+            ensure(c->d_intra, c->intra_cap, b_scr + b_edge + 3 * b_map, "cudaMalloc(intra reconstruction)"));
+        uint8_t* d_flags = base + b_scr + b_edge;
+        uint8_t* d_mq = d_flags + b_map;
+        uint8_t* d_der = d_mq + b_map;
+        if (overlap == 2) ck(cudaMemcpyAsync(d_flags, flags, mbs, cudaMemcpyHostToDevice, c->stream), "upload overlap flags");
+        if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "upload MQUANT");
+        if (derived) ck(cudaMemcpyAsync(d_der, derived, mbs, cudaMemcpyHostToDevice, c->stream), "upload derived flags");
+        Timer tm(c, kXform);
+        ck(launch_intra_recon(P, fs.view(), overlap, overlap == 2 ? d_flags : nullptr, mquant ? d_mq : nullptr,
+                              derived ? d_der : nullptr, base, base + b_scr, d_y, d_u, d_v, c->stream),
+           "intra reconstruction launch");
+        tm.stop(overlap ? 4 : 3);
+        ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");  // the copies read the caller's arrays
+        return VC1CU_OK;
+    });
 }
 
 // The per-macroblock byte map of an overlap call on the device (stream-ordered after any launch

@@ -1295,6 +1295,214 @@ __global__ void __launch_bounds__(32 * kTrdWarps) trd_kernel(const __grid_consta
             A.levels[(size_t)item * 384 + i] = pool[chosen_all[warp][i >> 6]].q[i & 63];
 }
 
+// ---- I-picture intra reconstruction (reconstruct_i_signed_padded, encoder_encode.cpp:814-887) ----
+
+// dc_scale (encoder_entropy.cpp:369-375): the DC step of MQUANT 1..31
+__device__ __forceinline__ int intra_dc_scale(int q) {
+    return q <= 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 4 : (q <= 5 ? 8 : q / 2 + 6)));
+}
+// DQScale (SMPTE 421M 8.1.3.4, dqscale_value :434-447): round(2^18 / n) for n = index + 1
+__device__ __forceinline__ int intra_dqscale(int index) {
+    const int n = index + 1;
+    return (0x40000 + n / 2) / n;
+}
+// reconstruct_dc_sample_with_bias (:383-389)
+__device__ __forceinline__ int intra_dc_sample(int qdc, int mq, int bias) {
+    int x = qdc * intra_dc_scale(mq);
+    x = arshift(3 * x + 1, 1);
+    x = arshift(3 * x + 16, 5);
+    return min(255, max(0, bias + x));
+}
+// choose_dc_for_mean_with_bias (:395-412): the DC level whose reconstruction is nearest the mean
+__device__ int intra_dc_for_mean(int mean, int mq, int bias) {
+    const int bits = 8 + ((mq == 1 || mq == 2) ? 3 - mq : 0);
+    const int maxq = (1 << bits) - 1;
+    int lo = -maxq, hi = maxq;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (intra_dc_sample(mid, mq, bias) < mean) lo = mid + 1;
+        else hi = mid;
+    }
+    int best = lo;
+    if (lo > -maxq && iabs(intra_dc_sample(lo - 1, mq, bias) - mean) <= iabs(intra_dc_sample(lo, mq, bias) - mean)) best = lo - 1;
+    return best;
+}
+// scale_dc_predictor (:449-456)
+__device__ __forceinline__ int intra_scale_dc(int value, int from_q, int to_q) {
+    from_q = iabs(from_q);
+    to_q = iabs(to_q);
+    if (!from_q || from_q == to_q) return value;
+    const int idx = intra_dc_scale(to_q) - 1;
+    if (idx < 0) return 0;
+    const long long v = (long long)value * intra_dc_scale(from_q) * intra_dqscale(idx);
+    return (int)((v + 0x20000) >> 18);
+}
+
+// The intra source, its MQUANT map and the per-block outputs of one I picture.
+struct IntraArgs {
+    DevParams P;
+    const uint8_t* y;
+    const uint8_t* u;
+    const uint8_t* v;
+    int pitch_y, pitch_c, sw, sh;  // the intra source's luma raster (the picture or its edge source)
+    const uint8_t* mquant;         // per MB (nullptr: PQINDEX)
+    const uint8_t* derived;        // per MB DQUANT-derived flag (nullptr: none)
+    int16_t* q;                    // [mb][6][64] AC levels
+    int* dc[3];                    // per plane block grid: the DC target, then the final DC
+    int* qg[3];                    // per plane block grid: MQUANT, negative when derived
+};
+
+__device__ __forceinline__ int intra_mq(const IntraArgs& A, int mb) {
+    return (A.mquant && A.mquant[mb] >= 1) ? (int)A.mquant[mb] : A.P.pq;
+}
+
+// One thread per (MB, block): forward_transform (:672-795; samples outside the source read the
+// pad value, 0 luma / 128 chroma, minus 128), scalar_quantize_level of the AC coefficients
+// (quantize_ac :2090-2144 at trellis 0) and choose_dc_for_mean of the padded block mean.
+__global__ void intra_fwd_kernel(const __grid_constant__ IntraArgs A) {
+    const DevParams& P = A.P;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.mbw * P.mbh * 6) return;
+    const int mb = i / 6, k = i % 6, mx = mb % P.mbw, my = mb / P.mbw;
+    const bool chroma = k >= 4;
+    const uint8_t* p = chroma ? (k == 4 ? A.u : A.v) : A.y;
+    const int pitch = chroma ? A.pitch_c : A.pitch_y, w = chroma ? A.sw / 2 : A.sw, h = chroma ? A.sh / 2 : A.sh;
+    const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
+    const int x0 = bx * 8, y0 = by * 8, pad = chroma ? 128 : 0;
+    const int mq = intra_mq(A, mb);
+    const bool derived = A.derived && A.derived[mb];
+    int r[8][8];
+    unsigned sum = 0;
+    for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x) {
+            const int sx = x0 + x, sy = y0 + y;
+            const int v = (sx < w && sy < h) ? (int)__ldg(p + (size_t)sy * pitch + sx) : pad;
+            sum += (unsigned)v;
+            r[y][x] = v - 128;
+        }
+    double tmp[8][8];
+    for (int a = 0; a < 8; ++a)
+        for (int x = 0; x < 8; ++x) {
+            double acc = 0.0;
+            for (int y = 0; y < 8; ++y) acc = __dadd_rn(acc, __dmul_rn(c_k8[a][y], (double)r[y][x]));
+            tmp[a][x] = acc;
+        }
+    int16_t* q = A.q + (size_t)i * 64;
+    q[0] = 0;
+    for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b) {
+            if (!a && !b) continue;
+            double acc = 0.0;
+            for (int x = 0; x < 8; ++x) acc = __dadd_rn(acc, __dmul_rn(tmp[a][x], c_k8[b][x]));
+            q[b * 8 + a] = (int16_t)trd_squant(P, __dmul_rn(1024.0, acc), mq, derived);  // c[row*8+col] = xform[col][row]
+        }
+    const int gw = chroma ? P.mbw : P.mbw * 2;
+    A.dc[chroma ? k - 3 : 0][by * gw + bx] = intra_dc_for_mean((int)((sum + 32u) / 64u), mq, 128);
+}
+
+// predict_dc_dquant + clamp_dc_target_for_diff (encoder_entropy.cpp:549-571, :426-432) along the
+// block grid of plane blockIdx.x (0 luma, 1 U, 2 V): a block's prediction reads its left, top
+// and top-left neighbours' final DC, so the grid is walked by anti-diagonals.
+__global__ void intra_dc_kernel(const __grid_constant__ IntraArgs A) {
+    const DevParams& P = A.P;
+    const int pl = blockIdx.x;
+    const int gw = pl ? P.mbw : P.mbw * 2, gh = pl ? P.mbh : P.mbh * 2;
+    int* g = A.dc[pl];
+    int* qg = A.qg[pl];
+    for (int d = 0; d < gw + gh - 1; ++d) {
+        for (int y = max(0, d - gw + 1) + (int)threadIdx.x; y <= min(d, gh - 1); y += blockDim.x) {
+            const int x = d - y;
+            const int mb = pl ? y * P.mbw + x : (y >> 1) * P.mbw + (x >> 1);
+            const int mq = intra_mq(A, mb);
+            const bool a_avail = y > 0, c_avail = x > 0;
+            int a = 0, b = 0, c = 0;
+            if (a_avail) a = intra_scale_dc(g[(y - 1) * gw + x], qg[(y - 1) * gw + x], mq);
+            if (c_avail) c = intra_scale_dc(g[y * gw + x - 1], qg[y * gw + x - 1], mq);
+            if (a_avail && c_avail) b = intra_scale_dc(g[(y - 1) * gw + x - 1], qg[(y - 1) * gw + x - 1], mq);
+            const bool left = c_avail && (!a_avail || iabs(a - b) <= iabs(b - c));
+            const int pred = left ? c : (a_avail ? a : 0);
+            const int bits = 8 + ((mq == 1 || mq == 2) ? 3 - mq : 0);
+            const int maxv = (1 << bits) - 1;
+            const int diff = min(maxv, max(-maxv, g[y * gw + x] - pred));
+            g[y * gw + x] = min(maxv, max(-maxv, pred + diff));
+            qg[y * gw + x] = (A.derived && A.derived[mb]) ? -mq : mq;
+        }
+        __syncthreads();
+    }
+}
+
+// One thread per (MB, block): the coefficients (DC * dc_scale, dequant_level of the AC levels),
+// inverse_transform_8x8 and the signed samples into the padded raster (rows packed).
+__global__ void intra_inv_kernel(const __grid_constant__ IntraArgs A, int32_t* oy, int32_t* ou, int32_t* ov) {
+    const DevParams& P = A.P;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.mbw * P.mbh * 6) return;
+    const int mb = i / 6, k = i % 6, mx = mb % P.mbw, my = mb / P.mbw;
+    const bool chroma = k >= 4;
+    const int bx = chroma ? mx : mx * 2 + (k & 1), by = chroma ? my : my * 2 + ((k >> 1) & 1);
+    const int gw = chroma ? P.mbw : P.mbw * 2;
+    const int mq = intra_mq(A, mb);
+    const bool derived = A.derived && A.derived[mb];
+    const int16_t* q = A.q + (size_t)i * 64;
+    int a[64], tmp[64];
+    a[0] = A.dc[chroma ? k - 3 : 0][by * gw + bx] * intra_dc_scale(mq);
+    for (int j = 1; j < 64; ++j) a[j] = trd_dequant(P, q[j], mq, derived);
+    for (int j = 0; j < 64; ++j) tmp[j] = 0;
+    for (int col = 0; col < 8; ++col) inv8(a + col, 8, tmp + col * 8, 1, 4, 3, 0);
+    for (int col = 0; col < 8; ++col) inv8(tmp + col, 8, a + col, 8, 64, 7, 1);
+    int32_t* o = chroma ? (k == 4 ? ou : ov) : oy;
+    const int ow = chroma ? P.mbw * 8 : P.mbw * 16;
+    for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x) o[(size_t)(by * 8 + y) * ow + bx * 8 + x] = a[y * 8 + x];
+}
+
+// make_overlap_edge_source (encoder_encode.cpp:13-63): the picture on the coded (whole-MB)
+// raster with the samples beyond the visible crop replaced by the nearest visible sample along an
+// active overlap edge (all edges, or those between two flagged macroblocks). One thread per
+// destination sample of one plane (blockIdx.y).
+__host__ __device__ inline int ovl_border(int visible, int coded) {
+    if (visible < 1 || visible >= coded) return -1;
+    const int rem = visible & 7;
+    const int edge = rem == 7 ? visible + 1 : (rem == 0 ? visible : (rem == 1 ? visible - 1 : -1));
+    return edge > 0 && edge < coded ? edge : -1;
+}
+
+struct EdgeArgs {
+    const uint8_t* in[3];
+    int in_pitch[3], sw[3], sh[3];
+    uint8_t* out[3];
+    int out_pitch[3], dw[3], dh[3], vw[3], vh[3], ex[3], ey[3];
+    const uint8_t* flags;
+    int all, mbw, mbh;
+};
+
+__global__ void edge_source_kernel(const __grid_constant__ EdgeArgs E) {
+    const int pl = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= E.dw[pl] * E.dh[pl]) return;
+    const int x = i % E.dw[pl], y = i / E.dw[pl];
+    const bool luma = pl == 0;
+    const int vw = E.vw[pl], vh = E.vh[pl];
+    int v = (x < E.sw[pl] && y < E.sh[pl]) ? (int)E.in[pl][(size_t)y * E.in_pitch[pl] + x] : (luma ? 0 : 128);
+    if (!(x < vw && y < vh)) {
+        auto active = [&](int ax, int ay, int bx2, int by2) {
+            if (E.all) return true;
+            const int a = (luma ? ay / 2 : ay) * E.mbw + (luma ? ax / 2 : ax);
+            const int b = (luma ? by2 / 2 : by2) * E.mbw + (luma ? bx2 / 2 : bx2);
+            const int n = E.mbw * E.mbh;
+            return a >= 0 && b >= 0 && a < n && b < n && E.flags[a] && E.flags[b];
+        };
+        const int ex = E.ex[pl], ey = E.ey[pl];
+        const bool right = x >= vw && ex >= 0 && active(ex / 8 - 1, y / 8, ex / 8, y / 8);
+        const bool bottom = y >= vh && ey >= 0 && active(x / 8, ey / 8 - 1, x / 8, ey / 8);
+        if (right || bottom) {
+            const int sx = min(max(x, 0), vw - 1), sy = min(max(y, 0), vh - 1);
+            v = E.in[pl][(size_t)sy * E.in_pitch[pl] + sx];
+        }
+    }
+    E.out[pl][(size_t)y * E.out_pitch[pl] + x] = (uint8_t)v;
+}
+
 // The DQUANT search's per-macroblock inputs (choose_dquant_transform_mb, encoder_aq.cpp:318-336):
 // the perceptual lambda scale of the MB's luma against its prediction with its adjacency term,
 // and the bright-detail-on-dark test of the source MB. One thread per MB.
@@ -1403,6 +1611,92 @@ cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const D
     const int mbs = P.mbw * P.mbh;
     if (mbs <= 0) return cudaSuccess;
     dquant_stats_kernel<<<(mbs + 127) / 128, 128, 0, s>>>(a, lscale, adjacency, bright);
+    return cudaGetLastError();
+}
+
+// The signed intra reconstruction of an I picture: the optional overlap edge source (flags: per
+// MB, nullptr with all = 0 for none), the forward transforms and AC levels, the DC chain, the
+// inverse transforms into the int32 planes oy / ou / ov (padded raster, rows packed). scratch
+// holds intra_scratch_bytes(P) bytes; edge: 1.5 * (mbw * 16) * (mbh * 16) bytes for the edge
+// source.
+size_t intra_scratch_bytes(const DevParams& P) {
+    const size_t mbs = (size_t)P.mbw * P.mbh;
+    return mbs * 6 * 64 * 2 + mbs * 6 * 4 * 2 + 256;
+}
+
+cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int overlap, const uint8_t* d_flags,
+                               const uint8_t* d_mquant, const uint8_t* d_derived, void* scratch, uint8_t* edge,
+                               int32_t* oy, int32_t* ou, int32_t* ov, cudaStream_t s) {
+    const int mbs = P.mbw * P.mbh;
+    if (mbs <= 0) return cudaSuccess;
+    IntraArgs A{};
+    A.P = P;
+    A.y = src.y;
+    A.u = src.u;
+    A.v = src.v;
+    A.pitch_y = src.pitch_y;
+    A.pitch_c = src.pitch_c;
+    A.sw = P.W;
+    A.sh = P.H;
+    cudaError_t e;
+    if (overlap) {
+        const int cw = P.mbw * 16, ch = P.mbh * 16, ccw = cw / 2, cch = ch / 2;
+        const int cvw = (P.vw + 1) / 2, cvh = (P.vh + 1) / 2;
+        const int vx = ovl_border(P.vw, cw), vy = ovl_border(P.vh, ch), cx = ovl_border(cvw, ccw), cy = ovl_border(cvh, cch);
+        if (vx >= 0 || vy >= 0 || cx >= 0 || cy >= 0) {
+            EdgeArgs E{};
+            const uint8_t* in[3] = {src.y, src.u, src.v};
+            for (int k = 0; k < 3; ++k) {
+                const bool l = k == 0;
+                E.in[k] = in[k];
+                E.in_pitch[k] = l ? src.pitch_y : src.pitch_c;
+                E.sw[k] = l ? P.W : P.W / 2;
+                E.sh[k] = l ? P.H : P.H / 2;
+                E.dw[k] = l ? cw : ccw;
+                E.dh[k] = l ? ch : cch;
+                E.out_pitch[k] = E.dw[k];
+                E.vw[k] = l ? P.vw : cvw;
+                E.vh[k] = l ? P.vh : cvh;
+                E.ex[k] = l ? vx : cx;
+                E.ey[k] = l ? vy : cy;
+            }
+            E.out[0] = edge;
+            E.out[1] = edge + (size_t)cw * ch;
+            E.out[2] = edge + (size_t)cw * ch + (size_t)ccw * cch;
+            E.flags = d_flags;
+            E.all = overlap == 1;
+            E.mbw = P.mbw;
+            E.mbh = P.mbh;
+            edge_source_kernel<<<dim3((unsigned)((cw * ch + 255) / 256), 3), 256, 0, s>>>(E);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            A.y = E.out[0];
+            A.u = E.out[1];
+            A.v = E.out[2];
+            A.pitch_y = cw;
+            A.pitch_c = ccw;
+            A.sw = cw;
+            A.sh = ch;
+        }
+    }
+    A.mquant = d_mquant;
+    A.derived = d_derived;
+    uint8_t* p = static_cast<uint8_t*>(scratch);
+    A.q = reinterpret_cast<int16_t*>(p);
+    p += (size_t)mbs * 6 * 64 * 2;
+    int* dc = reinterpret_cast<int*>(p);
+    int* qg = dc + (size_t)mbs * 6;
+    A.dc[0] = dc;
+    A.dc[1] = dc + (size_t)mbs * 4;
+    A.dc[2] = dc + (size_t)mbs * 5;
+    A.qg[0] = qg;
+    A.qg[1] = qg + (size_t)mbs * 4;
+    A.qg[2] = qg + (size_t)mbs * 5;
+    const unsigned blocks = (unsigned)((mbs * 6 + 127) / 128);
+    intra_fwd_kernel<<<blocks, 128, 0, s>>>(A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    intra_dc_kernel<<<3, 256, 0, s>>>(A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    intra_inv_kernel<<<blocks, 128, 0, s>>>(A, oy, ou, ov);
     return cudaGetLastError();
 }
 

@@ -352,6 +352,7 @@ class Reference:
         L.ref_p_mode_scores.restype = i32
         L.ref_b_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp, vp, i32, i32, vp, C.POINTER(i32)]
         L.ref_b_mode_scores.restype = i32
+        L.ref_reconstruct_intra.argtypes = [vp, i32, C.c_double, vp, i32, vp, vp, vp, vp, vp, vp]
         L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
@@ -591,6 +592,22 @@ class Reference:
         if rc:
             raise RuntimeError("reference B mode scoring threw")
         return scores, chosen.value
+
+    def reconstruct_intra(self, frame, overlap=0, flags=None, dquant=False, aq_strength=0.0):
+        """reconstruct_i_signed_padded at trellis 0: the signed int32 planes of the padded raster
+        and the DQUANT plan's per-MB MQUANT and derived flags."""
+        mbw, mbh = mbs_of(self.p)
+        pw, ph = mbw * 16, mbh * 16
+        y = np.zeros((ph, pw), np.int32)
+        u = np.zeros((ph // 2, pw // 2), np.int32)
+        v = np.zeros_like(u)
+        mq = np.zeros(mbw * mbh, np.uint8)
+        der = np.zeros(mbw * mbh, np.uint8)
+        fl = None if flags is None else np.ascontiguousarray(flags, np.uint8)
+        self.lib.ref_reconstruct_intra(self.h, int(dquant), aq_strength, self._f(frame), overlap,
+                                       None if fl is None else fl.ctypes.data, y.ctypes.data, u.ctypes.data,
+                                       v.ctypes.data, mq.ctypes.data, der.ctypes.data)
+        return (y, u, v), mq, der
 
     def estimate_p_motion_bits(self, a: Analysis, mode: int, intensity: bool = False) -> int:
         """estimate_p_motion_bits of analysis a made in mode (None when the reference throws)."""

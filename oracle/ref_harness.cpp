@@ -547,6 +547,42 @@ int ref_b_mode_scores(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* past, 
     }
 }
 
+// reconstruct_i_signed_padded (encoder_encode.cpp:814-887) at trellis 0, DQUANT on (with the
+// perceptual scale at aq_strength) or off, with the overlap plan (mode 0 none, 1 all, 2 select
+// with flags) whose edge source it reads; the signed planes of the padded raster go to y, u, v.
+// mquant / derived (when set) receive the DQUANT plan the function forms (choose_intra_mquant,
+// make_dquant_plan, dquant_mb_derived; :826-833).
+void ref_reconstruct_intra(void* h, int dquant, double aq_strength, void* src, int overlap, const uint8_t* flags,
+                           int32_t* y, int32_t* u, int32_t* v, uint8_t* mquant, uint8_t* derived) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.trellis = 0;
+    c.dquant = dquant != 0;
+    c.adaptive_quality = aq_strength > 0.0;
+    c.aq_strength = aq_strength;
+    const Vc1Encoder e(c);
+    const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
+    const size_t mbs = static_cast<size_t>(mbw) * mbh;
+    Vc1Encoder::OverlapPlan plan;
+    plan.mode = overlap == 1 ? Vc1Encoder::OverlapMode::All : (overlap == 2 ? Vc1Encoder::OverlapMode::Select : Vc1Encoder::OverlapMode::None);
+    plan.flags.assign(mbs, overlap == 1 ? 1 : 0);
+    if (overlap == 2) plan.flags.assign(flags, flags + mbs);
+    const auto sf = e.reconstruct_i_signed_padded(F(src), &plan);
+    std::copy(sf.y.begin(), sf.y.end(), y);
+    std::copy(sf.u.begin(), sf.u.end(), u);
+    std::copy(sf.v.begin(), sf.v.end(), v);
+    if (mquant || derived) {
+        std::vector<int> desired(mbs, c.pqindex);
+        if (c.dquant)
+            for (int my = 0; my < mbh; ++my)
+                for (int mx = 0; mx < mbw; ++mx) desired[static_cast<size_t>(my) * mbw + mx] = e.choose_intra_mquant(F(src), mx, my);
+        const auto dplan = e.make_dquant_plan(desired, mbw, mbh);
+        for (size_t i = 0; i < mbs; ++i) {
+            if (mquant) mquant[i] = static_cast<uint8_t>(dplan.mquant.empty() ? c.pqindex : dplan.mquant[i]);
+            if (derived) derived[i] = Vc1Encoder::dquant_mb_derived(dplan, i, mbw) ? 1 : 0;
+        }
+    }
+}
+
 // estimate_p_motion_bits of an analysis given as host arrays (mbw*mbh vectors, 4 block vectors
 // per MB, the 4-MV and intra flags) made in `mode`; UINT64_MAX when the reference throws.
 uint64_t ref_estimate_p_motion_bits(void* h, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs, const uint8_t* use_4mv,
