@@ -759,6 +759,20 @@ int vc1cu_reconstruct_intra(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, i
                             const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v);
 
 /*
+ * The I picture's overlap plan, Vc1Encoder::choose_i_overlap_plan (src/encoder_filter.cpp:277-343),
+ * for an Advanced Profile picture whose sequence sets OVERLAP: at PQINDEX >= 9 every edge (ALL);
+ * below, the intra reconstruction of frame slot src_id without smoothing and with every edge
+ * smoothed (as vc1cu_reconstruct_intra and vc1cu_overlap_smooth), each macroblock flagged when
+ * smoothing lowers its reconstruction error (overlap_sse_region, :246-266) by more than
+ * 4 * PQINDEX^2, then NONE, ALL or SELECT by total error plus 8 * PQINDEX^2 per bit of syntax
+ * (SELECT: its flags as the cheapest OVERFLAGS bitplane). mquant / derived: the picture's DQUANT
+ * plan as for vc1cu_reconstruct_intra (NULL: PQINDEX). *mode (0 none, 1 all, 2 select) and flags
+ * (HOST mbw*mbh) take the plan as the reference returns it. Synchronous.
+ */
+int vc1cu_choose_i_overlap(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, const uint8_t* mquant,
+                           const uint8_t* derived, int* mode, uint8_t* flags);
+
+/*
  * Overlap smoothing of a signed (unclamped, unbiased) reconstruction in place:
  * apply_overlap_plane_signed (src/encoder_filter.cpp:217-243) on each plane, as
  * Vc1Encoder::apply_i_overlap (:344-352) and apply_p_overlap (:354-365) call it. d_y, d_u, d_v

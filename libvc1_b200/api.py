@@ -46,7 +46,7 @@ EXPORTS = (
     "vc1cu_lp_propose", "vc1cu_lp_read_sample", "vc1cu_lp_analyze", "vc1cu_core_passes_multi",
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
     "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd", "vc1cu_loop_filter_p_main",
-    "vc1cu_choose_dquant", "vc1cu_reconstruct_intra",
+    "vc1cu_choose_dquant", "vc1cu_reconstruct_intra", "vc1cu_choose_i_overlap",
 )
 
 
@@ -124,6 +124,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_choose_dquant.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, i32, i32, vp, vp, vp, vp]
     L.vc1cu_reconstruct_intra.argtypes = [vp, PP, i32, i32, vp, vp, vp, vp, vp, vp]
+    L.vc1cu_choose_i_overlap.argtypes = [vp, PP, i32, vp, vp, C.POINTER(i32), vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
     L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
     L.vc1cu_b_mode_rd.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
@@ -549,6 +550,18 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_reconstruct_intra(self._h, C.byref(params), src_id, overlap,
                                                     *[None if a is None else a.ctypes.data for a in arrs], d_y, d_u,
                                                     d_v))
+
+    def choose_i_overlap(self, params: Params, src_id: int, mquant=None, derived=None):
+        """The I picture's overlap plan (vc1cu_choose_i_overlap): (mode 0 none / 1 all / 2 select,
+        per-MB flags)."""
+        mbw, mbh = mbs_of(params)
+        flags = np.zeros(mbw * mbh, np.uint8)
+        mode = C.c_int32()
+        arrs = [None if a is None else np.ascontiguousarray(a, np.uint8) for a in (mquant, derived)]
+        self._check(self._L.vc1cu_choose_i_overlap(self._h, C.byref(params), src_id,
+                                                   *[None if a is None else a.ctypes.data for a in arrs],
+                                                   C.byref(mode), flags.ctypes.data))
+        return mode.value, flags
 
     def overlap_smooth(self, params: Params, d_y: int, d_u: int, d_v: int, flags=None, all_edges: bool = False):
         """In-place overlap smoothing of DEVICE int32 signed planes (padded raster, rows packed):

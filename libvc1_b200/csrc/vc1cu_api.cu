@@ -64,6 +64,10 @@ cudaError_t launch_trd(const DevParams& P, const DevFrame& src, const DevFrame& 
 cudaError_t trd_frame_mean(const DevParams& P, const DevFrame& src, const vc1cu_trd_cfg& cfg, unsigned long long* d_sum,
                            cudaStream_t s, double* mean);
 size_t intra_scratch_bytes(const DevParams& P);
+cudaError_t launch_overlap_sse(const int32_t* sy, const int32_t* su, const int32_t* sv, const uint8_t* oy,
+                               const uint8_t* ou, const uint8_t* ov, int pitch_y, int pitch_c, int W, int H, int bias,
+                               unsigned long long* sse, cudaStream_t s);
+cudaError_t launch_bitplane_bits(const uint8_t* plane, int w, int h, unsigned long long* out, cudaStream_t s);
 cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int overlap, const uint8_t* d_flags,
                                const uint8_t* d_mquant, const uint8_t* d_derived, void* scratch, uint8_t* edge,
                                int32_t* oy, int32_t* ou, int32_t* ov, cudaStream_t s);
@@ -305,6 +309,8 @@ struct vc1cu_ctx {
     size_t dq_cap = 0;
     void* d_intra = nullptr;    // the intra reconstruction's levels, DC grids, maps and edge source
     size_t intra_cap = 0;
+    void* d_iovl = nullptr;     // the I overlap plan's three signed reconstructions and error sums
+    size_t iovl_cap = 0;
     void* d_ic = nullptr;      // intensity-estimate scratch (one block per picture) and descriptors
     size_t ic_cap = 0;
     void* d_icdesc = nullptr;
@@ -1885,6 +1891,7 @@ int vc1cu_close(vc1cu_ctx* c) {
     if (c->d_mrd) cudaFree(c->d_mrd);
     if (c->d_dq) cudaFree(c->d_dq);
     if (c->d_intra) cudaFree(c->d_intra);
+    if (c->d_iovl) cudaFree(c->d_iovl);
     if (c->d_lf) cudaFree(c->d_lf);
     if (c->d_ovl) cudaFree(c->d_ovl);
     if (c->d_gcopy) cudaFree(c->d_gcopy);
@@ -3306,6 +3313,35 @@ int vc1cu_loop_filter_p_main(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, 
     return loop_filter_p(c, p, frame_id, block_mvs, cbp, tt, intra, 1);
 }
 
+// The signed intra reconstruction of frame slot src_id (HOST flags / mquant / derived, copied on the
+// context stream) into the device planes d_y, d_u, d_v.
+static void intra_recon(vc1cu_ctx* c, const DevParams& P, FrameSlot& fs, int overlap, const uint8_t* flags,
+                        const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v) {
+    const size_t mbs = (size_t)P.mbw * P.mbh;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t b_scr = al(intra_scratch_bytes(P)), b_edge = al(mbs * 256 * 3 / 2), b_map = al(mbs);
+    uint8_t* base = static_cast<uint8_t*>(
+        ensure(c->d_intra, c->intra_cap, b_scr + b_edge + 3 * b_map, "cudaMalloc(intra reconstruction)"));
+    uint8_t* d_flags = base + b_scr + b_edge;
+    uint8_t* d_mq = d_flags + b_map;
+    uint8_t* d_der = d_mq + b_map;
+    if (overlap == 2) ck(cudaMemcpyAsync(d_flags, flags, mbs, cudaMemcpyHostToDevice, c->stream), "upload overlap flags");
+    if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "upload MQUANT");
+    if (derived) ck(cudaMemcpyAsync(d_der, derived, mbs, cudaMemcpyHostToDevice, c->stream), "upload derived flags");
+    Timer tm(c, kXform);
+    ck(launch_intra_recon(P, fs.view(), overlap, overlap == 2 ? d_flags : nullptr, mquant ? d_mq : nullptr,
+                          derived ? d_der : nullptr, base, base + b_scr, d_y, d_u, d_v, c->stream),
+       "intra reconstruction launch");
+    tm.stop(overlap ? 4 : 3);
+}
+
+static void check_intra_args(const DevParams& P, FrameSlot& fs, const uint8_t* mquant) {
+    if (fs.w != P.W || fs.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
+    if (mquant)
+        for (size_t i = 0; i < (size_t)P.mbw * P.mbh; ++i)
+            if (mquant[i] < 1 || mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 1..31"};
+}
+
 int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int overlap, const uint8_t* flags,
                             const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v) {
     return guarded(c, [&]() -> int {
@@ -3317,27 +3353,100 @@ int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int
         const int rc = make_dev_params(p, P, why);
         if (rc) throw Fail{rc, why};
         FrameSlot& fs = frame_slot(c, src_id);
-        if (fs.w != P.W || fs.h != P.H) throw Fail{VC1CU_ERR_ARG, "frame size does not match the configuration"};
-        const size_t mbs = (size_t)P.mbw * P.mbh;
-        if (mquant)
-            for (size_t i = 0; i < mbs; ++i)
-                if (mquant[i] < 1 || mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 1..31"};
-        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-        const size_t b_scr = al(intra_scratch_bytes(P)), b_edge = al(mbs * 256 * 3 / 2), b_map = al(mbs);
-        uint8_t* base = static_cast<uint8_t*>(
-            ensure(c->d_intra, c->intra_cap, b_scr + b_edge + 3 * b_map, "cudaMalloc(intra reconstruction)"));
-        uint8_t* d_flags = base + b_scr + b_edge;
-        uint8_t* d_mq = d_flags + b_map;
-        uint8_t* d_der = d_mq + b_map;
-        if (overlap == 2) ck(cudaMemcpyAsync(d_flags, flags, mbs, cudaMemcpyHostToDevice, c->stream), "upload overlap flags");
-        if (mquant) ck(cudaMemcpyAsync(d_mq, mquant, mbs, cudaMemcpyHostToDevice, c->stream), "upload MQUANT");
-        if (derived) ck(cudaMemcpyAsync(d_der, derived, mbs, cudaMemcpyHostToDevice, c->stream), "upload derived flags");
-        Timer tm(c, kXform);
-        ck(launch_intra_recon(P, fs.view(), overlap, overlap == 2 ? d_flags : nullptr, mquant ? d_mq : nullptr,
-                              derived ? d_der : nullptr, base, base + b_scr, d_y, d_u, d_v, c->stream),
-           "intra reconstruction launch");
-        tm.stop(overlap ? 4 : 3);
+        check_intra_args(P, fs, mquant);
+        intra_recon(c, P, fs, overlap, flags, mquant, derived, d_y, d_u, d_v);
         ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");  // the copies read the caller's arrays
+        return VC1CU_OK;
+    });
+}
+
+int vc1cu_choose_i_overlap(vc1cu_ctx* c, const vc1cu_params* p, int src_id, const uint8_t* mquant, const uint8_t* derived,
+                           int* mode, uint8_t* flags) {
+    return guarded(c, [&]() -> int {
+        if (!mode || !flags) throw Fail{VC1CU_ERR_ARG, "null output"};
+        DevParams P;
+        std::string why;
+        const int rc = make_dev_params(p, P, why);
+        if (rc) throw Fail{rc, why};
+        FrameSlot& fs = frame_slot(c, src_id);
+        check_intra_args(P, fs, mquant);
+        const size_t mbs = (size_t)P.mbw * P.mbh;
+        std::fill(flags, flags + mbs, (uint8_t)0);
+        if (P.pq >= 9) {  // unconditional overlap above the CONDOVER range (:290-294)
+            *mode = 1;
+            return VC1CU_OK;
+        }
+        // three signed reconstructions (no smoothing, every edge, the selected edges), their
+        // per-MB errors, the flags and the OVERFLAGS bitplane's bits
+        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t ny = mbs * 256, nc = mbs * 64, b_rec = al(4 * (ny + 2 * nc)), b_sse = al(8 * mbs);
+        uint8_t* base = static_cast<uint8_t*>(
+            ensure(c->d_iovl, c->iovl_cap, 3 * b_rec + 3 * b_sse + al(mbs) + 256, "cudaMalloc(overlap plan)"));
+        auto rec = [&](int k, int pl) {
+            int32_t* r = reinterpret_cast<int32_t*>(base + (size_t)k * b_rec);
+            return pl == 0 ? r : (pl == 1 ? r + ny : r + ny + nc);
+        };
+        auto* sse = reinterpret_cast<unsigned long long*>(base + 3 * b_rec);
+        uint8_t* d_flags = base + 3 * b_rec + 3 * b_sse;
+        auto* d_bits = reinterpret_cast<unsigned long long*>(d_flags + al(mbs));
+        const DevFrame src = fs.view();
+        auto errors = [&](int k) {
+            ck(launch_overlap_sse(rec(k, 0), rec(k, 1), rec(k, 2), src.y, src.u, src.v, src.pitch_y, src.pitch_c, P.W, P.H,
+                                  128, sse + (size_t)k * mbs, c->stream),
+               "overlap error launch");
+        };
+        intra_recon(c, P, fs, 0, nullptr, mquant, derived, rec(0, 0), rec(0, 1), rec(0, 2));
+        ck(cudaMemcpyAsync(rec(1, 0), rec(0, 0), 4 * (ny + 2 * nc), cudaMemcpyDeviceToDevice, c->stream), "copy reconstruction");
+        ck(launch_overlap(rec(1, 0), rec(1, 1), rec(1, 2), P.mbw, P.mbh, nullptr, 1, c->stream), "overlap launch");
+        errors(0);
+        errors(1);
+        std::vector<unsigned long long> e((size_t)2 * mbs);
+        ck(cudaMemcpyAsync(e.data(), sse, 16 * mbs, cudaMemcpyDeviceToHost, c->stream), "read errors");
+        sync_checked(c);
+        const long double pq2 = static_cast<long double>(P.pq * P.pq);
+        bool any = false, every = true;
+        for (size_t i = 0; i < mbs; ++i) {
+            const bool on = static_cast<long double>(e[mbs + i]) + pq2 * 4.0L < static_cast<long double>(e[i]);
+            flags[i] = on ? 1 : 0;
+            any |= on;
+            every &= on;
+        }
+        if (!any) {
+            *mode = 0;
+            return VC1CU_OK;
+        }
+        if (every) {
+            *mode = 1;
+            return VC1CU_OK;
+        }
+        ck(cudaMemcpyAsync(d_flags, flags, mbs, cudaMemcpyHostToDevice, c->stream), "upload flags");
+        ck(launch_bitplane_bits(d_flags, P.mbw, P.mbh, d_bits, c->stream), "bitplane launch");
+        ck(cudaMemcpyAsync(rec(2, 0), rec(0, 0), 4 * (ny + 2 * nc), cudaMemcpyDeviceToDevice, c->stream), "copy reconstruction");
+        ck(launch_overlap(rec(2, 0), rec(2, 1), rec(2, 2), P.mbw, P.mbh, d_flags, 0, c->stream), "overlap launch");
+        errors(2);
+        std::vector<unsigned long long> e2(mbs);
+        unsigned long long bits = 0;
+        ck(cudaMemcpyAsync(e2.data(), sse + 2 * mbs, 8 * mbs, cudaMemcpyDeviceToHost, c->stream), "read errors");
+        ck(cudaMemcpyAsync(&bits, d_bits, 8, cudaMemcpyDeviceToHost, c->stream), "read bitplane bits");
+        sync_checked(c);
+        long double t0 = 0.0L, t1 = 0.0L, t2 = 0.0L;
+        for (size_t i = 0; i < mbs; ++i) {
+            t0 += static_cast<long double>(e[i]);
+            t1 += static_cast<long double>(e[mbs + i]);
+            t2 += static_cast<long double>(e2[i]);
+        }
+        const long double lambda = pq2 * 8.0L;
+        const long double nscore = t0 + lambda, ascore = t1 + 2.0L * lambda;
+        const long double sscore = t2 + lambda * (2.0L + static_cast<long double>(bits));
+        if (nscore <= ascore && nscore <= sscore) {
+            *mode = 0;
+            std::fill(flags, flags + mbs, (uint8_t)0);
+        } else if (ascore <= sscore) {
+            *mode = 1;
+            std::fill(flags, flags + mbs, (uint8_t)1);
+        } else {
+            *mode = 2;
+        }
         return VC1CU_OK;
     });
 }

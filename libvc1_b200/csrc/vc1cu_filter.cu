@@ -356,6 +356,43 @@ cudaError_t launch_overlap(int32_t* y, int32_t* u, int32_t* v, int mbw, int mbh,
     return cudaGetLastError();
 }
 
+// overlap_sse_region (encoder_filter.cpp:246-266) of every MB: the squared error of clamp(s + bias)
+// of the padded signed planes against the source (coordinates clamped into it) over the MB's
+// 16x16 luma and 8x8 chroma blocks. Integer sums, exact like the reference's long double ones.
+// One thread per MB.
+__global__ void overlap_sse_kernel(const int32_t* sy, const int32_t* su, const int32_t* sv, const uint8_t* oy,
+                                   const uint8_t* ou, const uint8_t* ov, int pitch_y, int pitch_c, int W, int H, int mbw,
+                                   int mbh, int bias, unsigned long long* sse) {
+    const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mb >= mbw * mbh) return;
+    const int mx = mb % mbw, my = mb / mbw;
+    unsigned long long e = 0;
+    auto plane = [&](const int32_t* rec, int rw, const uint8_t* org, int pitch, int ow, int oh, int x0, int y0, int n) {
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const int rx = x0 + x, ry = y0 + y;
+                const int sx = imin(imax(rx, 0), ow - 1), sy = imin(imax(ry, 0), oh - 1);
+                const int r = imin(255, imax(0, rec[(size_t)ry * rw + rx] + bias));
+                const int d = r - (int)org[(size_t)sy * pitch + sx];
+                e += (unsigned long long)(d * d);
+            }
+    };
+    plane(sy, mbw * 16, oy, pitch_y, W, H, mx * 16, my * 16, 16);
+    plane(su, mbw * 8, ou, pitch_c, W / 2, H / 2, mx * 8, my * 8, 8);
+    plane(sv, mbw * 8, ov, pitch_c, W / 2, H / 2, mx * 8, my * 8, 8);
+    sse[mb] = e;
+}
+
+cudaError_t launch_overlap_sse(const int32_t* sy, const int32_t* su, const int32_t* sv, const uint8_t* oy,
+                               const uint8_t* ou, const uint8_t* ov, int pitch_y, int pitch_c, int W, int H, int bias,
+                               unsigned long long* sse, cudaStream_t s) {
+    const int mbw = (W + 15) / 16, mbh = (H + 15) / 16;
+    if (mbw * mbh <= 0) return cudaSuccess;
+    overlap_sse_kernel<<<(mbw * mbh + 127) / 128, 128, 0, s>>>(sy, su, sv, oy, ou, ov, pitch_y, pitch_c, W, H, mbw, mbh, bias,
+                                                               sse);
+    return cudaGetLastError();
+}
+
 // clamp(s + bias) of the padded signed planes into a frame (its visible w x h), all macroblocks
 // or the flagged ones; thread = 4 samples of a row.
 struct StoreArgs {

@@ -190,4 +190,10 @@ cudaError_t launch_p_motion_bits(const DevParams& P, const DevResult& r, int mod
     return e;
 }
 
+// choose_bitplane's least total bits of a w x h plane into *out (device).
+cudaError_t launch_bitplane_bits(const uint8_t* plane, int w, int h, unsigned long long* out, cudaStream_t s) {
+    bitplane_bits_kernel<<<1, 512, 0, s>>>(plane, w, h, out);
+    return cudaGetLastError();
+}
+
 }  // namespace vc1cu

@@ -353,6 +353,7 @@ class Reference:
         L.ref_b_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp, vp, i32, i32, vp, C.POINTER(i32)]
         L.ref_b_mode_scores.restype = i32
         L.ref_reconstruct_intra.argtypes = [vp, i32, C.c_double, vp, i32, vp, vp, vp, vp, vp, vp]
+        L.ref_choose_i_overlap.argtypes = [vp, i32, C.c_double, vp, C.POINTER(i32), vp]
         L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
@@ -608,6 +609,14 @@ class Reference:
                                        None if fl is None else fl.ctypes.data, y.ctypes.data, u.ctypes.data,
                                        v.ctypes.data, mq.ctypes.data, der.ctypes.data)
         return (y, u, v), mq, der
+
+    def choose_i_overlap(self, frame, dquant=False, aq_strength=0.0):
+        """choose_i_overlap_plan with OVERLAP on: (mode 0 none / 1 all / 2 select, per-MB flags)."""
+        mbw, mbh = mbs_of(self.p)
+        flags = np.zeros(mbw * mbh, np.uint8)
+        mode = i32()
+        self.lib.ref_choose_i_overlap(self.h, int(dquant), aq_strength, self._f(frame), C.byref(mode), flags.ctypes.data)
+        return mode.value, flags
 
     def estimate_p_motion_bits(self, a: Analysis, mode: int, intensity: bool = False) -> int:
         """estimate_p_motion_bits of analysis a made in mode (None when the reference throws)."""

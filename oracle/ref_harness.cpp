@@ -583,6 +583,21 @@ void ref_reconstruct_intra(void* h, int dquant, double aq_strength, void* src, i
     }
 }
 
+// choose_i_overlap_plan (encoder_filter.cpp:277-343) with OVERLAP on, trellis 0, DQUANT on (with
+// the perceptual scale at aq_strength) or off: the plan's mode (0 none, 1 all, 2 select) and flags.
+void ref_choose_i_overlap(void* h, int dquant, double aq_strength, void* src, int* mode, uint8_t* flags) {
+    EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
+    c.trellis = 0;
+    c.overlap = true;
+    c.dquant = dquant != 0;
+    c.adaptive_quality = aq_strength > 0.0;
+    c.aq_strength = aq_strength;
+    const Vc1Encoder e(c);
+    const auto plan = e.choose_i_overlap_plan(F(src));
+    *mode = static_cast<int>(plan.mode);
+    std::copy(plan.flags.begin(), plan.flags.end(), flags);
+}
+
 // estimate_p_motion_bits of an analysis given as host arrays (mbw*mbh vectors, 4 block vectors
 // per MB, the 4-MV and intra flags) made in `mode`; UINT64_MAX when the reference throws.
 uint64_t ref_estimate_p_motion_bits(void* h, const vc1cu_mv* mvs, const vc1cu_mv* block_mvs, const uint8_t* use_4mv,

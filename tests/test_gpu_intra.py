@@ -2,7 +2,10 @@
 reference's own Vc1Encoder::reconstruct_i_signed_padded (oracle/_ref, scalar path, trellis 0),
 bit for bit on the padded raster: full and cropped rasters, the uniform, non-uniform and half-step
 quantisers, PQINDEX 1-2 (the wider DC range), overlap plans none / all / select (the edge source
-the transform reads) and a DQUANT plan whose per-MB MQUANT scales the DC predictors."""
+the transform reads) and a DQUANT plan whose per-MB MQUANT scales the DC predictors; and the I
+overlap plan (vc1cu_choose_i_overlap) against choose_i_overlap_plan: every macroblock gaining
+(ALL), mixed gains scored against the OVERFLAGS bits, none gaining, PQINDEX above the CONDOVER
+range, a cropped raster and a DQUANT plan."""
 import numpy as np
 import pytest
 
@@ -48,3 +51,43 @@ def test_intra_reconstruction_matches_reference(ctx, case):
     for got, exp, c in zip(d, want, "yuv"):
         g = got.cpu().numpy()
         assert np.array_equal(g, exp), (c, np.argwhere(g != exp)[:4])
+
+
+def _overlap_content(kind, w, h):
+    yy, xx = np.mgrid[0:h, 0:w]
+    g = 40 + 0.8 * xx * 176 / w + 0.5 * yy * 144 / h
+    if kind == "gradient":
+        y = g
+    else:  # a textured quadrant in the gradient: some macroblocks gain from smoothing, some lose
+        t = 128 + 60 * np.sin(xx / 2.3) * np.cos(yy / 1.9) + np.random.default_rng(3).normal(0, 10, (h, w))
+        y = np.where((xx < w // 2) & (yy < h // 2), t, g)
+    y = np.clip(np.rint(y), 0, 255).astype(np.uint8)
+    u = np.full((h // 2, w // 2), 128, np.uint8)
+    return y, u, u.copy()
+
+
+OVERLAP_PLANS = {
+    # (w, h, display, pq, content, dquant): the plan the reference takes
+    "gradient_all": (176, 144, None, 3, "gradient", False),
+    "mixed_scored_none": (176, 144, None, 3, "mixed", False),
+    "texture_none": (176, 144, None, 5, "synth", False),
+    "above_condover_all": (176, 144, None, 10, "synth", False),
+    "cropped_gradient": (322, 242, (317, 237), 3, "gradient", False),
+    "dquant_plan": (176, 144, None, 4, "mixed", True),
+}
+
+
+@pytest.mark.parametrize("case", sorted(OVERLAP_PLANS))
+def test_i_overlap_plan_matches_reference(ctx, case):
+    """vc1cu_choose_i_overlap against the reference's choose_i_overlap_plan: the mode and flags."""
+    w, h, disp, pq, content, dquant = OVERLAP_PLANS[case]
+    kw = dict(display_width=disp[0], display_height=disp[1]) if disp else {}
+    p = make_params(w, h, pqindex=pq, **kw)
+    frame = synth.generate(w, h, 1, 7).frame(0) if content == "synth" else _overlap_content(content, w, h)
+    R = Reference(p)
+    want_mode, want_flags = R.choose_i_overlap(frame, dquant=dquant, aq_strength=1.0 if dquant else 0.0)
+    _, mq, der = R.reconstruct_intra(frame, 0, None, dquant=dquant, aq_strength=1.0 if dquant else 0.0)
+    ctx.upload_frame(0, *frame)
+    mode, flags = ctx.choose_i_overlap(p, 0, mquant=mq if dquant else None, derived=der if dquant else None)
+    assert mode == want_mode
+    assert np.array_equal(flags, want_flags)
