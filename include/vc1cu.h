@@ -743,9 +743,12 @@ int vc1cu_loop_filter_p_main(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id
 
 /*
  * The signed intra reconstruction of an I picture, Vc1Encoder::reconstruct_i_signed_padded
- * (src/encoder_encode.cpp:814-887) with scalar AC quantisation (trellis 0) and AC coding: for every
- * 8x8 block of frame slot src_id the intra forward transform (forward_transform, samples outside
- * the source read 0 luma / 128 chroma), the AC levels at the MB's MQUANT, the DC level whose
+ * (src/encoder_encode.cpp:814-887) with AC coding: for every 8x8 block of frame slot src_id the
+ * intra forward transform (forward_transform, samples outside the source read 0 luma / 128
+ * chroma), the AC levels at the MB's MQUANT (quantize_ac, src/encoder_transform.cpp:2090-2144:
+ * scalar, or with cfg->trellis 1 / 2 the trellis along the intra scan with the intra-family rates
+ * and, with cfg->adaptive_quality, the perceptual lambda scale of the block; cfg's other fields
+ * are not read, NULL: scalar), the DC level whose
  * reconstruction is nearest the padded block mean, predicted from its neighbours and clamped to
  * the DC range (predict_dc_dquant with the DQUANT scaling, clamp_dc_target_for_diff), the
  * dequantised coefficients and the 8x8 inverse transform, into the DEVICE int32 planes d_y, d_u,
@@ -755,8 +758,9 @@ int vc1cu_loop_filter_p_main(vc1cu_ctx* ctx, const vc1cu_params* p, int frame_id
  * MQUANT (1..31) and DQUANT-derived flags of the picture's DQUANT plan, or NULL for PQINDEX and
  * none. Returns once its inputs are copied.
  */
-int vc1cu_reconstruct_intra(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, int overlap, const uint8_t* flags,
-                            const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v);
+int vc1cu_reconstruct_intra(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id, int overlap,
+                            const uint8_t* flags, const uint8_t* mquant, const uint8_t* derived, int32_t* d_y,
+                            int32_t* d_u, int32_t* d_v);
 
 /*
  * The I picture's overlap plan, Vc1Encoder::choose_i_overlap_plan (src/encoder_filter.cpp:277-343),
@@ -765,12 +769,13 @@ int vc1cu_reconstruct_intra(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, i
  * smoothed (as vc1cu_reconstruct_intra and vc1cu_overlap_smooth), each macroblock flagged when
  * smoothing lowers its reconstruction error (overlap_sse_region, :246-266) by more than
  * 4 * PQINDEX^2, then NONE, ALL or SELECT by total error plus 8 * PQINDEX^2 per bit of syntax
- * (SELECT: its flags as the cheapest OVERFLAGS bitplane). mquant / derived: the picture's DQUANT
- * plan as for vc1cu_reconstruct_intra (NULL: PQINDEX). *mode (0 none, 1 all, 2 select) and flags
+ * (SELECT: its flags as the cheapest OVERFLAGS bitplane). cfg, mquant / derived: the AC
+ * quantisation settings and the picture's DQUANT plan as for vc1cu_reconstruct_intra (NULL:
+ * scalar levels, PQINDEX). *mode (0 none, 1 all, 2 select) and flags
  * (HOST mbw*mbh) take the plan as the reference returns it. Synchronous.
  */
-int vc1cu_choose_i_overlap(vc1cu_ctx* ctx, const vc1cu_params* p, int src_id, const uint8_t* mquant,
-                           const uint8_t* derived, int* mode, uint8_t* flags);
+int vc1cu_choose_i_overlap(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id,
+                           const uint8_t* mquant, const uint8_t* derived, int* mode, uint8_t* flags);
 
 /*
  * Overlap smoothing of a signed (unclamped, unbiased) reconstruction in place:

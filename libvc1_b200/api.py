@@ -123,8 +123,8 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_choose_dquant.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, i32, i32, vp, vp, vp, vp]
-    L.vc1cu_reconstruct_intra.argtypes = [vp, PP, i32, i32, vp, vp, vp, vp, vp, vp]
-    L.vc1cu_choose_i_overlap.argtypes = [vp, PP, i32, vp, vp, C.POINTER(i32), vp]
+    L.vc1cu_reconstruct_intra.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp, vp, vp, vp]
+    L.vc1cu_choose_i_overlap.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, vp, vp, C.POINTER(i32), vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
     L.vc1cu_analyze_p_picture.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, C.POINTER(PpicInfo)]
     L.vc1cu_b_mode_rd.argtypes = [vp, PP, C.POINTER(PpicCfg), i32, i32, i32, i32, i32, i32, C.POINTER(i32),
@@ -542,23 +542,26 @@ class CudaComputeContext:
         self._check(fn(self._h, C.byref(params), frame_id, b.ctypes.data, cb.ctypes.data, t.ctypes.data, i.ctypes.data))
 
     def reconstruct_intra(self, params: Params, src_id: int, d_y: int, d_u: int, d_v: int, overlap: int = 0,
-                          flags=None, mquant=None, derived=None):
+                          flags=None, mquant=None, derived=None, cfg: TrdCfg = None):
         """The signed intra reconstruction of I picture src_id into DEVICE int32 planes of the padded
         raster (vc1cu_reconstruct_intra): overlap 0 none / 1 all / 2 select with per-MB flags; the
-        DQUANT plan's per-MB MQUANT and derived flags, or None for PQINDEX."""
+        DQUANT plan's per-MB MQUANT and derived flags, or None for PQINDEX; cfg's trellis,
+        adaptive_quality, aq_strength and hrd_enabled (None: scalar levels)."""
         arrs = [None if a is None else np.ascontiguousarray(a, np.uint8) for a in (flags, mquant, derived)]
-        self._check(self._L.vc1cu_reconstruct_intra(self._h, C.byref(params), src_id, overlap,
+        self._check(self._L.vc1cu_reconstruct_intra(self._h, C.byref(params), None if cfg is None else C.byref(cfg),
+                                                    src_id, overlap,
                                                     *[None if a is None else a.ctypes.data for a in arrs], d_y, d_u,
                                                     d_v))
 
-    def choose_i_overlap(self, params: Params, src_id: int, mquant=None, derived=None):
+    def choose_i_overlap(self, params: Params, src_id: int, mquant=None, derived=None, cfg: TrdCfg = None):
         """The I picture's overlap plan (vc1cu_choose_i_overlap): (mode 0 none / 1 all / 2 select,
-        per-MB flags)."""
+        per-MB flags); cfg as for reconstruct_intra."""
         mbw, mbh = mbs_of(params)
         flags = np.zeros(mbw * mbh, np.uint8)
         mode = C.c_int32()
         arrs = [None if a is None else np.ascontiguousarray(a, np.uint8) for a in (mquant, derived)]
-        self._check(self._L.vc1cu_choose_i_overlap(self._h, C.byref(params), src_id,
+        self._check(self._L.vc1cu_choose_i_overlap(self._h, C.byref(params), None if cfg is None else C.byref(cfg),
+                                                   src_id,
                                                    *[None if a is None else a.ctypes.data for a in arrs],
                                                    C.byref(mode), flags.ctypes.data))
         return mode.value, flags

@@ -2,7 +2,7 @@
 
 The lengths are bitstream-format data (SMPTE ST 421: the eight progressive AC run/level VLC
 tables and their escape codes, the P-picture CBPCY table, TTMB / TTBLK / SUBBLKPAT, the
-progressive inter scans, the four MVDATA tables and the bitplane IMODE / NORM-2 / NORM-6 codes). They are read from the reference tree, whose tables state them, and
+progressive inter and intra scans, the four MVDATA tables and the bitplane IMODE / NORM-2 / NORM-6 codes). They are read from the reference tree, whose tables state them, and
 only the lengths (never the code words) are kept. Run it where the reference tree is present:
 
     python libvc1_b200/csrc/gen_entropy_lengths.py [reference tree]    (default $LIBVC1_REFERENCE
@@ -47,8 +47,8 @@ def main():
     out = ["// vc1cu_entropy_lengths.h - VC-1 code lengths of the transform RD's bit estimates.",
            "// Generated by gen_entropy_lengths.py (do not edit): bitstream-format data of SMPTE ST 421",
            "// (AC run/level tables and escapes of the eight progressive coding sets, P CBPCY, TTMB,",
-           "// TTBLK, SUBBLKPAT, the progressive inter scans, MVDATA, IMODE, NORM-2, NORM-6); lengths only,",
-           "// no code words.",
+           "// TTBLK, SUBBLKPAT, the progressive inter and intra scans, MVDATA, IMODE, NORM-2, NORM-6); lengths",
+           "// only, no code words.",
            "// The small tables' storage is VC1CU_ENT_TABLE (constexpr unless the includer puts them in",
            "// device constant memory); the AC entries are host data (dense tables are built from them).",
            "#pragma once", "", "#include <cstdint>", "", "#ifndef VC1CU_ENT_TABLE", "#define VC1CU_ENT_TABLE constexpr",
@@ -80,7 +80,8 @@ def main():
         assert len(v) == 3 * n, name
         out.append(f"VC1CU_ENT_TABLE uint8_t {name}[3][{n}] = {{" +
                    ", ".join("{" + ", ".join(map(str, v[r * n:(r + 1) * n])) + "}" for r in range(3)) + "};")
-    for name, n in (("kInterScan", 64), ("kInterScan8x4", 32), ("kInterScan4x8", 32), ("kInterScan4x4", 16)):
+    for name, n in (("kInterScan", 64), ("kInterScan8x4", 32), ("kInterScan4x8", 32), ("kInterScan4x4", 16),
+                    ("kIntraScan", 64)):
         v = _ints(_block(inh, name))
         assert len(v) == n, name
         out.append(f"VC1CU_ENT_TABLE uint8_t {name}[{n}] = {{" + ", ".join(map(str, v)) + "};")

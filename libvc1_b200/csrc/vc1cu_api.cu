@@ -70,7 +70,8 @@ cudaError_t launch_overlap_sse(const int32_t* sy, const int32_t* su, const int32
 cudaError_t launch_bitplane_bits(const uint8_t* plane, int w, int h, unsigned long long* out, cudaStream_t s);
 cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int overlap, const uint8_t* d_flags,
                                const uint8_t* d_mquant, const uint8_t* d_derived, void* scratch, uint8_t* edge,
-                               int32_t* oy, int32_t* ou, int32_t* ov, cudaStream_t s);
+                               int32_t* oy, int32_t* ou, int32_t* ov, const void* tables, const vc1cu_trd_cfg& cfg,
+                               cudaStream_t s);
 cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const DevFrame& pred, const vc1cu_trd_cfg& cfg,
                                 double frame_mean, double* lscale, double* adjacency, uint8_t* bright, cudaStream_t s);
 cudaError_t launch_bpictures(const DevParams& P, const BDesc* d_descs, int n, cudaStream_t s);
@@ -3314,9 +3315,10 @@ int vc1cu_loop_filter_p_main(vc1cu_ctx* c, const vc1cu_params* p, int frame_id, 
 }
 
 // The signed intra reconstruction of frame slot src_id (HOST flags / mquant / derived, copied on the
-// context stream) into the device planes d_y, d_u, d_v.
-static void intra_recon(vc1cu_ctx* c, const DevParams& P, FrameSlot& fs, int overlap, const uint8_t* flags,
-                        const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v) {
+// context stream) into the device planes d_y, d_u, d_v, with the trellis and perceptual settings of cfg.
+static void intra_recon(vc1cu_ctx* c, const DevParams& P, const vc1cu_trd_cfg& cfg, FrameSlot& fs, int overlap,
+                        const uint8_t* flags, const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u,
+                        int32_t* d_v) {
     const size_t mbs = (size_t)P.mbw * P.mbh;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b_scr = al(intra_scratch_bytes(P)), b_edge = al(mbs * 256 * 3 / 2), b_map = al(mbs);
@@ -3330,9 +3332,23 @@ static void intra_recon(vc1cu_ctx* c, const DevParams& P, FrameSlot& fs, int ove
     if (derived) ck(cudaMemcpyAsync(d_der, derived, mbs, cudaMemcpyHostToDevice, c->stream), "upload derived flags");
     Timer tm(c, kXform);
     ck(launch_intra_recon(P, fs.view(), overlap, overlap == 2 ? d_flags : nullptr, mquant ? d_mq : nullptr,
-                          derived ? d_der : nullptr, base, base + b_scr, d_y, d_u, d_v, c->stream),
+                          derived ? d_der : nullptr, base, base + b_scr, d_y, d_u, d_v,
+                          cfg.trellis > 0 ? trd_tables(c) : nullptr, cfg, c->stream),
        "intra reconstruction launch");
     tm.stop(overlap ? 4 : 3);
+}
+
+// The intra settings of cfg (NULL: scalar levels, no perceptual scale).
+static vc1cu_trd_cfg intra_cfg(const vc1cu_trd_cfg* cfg) {
+    vc1cu_trd_cfg k{};
+    if (cfg) {
+        if (cfg->trellis < 0 || cfg->trellis > 2) throw Fail{VC1CU_ERR_ARG, "trellis is 0, 1 or 2"};
+        k.trellis = cfg->trellis;
+        k.adaptive_quality = cfg->adaptive_quality;
+        k.aq_strength = cfg->aq_strength;
+        k.hrd_enabled = cfg->hrd_enabled;
+    }
+    return k;
 }
 
 static void check_intra_args(const DevParams& P, FrameSlot& fs, const uint8_t* mquant) {
@@ -3342,8 +3358,9 @@ static void check_intra_args(const DevParams& P, FrameSlot& fs, const uint8_t* m
             if (mquant[i] < 1 || mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 1..31"};
 }
 
-int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int overlap, const uint8_t* flags,
-                            const uint8_t* mquant, const uint8_t* derived, int32_t* d_y, int32_t* d_u, int32_t* d_v) {
+int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id, int overlap,
+                            const uint8_t* flags, const uint8_t* mquant, const uint8_t* derived, int32_t* d_y,
+                            int32_t* d_u, int32_t* d_v) {
     return guarded(c, [&]() -> int {
         if (!d_y || !d_u || !d_v) throw Fail{VC1CU_ERR_ARG, "null signed plane"};
         if (overlap < 0 || overlap > 2) throw Fail{VC1CU_ERR_ARG, "overlap is 0 none, 1 all or 2 select"};
@@ -3354,14 +3371,14 @@ int vc1cu_reconstruct_intra(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int
         if (rc) throw Fail{rc, why};
         FrameSlot& fs = frame_slot(c, src_id);
         check_intra_args(P, fs, mquant);
-        intra_recon(c, P, fs, overlap, flags, mquant, derived, d_y, d_u, d_v);
+        intra_recon(c, P, intra_cfg(cfg), fs, overlap, flags, mquant, derived, d_y, d_u, d_v);
         ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");  // the copies read the caller's arrays
         return VC1CU_OK;
     });
 }
 
-int vc1cu_choose_i_overlap(vc1cu_ctx* c, const vc1cu_params* p, int src_id, const uint8_t* mquant, const uint8_t* derived,
-                           int* mode, uint8_t* flags) {
+int vc1cu_choose_i_overlap(vc1cu_ctx* c, const vc1cu_params* p, const vc1cu_trd_cfg* cfg, int src_id,
+                           const uint8_t* mquant, const uint8_t* derived, int* mode, uint8_t* flags) {
     return guarded(c, [&]() -> int {
         if (!mode || !flags) throw Fail{VC1CU_ERR_ARG, "null output"};
         DevParams P;
@@ -3370,6 +3387,7 @@ int vc1cu_choose_i_overlap(vc1cu_ctx* c, const vc1cu_params* p, int src_id, cons
         if (rc) throw Fail{rc, why};
         FrameSlot& fs = frame_slot(c, src_id);
         check_intra_args(P, fs, mquant);
+        const vc1cu_trd_cfg icfg = intra_cfg(cfg);
         const size_t mbs = (size_t)P.mbw * P.mbh;
         std::fill(flags, flags + mbs, (uint8_t)0);
         if (P.pq >= 9) {  // unconditional overlap above the CONDOVER range (:290-294)
@@ -3395,7 +3413,7 @@ int vc1cu_choose_i_overlap(vc1cu_ctx* c, const vc1cu_params* p, int src_id, cons
                                   128, sse + (size_t)k * mbs, c->stream),
                "overlap error launch");
         };
-        intra_recon(c, P, fs, 0, nullptr, mquant, derived, rec(0, 0), rec(0, 1), rec(0, 2));
+        intra_recon(c, P, icfg, fs, 0, nullptr, mquant, derived, rec(0, 0), rec(0, 1), rec(0, 2));
         ck(cudaMemcpyAsync(rec(1, 0), rec(0, 0), 4 * (ny + 2 * nc), cudaMemcpyDeviceToDevice, c->stream), "copy reconstruction");
         ck(launch_overlap(rec(1, 0), rec(1, 1), rec(1, 2), P.mbw, P.mbh, nullptr, 1, c->stream), "overlap launch");
         errors(0);

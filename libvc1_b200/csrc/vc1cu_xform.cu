@@ -705,10 +705,11 @@ __device__ int rate_for_set(const DevParams& P, const TrdTables* T, int run, int
     return imin(best, esc + 2 + 1 + 6 + 1 + esc3_level_bits(P));
 }
 
-// trellis_rate_bits (:1843-1857), inter family: the lower envelope of coding sets 1, 3, 5
-__device__ int rate_inter(const DevParams& P, const TrdTables* T, int run, int level, bool last) {
+// trellis_rate_bits (:1843-1857): the lower envelope of coding sets 1, 3, 5 (inter family) or
+// 0, 2, 4 (intra family)
+__device__ int rate_family(const DevParams& P, const TrdTables* T, int run, int level, bool last, bool intra) {
     int bits = 1000000;
-    for (int s = 1; s <= 5; s += 2) bits = imin(bits, rate_for_set(P, T, run, level, last, s));
+    for (int s = intra ? 0 : 1; s <= 5; s += 2) bits = imin(bits, rate_for_set(P, T, run, level, last, s));
     return bits;
 }
 
@@ -850,7 +851,7 @@ __device__ uint32_t parent_ttblk_bits(const DevParams& P, const TParent& p) {
     return (uint32_t)bits;
 }
 
-// ---- trellis_quantize (:1873-2088), inter family, first_scan 0 ----------------------------
+// ---- trellis_quantize (:1873-2088) ---------------------------------------------------------
 
 // trellis_coeff_weight (:1859-1871)
 __device__ __forceinline__ double trellis_weight(int t, int index) {
@@ -875,15 +876,16 @@ __device__ __forceinline__ bool tstate_less(const TState& a, const TState& b) {
     return a.distortion < b.distortion;
 }
 
-// Levels q (partition-local 8-stride) of coefficients c for transform type t. The beam's paths are
-// kept as back-pointers per scan position (the state each survivor extends, its level there).
-__device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, double lambda_scale, int mquant, int* q) {
+// Levels q (partition-local 8-stride) of coefficients c for transform type t along scan[0..n); the
+// trellis decides positions first_scan..n-1 (1 for intra blocks, whose DC is coded apart, leaving
+// q[scan[0]] zero) with the rates of the intra or inter family. The beam's paths are kept as
+// back-pointers per scan position (the state each survivor extends, its level there).
+__device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, double lambda_scale, int mquant, int* q,
+                                 const uint8_t* scan, int n, int first_scan, bool intra) {
     const DevParams& P = A.P;
     const bool derived = mquant != P.pq;
     const double qscale = (double)trd_double_quant(P, mquant, derived);
     const int max_level = trd_max_level(P);
-    int n;
-    const uint8_t* scan = inter_scan(t, n);
     int scalar[64];
     for (int i = 0; i < 64; ++i) scalar[i] = 0;
     for (int s = 0; s < n; ++s) scalar[scan[s]] = trd_squant(P, c[scan[s]], mquant, derived);
@@ -894,8 +896,8 @@ __device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, doubl
     uint16_t bp[64][8];  // back-pointer: from state (3 bits) | level + 4096 (13 bits)
     TState states[8];
     int count = 1;
-    states[0] = TState{0.0, 0.0, 0u, -1, -1, 0};
-    for (int s = 0; s < n; ++s) {
+    states[0] = TState{0.0, 0.0, 0u, first_scan - 1, -1, 0};
+    for (int s = first_scan; s < n; ++s) {
         const int idx = scan[s];
         const int q0 = scalar[idx];
         int cand[4], nc = 0;
@@ -928,7 +930,7 @@ __device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, doubl
                 ns.from = si;
                 ns.level = level;
                 if (level != 0) {
-                    const int rb = rate_inter(P, A.tab, s - st.last_scan - 1, level, false);
+                    const int rb = rate_family(P, A.tab, s - st.last_scan - 1, level, false, intra);
                     if (rb >= 1000000) continue;
                     ns.bits += (uint32_t)rb;
                     ns.last_scan = s;
@@ -960,19 +962,19 @@ __device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, doubl
         int next_pos = -1, next_level = 0;  // the coefficient after this one on the path (towards the end)
         int j = si;
         bool first = true;
-        for (int s = n - 1; s >= 0; --s) {
+        for (int s = n - 1; s >= first_scan; --s) {
             const int level = (int)(bp[s][j] & 0x1FFF) - 4096;
             const int from = bp[s][j] >> 13;
             if (level != 0) {
                 if (next_pos >= 0)
-                    bits += (uint32_t)rate_inter(P, A.tab, next_pos - s - 1, next_level, first);
+                    bits += (uint32_t)rate_family(P, A.tab, next_pos - s - 1, next_level, first, intra);
                 if (next_pos >= 0) first = false;
                 next_pos = s;
                 next_level = level;
             }
             j = from;
         }
-        if (next_pos >= 0) bits += (uint32_t)rate_inter(P, A.tab, next_pos - (-1) - 1, next_level, first);
+        if (next_pos >= 0) bits += (uint32_t)rate_family(P, A.tab, next_pos - first_scan, next_level, first, intra);
         const double rd = states[si].distortion + lambda * (double)bits;
         if (rd < best_rd) {
             best = si;
@@ -981,7 +983,7 @@ __device__ void trellis_quantize(const TrdArgs& A, const double* c, int t, doubl
     }
     for (int i = 0; i < 64; ++i) q[i] = 0;
     int j = best;
-    for (int s = n - 1; s >= 0; --s) {
+    for (int s = n - 1; s >= first_scan; --s) {
         const int level = (int)(bp[s][j] & 0x1FFF) - 4096;
         if (level != 0) q[scan[s]] = level;
         j = bp[s][j] >> 13;
@@ -1018,7 +1020,9 @@ __device__ void eval_parent(const TrdArgs& A, int mx, int my, int k, int t, bool
             if (allow_trellis && A.cfg.trellis > 0) {
                 const double ls = aq_scale(A, sp, spitch, w, h, x0, y0, bw, bh, pp, ppitch, chroma ? A.src.y : nullptr,
                                            A.src.pitch_y);
-                trellis_quantize(A, c, t, ls, mquant, q);
+                int n;
+                const uint8_t* scan = inter_scan(t, n);
+                trellis_quantize(A, c, t, ls, mquant, q, scan, n, 0, false);
             } else {
                 for (int y = 0; y < bh; ++y)
                     for (int x = 0; x < bw; ++x) q[y * 8 + x] = trd_squant(P, c[y * 8 + x], mquant, derived);
@@ -1350,6 +1354,7 @@ struct IntraArgs {
     int16_t* q;                    // [mb][6][64] AC levels
     int* dc[3];                    // per plane block grid: the DC target, then the final DC
     int* qg[3];                    // per plane block grid: MQUANT, negative when derived
+    TrdArgs trd;                   // P, tab, cfg (trellis, hrd_enabled, AQ) and the intra source's luma mean
 };
 
 __device__ __forceinline__ int intra_mq(const IntraArgs& A, int mb) {
@@ -1357,8 +1362,10 @@ __device__ __forceinline__ int intra_mq(const IntraArgs& A, int mb) {
 }
 
 // One thread per (MB, block): forward_transform (:672-795; samples outside the source read the
-// pad value, 0 luma / 128 chroma, minus 128), scalar_quantize_level of the AC coefficients
-// (quantize_ac :2090-2144 at trellis 0) and choose_dc_for_mean of the padded block mean.
+// pad value, 0 luma / 128 chroma, minus 128), the AC levels of quantize_ac (:2090-2144: scalar, or
+// the trellis along the intra scan from position 1 with the intra-family rates and the perceptual
+// lambda scale of the block, chroma judged against the intra source's luma) and
+// choose_dc_for_mean of the padded block mean.
 __global__ void intra_fwd_kernel(const __grid_constant__ IntraArgs A) {
     const DevParams& P = A.P;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1389,13 +1396,26 @@ __global__ void intra_fwd_kernel(const __grid_constant__ IntraArgs A) {
         }
     int16_t* q = A.q + (size_t)i * 64;
     q[0] = 0;
+    const bool trellis = A.trd.cfg.trellis > 0 && !(A.trd.cfg.hrd_enabled && mq == 1);
+    double c[64];
     for (int a = 0; a < 8; ++a)
         for (int b = 0; b < 8; ++b) {
             if (!a && !b) continue;
             double acc = 0.0;
             for (int x = 0; x < 8; ++x) acc = __dadd_rn(acc, __dmul_rn(tmp[a][x], c_k8[b][x]));
-            q[b * 8 + a] = (int16_t)trd_squant(P, __dmul_rn(1024.0, acc), mq, derived);  // c[row*8+col] = xform[col][row]
+            c[b * 8 + a] = __dmul_rn(1024.0, acc);  // c[row*8+col] = xform[col][row]
+            if (!trellis) q[b * 8 + a] = (int16_t)trd_squant(P, c[b * 8 + a], mq, derived);
         }
+    if (trellis) {
+        c[0] = 0.0;  // the DC stays out of the trellis (first_scan 1)
+        // the luma context is read as a coded-width raster (stats(*luma_context, width, height, ...)):
+        // an edge source of a cropped picture is a padded-width raster read at the coded width
+        const int lpitch = A.sw == P.W ? A.pitch_y : P.W;
+        const double ls = aq_scale(A.trd, p, pitch, w, h, x0, y0, 8, 8, nullptr, 0, chroma ? A.y : nullptr, lpitch);
+        int lv[64];
+        trellis_quantize(A.trd, c, 1, ls, mq, lv, ent::kIntraScan, 64, 1, !chroma);
+        for (int j = 1; j < 64; ++j) q[j] = (int16_t)lv[j];
+    }
     const int gw = chroma ? P.mbw : P.mbw * 2;
     A.dc[chroma ? k - 3 : 0][by * gw + bx] = intra_dc_for_mean((int)((sum + 32u) / 64u), mq, 128);
 }
@@ -1618,7 +1638,8 @@ cudaError_t launch_dquant_stats(const DevParams& P, const DevFrame& src, const D
 // MB, nullptr with all = 0 for none), the forward transforms and AC levels, the DC chain, the
 // inverse transforms into the int32 planes oy / ou / ov (padded raster, rows packed). scratch
 // holds intra_scratch_bytes(P) bytes; edge: 1.5 * (mbw * 16) * (mbh * 16) bytes for the edge
-// source.
+// source. tables / cfg: the AC length tables and the trellis and perceptual settings (trellis 0:
+// scalar levels); the trellis's lambda scale reads the intra source's luma mean, taken here.
 size_t intra_scratch_bytes(const DevParams& P) {
     const size_t mbs = (size_t)P.mbw * P.mbh;
     return mbs * 6 * 64 * 2 + mbs * 6 * 4 * 2 + 256;
@@ -1626,7 +1647,8 @@ size_t intra_scratch_bytes(const DevParams& P) {
 
 cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int overlap, const uint8_t* d_flags,
                                const uint8_t* d_mquant, const uint8_t* d_derived, void* scratch, uint8_t* edge,
-                               int32_t* oy, int32_t* ou, int32_t* ov, cudaStream_t s) {
+                               int32_t* oy, int32_t* ou, int32_t* ov, const void* tables, const vc1cu_trd_cfg& cfg,
+                               cudaStream_t s) {
     const int mbs = P.mbw * P.mbh;
     if (mbs <= 0) return cudaSuccess;
     IntraArgs A{};
@@ -1691,6 +1713,20 @@ cudaError_t launch_intra_recon(const DevParams& P, const DevFrame& src, int over
     A.qg[0] = qg;
     A.qg[1] = qg + (size_t)mbs * 4;
     A.qg[2] = qg + (size_t)mbs * 5;
+    A.trd.P = P;
+    A.trd.tab = static_cast<const TrdTables*>(tables);
+    A.trd.cfg = cfg;
+    A.trd.frame_mean = 0.0;
+    if (cfg.trellis > 0) {  // cached_luma_mean of the intra source's luma (the picture or its edge source)
+        DevParams sp = P;
+        sp.W = A.sw;
+        sp.H = A.sh;
+        DevFrame sf{};
+        sf.y = A.y;
+        sf.pitch_y = A.pitch_y;
+        unsigned long long* d_sum = reinterpret_cast<unsigned long long*>(qg + (size_t)mbs * 6);
+        if ((e = frame_mean_for(sp, sf, cfg, d_sum, s, A.trd.frame_mean)) != cudaSuccess) return e;
+    }
     const unsigned blocks = (unsigned)((mbs * 6 + 127) / 128);
     intra_fwd_kernel<<<blocks, 128, 0, s>>>(A);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -352,8 +352,8 @@ class Reference:
         L.ref_p_mode_scores.restype = i32
         L.ref_b_mode_scores.argtypes = [vp, C.POINTER(PpicCfg), vp, vp, vp, vp, vp, i32, i32, vp, C.POINTER(i32)]
         L.ref_b_mode_scores.restype = i32
-        L.ref_reconstruct_intra.argtypes = [vp, i32, C.c_double, vp, i32, vp, vp, vp, vp, vp, vp]
-        L.ref_choose_i_overlap.argtypes = [vp, i32, C.c_double, vp, C.POINTER(i32), vp]
+        L.ref_reconstruct_intra.argtypes = [vp, i32, C.c_double, i32, vp, i32, vp, vp, vp, vp, vp, vp]
+        L.ref_choose_i_overlap.argtypes = [vp, i32, C.c_double, i32, vp, C.POINTER(i32), vp]
         L.ref_estimate_p_motion_bits.argtypes = [vp, vp, vp, vp, vp, i32, i32]
         L.ref_estimate_p_motion_bits.restype = u64
         L.ref_motion_compensate.argtypes = [vp, vp, vp, vp, vp, i32, vp]
@@ -594,9 +594,9 @@ class Reference:
             raise RuntimeError("reference B mode scoring threw")
         return scores, chosen.value
 
-    def reconstruct_intra(self, frame, overlap=0, flags=None, dquant=False, aq_strength=0.0):
-        """reconstruct_i_signed_padded at trellis 0: the signed int32 planes of the padded raster
-        and the DQUANT plan's per-MB MQUANT and derived flags."""
+    def reconstruct_intra(self, frame, overlap=0, flags=None, dquant=False, aq_strength=0.0, trellis=0):
+        """reconstruct_i_signed_padded (AQ on when aq_strength > 0): the signed int32 planes of the
+        padded raster and the DQUANT plan's per-MB MQUANT and derived flags."""
         mbw, mbh = mbs_of(self.p)
         pw, ph = mbw * 16, mbh * 16
         y = np.zeros((ph, pw), np.int32)
@@ -605,17 +605,18 @@ class Reference:
         mq = np.zeros(mbw * mbh, np.uint8)
         der = np.zeros(mbw * mbh, np.uint8)
         fl = None if flags is None else np.ascontiguousarray(flags, np.uint8)
-        self.lib.ref_reconstruct_intra(self.h, int(dquant), aq_strength, self._f(frame), overlap,
+        self.lib.ref_reconstruct_intra(self.h, int(dquant), aq_strength, int(trellis), self._f(frame), overlap,
                                        None if fl is None else fl.ctypes.data, y.ctypes.data, u.ctypes.data,
                                        v.ctypes.data, mq.ctypes.data, der.ctypes.data)
         return (y, u, v), mq, der
 
-    def choose_i_overlap(self, frame, dquant=False, aq_strength=0.0):
+    def choose_i_overlap(self, frame, dquant=False, aq_strength=0.0, trellis=0):
         """choose_i_overlap_plan with OVERLAP on: (mode 0 none / 1 all / 2 select, per-MB flags)."""
         mbw, mbh = mbs_of(self.p)
         flags = np.zeros(mbw * mbh, np.uint8)
         mode = i32()
-        self.lib.ref_choose_i_overlap(self.h, int(dquant), aq_strength, self._f(frame), C.byref(mode), flags.ctypes.data)
+        self.lib.ref_choose_i_overlap(self.h, int(dquant), aq_strength, int(trellis), self._f(frame), C.byref(mode),
+                                      flags.ctypes.data)
         return mode.value, flags
 
     def estimate_p_motion_bits(self, a: Analysis, mode: int, intensity: bool = False) -> int:

@@ -547,15 +547,15 @@ int ref_b_mode_scores(void* h, const vc1cu_ppic_cfg* pc, void* cur, void* past, 
     }
 }
 
-// reconstruct_i_signed_padded (encoder_encode.cpp:814-887) at trellis 0, DQUANT on (with the
-// perceptual scale at aq_strength) or off, with the overlap plan (mode 0 none, 1 all, 2 select
+// reconstruct_i_signed_padded (encoder_encode.cpp:814-887) at the given trellis (0 scalar, 1, 2),
+// DQUANT on or off, the perceptual scale at aq_strength (0: off), with the overlap plan (mode 0 none, 1 all, 2 select
 // with flags) whose edge source it reads; the signed planes of the padded raster go to y, u, v.
 // mquant / derived (when set) receive the DQUANT plan the function forms (choose_intra_mquant,
 // make_dquant_plan, dquant_mb_derived; :826-833).
-void ref_reconstruct_intra(void* h, int dquant, double aq_strength, void* src, int overlap, const uint8_t* flags,
-                           int32_t* y, int32_t* u, int32_t* v, uint8_t* mquant, uint8_t* derived) {
+void ref_reconstruct_intra(void* h, int dquant, double aq_strength, int trellis, void* src, int overlap,
+                           const uint8_t* flags, int32_t* y, int32_t* u, int32_t* v, uint8_t* mquant, uint8_t* derived) {
     EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
-    c.trellis = 0;
+    c.trellis = trellis;
     c.dquant = dquant != 0;
     c.adaptive_quality = aq_strength > 0.0;
     c.aq_strength = aq_strength;
@@ -583,11 +583,11 @@ void ref_reconstruct_intra(void* h, int dquant, double aq_strength, void* src, i
     }
 }
 
-// choose_i_overlap_plan (encoder_filter.cpp:277-343) with OVERLAP on, trellis 0, DQUANT on (with
-// the perceptual scale at aq_strength) or off: the plan's mode (0 none, 1 all, 2 select) and flags.
-void ref_choose_i_overlap(void* h, int dquant, double aq_strength, void* src, int* mode, uint8_t* flags) {
+// choose_i_overlap_plan (encoder_filter.cpp:277-343) with OVERLAP on, the given trellis, DQUANT on or
+// off, the perceptual scale at aq_strength (0: off): the plan's mode (0 none, 1 all, 2 select) and flags.
+void ref_choose_i_overlap(void* h, int dquant, double aq_strength, int trellis, void* src, int* mode, uint8_t* flags) {
     EncoderConfig c = static_cast<RefEncoder*>(h)->cfg;
-    c.trellis = 0;
+    c.trellis = trellis;
     c.overlap = true;
     c.dquant = dquant != 0;
     c.adaptive_quality = aq_strength > 0.0;
