@@ -642,6 +642,17 @@ int vc1cu_choose_dquant(vc1cu_ctx* ctx, const vc1cu_params* p, const vc1cu_trd_c
 int vc1cu_reconstruct(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
                       const uint8_t* block_types, int out_id);
 
+/*
+ * vc1cu_reconstruct under a DQUANT plan: each MB's levels dequantised at its MQUANT (dequant_level,
+ * :1058-1065; a derived MQUANT, or one other than PQINDEX, without the HALFQP half step), as the
+ * picture coder reconstructs the decisions of vc1cu_choose_dquant. mquant: HOST mbw*mbh MQUANTs
+ * (1..31); derived: HOST mbw*mbh DQUANT-derived flags, or NULL for none. Returns once the host
+ * arrays are copied.
+ */
+int vc1cu_reconstruct_dquant(vc1cu_ctx* ctx, const vc1cu_params* p, int pred_id, const int16_t* d_levels,
+                             int type_mask, const uint8_t* block_types, const uint8_t* mquant, const uint8_t* derived,
+                             int out_id);
+
 /* ---- the P picture's motion-mode decision (Vc1Encoder::analyze_p_picture) ---------- */
 
 /*

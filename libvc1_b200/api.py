@@ -47,6 +47,7 @@ EXPORTS = (
     "vc1cu_graph_begin", "vc1cu_graph_end", "vc1cu_graph_launch", "vc1cu_graph_destroy", "vc1cu_autotune",
     "vc1cu_p_motion_bits", "vc1cu_analyze_p_picture", "vc1cu_b_mode_rd", "vc1cu_loop_filter_p_main",
     "vc1cu_choose_dquant", "vc1cu_reconstruct_intra", "vc1cu_choose_i_overlap",
+    "vc1cu_reconstruct_dquant",
 )
 
 
@@ -123,6 +124,7 @@ def load_library(path: str = LIB_PATH):
     L.vc1cu_debug_index_faults.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_ulonglong), i32]
     L.vc1cu_choose_transform.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp]
     L.vc1cu_choose_dquant.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, i32, i32, vp, vp, vp, vp]
+    L.vc1cu_reconstruct_dquant.argtypes = [vp, PP, i32, vp, i32, vp, vp, vp, i32]
     L.vc1cu_reconstruct_intra.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, i32, vp, vp, vp, vp, vp, vp]
     L.vc1cu_choose_i_overlap.argtypes = [vp, PP, C.POINTER(TrdCfg), i32, vp, vp, C.POINTER(i32), vp]
     L.vc1cu_p_motion_bits.argtypes = [vp, PP, i32, i32, i32, C.POINTER(C.c_uint64)]
@@ -580,10 +582,20 @@ class CudaComputeContext:
         self._check(self._L.vc1cu_store_signed(self._h, C.byref(params), d_y, d_u, d_v, int(bias),
                                                None if m is None else m.ctypes.data, out_id))
 
-    def reconstruct(self, params: Params, pred_id: int, d_levels: int, type_mask: int, block_types, out_id: int):
+    def reconstruct(self, params: Params, pred_id: int, d_levels: int, type_mask: int, block_types, out_id: int,
+                    mquant=None, derived=None):
         """Frame slot out_id = pred_id + the inverse-transformed levels of each block's type
-        (device levels in forward_quant_device's layout; block_types: (mbs, 6) TransformType codes)."""
+        (device levels in forward_quant_device's layout; block_types: (mbs, 6) TransformType codes),
+        dequantised at PQINDEX or at the per-MB MQUANT and derived flags of a DQUANT plan
+        (vc1cu_reconstruct_dquant)."""
         bt = np.ascontiguousarray(block_types, np.uint8)
+        if mquant is not None:
+            mq = np.ascontiguousarray(mquant, np.uint8)
+            der = None if derived is None else np.ascontiguousarray(derived, np.uint8)
+            self._check(self._L.vc1cu_reconstruct_dquant(self._h, C.byref(params), pred_id, d_levels, type_mask,
+                                                          bt.ctypes.data, mq.ctypes.data,
+                                                          None if der is None else der.ctypes.data, out_id))
+            return
         self._check(self._L.vc1cu_reconstruct(self._h, C.byref(params), pred_id, d_levels, type_mask, bt.ctypes.data,
                                               out_id))
 

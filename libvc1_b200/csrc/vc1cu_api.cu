@@ -88,7 +88,8 @@ cudaError_t launch_store_signed(const int32_t* y, const int32_t* u, const int32_
                                 int W, int H, cudaStream_t s);
 void launch_fast_tt(const DevParams& P, const DevFrame& src, const DevFrame& pred, uint8_t* types, cudaStream_t s);
 void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
-                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
+                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s,
+                  const uint8_t* mquant = nullptr, const uint8_t* derived = nullptr);
 cudaError_t launch_b_mc(const DevParams& P, const DevFrame& cur, const DevFrame& past, const DevFrame& fut,
                         const uint8_t* modes, const int2* fmv, const int2* bmv, int mode, uint8_t* dy, uint8_t* du,
                         uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s);
@@ -3515,8 +3516,8 @@ int vc1cu_store_signed(vc1cu_ctx* c, const vc1cu_params* p, const int32_t* d_y, 
     });
 }
 
-int vc1cu_reconstruct(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
-                      const uint8_t* block_types, int out_id) {
+static int reconstruct(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
+                       const uint8_t* block_types, const uint8_t* mquant, const uint8_t* derived, int out_id) {
     return guarded(c, [&]() -> int {
         if (!d_levels || !block_types) throw Fail{VC1CU_ERR_ARG, "null levels or block types"};
         if (type_mask < 1 || type_mask > 15) throw Fail{VC1CU_ERR_ARG, "type_mask must select 1..4 transform types"};
@@ -3536,17 +3537,37 @@ int vc1cu_reconstruct(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const in
         const DevFrame pred = fp.view();
         FrameSlot& fo = alloc_frame(c, out_id, P.W, P.H);
         const DevFrame o = fo.view();
-        uint8_t* dt = static_cast<uint8_t*>(ensure(c->d_btypes, c->btypes_cap, (size_t)mbs * 6, "cudaMalloc(block types)"));
+        if (mquant)
+            for (int i = 0; i < mbs; ++i)
+                if (mquant[i] < 1 || mquant[i] > 31) throw Fail{VC1CU_ERR_ARG, "MQUANT must be 1..31"};
+        // block types, then the per-MB MQUANT and derived flags (8 bytes per MB in all)
+        uint8_t* dt = static_cast<uint8_t*>(ensure(c->d_btypes, c->btypes_cap, (size_t)mbs * 8, "cudaMalloc(block types)"));
         ck(cudaMemcpyAsync(dt, block_types, (size_t)mbs * 6, cudaMemcpyHostToDevice, c->stream), "upload block types");
+        uint8_t* dmq = dt + (size_t)mbs * 6;
+        uint8_t* dder = dmq + mbs;
+        if (mquant) ck(cudaMemcpyAsync(dmq, mquant, (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload MQUANT");
+        if (derived) ck(cudaMemcpyAsync(dder, derived, (size_t)mbs, cudaMemcpyHostToDevice, c->stream), "upload derived flags");
         int ti[4], n = 0;
         for (int t = 0; t < 4; ++t) ti[t] = (type_mask >> t) & 1 ? n++ : -1;
         Timer tm(c, kXform);
         launch_recon(P, pred, d_levels, make_int4(ti[0], ti[1], ti[2], ti[3]), dt, (uint8_t*)o.y, (uint8_t*)o.u, (uint8_t*)o.v,
-                     fo.pitch_y, fo.pitch_c, c->stream);
+                     fo.pitch_y, fo.pitch_c, c->stream, mquant ? dmq : nullptr, mquant && derived ? dder : nullptr);
         ck(cudaGetLastError(), "reconstruction launch");
         tm.stop(1);
+        if (mquant) ck(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");  // the copies read the caller's arrays
         return VC1CU_OK;
     });
+}
+
+int vc1cu_reconstruct(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
+                      const uint8_t* block_types, int out_id) {
+    return reconstruct(c, p, pred_id, d_levels, type_mask, block_types, nullptr, nullptr, out_id);
+}
+
+int vc1cu_reconstruct_dquant(vc1cu_ctx* c, const vc1cu_params* p, int pred_id, const int16_t* d_levels, int type_mask,
+                             const uint8_t* block_types, const uint8_t* mquant, const uint8_t* derived, int out_id) {
+    if (!mquant) return guarded(c, [&]() -> int { throw Fail{VC1CU_ERR_ARG, "null MQUANT"}; });
+    return reconstruct(c, p, pred_id, d_levels, type_mask, block_types, mquant, derived, out_id);
 }
 
 int vc1cu_forward_quant_device(vc1cu_ctx* c, const vc1cu_params* p, int src_id, int pred_id, int type_mask,

@@ -230,12 +230,22 @@ __device__ __forceinline__ void inv4(const int* s, int st, int* o, int ot, int b
     o[3 * ot] = arshift(t1 - t3, shift);
 }
 
-// One thread per (MB, parent): every partition of the block's chosen type dequantised,
-// inverse-transformed (with the DC-only shortcut of a partition whose only level is its DC)
-// and added to the prediction with 8-bit clamping. tindex[t] is type t's index in the levels
-// layout [type][mb][parent][64] (-1 for a type the layout does not hold).
+// dequant_level (encoder_transform.cpp:1052-1065) at an MB's MQUANT: a DQUANT-derived MQUANT, or one
+// other than PQINDEX, takes no HALFQP half step
+__device__ __forceinline__ int dequant_mq(const DevParams& P, int level, int mquant, bool derived) {
+    if (!level) return 0;
+    const int v = level * (2 * mquant + ((!derived && mquant == P.pq && P.halfqp) ? 1 : 0));
+    return P.nonuniform ? v + (level > 0 ? mquant : -mquant) : v;
+}
+
+// One thread per (MB, parent): every partition of the block's chosen type dequantised at PQINDEX
+// or at the MB's MQUANT (mquant / derived: per-MB device arrays, or nullptr), inverse-transformed
+// (with the DC-only shortcut of a partition whose only level is its DC) and added to the
+// prediction with 8-bit clamping. tindex[t] is type t's index in the levels layout
+// [type][mb][parent][64] (-1 for a type the layout does not hold).
 __global__ void recon_kernel(const __grid_constant__ DevParams P, DevFrame pred, const int16_t* levels, int4 tindex,
-                             const uint8_t* block_types, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c) {
+                             const uint8_t* block_types, uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c,
+                             const uint8_t* mquant, const uint8_t* derived) {
     const int mbs = P.mbw * P.mbh;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= mbs * 6) return;
@@ -243,6 +253,8 @@ __global__ void recon_kernel(const __grid_constant__ DevParams P, DevFrame pred,
     const int t = block_types[idx];
     const int ti = t == 1 ? tindex.x : (t == 2 ? tindex.y : (t == 3 ? tindex.z : tindex.w));
     const int16_t* q64 = levels + (((size_t)ti * mbs + mb) * 6 + k) * 64;
+    const int mq = mquant ? (int)mquant[mb] : P.pq;
+    const bool der = derived && derived[mb];
     int res[64];
 #pragma unroll
     for (int i = 0; i < 64; ++i) res[i] = 0;
@@ -259,7 +271,7 @@ __global__ void recon_kernel(const __grid_constant__ DevParams P, DevFrame pred,
                 const int lv = (y < bh && x < bw) ? q64[(oy + y) * 8 + ox + x] : 0;
                 nonzero += lv != 0;
                 if (!y && !x) q0 = lv;
-                a[y * 8 + x] = dequant(P, lv);
+                a[y * 8 + x] = mquant ? dequant_mq(P, lv, mq, der) : dequant(P, lv);
                 tmp[y * 8 + x] = 0;
             }
         if (nonzero == 1 && q0 != 0) {
@@ -302,9 +314,11 @@ __global__ void recon_kernel(const __grid_constant__ DevParams P, DevFrame pred,
 }
 
 void launch_recon(const DevParams& P, const DevFrame& pred, const int16_t* levels, int4 tindex, const uint8_t* block_types,
-                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s) {
+                  uint8_t* dy, uint8_t* du, uint8_t* dv, int pitch_y, int pitch_c, cudaStream_t s, const uint8_t* mquant,
+                  const uint8_t* derived) {
     const int n = P.mbw * P.mbh * 6;
-    recon_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, pred, levels, tindex, block_types, dy, du, dv, pitch_y, pitch_c);
+    recon_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(P, pred, levels, tindex, block_types, dy, du, dv, pitch_y, pitch_c,
+                                                             mquant, derived);
 }
 
 // ---- transform type of the throughput preset (encoder_transform.cpp:1605-1712) ----------------

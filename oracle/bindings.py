@@ -366,7 +366,7 @@ class Reference:
         L.ref_scene_change_score.argtypes = [vp, vp, vp, i32, C.c_double]
         L.ref_scene_change_score.restype = C.c_double
         L.ref_b_predict.argtypes = [vp, vp, vp, vp, vp, vp, vp, i32, vp]
-        L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp]
+        L.ref_reconstruct.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp]
         L.ref_loop_filter_i.argtypes = [vp, vp]
         L.ref_loop_filter_p.argtypes = [vp, vp, vp, vp, vp, vp, i32]
         L.ref_overlap.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
@@ -508,13 +508,15 @@ class Reference:
         self.lib.ref_fast_transform_types(self.h, self._f(src), self._f(pred), out.ctypes.data)
         return out
 
-    def reconstruct(self, pred, levels, type_mask, block_types):
+    def reconstruct(self, pred, levels, type_mask, block_types, mquant=None, derived=None):
         h, w = self.p.height, self.p.width
         dst = self.frame((np.zeros((h, w), np.uint8), np.zeros((h // 2, w // 2), np.uint8),
                           np.zeros((h // 2, w // 2), np.uint8)))
         lv = np.ascontiguousarray(levels, np.int16)
         bt = np.ascontiguousarray(block_types, np.uint8)
-        self.lib.ref_reconstruct(self.h, self._f(pred), lv.ctypes.data, type_mask, bt.ctypes.data, dst.h)
+        mq, der = [None if a is None else np.ascontiguousarray(a, np.uint8) for a in (mquant, derived)]
+        self.lib.ref_reconstruct(self.h, self._f(pred), lv.ctypes.data, type_mask, bt.ctypes.data,
+                                 None if mq is None else mq.ctypes.data, None if der is None else der.ctypes.data, dst.h)
         y = np.zeros((h, w), np.uint8)
         u = np.zeros((h // 2, w // 2), np.uint8)
         v = np.zeros_like(u)

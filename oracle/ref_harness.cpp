@@ -328,8 +328,10 @@ void ref_b_predict(void* h, void* cur, void* past, void* future, const uint8_t* 
 
 // Reconstruction of each (MB, parent) with its chosen transform type as
 // evaluate_transform_parent forms it (encoder_transform.cpp:1569-1585): inverse_partition of
-// every partition's levels (layout of ref_forward_quant for type_mask) added to the prediction.
-void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, const uint8_t* block_types, void* dst) {
+// every partition's levels (layout of ref_forward_quant for type_mask) added to the prediction;
+// dequantised at PQINDEX, or at per-MB mquant with the derived flags (either may be null).
+void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, const uint8_t* block_types,
+                     const uint8_t* mquant, const uint8_t* derived, void* dst) {
     auto& e = E(h);
     const auto& c = static_cast<RefEncoder*>(h)->cfg;
     const int mbw = (c.width + 15) / 16, mbh = (c.height + 15) / 16;
@@ -357,7 +359,8 @@ void ref_reconstruct(void* h, void* pred, const int16_t* levels, int type_mask, 
                     std::array<int, 64> q{};
                     for (int y = 0; y < bh; ++y)
                         for (int x = 0; x < bw; ++x) q[y * 8 + x] = q64[(oy + y) * 8 + ox + x];
-                    const auto r = e.inverse_partition(type, q, c.pqindex, false);
+                    const auto r = e.inverse_partition(type, q, mquant ? mquant[mb] : c.pqindex,
+                                                       derived ? derived[mb] != 0 : false);
                     for (int y = 0; y < bh; ++y)
                         for (int x = 0; x < bw; ++x) residual[(oy + y) * 8 + ox + x] = r[y * 8 + x];
                 }

@@ -86,3 +86,41 @@ def test_reconstruction_rejects_a_type_outside_the_mask(ctx):
     ctx.reconstruct(p, 1, lv.data_ptr(), 1, np.ones((12, 6), np.uint8), 2)
     for got, want in zip(ctx.download_frame(2, 64, 48), clip.frame(0)):
         assert np.array_equal(got, want)  # zero levels reproduce the prediction
+
+
+DQUANT_RASTERS = [(176, 144, 7, 0, 1), (98, 66, 6, 1, 0), (130, 98, 14, 0, 0)]
+
+
+@pytest.mark.parametrize("raster", DQUANT_RASTERS)
+def test_reconstruction_under_dquant_matches_reference(ctx, raster):
+    """vc1cu_reconstruct_dquant against the reference's inverse_partition at each MB's MQUANT
+    (derived flags drop the HALFQP half step), every transform type, random sparse levels."""
+    import torch
+
+    from oracle.bindings import Reference, ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    w, h, pq, nu, hq = raster
+    p = make_params(w, h, pqindex=pq, nonuniform=nu, halfqp=hq)
+    mbw, mbh = (w + 15) // 16, (h + 15) // 16
+    mbs = mbw * mbh
+    rng = np.random.default_rng(w + pq)
+    pred = synth.generate(w, h, 1, pq).frame(0)
+    levels = (rng.integers(-24, 25, (4, mbs, 6, 64)) * (rng.random((4, mbs, 6, 64)) < 0.15)).astype(np.int16)
+    levels[:, :, :, 0] = rng.integers(-60, 61, (4, mbs, 6))
+    dc_only = rng.random((4, mbs, 6)) < 0.2  # the DC-only shortcut
+    levels[:, :, :, 1:][dc_only] = 0
+    types = rng.integers(1, 5, (mbs, 6)).astype(np.uint8)
+    mq = rng.integers(1, 32, mbs).astype(np.uint8)
+    mq[::5] = pq  # PQINDEX, with and without the derived flag
+    der = (rng.random(mbs) < 0.5).astype(np.uint8)
+    ctx.upload_frame(1, *pred)
+    lv = _device(levels)
+    ctx.reconstruct(p, 1, lv.data_ptr(), 15, types, 2, mquant=mq, derived=der)
+    got = ctx.download_frame(2, w, h)
+    want = Reference(p).reconstruct(pred, levels, 15, types, mq, der)
+    for g, e, c in zip(got, want, "yuv"):
+        assert np.array_equal(g, e), (c, np.argwhere(g != e)[:4])
+    plain = Reference(p).reconstruct(pred, levels, 15, types)
+    assert any(not np.array_equal(a, b) for a, b in zip(want, plain))
