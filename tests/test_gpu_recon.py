@@ -124,3 +124,19 @@ def test_reconstruction_under_dquant_matches_reference(ctx, raster):
         assert np.array_equal(g, e), (c, np.argwhere(g != e)[:4])
     plain = Reference(p).reconstruct(pred, levels, 15, types)
     assert any(not np.array_equal(a, b) for a, b in zip(want, plain))
+
+
+def test_dquant_reconstruction_rejects_mquant_outside_1_to_31(ctx):
+    p = make_params(64, 48, pqindex=8, search_range=8, local_search_range=8)
+    ctx.upload_frame(1, *synth.generate(64, 48, 1, 3).frame(0))
+    lv = _device(np.zeros((1, 12, 6, 64), np.int16))
+    mq = np.full(12, 8, np.uint8)
+    mq[5] = 0
+    with pytest.raises(Vc1cuError):
+        ctx.reconstruct(p, 1, lv.data_ptr(), 1, np.ones((12, 6), np.uint8), 2, mquant=mq)
+    mq[5] = 32
+    with pytest.raises(Vc1cuError):
+        ctx.reconstruct(p, 1, lv.data_ptr(), 1, np.ones((12, 6), np.uint8), 2, mquant=mq)
+    mq[5] = 31
+    ctx.reconstruct(p, 1, lv.data_ptr(), 1, np.ones((12, 6), np.uint8), 2, mquant=mq)
+    ctx.synchronize()
