@@ -1378,7 +1378,7 @@ __device__ __forceinline__ int intra_mq(const IntraArgs& A, int mb) {
 // One thread per (MB, block): forward_transform (:672-795; samples outside the source read the
 // pad value, 0 luma / 128 chroma, minus 128), the AC levels of quantize_ac (:2090-2144: scalar, or
 // the trellis along the intra scan from position 1 with the intra-family rates and the perceptual
-// lambda scale of the block, chroma judged against the intra source's luma) and
+// lambda scale of the block, chroma weighed against the intra source's luma) and
 // choose_dc_for_mean of the padded block mean.
 __global__ void intra_fwd_kernel(const __grid_constant__ IntraArgs A) {
     const DevParams& P = A.P;
